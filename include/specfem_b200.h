@@ -1,0 +1,241 @@
+/*
+ * specfem_b200.h -- C ABI of the B200-native SEM time-marching path.
+ *
+ * The library replaces the device side of SPECFEM++'s 2D time-marching path:
+ * `specfem::kokkos_kernels::domain_kernels`, the Newmark `time_scheme`,
+ * `specfem::kokkos_kernels::frechet_kernels` and the loop of
+ * `specfem::solver::time_marching`.  The reference interfaces are C++ class
+ * templates; each entry point below names the member function it stands in
+ * for.  All entry points return 0 on success and a negative SFB_E* code on
+ * failure; sfb_last_error() gives the message.  Buffers passed in are
+ * caller-owned host memory; device memory is owned by the context.  One
+ * context = one CUDA stream; a context is not thread-safe.
+ *
+ * Integer tags equal the reference's enum ordinals:
+ *   medium   (include/enumerations/medium.hpp:39):  0 elastic_psv,
+ *            1 elastic_sh, 3 acoustic
+ *   boundary (include/enumerations/medium.hpp:61):  0 none,
+ *            1 acoustic_free_surface, 2 stacey, 3 composite_stacey_dirichlet
+ *   seismogram type (include/enumerations/wavefield.hpp:17): 0 displacement,
+ *            1 velocity, 2 acceleration, 3 pressure
+ *   wavefield (include/enumerations/wavefield.hpp simulation_field):
+ *            0 forward, 1 adjoint, 2 backward
+ */
+#ifndef SPECFEM_B200_H
+#define SPECFEM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+#define SFB_API extern "C" __attribute__((visibility("default")))
+#else
+#define SFB_API __attribute__((visibility("default")))
+#endif
+
+#define SFB_OK 0
+#define SFB_E_INVALID -1     /* bad argument / unsupported configuration      */
+#define SFB_E_CUDA -2        /* CUDA runtime error                             */
+#define SFB_E_IO -3          /* file not found / unreadable / malformed        */
+#define SFB_E_STATE -4       /* call out of order (e.g. step before init)      */
+#define SFB_E_ACCOUNTING -5  /* DOF / element accounting mismatch              */
+#define SFB_E_NONFINITE -6   /* wavefield watchdog saw NaN/Inf                 */
+#define SFB_E_NOMEM -7       /* device allocation failed                       */
+
+#define SFB_WAVEFIELD_FORWARD 0
+#define SFB_WAVEFIELD_ADJOINT 1
+#define SFB_WAVEFIELD_BACKWARD 2
+
+typedef struct sfb_context sfb_context;
+
+/* ---------------------------------------------------------------------------
+ * Problem description for a structured mesh (the benchmark workloads).  The
+ * reference builds the same objects from xmeshfem2D output
+ * (src/io/mesh/impl/fortran/dim2/mesh.cpp:26) and the YAML source / station
+ * files (src/io/sources.cpp:25, src/io/receivers.cpp).
+ * ------------------------------------------------------------------------- */
+typedef struct sfb_material {
+  double rho, vp, vs; /* vs == 0 marks an acoustic material */
+} sfb_material;
+
+typedef struct sfb_source_desc {
+  int kind;        /* 0 force, 1 moment tensor                              */
+  int shot;        /* shot index in [0, nshots)                              */
+  int wavefield;   /* 0: forward (backward in combined runs), 1: adjoint     */
+  int stf;         /* 0 Ricker, 1 Dirac, 2 dGaussian, 3 table                */
+  double x, z;
+  double angle;    /* force direction in degrees (0 = -z, as the reference)  */
+  double mxx, mzz, mxz;
+  double f0, tshift, factor;
+  const float *stf_table; /* stf == 3: [nstep][ncomp] samples, else NULL     */
+} sfb_source_desc;
+
+typedef struct sfb_receiver_desc {
+  const char *network, *station;
+  double x, z, angle;
+} sfb_receiver_desc;
+
+typedef struct sfb_structured_desc {
+  int nx, nz;                  /* elements along x and z                    */
+  double x0, x1, z0, z1;       /* domain                                    */
+  int absorb[4];               /* Stacey on bottom, right, top, left        */
+  int ngll;                    /* 5 (GLL4)                                  */
+  int elastic_sh;              /* 1: elastic elements carry SH waves        */
+  int nmaterials;
+  const sfb_material *materials;
+  const int *element_material; /* [nx*nz], element ispec = iz*nx + ix       */
+  /* Optional per-GLL-point model [nx*nz][ngll][ngll] (NULL = per element). */
+  const float *gll_rho, *gll_vp, *gll_vs;
+  double dt;
+  int nstep;
+  double t0;                   /* 0: derive from sources (reference rule)   */
+  int nshots;                  /* independent wavefields advanced together  */
+  int nsources;
+  const sfb_source_desc *sources;
+  int nreceivers;
+  const sfb_receiver_desc *receivers;
+  int nseismogram_types;
+  const int *seismogram_types;
+  int nstep_between_samples;
+  int simulation;              /* 0 forward, 1 combined (adjoint+backward)  */
+  int save_boundary_values;    /* forward: keep the Stacey replay store     */
+} sfb_structured_desc;
+
+/* ---- context life cycle (replaces specfem::compute::assembly) ---------- */
+
+/* Build from a reference YAML parameter file (src/specfem2d.cpp:3-38,
+ * src/parameter_parser/setup.cpp): reads the mesh database, sources and
+ * stations it names.  `default_file` may be NULL. */
+SFB_API int sfb_create_from_yaml(const char *parameter_file,
+                                 const char *default_file, sfb_context **out);
+SFB_API int sfb_create_structured(const sfb_structured_desc *desc,
+                                  sfb_context **out);
+SFB_API void sfb_destroy(sfb_context *ctx);
+/* Message of the last failure on `ctx` (or of the last failed create when
+ * ctx is NULL).  Valid until the next call on the same context. */
+SFB_API const char *sfb_last_error(const sfb_context *ctx);
+
+typedef struct sfb_info {
+  int ngll, nspec, nshots, nstep, nstep_between_samples, max_sig_step;
+  int nglob[4];          /* DOF points per medium tag                        */
+  int nelements[4];      /* elements per medium tag                          */
+  int nreceivers, nseismogram_types, nsources;
+  int simulation;        /* 0 forward, 1 combined                            */
+  double dt, t0;
+  size_t device_bytes;   /* device memory held by the context                */
+} sfb_info;
+SFB_API int sfb_get_info(const sfb_context *ctx, sfb_info *info);
+
+/* ---- domain_kernels (include/kokkos_kernels/domain_kernels.hpp) -------- */
+
+/* domain_kernels::initialize(dt) (:136-163): mass matrix (FP64 accumulation,
+ * FP32 inverse) for every medium of `wavefield`. */
+SFB_API int sfb_domain_initialize(sfb_context *ctx, int wavefield, double dt);
+/* domain_kernels::update_wavefields<medium>(istep) (:68-126): coupling,
+ * sources, stiffness (+ Stacey / free surface), divide by mass.  Writes the
+ * number of elements updated. */
+SFB_API int sfb_domain_update_wavefields(sfb_context *ctx, int wavefield,
+                                         int medium, int istep,
+                                         int *elements_updated);
+/* domain_kernels::compute_seismograms(isig_step) (:175-186). */
+SFB_API int sfb_domain_compute_seismograms(sfb_context *ctx, int wavefield,
+                                           int isig_step);
+
+/* ---- time_scheme::newmark (include/timescheme/newmark.tpp) ------------- */
+
+/* apply_predictor_phase_{forward,backward}(medium) (:60-117, :221-242) and
+ * apply_corrector_phase_{forward,backward}(medium) (:11-56, :181-199); the
+ * backward wavefield uses -dt.  Writes the number of DOFs updated. */
+SFB_API int sfb_newmark_predictor(sfb_context *ctx, int wavefield, int medium,
+                                  int *dofs_updated);
+SFB_API int sfb_newmark_corrector(sfb_context *ctx, int wavefield, int medium,
+                                  int *dofs_updated);
+
+/* ---- frechet_kernels::compute_derivatives(dt)
+ *      (include/kokkos_kernels/frechet_kernels.hpp:29-49) ---------------- */
+SFB_API int sfb_frechet_compute_derivatives(sfb_context *ctx, double dt);
+
+/* ---- solver::time_marching::run (include/solver/time_marching.tpp) ----- */
+
+/* Forward loop, fused: one stiffness launch per medium and one update
+ * launch per step, optionally captured once into a CUDA graph
+ * (use_graph != 0).  Runs `nstep` steps starting at the context's current
+ * step (`time_marching<forward>::run`, :9-124). */
+SFB_API int sfb_run_forward(sfb_context *ctx, int nstep, int use_graph);
+/* The same loop through the reference-granularity entry points above
+ * (predictor / update_wavefields / corrector per medium), with the
+ * reference's DOF and element accounting checks (:90-108). */
+SFB_API int sfb_run_forward_unfused(sfb_context *ctx, int nstep);
+/* Combined adjoint + backward loop with Frechet accumulation
+ * (`time_marching<combined>::run`, :126-247).  Needs the forward run's last
+ * state and Stacey replay store (sfb_copy_forward_to_backward). */
+SFB_API int sfb_run_combined(sfb_context *ctx, int nstep, int use_graph);
+
+/* ---- data movement ------------------------------------------------------ */
+
+/* Seismograms [max_sig_step][ntypes][nreceivers][2] per shot, in the
+ * reference's receiver frame after the angle rotation; `shot` selects the
+ * wavefield copy.  count = number of floats the buffer holds. */
+SFB_API int sfb_get_seismograms(const sfb_context *ctx, int wavefield,
+                                int shot, float *host, size_t count);
+/* Field arrays of one medium: which = 0 displacement, 1 velocity,
+ * 2 acceleration, 3 inverse mass; layout [ncomp][nglob] for `shot`. */
+SFB_API int sfb_get_field(const sfb_context *ctx, int wavefield, int medium,
+                          int which, int shot, float *host, size_t count);
+SFB_API int sfb_set_field(sfb_context *ctx, int wavefield, int medium,
+                          int which, int shot, const float *host,
+                          size_t count);
+/* Replace the adjoint source time functions (combined runs):
+ * [nstep][nreceivers][2] for `shot`, receiver r acting at its station. */
+SFB_API int sfb_set_adjoint_sources(sfb_context *ctx, int shot,
+                                    const float *host, size_t count);
+/* Frechet kernels summed over shots, per local point [nspec][ngll][ngll]:
+ * which = 0 rho, 1 mu, 2 kappa, 3 rhop, 4 alpha, 5 beta (elastic) or
+ * 0 rho, 1 kappa (acoustic points).  FP64. */
+SFB_API int sfb_get_kernels(const sfb_context *ctx, int which, double *host,
+                            size_t count);
+/* Move the forward run's end state and Stacey replay store into the
+ * backward wavefield of `dst` (reference: wavefield writer / reader tasks,
+ * include/io/wavefield/{writer,reader}.tpp). */
+SFB_API int sfb_copy_forward_to_backward(const sfb_context *src,
+                                         sfb_context *dst);
+/* Write the seismograms as the reference's ASCII traces
+ * (src/io/seismogram/writer.cpp:23-88) into `directory`. */
+SFB_API int sfb_write_seismograms(const sfb_context *ctx, int wavefield,
+                                  int shot, const char *directory);
+
+/* ---- problem export (host arrays; valid while the context lives) ------- */
+
+/* Flat host view of the assembled problem, for checkers and tools that need
+ * the same discrete inputs the device kernels read. */
+typedef struct sfb_problem_view {
+  int ngll, nspec, nshots, nstep, nstep_between_samples;
+  double dt, t0;
+  const double *xi, *wgll, *hprime; /* [ngll], [ngll], [ngll*ngll] l_j'(xi_i) */
+  const int *medium;                /* [nspec]                                */
+  const int *iglob;                 /* [nloc] index in own medium's field    */
+  int nglob[4];
+  const float *xix, *xiz, *gammax, *gammaz, *jacobian;   /* [nloc] */
+  const float *kappa, *mu, *rho, *rho_inverse;           /* [nloc] */
+  const uint8_t *bnd;               /* [nloc] bit0 Stacey, bit1 free surface */
+  const float *bnd_nx, *bnd_nz, *bnd_w;                  /* [nloc] */
+  int ncouple_acoustic, ncouple_elastic;
+  const int *couple_acoustic_self, *couple_acoustic_other; /* iglob pairs    */
+  const float *couple_acoustic_factor, *couple_acoustic_nx, *couple_acoustic_nz;
+  const int *couple_elastic_self, *couple_elastic_other;
+  const float *couple_elastic_factor, *couple_elastic_nx, *couple_elastic_nz;
+  int nsources;
+  const int *src_ispec, *src_shot, *src_wavefield;       /* [nsources]      */
+  const float *src_array;           /* [nsources][2][ngll][ngll]             */
+  const float *src_stf;             /* [nsources][nstep][2]                  */
+  int nreceivers;
+  const int *rec_ispec;             /* [nreceivers]                          */
+  const float *rec_lagrange;        /* [nreceivers][ngll][ngll]              */
+  const float *rec_sin, *rec_cos;   /* [nreceivers]                          */
+  int nseismogram_types;
+  const int *seismogram_types;
+} sfb_problem_view;
+SFB_API int sfb_get_problem_view(const sfb_context *ctx,
+                                 sfb_problem_view *view);
+
+#endif /* SPECFEM_B200_H */

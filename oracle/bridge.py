@@ -1,0 +1,80 @@
+"""ORACLE (test infrastructure): Python bridge to ``oracle/_build/liboracle.so``.
+
+Only tests, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+``bench.py`` import this module, as the checker.  It runs the CPU
+restatement of the reference on the problem view exported by a product
+``Simulation`` so both sides start from identical discrete inputs.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "_build", "liboracle.so")
+_lib = None
+
+
+def build():
+    r = subprocess.run(["make", "-C", HERE], capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("oracle build failed:\n" + r.stdout + r.stderr)
+    return LIB
+
+
+def load():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        lib = C.CDLL(LIB)
+        lib.oracle_forward.restype = C.c_int
+        lib.oracle_forward.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int,
+                                       C.POINTER(C.c_float), C.POINTER(C.POINTER(C.c_float)),
+                                       C.POINTER(C.c_float)]
+        lib.oracle_last_error.restype = C.c_char_p
+        _lib = lib
+    return _lib
+
+
+def forward(sim, precision: int = 32, shot: int = 0, nstep=None, threads: int = 1,
+            want_fields: bool = False, want_stacey: bool = False):
+    """Run the oracle forward on ``sim``'s problem.  Returns a dict with
+    ``seismograms`` [nsig][ntypes][nrec][2] and optionally the final fields
+    (keys ``psv``, ``sh``, ``acoustic`` -> (u, v, a, minv) arrays [nc][nglob])."""
+    lib = load()
+    view = sim.problem_view()
+    info = sim.info()
+    if nstep is None:
+        nstep = info.nstep
+    seis = np.zeros((info.max_sig_step, info.nseismogram_types, info.nreceivers, 2), dtype=np.float32)
+    fields = {}
+    ptrs = (C.POINTER(C.c_float) * 12)()
+    bufs = []
+    if want_fields:
+        k = 0
+        for name, med, nc in (("psv", 0, 2), ("sh", 1, 1), ("acoustic", 3, 1)):
+            arrs = [np.zeros((nc, info.nglob[med]), dtype=np.float32) for _ in range(4)]
+            fields[name] = arrs
+            for a in arrs:
+                ptrs[k] = a.ctypes.data_as(C.POINTER(C.c_float))
+                bufs.append(a)
+                k += 1
+    store = None
+    if want_stacey:
+        store = np.zeros((nstep, info.nspec, info.ngll, info.ngll, 2), dtype=np.float32)
+    rc = lib.oracle_forward(C.addressof(view), precision, shot, nstep, threads,
+                            seis.ctypes.data_as(C.POINTER(C.c_float)),
+                            ptrs if want_fields else None,
+                            store.ctypes.data_as(C.POINTER(C.c_float)) if store is not None else None)
+    if rc != 0:
+        raise RuntimeError("oracle failed: " + lib.oracle_last_error().decode())
+    out = {"seismograms": seis}
+    if want_fields:
+        out.update(fields)
+    if store is not None:
+        out["stacey_store"] = store
+    return out

@@ -1,0 +1,527 @@
+// ORACLE -- test infrastructure only.  A CPU restatement of SPECFEM++'s 2D
+// time-marching path, used by the tests, the smoke check and the CPU
+// baseline leg of bench.py as the checker.  It is never linked into, loaded
+// by or called from the product library.
+//
+// It consumes the flat problem view the product exports
+// (sfb_get_problem_view in include/specfem_b200.h) so that both sides start
+// from identical discrete inputs, and restates, in the reference's step
+// order and operation order:
+//   time loop        include/solver/time_marching.tpp:9-124 (forward),
+//                    :126-247 (combined)
+//   Newmark          include/timescheme/newmark.tpp:11-117, 181-242
+//   update_wavefields include/kokkos_kernels/domain_kernels.hpp:68-126
+//   stiffness        include/kokkos_kernels/impl/compute_stiffness_interaction.tpp:140-260
+//   gradient         include/algorithms/gradient.hpp:36-111
+//   divergence       include/algorithms/divergence.hpp:40-103
+//   stress           include/medium/dim2/elastic/isotropic/stress.hpp:14-85,
+//                    include/medium/dim2/acoustic/isotropic/stress.hpp:15-31
+//   F = J T d(xi)/dx core/specfem/point/stress.hpp:117-139
+//   Stacey           include/boundary_conditions/stacey/stacey.tpp:41-250, 625-677
+//   free surface     include/boundary_conditions/dirichlet/dirichlet.hpp:19-43
+//   mass matrix      include/kokkos_kernels/impl/compute_mass_matrix.tpp:80-113,
+//                    invert_mass_matrix.tpp:40-47, divide_mass_matrix.tpp:40-49
+//   sources          include/kokkos_kernels/impl/compute_source_interaction.tpp:77-95
+//   coupling         include/coupled_interface/coupled_interface.tpp:55-86,
+//                    impl/compute_coupling.hpp:22-56
+//   seismograms      include/kokkos_kernels/impl/compute_seismogram.tpp:98-135,
+//                    include/medium/dim2/*/isotropic/wavefield.hpp,
+//                    include/compute/receivers/receivers.hpp:126-141 (rotation)
+//   Frechet kernels  include/kokkos_kernels/impl/compute_material_derivatives.tpp:84-153,
+//                    include/medium/dim2/elastic/isotropic/frechet_derivative.hpp:14-196,
+//                    include/medium/dim2/acoustic/isotropic/frechet_derivative.hpp:12-41
+// Templated on the arithmetic type: float restates the reference's FP32
+// build, double gives the FP64 oracle of the same discrete problem.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#include "../include/specfem_b200.h"
+
+namespace {
+
+constexpr int ACOUSTIC = 3, PSV = 0, SH = 1;
+
+template <typename T> struct Field {
+  int nglob = 0, nc = 0;
+  std::vector<T> u, v, a, minv;  // [nc][nglob]
+  void init(int n, int c) {
+    nglob = n;
+    nc = c;
+    u.assign(static_cast<size_t>(n) * c, T(0));
+    v = u;
+    a = u;
+    minv = u;
+  }
+};
+
+template <typename T> struct Sim {
+  const sfb_problem_view &pv;
+  int n, nspec, shot;
+  T dt, dt2, dtsq2;
+  Field<T> f[4];  // by medium tag
+  std::vector<T> hp, hpw, w;  // hprime, hprime_wgll(ix,l)=hprime(l,ix)w(l), weights
+  std::vector<std::vector<int>> elems;  // per medium
+  bool store_stacey = false;
+  int istep_store = 0;
+  std::vector<float> *stacey_store = nullptr;  // [nstep][nloc][2] accelerations
+  const std::vector<float> *stacey_replay = nullptr;
+  bool backward = false;
+  int threads = 1;
+  // Optional adjoint sources: [nstep][nrec][2] acting through receiver arrays.
+  const float *adjoint_stf = nullptr;
+
+  Sim(const sfb_problem_view &v, int s) : pv(v), n(v.ngll), nspec(v.nspec), shot(s) {
+    dt = static_cast<T>(v.dt);
+    dt2 = static_cast<T>(v.dt / 2.0);
+    dtsq2 = static_cast<T>(v.dt * v.dt / 2.0);
+    hp.resize(n * n);
+    hpw.resize(n * n);
+    w.resize(n);
+    for (int i = 0; i < n; ++i) w[i] = static_cast<T>(static_cast<float>(v.wgll[i]));
+    for (int i = 0; i < n * n; ++i) hp[i] = static_cast<T>(static_cast<float>(v.hprime[i]));
+    // element_quadrature.hprime_wgll(ix, iz) = hprime(iz, ix) * w(iz)
+    // (include/compute/compute_mesh.hpp:265-277)
+    for (int ix = 0; ix < n; ++ix)
+      for (int l = 0; l < n; ++l) hpw[ix * n + l] = hp[l * n + ix] * w[l];
+    elems.resize(4);
+    for (int e = 0; e < nspec; ++e) elems[v.medium[e]].push_back(e);
+    f[ACOUSTIC].init(v.nglob[ACOUSTIC], 1);
+    f[PSV].init(v.nglob[PSV], 2);
+    f[SH].init(v.nglob[SH], 1);
+  }
+
+  size_t P(int e, int iz, int ix) const { return (static_cast<size_t>(e) * n + iz) * n + ix; }
+
+  // ---- Newmark (newmark.tpp:60-117 predictor, :11-56 corrector) ---------
+  void predictor(int m, T sgn) {
+    Field<T> &F = f[m];
+    const T d = sgn * dt, d2 = sgn * dt2, dsq = dtsq2;
+    for (size_t i = 0; i < F.u.size(); ++i) {
+      F.u[i] += d * F.v[i] + dsq * F.a[i];
+      F.v[i] += d2 * F.a[i];
+      F.a[i] = T(0);
+    }
+  }
+  void corrector(int m, T sgn) {
+    Field<T> &F = f[m];
+    const T d2 = sgn * dt2;
+    for (size_t i = 0; i < F.u.size(); ++i) F.v[i] += d2 * F.a[i];
+  }
+
+  // ---- mass matrix (compute_mass_matrix.tpp, stacey.tpp:644-677) --------
+  void stacey_terms(int m, size_t p, const T *vel, T *out) const {
+    const T nx = pv.bnd_nx[p], nz = pv.bnd_nz[p], we = pv.bnd_w[p];
+    const T jac1d = std::sqrt(nx * nx + nz * nz);
+    if (m == PSV) {
+      const T kappa = pv.kappa[p], mu = pv.mu[p], rho = pv.rho[p];
+      const T l2m = kappa + static_cast<T>(static_cast<float>(4.0 / 3.0)) * mu;
+      const T rho_vp = std::sqrt(l2m / rho) * rho;
+      const T rho_vs = std::sqrt(rho * mu);
+      const T vn = vel[0] * nx + vel[1] * nz;
+      const T dn[2] = {nx, nz};
+      for (int c = 0; c < 2; ++c) {
+        const T fac = ((vn * dn[c] / (jac1d * jac1d)) * (rho_vp - rho_vs)) + vel[c] * rho_vs;
+        out[c] += T(-1) * fac * jac1d * we;
+      }
+    } else if (m == SH) {
+      const T rho_vs = std::sqrt(static_cast<T>(pv.rho[p]) * static_cast<T>(pv.mu[p]));
+      const T fac = we * jac1d;
+      out[0] += T(-1) * fac * rho_vs * vel[0];
+    } else {
+      const T rvi = std::sqrt(static_cast<T>(pv.rho_inverse[p]) * (T(1) / static_cast<T>(pv.kappa[p])));
+      const T fac = we * jac1d;
+      out[0] += T(-1) * fac * rvi * vel[0];
+    }
+  }
+
+  void init_mass() {
+    for (int m : {ACOUSTIC, PSV, SH}) {
+      Field<T> &F = f[m];
+      std::vector<double> mass(F.minv.size(), 0.0);
+      std::vector<T> massT(F.minv.size(), T(0));
+      for (int e : elems[m])
+        for (int iz = 0; iz < n; ++iz)
+          for (int ix = 0; ix < n; ++ix) {
+            const size_t p = P(e, iz, ix);
+            T mm[2];
+            const T base = (m == ACOUSTIC) ? T(1) / static_cast<T>(pv.kappa[p]) : static_cast<T>(pv.rho[p]);
+            for (int c = 0; c < F.nc; ++c) mm[c] = base * (w[ix] * w[iz] * static_cast<T>(pv.jacobian[p]));
+            if (pv.bnd[p] & 1) {
+              const T vf[2] = {T(-1) * dt * T(0.5), T(-1) * dt * T(0.5)};
+              stacey_terms(m, p, vf, mm);
+            }
+            const int g = pv.iglob[p];
+            for (int c = 0; c < F.nc; ++c) massT[static_cast<size_t>(c) * F.nglob + g] += mm[c];
+          }
+      for (size_t i = 0; i < massT.size(); ++i) F.minv[i] = T(1) / massT[i];
+    }
+  }
+
+  // ---- stiffness (compute_stiffness_interaction.tpp:140-260) ------------
+  void stiffness(int m, int istep) {
+    Field<T> &F = f[m];
+    const int nc = F.nc;
+    const std::vector<int> &E = elems[m];
+    const int nn = n * n;
+    if (backward && stacey_replay) {
+      // Stacey elements replay the stored element-local acceleration
+      // (:123-137); other elements are computed below.
+    }
+#pragma omp parallel for num_threads(threads) schedule(static)
+    for (long ie = 0; ie < static_cast<long>(E.size()); ++ie) {
+      const int e = E[ie];
+      T u[8 * 8 * 2], Fs[8 * 8 * 2 * 2];
+      bool replay = false;
+      if (backward && stacey_replay) {
+        for (int k = 0; k < nn && !replay; ++k) replay = pv.bnd[static_cast<size_t>(e) * nn + k] & 1;
+        // Only elements carrying Stacey points are replayed; the reference
+        // keys this on the element boundary tag (stacey or composite).
+      }
+      if (replay) {
+        for (int k = 0; k < nn; ++k) {
+          const size_t p = static_cast<size_t>(e) * nn + k;
+          const float *src = &(*stacey_replay)[(static_cast<size_t>(istep) * pv.nspec * nn + p) * 2];
+          const int g = pv.iglob[p];
+          for (int c = 0; c < nc; ++c) {
+            T val = static_cast<T>(src[c]);
+#pragma omp atomic
+            F.a[static_cast<size_t>(c) * F.nglob + g] += val;
+          }
+        }
+        continue;
+      }
+      for (int k = 0; k < nn; ++k) {
+        const int g = pv.iglob[static_cast<size_t>(e) * nn + k];
+        for (int c = 0; c < nc; ++c) u[k * nc + c] = F.u[static_cast<size_t>(c) * F.nglob + g];
+      }
+      // gradient + stress + stress integrand
+      for (int iz = 0; iz < n; ++iz)
+        for (int ix = 0; ix < n; ++ix) {
+          const size_t p = P(e, iz, ix);
+          T dxi[2] = {T(0), T(0)}, dga[2] = {T(0), T(0)};
+          for (int l = 0; l < n; ++l)
+            for (int c = 0; c < nc; ++c) {
+              dxi[c] += hp[ix * n + l] * u[(iz * n + l) * nc + c];
+              dga[c] += hp[iz * n + l] * u[(l * n + ix) * nc + c];
+            }
+          const T xix = pv.xix[p], xiz = pv.xiz[p], gax = pv.gammax[p], gaz = pv.gammaz[p];
+          const T J = pv.jacobian[p];
+          T du[2][2];
+          for (int c = 0; c < nc; ++c) {
+            du[c][0] = xix * dxi[c] + gax * dga[c];
+            du[c][1] = xiz * dxi[c] + gaz * dga[c];
+          }
+          T Tm[2][2];
+          if (m == PSV) {
+            const T kappa = pv.kappa[p], mu = pv.mu[p];
+            const T l2m = kappa + static_cast<T>(static_cast<float>(4.0 / 3.0)) * mu;
+            const T lam = l2m - T(2) * mu;
+            const T sxx = l2m * du[0][0] + lam * du[1][1];
+            const T szz = l2m * du[1][1] + lam * du[0][0];
+            const T sxz = mu * (du[0][1] + du[1][0]);
+            Tm[0][0] = sxx;
+            Tm[0][1] = sxz;
+            Tm[1][0] = sxz;
+            Tm[1][1] = szz;
+          } else if (m == SH) {
+            const T mu = pv.mu[p];
+            Tm[0][0] = mu * du[0][0];
+            Tm[0][1] = mu * du[0][1];
+          } else {
+            const T ri = pv.rho_inverse[p];
+            Tm[0][0] = ri * du[0][0];
+            Tm[0][1] = ri * du[0][1];
+          }
+          const int k = iz * n + ix;
+          for (int c = 0; c < nc; ++c) {
+            Fs[(k * nc + c) * 2 + 0] = J * (Tm[c][0] * xix + Tm[c][1] * xiz);
+            Fs[(k * nc + c) * 2 + 1] = J * (Tm[c][0] * gax + Tm[c][1] * gaz);
+          }
+        }
+      // divergence, sign, boundary conditions, scatter
+      for (int iz = 0; iz < n; ++iz)
+        for (int ix = 0; ix < n; ++ix) {
+          const size_t p = P(e, iz, ix);
+          T t1[2] = {T(0), T(0)}, t2[2] = {T(0), T(0)};
+          for (int l = 0; l < n; ++l)
+            for (int c = 0; c < nc; ++c) {
+              t1[c] += Fs[((iz * n + l) * nc + c) * 2 + 0] * hpw[ix * n + l];
+              t2[c] += Fs[((l * n + ix) * nc + c) * 2 + 1] * hpw[iz * n + l];
+            }
+          T acc[2];
+          for (int c = 0; c < nc; ++c) acc[c] = (w[iz] * t1[c] + w[ix] * t2[c]) * T(-1);
+          const uint8_t b = pv.bnd[p];
+          const int g = pv.iglob[p];
+          if (b & 1) {
+            T vel[2];
+            for (int c = 0; c < nc; ++c) vel[c] = F.v[static_cast<size_t>(c) * F.nglob + g];
+            stacey_terms(m, p, vel, acc);
+          }
+          if (b & 2)
+            for (int c = 0; c < nc; ++c) acc[c] = T(0);
+          if (store_stacey && stacey_store) {
+            // Forward runs keep the element-local acceleration of every
+            // point of a Stacey element (compute_stiffness_interaction.tpp:251-255).
+            bool stacey_elem = false;
+            for (int k = 0; k < nn && !stacey_elem; ++k) stacey_elem = pv.bnd[static_cast<size_t>(e) * nn + k] & 1;
+            if (stacey_elem) {
+              float *dst = &(*stacey_store)[(static_cast<size_t>(istep) * pv.nspec * nn + p) * 2];
+              for (int c = 0; c < nc; ++c) dst[c] = static_cast<float>(acc[c]);
+            }
+          }
+          for (int c = 0; c < nc; ++c) {
+#pragma omp atomic
+            F.a[static_cast<size_t>(c) * F.nglob + g] += acc[c];
+          }
+        }
+    }
+  }
+
+  // ---- sources (compute_source_interaction.tpp:77-95) --------------------
+  void sources(int m, int istep, int wavefield_sel) {
+    Field<T> &F = f[m];
+    for (int s = 0; s < pv.nsources; ++s) {
+      if (pv.src_shot[s] != shot || pv.src_wavefield[s] != wavefield_sel) continue;
+      const int e = pv.src_ispec[s];
+      if (pv.medium[e] != m) continue;
+      for (int iz = 0; iz < n; ++iz)
+        for (int ix = 0; ix < n; ++ix) {
+          const size_t p = P(e, iz, ix);
+          const int g = pv.iglob[p];
+          for (int c = 0; c < F.nc; ++c) {
+            const T stf = pv.src_stf[(static_cast<size_t>(s) * pv.nstep + istep) * 2 + c];
+            const T arr = pv.src_array[((static_cast<size_t>(s) * 2 + c) * n + iz) * n + ix];
+            T val = stf * arr;
+            if (m == ACOUSTIC) val = stf * arr / static_cast<T>(pv.kappa[p]);
+            F.a[static_cast<size_t>(c) * F.nglob + g] += val;
+          }
+        }
+    }
+  }
+
+  // Adjoint sources: receiver r injects stf[istep][r][c] * lagrange.
+  void adjoint_sources(int m, int istep) {
+    if (!adjoint_stf) return;
+    Field<T> &F = f[m];
+    for (int r = 0; r < pv.nreceivers; ++r) {
+      const int e = pv.rec_ispec[r];
+      if (pv.medium[e] != m) continue;
+      for (int iz = 0; iz < n; ++iz)
+        for (int ix = 0; ix < n; ++ix) {
+          const size_t p = P(e, iz, ix);
+          const int g = pv.iglob[p];
+          const T h = pv.rec_lagrange[(static_cast<size_t>(r) * n + iz) * n + ix];
+          for (int c = 0; c < F.nc; ++c) {
+            const T stf = adjoint_stf[(static_cast<size_t>(istep) * pv.nreceivers + r) * 2 + c];
+            T val = stf * h;
+            if (m == ACOUSTIC) val = stf * h / static_cast<T>(pv.kappa[p]);
+            F.a[static_cast<size_t>(c) * F.nglob + g] += val;
+          }
+        }
+    }
+  }
+
+  // ---- coupling (coupled_interface.tpp:55-86) ----------------------------
+  void coupling(int m) {
+    if (m == ACOUSTIC) {
+      Field<T> &S = f[ACOUSTIC];
+      const Field<T> &C = f[PSV];
+      for (int i = 0; i < pv.ncouple_acoustic; ++i) {
+        const int gs = pv.couple_acoustic_self[i], gc = pv.couple_acoustic_other[i];
+        const T fac = pv.couple_acoustic_factor[i];
+        const T nx = pv.couple_acoustic_nx[i], nz = pv.couple_acoustic_nz[i];
+        S.a[gs] += fac * (nx * C.u[gc] + nz * C.u[static_cast<size_t>(C.nglob) + gc]);
+      }
+    } else if (m == PSV) {
+      Field<T> &S = f[PSV];
+      const Field<T> &C = f[ACOUSTIC];
+      for (int i = 0; i < pv.ncouple_elastic; ++i) {
+        const int gs = pv.couple_elastic_self[i], gc = pv.couple_elastic_other[i];
+        const T fac = pv.couple_elastic_factor[i];
+        const T nx = pv.couple_elastic_nx[i], nz = pv.couple_elastic_nz[i];
+        S.a[gs] += fac * nx * C.a[gc];
+        S.a[static_cast<size_t>(S.nglob) + gs] += fac * nz * C.a[gc];
+      }
+    }
+  }
+
+  void divide_mass(int m) {
+    Field<T> &F = f[m];
+    for (size_t i = 0; i < F.a.size(); ++i) F.a[i] = F.a[i] * F.minv[i];
+  }
+
+  // update_wavefields<medium>(istep), domain_kernels.hpp:68-126
+  int update(int m, int istep, int src_sel) {
+    if (elems[m].empty()) return 0;
+    coupling(m);
+    sources(m, istep, src_sel);
+    adjoint_sources(m, istep);
+    stiffness(m, istep);
+    divide_mass(m);
+    return static_cast<int>(elems[m].size());
+  }
+
+  // ---- seismograms (compute_seismogram.tpp, wavefield.hpp) ---------------
+  void seismograms(float *out, int isig) {
+    const int ntypes = pv.nseismogram_types, nrec = pv.nreceivers;
+    for (int r = 0; r < nrec; ++r) {
+      const int e = pv.rec_ispec[r];
+      const int m = pv.medium[e];
+      const Field<T> &F = f[m];
+      for (int it = 0; it < ntypes; ++it) {
+        const int type = pv.seismogram_types[it];
+        T acc[2] = {T(0), T(0)};
+        // wavefield value at every point of the element
+        std::vector<T> wf(static_cast<size_t>(n) * n * 2, T(0));
+        const std::vector<T> *src = &F.u;
+        if (type == 1) src = &F.v;
+        if (type == 2) src = &F.a;
+        const bool need_grad = (m == ACOUSTIC && type != 3) || (m == PSV && type == 3);
+        if (m == ACOUSTIC && type == 3) src = &F.a;
+        if (need_grad) {
+          for (int iz = 0; iz < n; ++iz)
+            for (int ix = 0; ix < n; ++ix) {
+              const size_t p = P(e, iz, ix);
+              T dxi[2] = {T(0), T(0)}, dga[2] = {T(0), T(0)};
+              for (int l = 0; l < n; ++l)
+                for (int c = 0; c < F.nc; ++c) {
+                  dxi[c] += hp[ix * n + l] * (*src)[static_cast<size_t>(c) * F.nglob + pv.iglob[P(e, iz, l)]];
+                  dga[c] += hp[iz * n + l] * (*src)[static_cast<size_t>(c) * F.nglob + pv.iglob[P(e, l, ix)]];
+                }
+              const T xix = pv.xix[p], xiz = pv.xiz[p], gax = pv.gammax[p], gaz = pv.gammaz[p];
+              T du[2][2];
+              for (int c = 0; c < F.nc; ++c) {
+                du[c][0] = xix * dxi[c] + gax * dga[c];
+                du[c][1] = xiz * dxi[c] + gaz * dga[c];
+              }
+              const int k = iz * n + ix;
+              if (m == ACOUSTIC) {
+                const T ri = pv.rho_inverse[p];
+                wf[k * 2 + 0] = ri * du[0][0];
+                wf[k * 2 + 1] = ri * du[0][1];
+              } else {
+                const T kappa = pv.kappa[p], mu = pv.mu[p];
+                const T l2m = kappa + static_cast<T>(static_cast<float>(4.0 / 3.0)) * mu;
+                const T lam = l2m - T(2) * mu;
+                wf[k * 2 + 0] = T(-1) * ((lam + static_cast<T>(2.0 / 3.0) * mu) * (du[0][0] + du[1][1]));
+                wf[k * 2 + 1] = T(0);
+              }
+            }
+        } else {
+          for (int iz = 0; iz < n; ++iz)
+            for (int ix = 0; ix < n; ++ix) {
+              const int g = pv.iglob[P(e, iz, ix)];
+              const int k = iz * n + ix;
+              if (m == ACOUSTIC) {  // pressure: -chi_ddot
+                wf[k * 2 + 0] = T(-1) * (*src)[g];
+                wf[k * 2 + 1] = T(0);
+              } else {
+                wf[k * 2 + 0] = (*src)[g];
+                wf[k * 2 + 1] = F.nc > 1 ? (*src)[static_cast<size_t>(F.nglob) + g] : T(0);
+              }
+            }
+        }
+        for (int k = 0; k < n * n; ++k) {
+          const T h = pv.rec_lagrange[static_cast<size_t>(r) * n * n + k];
+          acc[0] += h * wf[k * 2 + 0];
+          acc[1] += h * wf[k * 2 + 1];
+        }
+        const T s = pv.rec_sin[r], c = pv.rec_cos[r];
+        float *o = out + ((static_cast<size_t>(isig) * ntypes + it) * nrec + r) * 2;
+        o[0] = static_cast<float>(c * acc[0] - s * acc[1]);
+        o[1] = static_cast<float>(s * acc[0] + c * acc[1]);
+      }
+    }
+  }
+
+  // time_marching<forward>::run body (time_marching.tpp:33-89)
+  void forward_step(int istep) {
+    int dofs = 0, elements = 0;
+    for (int m : {ACOUSTIC, PSV, SH}) predictor(m, T(1)), dofs += static_cast<int>(f[m].u.size());
+    elements += update(ACOUSTIC, istep, 0);
+    corrector(ACOUSTIC, T(1));
+    dofs += static_cast<int>(f[ACOUSTIC].u.size());
+    elements += update(PSV, istep, 0);
+    elements += update(SH, istep, 0);
+    corrector(PSV, T(1));
+    corrector(SH, T(1));
+    dofs += static_cast<int>(f[PSV].u.size() + f[SH].u.size());
+    int total_dofs = 0;
+    for (int m : {ACOUSTIC, PSV, SH}) total_dofs += 2 * static_cast<int>(f[m].u.size());
+    if (dofs != total_dofs || elements != nspec)
+      throw std::runtime_error("The time loop has not updated all the degrees of freedom");
+  }
+};
+
+template <typename T>
+int run_forward(const sfb_problem_view *pv, int shot, int nstep, int threads,
+                float *seis, float **fields_out, float *stacey_store_out) {
+  Sim<T> s(*pv, shot);
+  s.threads = threads;
+  std::vector<float> store;
+  if (stacey_store_out) {
+    store.assign(static_cast<size_t>(nstep) * pv->nspec * pv->ngll * pv->ngll * 2, 0.f);
+    s.store_stacey = true;
+    s.stacey_store = &store;
+  }
+  s.init_mass();
+  const int nsbs = pv->nstep_between_samples;
+  const int max_sig = pv->nstep / nsbs;
+  int isig = 0;
+  for (int istep = 0; istep < nstep; ++istep) {
+    s.forward_step(istep);
+    if (istep % nsbs == 0 && isig < max_sig) {
+      if (seis) s.seismograms(seis, isig);
+      ++isig;
+    }
+  }
+  if (fields_out) {
+    int k = 0;
+    for (int m : {PSV, SH, ACOUSTIC}) {
+      for (auto *vec : {&s.f[m].u, &s.f[m].v, &s.f[m].a, &s.f[m].minv}) {
+        if (fields_out[k])
+          for (size_t i = 0; i < vec->size(); ++i) fields_out[k][i] = static_cast<float>((*vec)[i]);
+        ++k;
+      }
+    }
+  }
+  if (stacey_store_out) std::memcpy(stacey_store_out, store.data(), store.size() * sizeof(float));
+  return 0;
+}
+
+thread_local std::string g_err;
+
+}  // namespace
+
+extern "C" {
+
+const char *oracle_last_error() { return g_err.c_str(); }
+
+// Forward run of `shot`, `nstep` steps.  seis: [max_sig_step][ntypes][nrec][2]
+// (may be NULL).  fields_out: 12 pointers (u, v, a, minv for P-SV, SH,
+// acoustic; each may be NULL) of [ncomp][nglob] floats.  stacey_store_out:
+// [nstep][nloc][2] or NULL.  precision: 32 or 64.
+int oracle_forward(const sfb_problem_view *pv, int precision, int shot,
+                   int nstep, int threads, float *seis, float **fields_out,
+                   float *stacey_store_out) {
+  try {
+    if (pv->ngll > 8) throw std::invalid_argument("ngll > 8");
+    if (precision == 64)
+      return run_forward<double>(pv, shot, nstep, threads, seis, fields_out, stacey_store_out);
+    return run_forward<float>(pv, shot, nstep, threads, seis, fields_out, stacey_store_out);
+  } catch (const std::exception &e) {
+    g_err = e.what();
+    return -1;
+  }
+}
+
+}  // extern "C"

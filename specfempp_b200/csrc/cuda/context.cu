@@ -1,0 +1,760 @@
+// C ABI of the SEM time-marching path (include/specfem_b200.h): context life
+// cycle, device upload, the reference-granularity entry points and the fused
+// CUDA-graph driver.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../../include/specfem_b200.h"
+#include "../host/problem.hpp"
+#include "kernels.cuh"
+
+namespace sfb {
+void write_seismograms_ascii(const Problem &P, const float *seis, int ntypes, int nrec,
+                             int max_sig, const std::string &dir);
+}
+
+using namespace sfb;
+
+namespace {
+
+thread_local std::string g_create_error;
+
+struct CudaError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+struct StateError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
+void ck(cudaError_t e, const char *what) {
+  if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <typename T> struct DBuf {
+  T *p = nullptr;
+  size_t n = 0;
+  void alloc(size_t count, size_t *total) {
+    free();
+    n = count;
+    if (count == 0) return;
+    ck(cudaMalloc(&p, count * sizeof(T)), "cudaMalloc");
+    ck(cudaMemset(p, 0, count * sizeof(T)), "cudaMemset");
+    if (total) *total += count * sizeof(T);
+  }
+  void upload(const std::vector<T> &h, size_t *total) {
+    alloc(h.size(), total);
+    if (!h.empty()) ck(cudaMemcpy(p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice), "upload");
+  }
+  void free() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  ~DBuf() { free(); }
+};
+
+constexpr int kMedia[3] = {dev::MED_PSV, dev::MED_SH, dev::MED_AC};
+
+struct WavefieldSet {
+  bool allocated = false;
+  dev::MediumFields f[4];
+  DBuf<float> u[4], v[4], a[4];
+  DBuf<float> seis;
+  DBuf<dev::Control> ctrl;
+  bool initialized = false;
+  int step = 0;  // host copy of the next step index
+};
+
+}  // namespace
+
+struct sfb_context {
+  Problem P;
+  std::string err;
+  bool on_device = false;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  size_t device_bytes = 0;
+  // element permutation: device element d holds mesh element perm[d]
+  std::vector<int> perm, inv;
+  int med_begin[4] = {0, 0, 0, 0}, med_count[4] = {0, 0, 0, 0}, med_interior[4] = {0, 0, 0, 0};
+  DBuf<int> iglob;
+  DBuf<float> xix, xiz, gax, gaz, jac, mat0[4], mat1[4], mat2[4];
+  DBuf<float> mat0_all, mat1_all, mat2_all;
+  DBuf<uint8_t> eflag, bnd;
+  DBuf<float> bnd_nx, bnd_nz, bnd_w;
+  DBuf<float> minv[4];
+  DBuf<double> mass[4];
+  // sources (forward / backward wavefield) and receivers
+  DBuf<int> src_elem, src_shot, src_medium;
+  DBuf<float> src_array, src_stf;
+  int nsrc = 0;
+  DBuf<int> rec_elem;
+  DBuf<float> rec_lag, rec_sin, rec_cos;
+  DBuf<int> cp_ac_self, cp_ac_other, cp_el_self, cp_el_other;
+  DBuf<float> cp_ac_f, cp_ac_nx, cp_ac_nz, cp_el_f, cp_el_nx, cp_el_nz;
+  DBuf<int> step_scratch;  // host-driven step index for the unfused path
+  WavefieldSet wf[3];
+  dev::Static st{};
+  bool mass_ready = false;
+  // Stacey replay store
+  DBuf<float> stacey_data;
+  DBuf<int> stacey_slot;
+  int nstacey = 0;
+  std::vector<float> host_seis;
+  cudaGraphExec_t graph = nullptr;
+  int graph_steps = 0;
+
+  ~sfb_context() {
+    if (graph) cudaGraphExecDestroy(graph);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace {
+
+int fail(sfb_context *ctx, int code, const std::string &msg) {
+  if (ctx) ctx->err = msg;
+  else g_create_error = msg;
+  return code;
+}
+
+template <typename F> int guarded(sfb_context *ctx, F &&fn) {
+  try {
+    return fn();
+  } catch (const CudaError &e) {
+    return fail(ctx, SFB_E_CUDA, e.what());
+  } catch (const StateError &e) {
+    return fail(ctx, SFB_E_STATE, e.what());
+  } catch (const std::invalid_argument &e) {
+    return fail(ctx, SFB_E_INVALID, e.what());
+  } catch (const std::bad_alloc &e) {
+    return fail(ctx, SFB_E_NOMEM, e.what());
+  } catch (const std::exception &e) {
+    const std::string m = e.what();
+    const bool io = m.find("open") != std::string::npos || m.find("database") != std::string::npos ||
+                    m.find("YAML") != std::string::npos;
+    return fail(ctx, io ? SFB_E_IO : SFB_E_INVALID, m);
+  }
+}
+
+int medium_index_ok(int m) { return m == 0 || m == 1 || m == 3; }
+
+void build_permutation(sfb_context *c) {
+  const Assembly &a = c->P.asmb;
+  const int nspec = a.nspec, nn = a.ngll * a.ngll;
+  std::vector<int> has_b(nspec, 0);
+  for (int e = 0; e < nspec; ++e)
+    for (int k = 0; k < nn; ++k)
+      if (a.bnd[static_cast<size_t>(e) * nn + k]) has_b[e] = 1;
+  c->perm.resize(nspec);
+  for (int e = 0; e < nspec; ++e) c->perm[e] = e;
+  auto rank = [](int m) { return m == 0 ? 0 : m == 1 ? 1 : 2; };
+  std::stable_sort(c->perm.begin(), c->perm.end(), [&](int x, int y) {
+    if (rank(a.medium[x]) != rank(a.medium[y])) return rank(a.medium[x]) < rank(a.medium[y]);
+    return has_b[x] < has_b[y];
+  });
+  c->inv.assign(nspec, 0);
+  for (int d = 0; d < nspec; ++d) c->inv[c->perm[d]] = d;
+  for (int m : kMedia) {
+    c->med_begin[m] = 0;
+    c->med_count[m] = 0;
+    c->med_interior[m] = 0;
+  }
+  for (int d = nspec - 1; d >= 0; --d) c->med_begin[a.medium[c->perm[d]]] = d;
+  for (int d = 0; d < nspec; ++d) {
+    const int m = a.medium[c->perm[d]];
+    c->med_count[m]++;
+    if (!has_b[c->perm[d]]) c->med_interior[m]++;
+  }
+}
+
+void ensure_device(sfb_context *c) {
+  if (c->on_device) return;
+  int ndev = 0;
+  const cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0)
+    throw CudaError(std::string("no CUDA device available: ") + cudaGetErrorString(e));
+  ck(cudaGetDevice(&c->device), "cudaGetDevice");
+  ck(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+  const Assembly &a = c->P.asmb;
+  const int n = a.ngll, nn = n * n;
+  const size_t nloc = a.nloc();
+  build_permutation(c);
+  // permuted static arrays
+  std::vector<int> iglob(nloc);
+  std::vector<float> xix(nloc), xiz(nloc), gax(nloc), gaz(nloc), jac(nloc), m0(nloc), m1(nloc),
+      m2(nloc), bnx(nloc), bnz(nloc), bw(nloc);
+  std::vector<uint8_t> bnd(nloc), eflag(a.nspec, 0);
+  for (int d = 0; d < a.nspec; ++d) {
+    const int e = c->perm[d];
+    const int m = a.medium[e];
+    for (int k = 0; k < nn; ++k) {
+      const size_t p = static_cast<size_t>(e) * nn + k, q = static_cast<size_t>(d) * nn + k;
+      iglob[q] = a.iglob[p];
+      xix[q] = a.xix[p];
+      xiz[q] = a.xiz[p];
+      gax[q] = a.gammax[p];
+      gaz[q] = a.gammaz[p];
+      jac[q] = a.jacobian[p];
+      if (m == MEDIUM_ELASTIC_PSV) {
+        m0[q] = a.kappa[p];
+        m1[q] = a.mu[p];
+        m2[q] = a.rho[p];
+      } else if (m == MEDIUM_ELASTIC_SH) {
+        m0[q] = a.mu[p];
+        m1[q] = a.rho[p];
+        m2[q] = 0.f;
+      } else {
+        m0[q] = a.rho_inverse[p];
+        m1[q] = a.kappa[p];
+        m2[q] = 0.f;
+      }
+      bnd[q] = a.bnd[p];
+      bnx[q] = a.bnd_nx[p];
+      bnz[q] = a.bnd_nz[p];
+      bw[q] = a.bnd_w[p];
+      eflag[d] |= a.bnd[p];
+    }
+  }
+  size_t *tot = &c->device_bytes;
+  c->iglob.upload(iglob, tot);
+  c->xix.upload(xix, tot);
+  c->xiz.upload(xiz, tot);
+  c->gax.upload(gax, tot);
+  c->gaz.upload(gaz, tot);
+  c->jac.upload(jac, tot);
+  c->mat0_all.upload(m0, tot);
+  c->mat1_all.upload(m1, tot);
+  c->mat2_all.upload(m2, tot);
+  c->bnd.upload(bnd, tot);
+  c->eflag.upload(eflag, tot);
+  c->bnd_nx.upload(bnx, tot);
+  c->bnd_nz.upload(bnz, tot);
+  c->bnd_w.upload(bw, tot);
+  c->st.ngll = n;
+  c->st.nspec = a.nspec;
+  c->st.iglob = c->iglob.p;
+  c->st.xix = c->xix.p;
+  c->st.xiz = c->xiz.p;
+  c->st.gax = c->gax.p;
+  c->st.gaz = c->gaz.p;
+  c->st.jac = c->jac.p;
+  c->st.mat0 = c->mat0_all.p;
+  c->st.mat1 = c->mat1_all.p;
+  c->st.mat2 = c->mat2_all.p;
+  c->st.eflag = c->eflag.p;
+  c->st.bnd = c->bnd.p;
+  c->st.bnd_nx = c->bnd_nx.p;
+  c->st.bnd_nz = c->bnd_nz.p;
+  c->st.bnd_w = c->bnd_w.p;
+  for (int m : kMedia) {
+    const size_t ld = static_cast<size_t>(a.nglob[m] + (a.nglob[m] & 1)) * a.ncomp(m);
+    c->minv[m].alloc(ld, tot);
+    c->mass[m].alloc(ld, tot);
+  }
+  // quadrature tables
+  std::vector<float> hp(nn), w(n);
+  for (int i = 0; i < nn; ++i) hp[i] = static_cast<float>(a.quad.hprime[i]);
+  for (int i = 0; i < n; ++i) w[i] = static_cast<float>(a.quad.w[i]);
+  dev::set_quadrature(n, hp.data(), w.data());
+  ck(cudaGetLastError(), "set_quadrature");
+  // sources (element ids translated to device order)
+  const Problem &P = c->P;
+  c->nsrc = static_cast<int>(P.v_src_ispec.size());
+  {
+    std::vector<int> el(c->nsrc), sh(c->nsrc), md(c->nsrc);
+    for (int i = 0; i < c->nsrc; ++i) {
+      el[i] = c->inv[P.v_src_ispec[i]];
+      sh[i] = P.v_src_shot[i];
+      md[i] = a.medium[P.v_src_ispec[i]];
+    }
+    c->src_elem.upload(el, tot);
+    c->src_shot.upload(sh, tot);
+    c->src_medium.upload(md, tot);
+    c->src_array.upload(P.v_src_array, tot);
+    c->src_stf.upload(P.v_src_stf, tot);
+  }
+  {
+    std::vector<int> el(P.v_rec_ispec.size());
+    for (size_t i = 0; i < el.size(); ++i) el[i] = c->inv[P.v_rec_ispec[i]];
+    c->rec_elem.upload(el, tot);
+    c->rec_lag.upload(P.v_rec_lagrange, tot);
+    c->rec_sin.upload(P.v_rec_sin, tot);
+    c->rec_cos.upload(P.v_rec_cos, tot);
+  }
+  c->cp_ac_self.upload(P.v_cp_ac_self, tot);
+  c->cp_ac_other.upload(P.v_cp_ac_other, tot);
+  c->cp_ac_f.upload(P.v_cp_ac_f, tot);
+  c->cp_ac_nx.upload(P.v_cp_ac_nx, tot);
+  c->cp_ac_nz.upload(P.v_cp_ac_nz, tot);
+  c->cp_el_self.upload(P.v_cp_el_self, tot);
+  c->cp_el_other.upload(P.v_cp_el_other, tot);
+  c->cp_el_f.upload(P.v_cp_el_f, tot);
+  c->cp_el_nx.upload(P.v_cp_el_nx, tot);
+  c->cp_el_nz.upload(P.v_cp_el_nz, tot);
+  c->step_scratch.alloc(4, tot);
+  c->on_device = true;
+}
+
+WavefieldSet &ensure_wavefield(sfb_context *c, int w) {
+  ensure_device(c);
+  WavefieldSet &W = c->wf[w];
+  if (W.allocated) return W;
+  const Assembly &a = c->P.asmb;
+  size_t *tot = &c->device_bytes;
+  const int S = c->P.nshots;
+  for (int m : kMedia) {
+    const size_t ld = static_cast<size_t>(a.nglob[m] + (a.nglob[m] & 1)) * a.ncomp(m);
+    W.u[m].alloc(ld * S, tot);
+    W.v[m].alloc(ld * S, tot);
+    W.a[m].alloc(ld * S, tot);
+    dev::MediumFields &f = W.f[m];
+    f.nglob = a.nglob[m];
+    f.nc = a.ncomp(m);
+    f.elem_begin = c->med_begin[m];
+    f.nelem = c->med_count[m];
+    f.nelem_interior = c->med_interior[m];
+    f.u = W.u[m].p;
+    f.v = W.v[m].p;
+    f.a = W.a[m].p;
+    f.minv = c->minv[m].p;
+    f.mass = c->mass[m].p;
+  }
+  const Problem &P = c->P;
+  const size_t nseis = static_cast<size_t>(S) * P.max_sig_step() * P.seismogram_types.size() *
+                       P.receivers.size() * 2;
+  W.seis.alloc(std::max<size_t>(nseis, 1), tot);
+  W.ctrl.alloc(1, tot);
+  W.allocated = true;
+  return W;
+}
+
+dev::SourceSet source_set(sfb_context *c) {
+  dev::SourceSet s{};
+  s.n = c->nsrc;
+  s.elem = c->src_elem.p;
+  s.shot = c->src_shot.p;
+  s.medium = c->src_medium.p;
+  s.array = c->src_array.p;
+  s.stf = c->src_stf.p;
+  s.nstep = c->P.nstep;
+  return s;
+}
+
+dev::ReceiverSet receiver_set(sfb_context *c, WavefieldSet &W) {
+  dev::ReceiverSet r{};
+  const Problem &P = c->P;
+  r.n = static_cast<int>(P.receivers.size());
+  r.elem = c->rec_elem.p;
+  r.lagrange = c->rec_lag.p;
+  r.sinv = c->rec_sin.p;
+  r.cosv = c->rec_cos.p;
+  r.ntypes = static_cast<int>(P.seismogram_types.size());
+  for (int i = 0; i < r.ntypes && i < 5; ++i) r.types[i] = P.seismogram_types[i];
+  r.max_sig = P.max_sig_step();
+  r.nsbs = P.nstep_between_samples;
+  r.seis = W.seis.p;
+  return r;
+}
+
+dev::CouplingSet coupling_acoustic(sfb_context *c) {
+  return {static_cast<int>(c->P.v_cp_ac_self.size()), c->cp_ac_self.p, c->cp_ac_other.p,
+          c->cp_ac_f.p, c->cp_ac_nx.p, c->cp_ac_nz.p};
+}
+dev::CouplingSet coupling_elastic(sfb_context *c) {
+  return {static_cast<int>(c->P.v_cp_el_self.size()), c->cp_el_self.p, c->cp_el_other.p,
+          c->cp_el_f.p, c->cp_el_nx.p, c->cp_el_nz.p};
+}
+
+void initialize_mass(sfb_context *c, double dt) {
+  ensure_device(c);
+  const Assembly &a = c->P.asmb;
+  for (int m : kMedia) {
+    dev::MediumFields f{};
+    f.nglob = a.nglob[m];
+    f.nc = a.ncomp(m);
+    f.elem_begin = c->med_begin[m];
+    f.nelem = c->med_count[m];
+    f.minv = c->minv[m].p;
+    f.mass = c->mass[m].p;
+    if (c->mass[m].n) ck(cudaMemsetAsync(c->mass[m].p, 0, c->mass[m].n * sizeof(double), c->stream), "memset mass");
+    dev::launch_mass(m, a.ngll, c->st, f, static_cast<float>(dt), c->stream);
+    dev::launch_invert_mass(f, c->stream);
+  }
+  ck(cudaGetLastError(), "mass kernels");
+  c->mass_ready = true;
+}
+
+void set_step(sfb_context *c, WavefieldSet &W, int istep) {
+  dev::Control h{istep};
+  ck(cudaMemcpyAsync(W.ctrl.p, &h, sizeof(h), cudaMemcpyHostToDevice, c->stream), "set step");
+  W.step = istep;
+}
+
+// One fused forward step: sources, coupling and stiffness per medium in the
+// reference order, seismograms, then the update kernels.
+void enqueue_fused_step(sfb_context *c, WavefieldSet &W, int last) {
+  const Problem &P = c->P;
+  const int S = P.nshots, n = P.asmb.ngll;
+  const float dt = static_cast<float>(P.dt);
+  const float dt2 = static_cast<float>(P.dt / 2.0), dtsq2 = static_cast<float>(P.dt * P.dt / 2.0);
+  const int *istep = &W.ctrl.p->istep;
+  dev::StaceyStore ss{};
+  if (P.save_boundary_values && c->stacey_data.p) {
+    ss.data = c->stacey_data.p;
+    ss.slot = c->stacey_slot.p;
+    ss.nstacey = c->nstacey;
+    ss.nstep = P.nstep;
+    ss.mode = 1;
+  }
+  dev::SourceSet src = source_set(c);
+  // acoustic first (time_marching.tpp:48-52)
+  dev::launch_coupling_acoustic(coupling_acoustic(c), W.f[dev::MED_AC], W.f[dev::MED_PSV], S, c->stream);
+  dev::launch_sources(n, c->st, src, W.f, S, dev::MED_AC, istep, 0, c->stream);
+  dev::launch_stiffness(dev::MED_AC, n, c->st, W.f[dev::MED_AC], S, ss, istep, c->stream);
+  // elastic (coupling reads the final acoustic acceleration = force * minv)
+  dev::launch_coupling_elastic(coupling_elastic(c), W.f[dev::MED_PSV], W.f[dev::MED_AC], S, 0, c->stream);
+  for (int m : {dev::MED_PSV, dev::MED_SH}) {
+    dev::launch_sources(n, c->st, src, W.f, S, m, istep, 0, c->stream);
+    dev::launch_stiffness(m, n, c->st, W.f[m], S, ss, istep, c->stream);
+  }
+  dev::launch_receivers(n, c->st, receiver_set(c, W), W.f, S, dt2, 1, istep, c->stream);
+  // update: the step counter advances with the last launched medium
+  int lastm = -1;
+  for (int m : kMedia)
+    if (W.f[m].nglob > 0) lastm = m;
+  for (int m : kMedia) {
+    if (W.f[m].nglob == 0) continue;
+    dev::launch_fused_update(W.f[m], S, dt, dt2, dtsq2, last, m == lastm ? W.ctrl.p : nullptr, c->stream);
+  }
+}
+
+void predictor_all(sfb_context *c, WavefieldSet &W, double sgn) {
+  const Problem &P = c->P;
+  for (int m : kMedia)
+    dev::launch_predictor(W.f[m], P.nshots, static_cast<float>(sgn * P.dt), static_cast<float>(sgn * P.dt / 2.0),
+                          static_cast<float>(P.dt * P.dt / 2.0), c->stream);
+}
+
+void run_forward_fused(sfb_context *c, int nstep, int use_graph) {
+  WavefieldSet &W = ensure_wavefield(c, SFB_WAVEFIELD_FORWARD);
+  if (!c->mass_ready) initialize_mass(c, c->P.dt);
+  if (nstep <= 0) return;
+  if (W.step + nstep > c->P.nstep)
+    throw std::invalid_argument("run would pass the configured number of steps");
+  set_step(c, W, W.step);
+  predictor_all(c, W, 1.0);
+  const int body = nstep - 1;
+  if (use_graph && body > 0) {
+    const int K = std::min(body, 25);
+    if (!c->graph || c->graph_steps != K) {
+      if (c->graph) cudaGraphExecDestroy(c->graph);
+      c->graph = nullptr;
+      cudaGraph_t g;
+      ck(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+      for (int k = 0; k < K; ++k) enqueue_fused_step(c, W, 0);
+      ck(cudaStreamEndCapture(c->stream, &g), "end capture");
+      ck(cudaGraphInstantiate(&c->graph, g, 0), "graph instantiate");
+      cudaGraphDestroy(g);
+      c->graph_steps = K;
+    }
+    int done = 0;
+    while (done + K <= body) {
+      ck(cudaGraphLaunch(c->graph, c->stream), "graph launch");
+      done += K;
+    }
+    for (; done < body; ++done) enqueue_fused_step(c, W, 0);
+  } else {
+    for (int k = 0; k < body; ++k) enqueue_fused_step(c, W, 0);
+  }
+  enqueue_fused_step(c, W, 1);
+  ck(cudaGetLastError(), "forward step kernels");
+  W.step += nstep;
+}
+
+int update_wavefields(sfb_context *c, int w, int medium, int istep) {
+  WavefieldSet &W = ensure_wavefield(c, w);
+  const Problem &P = c->P;
+  const int S = P.nshots, n = P.asmb.ngll;
+  set_step(c, W, istep);
+  const int *is = &W.ctrl.p->istep;
+  dev::StaceyStore ss{};
+  dev::SourceSet src = source_set(c);
+  if (medium == dev::MED_AC) {
+    dev::launch_coupling_acoustic(coupling_acoustic(c), W.f[dev::MED_AC], W.f[dev::MED_PSV], S, c->stream);
+  } else if (medium == dev::MED_PSV) {
+    dev::launch_coupling_elastic(coupling_elastic(c), W.f[dev::MED_PSV], W.f[dev::MED_AC], S, 1, c->stream);
+  }
+  if (w != SFB_WAVEFIELD_ADJOINT) dev::launch_sources(n, c->st, src, W.f, S, medium, is, 0, c->stream);
+  dev::launch_stiffness(medium, n, c->st, W.f[medium], S, ss, is, c->stream);
+  dev::launch_divide(W.f[medium], S, c->stream);
+  ck(cudaGetLastError(), "update_wavefields");
+  return W.f[medium].nelem;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+
+SFB_API const char *sfb_last_error(const sfb_context *ctx) {
+  return ctx ? ctx->err.c_str() : g_create_error.c_str();
+}
+
+SFB_API int sfb_create_from_yaml(const char *parameter_file, const char *default_file, sfb_context **out) {
+  if (!parameter_file || !out) return fail(nullptr, SFB_E_INVALID, "null argument");
+  *out = nullptr;
+  return guarded(nullptr, [&]() {
+    std::unique_ptr<sfb_context> c(new sfb_context());
+    c->P = problem_from_yaml(parameter_file, default_file ? default_file : "");
+    *out = c.release();
+    return SFB_OK;
+  });
+}
+
+SFB_API int sfb_create_structured(const sfb_structured_desc *desc, sfb_context **out) {
+  if (!desc || !out) return fail(nullptr, SFB_E_INVALID, "null argument");
+  *out = nullptr;
+  return guarded(nullptr, [&]() {
+    std::unique_ptr<sfb_context> c(new sfb_context());
+    c->P = problem_from_structured(*desc);
+    *out = c.release();
+    return SFB_OK;
+  });
+}
+
+SFB_API void sfb_destroy(sfb_context *ctx) { delete ctx; }
+
+SFB_API int sfb_get_info(const sfb_context *ctx, sfb_info *info) {
+  if (!ctx || !info) return SFB_E_INVALID;
+  const Problem &P = ctx->P;
+  *info = sfb_info{};
+  info->ngll = P.asmb.ngll;
+  info->nspec = P.asmb.nspec;
+  info->nshots = P.nshots;
+  info->nstep = P.nstep;
+  info->nstep_between_samples = P.nstep_between_samples;
+  info->max_sig_step = P.max_sig_step();
+  for (int m = 0; m < 4; ++m) {
+    info->nglob[m] = P.asmb.nglob[m];
+    info->nelements[m] = P.asmb.count_elements(m);
+  }
+  info->nreceivers = static_cast<int>(P.receivers.size());
+  info->nseismogram_types = static_cast<int>(P.seismogram_types.size());
+  info->nsources = static_cast<int>(P.sources.size());
+  info->simulation = P.simulation;
+  info->dt = P.dt;
+  info->t0 = P.t0;
+  info->device_bytes = ctx->device_bytes;
+  return SFB_OK;
+}
+
+SFB_API int sfb_get_problem_view(const sfb_context *ctx, sfb_problem_view *view) {
+  if (!ctx || !view) return SFB_E_INVALID;
+  ctx->P.fill_view(view);
+  return SFB_OK;
+}
+
+SFB_API int sfb_domain_initialize(sfb_context *ctx, int wavefield, double dt) {
+  if (!ctx) return SFB_E_INVALID;
+  return guarded(ctx, [&]() {
+    if (wavefield < 0 || wavefield > 2) throw std::invalid_argument("bad wavefield");
+    ensure_wavefield(ctx, wavefield);
+    initialize_mass(ctx, dt);
+    ctx->wf[wavefield].initialized = true;
+    return SFB_OK;
+  });
+}
+
+SFB_API int sfb_domain_update_wavefields(sfb_context *ctx, int wavefield, int medium, int istep,
+                                         int *elements_updated) {
+  if (!ctx) return SFB_E_INVALID;
+  return guarded(ctx, [&]() {
+    if (!medium_index_ok(medium)) throw std::invalid_argument("unsupported medium tag");
+    if (!ctx->mass_ready) throw StateError("domain_kernels::initialize has not been called");
+    const int n = update_wavefields(ctx, wavefield, medium, istep);
+    if (elements_updated) *elements_updated = n;
+    return SFB_OK;
+  });
+}
+
+SFB_API int sfb_domain_compute_seismograms(sfb_context *ctx, int wavefield, int isig_step) {
+  if (!ctx) return SFB_E_INVALID;
+  return guarded(ctx, [&]() {
+    WavefieldSet &W = ensure_wavefield(ctx, wavefield);
+    // the kernel derives isig from the step counter: isig * nsbs
+    set_step(ctx, W, isig_step * ctx->P.nstep_between_samples);
+    dev::launch_receivers(ctx->P.asmb.ngll, ctx->st, receiver_set(ctx, W), W.f, ctx->P.nshots, 0.f, 0,
+                          &W.ctrl.p->istep, ctx->stream);
+    ck(cudaGetLastError(), "compute_seismograms");
+    return SFB_OK;
+  });
+}
+
+SFB_API int sfb_newmark_predictor(sfb_context *ctx, int wavefield, int medium, int *dofs) {
+  if (!ctx) return SFB_E_INVALID;
+  return guarded(ctx, [&]() {
+    if (!medium_index_ok(medium)) throw std::invalid_argument("unsupported medium tag");
+    WavefieldSet &W = ensure_wavefield(ctx, wavefield);
+    const double sgn = wavefield == SFB_WAVEFIELD_BACKWARD ? -1.0 : 1.0;
+    const Problem &P = ctx->P;
+    dev::launch_predictor(W.f[medium], P.nshots, static_cast<float>(sgn * P.dt),
+                          static_cast<float>(sgn * P.dt / 2.0), static_cast<float>(P.dt * P.dt / 2.0),
+                          ctx->stream);
+    ck(cudaGetLastError(), "predictor");
+    if (dofs) *dofs = W.f[medium].nglob * W.f[medium].nc;
+    return SFB_OK;
+  });
+}
+
+SFB_API int sfb_newmark_corrector(sfb_context *ctx, int wavefield, int medium, int *dofs) {
+  if (!ctx) return SFB_E_INVALID;
+  return guarded(ctx, [&]() {
+    if (!medium_index_ok(medium)) throw std::invalid_argument("unsupported medium tag");
+    WavefieldSet &W = ensure_wavefield(ctx, wavefield);
+    const double sgn = wavefield == SFB_WAVEFIELD_BACKWARD ? -1.0 : 1.0;
+    dev::launch_corrector(W.f[medium], ctx->P.nshots, static_cast<float>(sgn * ctx->P.dt / 2.0), ctx->stream);
+    ck(cudaGetLastError(), "corrector");
+    if (dofs) *dofs = W.f[medium].nglob * W.f[medium].nc;
+    return SFB_OK;
+  });
+}
+
+SFB_API int sfb_run_forward(sfb_context *ctx, int nstep, int use_graph) {
+  if (!ctx) return SFB_E_INVALID;
+  return guarded(ctx, [&]() {
+    run_forward_fused(ctx, nstep, use_graph);
+    ck(cudaStreamSynchronize(ctx->stream), "forward run");
+    return SFB_OK;
+  });
+}
+
+SFB_API int sfb_run_forward_unfused(sfb_context *ctx, int nstep) {
+  if (!ctx) return SFB_E_INVALID;
+  return guarded(ctx, [&]() {
+    WavefieldSet &W = ensure_wavefield(ctx, SFB_WAVEFIELD_FORWARD);
+    if (!ctx->mass_ready) initialize_mass(ctx, ctx->P.dt);
+    const Problem &P = ctx->P;
+    int total_dofs = 0;
+    for (int m : kMedia) total_dofs += 2 * P.asmb.nglob[m] * P.asmb.ncomp(m);
+    const int start = W.step;
+    if (start + nstep > P.nstep) throw std::invalid_argument("run would pass the configured number of steps");
+    int isig = start / P.nstep_between_samples;
+    for (int istep = start; istep < start + nstep; ++istep) {
+      int dofs = 0, elements = 0, k = 0;
+      for (int m : {dev::MED_AC, dev::MED_PSV, dev::MED_SH}) {
+        sfb_newmark_predictor(ctx, 0, m, &k);
+        dofs += k;
+      }
+      elements += update_wavefields(ctx, 0, dev::MED_AC, istep);
+      sfb_newmark_corrector(ctx, 0, dev::MED_AC, &k);
+      dofs += k;
+      elements += update_wavefields(ctx, 0, dev::MED_PSV, istep);
+      elements += update_wavefields(ctx, 0, dev::MED_SH, istep);
+      sfb_newmark_corrector(ctx, 0, dev::MED_PSV, &k);
+      dofs += k;
+      sfb_newmark_corrector(ctx, 0, dev::MED_SH, &k);
+      dofs += k;
+      if (istep % P.nstep_between_samples == 0 && isig < P.max_sig_step()) {
+        set_step(ctx, W, istep);
+        dev::launch_receivers(P.asmb.ngll, ctx->st, receiver_set(ctx, W), W.f, P.nshots, 0.f, 0,
+                              &W.ctrl.p->istep, ctx->stream);
+        ++isig;
+      }
+      if (!ctx->err.empty()) throw std::runtime_error(ctx->err);
+      if (dofs != total_dofs || elements != P.asmb.nspec)
+        return fail(ctx, SFB_E_ACCOUNTING,
+                    "The time loop has not updated all the degrees of freedom (" + std::to_string(dofs) +
+                        " of " + std::to_string(total_dofs) + ") or elements (" + std::to_string(elements) +
+                        " of " + std::to_string(P.asmb.nspec) + ")");
+    }
+    ck(cudaStreamSynchronize(ctx->stream), "unfused forward run");
+    W.step = start + nstep;
+    return SFB_OK;
+  });
+}
+
+SFB_API int sfb_get_seismograms(const sfb_context *cctx, int wavefield, int shot, float *host, size_t count) {
+  sfb_context *ctx = const_cast<sfb_context *>(cctx);
+  if (!ctx || !host) return SFB_E_INVALID;
+  return guarded(ctx, [&]() {
+    WavefieldSet &W = ensure_wavefield(ctx, wavefield);
+    const Problem &P = ctx->P;
+    const size_t per = static_cast<size_t>(P.max_sig_step()) * P.seismogram_types.size() * P.receivers.size() * 2;
+    if (shot < 0 || shot >= P.nshots) throw std::invalid_argument("shot out of range");
+    if (count < per) throw std::invalid_argument("seismogram buffer too small");
+    ck(cudaStreamSynchronize(ctx->stream), "sync");
+    if (per) ck(cudaMemcpy(host, W.seis.p + shot * per, per * sizeof(float), cudaMemcpyDeviceToHost), "seis d2h");
+    return SFB_OK;
+  });
+}
+
+SFB_API int sfb_get_field(const sfb_context *cctx, int wavefield, int medium, int which, int shot, float *host,
+                          size_t count) {
+  sfb_context *ctx = const_cast<sfb_context *>(cctx);
+  if (!ctx || !host) return SFB_E_INVALID;
+  return guarded(ctx, [&]() {
+    if (!medium_index_ok(medium)) throw std::invalid_argument("unsupported medium tag");
+    WavefieldSet &W = ensure_wavefield(ctx, wavefield);
+    const dev::MediumFields &f = W.f[medium];
+    const size_t n = static_cast<size_t>(f.nglob) * f.nc;
+    const size_t ld = static_cast<size_t>(f.nglob + (f.nglob & 1)) * f.nc;
+    if (count < n) throw std::invalid_argument("field buffer too small");
+    if (shot < 0 || shot >= ctx->P.nshots) throw std::invalid_argument("shot out of range");
+    const float *src = which == 0 ? f.u : which == 1 ? f.v : which == 2 ? f.a : f.minv;
+    if (which == 3) shot = 0;
+    std::vector<float> tmp(n);
+    ck(cudaStreamSynchronize(ctx->stream), "sync");
+    if (n) ck(cudaMemcpy(tmp.data(), src + shot * ld, n * sizeof(float), cudaMemcpyDeviceToHost), "field d2h");
+    // device layout interleaves components; the ABI layout is [ncomp][nglob]
+    for (int c = 0; c < f.nc; ++c)
+      for (int g = 0; g < f.nglob; ++g) host[static_cast<size_t>(c) * f.nglob + g] = tmp[static_cast<size_t>(g) * f.nc + c];
+    return SFB_OK;
+  });
+}
+
+SFB_API int sfb_set_field(sfb_context *ctx, int wavefield, int medium, int which, int shot, const float *host,
+                          size_t count) {
+  if (!ctx || !host) return SFB_E_INVALID;
+  return guarded(ctx, [&]() {
+    if (!medium_index_ok(medium) || which < 0 || which > 2) throw std::invalid_argument("bad field selector");
+    WavefieldSet &W = ensure_wavefield(ctx, wavefield);
+    const dev::MediumFields &f = W.f[medium];
+    const size_t n = static_cast<size_t>(f.nglob) * f.nc;
+    const size_t ld = static_cast<size_t>(f.nglob + (f.nglob & 1)) * f.nc;
+    if (count < n) throw std::invalid_argument("field buffer too small");
+    if (shot < 0 || shot >= ctx->P.nshots) throw std::invalid_argument("shot out of range");
+    std::vector<float> tmp(n);
+    for (int c = 0; c < f.nc; ++c)
+      for (int g = 0; g < f.nglob; ++g) tmp[static_cast<size_t>(g) * f.nc + c] = host[static_cast<size_t>(c) * f.nglob + g];
+    float *dst = which == 0 ? f.u : which == 1 ? f.v : f.a;
+    ck(cudaStreamSynchronize(ctx->stream), "sync");
+    if (n) ck(cudaMemcpy(dst + shot * ld, tmp.data(), n * sizeof(float), cudaMemcpyHostToDevice), "field h2d");
+    return SFB_OK;
+  });
+}
+
+SFB_API int sfb_write_seismograms(const sfb_context *cctx, int wavefield, int shot, const char *directory) {
+  sfb_context *ctx = const_cast<sfb_context *>(cctx);
+  if (!ctx || !directory) return SFB_E_INVALID;
+  const Problem &P = ctx->P;
+  const size_t per = static_cast<size_t>(P.max_sig_step()) * P.seismogram_types.size() * P.receivers.size() * 2;
+  std::vector<float> buf(std::max<size_t>(per, 1));
+  const int rc = sfb_get_seismograms(ctx, wavefield, shot, buf.data(), buf.size());
+  if (rc) return rc;
+  return guarded(ctx, [&]() {
+    write_seismograms_ascii(P, buf.data(), static_cast<int>(P.seismogram_types.size()),
+                            static_cast<int>(P.receivers.size()), P.max_sig_step(), directory);
+    return SFB_OK;
+  });
+}
+
+// Entry points of the adjoint path are provided by adjoint.cu.

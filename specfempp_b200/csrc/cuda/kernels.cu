@@ -1,0 +1,614 @@
+// sm_100a kernels of the SEM time-marching path.  See kernels.cuh for the
+// HBM layout.  Reference operation order is kept so that results track the
+// reference's FP32 arithmetic:
+//   gradient   include/algorithms/gradient.hpp:78-98
+//   stress     include/medium/dim2/elastic/isotropic/stress.hpp:14-85,
+//              include/medium/dim2/acoustic/isotropic/stress.hpp:15-31
+//   F = J T dxi/dx   core/specfem/point/stress.hpp:123-137
+//   divergence include/algorithms/divergence.hpp:83-99 (then * -1)
+//   Stacey     include/boundary_conditions/stacey/stacey.tpp:41-212
+//   free surface include/boundary_conditions/dirichlet/dirichlet.hpp:19-43
+#include "kernels.cuh"
+
+#include <cstdio>
+
+namespace sfb {
+namespace dev {
+
+__constant__ float c_hp[64];   // hprime[i*N + j] = l_j'(xi_i)
+__constant__ float c_hpw[64];  // hprime_wgll[ix*N + l] = hprime[l*N + ix] * w[l]
+__constant__ float c_w[8];
+
+void set_quadrature(int n, const float *hp, const float *w) {
+  float hpw[64];
+  for (int ix = 0; ix < n; ++ix)
+    for (int l = 0; l < n; ++l) hpw[ix * n + l] = hp[l * n + ix] * w[l];
+  cudaMemcpyToSymbol(c_hp, hp, sizeof(float) * n * n);
+  cudaMemcpyToSymbol(c_hpw, hpw, sizeof(float) * n * n);
+  cudaMemcpyToSymbol(c_w, w, sizeof(float) * n);
+}
+
+namespace {
+
+template <int NC> struct Vec;
+template <> struct Vec<1> {
+  using T = float;
+  __device__ static T zero() { return 0.f; }
+};
+template <> struct Vec<2> {
+  using T = float2;
+  __device__ static T zero() { return make_float2(0.f, 0.f); }
+};
+
+__device__ __forceinline__ float comp(float v, int) { return v; }
+__device__ __forceinline__ float comp(float2 v, int c) { return c == 0 ? v.x : v.y; }
+__device__ __forceinline__ void set_comp(float &v, int, float x) { v = x; }
+__device__ __forceinline__ void set_comp(float2 &v, int c, float x) {
+  if (c == 0) v.x = x; else v.y = x;
+}
+
+// Vector reduction into global memory (RED.E.ADD.F32x2 on sm_90+).
+__device__ __forceinline__ void red_add(float *p, float v) { atomicAdd(p, v); }
+__device__ __forceinline__ void red_add(float2 *p, float2 v) { atomicAdd(p, v); }
+
+// Stacey traction added to `acc` for velocity `vel` (stacey.tpp:41-75 P-SV,
+// :125-145 SH, :178-212 acoustic).
+template <int MED>
+__device__ __forceinline__ void stacey(float m0, float m1, float m2, float nx, float nz,
+                                       float we, const float *vel, float *acc) {
+  const float jac1d = sqrtf(nx * nx + nz * nz);
+  if (MED == MED_PSV) {
+    const float kappa = m0, mu = m1, rho = m2;
+    const float l2m = kappa + static_cast<float>(4.0 / 3.0) * mu;
+    const float rho_vp = sqrtf(l2m / rho) * rho;
+    const float rho_vs = sqrtf(rho * mu);
+    const float vn = vel[0] * nx + vel[1] * nz;
+    const float dn[2] = {nx, nz};
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      const float fac = ((vn * dn[c] / (jac1d * jac1d)) * (rho_vp - rho_vs)) + vel[c] * rho_vs;
+      acc[c] += -1.0f * fac * jac1d * we;
+    }
+  } else if (MED == MED_SH) {
+    const float mu = m0, rho = m1;
+    const float rho_vs = sqrtf(rho * mu);
+    const float fac = we * jac1d;
+    acc[0] += -1.0f * fac * rho_vs * vel[0];
+  } else {
+    const float rho_inv = m0, kappa = m1;
+    const float rvi = sqrtf(rho_inv * (1.0f / kappa));
+    const float fac = we * jac1d;
+    acc[0] += -1.0f * fac * rvi * vel[0];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Stiffness: one block = EPB elements x N threads; thread (el, iz) owns row
+// iz of element el.  The row's geometry, material and global indices are
+// loaded once into registers and reused for every shot; displacement and the
+// gamma-part of the stress integrand go through shared memory for the column
+// contractions; the xi-contractions stay in registers.
+// ---------------------------------------------------------------------------
+template <int MED, int N, int EPB>
+__global__ void __launch_bounds__(N * EPB)
+k_stiffness(Static st, MediumFields f, int nshots, StaceyStore ss, const int *istep_dev) {
+  constexpr int NC = (MED == MED_PSV) ? 2 : 1;
+  using V = typename Vec<NC>::T;
+  __shared__ V s_u[EPB][N * N];
+  __shared__ V s_fg[EPB][N * N];
+
+  const int el = threadIdx.x / N, iz = threadIdx.x % N;
+  const int li = blockIdx.x * EPB + el;
+  const bool valid = li < f.nelem;
+  const int e = f.elem_begin + (valid ? li : 0);
+  const size_t p0 = (static_cast<size_t>(e) * N + iz) * N;
+
+  int g[N];
+  float xix[N], xiz[N], gax[N], gaz[N], jac[N], m0[N], m1[N];
+#pragma unroll
+  for (int ix = 0; ix < N; ++ix) {
+    g[ix] = __ldg(st.iglob + p0 + ix);
+    xix[ix] = __ldg(st.xix + p0 + ix);
+    xiz[ix] = __ldg(st.xiz + p0 + ix);
+    gax[ix] = __ldg(st.gax + p0 + ix);
+    gaz[ix] = __ldg(st.gaz + p0 + ix);
+    jac[ix] = __ldg(st.jac + p0 + ix);
+    m0[ix] = __ldg(st.mat0 + p0 + ix);
+    m1[ix] = __ldg(st.mat1 + p0 + ix);
+  }
+  float hpz[N], hpwz[N];
+#pragma unroll
+  for (int l = 0; l < N; ++l) {
+    hpz[l] = c_hp[iz * N + l];
+    hpwz[l] = c_hpw[iz * N + l];
+  }
+  const uint8_t eflag = valid ? st.eflag[e] : 0;
+  const int slot = (ss.mode != 0 && valid) ? ss.slot[e] : -1;
+  const int istep = (ss.mode != 0) ? *istep_dev : 0;
+
+  for (int s = blockIdx.y; s < nshots; s += gridDim.y) {
+    const V *U = reinterpret_cast<const V *>(f.u) + static_cast<size_t>(s) * (f.nglob + (f.nglob & 1));
+    V *A = reinterpret_cast<V *>(f.a) + static_cast<size_t>(s) * (f.nglob + (f.nglob & 1));
+    V ur[N];
+#pragma unroll
+    for (int ix = 0; ix < N; ++ix) {
+      ur[ix] = valid ? U[g[ix]] : Vec<NC>::zero();
+      s_u[el][iz * N + ix] = ur[ix];
+    }
+    __syncthreads();
+    V fx[N];
+#pragma unroll
+    for (int ix = 0; ix < N; ++ix) {
+      float dxi[NC], dga[NC];
+#pragma unroll
+      for (int c = 0; c < NC; ++c) { dxi[c] = 0.f; dga[c] = 0.f; }
+#pragma unroll
+      for (int l = 0; l < N; ++l) {
+        const V col = s_u[el][l * N + ix];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+          dxi[c] += c_hp[ix * N + l] * comp(ur[l], c);
+          dga[c] += hpz[l] * comp(col, c);
+        }
+      }
+      float du[NC][2];
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        du[c][0] = xix[ix] * dxi[c] + gax[ix] * dga[c];
+        du[c][1] = xiz[ix] * dxi[c] + gaz[ix] * dga[c];
+      }
+      float T[NC][2];
+      if constexpr (MED == MED_PSV) {
+        const float kappa = m0[ix], mu = m1[ix];
+        const float l2m = kappa + static_cast<float>(4.0 / 3.0) * mu;
+        const float lam = l2m - 2.0f * mu;
+        T[0][0] = l2m * du[0][0] + lam * du[1][1];  // sigma_xx
+        T[1][1] = l2m * du[1][1] + lam * du[0][0];  // sigma_zz
+        T[0][1] = mu * (du[0][1] + du[1][0]);       // sigma_xz
+        T[1][0] = T[0][1];
+      } else {
+        const float k = m0[ix];  // SH: mu; acoustic: rho_inverse
+        T[0][0] = k * du[0][0];
+        T[0][1] = k * du[0][1];
+      }
+      V f0, f1;
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        set_comp(f0, c, jac[ix] * (T[c][0] * xix[ix] + T[c][1] * xiz[ix]));
+        set_comp(f1, c, jac[ix] * (T[c][0] * gax[ix] + T[c][1] * gaz[ix]));
+      }
+      fx[ix] = f0;
+      s_fg[el][iz * N + ix] = f1;
+    }
+    __syncthreads();
+    if (valid) {
+#pragma unroll
+      for (int ix = 0; ix < N; ++ix) {
+        float t1[NC], t2[NC];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) { t1[c] = 0.f; t2[c] = 0.f; }
+#pragma unroll
+        for (int l = 0; l < N; ++l) {
+          const V col = s_fg[el][l * N + ix];
+#pragma unroll
+          for (int c = 0; c < NC; ++c) {
+            t1[c] += comp(fx[l], c) * c_hpw[ix * N + l];
+            t2[c] += comp(col, c) * hpwz[l];
+          }
+        }
+        float acc[2];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) acc[c] = (c_w[iz] * t1[c] + c_w[ix] * t2[c]) * -1.0f;
+        if (eflag) {
+          const size_t p = p0 + ix;
+          const uint8_t b = st.bnd[p];
+          if (b & 1) {
+            const V *Vv = reinterpret_cast<const V *>(f.v) + static_cast<size_t>(s) * (f.nglob + (f.nglob & 1));
+            const V vv = Vv[g[ix]];
+            float vel[2];
+#pragma unroll
+            for (int c = 0; c < NC; ++c) vel[c] = comp(vv, c);
+            stacey<MED>(m0[ix], m1[ix], st.mat2 ? st.mat2[p] : 0.f, st.bnd_nx[p], st.bnd_nz[p],
+                        st.bnd_w[p], vel, acc);
+          }
+          if (b & 2) {
+#pragma unroll
+            for (int c = 0; c < NC; ++c) acc[c] = 0.f;
+          }
+        }
+        if (slot >= 0) {
+          const size_t base =
+              ((((static_cast<size_t>(s) * ss.nstep + istep) * ss.nstacey + slot) * N + iz) * N + ix) * NC;
+          if (ss.mode == 1) {
+#pragma unroll
+            for (int c = 0; c < NC; ++c) ss.data[base + c] = acc[c];
+          } else {
+#pragma unroll
+            for (int c = 0; c < NC; ++c) acc[c] = ss.data[base + c];
+          }
+        }
+        V out;
+#pragma unroll
+        for (int c = 0; c < NC; ++c) set_comp(out, c, acc[c]);
+        red_add(A + g[ix], out);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Point sources (compute_source_interaction.tpp:77-95): one block per source.
+// ---------------------------------------------------------------------------
+__global__ void k_sources(Static st, SourceSet src, MediumFields f, int medium, int N,
+                          const int *istep_dev, int wavefield_sel) {
+  const int i = blockIdx.x;
+  const int k = threadIdx.x;
+  if (k >= N * N) return;
+  if (src.medium[i] != medium) return;
+  const int istep = *istep_dev;
+  if (istep < 0 || istep >= src.nstep) return;
+  const int e = src.elem[i];
+  const size_t p = static_cast<size_t>(e) * N * N + k;
+  const int gi = st.iglob[p];
+  const int s = src.shot[i];
+  const size_t ld = static_cast<size_t>(f.nglob + (f.nglob & 1)) * f.nc;
+  float *A = f.a + s * ld;
+  for (int c = 0; c < f.nc; ++c) {
+    const float stf = src.stf[(static_cast<size_t>(i) * src.nstep + istep) * 2 + c];
+    const float arr = src.array[(static_cast<size_t>(i) * 2 + c) * N * N + k];
+    float val = stf * arr;
+    if (medium == MED_AC) val = stf * arr / st.mat1[p];
+    atomicAdd(A + static_cast<size_t>(gi) * f.nc + c, val);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Fluid-solid coupling (coupled_interface.tpp:55-86, compute_coupling.hpp).
+// ---------------------------------------------------------------------------
+__global__ void k_couple_acoustic(CouplingSet c, MediumFields ac, MediumFields el, int nshots) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int s = blockIdx.y;
+  if (i >= c.n || s >= nshots) return;
+  const float2 *U = reinterpret_cast<const float2 *>(el.u) + static_cast<size_t>(s) * (el.nglob + (el.nglob & 1));
+  float *A = ac.a + static_cast<size_t>(s) * (ac.nglob + (ac.nglob & 1));
+  const float2 u = U[c.other[i]];
+  atomicAdd(A + c.self[i], c.factor[i] * (c.nx[i] * u.x + c.nz[i] * u.y));
+}
+
+__global__ void k_couple_elastic(CouplingSet c, MediumFields el, MediumFields ac, int nshots,
+                                 int ac_divided) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int s = blockIdx.y;
+  if (i >= c.n || s >= nshots) return;
+  const float *Aac = ac.a + static_cast<size_t>(s) * (ac.nglob + (ac.nglob & 1));
+  float *A = el.a + static_cast<size_t>(s) * (el.nglob + (el.nglob & 1)) * 2;
+  const int o = c.other[i];
+  const float chi_dd = ac_divided ? Aac[o] : Aac[o] * ac.minv[o];
+  const int g = c.self[i];
+  atomicAdd(A + 2 * g, c.factor[i] * c.nx[i] * chi_dd);
+  atomicAdd(A + 2 * g + 1, c.factor[i] * c.nz[i] * chi_dd);
+}
+
+// ---------------------------------------------------------------------------
+// Receivers (compute_seismogram.tpp:98-135, wavefield.hpp): one block of 64
+// threads per (receiver, shot).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float ld_comp(const MediumFields &f, int which, int s, int g, int c,
+                                         float dt2, int mode) {
+  const size_t ld = static_cast<size_t>(f.nglob + (f.nglob & 1)) * f.nc;
+  const size_t idx = s * ld + static_cast<size_t>(g) * f.nc + c;
+  const size_t m = static_cast<size_t>(g) * f.nc + c;
+  if (which == 0) return f.u[idx];
+  if (mode == 0) return which == 1 ? f.v[idx] : f.a[idx];
+  const float a = f.a[idx] * f.minv[m];
+  if (which == 2) return a;
+  return f.v[idx] + dt2 * a;
+}
+
+__global__ void k_receivers(Static st, ReceiverSet rec, MediumFields f_psv, MediumFields f_sh,
+                            MediumFields f_ac, int N, float dt2, int mode, const int *istep_dev) {
+  __shared__ float s_val[2][64];
+  __shared__ float s_red[2][64];
+  const int r = blockIdx.x, s = blockIdx.y, k = threadIdx.x;
+  const int istep = *istep_dev;
+  if (istep % rec.nsbs != 0) return;
+  const int isig = istep / rec.nsbs;
+  if (isig >= rec.max_sig) return;
+  const int e = rec.elem[r];
+  const int NN = N * N;
+  const int iz = k / N, ix = k % N;
+  const size_t p = static_cast<size_t>(e) * NN + k;
+  // medium of this receiver's element: decided from the element ranges
+  int med;
+  const MediumFields *F;
+  if (e >= f_psv.elem_begin && e < f_psv.elem_begin + f_psv.nelem) { med = MED_PSV; F = &f_psv; }
+  else if (e >= f_sh.elem_begin && e < f_sh.elem_begin + f_sh.nelem) { med = MED_SH; F = &f_sh; }
+  else { med = MED_AC; F = &f_ac; }
+  const int g = (k < NN) ? st.iglob[p] : 0;
+  const float h = (k < NN) ? rec.lagrange[static_cast<size_t>(r) * NN + k] : 0.f;
+  for (int it = 0; it < rec.ntypes; ++it) {
+    const int type = rec.types[it];
+    float w0 = 0.f, w1 = 0.f;
+    const bool need_grad = (med == MED_AC && type != 3) || (med == MED_PSV && type == 3);
+    if (need_grad) {
+      // field on all points of the element, then gradient at this point
+      const int which = (med == MED_AC) ? (type == 3 ? 2 : type) : 0;
+      if (k < NN) {
+        s_val[0][k] = ld_comp(*F, which, s, g, 0, dt2, mode);
+        s_val[1][k] = (F->nc > 1) ? ld_comp(*F, which, s, g, 1, dt2, mode) : 0.f;
+      }
+      __syncthreads();
+      if (k < NN) {
+        float dxi[2] = {0.f, 0.f}, dga[2] = {0.f, 0.f};
+        for (int l = 0; l < N; ++l)
+          for (int c = 0; c < F->nc; ++c) {
+            dxi[c] += c_hp[ix * N + l] * s_val[c][iz * N + l];
+            dga[c] += c_hp[iz * N + l] * s_val[c][l * N + ix];
+          }
+        const float xix = st.xix[p], xiz = st.xiz[p], gax = st.gax[p], gaz = st.gaz[p];
+        float du[2][2];
+        for (int c = 0; c < F->nc; ++c) {
+          du[c][0] = xix * dxi[c] + gax * dga[c];
+          du[c][1] = xiz * dxi[c] + gaz * dga[c];
+        }
+        if (med == MED_AC) {
+          const float ri = st.mat0[p];
+          w0 = ri * du[0][0];
+          w1 = ri * du[0][1];
+        } else {
+          const float kappa = st.mat0[p], mu = st.mat1[p];
+          const float l2m = kappa + static_cast<float>(4.0 / 3.0) * mu;
+          const float lam = l2m - 2.0f * mu;
+          w0 = -1.0f * ((lam + static_cast<float>(2.0 / 3.0) * mu) * (du[0][0] + du[1][1]));
+          w1 = 0.f;
+        }
+      }
+      __syncthreads();
+    } else if (k < NN) {
+      if (med == MED_AC) {  // pressure = -chi_ddot
+        w0 = -1.0f * ld_comp(*F, 2, s, g, 0, dt2, mode);
+      } else {
+        w0 = ld_comp(*F, type, s, g, 0, dt2, mode);
+        w1 = (F->nc > 1) ? ld_comp(*F, type, s, g, 1, dt2, mode) : 0.f;
+      }
+    }
+    s_red[0][k] = h * w0;
+    s_red[1][k] = h * w1;
+    __syncthreads();
+    if (k == 0) {
+      float a0 = 0.f, a1 = 0.f;
+      for (int j = 0; j < NN; ++j) {
+        a0 += s_red[0][j];
+        a1 += s_red[1][j];
+      }
+      const float sn = rec.sinv[r], cs = rec.cosv[r];
+      float *o = rec.seis + ((((static_cast<size_t>(s) * rec.max_sig + isig) * rec.ntypes + it) *
+                              rec.n + r) * 2);
+      o[0] = cs * a0 - sn * a1;
+      o[1] = sn * a0 + cs * a1;
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Newmark (newmark.tpp) and the fused update.  Fields of one medium are
+// [S][ld] floats with ld = (nglob + nglob%2) * nc, a multiple of 4 for P-SV
+// and of 2 otherwise; the float4 / float2 paths below rely on that.
+// ---------------------------------------------------------------------------
+__global__ void k_predictor(float *u, float *v, float *a, size_t n, float dt, float dt2,
+                            float dtsq2) {
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const float ai = a[i];
+    const float vi = v[i];
+    u[i] += dt * vi + dtsq2 * ai;
+    v[i] = vi + dt2 * ai;
+    a[i] = 0.f;
+  }
+}
+__global__ void k_corrector(float *v, const float *a, size_t n, float dt2) {
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x)
+    v[i] += dt2 * a[i];
+}
+__global__ void k_divide(float *a, const float *minv, size_t ld, int nshots) {
+  for (size_t j = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; j < ld;
+       j += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const float m = minv[j];
+    for (int s = 0; s < nshots; ++s) a[s * ld + j] = a[s * ld + j] * m;
+  }
+}
+
+template <bool LAST>
+__global__ void k_fused_update(float2 *u, float2 *v, float2 *a, const float2 *minv, size_t ld2,
+                               int nshots, float dt, float dt2, float dtsq2, Control *ctrl) {
+  if (ctrl && blockIdx.x == 0 && threadIdx.x == 0) ctrl->istep += 1;
+  for (size_t j = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; j < ld2;
+       j += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const float2 m = minv[j];
+    for (int s = 0; s < nshots; ++s) {
+      const size_t i = s * ld2 + j;
+      const float2 r = a[i];
+      float2 acc, vel = v[i];
+      acc.x = r.x * m.x;
+      acc.y = r.y * m.y;
+      vel.x += dt2 * acc.x;  // corrector (newmark.tpp:44-47)
+      vel.y += dt2 * acc.y;
+      if (LAST) {
+        a[i] = acc;
+        v[i] = vel;
+      } else {
+        float2 uu = u[i];  // next predictor (newmark.tpp:98-105)
+        uu.x += dt * vel.x + dtsq2 * acc.x;
+        uu.y += dt * vel.y + dtsq2 * acc.y;
+        vel.x += dt2 * acc.x;
+        vel.y += dt2 * acc.y;
+        u[i] = uu;
+        v[i] = vel;
+        a[i] = make_float2(0.f, 0.f);
+      }
+    }
+  }
+}
+
+__global__ void k_advance(Control *ctrl) { ctrl->istep += 1; }
+
+// Mass matrix (compute_mass_matrix.tpp:80-113) accumulated in FP64.
+template <int MED>
+__global__ void k_mass(Static st, MediumFields f, int N, float dt) {
+  constexpr int NC = (MED == MED_PSV) ? 2 : 1;
+  const size_t nn = static_cast<size_t>(N) * N;
+  const size_t total = static_cast<size_t>(f.nelem) * nn;
+  for (size_t t = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; t < total;
+       t += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const int e = f.elem_begin + static_cast<int>(t / nn);
+    const int k = static_cast<int>(t % nn);
+    const int iz = k / N, ix = k % N;
+    const size_t p = static_cast<size_t>(e) * nn + k;
+    float base;
+    if (MED == MED_PSV) base = st.mat2[p];        // rho
+    else if (MED == MED_SH) base = st.mat1[p];    // rho
+    else base = 1.0f / st.mat1[p];                // 1 / kappa
+    float mm[2];
+    for (int c = 0; c < NC; ++c) mm[c] = base * (c_w[ix] * c_w[iz] * st.jac[p]);
+    if (st.bnd[p] & 1) {
+      const float vf[2] = {-1.0f * dt * 0.5f, -1.0f * dt * 0.5f};
+      stacey<MED>(st.mat0[p], st.mat1[p], st.mat2 ? st.mat2[p] : 0.f, st.bnd_nx[p], st.bnd_nz[p],
+                  st.bnd_w[p], vf, mm);
+    }
+    const int g = st.iglob[p];
+    for (int c = 0; c < NC; ++c) atomicAdd(f.mass + static_cast<size_t>(g) * NC + c, static_cast<double>(mm[c]));
+  }
+}
+
+__global__ void k_invert(const double *mass, float *minv, size_t n) {
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x)
+    minv[i] = static_cast<float>(1.0 / mass[i]);
+}
+
+__global__ void k_zero(float *p, size_t n) {
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x)
+    p[i] = 0.f;
+}
+
+int grid_for(size_t n, int block) {
+  size_t g = (n + block - 1) / block;
+  const size_t cap = 148 * 32;  // 148 SMs x resident blocks
+  if (g > cap) g = cap;
+  if (g < 1) g = 1;
+  return static_cast<int>(g);
+}
+
+size_t field_ld(const MediumFields &f) { return static_cast<size_t>(f.nglob + (f.nglob & 1)) * f.nc; }
+
+}  // namespace
+
+void launch_stiffness(int medium, int ngll, const Static &st, const MediumFields &f, int nshots,
+                      const StaceyStore &ss, const int *istep_dev, cudaStream_t stream) {
+  if (f.nelem == 0) return;
+  if (ngll == 5) {
+    constexpr int N = 5, EPB = 32;
+    dim3 grid((f.nelem + EPB - 1) / EPB, 1);
+    if (medium == MED_PSV) k_stiffness<MED_PSV, N, EPB><<<grid, N * EPB, 0, stream>>>(st, f, nshots, ss, istep_dev);
+    else if (medium == MED_SH) k_stiffness<MED_SH, N, EPB><<<grid, N * EPB, 0, stream>>>(st, f, nshots, ss, istep_dev);
+    else k_stiffness<MED_AC, N, EPB><<<grid, N * EPB, 0, stream>>>(st, f, nshots, ss, istep_dev);
+  } else if (ngll == 8) {
+    constexpr int N = 8, EPB = 16;
+    dim3 grid((f.nelem + EPB - 1) / EPB, 1);
+    if (medium == MED_PSV) k_stiffness<MED_PSV, N, EPB><<<grid, N * EPB, 0, stream>>>(st, f, nshots, ss, istep_dev);
+    else if (medium == MED_SH) k_stiffness<MED_SH, N, EPB><<<grid, N * EPB, 0, stream>>>(st, f, nshots, ss, istep_dev);
+    else k_stiffness<MED_AC, N, EPB><<<grid, N * EPB, 0, stream>>>(st, f, nshots, ss, istep_dev);
+  }
+}
+
+void launch_sources(int ngll, const Static &st, const SourceSet &src, MediumFields *fields,
+                    int nshots, int medium, const int *istep_dev, int, cudaStream_t stream) {
+  if (src.n == 0) return;
+  const MediumFields &f = fields[medium];
+  if (f.nelem == 0) return;
+  k_sources<<<src.n, ngll * ngll <= 32 ? 32 : 64, 0, stream>>>(st, src, f, medium, ngll, istep_dev, 0);
+  (void)nshots;
+}
+
+void launch_coupling_acoustic(const CouplingSet &c, const MediumFields &ac, const MediumFields &el,
+                              int nshots, cudaStream_t stream) {
+  if (c.n == 0) return;
+  dim3 grid((c.n + 127) / 128, nshots);
+  k_couple_acoustic<<<grid, 128, 0, stream>>>(c, ac, el, nshots);
+}
+
+void launch_coupling_elastic(const CouplingSet &c, const MediumFields &el, const MediumFields &ac,
+                             int nshots, int ac_divided, cudaStream_t stream) {
+  if (c.n == 0) return;
+  dim3 grid((c.n + 127) / 128, nshots);
+  k_couple_elastic<<<grid, 128, 0, stream>>>(c, el, ac, nshots, ac_divided);
+}
+
+void launch_receivers(int ngll, const Static &st, const ReceiverSet &rec, const MediumFields *fields,
+                      int nshots, float dt2, int mode, const int *istep_dev, cudaStream_t stream) {
+  if (rec.n == 0 || rec.ntypes == 0) return;
+  dim3 grid(rec.n, nshots);
+  k_receivers<<<grid, 64, 0, stream>>>(st, rec, fields[MED_PSV], fields[MED_SH], fields[MED_AC], ngll,
+                                       dt2, mode, istep_dev);
+}
+
+void launch_predictor(const MediumFields &f, int nshots, float dt, float dt2, float dtsq2,
+                      cudaStream_t stream) {
+  const size_t n = field_ld(f) * nshots;
+  if (n == 0) return;
+  k_predictor<<<grid_for(n, 256), 256, 0, stream>>>(f.u, f.v, f.a, n, dt, dt2, dtsq2);
+}
+void launch_corrector(const MediumFields &f, int nshots, float dt2, cudaStream_t stream) {
+  const size_t n = field_ld(f) * nshots;
+  if (n == 0) return;
+  k_corrector<<<grid_for(n, 256), 256, 0, stream>>>(f.v, f.a, n, dt2);
+}
+void launch_divide(const MediumFields &f, int nshots, cudaStream_t stream) {
+  const size_t ld = field_ld(f);
+  if (ld == 0) return;
+  k_divide<<<grid_for(ld, 256), 256, 0, stream>>>(f.a, f.minv, ld, nshots);
+}
+void launch_fused_update(const MediumFields &f, int nshots, float dt, float dt2, float dtsq2,
+                         int last, Control *ctrl, cudaStream_t stream) {
+  const size_t ld2 = field_ld(f) / 2;
+  if (ld2 == 0) {
+    if (ctrl) k_advance<<<1, 1, 0, stream>>>(ctrl);
+    return;
+  }
+  const int grid = grid_for(ld2, 256);
+  if (last)
+    k_fused_update<true><<<grid, 256, 0, stream>>>(reinterpret_cast<float2 *>(f.u), reinterpret_cast<float2 *>(f.v),
+                                                   reinterpret_cast<float2 *>(f.a), reinterpret_cast<const float2 *>(f.minv),
+                                                   ld2, nshots, dt, dt2, dtsq2, ctrl);
+  else
+    k_fused_update<false><<<grid, 256, 0, stream>>>(reinterpret_cast<float2 *>(f.u), reinterpret_cast<float2 *>(f.v),
+                                                    reinterpret_cast<float2 *>(f.a), reinterpret_cast<const float2 *>(f.minv),
+                                                    ld2, nshots, dt, dt2, dtsq2, ctrl);
+}
+void launch_advance_step(Control *ctrl, cudaStream_t stream) { k_advance<<<1, 1, 0, stream>>>(ctrl); }
+
+void launch_mass(int medium, int ngll, const Static &st, const MediumFields &f, float dt,
+                 cudaStream_t stream) {
+  if (f.nelem == 0) return;
+  const size_t n = static_cast<size_t>(f.nelem) * ngll * ngll;
+  const int grid = grid_for(n, 256);
+  if (medium == MED_PSV) k_mass<MED_PSV><<<grid, 256, 0, stream>>>(st, f, ngll, dt);
+  else if (medium == MED_SH) k_mass<MED_SH><<<grid, 256, 0, stream>>>(st, f, ngll, dt);
+  else k_mass<MED_AC><<<grid, 256, 0, stream>>>(st, f, ngll, dt);
+}
+void launch_invert_mass(const MediumFields &f, cudaStream_t stream) {
+  const size_t n = static_cast<size_t>(f.nglob) * f.nc;
+  if (n == 0) return;
+  k_invert<<<grid_for(n, 256), 256, 0, stream>>>(f.mass, f.minv, n);
+}
+void launch_zero(float *p, size_t n, cudaStream_t stream) {
+  if (n == 0) return;
+  k_zero<<<grid_for(n, 256), 256, 0, stream>>>(p, n);
+}
+
+}  // namespace dev
+}  // namespace sfb

@@ -1,0 +1,52 @@
+// A complete simulation problem on the host: assembly, located sources and
+// receivers, time stepping and output settings.  Built either from the
+// reference's YAML parameter file (src/parameter_parser/setup.cpp) or from a
+// structured-mesh description (the benchmark workloads).
+#pragma once
+#include <string>
+#include <vector>
+
+#include "../../../include/specfem_b200.h"
+#include "assembly.hpp"
+
+namespace sfb {
+
+struct Problem {
+  Assembly asmb;
+  double dt = 0, t0 = 0;
+  int nstep = 0;
+  int nshots = 1;
+  int simulation = 0;  // 0 forward, 1 combined
+  int nstep_between_samples = 1;
+  std::vector<int> seismogram_types;
+  std::vector<Source> sources;             // as described
+  std::vector<int> source_shot;            // [nsources]
+  std::vector<LocatedSource> located_sources;
+  std::vector<Receiver> receivers;
+  std::vector<LocatedReceiver> located_receivers;
+  bool save_boundary_values = false;
+  bool elastic_sh = false;
+  // Output settings from the YAML file.
+  std::string seismogram_dir;
+  bool write_seismograms = false;
+  std::string wavefield_dir;   // forward: writer.wavefield; combined: reader
+  std::string kernel_dir;      // combined: writer.kernels
+
+  int max_sig_step() const { return nstep / nstep_between_samples; }
+
+  // Flattened copies backing sfb_problem_view.
+  std::vector<int> v_src_ispec, v_src_shot, v_src_wavefield;
+  std::vector<float> v_src_array, v_src_stf;
+  std::vector<int> v_rec_ispec;
+  std::vector<float> v_rec_lagrange, v_rec_sin, v_rec_cos;
+  std::vector<int> v_cp_ac_self, v_cp_ac_other, v_cp_el_self, v_cp_el_other;
+  std::vector<float> v_cp_ac_f, v_cp_ac_nx, v_cp_ac_nz, v_cp_el_f, v_cp_el_nx, v_cp_el_nz;
+  void finalize();  // locate sources / receivers and fill the flat copies
+  void fill_view(sfb_problem_view *v) const;
+};
+
+Problem problem_from_yaml(const std::string &parameter_file,
+                          const std::string &default_file);
+Problem problem_from_structured(const sfb_structured_desc &d);
+
+}  // namespace sfb

@@ -1,0 +1,233 @@
+"""Python host API over the C ABI: one ``Simulation`` per library context.
+
+Mirrors the reference's Python surface (``specfempp_core._execute`` runs a
+YAML parameter file, src/python/core.cpp:46-66) and adds array access for
+seismograms, fields and Frechet kernels.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _capi as A
+
+
+@dataclass
+class Material:
+    rho: float
+    vp: float
+    vs: float = 0.0  # 0 -> acoustic
+
+
+@dataclass
+class ForceSource:
+    x: float
+    z: float
+    f0: float
+    factor: float = 1e10
+    angle: float = 0.0
+    tshift: float = 0.0
+    stf: str = "ricker"  # ricker | dirac | dgaussian
+    shot: int = 0
+    kind: str = "force"  # force | moment_tensor
+    mxx: float = 0.0
+    mzz: float = 0.0
+    mxz: float = 0.0
+
+
+@dataclass
+class Station:
+    x: float
+    z: float
+    network: str = "AA"
+    station: str = ""
+    angle: float = 0.0
+
+
+@dataclass
+class StructuredProblem:
+    """A structured quad mesh problem (benchmark workloads)."""
+    nx: int
+    nz: int
+    x0: float
+    x1: float
+    z0: float
+    z1: float
+    materials: Sequence[Material]
+    element_material: Optional[np.ndarray] = None  # [nz*nx] int32
+    gll_model: Optional[tuple] = None  # (rho, vp, vs) float32 arrays [nspec, ngll, ngll]
+    absorb: tuple = (True, True, False, True)  # bottom, right, top, left
+    ngll: int = 5
+    elastic_sh: bool = False
+    dt: float = 1e-3
+    nstep: int = 100
+    t0: float = 0.0
+    nshots: int = 1
+    sources: Sequence[ForceSource] = field(default_factory=list)
+    stations: Sequence[Station] = field(default_factory=list)
+    seismogram_types: Sequence[str] = ("displacement",)
+    nstep_between_samples: int = 1
+    simulation: int = 0
+    save_boundary_values: bool = False
+
+
+def _fptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+class Simulation:
+    """A simulation context (device buffers are created on first GPU use)."""
+
+    def __init__(self, handle):
+        self._h = handle
+        self._lib = A.load()
+        self._keep = []
+
+    # ---- construction ---------------------------------------------------
+    @classmethod
+    def from_yaml(cls, parameter_file: str, default_file: Optional[str] = None) -> "Simulation":
+        lib = A.load()
+        h = C.c_void_p()
+        rc = lib.sfb_create_from_yaml(parameter_file.encode(),
+                                      default_file.encode() if default_file else None, C.byref(h))
+        A.check(rc, None)
+        return cls(h)
+
+    @classmethod
+    def structured(cls, p: StructuredProblem) -> "Simulation":
+        lib = A.load()
+        keep = []
+        d = A.sfb_structured_desc()
+        d.nx, d.nz = p.nx, p.nz
+        d.x0, d.x1, d.z0, d.z1 = p.x0, p.x1, p.z0, p.z1
+        for k in range(4):
+            d.absorb[k] = 1 if p.absorb[k] else 0
+        d.ngll = p.ngll
+        d.elastic_sh = 1 if p.elastic_sh else 0
+        mats = (A.sfb_material * len(p.materials))(*[A.sfb_material(m.rho, m.vp, m.vs) for m in p.materials])
+        keep.append(mats)
+        d.nmaterials = len(p.materials)
+        d.materials = mats
+        em = p.element_material
+        if em is None:
+            em = np.zeros(p.nx * p.nz, dtype=np.int32)
+        em = np.ascontiguousarray(em, dtype=np.int32)
+        keep.append(em)
+        d.element_material = em.ctypes.data_as(C.POINTER(C.c_int))
+        if p.gll_model is not None:
+            arrs = [np.ascontiguousarray(a, dtype=np.float32) for a in p.gll_model]
+            keep += arrs
+            d.gll_rho, d.gll_vp, d.gll_vs = (_fptr(a) for a in arrs)
+        d.dt, d.nstep, d.t0, d.nshots = p.dt, p.nstep, p.t0, p.nshots
+        srcs = (A.sfb_source_desc * max(1, len(p.sources)))()
+        stf_code = {"ricker": 0, "dirac": 1, "dgaussian": 2}
+        for i, s in enumerate(p.sources):
+            srcs[i].kind = 0 if s.kind == "force" else 1
+            srcs[i].shot = s.shot
+            srcs[i].wavefield = 0
+            srcs[i].stf = stf_code[s.stf]
+            srcs[i].x, srcs[i].z, srcs[i].angle = s.x, s.z, s.angle
+            srcs[i].mxx, srcs[i].mzz, srcs[i].mxz = s.mxx, s.mzz, s.mxz
+            srcs[i].f0 = s.f0 if s.stf != "dirac" else 1.0 / (10.0 * p.dt)
+            srcs[i].tshift, srcs[i].factor = s.tshift, s.factor
+        keep.append(srcs)
+        d.nsources, d.sources = len(p.sources), srcs
+        recs = (A.sfb_receiver_desc * max(1, len(p.stations)))()
+        names = []
+        for i, r in enumerate(p.stations):
+            net = r.network.encode()
+            sta = (r.station or "S%04d" % (i + 1)).encode()
+            names += [net, sta]
+            recs[i].network, recs[i].station = net, sta
+            recs[i].x, recs[i].z, recs[i].angle = r.x, r.z, r.angle
+        keep += [recs, names]
+        d.nreceivers, d.receivers = len(p.stations), recs
+        types = np.array([A.SEISMOGRAM_TYPES[t] for t in p.seismogram_types], dtype=np.int32)
+        keep.append(types)
+        d.nseismogram_types = len(types)
+        d.seismogram_types = types.ctypes.data_as(C.POINTER(C.c_int))
+        d.nstep_between_samples = p.nstep_between_samples
+        d.simulation = p.simulation
+        d.save_boundary_values = 1 if p.save_boundary_values else 0
+        h = C.c_void_p()
+        A.check(lib.sfb_create_structured(C.byref(d), C.byref(h)), None)
+        return cls(h)
+
+    def close(self):
+        if self._h:
+            self._lib.sfb_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def _check(self, rc):
+        return A.check(rc, self._h)
+
+    # ---- info / view ----------------------------------------------------
+    def info(self) -> A.sfb_info:
+        i = A.sfb_info()
+        self._check(self._lib.sfb_get_info(self._h, C.byref(i)))
+        return i
+
+    def problem_view(self) -> A.sfb_problem_view:
+        v = A.sfb_problem_view()
+        self._check(self._lib.sfb_get_problem_view(self._h, C.byref(v)))
+        return v
+
+    # ---- reference-granularity entry points ------------------------------
+    def initialize(self, wavefield: int = 0, dt: Optional[float] = None):
+        if dt is None:
+            dt = self.info().dt
+        self._check(self._lib.sfb_domain_initialize(self._h, wavefield, dt))
+
+    def run_forward(self, nstep: Optional[int] = None, graph: bool = True):
+        if nstep is None:
+            nstep = self.info().nstep
+        self._check(self._lib.sfb_run_forward(self._h, nstep, 1 if graph else 0))
+
+    def run_forward_unfused(self, nstep: Optional[int] = None):
+        if nstep is None:
+            nstep = self.info().nstep
+        self._check(self._lib.sfb_run_forward_unfused(self._h, nstep))
+
+    def seismograms(self, wavefield: int = 0, shot: int = 0) -> np.ndarray:
+        i = self.info()
+        out = np.zeros((i.max_sig_step, i.nseismogram_types, i.nreceivers, 2), dtype=np.float32)
+        self._check(self._lib.sfb_get_seismograms(self._h, wavefield, shot, _fptr(out), out.size))
+        return out
+
+    def field(self, medium: int, which: int, wavefield: int = 0, shot: int = 0) -> np.ndarray:
+        i = self.info()
+        nc = 2 if medium == A.MEDIUM_ELASTIC_PSV else 1
+        out = np.zeros((nc, i.nglob[medium]), dtype=np.float32)
+        self._check(self._lib.sfb_get_field(self._h, wavefield, medium, which, shot, _fptr(out), out.size))
+        return out
+
+    def set_field(self, medium: int, which: int, values: np.ndarray, wavefield: int = 0, shot: int = 0):
+        v = np.ascontiguousarray(values, dtype=np.float32)
+        self._check(self._lib.sfb_set_field(self._h, wavefield, medium, which, shot, _fptr(v), v.size))
+
+    def write_seismograms(self, directory: str, wavefield: int = 0, shot: int = 0):
+        self._check(self._lib.sfb_write_seismograms(self._h, wavefield, shot, directory.encode()))
+
+    def seismogram_times(self) -> np.ndarray:
+        i = self.info()
+        k = np.arange(i.max_sig_step, dtype=np.float32)
+        return (k * np.float32(i.dt) * np.float32(i.nstep_between_samples) + np.float32(i.t0)).astype(np.float32)
