@@ -1,0 +1,337 @@
+#!/usr/bin/env python
+"""Benchmark of the SEM time-marching hot path on B200.
+
+Workload (default): the coupled acoustic-elastic forward of 400 x 300 NGLL=5
+elements over 20 km x 15 km (see specfempp_b200/workloads.py), synthetic
+seeded model, FP32.  A "step" is one Newmark time step of the whole domain.
+The metric is GLL point updates per second: nshots * nglob * steps / time,
+nglob summed over media.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload coupled|plain|batched]
+
+Under torchrun each rank runs an independent replica (the path does not
+shard; "replicas only"); the reported value sums all ranks' point updates
+over the slowest rank's device time.  `--impl reference` times the CPU
+restatement of the reference (oracle/) on the host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+GRAPH_STEPS = 26  # one CUDA-graph chunk (25 fused steps) + the closing step
+
+
+def env_int(name, default):
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+def make_problem(workload: str, nstep: int):
+    from specfempp_b200 import workloads as W
+    if workload == "coupled":
+        return W.coupled(1.0, nstep=nstep, seismogram_types=("pressure",))
+    if workload == "plain":
+        return W.plain_elastic(1.0, nstep=nstep)
+    if workload == "batched":
+        return W.batched(1.0, nshots=64, nstep=nstep)
+    raise SystemExit("unknown workload " + workload)
+
+
+def workload_config(workload, info, p):
+    return {
+        "workload": {"coupled": "coupled acoustic-elastic 2D forward, 400x300 NGLL=5 elements, 20x15 km",
+                     "plain": "plain elastic P-SV 2D forward, 100x80 NGLL=5 elements, 4x3 km",
+                     "batched": "batched elastic P-SV 2D forward, 800x400 NGLL=5 elements, 64 shots"}[workload],
+        "nspec": int(info.nspec),
+        "nglob": int(sum(info.nglob)),
+        "nshots": int(info.nshots),
+        "dt": float(info.dt),
+        "receivers": int(info.nreceivers),
+    }
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.samples = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.QUERY,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                self.samples.append(parts)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4)
+                          if s[5 + k].lower() in ("active", "1")})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic(name):
+    """DRAM bytes per launch of the dominant kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", name)
+    try:
+        for line in open(path):
+            if line.startswith("dram_bytes_per_launch_full_size:"):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+def stiffness_bytes(info, problem_view, medium):
+    """Algorithmic bytes of one stiffness launch of `medium`: per local point
+    4 (global index) + 4 * 5 (geometry) + 4 * P (material; P = 3 elastic,
+    2 acoustic), plus one read of the displacement and one write of the force
+    per shot and DOF."""
+    nel = info.nelements[medium]
+    nn = info.ngll * info.ngll
+    P = 3 if medium in (0, 1) else 2
+    C = 2 if medium == 0 else 1
+    return nel * nn * (4 + 4 * 5 + 4 * P) + info.nshots * info.nglob[medium] * C * 4 * 2
+
+
+def cpu_rate(workload, nstep_hint, threads, budget_s=12.0, sample_steps=None):
+    """GLL point updates/s of the oracle (FP32 CPU restatement) on the host cores."""
+    from oracle import bridge
+    from specfempp_b200 import Simulation
+    probe = 3
+    p = make_problem(workload, max(probe, 4))
+    sim = Simulation.structured(p)
+    t = time.perf_counter()
+    bridge.forward(sim, 32, nstep=probe, threads=threads)
+    per_step = (time.perf_counter() - t) / probe
+    n = sample_steps or max(4, min(400, int(budget_s / max(per_step, 1e-6))))
+    p = make_problem(workload, n)
+    sim = Simulation.structured(p)
+    info = sim.info()
+    t = time.perf_counter()
+    bridge.forward(sim, 32, nstep=n, threads=threads)
+    dt = time.perf_counter() - t
+    updates = info.nshots * sum(info.nglob) * n
+    return updates / dt, n, dt, info
+
+
+def run_reference(args):
+    rank = env_int("RANK", 0)
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    # warm-up (untimed), then the timed sample: each step is one full time step
+    cpu_rate(args.workload, None, threads, sample_steps=max(1, min(args.warmup, 3)))
+    steps = max(1, min(args.steps, 200))
+    rate, n, dt, info = cpu_rate(args.workload, None, threads, sample_steps=steps)
+    line = {
+        "impl": "reference", "metric": "GLL pt-updates/s", "value": rate, "unit": "GLL-point-updates/s",
+        "n_gpus": args.gpus, "steps": n, "warmup": args.warmup, "ms_per_step": 1000.0 * dt / n,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded model with the workload's shapes and distributions)",
+        "config": workload_config(args.workload, info, None),
+        "cpu_baseline": {"value": rate, "unit": "GLL-point-updates/s", "cores": threads, "kind": "port",
+                         "sample": "%d full time steps of the workload (oracle FP32, OpenMP over elements)" % n},
+        "e2e": {"value": rate, "unit": "GLL-point-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import ctypes as C
+    import torch
+    import torch.distributed as dist
+    from specfempp_b200 import Simulation, _capi as A
+
+    world = env_int("WORLD_SIZE", 1)
+    rank = env_int("RANK", 0)
+    local = env_int("LOCAL_RANK", 0)
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    K, Wm = args.steps, args.warmup
+    nstep_total = GRAPH_STEPS + Wm + 2 * K + 2
+    p = make_problem(args.workload, nstep_total)
+    sim = Simulation.structured(p)
+    sim.initialize()
+    info = sim.info()
+    lib = A.load()
+    ptr = C.c_void_p()
+    A.check(lib.sfb_get_stream(sim.handle, C.byref(ptr)), sim.handle)
+    stream = torch.cuda.ExternalStream(ptr.value)
+
+    # set-up: capture the CUDA graph of one 25-step chunk, then W warm-up steps
+    sim.run_forward(GRAPH_STEPS)
+    sim.run_forward(Wm)
+    launches0 = sim.info().kernel_launches
+
+    sampler = ClockSampler(local)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    sim.run_forward(K)
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1)
+    launches = sim.info().kernel_launches - launches0
+    if world > 1:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    npts = sum(info.nglob)
+    value = world * info.nshots * npts * K / (ms / 1000.0)
+
+    # end to end through the C ABI with host buffers: upload the source time
+    # functions (H2D), run K steps, read the seismograms back (D2H)
+    view = sim.problem_view()
+    nsrc = view.nsources
+    stf = [np.ctypeslib.as_array(view.src_stf, shape=(nsrc * info.nstep * 2,))[i * info.nstep * 2:(i + 1) * info.nstep * 2].copy()
+           for i in range(nsrc)]
+    stf_pinned = [torch.from_numpy(s).pin_memory() for s in stf]
+    seis = torch.empty((info.max_sig_step, info.nseismogram_types, info.nreceivers, 2),
+                       dtype=torch.float32).pin_memory()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for i in range(nsrc):
+        A.check(lib.sfb_set_source_time_function(sim.handle, i, C.cast(stf_pinned[i].data_ptr(), C.POINTER(C.c_float)),
+                                                 stf_pinned[i].numel()), sim.handle)
+    sim.run_forward(K)
+    A.check(lib.sfb_get_seismograms(sim.handle, 0, 0, C.cast(seis.data_ptr(), C.POINTER(C.c_float)), seis.numel()),
+            sim.handle)
+    f1.record(stream)
+    f1.synchronize()
+    ms_e2e = f0.elapsed_time(f1)
+    if world > 1:
+        t = torch.tensor([ms_e2e], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+    e2e_value = world * info.nshots * npts * K / (ms_e2e / 1000.0)
+    h2d = nsrc * 2 * 4  # one STF sample pair per source per step
+    d2h = info.nshots * info.nseismogram_types * info.nreceivers * 2 * 4 // max(1, info.nstep_between_samples)
+
+    # roofline of the dominant kernel (elastic stiffness)
+    dominant = 0 if info.nelements[0] > 0 else (3 if info.nelements[3] > 0 else 1)
+    mean_ms = C.c_double()
+    A.check(lib.sfb_time_stiffness(sim.handle, dominant, 20, C.byref(mean_ms)), sim.handle)
+    bytes_launch = stiffness_bytes(info, view, dominant)
+    achieved = bytes_launch / (mean_ms.value / 1000.0) / 1e9
+    peak, peak_kind = measured_peak()
+    traffic = profiled_traffic("stiffness_%s.txt" % args.workload)
+
+    if rank != 0:
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        return 0
+    line = {
+        "metric": "GLL pt-updates/s", "value": value, "unit": "GLL-point-updates/s", "n_gpus": world,
+        "steps": K, "warmup": Wm, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded model with the workload's shapes and distributions)",
+        "config": dict(workload_config(args.workload, info, p), parallelism="replicas" if world > 1 else "single",
+                       l2_policy="working set %.0f MB > 126 MB L2; no flush" % (info.device_bytes / 1e6)),
+        "roofline": {"bound": "hbm", "kernel": "stiffness (medium %d)" % dominant, "achieved": achieved,
+                     "peak": peak, "peak_kind": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
+                     "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                     "algorithmic_bytes_per_launch": bytes_launch, "mean_launch_ms": mean_ms.value},
+        "e2e": {"value": e2e_value, "unit": "GLL-point-updates/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        rate, n, dt, _ = cpu_rate(args.workload, None, threads, budget_s=args.cpu_seconds)
+        line["cpu_baseline"] = {"value": rate, "unit": "GLL-point-updates/s", "cores": threads, "kind": "port",
+                                "sample": "%d full time steps of the workload (oracle FP32, OpenMP over elements), %.1f s" % (n, dt)}
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="coupled", choices=["coupled", "plain", "batched"])
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -123,6 +123,7 @@ typedef struct sfb_info {
   int simulation;        /* 0 forward, 1 combined                            */
   double dt, t0;
   size_t device_bytes;   /* device memory held by the context                */
+  uint64_t kernel_launches; /* kernels this context has launched so far      */
 } sfb_info;
 SFB_API int sfb_get_info(const sfb_context *ctx, sfb_info *info);
 
@@ -203,6 +204,24 @@ SFB_API int sfb_copy_forward_to_backward(const sfb_context *src,
  * (src/io/seismogram/writer.cpp:23-88) into `directory`. */
 SFB_API int sfb_write_seismograms(const sfb_context *ctx, int wavefield,
                                   int shot, const char *directory);
+
+/* Replace the source time function of source `isource` ([nstep][2] samples,
+ * the second column only used by two-component media).  The reference's
+ * counterpart is an `external` source time function
+ * (src/source_time_function/external.cpp). */
+SFB_API int sfb_set_source_time_function(sfb_context *ctx, int isource,
+                                         const float *host, size_t count);
+
+/* ---- measurement hooks (no reference counterpart) ----------------------- */
+
+/* The CUDA stream all work of `ctx` is enqueued on (cudaStream_t). */
+SFB_API int sfb_get_stream(const sfb_context *ctx, void **stream);
+/* Launch the stiffness kernel of `medium` (forward wavefield) `reps` times on
+ * the context stream between two CUDA events and report the mean duration in
+ * milliseconds.  The force accumulator is cleared afterwards, so a run can
+ * follow. */
+SFB_API int sfb_time_stiffness(sfb_context *ctx, int medium, int reps,
+                               double *mean_ms);
 
 /* ---- problem export (host arrays; valid while the context lives) ------- */
 

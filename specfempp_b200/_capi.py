@@ -77,7 +77,7 @@ class sfb_info(C.Structure):
         ("nglob", C.c_int * 4), ("nelements", C.c_int * 4),
         ("nreceivers", C.c_int), ("nseismogram_types", C.c_int), ("nsources", C.c_int),
         ("simulation", C.c_int), ("dt", C.c_double), ("t0", C.c_double),
-        ("device_bytes", C.c_size_t),
+        ("device_bytes", C.c_size_t), ("kernel_launches", C.c_uint64),
     ]
 
 
@@ -134,6 +134,9 @@ SIGNATURES = {
     "sfb_copy_forward_to_backward": (C.c_int, [_ctx, _ctx]),
     "sfb_write_seismograms": (C.c_int, [_ctx, C.c_int, C.c_int, C.c_char_p]),
     "sfb_get_problem_view": (C.c_int, [_ctx, _P(sfb_problem_view)]),
+    "sfb_set_source_time_function": (C.c_int, [_ctx, C.c_int, _P(C.c_float), C.c_size_t]),
+    "sfb_get_stream": (C.c_int, [_ctx, _P(C.c_void_p)]),
+    "sfb_time_stiffness": (C.c_int, [_ctx, C.c_int, C.c_int, _P(C.c_double)]),
 }
 
 _lib = None

@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <stdexcept>
@@ -89,6 +90,8 @@ struct sfb_context {
   DBuf<float> mat0_all, mat1_all, mat2_all;
   DBuf<uint8_t> eflag, bnd;
   DBuf<float> bnd_nx, bnd_nz, bnd_w;
+  DBuf<float> pack;  // [nspec][8][N*N] static block for the TMA-fed stiffness kernel
+  DBuf<int> dflag;   // device error flag
   DBuf<float> minv[4];
   DBuf<double> mass[4];
   // sources (forward / backward wavefield) and receivers
@@ -108,8 +111,18 @@ struct sfb_context {
   DBuf<int> stacey_slot;
   int nstacey = 0;
   std::vector<float> host_seis;
+  // seismogram taps per medium (fused path)
+  struct Taps {
+    DBuf<uint32_t> mask;
+    DBuf<int> sup_g, sup_begin, slot, which;
+    DBuf<float> w;
+    int nsup = 0;
+  } taps[4];
+  bool taps_ready = false;
+  DBuf<unsigned> done;  // CTA completion counter of the update kernel
   cudaGraphExec_t graph = nullptr;
   int graph_steps = 0;
+  uint64_t launches = 0;  // kernels launched so far (graph replays included)
 
   ~sfb_context() {
     if (graph) cudaGraphExecDestroy(graph);
@@ -223,7 +236,26 @@ void ensure_device(sfb_context *c) {
       eflag[d] |= a.bnd[p];
     }
   }
+  // packed per-element static block: iglob, xix, xiz, gammax, gammaz, jac, mat0, mat1
+  std::vector<float> pack(nloc * dev::kPackFields);
+  for (int d = 0; d < a.nspec; ++d)
+    for (int k = 0; k < nn; ++k) {
+      const size_t q = static_cast<size_t>(d) * nn + k;
+      float *blk = &pack[static_cast<size_t>(d) * dev::kPackFields * nn];
+      int gi = iglob[q];
+      std::memcpy(&blk[0 * nn + k], &gi, 4);
+      blk[1 * nn + k] = xix[q];
+      blk[2 * nn + k] = xiz[q];
+      blk[3 * nn + k] = gax[q];
+      blk[4 * nn + k] = gaz[q];
+      blk[5 * nn + k] = jac[q];
+      blk[6 * nn + k] = m0[q];
+      blk[7 * nn + k] = m1[q];
+    }
   size_t *tot = &c->device_bytes;
+  c->pack.upload(pack, tot);
+  c->dflag.alloc(1, tot);
+  if (const char *v = std::getenv("SFB_STIFFNESS")) dev::set_stiffness_variant(std::string(v) == "registers" ? 1 : 0);
   c->iglob.upload(iglob, tot);
   c->xix.upload(xix, tot);
   c->xiz.upload(xiz, tot);
@@ -254,6 +286,8 @@ void ensure_device(sfb_context *c) {
   c->st.bnd_nx = c->bnd_nx.p;
   c->st.bnd_nz = c->bnd_nz.p;
   c->st.bnd_w = c->bnd_w.p;
+  c->st.pack = c->pack.p;
+  c->st.err = c->dflag.p;
   for (int m : kMedia) {
     const size_t ld = static_cast<size_t>(a.nglob[m] + (a.nglob[m] & 1)) * a.ncomp(m);
     c->minv[m].alloc(ld, tot);
@@ -398,6 +432,142 @@ void set_step(sfb_context *c, WavefieldSet &W, int istep) {
   W.step = istep;
 }
 
+
+// Seismograms of the fused path as a sparse linear map of nodal values:
+// for every receiver, seismogram type and output component, the weights of
+// the element's nodal (field, component) values.  They fold the Lagrange
+// interpolant, the gradient operator and material of the pressure /
+// acoustic-displacement transforms (include/medium/dim2/*/isotropic/
+// wavefield.hpp) and the receiver rotation (receivers.hpp:126-141).
+void build_taps(sfb_context *c) {
+  if (c->taps_ready) return;
+  const Problem &P = c->P;
+  const Assembly &a = P.asmb;
+  const int n = a.ngll, nn = n * n;
+  const int nrec = static_cast<int>(P.receivers.size());
+  const int ntypes = static_cast<int>(P.seismogram_types.size());
+  struct E { int g, slot, which; double w; };
+  std::vector<E> ent[4];
+  for (int r = 0; r < nrec; ++r) {
+    const LocatedReceiver &L = P.located_receivers[r];
+    const int e = L.ispec, m = a.medium[e];
+    const double cs = L.cos_angle, sn = L.sin_angle;
+    for (int it = 0; it < ntypes; ++it) {
+      const int type = P.seismogram_types[it];
+      std::vector<double> W(static_cast<size_t>(nn) * 4, 0.0);  // [q][ic][oc]
+      auto add = [&](int q, int ic, double v0, double v1) {
+        W[(q * 2 + ic) * 2 + 0] += cs * v0 - sn * v1;
+        W[(q * 2 + ic) * 2 + 1] += sn * v0 + cs * v1;
+      };
+      int which = type;
+      for (int k = 0; k < nn; ++k) {
+        const double h = L.lagrange[k];
+        const size_t p = static_cast<size_t>(e) * nn + k;
+        const int kz = k / n, kx = k % n;
+        if (m != MEDIUM_ACOUSTIC && type <= 2) {
+          add(k, 0, h, 0.0);  // wavefield = (u0, u1): out = R (sum h u0, sum h u1)
+          if (m == MEDIUM_ELASTIC_PSV) add(k, 1, 0.0, h);
+        } else if (m == MEDIUM_ELASTIC_PSV && type == 3) {
+          which = 0;
+          const double l2m = a.kappa[p] + (4.0 / 3.0) * a.mu[p];
+          const double cf = -((l2m - 2.0 * a.mu[p]) + (2.0 / 3.0) * a.mu[p]) * h;
+          for (int l = 0; l < n; ++l) {
+            const double hx = a.quad.hprime[kx * n + l], hz = a.quad.hprime[kz * n + l];
+            add(kz * n + l, 0, cf * a.xix[p] * hx, 0.0);
+            add(l * n + kx, 0, cf * a.gammax[p] * hz, 0.0);
+            add(kz * n + l, 1, cf * a.xiz[p] * hx, 0.0);
+            add(l * n + kx, 1, cf * a.gammaz[p] * hz, 0.0);
+          }
+        } else if (m == MEDIUM_ACOUSTIC && type == 3) {
+          which = 2;
+          add(k, 0, -h, 0.0);
+        } else if (m == MEDIUM_ACOUSTIC) {
+          const double ri = a.rho_inverse[p];
+          for (int l = 0; l < n; ++l) {
+            const double hx = a.quad.hprime[kx * n + l], hz = a.quad.hprime[kz * n + l];
+            add(kz * n + l, 0, h * ri * a.xix[p] * hx, h * ri * a.xiz[p] * hx);
+            add(l * n + kx, 0, h * ri * a.gammax[p] * hz, h * ri * a.gammaz[p] * hz);
+          }
+        }
+      }
+      const int nc = a.ncomp(m);
+      for (int q = 0; q < nn; ++q)
+        for (int ic = 0; ic < nc; ++ic)
+          for (int oc = 0; oc < 2; ++oc) {
+            const double w = W[(q * 2 + ic) * 2 + oc];
+            if (w == 0.0) continue;
+            ent[m].push_back({a.iglob[static_cast<size_t>(e) * nn + q], (it * nrec + r) * 2 + oc, which * 2 + ic, w});
+          }
+    }
+  }
+  size_t *tot = &c->device_bytes;
+  for (int m : kMedia) {
+    auto &T = c->taps[m];
+    auto &v = ent[m];
+    std::sort(v.begin(), v.end(), [](const E &x, const E &y) { return x.g < y.g; });
+    std::vector<int> sup_g, sup_begin, slot, which;
+    std::vector<float> w;
+    for (size_t i = 0; i < v.size(); ++i) {
+      if (sup_g.empty() || sup_g.back() != v[i].g) {
+        sup_g.push_back(v[i].g);
+        sup_begin.push_back(static_cast<int>(slot.size()));
+      }
+      slot.push_back(v[i].slot);
+      which.push_back(v[i].which);
+      w.push_back(static_cast<float>(v[i].w));
+    }
+    sup_begin.push_back(static_cast<int>(slot.size()));
+    const int nglob = a.nglob[m];
+    std::vector<uint32_t> mask((nglob + 2 + 31) / 32, 0u);
+    for (int g : sup_g) mask[g >> 5] |= 1u << (g & 31);
+    T.nsup = static_cast<int>(sup_g.size());
+    T.mask.upload(mask, tot);
+    T.sup_g.upload(sup_g, tot);
+    T.sup_begin.upload(sup_begin, tot);
+    T.slot.upload(slot, tot);
+    T.which.upload(which, tot);
+    T.w.upload(w, tot);
+  }
+  c->done.alloc(1, tot);
+  c->taps_ready = true;
+}
+
+dev::UpdateParams update_params(sfb_context *c, WavefieldSet &W, int last, bool advance, bool taps) {
+  const Problem &P = c->P;
+  dev::UpdateParams u{};
+  u.nm = 0;
+  u.begin[0] = 0;
+  for (int m : kMedia) {
+    const dev::MediumFields &f = W.f[m];
+    if (f.nglob == 0) continue;
+    dev::UpdateMedium &M = u.m[u.nm];
+    M.u = f.u;
+    M.v = f.v;
+    M.a = f.a;
+    M.minv = f.minv;
+    M.ld2 = static_cast<size_t>(f.nglob + (f.nglob & 1)) * f.nc / 2;
+    M.nc = f.nc;
+    if (taps && c->taps[m].nsup > 0) {
+      const auto &T = c->taps[m];
+      M.taps = {T.nsup, T.mask.p, T.sup_g.p, T.sup_begin.p, T.slot.p, T.which.p, T.w.p};
+    }
+    u.begin[u.nm + 1] = u.begin[u.nm] + M.ld2;
+    ++u.nm;
+  }
+  u.nshots = P.nshots;
+  u.dt = static_cast<float>(P.dt);
+  u.dt2 = static_cast<float>(P.dt / 2.0);
+  u.dtsq2 = static_cast<float>(P.dt * P.dt / 2.0);
+  u.last = last;
+  u.ctrl = advance ? W.ctrl.p : nullptr;
+  u.done = c->done.p;
+  u.seis = taps ? W.seis.p : nullptr;
+  u.slots = static_cast<int>(P.seismogram_types.size() * P.receivers.size() * 2);
+  u.max_sig = P.max_sig_step();
+  u.nsbs = P.nstep_between_samples;
+  return u;
+}
+
 // One fused forward step: sources, coupling and stiffness per medium in the
 // reference order, seismograms, then the update kernels.
 void enqueue_fused_step(sfb_context *c, WavefieldSet &W, int last) {
@@ -415,18 +585,39 @@ void enqueue_fused_step(sfb_context *c, WavefieldSet &W, int last) {
     ss.mode = 1;
   }
   dev::SourceSet src = source_set(c);
-  // acoustic first (time_marching.tpp:48-52)
+  if (dev::stiffness_fuses_tail(c->st)) {
+    // acoustic first (time_marching.tpp:48-52): stiffness + sources + coupling
+    // from the predicted elastic displacement, in one launch
+    dev::TailWork ta{};
+    ta.src = src;
+    ta.cp = coupling_acoustic(c);
+    ta.other = W.f[dev::MED_PSV];
+    ta.cp_mode = ta.cp.n > 0 ? 1 : 0;
+    dev::launch_stiffness(dev::MED_AC, n, c->st, W.f[dev::MED_AC], S, ss, istep, c->stream, &ta);
+    // elastic: coupling reads the final acoustic acceleration = force * minv
+    dev::TailWork te{};
+    te.src = src;
+    te.cp = coupling_elastic(c);
+    te.other = W.f[dev::MED_AC];
+    te.cp_mode = te.cp.n > 0 ? 2 : 0;
+    te.other_divided = 0;
+    dev::launch_stiffness(dev::MED_PSV, n, c->st, W.f[dev::MED_PSV], S, ss, istep, c->stream, &te);
+    dev::TailWork tsh{};
+    tsh.src = src;
+    dev::launch_stiffness(dev::MED_SH, n, c->st, W.f[dev::MED_SH], S, ss, istep, c->stream, &tsh);
+    build_taps(c);
+    dev::launch_update_all(update_params(c, W, last, true, true), c->stream);
+    return;
+  }
   dev::launch_coupling_acoustic(coupling_acoustic(c), W.f[dev::MED_AC], W.f[dev::MED_PSV], S, c->stream);
   dev::launch_sources(n, c->st, src, W.f, S, dev::MED_AC, istep, 0, c->stream);
   dev::launch_stiffness(dev::MED_AC, n, c->st, W.f[dev::MED_AC], S, ss, istep, c->stream);
-  // elastic (coupling reads the final acoustic acceleration = force * minv)
   dev::launch_coupling_elastic(coupling_elastic(c), W.f[dev::MED_PSV], W.f[dev::MED_AC], S, 0, c->stream);
   for (int m : {dev::MED_PSV, dev::MED_SH}) {
     dev::launch_sources(n, c->st, src, W.f, S, m, istep, 0, c->stream);
     dev::launch_stiffness(m, n, c->st, W.f[m], S, ss, istep, c->stream);
   }
   dev::launch_receivers(n, c->st, receiver_set(c, W), W.f, S, dt2, 1, istep, c->stream);
-  // update: the step counter advances with the last launched medium
   int lastm = -1;
   for (int m : kMedia)
     if (W.f[m].nglob > 0) lastm = m;
@@ -434,6 +625,29 @@ void enqueue_fused_step(sfb_context *c, WavefieldSet &W, int last) {
     if (W.f[m].nglob == 0) continue;
     dev::launch_fused_update(W.f[m], S, dt, dt2, dtsq2, last, m == lastm ? W.ctrl.p : nullptr, c->stream);
   }
+}
+
+// Number of kernels one fused step launches (mirrors the skip conditions of
+// the launchers in kernels.cu).
+int fused_step_launches(sfb_context *c, WavefieldSet &W) {
+  const Problem &P = c->P;
+  int n = 0;
+  if (dev::stiffness_fuses_tail(c->st)) {
+    for (int m : {dev::MED_AC, dev::MED_PSV, dev::MED_SH})
+      if (W.f[m].nelem > 0) ++n;
+    return n + 1;  // one update launch
+  }
+  if (!P.v_cp_ac_self.empty()) ++n;
+  if (!P.v_cp_el_self.empty()) ++n;
+  for (int m : {dev::MED_AC, dev::MED_PSV, dev::MED_SH}) {
+    if (W.f[m].nelem == 0) continue;
+    ++n;                       // stiffness
+    if (c->nsrc > 0) ++n;      // sources
+  }
+  if (!P.receivers.empty() && !P.seismogram_types.empty()) ++n;
+  for (int m : kMedia)
+    if (W.f[m].nglob > 0) ++n;  // update
+  return n;
 }
 
 void predictor_all(sfb_context *c, WavefieldSet &W, double sgn) {
@@ -449,11 +663,15 @@ void run_forward_fused(sfb_context *c, int nstep, int use_graph) {
   if (nstep <= 0) return;
   if (W.step + nstep > c->P.nstep)
     throw std::invalid_argument("run would pass the configured number of steps");
+  if (dev::stiffness_fuses_tail(c->st)) build_taps(c);
   set_step(c, W, W.step);
   predictor_all(c, W, 1.0);
+  for (int m : kMedia)
+    if (W.f[m].nglob > 0) ++c->launches;
+  c->launches += static_cast<uint64_t>(fused_step_launches(c, W)) * nstep;
   const int body = nstep - 1;
-  if (use_graph && body > 0) {
-    const int K = std::min(body, 25);
+  constexpr int K = 25;  // fused steps per CUDA graph
+  if (use_graph && body >= K) {
     if (!c->graph || c->graph_steps != K) {
       if (c->graph) cudaGraphExecDestroy(c->graph);
       c->graph = nullptr;
@@ -554,6 +772,7 @@ SFB_API int sfb_get_info(const sfb_context *ctx, sfb_info *info) {
   info->dt = P.dt;
   info->t0 = P.t0;
   info->device_bytes = ctx->device_bytes;
+  info->kernel_launches = ctx->launches;
   return SFB_OK;
 }
 
@@ -628,11 +847,24 @@ SFB_API int sfb_newmark_corrector(sfb_context *ctx, int wavefield, int medium, i
   });
 }
 
+// A bounded device-side wait that expired leaves a flag; report it.
+void check_device_flag(sfb_context *c) {
+  if (!c->dflag.p) return;
+  int h = 0;
+  ck(cudaMemcpy(&h, c->dflag.p, sizeof(int), cudaMemcpyDeviceToHost), "error flag");
+  if (h != 0) {
+    const int zero = 0;
+    cudaMemcpy(c->dflag.p, &zero, sizeof(int), cudaMemcpyHostToDevice);
+    throw CudaError("a device-side wait timed out (bounded mbarrier wait in the stiffness kernel)");
+  }
+}
+
 SFB_API int sfb_run_forward(sfb_context *ctx, int nstep, int use_graph) {
   if (!ctx) return SFB_E_INVALID;
   return guarded(ctx, [&]() {
     run_forward_fused(ctx, nstep, use_graph);
     ck(cudaStreamSynchronize(ctx->stream), "forward run");
+    check_device_flag(ctx);
     return SFB_OK;
   });
 }
@@ -753,6 +985,61 @@ SFB_API int sfb_write_seismograms(const sfb_context *cctx, int wavefield, int sh
   return guarded(ctx, [&]() {
     write_seismograms_ascii(P, buf.data(), static_cast<int>(P.seismogram_types.size()),
                             static_cast<int>(P.receivers.size()), P.max_sig_step(), directory);
+    return SFB_OK;
+  });
+}
+
+SFB_API int sfb_set_source_time_function(sfb_context *ctx, int isource, const float *host, size_t count) {
+  if (!ctx || !host) return SFB_E_INVALID;
+  return guarded(ctx, [&]() {
+    Problem &P = ctx->P;
+    if (isource < 0 || isource >= static_cast<int>(P.v_src_ispec.size())) throw std::invalid_argument("source index out of range");
+    const size_t n = static_cast<size_t>(P.nstep) * 2;
+    if (count < n) throw std::invalid_argument("source time function buffer too small");
+    std::copy(host, host + n, P.v_src_stf.begin() + static_cast<size_t>(isource) * n);
+    if (ctx->on_device)
+      ck(cudaMemcpyAsync(ctx->src_stf.p + static_cast<size_t>(isource) * n, host, n * sizeof(float),
+                         cudaMemcpyHostToDevice, ctx->stream), "stf h2d");
+    return SFB_OK;
+  });
+}
+
+SFB_API int sfb_get_stream(const sfb_context *cctx, void **stream) {
+  sfb_context *ctx = const_cast<sfb_context *>(cctx);
+  if (!ctx || !stream) return SFB_E_INVALID;
+  return guarded(ctx, [&]() {
+    ensure_device(ctx);
+    *stream = static_cast<void *>(ctx->stream);
+    return SFB_OK;
+  });
+}
+
+SFB_API int sfb_time_stiffness(sfb_context *ctx, int medium, int reps, double *mean_ms) {
+  if (!ctx || !mean_ms || reps < 1) return SFB_E_INVALID;
+  return guarded(ctx, [&]() {
+    if (!medium_index_ok(medium)) throw std::invalid_argument("unsupported medium tag");
+    WavefieldSet &W = ensure_wavefield(ctx, SFB_WAVEFIELD_FORWARD);
+    const int n = ctx->P.asmb.ngll;
+    dev::StaceyStore ss{};
+    cudaEvent_t e0, e1;
+    ck(cudaEventCreate(&e0), "event");
+    ck(cudaEventCreate(&e1), "event");
+    ck(cudaEventRecord(e0, ctx->stream), "event record");
+    for (int r = 0; r < reps; ++r)
+      dev::launch_stiffness(medium, n, ctx->st, W.f[medium], ctx->P.nshots, ss, &W.ctrl.p->istep, ctx->stream);
+    ck(cudaEventRecord(e1, ctx->stream), "event record");
+    ck(cudaEventSynchronize(e1), "event sync");
+    float ms = 0.f;
+    ck(cudaEventElapsedTime(&ms, e0, e1), "elapsed");
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    ctx->launches += reps;
+    *mean_ms = ms / reps;
+    // the repeated launches accumulated into the force array: clear it
+    const dev::MediumFields &f = W.f[medium];
+    const size_t ld = static_cast<size_t>(f.nglob + (f.nglob & 1)) * f.nc;
+    if (ld) ck(cudaMemsetAsync(f.a, 0, ld * ctx->P.nshots * sizeof(float), ctx->stream), "clear force");
+    ck(cudaStreamSynchronize(ctx->stream), "sync");
     return SFB_OK;
   });
 }

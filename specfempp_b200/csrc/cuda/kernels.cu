@@ -10,6 +10,7 @@
 //   free surface include/boundary_conditions/dirichlet/dirichlet.hpp:19-43
 #include "kernels.cuh"
 
+#include <algorithm>
 #include <cstdio>
 
 namespace sfb {
@@ -237,6 +238,348 @@ k_stiffness(Static st, MediumFields f, int nshots, StaceyStore ss, const int *is
   }
 }
 
+
+// ---------------------------------------------------------------------------
+// TMA-fed persistent stiffness.  Each CTA walks chunks of EPB elements; the
+// chunk's packed static block (iglob, geometry, material: 8 x N*N words per
+// element, contiguous in HBM) arrives in shared memory by one bulk async copy
+// (cp.async.bulk, no multicast) completing on an mbarrier, double-buffered so
+// the next chunk streams in while this one is computed.  Thread (el, iz) owns
+// row iz of element el exactly as in k_stiffness.  Every mbarrier wait is
+// bounded; on expiry the kernel records SFB_DEVICE_WAIT_TIMEOUT in st.err and
+// the CTA returns.
+// ---------------------------------------------------------------------------
+constexpr int kWaitTimeout = 1;
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait (about 2 s at 2 GHz).  Returns false on expiry.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
+  const long long t0 = clock64();
+  while (!mbar_try_wait(bar, parity)) {
+    if (clock64() - t0 > (1LL << 32)) return false;
+  }
+  return true;
+}
+
+// Row-per-thread stiffness fed by bulk async copies, software-pipelined.
+// A CTA owns EPB elements; thread (el, iz) owns row iz of element el (N
+// points: the xi-contractions stay in registers, the gamma-contractions read
+// columns from shared memory).  CTAs walk element chunks persistently:
+//   - the next chunk's packed static block (iglob, geometry, material:
+//     8 x N*N words per element, contiguous in HBM) streams into the other
+//     shared-memory stage by one cp.async.bulk (no multicast) completing on
+//     an mbarrier while this chunk is computed;
+//   - before leaving a chunk, the thread already issues the displacement
+//     gathers of its row in the next chunk, so their latency overlaps the
+//     barrier, the force reductions and the next chunk's set-up.
+// After the chunks every CTA takes a slice of the medium's point sources
+// and fluid-solid coupling points (TailWork); they only add into the same
+// force array.  Every mbarrier wait is bounded (SFB_DEVICE_WAIT_TIMEOUT).
+template <int MED, int N, int EPB, int MINB>
+__global__ void __launch_bounds__(N * EPB, MINB)
+k_stiffness_rp(Static st, MediumFields f, int nshots, StaceyStore ss, const int *istep_dev, TailWork tw) {
+  constexpr int NC = (MED == MED_PSV) ? 2 : 1;
+  constexpr int NN = N * N;
+  constexpr int ELEM_WORDS = kPackFields * NN;
+  constexpr int STAGE_WORDS = EPB * ELEM_WORDS;
+  using V = typename Vec<NC>::T;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  float *stage = reinterpret_cast<float *>(smem_raw);      // [2][STAGE_WORDS]
+  V *s_u = reinterpret_cast<V *>(stage + 2 * STAGE_WORDS);  // [EPB][NN]
+  V *s_fg = s_u + EPB * NN;                                 // [EPB][NN] F(., gamma)
+  uint64_t *bar = reinterpret_cast<uint64_t *>(s_fg + EPB * NN);
+
+  const int t = threadIdx.x;
+  const int el = t / N, iz = t % N;
+  const int nchunks = (f.nelem + EPB - 1) / EPB;
+  if (t == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  auto issue = [&](int chunk, int stg) {
+    const int first = chunk * EPB;
+    const int count = min(EPB, f.nelem - first);
+    const uint32_t bytes = static_cast<uint32_t>(count) * ELEM_WORDS * 4u;
+    const float *src = st.pack + static_cast<size_t>(f.elem_begin + first) * ELEM_WORDS;
+    mbar_arrive_expect_tx(&bar[stg], bytes);
+    bulk_load(stage + stg * STAGE_WORDS, src, bytes, &bar[stg]);
+  };
+  float hpz[N], hpwz[N];
+#pragma unroll
+  for (int l = 0; l < N; ++l) {
+    hpz[l] = c_hp[iz * N + l];
+    hpwz[l] = c_hpw[iz * N + l];
+  }
+  const float wz = c_w[iz];
+  const int istep = (ss.mode != 0 || tw.src.n > 0) ? *istep_dev : 0;
+  const size_t ldv = static_cast<size_t>(f.nglob + (f.nglob & 1));
+  const V *vbase = reinterpret_cast<const V *>(f.u);
+  V *abase = reinterpret_cast<V *>(f.a);
+  bool ok = true;
+
+  // prologue: first chunk's static block and displacement gathers
+  int g[N];
+  V ur[N];
+  if (blockIdx.x < nchunks) {
+    if (t == 0) issue(blockIdx.x, 0);
+    if (!mbar_wait_bounded(&bar[0], 0)) ok = false;
+    const int li = blockIdx.x * EPB + el;
+    const float *blk = stage + el * ELEM_WORDS;
+#pragma unroll
+    for (int ix = 0; ix < N; ++ix) {
+      g[ix] = (ok && li < f.nelem) ? __float_as_int(blk[iz * N + ix]) : 0;
+      ur[ix] = (ok && li < f.nelem) ? vbase[g[ix]] : Vec<NC>::zero();
+    }
+  }
+
+  int iter = 0;
+  for (int chunk = blockIdx.x; ok && chunk < nchunks; chunk += gridDim.x, ++iter) {
+    const int stg = iter & 1;
+    const int next = chunk + gridDim.x;
+    if (t == 0 && next < nchunks) issue(next, stg ^ 1);
+    const float *blk = stage + stg * STAGE_WORDS + el * ELEM_WORDS;
+    const int li = chunk * EPB + el;
+    const bool valid = li < f.nelem;
+    const int e = f.elem_begin + (valid ? li : 0);
+    const uint8_t eflag = valid ? st.eflag[e] : 0;
+    const int slot = (ss.mode != 0 && valid) ? ss.slot[e] : -1;
+    for (int s = 0; s < nshots; ++s) {
+      if (s > 0) {
+#pragma unroll
+        for (int ix = 0; ix < N; ++ix) ur[ix] = valid ? vbase[s * ldv + g[ix]] : Vec<NC>::zero();
+      }
+#pragma unroll
+      for (int ix = 0; ix < N; ++ix) s_u[el * NN + iz * N + ix] = ur[ix];
+      __syncthreads();
+      V fx[N];
+#pragma unroll
+      for (int ix = 0; ix < N; ++ix) {
+        const int k = iz * N + ix;
+        const float xix = blk[1 * NN + k], xiz = blk[2 * NN + k];
+        const float gax = blk[3 * NN + k], gaz = blk[4 * NN + k];
+        const float jac = blk[5 * NN + k], m0 = blk[6 * NN + k], m1 = blk[7 * NN + k];
+        float dxi[NC], dga[NC];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) { dxi[c] = 0.f; dga[c] = 0.f; }
+#pragma unroll
+        for (int l = 0; l < N; ++l) {
+          const V col = s_u[el * NN + l * N + ix];
+#pragma unroll
+          for (int c = 0; c < NC; ++c) {
+            dxi[c] += c_hp[ix * N + l] * comp(ur[l], c);
+            dga[c] += hpz[l] * comp(col, c);
+          }
+        }
+        float du[NC][2];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+          du[c][0] = xix * dxi[c] + gax * dga[c];
+          du[c][1] = xiz * dxi[c] + gaz * dga[c];
+        }
+        float T[NC][2];
+        if constexpr (MED == MED_PSV) {
+          const float l2m = m0 + static_cast<float>(4.0 / 3.0) * m1;
+          const float lam = l2m - 2.0f * m1;
+          T[0][0] = l2m * du[0][0] + lam * du[1][1];
+          T[1][1] = l2m * du[1][1] + lam * du[0][0];
+          T[0][1] = m1 * (du[0][1] + du[1][0]);
+          T[1][0] = T[0][1];
+        } else {
+          T[0][0] = m0 * du[0][0];
+          T[0][1] = m0 * du[0][1];
+        }
+        V f0, f1;
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+          set_comp(f0, c, jac * (T[c][0] * xix + T[c][1] * xiz));
+          set_comp(f1, c, jac * (T[c][0] * gax + T[c][1] * gaz));
+        }
+        fx[ix] = f0;
+        s_fg[el * NN + k] = f1;
+      }
+      __syncthreads();
+      float accr[N][2];
+#pragma unroll
+      for (int ix = 0; ix < N; ++ix) {
+        float t1[NC], t2[NC];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) { t1[c] = 0.f; t2[c] = 0.f; }
+#pragma unroll
+        for (int l = 0; l < N; ++l) {
+          const V col = s_fg[el * NN + l * N + ix];
+#pragma unroll
+          for (int c = 0; c < NC; ++c) {
+            t1[c] += comp(fx[l], c) * c_hpw[ix * N + l];
+            t2[c] += comp(col, c) * hpwz[l];
+          }
+        }
+#pragma unroll
+        for (int c = 0; c < NC; ++c) accr[ix][c] = (wz * t1[c] + c_w[ix] * t2[c]) * -1.0f;
+      }
+      if (eflag) {
+#pragma unroll
+        for (int ix = 0; ix < N; ++ix) {
+          const size_t p = (static_cast<size_t>(e) * N + iz) * N + ix;
+          const uint8_t b = st.bnd[p];
+          if (b & 1) {
+            const V vv = reinterpret_cast<const V *>(f.v)[s * ldv + g[ix]];
+            float vel[2];
+#pragma unroll
+            for (int c = 0; c < NC; ++c) vel[c] = comp(vv, c);
+            stacey<MED>(blk[6 * NN + iz * N + ix], blk[7 * NN + iz * N + ix], st.mat2 ? st.mat2[p] : 0.f,
+                        st.bnd_nx[p], st.bnd_nz[p], st.bnd_w[p], vel, accr[ix]);
+          }
+          if (b & 2) {
+#pragma unroll
+            for (int c = 0; c < NC; ++c) accr[ix][c] = 0.f;
+          }
+        }
+      }
+      if (slot >= 0) {
+#pragma unroll
+        for (int ix = 0; ix < N; ++ix) {
+          const size_t base =
+              ((((static_cast<size_t>(s) * ss.nstep + istep) * ss.nstacey + slot) * N + iz) * N + ix) * NC;
+          if (ss.mode == 1) {
+#pragma unroll
+            for (int c = 0; c < NC; ++c) ss.data[base + c] = accr[ix][c];
+          } else {
+#pragma unroll
+            for (int c = 0; c < NC; ++c) accr[ix][c] = ss.data[base + c];
+          }
+        }
+      }
+      const bool last_shot = (s + 1 == nshots);
+      int gnext[N];
+      if (last_shot && next < nchunks) {
+        // next chunk: its static block is (or soon will be) in the other
+        // stage; take its indices and start its displacement gathers now
+        if (!mbar_wait_bounded(&bar[stg ^ 1], ((iter + 1) >> 1) & 1)) {
+          ok = false;
+        } else {
+          const float *nblk = stage + (stg ^ 1) * STAGE_WORDS + el * ELEM_WORDS;
+          const bool nvalid = next * EPB + el < f.nelem;
+#pragma unroll
+          for (int ix = 0; ix < N; ++ix) gnext[ix] = nvalid ? __float_as_int(nblk[iz * N + ix]) : 0;
+        }
+      }
+      if (valid) {
+#pragma unroll
+        for (int ix = 0; ix < N; ++ix) {
+          V out;
+#pragma unroll
+          for (int c = 0; c < NC; ++c) set_comp(out, c, accr[ix][c]);
+          red_add(abase + s * ldv + g[ix], out);
+        }
+      }
+      if (last_shot && next < nchunks && ok) {
+        const bool nvalid = next * EPB + el < f.nelem;
+#pragma unroll
+        for (int ix = 0; ix < N; ++ix) {
+          g[ix] = gnext[ix];
+          ur[ix] = nvalid ? vbase[g[ix]] : Vec<NC>::zero();
+        }
+      }
+      __syncthreads();
+    }
+  }
+  if (!ok) {
+    if (t == 0) atomicExch(st.err, kWaitTimeout);
+    return;
+  }
+
+  // ---- tail: point sources and fluid-solid coupling of this medium --------
+  const int gtid = blockIdx.x * blockDim.x + t;
+  const int gstride = gridDim.x * blockDim.x;
+  if (tw.src.n > 0 && istep >= 0 && istep < tw.src.nstep) {
+    for (int idx = gtid; idx < tw.src.n * NN; idx += gstride) {
+      const int i = idx / NN, kk = idx % NN;
+      if (tw.src.medium[i] != MED) continue;
+      const size_t p = static_cast<size_t>(tw.src.elem[i]) * NN + kk;
+      const int gi = st.iglob[p];
+      float *A = f.a + static_cast<size_t>(tw.src.shot[i]) * ldv * NC;
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        const float stf = tw.src.stf[(static_cast<size_t>(i) * tw.src.nstep + istep) * 2 + c];
+        const float arr = tw.src.array[(static_cast<size_t>(i) * 2 + c) * NN + kk];
+        float val = stf * arr;
+        if (MED == MED_AC) val = stf * arr / st.mat1[p];
+        atomicAdd(A + static_cast<size_t>(gi) * NC + c, val);
+      }
+    }
+  }
+  if (tw.cp_mode != 0) {
+    const int n = tw.cp.n;
+    for (int idx = gtid; idx < n * nshots; idx += gstride) {
+      const int i = idx % n, s = idx / n;
+      const MediumFields &o = tw.other;
+      const size_t ldo = static_cast<size_t>(o.nglob + (o.nglob & 1));
+      if (tw.cp_mode == 1) {  // acoustic self += w (n . u_elastic)
+        const float2 u = reinterpret_cast<const float2 *>(o.u)[s * ldo + tw.cp.other[i]];
+        atomicAdd(f.a + s * ldv + tw.cp.self[i], tw.cp.factor[i] * (tw.cp.nx[i] * u.x + tw.cp.nz[i] * u.y));
+      } else {  // elastic self += w n chi_ddot
+        const int oi = tw.cp.other[i];
+        const float r = o.a[s * ldo + oi];
+        const float chi_dd = tw.other_divided ? r : r * o.minv[oi];
+        float *A = f.a + (s * ldv + tw.cp.self[i]) * 2;
+        atomicAdd(A, tw.cp.factor[i] * tw.cp.nx[i] * chi_dd);
+        atomicAdd(A + 1, tw.cp.factor[i] * tw.cp.nz[i] * chi_dd);
+      }
+    }
+  }
+}
+
+template <int MED, int N, int EPB>
+size_t rp_smem_bytes() {
+  constexpr int NC = (MED == MED_PSV) ? 2 : 1;
+  return 2 * EPB * kPackFields * N * N * 4 + 2 * EPB * N * N * NC * 4 + 16;
+}
+
+template <int MED, int N, int EPB, int MINB>
+void launch_rp(const Static &st, const MediumFields &f, int nshots, const StaceyStore &ss, const int *istep_dev,
+               const TailWork &tw, cudaStream_t stream) {
+  static int blocks_per_sm = -1, nsm = 0;
+  const size_t smem = rp_smem_bytes<MED, N, EPB>();
+  if (blocks_per_sm < 0) {
+    cudaFuncSetAttribute(k_stiffness_rp<MED, N, EPB, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         static_cast<int>(smem));
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_stiffness_rp<MED, N, EPB, MINB>, N * EPB, smem);
+    if (blocks_per_sm < 1) blocks_per_sm = 1;
+  }
+  const int nchunks = (f.nelem + EPB - 1) / EPB;
+  const int grid = std::max(1, std::min(nchunks, nsm * blocks_per_sm));
+  k_stiffness_rp<MED, N, EPB, MINB><<<grid, N * EPB, smem, stream>>>(st, f, nshots, ss, istep_dev, tw);
+}
+
 // ---------------------------------------------------------------------------
 // Point sources (compute_source_interaction.tpp:77-95): one block per source.
 // ---------------------------------------------------------------------------
@@ -455,6 +798,99 @@ __global__ void k_fused_update(float2 *u, float2 *v, float2 *a, const float2 *mi
 
 __global__ void k_advance(Control *ctrl) { ctrl->istep += 1; }
 
+// ---------------------------------------------------------------------------
+// Unified update: for every medium and shot, a = force * minv, v += dt/2 a
+// (corrector, newmark.tpp:44-47), seismogram taps on (u, v, a), then unless
+// this is the last step the next predictor u += dt v + dt^2/2 a,
+// v += dt/2 a, force = 0 (newmark.tpp:98-105).  The step counter is read at
+// entry by every CTA and advanced by the last CTA to finish.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void apply_taps(const ReceiverTaps &tp, int g, const float fv[3], float *seis_row) {
+  if (!((tp.mask[g >> 5] >> (g & 31)) & 1u)) return;
+  int lo = 0, hi = tp.nsup - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (tp.sup_g[mid] < g) lo = mid + 1; else hi = mid;
+  }
+  if (tp.sup_g[lo] != g) return;
+  for (int q = tp.sup_begin[lo]; q < tp.sup_begin[lo + 1]; ++q) {
+    const int wh = tp.which[q];
+    atomicAdd(seis_row + tp.slot[q], tp.w[q] * fv[wh]);
+  }
+}
+
+__global__ void k_update_all(UpdateParams P) {
+  const int istep = P.ctrl ? P.ctrl->istep : -1;
+  const bool record = P.seis != nullptr && istep >= 0 && (istep % P.nsbs) == 0 && (istep / P.nsbs) < P.max_sig;
+  const int isig = record ? istep / P.nsbs : 0;
+  const size_t total = P.begin[P.nm];
+  for (size_t j = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; j < total;
+       j += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    int mi = 0;
+    while (mi + 1 < P.nm && j >= P.begin[mi + 1]) ++mi;
+    const UpdateMedium &M = P.m[mi];
+    const size_t jj = j - P.begin[mi];
+    const float2 m = reinterpret_cast<const float2 *>(M.minv)[jj];
+    float2 *U = reinterpret_cast<float2 *>(M.u);
+    float2 *Vv = reinterpret_cast<float2 *>(M.v);
+    float2 *A = reinterpret_cast<float2 *>(M.a);
+    bool tapped = false;
+    if (record && M.taps.nsup > 0) {
+      const int g0 = (M.nc == 2) ? static_cast<int>(jj) : static_cast<int>(2 * jj);
+      tapped = ((M.taps.mask[g0 >> 5] >> (g0 & 31)) & 1u) != 0;
+      if (M.nc == 1) tapped = tapped || (((M.taps.mask[(g0 + 1) >> 5] >> ((g0 + 1) & 31)) & 1u) != 0);
+    }
+    for (int s = 0; s < P.nshots; ++s) {
+      const size_t i = s * M.ld2 + jj;
+      const float2 r = A[i];
+      float2 acc, vel = Vv[i];
+      acc.x = r.x * m.x;
+      acc.y = r.y * m.y;
+      vel.x += P.dt2 * acc.x;
+      vel.y += P.dt2 * acc.y;
+      float2 uu = U[i];
+      if (tapped) {
+        float *row = P.seis + (static_cast<size_t>(s) * P.max_sig + isig) * P.slots;
+        if (M.nc == 2) {
+          const float fv[6] = {uu.x, uu.y, vel.x, vel.y, acc.x, acc.y};
+          // which = field * 2 + component
+          apply_taps(M.taps, static_cast<int>(jj), fv, row);
+        } else {
+          const float f0[6] = {uu.x, 0.f, vel.x, 0.f, acc.x, 0.f};
+          const float f1[6] = {uu.y, 0.f, vel.y, 0.f, acc.y, 0.f};
+          apply_taps(M.taps, static_cast<int>(2 * jj), f0, row);
+          apply_taps(M.taps, static_cast<int>(2 * jj + 1), f1, row);
+        }
+      }
+      if (P.last) {
+        A[i] = acc;
+        Vv[i] = vel;
+      } else {
+        uu.x += P.dt * vel.x + P.dtsq2 * acc.x;
+        uu.y += P.dt * vel.y + P.dtsq2 * acc.y;
+        vel.x += P.dt2 * acc.x;
+        vel.y += P.dt2 * acc.y;
+        U[i] = uu;
+        Vv[i] = vel;
+        A[i] = make_float2(0.f, 0.f);
+      }
+    }
+  }
+  if (P.ctrl) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      const unsigned prev = atomicAdd(P.done, 1u);
+      if (prev == gridDim.x - 1) {
+        P.ctrl->istep = istep + 1;
+        *P.done = 0u;
+        __threadfence();
+      }
+    }
+  }
+}
+
+
 // Mass matrix (compute_mass_matrix.tpp:80-113) accumulated in FP64.
 template <int MED>
 __global__ void k_mass(Static st, MediumFields f, int N, float dt) {
@@ -507,9 +943,28 @@ size_t field_ld(const MediumFields &f) { return static_cast<size_t>(f.nglob + (f
 
 }  // namespace
 
+static int g_stiffness_variant = 0;
+void set_stiffness_variant(int v) { g_stiffness_variant = v; }
+
 void launch_stiffness(int medium, int ngll, const Static &st, const MediumFields &f, int nshots,
-                      const StaceyStore &ss, const int *istep_dev, cudaStream_t stream) {
+                      const StaceyStore &ss, const int *istep_dev, cudaStream_t stream, const TailWork *tw) {
   if (f.nelem == 0) return;
+  if (g_stiffness_variant == 0 && st.pack != nullptr) {
+    const TailWork none{};
+    const TailWork &w = tw ? *tw : none;
+    if (ngll == 5) {
+      if (medium == MED_PSV) launch_rp<MED_PSV, 5, 32, 3>(st, f, nshots, ss, istep_dev, w, stream);
+      else if (medium == MED_SH) launch_rp<MED_SH, 5, 32, 3>(st, f, nshots, ss, istep_dev, w, stream);
+      else launch_rp<MED_AC, 5, 32, 3>(st, f, nshots, ss, istep_dev, w, stream);
+      return;
+    }
+    if (ngll == 8) {
+      if (medium == MED_PSV) launch_rp<MED_PSV, 8, 16, 2>(st, f, nshots, ss, istep_dev, w, stream);
+      else if (medium == MED_SH) launch_rp<MED_SH, 8, 16, 2>(st, f, nshots, ss, istep_dev, w, stream);
+      else launch_rp<MED_AC, 8, 16, 2>(st, f, nshots, ss, istep_dev, w, stream);
+      return;
+    }
+  }
   if (ngll == 5) {
     constexpr int N = 5, EPB = 32;
     dim3 grid((f.nelem + EPB - 1) / EPB, 1);
@@ -590,6 +1045,25 @@ void launch_fused_update(const MediumFields &f, int nshots, float dt, float dt2,
                                                     ld2, nshots, dt, dt2, dtsq2, ctrl);
 }
 void launch_advance_step(Control *ctrl, cudaStream_t stream) { k_advance<<<1, 1, 0, stream>>>(ctrl); }
+
+void launch_update_all(const UpdateParams &p, cudaStream_t stream) {
+  const size_t total = p.begin[p.nm];
+  if (total == 0) {
+    if (p.ctrl) k_advance<<<1, 1, 0, stream>>>(p.ctrl);
+    return;
+  }
+  static int nsm = 0;
+  if (nsm == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  }
+  const size_t want = (total + 255) / 256;
+  const int grid = static_cast<int>(std::min<size_t>(want, static_cast<size_t>(nsm) * 8));
+  k_update_all<<<std::max(grid, 1), 256, 0, stream>>>(p);
+}
+
+bool stiffness_fuses_tail(const Static &st) { return g_stiffness_variant == 0 && st.pack != nullptr; }
 
 void launch_mass(int medium, int ngll, const Static &st, const MediumFields &f, float dt,
                  cudaStream_t stream) {

@@ -27,6 +27,10 @@ struct Static {
   const uint8_t *eflag;  // per device element: bit0 Stacey points, bit1 free-surface points
   const uint8_t *bnd;    // per local point
   const float *bnd_nx, *bnd_nz, *bnd_w;
+  // Packed per-element block for the TMA-fed stiffness kernel:
+  // pack[e][8][N*N] = iglob (int bits), xix, xiz, gammax, gammaz, jac, mat0, mat1.
+  const float *pack;
+  int *err;              // device error flag (bounded waits that expired)
 };
 
 struct MediumFields {
@@ -80,12 +84,64 @@ struct StaceyStore {
   int mode;          // 0 none, 1 store (forward), 2 replay (backward)
 };
 
+// Work folded into the tail of a stiffness launch: the medium's point sources
+// and the coupling points where this medium receives from the other one.
+struct TailWork {
+  SourceSet src;       // only entries whose medium matches are applied
+  CouplingSet cp;
+  MediumFields other;  // the coupled medium
+  int cp_mode;         // 0 none, 1 acoustic <- elastic displacement, 2 elastic <- acoustic acceleration
+  int other_divided;   // mode 2: the acoustic array already holds chi_ddot
+};
+
+// Seismograms as a sparse linear map of nodal values, applied inside the
+// update kernel: seis[s][isig][slot] += w * field_which(g).  `mask` has one
+// bit per point of the medium; `sup_g` lists the tapped points (sorted) and
+// [sup_begin[q], sup_begin[q+1]) their entries.
+struct ReceiverTaps {
+  int nsup;
+  const uint32_t *mask;
+  const int *sup_g, *sup_begin;
+  const int *slot;    // (type * nrec + rec) * 2 + out component
+  const int *which;   // field (0 u, 1 v, 2 a) * 2 + input component
+  const float *w;
+};
+
+struct UpdateMedium {
+  float *u, *v, *a;
+  const float *minv;
+  size_t ld2;    // float2 pairs per shot row
+  int nc;        // components per point (1: a pair holds two points)
+  ReceiverTaps taps;
+};
+
+struct UpdateParams {
+  UpdateMedium m[3];
+  int nm;
+  size_t begin[4];  // pair ranges of the media in the flat index space
+  int nshots;
+  float dt, dt2, dtsq2;
+  int last;               // 1: finish the step (no predictor for the next one)
+  Control *ctrl;          // step counter, advanced by the last CTA to finish
+  unsigned *done;         // CTA completion counter (zero between launches)
+  float *seis;            // [S][max_sig][slots]
+  int slots, max_sig, nsbs;
+};
+
 // ---- launchers (kernels.cu) ----
 void set_quadrature(int ngll, const float *hprime, const float *wgll);
 
+// With the TMA kernel (default) `tw` (may be null) is executed in the same
+// launch; the register-staged variant ignores it (callers then launch the
+// sources / coupling kernels separately).
 void launch_stiffness(int medium, int ngll, const Static &st, const MediumFields &f,
                       int nshots, const StaceyStore &ss, const int *istep_dev,
-                      cudaStream_t stream);
+                      cudaStream_t stream, const TailWork *tw = nullptr);
+bool stiffness_fuses_tail(const Static &st);
+// Variant selector for the stiffness kernel: 0 = TMA-fed persistent
+// (default), 1 = register-staged.
+void set_stiffness_variant(int v);
+constexpr int kPackFields = 8;
 void launch_sources(int ngll, const Static &st, const SourceSet &src,
                     MediumFields *fields, int nshots, int medium, const int *istep_dev,
                     int adjoint_only, cudaStream_t stream);
@@ -110,6 +166,9 @@ void launch_divide(const MediumFields &f, int nshots, cudaStream_t stream);
 void launch_fused_update(const MediumFields &f, int nshots, float dt, float dt2,
                          float dtsq2, int last, Control *ctrl, cudaStream_t stream);
 void launch_advance_step(Control *ctrl, cudaStream_t stream);
+// Fused divide + corrector (+ predictor of the next step) for every medium in
+// one launch, with the seismogram taps.
+void launch_update_all(const UpdateParams &p, cudaStream_t stream);
 void launch_mass(int medium, int ngll, const Static &st, const MediumFields &f, float dt,
                  cudaStream_t stream);
 void launch_invert_mass(const MediumFields &f, cudaStream_t stream);
