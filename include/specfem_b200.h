@@ -42,6 +42,10 @@
 #define SFB_E_NONFINITE -6   /* wavefield watchdog saw NaN/Inf                 */
 #define SFB_E_NOMEM -7       /* device allocation failed                       */
 
+#define SFB_MEDIUM_ELASTIC_PSV 0
+#define SFB_MEDIUM_ELASTIC_SH 1
+#define SFB_MEDIUM_ACOUSTIC 3
+
 #define SFB_WAVEFIELD_FORWARD 0
 #define SFB_WAVEFIELD_ADJOINT 1
 #define SFB_WAVEFIELD_BACKWARD 2
@@ -256,5 +260,36 @@ typedef struct sfb_problem_view {
 } sfb_problem_view;
 SFB_API int sfb_get_problem_view(const sfb_context *ctx,
                                  sfb_problem_view *view);
+
+/* ---- assembly without device allocation -------------------------------- */
+
+/* No counterpart in the reference.  Assembles the mass matrix of one medium
+ * in FP64 and writes its FP32 inverse, for callers that cannot allocate
+ * device memory where they need it: a host framework that hands out every
+ * device buffer from its own pool, code running inside a CUDA stream capture
+ * (cudaMalloc is not allowed there), or a real-time loop that must not touch
+ * the allocator.  The caller passes device inputs (per local point of the
+ * medium's `nelem` elements, point p = (e * ngll + iz) * ngll + ix: the
+ * medium-local point index, the Jacobian, the material -- P-SV: kappa, mu,
+ * rho; SH: mu, rho, unused; acoustic: rho_inverse, kappa, unused -- and
+ * optionally the Stacey tags / normals / weights, NULL for none), the host
+ * GLL weights, and the device output minv[npoints * ncomp] (components
+ * interleaved).  Work is enqueued on `stream` (a cudaStream_t, NULL for the
+ * default stream).
+ * The only scratch is a fixed FP64 device array of SFB_NOALLOC_MAX_DOFS
+ * entries (16 MiB) that every GPU loading the library holds until exit;
+ * npoints * ncomp above that limit is rejected with SFB_E_INVALID.  The
+ * first call on a device looks up the array's address, so make it before any
+ * stream capture.  All calls on a device share the array: each call clears
+ * what it uses, and calls that overlap on the GPU race.  Errors are reported
+ * through sfb_noalloc_last_error(). */
+#define SFB_NOALLOC_MAX_DOFS (1 << 21)
+SFB_API int sfb_assemble_inverse_mass_noalloc(
+    int medium, int ngll, int nelem, int npoints, const int *iglob,
+    const float *jacobian, const float *mat0, const float *mat1,
+    const float *mat2, const uint8_t *bnd, const float *bnd_nx,
+    const float *bnd_nz, const float *bnd_w, const double *wgll, double dt,
+    float *minv, void *stream);
+SFB_API const char *sfb_noalloc_last_error(void);
 
 #endif /* SPECFEM_B200_H */

@@ -137,6 +137,11 @@ SIGNATURES = {
     "sfb_set_source_time_function": (C.c_int, [_ctx, C.c_int, _P(C.c_float), C.c_size_t]),
     "sfb_get_stream": (C.c_int, [_ctx, _P(C.c_void_p)]),
     "sfb_time_stiffness": (C.c_int, [_ctx, C.c_int, C.c_int, _P(C.c_double)]),
+    "sfb_assemble_inverse_mass_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p,
+                                                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                    _P(C.c_double), C.c_double, C.c_void_p, C.c_void_p]),
+    "sfb_noalloc_last_error": (C.c_char_p, []),
 }
 
 _lib = None
