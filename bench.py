@@ -41,14 +41,17 @@ def env_int(name, default):
         return default
 
 
+SCALE = 1.0  # element-count scale of the workload (1 = the full configuration)
+
+
 def make_problem(workload: str, nstep: int):
     from specfempp_b200 import workloads as W
     if workload == "coupled":
-        return W.coupled(1.0, nstep=nstep, seismogram_types=("pressure",))
+        return W.coupled(SCALE, nstep=nstep, seismogram_types=("pressure",))
     if workload == "plain":
-        return W.plain_elastic(1.0, nstep=nstep)
+        return W.plain_elastic(SCALE, nstep=nstep)
     if workload == "batched":
-        return W.batched(1.0, nshots=64, nstep=nstep)
+        return W.batched(SCALE, nshots=64, nstep=nstep)
     raise SystemExit("unknown workload " + workload)
 
 
@@ -293,7 +296,8 @@ def run_ours(args):
         "steps": K, "warmup": Wm, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded model with the workload's shapes and distributions)",
-        "config": dict(workload_config(args.workload, info, p), parallelism="replicas" if world > 1 else "single",
+        "config": dict(workload_config(args.workload, info, p), scale=SCALE,
+                       parallelism="replicas" if world > 1 else "single",
                        l2_policy="working set %.0f MB > 126 MB L2; no flush" % (info.device_bytes / 1e6)),
         "roofline": {"bound": "hbm", "kernel": "stiffness (medium %d)" % dominant, "achieved": achieved,
                      "peak": peak, "peak_kind": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
@@ -325,7 +329,11 @@ def main():
     ap.add_argument("--workload", default="coupled", choices=["coupled", "plain", "batched"])
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--scale", type=float, default=1.0,
+                    help="shrink the workload's element counts (profiling captures); 1 = full size")
     args = ap.parse_args()
+    global SCALE
+    SCALE = args.scale
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

@@ -255,7 +255,6 @@ void ensure_device(sfb_context *c) {
   size_t *tot = &c->device_bytes;
   c->pack.upload(pack, tot);
   c->dflag.alloc(1, tot);
-  if (const char *v = std::getenv("SFB_STIFFNESS")) dev::set_stiffness_variant(std::string(v) == "registers" ? 1 : 0);
   c->iglob.upload(iglob, tot);
   c->xix.upload(xix, tot);
   c->xiz.upload(xiz, tot);
@@ -545,7 +544,7 @@ dev::UpdateParams update_params(sfb_context *c, WavefieldSet &W, int last, bool 
     M.v = f.v;
     M.a = f.a;
     M.minv = f.minv;
-    M.ld2 = static_cast<size_t>(f.nglob + (f.nglob & 1)) * f.nc / 2;
+    M.ld2 = static_cast<size_t>(f.nglob + (f.nglob & 1)) * f.nc * P.nshots / 2;
     M.nc = f.nc;
     if (taps && c->taps[m].nsup > 0) {
       const auto &T = c->taps[m];
@@ -555,6 +554,8 @@ dev::UpdateParams update_params(sfb_context *c, WavefieldSet &W, int last, bool 
     ++u.nm;
   }
   u.nshots = P.nshots;
+  u.sdiv = dev::FastDiv::make(static_cast<uint32_t>(P.nshots));
+  if (u.begin[u.nm] * 2 >= (1ull << 32)) throw std::invalid_argument("field too large for 32-bit update indexing");
   u.dt = static_cast<float>(P.dt);
   u.dt2 = static_cast<float>(P.dt / 2.0);
   u.dtsq2 = static_cast<float>(P.dt * P.dt / 2.0);
@@ -585,69 +586,40 @@ void enqueue_fused_step(sfb_context *c, WavefieldSet &W, int last) {
     ss.mode = 1;
   }
   dev::SourceSet src = source_set(c);
-  if (dev::stiffness_fuses_tail(c->st)) {
-    // acoustic first (time_marching.tpp:48-52): stiffness + sources + coupling
-    // from the predicted elastic displacement, in one launch
-    dev::TailWork ta{};
-    ta.src = src;
-    ta.cp = coupling_acoustic(c);
-    ta.other = W.f[dev::MED_PSV];
-    ta.cp_mode = ta.cp.n > 0 ? 1 : 0;
-    dev::launch_stiffness(dev::MED_AC, n, c->st, W.f[dev::MED_AC], S, ss, istep, c->stream, &ta);
-    // elastic: coupling reads the final acoustic acceleration = force * minv
-    dev::TailWork te{};
-    te.src = src;
-    te.cp = coupling_elastic(c);
-    te.other = W.f[dev::MED_AC];
-    te.cp_mode = te.cp.n > 0 ? 2 : 0;
-    te.other_divided = 0;
-    dev::launch_stiffness(dev::MED_PSV, n, c->st, W.f[dev::MED_PSV], S, ss, istep, c->stream, &te);
-    dev::TailWork tsh{};
-    tsh.src = src;
-    dev::launch_stiffness(dev::MED_SH, n, c->st, W.f[dev::MED_SH], S, ss, istep, c->stream, &tsh);
-    build_taps(c);
-    dev::launch_update_all(update_params(c, W, last, true, true), c->stream);
-    return;
-  }
-  dev::launch_coupling_acoustic(coupling_acoustic(c), W.f[dev::MED_AC], W.f[dev::MED_PSV], S, c->stream);
-  dev::launch_sources(n, c->st, src, W.f, S, dev::MED_AC, istep, 0, c->stream);
-  dev::launch_stiffness(dev::MED_AC, n, c->st, W.f[dev::MED_AC], S, ss, istep, c->stream);
-  dev::launch_coupling_elastic(coupling_elastic(c), W.f[dev::MED_PSV], W.f[dev::MED_AC], S, 0, c->stream);
-  for (int m : {dev::MED_PSV, dev::MED_SH}) {
-    dev::launch_sources(n, c->st, src, W.f, S, m, istep, 0, c->stream);
-    dev::launch_stiffness(m, n, c->st, W.f[m], S, ss, istep, c->stream);
-  }
-  dev::launch_receivers(n, c->st, receiver_set(c, W), W.f, S, dt2, 1, istep, c->stream);
-  int lastm = -1;
-  for (int m : kMedia)
-    if (W.f[m].nglob > 0) lastm = m;
-  for (int m : kMedia) {
-    if (W.f[m].nglob == 0) continue;
-    dev::launch_fused_update(W.f[m], S, dt, dt2, dtsq2, last, m == lastm ? W.ctrl.p : nullptr, c->stream);
-  }
+  // acoustic first (time_marching.tpp:48-52): stiffness + sources + coupling
+  // from the predicted elastic displacement, in one launch
+  dev::TailWork ta{};
+  ta.src = src;
+  ta.cp = coupling_acoustic(c);
+  ta.other = W.f[dev::MED_PSV];
+  ta.cp_mode = ta.cp.n > 0 ? 1 : 0;
+  dev::launch_stiffness(dev::MED_AC, n, c->st, W.f[dev::MED_AC], S, ss, istep, c->stream, &ta);
+  // elastic: coupling reads the final acoustic acceleration = force * minv
+  dev::TailWork te{};
+  te.src = src;
+  te.cp = coupling_elastic(c);
+  te.other = W.f[dev::MED_AC];
+  te.cp_mode = te.cp.n > 0 ? 2 : 0;
+  te.other_divided = 0;
+  dev::launch_stiffness(dev::MED_PSV, n, c->st, W.f[dev::MED_PSV], S, ss, istep, c->stream, &te);
+  dev::TailWork tsh{};
+  tsh.src = src;
+  dev::launch_stiffness(dev::MED_SH, n, c->st, W.f[dev::MED_SH], S, ss, istep, c->stream, &tsh);
+  build_taps(c);
+  dev::launch_update_all(update_params(c, W, last, true, true), c->stream);
+  (void)dt;
+  (void)dt2;
+  (void)dtsq2;
 }
 
 // Number of kernels one fused step launches (mirrors the skip conditions of
 // the launchers in kernels.cu).
 int fused_step_launches(sfb_context *c, WavefieldSet &W) {
-  const Problem &P = c->P;
   int n = 0;
-  if (dev::stiffness_fuses_tail(c->st)) {
-    for (int m : {dev::MED_AC, dev::MED_PSV, dev::MED_SH})
-      if (W.f[m].nelem > 0) ++n;
-    return n + 1;  // one update launch
-  }
-  if (!P.v_cp_ac_self.empty()) ++n;
-  if (!P.v_cp_el_self.empty()) ++n;
-  for (int m : {dev::MED_AC, dev::MED_PSV, dev::MED_SH}) {
-    if (W.f[m].nelem == 0) continue;
-    ++n;                       // stiffness
-    if (c->nsrc > 0) ++n;      // sources
-  }
-  if (!P.receivers.empty() && !P.seismogram_types.empty()) ++n;
-  for (int m : kMedia)
-    if (W.f[m].nglob > 0) ++n;  // update
-  return n;
+  for (int m : {dev::MED_AC, dev::MED_PSV, dev::MED_SH})
+    if (W.f[m].nelem > 0) ++n;  // stiffness (+ sources + coupling)
+  (void)c;
+  return n + 1;                 // one update launch for all media
 }
 
 void predictor_all(sfb_context *c, WavefieldSet &W, double sgn) {
@@ -663,7 +635,7 @@ void run_forward_fused(sfb_context *c, int nstep, int use_graph) {
   if (nstep <= 0) return;
   if (W.step + nstep > c->P.nstep)
     throw std::invalid_argument("run would pass the configured number of steps");
-  if (dev::stiffness_fuses_tail(c->st)) build_taps(c);
+  build_taps(c);
   set_step(c, W, W.step);
   predictor_all(c, W, 1.0);
   for (int m : kMedia)
@@ -938,15 +910,19 @@ SFB_API int sfb_get_field(const sfb_context *cctx, int wavefield, int medium, in
     WavefieldSet &W = ensure_wavefield(ctx, wavefield);
     const dev::MediumFields &f = W.f[medium];
     const size_t n = static_cast<size_t>(f.nglob) * f.nc;
-    const size_t ld = static_cast<size_t>(f.nglob + (f.nglob & 1)) * f.nc;
     if (count < n) throw std::invalid_argument("field buffer too small");
     if (shot < 0 || shot >= ctx->P.nshots) throw std::invalid_argument("shot out of range");
     const float *src = which == 0 ? f.u : which == 1 ? f.v : which == 2 ? f.a : f.minv;
+    const int S = (which == 3) ? 1 : ctx->P.nshots;
     if (which == 3) shot = 0;
     std::vector<float> tmp(n);
     ck(cudaStreamSynchronize(ctx->stream), "sync");
-    if (n) ck(cudaMemcpy(tmp.data(), src + shot * ld, n * sizeof(float), cudaMemcpyDeviceToHost), "field d2h");
-    // device layout interleaves components; the ABI layout is [ncomp][nglob]
+    // device layout [g][s][c]: gather shot `shot`, then transpose to [c][g]
+    if (n)
+      ck(cudaMemcpy2D(tmp.data(), f.nc * sizeof(float), src + static_cast<size_t>(shot) * f.nc,
+                      static_cast<size_t>(S) * f.nc * sizeof(float), f.nc * sizeof(float), f.nglob,
+                      cudaMemcpyDeviceToHost),
+         "field d2h");
     for (int c = 0; c < f.nc; ++c)
       for (int g = 0; g < f.nglob; ++g) host[static_cast<size_t>(c) * f.nglob + g] = tmp[static_cast<size_t>(g) * f.nc + c];
     return SFB_OK;
@@ -961,15 +937,18 @@ SFB_API int sfb_set_field(sfb_context *ctx, int wavefield, int medium, int which
     WavefieldSet &W = ensure_wavefield(ctx, wavefield);
     const dev::MediumFields &f = W.f[medium];
     const size_t n = static_cast<size_t>(f.nglob) * f.nc;
-    const size_t ld = static_cast<size_t>(f.nglob + (f.nglob & 1)) * f.nc;
     if (count < n) throw std::invalid_argument("field buffer too small");
     if (shot < 0 || shot >= ctx->P.nshots) throw std::invalid_argument("shot out of range");
     std::vector<float> tmp(n);
     for (int c = 0; c < f.nc; ++c)
       for (int g = 0; g < f.nglob; ++g) tmp[static_cast<size_t>(g) * f.nc + c] = host[static_cast<size_t>(c) * f.nglob + g];
     float *dst = which == 0 ? f.u : which == 1 ? f.v : f.a;
+    const int S = ctx->P.nshots;
     ck(cudaStreamSynchronize(ctx->stream), "sync");
-    if (n) ck(cudaMemcpy(dst + shot * ld, tmp.data(), n * sizeof(float), cudaMemcpyHostToDevice), "field h2d");
+    if (n)
+      ck(cudaMemcpy2D(dst + static_cast<size_t>(shot) * f.nc, static_cast<size_t>(S) * f.nc * sizeof(float),
+                      tmp.data(), f.nc * sizeof(float), f.nc * sizeof(float), f.nglob, cudaMemcpyHostToDevice),
+         "field h2d");
     return SFB_OK;
   });
 }

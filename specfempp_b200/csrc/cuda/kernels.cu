@@ -84,170 +84,9 @@ __device__ __forceinline__ void stacey(float m0, float m1, float m2, float nx, f
 }
 
 // ---------------------------------------------------------------------------
-// Stiffness: one block = EPB elements x N threads; thread (el, iz) owns row
-// iz of element el.  The row's geometry, material and global indices are
-// loaded once into registers and reused for every shot; displacement and the
-// gamma-part of the stress integrand go through shared memory for the column
-// contractions; the xi-contractions stay in registers.
-// ---------------------------------------------------------------------------
-template <int MED, int N, int EPB>
-__global__ void __launch_bounds__(N * EPB)
-k_stiffness(Static st, MediumFields f, int nshots, StaceyStore ss, const int *istep_dev) {
-  constexpr int NC = (MED == MED_PSV) ? 2 : 1;
-  using V = typename Vec<NC>::T;
-  __shared__ V s_u[EPB][N * N];
-  __shared__ V s_fg[EPB][N * N];
-
-  const int el = threadIdx.x / N, iz = threadIdx.x % N;
-  const int li = blockIdx.x * EPB + el;
-  const bool valid = li < f.nelem;
-  const int e = f.elem_begin + (valid ? li : 0);
-  const size_t p0 = (static_cast<size_t>(e) * N + iz) * N;
-
-  int g[N];
-  float xix[N], xiz[N], gax[N], gaz[N], jac[N], m0[N], m1[N];
-#pragma unroll
-  for (int ix = 0; ix < N; ++ix) {
-    g[ix] = __ldg(st.iglob + p0 + ix);
-    xix[ix] = __ldg(st.xix + p0 + ix);
-    xiz[ix] = __ldg(st.xiz + p0 + ix);
-    gax[ix] = __ldg(st.gax + p0 + ix);
-    gaz[ix] = __ldg(st.gaz + p0 + ix);
-    jac[ix] = __ldg(st.jac + p0 + ix);
-    m0[ix] = __ldg(st.mat0 + p0 + ix);
-    m1[ix] = __ldg(st.mat1 + p0 + ix);
-  }
-  float hpz[N], hpwz[N];
-#pragma unroll
-  for (int l = 0; l < N; ++l) {
-    hpz[l] = c_hp[iz * N + l];
-    hpwz[l] = c_hpw[iz * N + l];
-  }
-  const uint8_t eflag = valid ? st.eflag[e] : 0;
-  const int slot = (ss.mode != 0 && valid) ? ss.slot[e] : -1;
-  const int istep = (ss.mode != 0) ? *istep_dev : 0;
-
-  for (int s = blockIdx.y; s < nshots; s += gridDim.y) {
-    const V *U = reinterpret_cast<const V *>(f.u) + static_cast<size_t>(s) * (f.nglob + (f.nglob & 1));
-    V *A = reinterpret_cast<V *>(f.a) + static_cast<size_t>(s) * (f.nglob + (f.nglob & 1));
-    V ur[N];
-#pragma unroll
-    for (int ix = 0; ix < N; ++ix) {
-      ur[ix] = valid ? U[g[ix]] : Vec<NC>::zero();
-      s_u[el][iz * N + ix] = ur[ix];
-    }
-    __syncthreads();
-    V fx[N];
-#pragma unroll
-    for (int ix = 0; ix < N; ++ix) {
-      float dxi[NC], dga[NC];
-#pragma unroll
-      for (int c = 0; c < NC; ++c) { dxi[c] = 0.f; dga[c] = 0.f; }
-#pragma unroll
-      for (int l = 0; l < N; ++l) {
-        const V col = s_u[el][l * N + ix];
-#pragma unroll
-        for (int c = 0; c < NC; ++c) {
-          dxi[c] += c_hp[ix * N + l] * comp(ur[l], c);
-          dga[c] += hpz[l] * comp(col, c);
-        }
-      }
-      float du[NC][2];
-#pragma unroll
-      for (int c = 0; c < NC; ++c) {
-        du[c][0] = xix[ix] * dxi[c] + gax[ix] * dga[c];
-        du[c][1] = xiz[ix] * dxi[c] + gaz[ix] * dga[c];
-      }
-      float T[NC][2];
-      if constexpr (MED == MED_PSV) {
-        const float kappa = m0[ix], mu = m1[ix];
-        const float l2m = kappa + static_cast<float>(4.0 / 3.0) * mu;
-        const float lam = l2m - 2.0f * mu;
-        T[0][0] = l2m * du[0][0] + lam * du[1][1];  // sigma_xx
-        T[1][1] = l2m * du[1][1] + lam * du[0][0];  // sigma_zz
-        T[0][1] = mu * (du[0][1] + du[1][0]);       // sigma_xz
-        T[1][0] = T[0][1];
-      } else {
-        const float k = m0[ix];  // SH: mu; acoustic: rho_inverse
-        T[0][0] = k * du[0][0];
-        T[0][1] = k * du[0][1];
-      }
-      V f0, f1;
-#pragma unroll
-      for (int c = 0; c < NC; ++c) {
-        set_comp(f0, c, jac[ix] * (T[c][0] * xix[ix] + T[c][1] * xiz[ix]));
-        set_comp(f1, c, jac[ix] * (T[c][0] * gax[ix] + T[c][1] * gaz[ix]));
-      }
-      fx[ix] = f0;
-      s_fg[el][iz * N + ix] = f1;
-    }
-    __syncthreads();
-    if (valid) {
-#pragma unroll
-      for (int ix = 0; ix < N; ++ix) {
-        float t1[NC], t2[NC];
-#pragma unroll
-        for (int c = 0; c < NC; ++c) { t1[c] = 0.f; t2[c] = 0.f; }
-#pragma unroll
-        for (int l = 0; l < N; ++l) {
-          const V col = s_fg[el][l * N + ix];
-#pragma unroll
-          for (int c = 0; c < NC; ++c) {
-            t1[c] += comp(fx[l], c) * c_hpw[ix * N + l];
-            t2[c] += comp(col, c) * hpwz[l];
-          }
-        }
-        float acc[2];
-#pragma unroll
-        for (int c = 0; c < NC; ++c) acc[c] = (c_w[iz] * t1[c] + c_w[ix] * t2[c]) * -1.0f;
-        if (eflag) {
-          const size_t p = p0 + ix;
-          const uint8_t b = st.bnd[p];
-          if (b & 1) {
-            const V *Vv = reinterpret_cast<const V *>(f.v) + static_cast<size_t>(s) * (f.nglob + (f.nglob & 1));
-            const V vv = Vv[g[ix]];
-            float vel[2];
-#pragma unroll
-            for (int c = 0; c < NC; ++c) vel[c] = comp(vv, c);
-            stacey<MED>(m0[ix], m1[ix], st.mat2 ? st.mat2[p] : 0.f, st.bnd_nx[p], st.bnd_nz[p],
-                        st.bnd_w[p], vel, acc);
-          }
-          if (b & 2) {
-#pragma unroll
-            for (int c = 0; c < NC; ++c) acc[c] = 0.f;
-          }
-        }
-        if (slot >= 0) {
-          const size_t base =
-              ((((static_cast<size_t>(s) * ss.nstep + istep) * ss.nstacey + slot) * N + iz) * N + ix) * NC;
-          if (ss.mode == 1) {
-#pragma unroll
-            for (int c = 0; c < NC; ++c) ss.data[base + c] = acc[c];
-          } else {
-#pragma unroll
-            for (int c = 0; c < NC; ++c) acc[c] = ss.data[base + c];
-          }
-        }
-        V out;
-#pragma unroll
-        for (int c = 0; c < NC; ++c) set_comp(out, c, acc[c]);
-        red_add(A + g[ix], out);
-      }
-    }
-    __syncthreads();
-  }
-}
-
-
-// ---------------------------------------------------------------------------
-// TMA-fed persistent stiffness.  Each CTA walks chunks of EPB elements; the
-// chunk's packed static block (iglob, geometry, material: 8 x N*N words per
-// element, contiguous in HBM) arrives in shared memory by one bulk async copy
-// (cp.async.bulk, no multicast) completing on an mbarrier, double-buffered so
-// the next chunk streams in while this one is computed.  Thread (el, iz) owns
-// row iz of element el exactly as in k_stiffness.  Every mbarrier wait is
-// bounded; on expiry the kernel records SFB_DEVICE_WAIT_TIMEOUT in st.err and
-// the CTA returns.
+// Bulk async copy (cp.async.bulk, no multicast) and mbarrier helpers.  Every
+// mbarrier wait is bounded; on expiry the kernel records kWaitTimeout in
+// st.err and the CTA returns.
 // ---------------------------------------------------------------------------
 constexpr int kWaitTimeout = 1;
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
@@ -283,6 +122,54 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity
     if (clock64() - t0 > (1LL << 32)) return false;
   }
   return true;
+}
+
+// Point sources and fluid-solid coupling of one medium, spread over all CTAs
+// of a stiffness launch (`cta`, `ncta`); they only add into the force array.
+// Fields are point-major, shot-minor: value (g, s) at g * S + s.
+template <int MED, int N>
+__device__ __forceinline__ void tail_work(const Static &st, const MediumFields &f, int S, int istep,
+                                          const TailWork &tw, int cta, int ncta) {
+  constexpr int NC = (MED == MED_PSV) ? 2 : 1;
+  constexpr int NN = N * N;
+  const int gtid = cta * blockDim.x + threadIdx.x;
+  const int gstride = ncta * blockDim.x;
+  if (tw.src.n > 0 && istep >= 0 && istep < tw.src.nstep) {
+    for (int idx = gtid; idx < tw.src.n * NN; idx += gstride) {
+      const int i = idx / NN, kk = idx % NN;
+      if (tw.src.medium[i] != MED) continue;
+      const size_t p = static_cast<size_t>(tw.src.elem[i]) * NN + kk;
+      const int gi = st.iglob[p];
+      float *A = f.a + (static_cast<size_t>(gi) * S + tw.src.shot[i]) * NC;
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        const float stf = tw.src.stf[(static_cast<size_t>(i) * tw.src.nstep + istep) * 2 + c];
+        const float arr = tw.src.array[(static_cast<size_t>(i) * 2 + c) * NN + kk];
+        float val = stf * arr;
+        if (MED == MED_AC) val = stf * arr / st.mat1[p];
+        atomicAdd(A + c, val);
+      }
+    }
+  }
+  if (tw.cp_mode != 0) {
+    const int n = tw.cp.n;
+    const MediumFields &o = tw.other;
+    for (int idx = gtid; idx < n * S; idx += gstride) {
+      const int i = idx / S, s = idx % S;
+      if (tw.cp_mode == 1) {  // acoustic self += w (n . u_elastic)
+        const float2 u = reinterpret_cast<const float2 *>(o.u)[static_cast<size_t>(tw.cp.other[i]) * S + s];
+        atomicAdd(f.a + static_cast<size_t>(tw.cp.self[i]) * S + s,
+                  tw.cp.factor[i] * (tw.cp.nx[i] * u.x + tw.cp.nz[i] * u.y));
+      } else {  // elastic self += w n chi_ddot
+        const int oi = tw.cp.other[i];
+        const float r = o.a[static_cast<size_t>(oi) * S + s];
+        const float chi_dd = tw.other_divided ? r : r * o.minv[oi];
+        float *A = f.a + (static_cast<size_t>(tw.cp.self[i]) * S + s) * 2;
+        atomicAdd(A, tw.cp.factor[i] * tw.cp.nx[i] * chi_dd);
+        atomicAdd(A + 1, tw.cp.factor[i] * tw.cp.nz[i] * chi_dd);
+      }
+    }
+  }
 }
 
 // Row-per-thread stiffness fed by bulk async copies, software-pipelined.
@@ -338,7 +225,6 @@ k_stiffness_rp(Static st, MediumFields f, int nshots, StaceyStore ss, const int 
   }
   const float wz = c_w[iz];
   const int istep = (ss.mode != 0 || tw.src.n > 0) ? *istep_dev : 0;
-  const size_t ldv = static_cast<size_t>(f.nglob + (f.nglob & 1));
   const V *vbase = reinterpret_cast<const V *>(f.u);
   V *abase = reinterpret_cast<V *>(f.a);
   bool ok = true;
@@ -354,7 +240,7 @@ k_stiffness_rp(Static st, MediumFields f, int nshots, StaceyStore ss, const int 
 #pragma unroll
     for (int ix = 0; ix < N; ++ix) {
       g[ix] = (ok && li < f.nelem) ? __float_as_int(blk[iz * N + ix]) : 0;
-      ur[ix] = (ok && li < f.nelem) ? vbase[g[ix]] : Vec<NC>::zero();
+      ur[ix] = (ok && li < f.nelem) ? vbase[static_cast<size_t>(g[ix]) * nshots] : Vec<NC>::zero();
     }
   }
 
@@ -372,7 +258,7 @@ k_stiffness_rp(Static st, MediumFields f, int nshots, StaceyStore ss, const int 
     for (int s = 0; s < nshots; ++s) {
       if (s > 0) {
 #pragma unroll
-        for (int ix = 0; ix < N; ++ix) ur[ix] = valid ? vbase[s * ldv + g[ix]] : Vec<NC>::zero();
+        for (int ix = 0; ix < N; ++ix) ur[ix] = valid ? vbase[static_cast<size_t>(g[ix]) * nshots + s] : Vec<NC>::zero();
       }
 #pragma unroll
       for (int ix = 0; ix < N; ++ix) s_u[el * NN + iz * N + ix] = ur[ix];
@@ -448,7 +334,7 @@ k_stiffness_rp(Static st, MediumFields f, int nshots, StaceyStore ss, const int 
           const size_t p = (static_cast<size_t>(e) * N + iz) * N + ix;
           const uint8_t b = st.bnd[p];
           if (b & 1) {
-            const V vv = reinterpret_cast<const V *>(f.v)[s * ldv + g[ix]];
+            const V vv = reinterpret_cast<const V *>(f.v)[static_cast<size_t>(g[ix]) * nshots + s];
             float vel[2];
 #pragma unroll
             for (int c = 0; c < NC; ++c) vel[c] = comp(vv, c);
@@ -495,7 +381,7 @@ k_stiffness_rp(Static st, MediumFields f, int nshots, StaceyStore ss, const int 
           V out;
 #pragma unroll
           for (int c = 0; c < NC; ++c) set_comp(out, c, accr[ix][c]);
-          red_add(abase + s * ldv + g[ix], out);
+          red_add(abase + static_cast<size_t>(g[ix]) * nshots + s, out);
         }
       }
       if (last_shot && next < nchunks && ok) {
@@ -503,7 +389,7 @@ k_stiffness_rp(Static st, MediumFields f, int nshots, StaceyStore ss, const int 
 #pragma unroll
         for (int ix = 0; ix < N; ++ix) {
           g[ix] = gnext[ix];
-          ur[ix] = nvalid ? vbase[g[ix]] : Vec<NC>::zero();
+          ur[ix] = nvalid ? vbase[static_cast<size_t>(g[ix]) * nshots] : Vec<NC>::zero();
         }
       }
       __syncthreads();
@@ -514,45 +400,7 @@ k_stiffness_rp(Static st, MediumFields f, int nshots, StaceyStore ss, const int 
     return;
   }
 
-  // ---- tail: point sources and fluid-solid coupling of this medium --------
-  const int gtid = blockIdx.x * blockDim.x + t;
-  const int gstride = gridDim.x * blockDim.x;
-  if (tw.src.n > 0 && istep >= 0 && istep < tw.src.nstep) {
-    for (int idx = gtid; idx < tw.src.n * NN; idx += gstride) {
-      const int i = idx / NN, kk = idx % NN;
-      if (tw.src.medium[i] != MED) continue;
-      const size_t p = static_cast<size_t>(tw.src.elem[i]) * NN + kk;
-      const int gi = st.iglob[p];
-      float *A = f.a + static_cast<size_t>(tw.src.shot[i]) * ldv * NC;
-#pragma unroll
-      for (int c = 0; c < NC; ++c) {
-        const float stf = tw.src.stf[(static_cast<size_t>(i) * tw.src.nstep + istep) * 2 + c];
-        const float arr = tw.src.array[(static_cast<size_t>(i) * 2 + c) * NN + kk];
-        float val = stf * arr;
-        if (MED == MED_AC) val = stf * arr / st.mat1[p];
-        atomicAdd(A + static_cast<size_t>(gi) * NC + c, val);
-      }
-    }
-  }
-  if (tw.cp_mode != 0) {
-    const int n = tw.cp.n;
-    for (int idx = gtid; idx < n * nshots; idx += gstride) {
-      const int i = idx % n, s = idx / n;
-      const MediumFields &o = tw.other;
-      const size_t ldo = static_cast<size_t>(o.nglob + (o.nglob & 1));
-      if (tw.cp_mode == 1) {  // acoustic self += w (n . u_elastic)
-        const float2 u = reinterpret_cast<const float2 *>(o.u)[s * ldo + tw.cp.other[i]];
-        atomicAdd(f.a + s * ldv + tw.cp.self[i], tw.cp.factor[i] * (tw.cp.nx[i] * u.x + tw.cp.nz[i] * u.y));
-      } else {  // elastic self += w n chi_ddot
-        const int oi = tw.cp.other[i];
-        const float r = o.a[s * ldo + oi];
-        const float chi_dd = tw.other_divided ? r : r * o.minv[oi];
-        float *A = f.a + (s * ldv + tw.cp.self[i]) * 2;
-        atomicAdd(A, tw.cp.factor[i] * tw.cp.nx[i] * chi_dd);
-        atomicAdd(A + 1, tw.cp.factor[i] * tw.cp.nz[i] * chi_dd);
-      }
-    }
-  }
+  tail_work<MED, N>(st, f, nshots, istep, tw, blockIdx.x, gridDim.x);
 }
 
 template <int MED, int N, int EPB>
@@ -580,11 +428,203 @@ void launch_rp(const Static &st, const MediumFields &f, int nshots, const Stacey
   k_stiffness_rp<MED, N, EPB, MINB><<<grid, N * EPB, smem, stream>>>(st, f, nshots, ss, istep_dev, tw);
 }
 
+// Shot-parallel stiffness for S > 1 independent wavefields (batched shots).
+// One CTA per element and group of 32 * SPL shots; warp iz owns row iz of the
+// element, lane l owns shots s0 = (group * 32 + l) * SPL .. s0 + SPL - 1.  In
+// the point-major, shot-minor layout the SPL shots of a lane are adjacent, so
+// each gather of u(g, s0..) and each reduction into f(g, s0..) is one 8- or
+// 16-byte access and a warp moves 32 * SPL * NC * 4 contiguous bytes.  The
+// element's packed static block (iglob, geometry, material) is staged once
+// in shared memory and read by warp-uniform broadcasts.  Row contractions
+// stay in registers, column contractions read shared memory.
+template <int NV> struct VecN;
+template <> struct VecN<1> { using T = float; };
+template <> struct VecN<2> { using T = float2; };
+template <> struct VecN<4> { using T = float4; };
+__device__ __forceinline__ float vget(const float &v, int) { return v; }
+__device__ __forceinline__ float vget(const float2 &v, int i) { return i == 0 ? v.x : v.y; }
+__device__ __forceinline__ float vget(const float4 &v, int i) {
+  return i == 0 ? v.x : i == 1 ? v.y : i == 2 ? v.z : v.w;
+}
+__device__ __forceinline__ void vset(float &v, int, float x) { v = x; }
+__device__ __forceinline__ void vset(float2 &v, int i, float x) { if (i == 0) v.x = x; else v.y = x; }
+__device__ __forceinline__ void vset(float4 &v, int i, float x) {
+  if (i == 0) v.x = x; else if (i == 1) v.y = x; else if (i == 2) v.z = x; else v.w = x;
+}
+__device__ __forceinline__ void vred(float *p, float v) { atomicAdd(p, v); }
+__device__ __forceinline__ void vred(float2 *p, float2 v) { atomicAdd(p, v); }
+__device__ __forceinline__ void vred(float4 *p, float4 v) { atomicAdd(p, v); }
+
+template <int MED, int N, int SPL, int MINB>
+__global__ void __launch_bounds__(N * 32, MINB)
+k_stiffness_shots(Static st, MediumFields f, int S, StaceyStore ss, const int *istep_dev, TailWork tw) {
+  constexpr int NC = (MED == MED_PSV) ? 2 : 1;
+  constexpr int NN = N * N;
+  constexpr int NV = NC * SPL;
+  using W = typename VecN<NV>::T;
+  __shared__ W s_u[NN * 32];
+  __shared__ W s_fg[NN * 32];
+  __shared__ float s_st[kPackFields * NN];
+  const int lane = threadIdx.x & 31, iz = threadIdx.x >> 5;
+  const int e = f.elem_begin + blockIdx.x;
+  const int s0 = (blockIdx.y * 32 + lane) * SPL;
+  const bool act = s0 < S;
+  const int istep = (ss.mode != 0 || tw.src.n > 0) ? *istep_dev : 0;
+  for (int i = threadIdx.x; i < kPackFields * NN; i += blockDim.x)
+    s_st[i] = st.pack[static_cast<size_t>(e) * kPackFields * NN + i];
+  __syncthreads();
+  int g[N];
+#pragma unroll
+  for (int ix = 0; ix < N; ++ix) g[ix] = __float_as_int(s_st[iz * N + ix]);
+  float hpz[N], hpwz[N];
+#pragma unroll
+  for (int l = 0; l < N; ++l) {
+    hpz[l] = c_hp[iz * N + l];
+    hpwz[l] = c_hpw[iz * N + l];
+  }
+  const float wz = c_w[iz];
+  // u(g, s) for s = s0 .. s0+SPL-1, components interleaved: (g*S + s0)*NC floats
+  const W *U = reinterpret_cast<const W *>(f.u);
+  W *A = reinterpret_cast<W *>(f.a);
+  const size_t Sv = static_cast<size_t>(S) / SPL;  // vectors per point
+  const size_t lofs = static_cast<size_t>(s0) / SPL;
+  W ur[N];
+#pragma unroll
+  for (int ix = 0; ix < N; ++ix) {
+    if (act) ur[ix] = U[g[ix] * Sv + lofs];
+    else { for (int q = 0; q < NV; ++q) vset(ur[ix], q, 0.f); }
+    s_u[(iz * N + ix) * 32 + lane] = ur[ix];
+  }
+  __syncthreads();
+  W fx[N];
+#pragma unroll
+  for (int ix = 0; ix < N; ++ix) {
+    const int k = iz * N + ix;
+    const float xix = s_st[1 * NN + k], xiz = s_st[2 * NN + k];
+    const float gax = s_st[3 * NN + k], gaz = s_st[4 * NN + k];
+    const float jac = s_st[5 * NN + k], m0 = s_st[6 * NN + k], m1 = s_st[7 * NN + k];
+    float dxi[NV], dga[NV];
+#pragma unroll
+    for (int q = 0; q < NV; ++q) { dxi[q] = 0.f; dga[q] = 0.f; }
+#pragma unroll
+    for (int l = 0; l < N; ++l) {
+      const W col = s_u[(l * N + ix) * 32 + lane];
+#pragma unroll
+      for (int q = 0; q < NV; ++q) {
+        dxi[q] += c_hp[ix * N + l] * vget(ur[l], q);
+        dga[q] += hpz[l] * vget(col, q);
+      }
+    }
+    W f0, f1;
+#pragma unroll
+    for (int j = 0; j < SPL; ++j) {
+      float du[NC][2];
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        du[c][0] = xix * dxi[j * NC + c] + gax * dga[j * NC + c];
+        du[c][1] = xiz * dxi[j * NC + c] + gaz * dga[j * NC + c];
+      }
+      float T[NC][2];
+      if constexpr (MED == MED_PSV) {
+        const float l2m = m0 + static_cast<float>(4.0 / 3.0) * m1;
+        const float lam = l2m - 2.0f * m1;
+        T[0][0] = l2m * du[0][0] + lam * du[1][1];
+        T[1][1] = l2m * du[1][1] + lam * du[0][0];
+        T[0][1] = m1 * (du[0][1] + du[1][0]);
+        T[1][0] = T[0][1];
+      } else {
+        T[0][0] = m0 * du[0][0];
+        T[0][1] = m0 * du[0][1];
+      }
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        vset(f0, j * NC + c, jac * (T[c][0] * xix + T[c][1] * xiz));
+        vset(f1, j * NC + c, jac * (T[c][0] * gax + T[c][1] * gaz));
+      }
+    }
+    fx[ix] = f0;
+    s_fg[k * 32 + lane] = f1;
+  }
+  __syncthreads();
+  const uint8_t eflag = st.eflag[e];
+  const int slot = (ss.mode != 0) ? ss.slot[e] : -1;
+#pragma unroll
+  for (int ix = 0; ix < N; ++ix) {
+    float t1[NV], t2[NV];
+#pragma unroll
+    for (int q = 0; q < NV; ++q) { t1[q] = 0.f; t2[q] = 0.f; }
+#pragma unroll
+    for (int l = 0; l < N; ++l) {
+      const W col = s_fg[(l * N + ix) * 32 + lane];
+#pragma unroll
+      for (int q = 0; q < NV; ++q) {
+        t1[q] += vget(fx[l], q) * c_hpw[ix * N + l];
+        t2[q] += vget(col, q) * hpwz[l];
+      }
+    }
+    W out;
+#pragma unroll
+    for (int j = 0; j < SPL; ++j) {
+      float acc[2];
+#pragma unroll
+      for (int c = 0; c < NC; ++c) acc[c] = (wz * t1[j * NC + c] + c_w[ix] * t2[j * NC + c]) * -1.0f;
+      if (eflag) {
+        const size_t p = (static_cast<size_t>(e) * N + iz) * N + ix;
+        const uint8_t b = st.bnd[p];
+        if ((b & 1) && act) {
+          const float *Vp = f.v + (static_cast<size_t>(g[ix]) * S + s0 + j) * NC;
+          float vel[2];
+#pragma unroll
+          for (int c = 0; c < NC; ++c) vel[c] = Vp[c];
+          stacey<MED>(s_st[6 * NN + iz * N + ix], s_st[7 * NN + iz * N + ix], st.mat2 ? st.mat2[p] : 0.f,
+                      st.bnd_nx[p], st.bnd_nz[p], st.bnd_w[p], vel, acc);
+        }
+        if (b & 2) {
+#pragma unroll
+          for (int c = 0; c < NC; ++c) acc[c] = 0.f;
+        }
+      }
+      if (slot >= 0 && act) {
+        const size_t base =
+            ((((static_cast<size_t>(s0 + j) * ss.nstep + istep) * ss.nstacey + slot) * N + iz) * N + ix) * NC;
+        if (ss.mode == 1) {
+#pragma unroll
+          for (int c = 0; c < NC; ++c) ss.data[base + c] = acc[c];
+        } else {
+#pragma unroll
+          for (int c = 0; c < NC; ++c) acc[c] = ss.data[base + c];
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < NC; ++c) vset(out, j * NC + c, acc[c]);
+    }
+    if (act) vred(A + g[ix] * Sv + lofs, out);
+  }
+  tail_work<MED, N>(st, f, S, istep, tw, blockIdx.y * gridDim.x + blockIdx.x, gridDim.x * gridDim.y);
+}
+
+template <int MED, int N, int MINB>
+void launch_shots(const Static &st, const MediumFields &f, int S, const StaceyStore &ss, const int *istep_dev,
+                  const TailWork &tw, cudaStream_t stream) {
+  // two shots per lane when the shared staging fits the static limit (NGLL 5)
+  if constexpr (N <= 5) {
+    if (S % 2 == 0) {
+      dim3 grid(f.nelem, (S / 2 + 31) / 32);
+      k_stiffness_shots<MED, N, 2, MINB><<<grid, N * 32, 0, stream>>>(st, f, S, ss, istep_dev, tw);
+      return;
+    }
+  }
+  {
+    dim3 grid(f.nelem, (S + 31) / 32);
+    k_stiffness_shots<MED, N, 1, MINB><<<grid, N * 32, 0, stream>>>(st, f, S, ss, istep_dev, tw);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Point sources (compute_source_interaction.tpp:77-95): one block per source.
 // ---------------------------------------------------------------------------
 __global__ void k_sources(Static st, SourceSet src, MediumFields f, int medium, int N,
-                          const int *istep_dev, int wavefield_sel) {
+                          const int *istep_dev, int nshots) {
   const int i = blockIdx.x;
   const int k = threadIdx.x;
   if (k >= N * N) return;
@@ -595,14 +635,13 @@ __global__ void k_sources(Static st, SourceSet src, MediumFields f, int medium, 
   const size_t p = static_cast<size_t>(e) * N * N + k;
   const int gi = st.iglob[p];
   const int s = src.shot[i];
-  const size_t ld = static_cast<size_t>(f.nglob + (f.nglob & 1)) * f.nc;
-  float *A = f.a + s * ld;
+  float *A = f.a + (static_cast<size_t>(gi) * nshots + s) * f.nc;
   for (int c = 0; c < f.nc; ++c) {
     const float stf = src.stf[(static_cast<size_t>(i) * src.nstep + istep) * 2 + c];
     const float arr = src.array[(static_cast<size_t>(i) * 2 + c) * N * N + k];
     float val = stf * arr;
     if (medium == MED_AC) val = stf * arr / st.mat1[p];
-    atomicAdd(A + static_cast<size_t>(gi) * f.nc + c, val);
+    atomicAdd(A + c, val);
   }
 }
 
@@ -613,10 +652,8 @@ __global__ void k_couple_acoustic(CouplingSet c, MediumFields ac, MediumFields e
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int s = blockIdx.y;
   if (i >= c.n || s >= nshots) return;
-  const float2 *U = reinterpret_cast<const float2 *>(el.u) + static_cast<size_t>(s) * (el.nglob + (el.nglob & 1));
-  float *A = ac.a + static_cast<size_t>(s) * (ac.nglob + (ac.nglob & 1));
-  const float2 u = U[c.other[i]];
-  atomicAdd(A + c.self[i], c.factor[i] * (c.nx[i] * u.x + c.nz[i] * u.y));
+  const float2 u = reinterpret_cast<const float2 *>(el.u)[static_cast<size_t>(c.other[i]) * nshots + s];
+  atomicAdd(ac.a + static_cast<size_t>(c.self[i]) * nshots + s, c.factor[i] * (c.nx[i] * u.x + c.nz[i] * u.y));
 }
 
 __global__ void k_couple_elastic(CouplingSet c, MediumFields el, MediumFields ac, int nshots,
@@ -624,13 +661,12 @@ __global__ void k_couple_elastic(CouplingSet c, MediumFields el, MediumFields ac
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int s = blockIdx.y;
   if (i >= c.n || s >= nshots) return;
-  const float *Aac = ac.a + static_cast<size_t>(s) * (ac.nglob + (ac.nglob & 1));
-  float *A = el.a + static_cast<size_t>(s) * (el.nglob + (el.nglob & 1)) * 2;
   const int o = c.other[i];
-  const float chi_dd = ac_divided ? Aac[o] : Aac[o] * ac.minv[o];
-  const int g = c.self[i];
-  atomicAdd(A + 2 * g, c.factor[i] * c.nx[i] * chi_dd);
-  atomicAdd(A + 2 * g + 1, c.factor[i] * c.nz[i] * chi_dd);
+  const float r = ac.a[static_cast<size_t>(o) * nshots + s];
+  const float chi_dd = ac_divided ? r : r * ac.minv[o];
+  float *A = el.a + (static_cast<size_t>(c.self[i]) * nshots + s) * 2;
+  atomicAdd(A, c.factor[i] * c.nx[i] * chi_dd);
+  atomicAdd(A + 1, c.factor[i] * c.nz[i] * chi_dd);
 }
 
 // ---------------------------------------------------------------------------
@@ -638,9 +674,8 @@ __global__ void k_couple_elastic(CouplingSet c, MediumFields el, MediumFields ac
 // threads per (receiver, shot).
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ float ld_comp(const MediumFields &f, int which, int s, int g, int c,
-                                         float dt2, int mode) {
-  const size_t ld = static_cast<size_t>(f.nglob + (f.nglob & 1)) * f.nc;
-  const size_t idx = s * ld + static_cast<size_t>(g) * f.nc + c;
+                                         float dt2, int mode, int S) {
+  const size_t idx = (static_cast<size_t>(g) * S + s) * f.nc + c;
   const size_t m = static_cast<size_t>(g) * f.nc + c;
   if (which == 0) return f.u[idx];
   if (mode == 0) return which == 1 ? f.v[idx] : f.a[idx];
@@ -650,7 +685,7 @@ __device__ __forceinline__ float ld_comp(const MediumFields &f, int which, int s
 }
 
 __global__ void k_receivers(Static st, ReceiverSet rec, MediumFields f_psv, MediumFields f_sh,
-                            MediumFields f_ac, int N, float dt2, int mode, const int *istep_dev) {
+                            MediumFields f_ac, int N, float dt2, int mode, const int *istep_dev, int S) {
   __shared__ float s_val[2][64];
   __shared__ float s_red[2][64];
   const int r = blockIdx.x, s = blockIdx.y, k = threadIdx.x;
@@ -678,8 +713,8 @@ __global__ void k_receivers(Static st, ReceiverSet rec, MediumFields f_psv, Medi
       // field on all points of the element, then gradient at this point
       const int which = (med == MED_AC) ? (type == 3 ? 2 : type) : 0;
       if (k < NN) {
-        s_val[0][k] = ld_comp(*F, which, s, g, 0, dt2, mode);
-        s_val[1][k] = (F->nc > 1) ? ld_comp(*F, which, s, g, 1, dt2, mode) : 0.f;
+        s_val[0][k] = ld_comp(*F, which, s, g, 0, dt2, mode, S);
+        s_val[1][k] = (F->nc > 1) ? ld_comp(*F, which, s, g, 1, dt2, mode, S) : 0.f;
       }
       __syncthreads();
       if (k < NN) {
@@ -710,10 +745,10 @@ __global__ void k_receivers(Static st, ReceiverSet rec, MediumFields f_psv, Medi
       __syncthreads();
     } else if (k < NN) {
       if (med == MED_AC) {  // pressure = -chi_ddot
-        w0 = -1.0f * ld_comp(*F, 2, s, g, 0, dt2, mode);
+        w0 = -1.0f * ld_comp(*F, 2, s, g, 0, dt2, mode, S);
       } else {
-        w0 = ld_comp(*F, type, s, g, 0, dt2, mode);
-        w1 = (F->nc > 1) ? ld_comp(*F, type, s, g, 1, dt2, mode) : 0.f;
+        w0 = ld_comp(*F, type, s, g, 0, dt2, mode, S);
+        w1 = (F->nc > 1) ? ld_comp(*F, type, s, g, 1, dt2, mode, S) : 0.f;
       }
     }
     s_red[0][k] = h * w0;
@@ -756,43 +791,11 @@ __global__ void k_corrector(float *v, const float *a, size_t n, float dt2) {
        i += static_cast<size_t>(gridDim.x) * blockDim.x)
     v[i] += dt2 * a[i];
 }
-__global__ void k_divide(float *a, const float *minv, size_t ld, int nshots) {
-  for (size_t j = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; j < ld;
-       j += static_cast<size_t>(gridDim.x) * blockDim.x) {
-    const float m = minv[j];
-    for (int s = 0; s < nshots; ++s) a[s * ld + j] = a[s * ld + j] * m;
-  }
-}
-
-template <bool LAST>
-__global__ void k_fused_update(float2 *u, float2 *v, float2 *a, const float2 *minv, size_t ld2,
-                               int nshots, float dt, float dt2, float dtsq2, Control *ctrl) {
-  if (ctrl && blockIdx.x == 0 && threadIdx.x == 0) ctrl->istep += 1;
-  for (size_t j = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; j < ld2;
-       j += static_cast<size_t>(gridDim.x) * blockDim.x) {
-    const float2 m = minv[j];
-    for (int s = 0; s < nshots; ++s) {
-      const size_t i = s * ld2 + j;
-      const float2 r = a[i];
-      float2 acc, vel = v[i];
-      acc.x = r.x * m.x;
-      acc.y = r.y * m.y;
-      vel.x += dt2 * acc.x;  // corrector (newmark.tpp:44-47)
-      vel.y += dt2 * acc.y;
-      if (LAST) {
-        a[i] = acc;
-        v[i] = vel;
-      } else {
-        float2 uu = u[i];  // next predictor (newmark.tpp:98-105)
-        uu.x += dt * vel.x + dtsq2 * acc.x;
-        uu.y += dt * vel.y + dtsq2 * acc.y;
-        vel.x += dt2 * acc.x;
-        vel.y += dt2 * acc.y;
-        u[i] = uu;
-        v[i] = vel;
-        a[i] = make_float2(0.f, 0.f);
-      }
-    }
+__global__ void k_divide(float *a, const float *minv, size_t n, int nshots, int nc) {
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const size_t c = i % nc, g = (i / nc) / nshots;
+    a[i] = a[i] * minv[g * nc + c];
   }
 }
 
@@ -824,56 +827,62 @@ __global__ void k_update_all(UpdateParams P) {
   const bool record = P.seis != nullptr && istep >= 0 && (istep % P.nsbs) == 0 && (istep / P.nsbs) < P.max_sig;
   const int isig = record ? istep / P.nsbs : 0;
   const size_t total = P.begin[P.nm];
+  const int S = P.nshots;
   for (size_t j = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; j < total;
        j += static_cast<size_t>(gridDim.x) * blockDim.x) {
     int mi = 0;
     while (mi + 1 < P.nm && j >= P.begin[mi + 1]) ++mi;
     const UpdateMedium &M = P.m[mi];
     const size_t jj = j - P.begin[mi];
-    const float2 m = reinterpret_cast<const float2 *>(M.minv)[jj];
+    // pair jj holds (g, s) with both components (nc = 2), or the two
+    // consecutive entries 2jj, 2jj + 1 of [g][s] (nc = 1)
+    int g0, s0, g1, s1;
+    float2 m;
+    if (M.nc == 2) {
+      const uint32_t n = static_cast<uint32_t>(jj);
+      g0 = g1 = static_cast<int>(P.sdiv.div(n));
+      s0 = s1 = static_cast<int>(n - static_cast<uint32_t>(g0) * S);
+      m = reinterpret_cast<const float2 *>(M.minv)[g0];
+    } else {
+      const uint32_t n0 = static_cast<uint32_t>(2 * jj), n1 = n0 + 1;
+      g0 = static_cast<int>(P.sdiv.div(n0));
+      s0 = static_cast<int>(n0 - static_cast<uint32_t>(g0) * S);
+      g1 = static_cast<int>(P.sdiv.div(n1));
+      s1 = static_cast<int>(n1 - static_cast<uint32_t>(g1) * S);
+      m = make_float2(M.minv[g0], M.minv[g1]);
+    }
     float2 *U = reinterpret_cast<float2 *>(M.u);
     float2 *Vv = reinterpret_cast<float2 *>(M.v);
     float2 *A = reinterpret_cast<float2 *>(M.a);
-    bool tapped = false;
+    const float2 r = A[jj];
+    float2 acc, vel = Vv[jj];
+    acc.x = r.x * m.x;
+    acc.y = r.y * m.y;
+    vel.x += P.dt2 * acc.x;  // corrector (newmark.tpp:44-47)
+    vel.y += P.dt2 * acc.y;
+    float2 uu = U[jj];
     if (record && M.taps.nsup > 0) {
-      const int g0 = (M.nc == 2) ? static_cast<int>(jj) : static_cast<int>(2 * jj);
-      tapped = ((M.taps.mask[g0 >> 5] >> (g0 & 31)) & 1u) != 0;
-      if (M.nc == 1) tapped = tapped || (((M.taps.mask[(g0 + 1) >> 5] >> ((g0 + 1) & 31)) & 1u) != 0);
+      if (M.nc == 2) {
+        const float fv[6] = {uu.x, uu.y, vel.x, vel.y, acc.x, acc.y};
+        apply_taps(M.taps, g0, fv, P.seis + (static_cast<size_t>(s0) * P.max_sig + isig) * P.slots);
+      } else {
+        const float f0[6] = {uu.x, 0.f, vel.x, 0.f, acc.x, 0.f};
+        const float f1[6] = {uu.y, 0.f, vel.y, 0.f, acc.y, 0.f};
+        apply_taps(M.taps, g0, f0, P.seis + (static_cast<size_t>(s0) * P.max_sig + isig) * P.slots);
+        apply_taps(M.taps, g1, f1, P.seis + (static_cast<size_t>(s1) * P.max_sig + isig) * P.slots);
+      }
     }
-    for (int s = 0; s < P.nshots; ++s) {
-      const size_t i = s * M.ld2 + jj;
-      const float2 r = A[i];
-      float2 acc, vel = Vv[i];
-      acc.x = r.x * m.x;
-      acc.y = r.y * m.y;
+    if (P.last) {
+      A[jj] = acc;
+      Vv[jj] = vel;
+    } else {
+      uu.x += P.dt * vel.x + P.dtsq2 * acc.x;  // next predictor (newmark.tpp:98-105)
+      uu.y += P.dt * vel.y + P.dtsq2 * acc.y;
       vel.x += P.dt2 * acc.x;
       vel.y += P.dt2 * acc.y;
-      float2 uu = U[i];
-      if (tapped) {
-        float *row = P.seis + (static_cast<size_t>(s) * P.max_sig + isig) * P.slots;
-        if (M.nc == 2) {
-          const float fv[6] = {uu.x, uu.y, vel.x, vel.y, acc.x, acc.y};
-          // which = field * 2 + component
-          apply_taps(M.taps, static_cast<int>(jj), fv, row);
-        } else {
-          const float f0[6] = {uu.x, 0.f, vel.x, 0.f, acc.x, 0.f};
-          const float f1[6] = {uu.y, 0.f, vel.y, 0.f, acc.y, 0.f};
-          apply_taps(M.taps, static_cast<int>(2 * jj), f0, row);
-          apply_taps(M.taps, static_cast<int>(2 * jj + 1), f1, row);
-        }
-      }
-      if (P.last) {
-        A[i] = acc;
-        Vv[i] = vel;
-      } else {
-        uu.x += P.dt * vel.x + P.dtsq2 * acc.x;
-        uu.y += P.dt * vel.y + P.dtsq2 * acc.y;
-        vel.x += P.dt2 * acc.x;
-        vel.y += P.dt2 * acc.y;
-        U[i] = uu;
-        Vv[i] = vel;
-        A[i] = make_float2(0.f, 0.f);
-      }
+      U[jj] = uu;
+      Vv[jj] = vel;
+      A[jj] = make_float2(0.f, 0.f);
     }
   }
   if (P.ctrl) {
@@ -889,7 +898,6 @@ __global__ void k_update_all(UpdateParams P) {
     }
   }
 }
-
 
 // Mass matrix (compute_mass_matrix.tpp:80-113) accumulated in FP64.
 template <int MED>
@@ -943,40 +951,31 @@ size_t field_ld(const MediumFields &f) { return static_cast<size_t>(f.nglob + (f
 
 }  // namespace
 
-static int g_stiffness_variant = 0;
-void set_stiffness_variant(int v) { g_stiffness_variant = v; }
-
 void launch_stiffness(int medium, int ngll, const Static &st, const MediumFields &f, int nshots,
                       const StaceyStore &ss, const int *istep_dev, cudaStream_t stream, const TailWork *tw) {
   if (f.nelem == 0) return;
-  if (g_stiffness_variant == 0 && st.pack != nullptr) {
-    const TailWork none{};
-    const TailWork &w = tw ? *tw : none;
+  const TailWork none{};
+  const TailWork &w = tw ? *tw : none;
+  if (nshots > 1) {
     if (ngll == 5) {
-      if (medium == MED_PSV) launch_rp<MED_PSV, 5, 32, 3>(st, f, nshots, ss, istep_dev, w, stream);
-      else if (medium == MED_SH) launch_rp<MED_SH, 5, 32, 3>(st, f, nshots, ss, istep_dev, w, stream);
-      else launch_rp<MED_AC, 5, 32, 3>(st, f, nshots, ss, istep_dev, w, stream);
-      return;
+      if (medium == MED_PSV) launch_shots<MED_PSV, 5, 4>(st, f, nshots, ss, istep_dev, w, stream);
+      else if (medium == MED_SH) launch_shots<MED_SH, 5, 6>(st, f, nshots, ss, istep_dev, w, stream);
+      else launch_shots<MED_AC, 5, 6>(st, f, nshots, ss, istep_dev, w, stream);
+    } else if (ngll == 8) {
+      if (medium == MED_PSV) launch_shots<MED_PSV, 8, 2>(st, f, nshots, ss, istep_dev, w, stream);
+      else if (medium == MED_SH) launch_shots<MED_SH, 8, 3>(st, f, nshots, ss, istep_dev, w, stream);
+      else launch_shots<MED_AC, 8, 3>(st, f, nshots, ss, istep_dev, w, stream);
     }
-    if (ngll == 8) {
-      if (medium == MED_PSV) launch_rp<MED_PSV, 8, 16, 2>(st, f, nshots, ss, istep_dev, w, stream);
-      else if (medium == MED_SH) launch_rp<MED_SH, 8, 16, 2>(st, f, nshots, ss, istep_dev, w, stream);
-      else launch_rp<MED_AC, 8, 16, 2>(st, f, nshots, ss, istep_dev, w, stream);
-      return;
-    }
+    return;
   }
   if (ngll == 5) {
-    constexpr int N = 5, EPB = 32;
-    dim3 grid((f.nelem + EPB - 1) / EPB, 1);
-    if (medium == MED_PSV) k_stiffness<MED_PSV, N, EPB><<<grid, N * EPB, 0, stream>>>(st, f, nshots, ss, istep_dev);
-    else if (medium == MED_SH) k_stiffness<MED_SH, N, EPB><<<grid, N * EPB, 0, stream>>>(st, f, nshots, ss, istep_dev);
-    else k_stiffness<MED_AC, N, EPB><<<grid, N * EPB, 0, stream>>>(st, f, nshots, ss, istep_dev);
+    if (medium == MED_PSV) launch_rp<MED_PSV, 5, 32, 3>(st, f, nshots, ss, istep_dev, w, stream);
+    else if (medium == MED_SH) launch_rp<MED_SH, 5, 32, 3>(st, f, nshots, ss, istep_dev, w, stream);
+    else launch_rp<MED_AC, 5, 32, 3>(st, f, nshots, ss, istep_dev, w, stream);
   } else if (ngll == 8) {
-    constexpr int N = 8, EPB = 16;
-    dim3 grid((f.nelem + EPB - 1) / EPB, 1);
-    if (medium == MED_PSV) k_stiffness<MED_PSV, N, EPB><<<grid, N * EPB, 0, stream>>>(st, f, nshots, ss, istep_dev);
-    else if (medium == MED_SH) k_stiffness<MED_SH, N, EPB><<<grid, N * EPB, 0, stream>>>(st, f, nshots, ss, istep_dev);
-    else k_stiffness<MED_AC, N, EPB><<<grid, N * EPB, 0, stream>>>(st, f, nshots, ss, istep_dev);
+    if (medium == MED_PSV) launch_rp<MED_PSV, 8, 16, 2>(st, f, nshots, ss, istep_dev, w, stream);
+    else if (medium == MED_SH) launch_rp<MED_SH, 8, 16, 2>(st, f, nshots, ss, istep_dev, w, stream);
+    else launch_rp<MED_AC, 8, 16, 2>(st, f, nshots, ss, istep_dev, w, stream);
   }
 }
 
@@ -985,8 +984,7 @@ void launch_sources(int ngll, const Static &st, const SourceSet &src, MediumFiel
   if (src.n == 0) return;
   const MediumFields &f = fields[medium];
   if (f.nelem == 0) return;
-  k_sources<<<src.n, ngll * ngll <= 32 ? 32 : 64, 0, stream>>>(st, src, f, medium, ngll, istep_dev, 0);
-  (void)nshots;
+  k_sources<<<src.n, ngll * ngll <= 32 ? 32 : 64, 0, stream>>>(st, src, f, medium, ngll, istep_dev, nshots);
 }
 
 void launch_coupling_acoustic(const CouplingSet &c, const MediumFields &ac, const MediumFields &el,
@@ -1008,7 +1006,7 @@ void launch_receivers(int ngll, const Static &st, const ReceiverSet &rec, const 
   if (rec.n == 0 || rec.ntypes == 0) return;
   dim3 grid(rec.n, nshots);
   k_receivers<<<grid, 64, 0, stream>>>(st, rec, fields[MED_PSV], fields[MED_SH], fields[MED_AC], ngll,
-                                       dt2, mode, istep_dev);
+                                       dt2, mode, istep_dev, nshots);
 }
 
 void launch_predictor(const MediumFields &f, int nshots, float dt, float dt2, float dtsq2,
@@ -1023,26 +1021,9 @@ void launch_corrector(const MediumFields &f, int nshots, float dt2, cudaStream_t
   k_corrector<<<grid_for(n, 256), 256, 0, stream>>>(f.v, f.a, n, dt2);
 }
 void launch_divide(const MediumFields &f, int nshots, cudaStream_t stream) {
-  const size_t ld = field_ld(f);
-  if (ld == 0) return;
-  k_divide<<<grid_for(ld, 256), 256, 0, stream>>>(f.a, f.minv, ld, nshots);
-}
-void launch_fused_update(const MediumFields &f, int nshots, float dt, float dt2, float dtsq2,
-                         int last, Control *ctrl, cudaStream_t stream) {
-  const size_t ld2 = field_ld(f) / 2;
-  if (ld2 == 0) {
-    if (ctrl) k_advance<<<1, 1, 0, stream>>>(ctrl);
-    return;
-  }
-  const int grid = grid_for(ld2, 256);
-  if (last)
-    k_fused_update<true><<<grid, 256, 0, stream>>>(reinterpret_cast<float2 *>(f.u), reinterpret_cast<float2 *>(f.v),
-                                                   reinterpret_cast<float2 *>(f.a), reinterpret_cast<const float2 *>(f.minv),
-                                                   ld2, nshots, dt, dt2, dtsq2, ctrl);
-  else
-    k_fused_update<false><<<grid, 256, 0, stream>>>(reinterpret_cast<float2 *>(f.u), reinterpret_cast<float2 *>(f.v),
-                                                    reinterpret_cast<float2 *>(f.a), reinterpret_cast<const float2 *>(f.minv),
-                                                    ld2, nshots, dt, dt2, dtsq2, ctrl);
+  const size_t n = field_ld(f) * nshots;
+  if (n == 0) return;
+  k_divide<<<grid_for(n, 256), 256, 0, stream>>>(f.a, f.minv, n, nshots, f.nc);
 }
 void launch_advance_step(Control *ctrl, cudaStream_t stream) { k_advance<<<1, 1, 0, stream>>>(ctrl); }
 
@@ -1063,7 +1044,6 @@ void launch_update_all(const UpdateParams &p, cudaStream_t stream) {
   k_update_all<<<std::max(grid, 1), 256, 0, stream>>>(p);
 }
 
-bool stiffness_fuses_tail(const Static &st) { return g_stiffness_variant == 0 && st.pack != nullptr; }
 
 void launch_mass(int medium, int ngll, const Static &st, const MediumFields &f, float dt,
                  cudaStream_t stream) {

@@ -8,8 +8,8 @@
 //     mat0, mat1, mat2                P-SV: kappa, mu, rho
 //                                     SH:   mu, rho, -
 //                                     acoustic: rho_inverse, kappa, -
-//   fields, shot-major: field[s][iglob] as float2 (P-SV) or float (SH,
-//   acoustic); the inverse mass has no shot index.
+//   fields, point-major and shot-minor: value (g, s) at g * S + s, as float2
+//   (P-SV) or float (SH, acoustic); the inverse mass has no shot index.
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -38,7 +38,7 @@ struct MediumFields {
   int nc;       // components
   int elem_begin, nelem;      // device element range
   int nelem_interior;         // elements [elem_begin, elem_begin+nelem_interior) have no boundary points
-  float *u, *v, *a;           // [S][nglob*nc]
+  float *u, *v, *a;           // [nglob + nglob % 2][S][nc]
   float *minv;                // [nglob*nc]
   double *mass;               // scratch for initialize, [nglob*nc]
 };
@@ -107,11 +107,30 @@ struct ReceiverTaps {
   const float *w;
 };
 
+// Unsigned 32-bit division by a runtime constant as multiply-high + shift
+// (round-up method): q = (umulhi(n, m) + n) >> l for every n < 2^32.
+struct FastDiv {
+  uint32_t d, m;
+  int l;
+  static FastDiv make(uint32_t d) {
+    FastDiv f{d, 0, 0};
+    while ((1ull << f.l) < d) ++f.l;
+    f.m = static_cast<uint32_t>(((1ull << 32) * ((1ull << f.l) - d)) / d + 1);
+    return f;
+  }
+#ifdef __CUDACC__
+  __device__ __forceinline__ uint32_t div(uint32_t n) const {
+    const uint32_t t = __umulhi(n, m);
+    return static_cast<uint32_t>((static_cast<uint64_t>(t) + n) >> l);
+  }
+#endif
+};
+
 struct UpdateMedium {
   float *u, *v, *a;
   const float *minv;
-  size_t ld2;    // float2 pairs per shot row
-  int nc;        // components per point (1: a pair holds two points)
+  size_t ld2;    // float2 pairs of the whole [g][s][c] array
+  int nc;        // components per point (1: a pair holds two entries)
   ReceiverTaps taps;
 };
 
@@ -120,6 +139,7 @@ struct UpdateParams {
   int nm;
   size_t begin[4];  // pair ranges of the media in the flat index space
   int nshots;
+  FastDiv sdiv;           // division by nshots
   float dt, dt2, dtsq2;
   int last;               // 1: finish the step (no predictor for the next one)
   Control *ctrl;          // step counter, advanced by the last CTA to finish
@@ -131,16 +151,12 @@ struct UpdateParams {
 // ---- launchers (kernels.cu) ----
 void set_quadrature(int ngll, const float *hprime, const float *wgll);
 
-// With the TMA kernel (default) `tw` (may be null) is executed in the same
-// launch; the register-staged variant ignores it (callers then launch the
-// sources / coupling kernels separately).
+// `tw` (may be null) is executed in the same launch.  One shot: the
+// TMA-fed row kernel; several shots: the shot-parallel kernel.
 void launch_stiffness(int medium, int ngll, const Static &st, const MediumFields &f,
                       int nshots, const StaceyStore &ss, const int *istep_dev,
                       cudaStream_t stream, const TailWork *tw = nullptr);
-bool stiffness_fuses_tail(const Static &st);
-// Variant selector for the stiffness kernel: 0 = TMA-fed persistent
-// (default), 1 = register-staged.
-void set_stiffness_variant(int v);
+
 constexpr int kPackFields = 8;
 void launch_sources(int ngll, const Static &st, const SourceSet &src,
                     MediumFields *fields, int nshots, int medium, const int *istep_dev,
@@ -161,10 +177,6 @@ void launch_predictor(const MediumFields &f, int nshots, float dt, float dt2, fl
                       cudaStream_t stream);
 void launch_corrector(const MediumFields &f, int nshots, float dt2, cudaStream_t stream);
 void launch_divide(const MediumFields &f, int nshots, cudaStream_t stream);
-// a = force * minv; v += dt2 a; then (last == 0) u += dt v + dtsq2 a,
-// v += dt2 a, force = 0.  `ctrl` (may be null) has its step advanced.
-void launch_fused_update(const MediumFields &f, int nshots, float dt, float dt2,
-                         float dtsq2, int last, Control *ctrl, cudaStream_t stream);
 void launch_advance_step(Control *ctrl, cudaStream_t stream);
 // Fused divide + corrector (+ predictor of the next step) for every medium in
 // one launch, with the seismogram taps.
