@@ -227,6 +227,17 @@ SFB_API int sfb_get_stream(const sfb_context *ctx, void **stream);
 SFB_API int sfb_time_stiffness(sfb_context *ctx, int medium, int reps,
                                double *mean_ms);
 
+/* Replace the model, per local point [nspec][ngll][ngll] (density, P and S
+ * velocity; S ignored in acoustic elements), as the reference's property
+ * reader does (include/io/property/reader.tpp:17-44).  Fields are not
+ * touched; the mass matrix is rebuilt on the next run. */
+SFB_API int sfb_set_model(sfb_context *ctx, const float *rho, const float *vp,
+                          const float *vs, size_t count);
+/* Zero every wavefield, the seismograms, the Stacey store and the Frechet
+ * kernels, and rewind the step counters (a new simulation on the same
+ * mesh). */
+SFB_API int sfb_reset(sfb_context *ctx);
+
 /* ---- problem export (host arrays; valid while the context lives) ------- */
 
 /* Flat host view of the assembled problem, for checkers and tools that need

@@ -35,6 +35,10 @@ def load():
         lib.oracle_forward.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int,
                                        C.POINTER(C.c_float), C.POINTER(C.POINTER(C.c_float)),
                                        C.POINTER(C.c_float)]
+        lib.oracle_combined.restype = C.c_int
+        lib.oracle_combined.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int,
+                                        C.POINTER(C.c_float), C.POINTER(C.POINTER(C.c_float)),
+                                        C.POINTER(C.c_float), C.POINTER(C.c_double), C.POINTER(C.c_float)]
         lib.oracle_last_error.restype = C.c_char_p
         _lib = lib
     return _lib
@@ -78,3 +82,41 @@ def forward(sim, precision: int = 32, shot: int = 0, nstep=None, threads: int = 
     if store is not None:
         out["stacey_store"] = store
     return out
+
+
+def combined(sim, adjoint_stf, fwd, precision: int = 64, shot: int = 0, threads: int = 1,
+             want_backward_seismograms: bool = False):
+    """Run the oracle's combined (adjoint + backward) loop.  ``fwd`` is the
+    result of ``forward(..., want_fields=True, want_stacey=True)`` (the
+    forward run's last state and Stacey store); ``adjoint_stf`` is
+    [nstep][nrec][2].  Returns FP64 kernels [nspec, ngll, ngll, 3]
+    (elastic: rho, mu, kappa; acoustic: rho, kappa, 0) and optionally the
+    backward seismograms."""
+    lib = load()
+    view = sim.problem_view()
+    info = sim.info()
+    nstep = info.nstep
+    stf = np.ascontiguousarray(adjoint_stf, dtype=np.float32)
+    assert stf.shape == (nstep, info.nreceivers, 2)
+    bufs = (C.POINTER(C.c_float) * 9)()
+    keep = []
+    k = 0
+    for name in ("psv", "sh", "acoustic"):
+        for which in range(3):
+            a = np.ascontiguousarray(fwd[name][which], dtype=np.float32)
+            keep.append(a)
+            bufs[k] = a.ctypes.data_as(C.POINTER(C.c_float))
+            k += 1
+    store = np.ascontiguousarray(fwd["stacey_store"], dtype=np.float32)
+    kernels = np.zeros((info.nspec, info.ngll, info.ngll, 3), dtype=np.float64)
+    bseis = None
+    if want_backward_seismograms:
+        bseis = np.zeros((info.max_sig_step, info.nseismogram_types, info.nreceivers, 2), dtype=np.float32)
+    rc = lib.oracle_combined(C.addressof(view), precision, shot, nstep, threads,
+                             stf.ctypes.data_as(C.POINTER(C.c_float)), bufs,
+                             store.ctypes.data_as(C.POINTER(C.c_float)),
+                             kernels.ctypes.data_as(C.POINTER(C.c_double)),
+                             bseis.ctypes.data_as(C.POINTER(C.c_float)) if bseis is not None else None)
+    if rc != 0:
+        raise RuntimeError("oracle failed: " + lib.oracle_last_error().decode())
+    return (kernels, bseis) if want_backward_seismograms else kernels

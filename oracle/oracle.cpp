@@ -289,6 +289,7 @@ template <typename T> struct Sim {
   // ---- sources (compute_source_interaction.tpp:77-95) --------------------
   void sources(int m, int istep, int wavefield_sel) {
     Field<T> &F = f[m];
+    if (wavefield_sel < 0) return;
     for (int s = 0; s < pv.nsources; ++s) {
       if (pv.src_shot[s] != shot || pv.src_wavefield[s] != wavefield_sel) continue;
       const int e = pv.src_ispec[s];
@@ -460,6 +461,64 @@ template <typename T> struct Sim {
     if (dofs != total_dofs || elements != nspec)
       throw std::runtime_error("The time loop has not updated all the degrees of freedom");
   }
+
+  // ---- Frechet kernels (compute_material_derivatives.tpp:84-153 and
+  // medium/dim2/*/isotropic/frechet_derivative.hpp), per local point,
+  // accumulated in FP64: k[p*3 + 0..2] = (rho, mu, kappa) for elastic,
+  // (rho, kappa, 0) for acoustic.
+  static void frechet(const Sim &adj, const Sim &bwd, T dt, double *k) {
+    const sfb_problem_view &pv = adj.pv;
+    const int n = adj.n, nn = n * n;
+    for (int e = 0; e < pv.nspec; ++e) {
+      const int m = pv.medium[e];
+      if (m == SH) continue;
+      const Field<T> &FA = adj.f[m], &FB = bwd.f[m];
+      const int nc = FA.nc;
+      for (int iz = 0; iz < n; ++iz)
+        for (int ix = 0; ix < n; ++ix) {
+          const size_t p = adj.P(e, iz, ix);
+          T da[2][2], db[2][2];
+          for (int w = 0; w < 2; ++w) {
+            const Field<T> &F = w == 0 ? FA : FB;
+            T dxi[2] = {T(0), T(0)}, dga[2] = {T(0), T(0)};
+            for (int l = 0; l < n; ++l)
+              for (int c = 0; c < nc; ++c) {
+                dxi[c] += adj.hp[ix * n + l] * F.u[static_cast<size_t>(c) * F.nglob + pv.iglob[adj.P(e, iz, l)]];
+                dga[c] += adj.hp[iz * n + l] * F.u[static_cast<size_t>(c) * F.nglob + pv.iglob[adj.P(e, l, ix)]];
+              }
+            T (*d)[2] = w == 0 ? da : db;
+            for (int c = 0; c < nc; ++c) {
+              d[c][0] = static_cast<T>(pv.xix[p]) * dxi[c] + static_cast<T>(pv.gammax[p]) * dga[c];
+              d[c][1] = static_cast<T>(pv.xiz[p]) * dxi[c] + static_cast<T>(pv.gammaz[p]) * dga[c];
+            }
+          }
+          const int g = pv.iglob[p];
+          if (m == PSV) {
+            const T kappa0 = pv.kappa[p], mu = pv.mu[p], rho = pv.rho[p];
+            const T l2m = kappa0 + static_cast<T>(static_cast<float>(4.0 / 3.0)) * mu;
+            const T kappa = l2m - mu;
+            const T ad_dsxx = da[0][0], ad_dsxz = T(0.5) * (da[1][0] + da[0][1]), ad_dszz = da[1][1];
+            const T b_dsxx = db[0][0], b_dsxz = T(0.5) * (db[1][0] + db[0][1]), b_dszz = db[1][1];
+            T kappa_kl = (ad_dsxx + ad_dszz) * (b_dsxx + b_dszz);
+            T mu_kl = (ad_dsxx * b_dsxx + ad_dszz * b_dszz + T(2) * ad_dsxz * b_dsxz -
+                       static_cast<T>(static_cast<float>(1.0 / 3.0)) * kappa_kl);
+            T rho_kl = FA.a[g] * FB.u[g] + FA.a[static_cast<size_t>(FA.nglob) + g] * FB.u[static_cast<size_t>(FB.nglob) + g];
+            kappa_kl = T(-1) * kappa * dt * kappa_kl;
+            mu_kl = T(-2) * mu * dt * mu_kl;
+            rho_kl = T(-1) * rho * dt * rho_kl;
+            k[p * 3 + 0] += static_cast<double>(rho_kl);
+            k[p * 3 + 1] += static_cast<double>(mu_kl);
+            k[p * 3 + 2] += static_cast<double>(kappa_kl);
+          } else {
+            const T ri = pv.rho_inverse[p], kap = pv.kappa[p];
+            const T rho_kl = (da[0][0] * db[0][0] + da[0][1] * db[0][1]) * ri * dt;
+            const T kappa_kl = FA.a[g] * FB.u[g] * T(1) / kap * dt;
+            k[p * 3 + 0] += static_cast<double>(rho_kl);
+            k[p * 3 + 1] += static_cast<double>(kappa_kl);
+          }
+        }
+    }
+  }
 };
 
 template <typename T>
@@ -498,6 +557,62 @@ int run_forward(const sfb_problem_view *pv, int shot, int nstep, int threads,
   return 0;
 }
 
+
+// time_marching<combined>::run (time_marching.tpp:126-247): adjoint wavefield
+// forward in reversed time with the adjoint sources, backward wavefield
+// reconstructed with -dt from the forward run's last state (`buffer`) with
+// Stacey elements replaying the stored element accelerations, Frechet
+// kernels accumulated every step.
+template <typename T>
+int run_combined(const sfb_problem_view *pv, int shot, int nstep, int threads, const float *adjoint_stf,
+                 const float *const *buffer, const std::vector<float> &store, double *kernels,
+                 float *bseis) {
+  Sim<T> adj(*pv, shot), bwd(*pv, shot);
+  adj.threads = bwd.threads = threads;
+  adj.adjoint_stf = adjoint_stf;
+  bwd.backward = true;
+  bwd.stacey_replay = &store;
+  adj.init_mass();
+  bwd.init_mass();
+  for (int e = 0; e < pv->nspec; ++e)
+    if (pv->medium[e] == SH) throw std::invalid_argument("combined SH runs are not supported by the reference");
+  const int nsbs = pv->nstep_between_samples;
+  const int max_sig = pv->nstep / nsbs;
+  int isig = 0;
+  for (int istep = nstep - 1; istep >= 0; --istep) {
+    // adjoint time step (forward-style dt), adjoint sources only
+    adj.predictor(ACOUSTIC, T(1));
+    adj.predictor(PSV, T(1));
+    adj.update(ACOUSTIC, istep, -1);
+    adj.corrector(ACOUSTIC, T(1));
+    adj.update(PSV, istep, -1);
+    adj.corrector(PSV, T(1));
+    // backward time step (-dt), elastic before acoustic, forward sources
+    bwd.predictor(PSV, T(-1));
+    bwd.predictor(ACOUSTIC, T(-1));
+    bwd.update(PSV, istep, 0);
+    bwd.corrector(PSV, T(-1));
+    bwd.update(ACOUSTIC, istep, 0);
+    bwd.corrector(ACOUSTIC, T(-1));
+    if (istep == nstep - 1) {
+      int k = 0;
+      for (int m : {PSV, SH, ACOUSTIC}) {
+        for (auto *vec : {&bwd.f[m].u, &bwd.f[m].v, &bwd.f[m].a}) {
+          const float *src = buffer[k++];
+          if (src)
+            for (size_t i = 0; i < vec->size(); ++i) (*vec)[i] = static_cast<T>(src[i]);
+        }
+      }
+    }
+    Sim<T>::frechet(adj, bwd, static_cast<T>(pv->dt), kernels);
+    if (istep % nsbs == 0 && isig < max_sig) {
+      if (bseis) bwd.seismograms(bseis, isig);
+      ++isig;
+    }
+  }
+  return 0;
+}
+
 thread_local std::string g_err;
 
 }  // namespace
@@ -518,6 +633,25 @@ int oracle_forward(const sfb_problem_view *pv, int precision, int shot,
     if (precision == 64)
       return run_forward<double>(pv, shot, nstep, threads, seis, fields_out, stacey_store_out);
     return run_forward<float>(pv, shot, nstep, threads, seis, fields_out, stacey_store_out);
+  } catch (const std::exception &e) {
+    g_err = e.what();
+    return -1;
+  }
+}
+
+// Combined run of `shot`: adjoint_stf [nstep][nrec][2]; buffer: 9 pointers
+// (u, v, a for P-SV, SH, acoustic; [ncomp][nglob] floats, NULL = zero);
+// stacey_store [nstep][nloc][2] from oracle_forward; kernels_out
+// [nloc][3] FP64 (accumulated into); bseis: backward seismograms or NULL.
+int oracle_combined(const sfb_problem_view *pv, int precision, int shot, int nstep, int threads,
+                    const float *adjoint_stf, const float *const *buffer, const float *stacey_store,
+                    double *kernels_out, float *bseis) {
+  try {
+    const size_t nloc = static_cast<size_t>(pv->nspec) * pv->ngll * pv->ngll;
+    std::vector<float> store(stacey_store, stacey_store + static_cast<size_t>(nstep) * nloc * 2);
+    if (precision == 64)
+      return run_combined<double>(pv, shot, nstep, threads, adjoint_stf, buffer, store, kernels_out, bseis);
+    return run_combined<float>(pv, shot, nstep, threads, adjoint_stf, buffer, store, kernels_out, bseis);
   } catch (const std::exception &e) {
     g_err = e.what();
     return -1;

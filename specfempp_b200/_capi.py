@@ -142,6 +142,8 @@ SIGNATURES = {
                                                     C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                                     _P(C.c_double), C.c_double, C.c_void_p, C.c_void_p]),
     "sfb_noalloc_last_error": (C.c_char_p, []),
+    "sfb_set_model": (C.c_int, [_ctx, _P(C.c_float), _P(C.c_float), _P(C.c_float), C.c_size_t]),
+    "sfb_reset": (C.c_int, [_ctx]),
 }
 
 _lib = None

@@ -107,9 +107,15 @@ struct sfb_context {
   dev::Static st{};
   bool mass_ready = false;
   // Stacey replay store
-  DBuf<float> stacey_data;
+  DBuf<float> stacey_data;  // [S][nstep][nstacey][N*N][2]
   DBuf<int> stacey_slot;
   int nstacey = 0;
+  // adjoint sources: one per (shot, receiver), receiver Lagrange arrays
+  DBuf<int> adj_elem, adj_shot, adj_medium;
+  DBuf<float> adj_array, adj_stf;
+  int nadj = 0;
+  DBuf<double> kern;        // Frechet accumulators [nspec][N*N][3], device element order
+  cudaGraphExec_t graph_combined = nullptr;
   std::vector<float> host_seis;
   // seismogram taps per medium (fused path)
   struct Taps {
@@ -126,6 +132,7 @@ struct sfb_context {
 
   ~sfb_context() {
     if (graph) cudaGraphExecDestroy(graph);
+    if (graph_combined) cudaGraphExecDestroy(graph_combined);
     if (stream) cudaStreamDestroy(stream);
   }
 };
@@ -333,6 +340,14 @@ void ensure_device(sfb_context *c) {
   c->cp_el_nx.upload(P.v_cp_el_nx, tot);
   c->cp_el_nz.upload(P.v_cp_el_nz, tot);
   c->step_scratch.alloc(4, tot);
+  // Stacey replay slots: one per device element carrying Stacey points
+  {
+    std::vector<int> slot(a.nspec, -1);
+    c->nstacey = 0;
+    for (int d = 0; d < a.nspec; ++d)
+      if (eflag[d] & 1) slot[d] = c->nstacey++;
+    c->stacey_slot.upload(slot, tot);
+  }
   c->on_device = true;
 }
 
@@ -561,6 +576,7 @@ dev::UpdateParams update_params(sfb_context *c, WavefieldSet &W, int last, bool 
   u.dtsq2 = static_cast<float>(P.dt * P.dt / 2.0);
   u.last = last;
   u.ctrl = advance ? W.ctrl.p : nullptr;
+  u.dir = 1;
   u.done = c->done.p;
   u.seis = taps ? W.seis.p : nullptr;
   u.slots = static_cast<int>(P.seismogram_types.size() * P.receivers.size() * 2);
@@ -629,8 +645,16 @@ void predictor_all(sfb_context *c, WavefieldSet &W, double sgn) {
                           static_cast<float>(P.dt * P.dt / 2.0), c->stream);
 }
 
+void ensure_store(sfb_context *c) {
+  const Problem &P = c->P;
+  if (c->stacey_data.p || c->nstacey == 0) return;
+  const size_t n = static_cast<size_t>(P.nshots) * P.nstep * c->nstacey * P.asmb.ngll * P.asmb.ngll * 2;
+  c->stacey_data.alloc(n, &c->device_bytes);
+}
+
 void run_forward_fused(sfb_context *c, int nstep, int use_graph) {
   WavefieldSet &W = ensure_wavefield(c, SFB_WAVEFIELD_FORWARD);
+  if (c->P.save_boundary_values) ensure_store(c);
   if (!c->mass_ready) initialize_mass(c, c->P.dt);
   if (nstep <= 0) return;
   if (W.step + nstep > c->P.nstep)
@@ -689,6 +713,233 @@ int update_wavefields(sfb_context *c, int w, int medium, int istep) {
   return W.f[medium].nelem;
 }
 
+
+// ===========================================================================
+// Combined (adjoint + backward) loop, time_marching<combined>::run
+// (include/solver/time_marching.tpp:126-247), fused per step:
+//   adjoint stiffness (acoustic, elastic) with adjoint sources and coupling,
+//   backward stiffness (elastic, acoustic) replaying the Stacey store, with
+//   the forward sources; the backward elastic update sees a zero acoustic
+//   acceleration (the reference predicts both media before updating the
+//   elastic one), so that coupling term is absent, as in the reference;
+//   Frechet accumulation from the adjoint displacement / acceleration and
+//   the backward displacement; then both updates (+dt adjoint, -dt
+//   backward); one step counter counts down.
+// ===========================================================================
+dev::SourceSet adjoint_source_set(sfb_context *c) {
+  dev::SourceSet s{};
+  s.n = c->nadj;
+  s.elem = c->adj_elem.p;
+  s.shot = c->adj_shot.p;
+  s.medium = c->adj_medium.p;
+  s.array = c->adj_array.p;
+  s.stf = c->adj_stf.p;
+  s.nstep = c->P.nstep;
+  return s;
+}
+
+void ensure_adjoint_sources(sfb_context *c) {
+  if (c->nadj > 0 || c->P.receivers.empty()) return;
+  ensure_device(c);
+  const Problem &P = c->P;
+  const Assembly &a = P.asmb;
+  const int nn = a.ngll * a.ngll, nrec = static_cast<int>(P.receivers.size()), S = P.nshots;
+  c->nadj = S * nrec;
+  std::vector<int> el(c->nadj), sh(c->nadj), md(c->nadj);
+  std::vector<float> arr(static_cast<size_t>(c->nadj) * 2 * nn, 0.f);
+  for (int s = 0; s < S; ++s)
+    for (int r = 0; r < nrec; ++r) {
+      const int i = s * nrec + r;
+      const LocatedReceiver &L = P.located_receivers[r];
+      el[i] = c->inv[L.ispec];
+      sh[i] = s;
+      md[i] = a.medium[L.ispec];
+      // reference: src/source/adjoint_source.cpp (lagrange in every component)
+      for (int cc = 0; cc < 2; ++cc)
+        for (int k = 0; k < nn; ++k) arr[(static_cast<size_t>(i) * 2 + cc) * nn + k] = L.lagrange[k];
+    }
+  size_t *tot = &c->device_bytes;
+  c->adj_elem.upload(el, tot);
+  c->adj_shot.upload(sh, tot);
+  c->adj_medium.upload(md, tot);
+  c->adj_array.upload(arr, tot);
+  c->adj_stf.alloc(static_cast<size_t>(c->nadj) * P.nstep * 2, tot);
+}
+
+dev::StaceyStore replay_store(sfb_context *c) {
+  dev::StaceyStore ss{};
+  if (c->stacey_data.p) {
+    ss.data = c->stacey_data.p;
+    ss.slot = c->stacey_slot.p;
+    ss.nstacey = c->nstacey;
+    ss.nstep = c->P.nstep;
+    ss.mode = 2;
+  }
+  return ss;
+}
+
+// Adjoint stiffness (both media) for the step held by the adjoint counter.
+void enqueue_adjoint_stiffness(sfb_context *c, WavefieldSet &A) {
+  const int S = c->P.nshots, n = c->P.asmb.ngll;
+  const int *istep = &A.ctrl.p->istep;
+  dev::StaceyStore none{};
+  dev::SourceSet src = adjoint_source_set(c);
+  dev::TailWork ta{};
+  ta.src = src;
+  ta.cp = coupling_acoustic(c);
+  ta.other = A.f[dev::MED_PSV];
+  ta.cp_mode = ta.cp.n > 0 ? 1 : 0;
+  dev::launch_stiffness(dev::MED_AC, n, c->st, A.f[dev::MED_AC], S, none, istep, c->stream, &ta);
+  dev::TailWork te{};
+  te.src = src;
+  te.cp = coupling_elastic(c);
+  te.other = A.f[dev::MED_AC];
+  te.cp_mode = te.cp.n > 0 ? 2 : 0;
+  dev::launch_stiffness(dev::MED_PSV, n, c->st, A.f[dev::MED_PSV], S, none, istep, c->stream, &te);
+}
+
+void enqueue_backward_stiffness(sfb_context *c, WavefieldSet &A, WavefieldSet &B) {
+  const int S = c->P.nshots, n = c->P.asmb.ngll;
+  const int *istep = &A.ctrl.p->istep;
+  dev::StaceyStore ss = replay_store(c);
+  dev::SourceSet src = source_set(c);
+  dev::TailWork te{};
+  te.src = src;  // elastic first; acoustic acceleration is zero at this point
+  dev::launch_stiffness(dev::MED_PSV, n, c->st, B.f[dev::MED_PSV], S, ss, istep, c->stream, &te);
+  dev::TailWork ta{};
+  ta.src = src;
+  ta.cp = coupling_acoustic(c);
+  ta.other = B.f[dev::MED_PSV];
+  ta.cp_mode = ta.cp.n > 0 ? 1 : 0;
+  dev::launch_stiffness(dev::MED_AC, n, c->st, B.f[dev::MED_AC], S, ss, istep, c->stream, &ta);
+}
+
+void enqueue_frechet(sfb_context *c, WavefieldSet &A, const dev::MediumFields *bwd_fields, int a_is_force) {
+  const float dt = static_cast<float>(c->P.dt);
+  for (int m : {dev::MED_PSV, dev::MED_AC})
+    dev::launch_frechet(m, c->P.asmb.ngll, c->st, A.f[m], bwd_fields[m], c->P.nshots, dt, c->kern.p, a_is_force,
+                        c->stream);
+}
+
+dev::UpdateParams update_params_signed(sfb_context *c, WavefieldSet &W, int last, bool advance, bool taps,
+                                       double sgn) {
+  dev::UpdateParams u = update_params(c, W, last, advance, taps);
+  u.dt = static_cast<float>(sgn * c->P.dt);
+  u.dt2 = static_cast<float>(sgn * c->P.dt / 2.0);
+  u.dir = -1;
+  return u;
+}
+
+void enqueue_combined_step(sfb_context *c, WavefieldSet &A, WavefieldSet &B, int last) {
+  enqueue_adjoint_stiffness(c, A);
+  enqueue_backward_stiffness(c, A, B);
+  enqueue_frechet(c, A, B.f, 1);
+  dev::UpdateParams ua = update_params_signed(c, A, last, false, false, 1.0);
+  dev::launch_update_all(ua, c->stream);
+  // the backward update records the backward seismograms and counts the
+  // shared step counter (held by the adjoint set) down
+  dev::UpdateParams ub = update_params_signed(c, B, last, false, true, -1.0);
+  ub.ctrl = A.ctrl.p;
+  dev::launch_update_all(ub, c->stream);
+}
+
+void copy_fields(sfb_context *c, WavefieldSet &dst, const WavefieldSet &src) {
+  for (int m : kMedia) {
+    const size_t n = dst.u[m].n;
+    if (!n) continue;
+    ck(cudaMemcpyAsync(dst.u[m].p, src.u[m].p, n * sizeof(float), cudaMemcpyDeviceToDevice, c->stream), "copy u");
+    ck(cudaMemcpyAsync(dst.v[m].p, src.v[m].p, n * sizeof(float), cudaMemcpyDeviceToDevice, c->stream), "copy v");
+    ck(cudaMemcpyAsync(dst.a[m].p, src.a[m].p, n * sizeof(float), cudaMemcpyDeviceToDevice, c->stream), "copy a");
+  }
+}
+
+void zero_fields(sfb_context *c, WavefieldSet &W) {
+  for (int m : kMedia) {
+    const size_t n = W.u[m].n;
+    if (!n) continue;
+    ck(cudaMemsetAsync(W.u[m].p, 0, n * sizeof(float), c->stream), "zero u");
+    ck(cudaMemsetAsync(W.v[m].p, 0, n * sizeof(float), c->stream), "zero v");
+    ck(cudaMemsetAsync(W.a[m].p, 0, n * sizeof(float), c->stream), "zero a");
+  }
+  if (W.seis.n) ck(cudaMemsetAsync(W.seis.p, 0, W.seis.n * sizeof(float), c->stream), "zero seis");
+}
+
+void run_combined_fused(sfb_context *c, int use_graph) {
+  const Problem &P = c->P;
+  for (int e = 0; e < P.asmb.nspec; ++e)
+    if (P.asmb.medium[e] == MEDIUM_ELASTIC_SH)
+      throw std::invalid_argument("combined SH runs are not supported (the reference's combined loop has no SH backward predictor)");
+  WavefieldSet &F = ensure_wavefield(c, SFB_WAVEFIELD_FORWARD);
+  if (F.step != P.nstep)
+    throw StateError("the combined run needs the forward run's final state: run " + std::to_string(P.nstep) +
+                     " forward steps first (done: " + std::to_string(F.step) + ")");
+  if (c->nstacey > 0 && !c->stacey_data.p)
+    throw StateError("the forward run did not keep the Stacey store (save_boundary_values)");
+  WavefieldSet &A = ensure_wavefield(c, SFB_WAVEFIELD_ADJOINT);
+  WavefieldSet &B = ensure_wavefield(c, SFB_WAVEFIELD_BACKWARD);
+  ensure_adjoint_sources(c);
+  if (!c->mass_ready) initialize_mass(c, P.dt);
+  build_taps(c);
+  const size_t nk = P.asmb.nloc() * 3;
+  if (!c->kern.p) c->kern.alloc(nk, &c->device_bytes);
+  ck(cudaMemsetAsync(c->kern.p, 0, nk * sizeof(double), c->stream), "zero kernels");
+  zero_fields(c, A);
+  zero_fields(c, B);
+  const int N = P.nstep;
+  set_step(c, A, N - 1);
+  // step N-1: adjoint from rest; the backward state is the forward run's last
+  // state (the reference overwrites its first backward step with it)
+  enqueue_adjoint_stiffness(c, A);
+  enqueue_frechet(c, A, F.f, 1);
+  {
+    dev::UpdateParams ua = update_params_signed(c, A, N == 1, true, false, 1.0);
+    dev::launch_update_all(ua, c->stream);
+  }
+  c->launches += 4;
+  if (N > 1) {
+    copy_fields(c, B, F);
+    for (int m : kMedia)
+      dev::launch_predictor(B.f[m], P.nshots, static_cast<float>(-P.dt), static_cast<float>(-P.dt / 2.0),
+                            static_cast<float>(P.dt * P.dt / 2.0), c->stream);
+    // backward seismogram of step N-1 is the forward run's last sample
+    const int nsbs = P.nstep_between_samples;
+    if ((N - 1) % nsbs == 0 && (N - 1) / nsbs < P.max_sig_step()) {
+      const size_t slots = P.seismogram_types.size() * P.receivers.size() * 2;
+      const size_t isig = static_cast<size_t>((N - 1) / nsbs);
+      for (int s = 0; s < P.nshots; ++s) {
+        const size_t off = (static_cast<size_t>(s) * P.max_sig_step() + isig) * slots;
+        if (slots)
+          ck(cudaMemcpyAsync(B.seis.p + off, F.seis.p + off, slots * sizeof(float), cudaMemcpyDeviceToDevice,
+                             c->stream),
+             "seismograms");
+      }
+    }
+  }
+  const int per_step = 7;
+  const int body = N - 2;  // steps N-2 .. 1 in the body, step 0 closes
+  constexpr int K = 25;
+  int done = 0;
+  if (use_graph && body >= K) {
+    if (!c->graph_combined) {
+      cudaGraph_t g;
+      ck(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+      for (int k = 0; k < K; ++k) enqueue_combined_step(c, A, B, 0);
+      ck(cudaStreamEndCapture(c->stream, &g), "end capture");
+      ck(cudaGraphInstantiate(&c->graph_combined, g, 0), "graph instantiate");
+      cudaGraphDestroy(g);
+    }
+    while (done + K <= body) {
+      ck(cudaGraphLaunch(c->graph_combined, c->stream), "graph launch");
+      done += K;
+    }
+  }
+  for (; done < body; ++done) enqueue_combined_step(c, A, B, 0);
+  if (N > 1) enqueue_combined_step(c, A, B, 1);
+  c->launches += static_cast<uint64_t>(per_step) * (N > 1 ? N - 1 : 0);
+  ck(cudaGetLastError(), "combined step kernels");
+  A.step = N;
+  B.step = N;
+}
 }  // namespace
 
 // ===========================================================================
@@ -1023,4 +1274,191 @@ SFB_API int sfb_time_stiffness(sfb_context *ctx, int medium, int reps, double *m
   });
 }
 
-// Entry points of the adjoint path are provided by adjoint.cu.
+
+SFB_API int sfb_run_combined(sfb_context *ctx, int nstep, int use_graph) {
+  if (!ctx) return SFB_E_INVALID;
+  return guarded(ctx, [&]() {
+    if (nstep != ctx->P.nstep) throw std::invalid_argument("the combined run covers the whole forward run (nstep)");
+    run_combined_fused(ctx, use_graph);
+    ck(cudaStreamSynchronize(ctx->stream), "combined run");
+    check_device_flag(ctx);
+    return SFB_OK;
+  });
+}
+
+SFB_API int sfb_frechet_compute_derivatives(sfb_context *ctx, double dt) {
+  if (!ctx) return SFB_E_INVALID;
+  return guarded(ctx, [&]() {
+    WavefieldSet &A = ensure_wavefield(ctx, SFB_WAVEFIELD_ADJOINT);
+    WavefieldSet &B = ensure_wavefield(ctx, SFB_WAVEFIELD_BACKWARD);
+    const size_t nk = ctx->P.asmb.nloc() * 3;
+    if (!ctx->kern.p) {
+      ctx->kern.alloc(nk, &ctx->device_bytes);
+    }
+    for (int m : {dev::MED_PSV, dev::MED_AC})
+      dev::launch_frechet(m, ctx->P.asmb.ngll, ctx->st, A.f[m], B.f[m], ctx->P.nshots, static_cast<float>(dt),
+                          ctx->kern.p, 0, ctx->stream);
+    ck(cudaGetLastError(), "frechet");
+    return SFB_OK;
+  });
+}
+
+SFB_API int sfb_set_adjoint_sources(sfb_context *ctx, int shot, const float *host, size_t count) {
+  if (!ctx || !host) return SFB_E_INVALID;
+  return guarded(ctx, [&]() {
+    const Problem &P = ctx->P;
+    if (shot < 0 || shot >= P.nshots) throw std::invalid_argument("shot out of range");
+    const int nrec = static_cast<int>(P.receivers.size());
+    const size_t n = static_cast<size_t>(P.nstep) * nrec * 2;
+    if (count < n) throw std::invalid_argument("adjoint source buffer too small ([nstep][nreceivers][2])");
+    ensure_adjoint_sources(ctx);
+    // device layout [source = shot * nrec + r][nstep][2]
+    std::vector<float> tmp(n);
+    for (int t = 0; t < P.nstep; ++t)
+      for (int r = 0; r < nrec; ++r)
+        for (int cc = 0; cc < 2; ++cc)
+          tmp[(static_cast<size_t>(r) * P.nstep + t) * 2 + cc] = host[(static_cast<size_t>(t) * nrec + r) * 2 + cc];
+    ck(cudaMemcpy(ctx->adj_stf.p + static_cast<size_t>(shot) * n, tmp.data(), n * sizeof(float),
+                  cudaMemcpyHostToDevice),
+       "adjoint stf h2d");
+    return SFB_OK;
+  });
+}
+
+SFB_API int sfb_get_kernels(const sfb_context *cctx, int which, double *host, size_t count) {
+  sfb_context *ctx = const_cast<sfb_context *>(cctx);
+  if (!ctx || !host) return SFB_E_INVALID;
+  return guarded(ctx, [&]() {
+    if (which < 0 || which > 5) throw std::invalid_argument("kernel selector must be in [0, 5]");
+    const Assembly &a = ctx->P.asmb;
+    const size_t nloc = a.nloc();
+    const int nn = a.ngll * a.ngll;
+    if (count < nloc) throw std::invalid_argument("kernel buffer too small ([nspec][ngll][ngll])");
+    if (!ctx->kern.p) throw StateError("no kernels have been accumulated");
+    std::vector<double> k(nloc * 3);
+    ck(cudaStreamSynchronize(ctx->stream), "sync");
+    ck(cudaMemcpy(k.data(), ctx->kern.p, k.size() * sizeof(double), cudaMemcpyDeviceToHost), "kernels d2h");
+    for (int e = 0; e < a.nspec; ++e) {
+      const int d = ctx->inv[e];
+      for (int q = 0; q < nn; ++q) {
+        const size_t p = static_cast<size_t>(e) * nn + q, pd = static_cast<size_t>(d) * nn + q;
+        const double k0 = k[pd * 3], k1 = k[pd * 3 + 1], k2 = k[pd * 3 + 2];
+        double v = 0.0;
+        if (a.medium[e] == MEDIUM_ACOUSTIC) {
+          v = which == 0 ? k0 : which == 2 ? k1 : 0.0;  // rho, kappa
+        } else {
+          // derived kernels (frechet_derivative.hpp:117-135), linear in the
+          // primaries at fixed model: kappa' = lambda + 2 mu - mu
+          const float mu = a.mu[p];
+          const float kap = a.kappa[p] + static_cast<float>(4.0 / 3.0) * mu - mu;
+          const double r = static_cast<double>(mu) / kap;
+          switch (which) {
+          case 0: v = k0; break;
+          case 1: v = k1; break;
+          case 2: v = k2; break;
+          case 3: v = k0 + k2 + k1; break;
+          case 4: v = 2.0 * (1.0 + 4.0 / 3.0 * r) * k2; break;
+          case 5: v = 2.0 * (k1 - 4.0 / 3.0 * r * k2); break;
+          }
+        }
+        host[p] = v;
+      }
+    }
+    return SFB_OK;
+  });
+}
+
+SFB_API int sfb_copy_forward_to_backward(const sfb_context *csrc, sfb_context *dst) {
+  sfb_context *src = const_cast<sfb_context *>(csrc);
+  if (!src || !dst) return SFB_E_INVALID;
+  return guarded(dst, [&]() {
+    if (src->P.asmb.nloc() != dst->P.asmb.nloc() || src->P.nstep != dst->P.nstep || src->P.nshots != dst->P.nshots)
+      throw std::invalid_argument("the two contexts do not describe the same problem");
+    WavefieldSet &S = ensure_wavefield(src, SFB_WAVEFIELD_FORWARD);
+    WavefieldSet &D = ensure_wavefield(dst, SFB_WAVEFIELD_FORWARD);
+    ck(cudaStreamSynchronize(src->stream), "sync src");
+    copy_fields(dst, D, S);
+    if (src->stacey_data.p) {
+      ensure_store(dst);
+      ck(cudaMemcpyAsync(dst->stacey_data.p, src->stacey_data.p, src->stacey_data.n * sizeof(float),
+                         cudaMemcpyDeviceToDevice, dst->stream),
+         "copy store");
+    }
+    ck(cudaStreamSynchronize(dst->stream), "sync dst");
+    D.step = S.step;
+    return SFB_OK;
+  });
+}
+
+SFB_API int sfb_set_model(sfb_context *ctx, const float *rho, const float *vp, const float *vs, size_t count) {
+  if (!ctx || !rho || !vp || !vs) return SFB_E_INVALID;
+  return guarded(ctx, [&]() {
+    Assembly &a = ctx->P.asmb;
+    const size_t nloc = a.nloc();
+    const int nn = a.ngll * a.ngll;
+    if (count < nloc) throw std::invalid_argument("model arrays too small ([nspec][ngll][ngll])");
+    for (size_t p = 0; p < nloc; ++p) {
+      const int e = static_cast<int>(p / nn);
+      const double r = rho[p], cp = vp[p], cs = vs[p];
+      if (a.medium[e] == MEDIUM_ACOUSTIC) {
+        a.kappa[p] = static_cast<float>(r * cp * cp);
+        a.rho_inverse[p] = 1.0f / static_cast<float>(r);
+        a.rho[p] = static_cast<float>(r);
+      } else {
+        a.kappa[p] = static_cast<float>(r * (cp * cp - (4.0 / 3.0) * cs * cs));
+        a.mu[p] = static_cast<float>(r * cs * cs);
+        a.rho[p] = static_cast<float>(r);
+        a.rho_inverse[p] = 1.0f / static_cast<float>(r);
+      }
+    }
+    if (ctx->on_device) {
+      // refresh the material words of the packed and SoA device arrays
+      std::vector<float> m0(nloc), m1(nloc), m2(nloc);
+      std::vector<float> pack(nloc * dev::kPackFields);
+      ck(cudaMemcpy(pack.data(), ctx->pack.p, pack.size() * sizeof(float), cudaMemcpyDeviceToHost), "pack d2h");
+      for (int d = 0; d < a.nspec; ++d) {
+        const int e = ctx->perm[d];
+        const int m = a.medium[e];
+        for (int k = 0; k < nn; ++k) {
+          const size_t p = static_cast<size_t>(e) * nn + k, q = static_cast<size_t>(d) * nn + k;
+          if (m == MEDIUM_ELASTIC_PSV) { m0[q] = a.kappa[p]; m1[q] = a.mu[p]; m2[q] = a.rho[p]; }
+          else if (m == MEDIUM_ELASTIC_SH) { m0[q] = a.mu[p]; m1[q] = a.rho[p]; m2[q] = 0.f; }
+          else { m0[q] = a.rho_inverse[p]; m1[q] = a.kappa[p]; m2[q] = 0.f; }
+          float *blk = &pack[static_cast<size_t>(d) * dev::kPackFields * nn];
+          blk[6 * nn + k] = m0[q];
+          blk[7 * nn + k] = m1[q];
+        }
+      }
+      ck(cudaMemcpy(ctx->pack.p, pack.data(), pack.size() * sizeof(float), cudaMemcpyHostToDevice), "pack h2d");
+      ck(cudaMemcpy(ctx->mat0_all.p, m0.data(), nloc * sizeof(float), cudaMemcpyHostToDevice), "mat0");
+      ck(cudaMemcpy(ctx->mat1_all.p, m1.data(), nloc * sizeof(float), cudaMemcpyHostToDevice), "mat1");
+      ck(cudaMemcpy(ctx->mat2_all.p, m2.data(), nloc * sizeof(float), cudaMemcpyHostToDevice), "mat2");
+      ctx->taps_ready = false;  // pressure taps carry the material
+      // captured graphs hold the old tap buffers
+      if (ctx->graph) cudaGraphExecDestroy(ctx->graph);
+      if (ctx->graph_combined) cudaGraphExecDestroy(ctx->graph_combined);
+      ctx->graph = nullptr;
+      ctx->graph_combined = nullptr;
+    }
+    ctx->mass_ready = false;
+    return SFB_OK;
+  });
+}
+
+SFB_API int sfb_reset(sfb_context *ctx) {
+  if (!ctx) return SFB_E_INVALID;
+  return guarded(ctx, [&]() {
+    if (!ctx->on_device) return SFB_OK;
+    for (int w = 0; w < 3; ++w) {
+      WavefieldSet &W = ctx->wf[w];
+      if (!W.allocated) continue;
+      zero_fields(ctx, W);
+      W.step = 0;
+    }
+    if (ctx->stacey_data.p) ck(cudaMemsetAsync(ctx->stacey_data.p, 0, ctx->stacey_data.n * sizeof(float), ctx->stream), "zero store");
+    if (ctx->kern.p) ck(cudaMemsetAsync(ctx->kern.p, 0, ctx->kern.n * sizeof(double), ctx->stream), "zero kernels");
+    ck(cudaStreamSynchronize(ctx->stream), "reset");
+    return SFB_OK;
+  });
+}
+

@@ -351,7 +351,7 @@ k_stiffness_rp(Static st, MediumFields f, int nshots, StaceyStore ss, const int 
 #pragma unroll
         for (int ix = 0; ix < N; ++ix) {
           const size_t base =
-              ((((static_cast<size_t>(s) * ss.nstep + istep) * ss.nstacey + slot) * N + iz) * N + ix) * NC;
+              ((((static_cast<size_t>(s) * ss.nstep + istep) * ss.nstacey + slot) * N + iz) * N + ix) * 2;
           if (ss.mode == 1) {
 #pragma unroll
             for (int c = 0; c < NC; ++c) ss.data[base + c] = accr[ix][c];
@@ -586,7 +586,7 @@ k_stiffness_shots(Static st, MediumFields f, int S, StaceyStore ss, const int *i
       }
       if (slot >= 0 && act) {
         const size_t base =
-            ((((static_cast<size_t>(s0 + j) * ss.nstep + istep) * ss.nstacey + slot) * N + iz) * N + ix) * NC;
+            ((((static_cast<size_t>(s0 + j) * ss.nstep + istep) * ss.nstacey + slot) * N + iz) * N + ix) * 2;
         if (ss.mode == 1) {
 #pragma unroll
           for (int c = 0; c < NC; ++c) ss.data[base + c] = acc[c];
@@ -891,11 +891,99 @@ __global__ void k_update_all(UpdateParams P) {
       __threadfence();
       const unsigned prev = atomicAdd(P.done, 1u);
       if (prev == gridDim.x - 1) {
-        P.ctrl->istep = istep + 1;
+        P.ctrl->istep = istep + P.dir;
         *P.done = 0u;
         __threadfence();
       }
     }
+  }
+}
+
+
+// ---------------------------------------------------------------------------
+// Frechet kernels (compute_material_derivatives.tpp:84-153 with
+// medium/dim2/elastic/isotropic/frechet_derivative.hpp:14-138 and
+// medium/dim2/acoustic/isotropic/frechet_derivative.hpp:12-41).  Thread per
+// local point, EPB elements per CTA; gradients of the adjoint and backward
+// displacements through shared memory; the per-step FP32 contributions of
+// all shots are summed in FP64 registers and added once into the per-point
+// FP64 accumulators kern[p][3] = (rho, mu, kappa) elastic, (rho, kappa, 0)
+// acoustic.  The adjoint acceleration is its force times the inverse mass.
+// ---------------------------------------------------------------------------
+template <int MED, int N, int EPB>
+__global__ void __launch_bounds__(EPB * N * N)
+k_frechet(Static st, MediumFields A, MediumFields B, int S, float dt, double *kern, int a_is_force) {
+  constexpr int NC = (MED == MED_PSV) ? 2 : 1;
+  constexpr int NN = N * N;
+  __shared__ float s_a[EPB][NC][NN];
+  __shared__ float s_b[EPB][NC][NN];
+  const int t = threadIdx.x;
+  const int el = t / NN, k = t % NN, iz = k / N, ix = k % N;
+  const int li = blockIdx.x * EPB + el;
+  const bool valid = li < A.nelem;
+  const int e = A.elem_begin + (valid ? li : 0);
+  const size_t p = static_cast<size_t>(e) * NN + k;
+  const int g = valid ? st.iglob[p] : 0;
+  const float xix = st.xix[p], xiz = st.xiz[p], gax = st.gax[p], gaz = st.gaz[p];
+  const float m0 = st.mat0[p], m1 = st.mat1[p];
+  const float m2 = st.mat2 ? st.mat2[p] : 0.f;
+  double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
+  for (int s = 0; s < S; ++s) {
+    const size_t base = (static_cast<size_t>(g) * S + s) * NC;
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      s_a[el][c][k] = valid ? A.u[base + c] : 0.f;
+      s_b[el][c][k] = valid ? B.u[base + c] : 0.f;
+    }
+    __syncthreads();
+    float da[NC][2], db[NC][2];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      float axi = 0.f, aga = 0.f, bxi = 0.f, bga = 0.f;
+#pragma unroll
+      for (int l = 0; l < N; ++l) {
+        axi += c_hp[ix * N + l] * s_a[el][c][iz * N + l];
+        aga += c_hp[iz * N + l] * s_a[el][c][l * N + ix];
+        bxi += c_hp[ix * N + l] * s_b[el][c][iz * N + l];
+        bga += c_hp[iz * N + l] * s_b[el][c][l * N + ix];
+      }
+      da[c][0] = xix * axi + gax * aga;
+      da[c][1] = xiz * axi + gaz * aga;
+      db[c][0] = xix * bxi + gax * bga;
+      db[c][1] = xiz * bxi + gaz * bga;
+    }
+    if (valid) {
+      if constexpr (MED == MED_PSV) {
+        const float l2m = m0 + static_cast<float>(4.0 / 3.0) * m1;
+        const float kappa = l2m - m1;
+        const float ad_dsxx = da[0][0], ad_dsxz = 0.5f * (da[1][0] + da[0][1]), ad_dszz = da[1][1];
+        const float b_dsxx = db[0][0], b_dsxz = 0.5f * (db[1][0] + db[0][1]), b_dszz = db[1][1];
+        float kappa_kl = (ad_dsxx + ad_dszz) * (b_dsxx + b_dszz);
+        float mu_kl = (ad_dsxx * b_dsxx + ad_dszz * b_dszz + 2.0f * ad_dsxz * b_dsxz -
+                       static_cast<float>(1.0 / 3.0) * kappa_kl);
+        const float ax = a_is_force ? A.a[base] * A.minv[static_cast<size_t>(g) * 2] : A.a[base];
+        const float az = a_is_force ? A.a[base + 1] * A.minv[static_cast<size_t>(g) * 2 + 1] : A.a[base + 1];
+        float rho_kl = ax * B.u[base] + az * B.u[base + 1];
+        kappa_kl = -1.0f * kappa * dt * kappa_kl;
+        mu_kl = -2.0f * m1 * dt * mu_kl;
+        rho_kl = -1.0f * m2 * dt * rho_kl;
+        acc0 += static_cast<double>(rho_kl);
+        acc1 += static_cast<double>(mu_kl);
+        acc2 += static_cast<double>(kappa_kl);
+      } else {
+        const float rho_kl = (da[0][0] * db[0][0] + da[0][1] * db[0][1]) * m0 * dt;
+        const float chi_dd = a_is_force ? A.a[base] * A.minv[g] : A.a[base];
+        const float kappa_kl = chi_dd * B.u[base] * 1.0f / m1 * dt;
+        acc0 += static_cast<double>(rho_kl);
+        acc1 += static_cast<double>(kappa_kl);
+      }
+    }
+    __syncthreads();
+  }
+  if (valid) {
+    kern[p * 3 + 0] += acc0;
+    kern[p * 3 + 1] += acc1;
+    kern[p * 3 + 2] += acc2;
   }
 }
 
@@ -1059,6 +1147,22 @@ void launch_invert_mass(const MediumFields &f, cudaStream_t stream) {
   if (n == 0) return;
   k_invert<<<grid_for(n, 256), 256, 0, stream>>>(f.mass, f.minv, n);
 }
+void launch_frechet(int medium, int ngll, const Static &st, const MediumFields &adj, const MediumFields &bwd,
+                    int nshots, float dt, double *kern, int a_is_force, cudaStream_t stream) {
+  if (adj.nelem == 0) return;
+  if (ngll == 5) {
+    constexpr int EPB = 8;
+    const int grid = (adj.nelem + EPB - 1) / EPB;
+    if (medium == MED_PSV) k_frechet<MED_PSV, 5, EPB><<<grid, EPB * 25, 0, stream>>>(st, adj, bwd, nshots, dt, kern, a_is_force);
+    else if (medium == MED_AC) k_frechet<MED_AC, 5, EPB><<<grid, EPB * 25, 0, stream>>>(st, adj, bwd, nshots, dt, kern, a_is_force);
+  } else if (ngll == 8) {
+    constexpr int EPB = 4;
+    const int grid = (adj.nelem + EPB - 1) / EPB;
+    if (medium == MED_PSV) k_frechet<MED_PSV, 8, EPB><<<grid, EPB * 64, 0, stream>>>(st, adj, bwd, nshots, dt, kern, a_is_force);
+    else if (medium == MED_AC) k_frechet<MED_AC, 8, EPB><<<grid, EPB * 64, 0, stream>>>(st, adj, bwd, nshots, dt, kern, a_is_force);
+  }
+}
+
 void launch_zero(float *p, size_t n, cudaStream_t stream) {
   if (n == 0) return;
   k_zero<<<grid_for(n, 256), 256, 0, stream>>>(p, n);

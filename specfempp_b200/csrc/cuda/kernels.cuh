@@ -75,7 +75,7 @@ struct CouplingSet {
 };
 
 // Stacey replay / store (adjoint reconstruction): element-local
-// accelerations of the Stacey elements, [nstep][nstacey][N*N][nc].
+// accelerations of the Stacey elements, [S][nstep][nstacey][N*N][2].
 struct StaceyStore {
   float *data;
   const int *slot;   // per device element: slot index or -1
@@ -143,6 +143,7 @@ struct UpdateParams {
   float dt, dt2, dtsq2;
   int last;               // 1: finish the step (no predictor for the next one)
   Control *ctrl;          // step counter, advanced by the last CTA to finish
+  int dir;                // +1 forward in time, -1 for the combined (reversed) loop
   unsigned *done;         // CTA completion counter (zero between launches)
   float *seis;            // [S][max_sig][slots]
   int slots, max_sig, nsbs;
@@ -185,6 +186,11 @@ void launch_mass(int medium, int ngll, const Static &st, const MediumFields &f, 
                  cudaStream_t stream);
 void launch_invert_mass(const MediumFields &f, cudaStream_t stream);
 void launch_zero(float *p, size_t n, cudaStream_t stream);
+// Frechet kernel accumulation for one medium (P-SV or acoustic) into
+// kern[p][3] (FP64, device element order).  a_is_force: the adjoint `a`
+// array holds the unassembled force of the fused loop (multiply by M^-1).
+void launch_frechet(int medium, int ngll, const Static &st, const MediumFields &adj, const MediumFields &bwd,
+                    int nshots, float dt, double *kern, int a_is_force, cudaStream_t stream);
 
 }  // namespace dev
 }  // namespace sfb

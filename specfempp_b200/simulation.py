@@ -231,3 +231,47 @@ class Simulation:
         i = self.info()
         k = np.arange(i.max_sig_step, dtype=np.float32)
         return (k * np.float32(i.dt) * np.float32(i.nstep_between_samples) + np.float32(i.t0)).astype(np.float32)
+
+    # ---- combined (adjoint + backward) run --------------------------------
+    def set_adjoint_sources(self, stf: np.ndarray, shot: int = 0):
+        """Adjoint source time functions [nstep][nreceivers][2] of `shot`
+        (receiver r acts at its station with its Lagrange weights)."""
+        a = np.ascontiguousarray(stf, dtype=np.float32)
+        self._check(self._lib.sfb_set_adjoint_sources(self._h, shot, _fptr(a), a.size))
+
+    def run_combined(self, graph: bool = True):
+        self._check(self._lib.sfb_run_combined(self._h, self.info().nstep, 1 if graph else 0))
+
+    def kernels(self, which: int) -> np.ndarray:
+        """Frechet kernel summed over shots, [nspec][ngll][ngll] FP64:
+        0 rho, 1 mu, 2 kappa, 3 rhop, 4 alpha, 5 beta (acoustic points:
+        0 rho, 2 kappa)."""
+        i = self.info()
+        out = np.zeros((i.nspec, i.ngll, i.ngll), dtype=np.float64)
+        self._check(self._lib.sfb_get_kernels(self._h, which, out.ctypes.data_as(C.POINTER(C.c_double)), out.size))
+        return out
+
+    def set_model(self, rho, vp, vs):
+        """Per-local-point model [nspec][ngll][ngll] (density, vp, vs)."""
+        arrs = [np.ascontiguousarray(a, dtype=np.float32) for a in (rho, vp, vs)]
+        self._check(self._lib.sfb_set_model(self._h, _fptr(arrs[0]), _fptr(arrs[1]), _fptr(arrs[2]), arrs[0].size))
+
+    def reset(self):
+        self._check(self._lib.sfb_reset(self._h))
+
+    def quadrature_volume(self) -> np.ndarray:
+        """w_x w_z J per local point [nspec][ngll][ngll] (FP64)."""
+        v = self.problem_view()
+        i = self.info()
+        n = i.ngll
+        w = np.ctypeslib.as_array(v.wgll, shape=(n,)).astype(np.float64)
+        J = np.ctypeslib.as_array(v.jacobian, shape=(i.nspec * n * n,)).reshape(i.nspec, n, n).astype(np.float64)
+        return w[None, :, None] * w[None, None, :] * J
+
+    def material(self):
+        """(kappa, mu, rho) per local point as stored (FP32 -> FP64)."""
+        v = self.problem_view()
+        i = self.info()
+        shape = (i.nspec, i.ngll, i.ngll)
+        get = lambda p: np.ctypeslib.as_array(p, shape=(int(np.prod(shape)),)).reshape(shape).astype(np.float64)
+        return get(v.kappa), get(v.mu), get(v.rho)
