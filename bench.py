@@ -8,10 +8,15 @@ The metric is GLL point updates per second: nshots * nglob * steps / time,
 nglob summed over media.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload coupled|plain|batched]
+                  [--workload coupled|plain|batched] [--no-secondary]
 
-Under torchrun each rank runs an independent replica (the path does not
-shard; "replicas only"); the reported value sums all ranks' point updates
+On one GPU the default line also carries `batched` (the 64-shot 800 x 400
+batched forward: rate and whole-step HBM fraction) and `fwi` (forward +
+adjoint gradient of 64 shots batched against one shot alone on the
+200 x 200 adjoint mesh: per-shot device time and speed-up).
+
+Under torchrun each rank runs an independent replica (the forward path does
+not shard; "replicas only"); the reported value sums all ranks' point updates
 over the slowest rank's device time.  `--impl reference` times the CPU
 restatement of the reference (oracle/) on the host cores instead.
 """
@@ -146,6 +151,108 @@ def stiffness_bytes(info, problem_view, medium):
     P = 3 if medium in (0, 1) else 2
     C = 2 if medium == 0 else 1
     return nel * nn * (4 + 4 * 5 + 4 * P) + info.nshots * info.nglob[medium] * C * 4 * 2
+
+
+def step_bytes(info):
+    """Algorithmic HBM bytes of one whole time step: per local point the
+    static block (4 index + 4 * 5 geometry + 4 * P material), per global
+    point the inverse mass (4 C), and per shot and global point 28 C bytes
+    (displacement read by the stiffness; u, v, a read and written by the
+    update)."""
+    nn = info.ngll * info.ngll
+    total = 0
+    for m, (P, C) in ((0, (3, 2)), (1, (3, 1)), (3, (2, 1))):
+        total += info.nelements[m] * nn * (4 + 20 + 4 * P) + info.nglob[m] * 4 * C
+        total += info.nshots * info.nglob[m] * 28 * C
+    return total
+
+
+def event_time(stream, fn):
+    import torch
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    fn()
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def sim_stream(sim):
+    import ctypes as C
+    import torch
+    from specfempp_b200 import _capi as A
+    ptr = C.c_void_p()
+    A.check(A.load().sfb_get_stream(sim.handle, C.byref(ptr)), sim.handle)
+    return torch.cuda.ExternalStream(ptr.value)
+
+
+def batched_forward(steps):
+    """The 64-shot batched forward (800 x 400 elements): device time per step
+    and whole-step algorithmic HBM bytes against the measured peak."""
+    import ctypes as C
+    from specfempp_b200 import Simulation, _capi as A
+    p = make_problem("batched", GRAPH_STEPS + 3 + steps + 1)
+    with Simulation.structured(p) as sim:
+        sim.initialize()
+        stream = sim_stream(sim)
+        sim.run_forward(GRAPH_STEPS)
+        sim.run_forward(3)
+        ms = event_time(stream, lambda: sim.run_forward(steps))
+        info = sim.info()
+        mean_ms = C.c_double()
+        A.check(A.load().sfb_time_stiffness(sim.handle, 0, 10, C.byref(mean_ms)), sim.handle)
+    peak, _ = measured_peak()
+    per_step = ms / steps
+    b = step_bytes(info)
+    return {
+        "workload": workload_config("batched", info, p)["workload"],
+        "value": info.nshots * sum(info.nglob) * steps / (ms / 1000.0), "unit": "GLL-point-updates/s",
+        "ms_per_step": per_step, "steps": steps,
+        "step_roofline": {"bound": "hbm", "algorithmic_bytes_per_step": b,
+                          "achieved": b / (per_step / 1000.0) / 1e9, "peak": peak, "unit": "GB/s",
+                          "frac": b / (per_step / 1000.0) / 1e9 / peak},
+        "stiffness_ms": mean_ms.value,
+    }
+
+
+def fwi_comparison(nshots=64, nstep=400, reps=2):
+    """Forward + combined (adjoint + backward + Frechet kernels) run of the
+    200 x 200 adjoint mesh: `nshots` shots batched in one context against one
+    shot alone (the plain single-shot path), per-shot device time, same GPU.
+    The adjoint sources are seeded synthetic residuals (cost does not depend
+    on their values)."""
+    from specfempp_b200 import Simulation
+    from specfempp_b200 import workloads as W
+
+    def timed(S):
+        p = W.adjoint_model(1.0, nshots=S, nstep=nstep)
+        p.save_boundary_values = True
+        with Simulation.structured(p) as sim:
+            info = sim.info()
+            rng = np.random.default_rng(3)
+            for s in range(S):
+                sim.set_adjoint_sources((1e-3 * rng.standard_normal((nstep, info.nreceivers, 2))).astype(np.float32),
+                                        shot=s)
+            stream = sim_stream(sim)
+            best = None
+            for r in range(reps + 1):  # the first run captures the graphs
+                sim.reset()
+                ms = event_time(stream, lambda: (sim.run_forward(), sim.run_combined()))
+                if r:
+                    best = ms if best is None else min(best, ms)
+            return best, info
+
+    ms_b, info_b = timed(nshots)
+    ms_1, info_1 = timed(1)
+    return {
+        "workload": "forward + adjoint gradient, 200x200 NGLL=5 elements, 10x10 km, %d receivers, "
+                    "%d steps (a slice of the 6000-step run; per-step cost is constant)" % (info_b.nreceivers, nstep),
+        "shots": nshots, "batched_ms_per_shot": ms_b / nshots, "single_shot_ms": ms_1,
+        "batched_shots_per_s": nshots / (ms_b / 1000.0), "single_shots_per_s": 1.0 / (ms_1 / 1000.0),
+        "per_shot_speedup": ms_1 / (ms_b / nshots),
+    }
 
 
 def cpu_rate(workload, nstep_hint, threads, budget_s=12.0, sample_steps=None):
@@ -308,6 +415,14 @@ def run_ours(args):
         "gpu_launches": int(launches),
         "clocks": clocks,
     }
+    step_b = step_bytes(info)
+    line["step_roofline"] = {"bound": "hbm", "algorithmic_bytes_per_step": step_b,
+                             "achieved": step_b / (ms / K / 1000.0) / 1e9, "peak": peak, "unit": "GB/s",
+                             "frac": step_b / (ms / K / 1000.0) / 1e9 / peak}
+    if world == 1 and args.workload == "coupled" and not args.no_secondary:
+        sim.close()
+        line["batched"] = batched_forward(min(K, 100))
+        line["fwi"] = fwi_comparison()
     if world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         rate, n, dt, _ = cpu_rate(args.workload, None, threads, budget_s=args.cpu_seconds)
@@ -329,6 +444,8 @@ def main():
     ap.add_argument("--workload", default="coupled", choices=["coupled", "plain", "batched"])
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-secondary", action="store_true",
+                    help="skip the batched-forward and batched-vs-single adjoint measurements")
     ap.add_argument("--scale", type=float, default=1.0,
                     help="shrink the workload's element counts (profiling captures); 1 = full size")
     args = ap.parse_args()
