@@ -128,8 +128,21 @@ typedef struct sfb_info {
   double dt, t0;
   size_t device_bytes;   /* device memory held by the context                */
   uint64_t kernel_launches; /* kernels this context has launched so far      */
+  int stiffness_variant[4]; /* batched (nshots > 1) stiffness kernel per medium
+                               tag: 0 not chosen yet, 1 two shots per lane in
+                               packed FP32x2, 2 two shots per lane scalar,
+                               3 one shot per lane                           */
+  int private_points;    /* P-SV points updated inside the batched stiffness
+                            launch of the forward run (0: none)             */
 } sfb_info;
 SFB_API int sfb_get_info(const sfb_context *ctx, sfb_info *info);
+
+/* Batched stiffness kernel of `medium` (values of sfb_info.stiffness_variant;
+ * 0 = let the autotuner choose).  The autotuner runs once, when the forward
+ * fields are first allocated, and times every variant on this mesh; a
+ * variant set before that is kept.  No reference counterpart (the
+ * reference's chunk size is a compile-time constant). */
+SFB_API int sfb_set_stiffness_variant(sfb_context *ctx, int medium, int variant);
 
 /* ---- domain_kernels (include/kokkos_kernels/domain_kernels.hpp) -------- */
 

@@ -78,6 +78,7 @@ class sfb_info(C.Structure):
         ("nreceivers", C.c_int), ("nseismogram_types", C.c_int), ("nsources", C.c_int),
         ("simulation", C.c_int), ("dt", C.c_double), ("t0", C.c_double),
         ("device_bytes", C.c_size_t), ("kernel_launches", C.c_uint64),
+        ("stiffness_variant", C.c_int * 4), ("private_points", C.c_int),
     ]
 
 
@@ -137,6 +138,7 @@ SIGNATURES = {
     "sfb_set_source_time_function": (C.c_int, [_ctx, C.c_int, _P(C.c_float), C.c_size_t]),
     "sfb_get_stream": (C.c_int, [_ctx, _P(C.c_void_p)]),
     "sfb_time_stiffness": (C.c_int, [_ctx, C.c_int, C.c_int, _P(C.c_double)]),
+    "sfb_set_stiffness_variant": (C.c_int, [_ctx, C.c_int, C.c_int]),
     "sfb_assemble_inverse_mass_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p,
                                                     C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                                     C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,

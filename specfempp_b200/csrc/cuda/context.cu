@@ -126,6 +126,14 @@ struct sfb_context {
   } taps[4];
   bool taps_ready = false;
   DBuf<unsigned> done;  // CTA completion counter of the update kernel
+  // batched P-SV forward: points updated inside the stiffness launch are
+  // left out of the update kernel, which walks `shared_points` instead
+  DBuf<int> shared_points;
+  int nshared_points = 0, nprivate_points = 0;
+  // batched stiffness kernel per medium (dev::kShots*), chosen by
+  // autotune_stiffness or set by the caller
+  int shots_variant[4] = {0, 0, 0, 0};
+  bool tuned = false;
   cudaGraphExec_t graph = nullptr;
   int graph_steps = 0;
   uint64_t launches = 0;  // kernels launched so far (graph replays included)
@@ -243,6 +251,38 @@ void ensure_device(sfb_context *c) {
       eflag[d] |= a.bnd[p];
     }
   }
+  // Element-private points of the batched P-SV forward.  An element
+  // qualifies when it has no boundary points and hosts no source or
+  // receiver; its (N-2)^2 interior points then belong to it alone (checked
+  // by counting references) and are updated inside its stiffness launch.
+  if (c->P.nshots > 1 && c->med_count[MEDIUM_ELASTIC_PSV] > 0 && n > 2) {
+    const int m = MEDIUM_ELASTIC_PSV;
+    std::vector<int> refs(a.nglob[m], 0);
+    for (int d = c->med_begin[m]; d < c->med_begin[m] + c->med_count[m]; ++d)
+      for (int k = 0; k < nn; ++k) ++refs[iglob[static_cast<size_t>(d) * nn + k]];
+    std::vector<uint8_t> busy(a.nspec, 0);
+    for (int i : c->P.v_src_ispec) busy[c->inv[i]] = 1;
+    for (const auto &r : c->P.located_receivers) busy[c->inv[r.ispec]] = 1;
+    std::vector<uint8_t> priv(a.nglob[m], 0);
+    for (int d = c->med_begin[m]; d < c->med_begin[m] + c->med_count[m]; ++d) {
+      if (eflag[d] || busy[d]) continue;
+      bool ok = true;
+      for (int iz = 1; iz < n - 1 && ok; ++iz)
+        for (int ix = 1; ix < n - 1; ++ix)
+          if (refs[iglob[static_cast<size_t>(d) * nn + iz * n + ix]] != 1) { ok = false; break; }
+      if (!ok) continue;
+      eflag[d] |= dev::kElemPrivate;
+      for (int iz = 1; iz < n - 1; ++iz)
+        for (int ix = 1; ix < n - 1; ++ix) priv[iglob[static_cast<size_t>(d) * nn + iz * n + ix]] = 1;
+    }
+    std::vector<int> shared;
+    shared.reserve(a.nglob[m]);
+    for (int g = 0; g < a.nglob[m]; ++g)
+      if (!priv[g]) shared.push_back(g);
+    c->nshared_points = static_cast<int>(shared.size());
+    c->nprivate_points = a.nglob[m] - c->nshared_points;
+    if (c->nprivate_points > 0) c->shared_points.upload(shared, &c->device_bytes);
+  }
   // packed per-element static block: iglob, xix, xiz, gammax, gammaz, jac, mat0, mat1
   std::vector<float> pack(nloc * dev::kPackFields);
   for (int d = 0; d < a.nspec; ++d)
@@ -305,6 +345,8 @@ void ensure_device(sfb_context *c) {
   for (int i = 0; i < n; ++i) w[i] = static_cast<float>(a.quad.w[i]);
   dev::set_quadrature(n, hp.data(), w.data());
   ck(cudaGetLastError(), "set_quadrature");
+  dev::init_kernel_attributes();
+  ck(cudaGetLastError(), "kernel attributes");
   // sources (element ids translated to device order)
   const Problem &P = c->P;
   c->nsrc = static_cast<int>(P.v_src_ispec.size());
@@ -351,6 +393,56 @@ void ensure_device(sfb_context *c) {
   c->on_device = true;
 }
 
+// Batched stiffness autotuner: with the freshly allocated (all zero)
+// forward fields, time every applicable kernel variant of each medium (one
+// warm-up and three timed launches, no sources, coupling or store) and keep
+// the fastest.  The launches add zero forces; the force arrays are cleared
+// afterwards all the same.
+void autotune_stiffness(sfb_context *c, WavefieldSet &W) {
+  const Problem &P = c->P;
+  const int S = P.nshots, n = P.asmb.ngll;
+  if (S < 2 || c->tuned) return;
+  c->tuned = true;
+  cudaEvent_t e0, e1;
+  ck(cudaEventCreate(&e0), "event");
+  ck(cudaEventCreate(&e1), "event");
+  const dev::StaceyStore none{};
+  for (int m : kMedia) {
+    if (c->shots_variant[m] != dev::kShotsAuto || W.f[m].nelem == 0) continue;
+    int cand[3], nc = 0;
+    if (S % 2 == 0 && n <= 5) {
+      cand[nc++] = dev::kShotsPacked;
+      cand[nc++] = dev::kShotsPair;
+    }
+    cand[nc++] = dev::kShotsSingle;
+    float best = 0.f;
+    int choice = cand[0];
+    for (int i = 0; i < nc && nc > 1; ++i) {
+      dev::launch_stiffness(m, n, c->st, W.f[m], S, none, &W.ctrl.p->istep, c->stream, nullptr, nullptr, cand[i]);
+      ck(cudaEventRecord(e0, c->stream), "event record");
+      for (int r = 0; r < 3; ++r)
+        dev::launch_stiffness(m, n, c->st, W.f[m], S, none, &W.ctrl.p->istep, c->stream, nullptr, nullptr, cand[i]);
+      ck(cudaEventRecord(e1, c->stream), "event record");
+      ck(cudaEventSynchronize(e1), "event sync");
+      float ms = 0.f;
+      ck(cudaEventElapsedTime(&ms, e0, e1), "elapsed");
+      c->launches += 4;
+      if (i == 0 || ms < best) {
+        best = ms;
+        choice = cand[i];
+      }
+    }
+    c->shots_variant[m] = choice;
+    const dev::MediumFields &f = W.f[m];
+    const size_t ld = static_cast<size_t>(f.nglob + (f.nglob & 1)) * f.nc * S;
+    ck(cudaMemsetAsync(f.a, 0, ld * sizeof(float), c->stream), "clear force");
+  }
+  ck(cudaGetLastError(), "autotune");
+  ck(cudaStreamSynchronize(c->stream), "autotune");
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+}
+
 WavefieldSet &ensure_wavefield(sfb_context *c, int w) {
   ensure_device(c);
   WavefieldSet &W = c->wf[w];
@@ -381,6 +473,7 @@ WavefieldSet &ensure_wavefield(sfb_context *c, int w) {
   W.seis.alloc(std::max<size_t>(nseis, 1), tot);
   W.ctrl.alloc(1, tot);
   W.allocated = true;
+  if (w == SFB_WAVEFIELD_FORWARD) autotune_stiffness(c, W);
   return W;
 }
 
@@ -546,7 +639,8 @@ void build_taps(sfb_context *c) {
   c->taps_ready = true;
 }
 
-dev::UpdateParams update_params(sfb_context *c, WavefieldSet &W, int last, bool advance, bool taps) {
+dev::UpdateParams update_params(sfb_context *c, WavefieldSet &W, int last, bool advance, bool taps,
+                                bool private_done = false) {
   const Problem &P = c->P;
   dev::UpdateParams u{};
   u.nm = 0;
@@ -561,6 +655,10 @@ dev::UpdateParams update_params(sfb_context *c, WavefieldSet &W, int last, bool 
     M.minv = f.minv;
     M.ld2 = static_cast<size_t>(f.nglob + (f.nglob & 1)) * f.nc * P.nshots / 2;
     M.nc = f.nc;
+    if (private_done && m == MEDIUM_ELASTIC_PSV && c->nprivate_points > 0) {
+      M.list = c->shared_points.p;
+      M.ld2 = static_cast<size_t>(c->nshared_points) * P.nshots;  // one float2 pair per (point, shot)
+    }
     if (taps && c->taps[m].nsup > 0) {
       const auto &T = c->taps[m];
       M.taps = {T.nsup, T.mask.p, T.sup_g.p, T.sup_begin.p, T.slot.p, T.which.p, T.w.p};
@@ -584,6 +682,10 @@ dev::UpdateParams update_params(sfb_context *c, WavefieldSet &W, int last, bool 
   u.nsbs = P.nstep_between_samples;
   return u;
 }
+
+// Element-private points are updated inside the batched P-SV stiffness launch
+// of the forward run unless an option needs every point in the update kernel.
+bool private_update_on(sfb_context *c) { return c->nprivate_points > 0; }
 
 // One fused forward step: sources, coupling and stiffness per medium in the
 // reference order, seismograms, then the update kernels.
@@ -609,7 +711,8 @@ void enqueue_fused_step(sfb_context *c, WavefieldSet &W, int last) {
   ta.cp = coupling_acoustic(c);
   ta.other = W.f[dev::MED_PSV];
   ta.cp_mode = ta.cp.n > 0 ? 1 : 0;
-  dev::launch_stiffness(dev::MED_AC, n, c->st, W.f[dev::MED_AC], S, ss, istep, c->stream, &ta);
+  dev::launch_stiffness(dev::MED_AC, n, c->st, W.f[dev::MED_AC], S, ss, istep, c->stream, &ta, nullptr,
+                        c->shots_variant[dev::MED_AC]);
   // elastic: coupling reads the final acoustic acceleration = force * minv
   dev::TailWork te{};
   te.src = src;
@@ -617,15 +720,25 @@ void enqueue_fused_step(sfb_context *c, WavefieldSet &W, int last) {
   te.other = W.f[dev::MED_AC];
   te.cp_mode = te.cp.n > 0 ? 2 : 0;
   te.other_divided = 0;
-  dev::launch_stiffness(dev::MED_PSV, n, c->st, W.f[dev::MED_PSV], S, ss, istep, c->stream, &te);
+  dev::FusedUpdate fu{};
+  const bool fused = private_update_on(c);
+  if (fused) {
+    fu.enabled = 1;
+    fu.minv = c->minv[dev::MED_PSV].p;
+    fu.v = W.f[dev::MED_PSV].v;
+    fu.dt = dt;
+    fu.dt2 = dt2;
+    fu.dtsq2 = dtsq2;
+    fu.last = last;
+  }
+  dev::launch_stiffness(dev::MED_PSV, n, c->st, W.f[dev::MED_PSV], S, ss, istep, c->stream, &te,
+                        fused ? &fu : nullptr, c->shots_variant[dev::MED_PSV]);
   dev::TailWork tsh{};
   tsh.src = src;
-  dev::launch_stiffness(dev::MED_SH, n, c->st, W.f[dev::MED_SH], S, ss, istep, c->stream, &tsh);
+  dev::launch_stiffness(dev::MED_SH, n, c->st, W.f[dev::MED_SH], S, ss, istep, c->stream, &tsh, nullptr,
+                        c->shots_variant[dev::MED_SH]);
   build_taps(c);
-  dev::launch_update_all(update_params(c, W, last, true, true), c->stream);
-  (void)dt;
-  (void)dt2;
-  (void)dtsq2;
+  dev::launch_update_all(update_params(c, W, last, true, true, fused), c->stream);
 }
 
 // Number of kernels one fused step launches (mirrors the skip conditions of
@@ -707,7 +820,8 @@ int update_wavefields(sfb_context *c, int w, int medium, int istep) {
     dev::launch_coupling_elastic(coupling_elastic(c), W.f[dev::MED_PSV], W.f[dev::MED_AC], S, 1, c->stream);
   }
   if (w != SFB_WAVEFIELD_ADJOINT) dev::launch_sources(n, c->st, src, W.f, S, medium, is, 0, c->stream);
-  dev::launch_stiffness(medium, n, c->st, W.f[medium], S, ss, is, c->stream);
+  dev::launch_stiffness(medium, n, c->st, W.f[medium], S, ss, is, c->stream, nullptr, nullptr,
+                        c->shots_variant[medium]);
   dev::launch_divide(W.f[medium], S, c->stream);
   ck(cudaGetLastError(), "update_wavefields");
   return W.f[medium].nelem;
@@ -789,13 +903,22 @@ void enqueue_adjoint_stiffness(sfb_context *c, WavefieldSet &A) {
   ta.cp = coupling_acoustic(c);
   ta.other = A.f[dev::MED_PSV];
   ta.cp_mode = ta.cp.n > 0 ? 1 : 0;
-  dev::launch_stiffness(dev::MED_AC, n, c->st, A.f[dev::MED_AC], S, none, istep, c->stream, &ta);
+  dev::launch_stiffness(dev::MED_AC, n, c->st, A.f[dev::MED_AC], S, none, istep, c->stream, &ta, nullptr,
+                        c->shots_variant[dev::MED_AC]);
   dev::TailWork te{};
   te.src = src;
   te.cp = coupling_elastic(c);
   te.other = A.f[dev::MED_AC];
   te.cp_mode = te.cp.n > 0 ? 2 : 0;
-  dev::launch_stiffness(dev::MED_PSV, n, c->st, A.f[dev::MED_PSV], S, none, istep, c->stream, &te);
+  dev::launch_stiffness(dev::MED_PSV, n, c->st, A.f[dev::MED_PSV], S, none, istep, c->stream, &te, nullptr,
+                        c->shots_variant[dev::MED_PSV]);
+}
+
+// The batched P-SV backward stiffness carries the Frechet kernels of its
+// medium (one launch instead of two, the backward gathers shared).
+bool frechet_fused(sfb_context *c) {
+  return c->med_count[MEDIUM_ELASTIC_PSV] > 0 &&
+         dev::frechet_fusable(dev::MED_PSV, c->P.asmb.ngll, c->P.nshots);
 }
 
 void enqueue_backward_stiffness(sfb_context *c, WavefieldSet &A, WavefieldSet &B) {
@@ -805,20 +928,36 @@ void enqueue_backward_stiffness(sfb_context *c, WavefieldSet &A, WavefieldSet &B
   dev::SourceSet src = source_set(c);
   dev::TailWork te{};
   te.src = src;  // elastic first; acoustic acceleration is zero at this point
-  dev::launch_stiffness(dev::MED_PSV, n, c->st, B.f[dev::MED_PSV], S, ss, istep, c->stream, &te);
+  if (frechet_fused(c)) {
+    dev::FrechetFuse fr{};
+    fr.enabled = 1;
+    fr.au = A.f[dev::MED_PSV].u;
+    fr.aa = A.f[dev::MED_PSV].a;
+    fr.minv = c->minv[dev::MED_PSV].p;
+    fr.kern = c->kern.p;
+    fr.dt = static_cast<float>(c->P.dt);
+    dev::launch_stiffness_frechet(n, c->st, B.f[dev::MED_PSV], S, ss, istep, te, fr, c->stream);
+  } else {
+    dev::launch_stiffness(dev::MED_PSV, n, c->st, B.f[dev::MED_PSV], S, ss, istep, c->stream, &te, nullptr,
+                          c->shots_variant[dev::MED_PSV]);
+  }
   dev::TailWork ta{};
   ta.src = src;
   ta.cp = coupling_acoustic(c);
   ta.other = B.f[dev::MED_PSV];
   ta.cp_mode = ta.cp.n > 0 ? 1 : 0;
-  dev::launch_stiffness(dev::MED_AC, n, c->st, B.f[dev::MED_AC], S, ss, istep, c->stream, &ta);
+  dev::launch_stiffness(dev::MED_AC, n, c->st, B.f[dev::MED_AC], S, ss, istep, c->stream, &ta, nullptr,
+                        c->shots_variant[dev::MED_AC]);
 }
 
-void enqueue_frechet(sfb_context *c, WavefieldSet &A, const dev::MediumFields *bwd_fields, int a_is_force) {
+void enqueue_frechet(sfb_context *c, WavefieldSet &A, const dev::MediumFields *bwd_fields, int a_is_force,
+                     bool psv_done = false) {
   const float dt = static_cast<float>(c->P.dt);
-  for (int m : {dev::MED_PSV, dev::MED_AC})
+  for (int m : {dev::MED_PSV, dev::MED_AC}) {
+    if (m == dev::MED_PSV && psv_done) continue;
     dev::launch_frechet(m, c->P.asmb.ngll, c->st, A.f[m], bwd_fields[m], c->P.nshots, dt, c->kern.p, a_is_force,
                         c->stream);
+  }
 }
 
 dev::UpdateParams update_params_signed(sfb_context *c, WavefieldSet &W, int last, bool advance, bool taps,
@@ -833,7 +972,7 @@ dev::UpdateParams update_params_signed(sfb_context *c, WavefieldSet &W, int last
 void enqueue_combined_step(sfb_context *c, WavefieldSet &A, WavefieldSet &B, int last) {
   enqueue_adjoint_stiffness(c, A);
   enqueue_backward_stiffness(c, A, B);
-  enqueue_frechet(c, A, B.f, 1);
+  enqueue_frechet(c, A, B.f, 1, frechet_fused(c));
   dev::UpdateParams ua = update_params_signed(c, A, last, false, false, 1.0);
   dev::launch_update_all(ua, c->stream);
   // the backward update records the backward seismograms and counts the
@@ -915,7 +1054,7 @@ void run_combined_fused(sfb_context *c, int use_graph) {
       }
     }
   }
-  const int per_step = 7;
+  const int per_step = 7 - (frechet_fused(c) ? 1 : 0);
   const int body = N - 2;  // steps N-2 .. 1 in the body, step 0 closes
   constexpr int K = 25;
   int done = 0;
@@ -996,7 +1135,23 @@ SFB_API int sfb_get_info(const sfb_context *ctx, sfb_info *info) {
   info->t0 = P.t0;
   info->device_bytes = ctx->device_bytes;
   info->kernel_launches = ctx->launches;
+  for (int m = 0; m < 4; ++m) info->stiffness_variant[m] = ctx->shots_variant[m];
+  info->private_points = ctx->nprivate_points;
   return SFB_OK;
+}
+
+SFB_API int sfb_set_stiffness_variant(sfb_context *ctx, int medium, int variant) {
+  if (!ctx) return SFB_E_INVALID;
+  return guarded(ctx, [&]() {
+    if (!medium_index_ok(medium)) throw std::invalid_argument("unsupported medium tag");
+    if (variant < dev::kShotsAuto || variant > dev::kShotsSingle) throw std::invalid_argument("unknown stiffness variant");
+    ctx->shots_variant[medium] = variant;
+    if (ctx->graph) cudaGraphExecDestroy(ctx->graph);  // captured launches use the old kernel
+    ctx->graph = nullptr;
+    if (ctx->graph_combined) cudaGraphExecDestroy(ctx->graph_combined);
+    ctx->graph_combined = nullptr;
+    return SFB_OK;
+  });
 }
 
 SFB_API int sfb_get_problem_view(const sfb_context *ctx, sfb_problem_view *view) {
@@ -1256,7 +1411,8 @@ SFB_API int sfb_time_stiffness(sfb_context *ctx, int medium, int reps, double *m
     ck(cudaEventCreate(&e1), "event");
     ck(cudaEventRecord(e0, ctx->stream), "event record");
     for (int r = 0; r < reps; ++r)
-      dev::launch_stiffness(medium, n, ctx->st, W.f[medium], ctx->P.nshots, ss, &W.ctrl.p->istep, ctx->stream);
+      dev::launch_stiffness(medium, n, ctx->st, W.f[medium], ctx->P.nshots, ss, &W.ctrl.p->istep, ctx->stream,
+                            nullptr, nullptr, ctx->shots_variant[medium]);
     ck(cudaEventRecord(e1, ctx->stream), "event record");
     ck(cudaEventSynchronize(e1), "event sync");
     float ms = 0.f;

@@ -19,6 +19,10 @@ namespace dev {
 __constant__ float c_hp[64];   // hprime[i*N + j] = l_j'(xi_i)
 __constant__ float c_hpw[64];  // hprime_wgll[ix*N + l] = hprime[l*N + ix] * w[l]
 __constant__ float c_w[8];
+// the same tables as (v, v) pairs for the packed two-shot arithmetic
+__constant__ float2 c_hp2[64];
+__constant__ float2 c_hpw2[64];
+__constant__ float2 c_w2[8];
 
 void set_quadrature(int n, const float *hp, const float *w) {
   float hpw[64];
@@ -27,6 +31,15 @@ void set_quadrature(int n, const float *hp, const float *w) {
   cudaMemcpyToSymbol(c_hp, hp, sizeof(float) * n * n);
   cudaMemcpyToSymbol(c_hpw, hpw, sizeof(float) * n * n);
   cudaMemcpyToSymbol(c_w, w, sizeof(float) * n);
+  float2 hp2[64], hpw2[64], w2[8];
+  for (int k = 0; k < n * n; ++k) {
+    hp2[k] = make_float2(hp[k], hp[k]);
+    hpw2[k] = make_float2(hpw[k], hpw[k]);
+  }
+  for (int k = 0; k < n; ++k) w2[k] = make_float2(w[k], w[k]);
+  cudaMemcpyToSymbol(c_hp2, hp2, sizeof(float2) * n * n);
+  cudaMemcpyToSymbol(c_hpw2, hpw2, sizeof(float2) * n * n);
+  cudaMemcpyToSymbol(c_w2, w2, sizeof(float2) * n);
 }
 
 namespace {
@@ -328,7 +341,7 @@ k_stiffness_rp(Static st, MediumFields f, int nshots, StaceyStore ss, const int 
 #pragma unroll
         for (int c = 0; c < NC; ++c) accr[ix][c] = (wz * t1[c] + c_w[ix] * t2[c]) * -1.0f;
       }
-      if (eflag) {
+      if (eflag & 3) {
 #pragma unroll
         for (int ix = 0; ix < N; ++ix) {
           const size_t p = (static_cast<size_t>(e) * N + iz) * N + ix;
@@ -457,7 +470,8 @@ __device__ __forceinline__ void vred(float4 *p, float4 v) { atomicAdd(p, v); }
 
 template <int MED, int N, int SPL, int MINB>
 __global__ void __launch_bounds__(N * 32, MINB)
-k_stiffness_shots(Static st, MediumFields f, int S, StaceyStore ss, const int *istep_dev, TailWork tw) {
+k_stiffness_shots(Static st, MediumFields f, int S, StaceyStore ss, const int *istep_dev, TailWork tw,
+                  FusedUpdate fu) {
   constexpr int NC = (MED == MED_PSV) ? 2 : 1;
   constexpr int NN = N * N;
   constexpr int NV = NC * SPL;
@@ -548,6 +562,7 @@ k_stiffness_shots(Static st, MediumFields f, int S, StaceyStore ss, const int *i
   __syncthreads();
   const uint8_t eflag = st.eflag[e];
   const int slot = (ss.mode != 0) ? ss.slot[e] : -1;
+  const bool fused = fu.enabled && (eflag & kElemPrivate) && iz >= 1 && iz <= N - 2;
 #pragma unroll
   for (int ix = 0; ix < N; ++ix) {
     float t1[NV], t2[NV];
@@ -568,7 +583,7 @@ k_stiffness_shots(Static st, MediumFields f, int S, StaceyStore ss, const int *i
       float acc[2];
 #pragma unroll
       for (int c = 0; c < NC; ++c) acc[c] = (wz * t1[j * NC + c] + c_w[ix] * t2[j * NC + c]) * -1.0f;
-      if (eflag) {
+      if (eflag & 3) {
         const size_t p = (static_cast<size_t>(e) * N + iz) * N + ix;
         const uint8_t b = st.bnd[p];
         if ((b & 1) && act) {
@@ -598,27 +613,369 @@ k_stiffness_shots(Static st, MediumFields f, int S, StaceyStore ss, const int *i
 #pragma unroll
       for (int c = 0; c < NC; ++c) vset(out, j * NC + c, acc[c]);
     }
-    if (act) vred(A + g[ix] * Sv + lofs, out);
+    if (!act) continue;
+    const size_t at = g[ix] * Sv + lofs;
+    if (fused && ix >= 1 && ix <= N - 2) {
+      // element-private point: a = force / M, corrector, next predictor
+      // (the update kernel's arithmetic, newmark.tpp:44-47 and 98-105);
+      // u comes back from the shared staging, not from registers
+      W *Vw = reinterpret_cast<W *>(fu.v);
+      W *Uw = reinterpret_cast<W *>(f.u);
+      W vel = Vw[at], uu = s_u[(iz * N + ix) * 32 + lane], aa;
+#pragma unroll
+      for (int q = 0; q < NV; ++q) {
+        const float a_q = vget(out, q) * fu.minv[g[ix] * NC + (q % NC)];
+        vset(aa, q, a_q);
+        vset(vel, q, vget(vel, q) + fu.dt2 * a_q);
+      }
+      if (fu.last) {
+        A[at] = aa;
+        Vw[at] = vel;
+      } else {
+#pragma unroll
+        for (int q = 0; q < NV; ++q) {
+          vset(uu, q, vget(uu, q) + fu.dt * vget(vel, q) + fu.dtsq2 * vget(aa, q));
+          vset(vel, q, vget(vel, q) + fu.dt2 * vget(aa, q));
+        }
+        Uw[at] = uu;
+        Vw[at] = vel;
+      }
+    } else {
+      vred(A + at, out);
+    }
   }
   tail_work<MED, N>(st, f, S, istep, tw, blockIdx.y * gridDim.x + blockIdx.x, gridDim.x * gridDim.y);
 }
 
+
+// ---------------------------------------------------------------------------
+// Batched stiffness, two shots per lane in packed FP32x2 arithmetic.  Same
+// work and launch shape as k_stiffness_shots<..., SPL = 2>, but every
+// per-point operation is applied to the (shot 0, shot 1) pair of one
+// component with one f32x2 instruction: the lane's float4 / float2 of a
+// point (memory order s0c0 s0c1 s1c0 s1c1) is held in component-major pair
+// order (s0c0 s1c0 s0c1 s1c1), geometry and material are staged in shared
+// memory as (v, v) pairs, and the quadrature tables come as pairs from
+// constant memory.  Each f32x2 lane rounds as one IEEE fma / mul / add.
+//
+// FR (P-SV only): the backward stiffness launch of the combined loop also
+// gathers the adjoint displacement and assembled adjoint force of the same
+// step and adds the step's Frechet kernels, summed over the launch's shots,
+// to the FP64 accumulators (see FrechetFuse).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 pr(const float4 &w, int c) { return c == 0 ? make_float2(w.x, w.y) : make_float2(w.z, w.w); }
+__device__ __forceinline__ float2 pr(const float2 &w, int) { return w; }
+__device__ __forceinline__ void setpr(float4 &w, int c, float2 v) {
+  if (c == 0) { w.x = v.x; w.y = v.y; } else { w.z = v.x; w.w = v.y; }
+}
+__device__ __forceinline__ void setpr(float2 &w, int, float2 v) { w = v; }
+// memory order <-> pair order (an involution)
+__device__ __forceinline__ float4 swz(const float4 &w) { return make_float4(w.x, w.z, w.y, w.w); }
+__device__ __forceinline__ float2 swz(const float2 &w) { return w; }
+
+template <int MED, int N, int MINB, bool FR = false>
+__global__ void __launch_bounds__(N * 32, MINB)
+k_stiffness_pk(Static st, MediumFields f, int S, StaceyStore ss, const int *istep_dev, TailWork tw,
+               FusedUpdate fu, FrechetFuse fr) {
+  constexpr int NC = (MED == MED_PSV) ? 2 : 1;
+  constexpr int NN = N * N;
+  using W = typename VecN<2 * NC>::T;
+  __shared__ W s_u[NN * 32];
+  __shared__ W s_fg[NN * 32];
+  __shared__ float2 s_g[8 * NN];  // xix, xiz, gammax, gammaz, jac, then P-SV (l+2m, l, m) / SH m / acoustic 1/rho
+  // FR: adjoint displacement staging and per-lane kernel values [3][NN][32]
+  extern __shared__ float4 s_dyn[];
+  W *s_ua = reinterpret_cast<W *>(s_dyn);
+  float *s_red = reinterpret_cast<float *>(s_dyn + (FR ? NN * 32 : 0));
+  const int lane = threadIdx.x & 31, iz = threadIdx.x >> 5;
+  const int e = f.elem_begin + blockIdx.x;
+  const int s0 = (blockIdx.y * 32 + lane) * 2;
+  const bool act = s0 < S;
+  const int istep = (ss.mode != 0 || tw.src.n > 0) ? *istep_dev : 0;
+  const float *blk = st.pack + static_cast<size_t>(e) * kPackFields * NN;
+  int g[N];
+#pragma unroll
+  for (int ix = 0; ix < N; ++ix) g[ix] = __float_as_int(__ldg(blk + iz * N + ix));
+  const W *U = reinterpret_cast<const W *>(f.u);
+  W *A = reinterpret_cast<W *>(f.a);
+  const size_t Sv = static_cast<size_t>(S) / 2;
+  const size_t lofs = static_cast<size_t>(s0) / 2;
+  W ur[N];
+#pragma unroll
+  for (int ix = 0; ix < N; ++ix) {
+    if (act) ur[ix] = swz(U[g[ix] * Sv + lofs]);
+    else { for (int c = 0; c < NC; ++c) setpr(ur[ix], c, make_float2(0.f, 0.f)); }
+    s_u[(iz * N + ix) * 32 + lane] = ur[ix];
+  }
+  if constexpr (FR) {
+    const W *UA = reinterpret_cast<const W *>(fr.au);
+#pragma unroll
+    for (int ix = 0; ix < N; ++ix) {
+      W w;
+      if (act) w = swz(UA[g[ix] * Sv + lofs]);
+      else { for (int c = 0; c < NC; ++c) setpr(w, c, make_float2(0.f, 0.f)); }
+      s_ua[(iz * N + ix) * 32 + lane] = w;
+    }
+  }
+  for (int k = threadIdx.x; k < NN; k += blockDim.x) {
+#pragma unroll
+    for (int q = 1; q <= 5; ++q) {
+      const float v = __ldg(blk + q * NN + k);
+      s_g[(q - 1) * NN + k] = make_float2(v, v);
+    }
+    const float m0 = __ldg(blk + 6 * NN + k), m1 = __ldg(blk + 7 * NN + k);
+    if constexpr (MED == MED_PSV) {
+      const float l2m = m0 + static_cast<float>(4.0 / 3.0) * m1;
+      const float lam = l2m - 2.0f * m1;
+      s_g[5 * NN + k] = make_float2(l2m, l2m);
+      s_g[6 * NN + k] = make_float2(lam, lam);
+      s_g[7 * NN + k] = make_float2(m1, m1);
+    } else {
+      s_g[5 * NN + k] = make_float2(m0, m0);  // SH: mu; acoustic: 1/rho
+    }
+  }
+  __syncthreads();
+  float2 hpz[N], hpwz[N];
+#pragma unroll
+  for (int l = 0; l < N; ++l) {
+    hpz[l] = c_hp2[iz * N + l];
+    hpwz[l] = c_hpw2[iz * N + l];
+  }
+  W fx[N];
+#pragma unroll
+  for (int ix = 0; ix < N; ++ix) {
+    const int k = iz * N + ix;
+    float2 dxi[NC], dga[NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) { dxi[c] = make_float2(0.f, 0.f); dga[c] = make_float2(0.f, 0.f); }
+#pragma unroll
+    for (int l = 0; l < N; ++l) {
+      const W col = s_u[(l * N + ix) * 32 + lane];
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        dxi[c] = fma2(c_hp2[ix * N + l], pr(ur[l], c), dxi[c]);
+        dga[c] = fma2(hpz[l], pr(col, c), dga[c]);
+      }
+    }
+    const float2 xix = s_g[0 * NN + k], xiz = s_g[1 * NN + k];
+    const float2 gax = s_g[2 * NN + k], gaz = s_g[3 * NN + k], jac = s_g[4 * NN + k];
+    float2 du[NC][2];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      du[c][0] = fma2(xix, dxi[c], mul2(gax, dga[c]));
+      du[c][1] = fma2(xiz, dxi[c], mul2(gaz, dga[c]));
+    }
+    float2 T[NC][2];
+    if constexpr (MED == MED_PSV) {
+      const float2 l2m = s_g[5 * NN + k], lam = s_g[6 * NN + k], mu = s_g[7 * NN + k];
+      T[0][0] = fma2(l2m, du[0][0], mul2(lam, du[1][1]));
+      T[1][1] = fma2(l2m, du[1][1], mul2(lam, du[0][0]));
+      T[0][1] = mul2(mu, add2(du[0][1], du[1][0]));
+      T[1][0] = T[0][1];
+    } else {
+      const float2 m = s_g[5 * NN + k];
+      T[0][0] = mul2(m, du[0][0]);
+      T[0][1] = mul2(m, du[0][1]);
+    }
+    W f1;
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      setpr(fx[ix], c, mul2(jac, fma2(T[c][0], xix, mul2(T[c][1], xiz))));
+      setpr(f1, c, mul2(jac, fma2(T[c][0], gax, mul2(T[c][1], gaz))));
+    }
+    s_fg[k * 32 + lane] = f1;
+    if constexpr (FR && MED == MED_PSV) {
+      // adjoint displacement gradient at this point (same operators)
+      float2 axi[2] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f)}, aga[2] = {axi[0], axi[1]};
+#pragma unroll
+      for (int l = 0; l < N; ++l) {
+        const W row = s_ua[(iz * N + l) * 32 + lane];
+        const W col = s_ua[(l * N + ix) * 32 + lane];
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+          axi[c] = fma2(c_hp2[ix * N + l], pr(row, c), axi[c]);
+          aga[c] = fma2(hpz[l], pr(col, c), aga[c]);
+        }
+      }
+      float2 da[2][2];
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        da[c][0] = fma2(xix, axi[c], mul2(gax, aga[c]));
+        da[c][1] = fma2(xiz, axi[c], mul2(gaz, aga[c]));
+      }
+      // frechet_derivative.hpp:14-116 per shot, before the material and dt
+      // factors (applied once to the sum over shots):
+      //   kappa ~ div(s_adj) div(s_bwd); mu ~ eps_adj : eps_bwd - div div / 3;
+      //   rho ~ a_adj . u_bwd
+      const float2 half = make_float2(0.5f, 0.5f), two = make_float2(2.0f, 2.0f);
+      const float2 mthird = make_float2(static_cast<float>(-1.0 / 3.0), static_cast<float>(-1.0 / 3.0));
+      const float2 a_xz = mul2(half, add2(da[1][0], da[0][1]));
+      const float2 b_xz = mul2(half, add2(du[1][0], du[0][1]));
+      const float2 kap = mul2(add2(da[0][0], da[1][1]), add2(du[0][0], du[1][1]));
+      float2 mu = fma2(da[0][0], du[0][0], mul2(da[1][1], du[1][1]));
+      mu = fma2(two, mul2(a_xz, b_xz), mu);
+      mu = fma2(mthird, kap, mu);
+      float2 rho = make_float2(0.f, 0.f);
+      if (act) {
+        const W fa = swz(reinterpret_cast<const W *>(fr.aa)[g[ix] * Sv + lofs]);
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+          const float mi = fr.minv[g[ix] * 2 + c];
+          rho = fma2(mul2(pr(fa, c), make_float2(mi, mi)), pr(ur[ix], c), rho);
+        }
+      }
+      s_red[(0 * NN + k) * 32 + lane] = act ? rho.x + rho.y : 0.f;
+      s_red[(1 * NN + k) * 32 + lane] = act ? mu.x + mu.y : 0.f;
+      s_red[(2 * NN + k) * 32 + lane] = act ? kap.x + kap.y : 0.f;
+    }
+  }
+  __syncthreads();
+  if constexpr (FR && MED == MED_PSV) {
+    // sum over this launch's shots (32 lanes), material and dt factors,
+    // FP64 accumulation (compute_material_derivatives.tpp:130-150)
+    for (int q = threadIdx.x; q < 3 * NN; q += blockDim.x) {
+      const float4 *r4 = reinterpret_cast<const float4 *>(s_red + q * 32);
+      float sum = 0.f;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const float4 v = r4[(j + q) & 7];  // rotated start: conflict-free quarter warps
+        sum += (v.x + v.y) + (v.z + v.w);
+      }
+      const int which = q / NN, k = q % NN;
+      const size_t p = static_cast<size_t>(e) * NN + k;
+      const float m0 = __ldg(blk + 6 * NN + k), m1 = __ldg(blk + 7 * NN + k);
+      float scale;
+      if (which == 0) scale = -1.0f * st.mat2[p] * fr.dt;                            // rho
+      else if (which == 1) scale = -2.0f * m1 * fr.dt;                               // mu
+      else scale = -1.0f * (m0 + static_cast<float>(4.0 / 3.0) * m1 - m1) * fr.dt;  // kappa' = lambda + mu
+      fr.kern[p * 3 + which] += static_cast<double>(sum * scale);
+    }
+  }
+  const uint8_t eflag = st.eflag[e];
+  const int slot = (ss.mode != 0) ? ss.slot[e] : -1;
+  const bool fused = fu.enabled && (eflag & kElemPrivate) && iz >= 1 && iz <= N - 2;
+  const float2 wz = c_w2[iz];
+  const float2 neg = make_float2(-1.0f, -1.0f);
+#pragma unroll
+  for (int ix = 0; ix < N; ++ix) {
+    float2 t1[NC], t2[NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) { t1[c] = make_float2(0.f, 0.f); t2[c] = make_float2(0.f, 0.f); }
+#pragma unroll
+    for (int l = 0; l < N; ++l) {
+      const W col = s_fg[(l * N + ix) * 32 + lane];
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        t1[c] = fma2(pr(fx[l], c), c_hpw2[ix * N + l], t1[c]);
+        t2[c] = fma2(pr(col, c), hpwz[l], t2[c]);
+      }
+    }
+    float2 acc[NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) acc[c] = mul2(fma2(wz, t1[c], mul2(c_w2[ix], t2[c])), neg);
+    if ((eflag & 3) || slot >= 0) {
+      // boundary elements: Stacey, free surface and the Stacey store, per shot
+      const size_t p = (static_cast<size_t>(e) * N + iz) * N + ix;
+      const uint8_t b = (eflag & 3) ? st.bnd[p] : 0;
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        float a2[2];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) a2[c] = j == 0 ? acc[c].x : acc[c].y;
+        if ((b & 1) && act) {
+          const float *Vp = f.v + (static_cast<size_t>(g[ix]) * S + s0 + j) * NC;
+          float vel[2];
+#pragma unroll
+          for (int c = 0; c < NC; ++c) vel[c] = Vp[c];
+          stacey<MED>(__ldg(blk + 6 * NN + iz * N + ix), __ldg(blk + 7 * NN + iz * N + ix),
+                      st.mat2 ? st.mat2[p] : 0.f, st.bnd_nx[p], st.bnd_nz[p], st.bnd_w[p], vel, a2);
+        }
+        if (b & 2) {
+#pragma unroll
+          for (int c = 0; c < NC; ++c) a2[c] = 0.f;
+        }
+        if (slot >= 0 && act) {
+          const size_t base =
+              ((((static_cast<size_t>(s0 + j) * ss.nstep + istep) * ss.nstacey + slot) * N + iz) * N + ix) * 2;
+          if (ss.mode == 1) {
+#pragma unroll
+            for (int c = 0; c < NC; ++c) ss.data[base + c] = a2[c];
+          } else {
+#pragma unroll
+            for (int c = 0; c < NC; ++c) a2[c] = ss.data[base + c];
+          }
+        }
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+          if (j == 0) acc[c].x = a2[c]; else acc[c].y = a2[c];
+        }
+      }
+    }
+    if (!act) continue;
+    const size_t at = g[ix] * Sv + lofs;
+    if (fused && ix >= 1 && ix <= N - 2) {
+      // element-private point: a = force / M, corrector, next predictor
+      // (the update kernel's arithmetic, newmark.tpp:44-47 and 98-105)
+      W *Vw = reinterpret_cast<W *>(fu.v);
+      W *Uw = reinterpret_cast<W *>(f.u);
+      W vel = swz(Vw[at]), uu = s_u[(iz * N + ix) * 32 + lane], aa;
+      const float2 dt = make_float2(fu.dt, fu.dt), dt2 = make_float2(fu.dt2, fu.dt2);
+      const float2 dtsq2 = make_float2(fu.dtsq2, fu.dtsq2);
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        const float mi = fu.minv[g[ix] * NC + c];
+        const float2 a_c = mul2(acc[c], make_float2(mi, mi));
+        setpr(aa, c, a_c);
+        setpr(vel, c, fma2(dt2, a_c, pr(vel, c)));
+      }
+      if (fu.last) {
+        A[at] = swz(aa);
+        Vw[at] = swz(vel);
+      } else {
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+          setpr(uu, c, fma2(dtsq2, pr(aa, c), fma2(dt, pr(vel, c), pr(uu, c))));
+          setpr(vel, c, fma2(dt2, pr(aa, c), pr(vel, c)));
+        }
+        Uw[at] = swz(uu);
+        Vw[at] = swz(vel);
+      }
+    } else {
+      W out;
+#pragma unroll
+      for (int c = 0; c < NC; ++c) setpr(out, c, acc[c]);
+      vred(A + at, swz(out));
+    }
+  }
+  tail_work<MED, N>(st, f, S, istep, tw, blockIdx.y * gridDim.x + blockIdx.x, gridDim.x * gridDim.y);
+}
+
+// variant: kShotsPacked (two shots per lane, f32x2), kShotsPair (two shots
+// per lane, scalar), kShotsSingle (one shot per lane); kShotsAuto picks the
+// packed kernel when it applies.  Two shots per lane need an even S and
+// (for the static shared staging) NGLL <= 5.
 template <int MED, int N, int MINB>
 void launch_shots(const Static &st, const MediumFields &f, int S, const StaceyStore &ss, const int *istep_dev,
-                  const TailWork &tw, cudaStream_t stream) {
-  // two shots per lane when the shared staging fits the static limit (NGLL 5)
+                  const TailWork &tw, const FusedUpdate &fu, int variant, cudaStream_t stream) {
   if constexpr (N <= 5) {
-    if (S % 2 == 0) {
+    if (S % 2 == 0 && variant != kShotsSingle) {
       dim3 grid(f.nelem, (S / 2 + 31) / 32);
-      k_stiffness_shots<MED, N, 2, MINB><<<grid, N * 32, 0, stream>>>(st, f, S, ss, istep_dev, tw);
+      if (variant == kShotsPair)
+        k_stiffness_shots<MED, N, 2, MINB><<<grid, N * 32, 0, stream>>>(st, f, S, ss, istep_dev, tw, fu);
+      else
+        k_stiffness_pk<MED, N, MINB><<<grid, N * 32, 0, stream>>>(st, f, S, ss, istep_dev, tw, fu, FrechetFuse{});
       return;
     }
   }
-  {
-    dim3 grid(f.nelem, (S + 31) / 32);
-    k_stiffness_shots<MED, N, 1, MINB><<<grid, N * 32, 0, stream>>>(st, f, S, ss, istep_dev, tw);
-  }
+  dim3 grid(f.nelem, (S + 31) / 32);
+  k_stiffness_shots<MED, N, 1, MINB><<<grid, N * 32, 0, stream>>>(st, f, S, ss, istep_dev, tw, fu);
 }
+
+constexpr size_t kFrechetDynSmem = (25 * 32) * sizeof(float4) + 3 * 25 * 32 * sizeof(float);
+
 
 // ---------------------------------------------------------------------------
 // Point sources (compute_source_interaction.tpp:77-95): one block per source.
@@ -838,10 +1195,13 @@ __global__ void k_update_all(UpdateParams P) {
     // consecutive entries 2jj, 2jj + 1 of [g][s] (nc = 1)
     int g0, s0, g1, s1;
     float2 m;
+    size_t at = jj;  // pair index in the field arrays
     if (M.nc == 2) {
       const uint32_t n = static_cast<uint32_t>(jj);
-      g0 = g1 = static_cast<int>(P.sdiv.div(n));
-      s0 = s1 = static_cast<int>(n - static_cast<uint32_t>(g0) * S);
+      const int k = static_cast<int>(P.sdiv.div(n));
+      s0 = s1 = static_cast<int>(n - static_cast<uint32_t>(k) * S);
+      g0 = g1 = M.list ? M.list[k] : k;
+      if (M.list) at = static_cast<size_t>(g0) * S + s0;
       m = reinterpret_cast<const float2 *>(M.minv)[g0];
     } else {
       const uint32_t n0 = static_cast<uint32_t>(2 * jj), n1 = n0 + 1;
@@ -854,13 +1214,13 @@ __global__ void k_update_all(UpdateParams P) {
     float2 *U = reinterpret_cast<float2 *>(M.u);
     float2 *Vv = reinterpret_cast<float2 *>(M.v);
     float2 *A = reinterpret_cast<float2 *>(M.a);
-    const float2 r = A[jj];
-    float2 acc, vel = Vv[jj];
+    const float2 r = A[at];
+    float2 acc, vel = Vv[at];
     acc.x = r.x * m.x;
     acc.y = r.y * m.y;
     vel.x += P.dt2 * acc.x;  // corrector (newmark.tpp:44-47)
     vel.y += P.dt2 * acc.y;
-    float2 uu = U[jj];
+    float2 uu = U[at];
     if (record && M.taps.nsup > 0) {
       if (M.nc == 2) {
         const float fv[6] = {uu.x, uu.y, vel.x, vel.y, acc.x, acc.y};
@@ -873,16 +1233,16 @@ __global__ void k_update_all(UpdateParams P) {
       }
     }
     if (P.last) {
-      A[jj] = acc;
-      Vv[jj] = vel;
+      A[at] = acc;
+      Vv[at] = vel;
     } else {
       uu.x += P.dt * vel.x + P.dtsq2 * acc.x;  // next predictor (newmark.tpp:98-105)
       uu.y += P.dt * vel.y + P.dtsq2 * acc.y;
       vel.x += P.dt2 * acc.x;
       vel.y += P.dt2 * acc.y;
-      U[jj] = uu;
-      Vv[jj] = vel;
-      A[jj] = make_float2(0.f, 0.f);
+      U[at] = uu;
+      Vv[at] = vel;
+      A[at] = make_float2(0.f, 0.f);
     }
   }
   if (P.ctrl) {
@@ -1039,20 +1399,42 @@ size_t field_ld(const MediumFields &f) { return static_cast<size_t>(f.nglob + (f
 
 }  // namespace
 
+void init_kernel_attributes() {
+  cudaFuncSetAttribute(k_stiffness_pk<MED_PSV, 5, 3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       static_cast<int>(kFrechetDynSmem));
+}
+
+bool frechet_fusable(int medium, int ngll, int nshots) {
+  return medium == MED_PSV && ngll == 5 && nshots > 1 && nshots % 2 == 0;
+}
+
+void launch_stiffness_frechet(int ngll, const Static &st, const MediumFields &f, int S, const StaceyStore &ss,
+                              const int *istep_dev, const TailWork &tw, const FrechetFuse &fr,
+                              cudaStream_t stream) {
+  if (f.nelem == 0 || !frechet_fusable(MED_PSV, ngll, S)) return;
+  dim3 grid(f.nelem, (S / 2 + 31) / 32);
+  k_stiffness_pk<MED_PSV, 5, 3, true><<<grid, 5 * 32, kFrechetDynSmem, stream>>>(st, f, S, ss, istep_dev, tw,
+                                                                                  FusedUpdate{}, fr);
+}
+
 void launch_stiffness(int medium, int ngll, const Static &st, const MediumFields &f, int nshots,
-                      const StaceyStore &ss, const int *istep_dev, cudaStream_t stream, const TailWork *tw) {
+                      const StaceyStore &ss, const int *istep_dev, cudaStream_t stream, const TailWork *tw,
+                      const FusedUpdate *fu, int variant) {
   if (f.nelem == 0) return;
   const TailWork none{};
   const TailWork &w = tw ? *tw : none;
+  const FusedUpdate nofu{};
+  // the in-launch update of private points exists for the batched P-SV kernels
+  const FusedUpdate &u = (fu && nshots > 1 && medium == MED_PSV) ? *fu : nofu;
   if (nshots > 1) {
     if (ngll == 5) {
-      if (medium == MED_PSV) launch_shots<MED_PSV, 5, 4>(st, f, nshots, ss, istep_dev, w, stream);
-      else if (medium == MED_SH) launch_shots<MED_SH, 5, 6>(st, f, nshots, ss, istep_dev, w, stream);
-      else launch_shots<MED_AC, 5, 6>(st, f, nshots, ss, istep_dev, w, stream);
+      if (medium == MED_PSV) launch_shots<MED_PSV, 5, 4>(st, f, nshots, ss, istep_dev, w, u, variant, stream);
+      else if (medium == MED_SH) launch_shots<MED_SH, 5, 5>(st, f, nshots, ss, istep_dev, w, nofu, variant, stream);
+      else launch_shots<MED_AC, 5, 5>(st, f, nshots, ss, istep_dev, w, nofu, variant, stream);
     } else if (ngll == 8) {
-      if (medium == MED_PSV) launch_shots<MED_PSV, 8, 2>(st, f, nshots, ss, istep_dev, w, stream);
-      else if (medium == MED_SH) launch_shots<MED_SH, 8, 3>(st, f, nshots, ss, istep_dev, w, stream);
-      else launch_shots<MED_AC, 8, 3>(st, f, nshots, ss, istep_dev, w, stream);
+      if (medium == MED_PSV) launch_shots<MED_PSV, 8, 2>(st, f, nshots, ss, istep_dev, w, u, variant, stream);
+      else if (medium == MED_SH) launch_shots<MED_SH, 8, 3>(st, f, nshots, ss, istep_dev, w, nofu, variant, stream);
+      else launch_shots<MED_AC, 8, 3>(st, f, nshots, ss, istep_dev, w, nofu, variant, stream);
     }
     return;
   }

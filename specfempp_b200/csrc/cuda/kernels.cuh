@@ -132,6 +132,38 @@ struct UpdateMedium {
   size_t ld2;    // float2 pairs of the whole [g][s][c] array
   int nc;        // components per point (1: a pair holds two entries)
   ReceiverTaps taps;
+  const int *list;  // nc = 2 only: update just these points (the rest were
+                    // updated inside the stiffness launch); null: every point
+};
+
+// Newmark update of element-private points inside the batched stiffness
+// launch.  A GLL point strictly inside an element belongs to that element
+// alone, so once the element's force is known the point's corrector and
+// next predictor can run in registers without the force ever reaching
+// memory.  Elements flagged kElemPrivate in `eflag` (no boundary points,
+// no source, no receiver) qualify; their (N-2)^2 interior points are left
+// out of the update kernel's point list.
+struct FusedUpdate {
+  int enabled;
+  const float *minv;   // [nglob][nc]
+  float *v;            // [g][S][nc]
+  float dt, dt2, dtsq2;
+  int last;            // 1: finish the step (store a and v, no predictor)
+};
+constexpr uint8_t kElemPrivate = 4;
+
+// Frechet kernels fused into the batched P-SV backward stiffness launch of
+// the combined loop: the launch that gathers the backward displacement and
+// forms its gradient also gathers the adjoint displacement and (assembled)
+// adjoint force of the same step and adds this step's rho / mu / kappa
+// kernels, summed over the launch's shots, to kern[p][3] (FP64).
+struct FrechetFuse {
+  int enabled;
+  const float *au;     // adjoint displacement [g][S][2]
+  const float *aa;     // adjoint force [g][S][2] (times minv = acceleration)
+  const float *minv;   // [nglob][2]
+  double *kern;        // [nspec * N * N][3]: rho, mu, kappa
+  float dt;
 };
 
 struct UpdateParams {
@@ -154,9 +186,21 @@ void set_quadrature(int ngll, const float *hprime, const float *wgll);
 
 // `tw` (may be null) is executed in the same launch.  One shot: the
 // TMA-fed row kernel; several shots: the shot-parallel kernel.
+// Kernel variants of the batched (nshots > 1) stiffness; see launch_shots.
+constexpr int kShotsAuto = 0, kShotsPacked = 1, kShotsPair = 2, kShotsSingle = 3;
 void launch_stiffness(int medium, int ngll, const Static &st, const MediumFields &f,
                       int nshots, const StaceyStore &ss, const int *istep_dev,
-                      cudaStream_t stream, const TailWork *tw = nullptr);
+                      cudaStream_t stream, const TailWork *tw = nullptr,
+                      const FusedUpdate *fu = nullptr, int variant = kShotsAuto);
+// True when launch_stiffness_frechet applies (P-SV, even nshots > 1, NGLL 5).
+bool frechet_fusable(int medium, int ngll, int nshots);
+// Backward stiffness of the batched P-SV medium with the Frechet kernels
+// fused in (see FrechetFuse).
+void launch_stiffness_frechet(int ngll, const Static &st, const MediumFields &bwd, int nshots,
+                              const StaceyStore &ss, const int *istep_dev, const TailWork &tw,
+                              const FrechetFuse &fr, cudaStream_t stream);
+// Once per process and device: kernel attributes (dynamic shared memory).
+void init_kernel_attributes();
 
 constexpr int kPackFields = 8;
 void launch_sources(int ngll, const Static &st, const SourceSet &src,

@@ -259,6 +259,11 @@ class Simulation:
     def reset(self):
         self._check(self._lib.sfb_reset(self._h))
 
+    def set_stiffness_variant(self, medium: int, variant: int):
+        """Batched stiffness kernel of `medium` (1 packed two-shot, 2 scalar
+        two-shot, 3 one shot per lane; 0 autotuned)."""
+        self._check(self._lib.sfb_set_stiffness_variant(self._h, medium, variant))
+
     def quadrature_volume(self) -> np.ndarray:
         """w_x w_z J per local point [nspec][ngll][ngll] (FP64)."""
         v = self.problem_view()

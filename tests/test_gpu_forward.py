@@ -86,6 +86,60 @@ def test_batched_shots_match_independent_oracle_runs():
     check(Simulation.structured(p), "batched", shots=range(4))
 
 
+@pytest.mark.parametrize("variant", [1, 2, 3])
+def test_batched_kernel_variants_and_private_update(variant):
+    """Every batched stiffness variant, with the element-private points
+    updated inside the stiffness launch and velocity / acceleration taps."""
+    p = W.batched(scale=0.04, nshots=4, nstep=250,
+                  seismogram_types=("displacement", "velocity", "acceleration"))
+    sim = Simulation.structured(p)
+    sim.set_stiffness_variant(0, variant)
+    check(sim, "batched variant %d" % variant, shots=range(4))
+    info = sim.info()
+    assert info.stiffness_variant[0] == variant
+    assert info.private_points > 0
+
+
+def test_batched_final_fields_and_split_runs():
+    """The private points finish the last step like the update kernel
+    does: final fields match the oracle, and 90 + 160 steps equal 250."""
+    from oracle import bridge
+    p = W.batched(scale=0.04, nshots=2, nstep=250)
+    a = Simulation.structured(p)
+    a.run_forward(250)
+    b = Simulation.structured(p)
+    b.run_forward(90)
+    b.run_forward(160)
+    for s in range(2):
+        assert rel_l2(b.seismograms(shot=s), a.seismograms(shot=s)) <= 1e-6
+        o = bridge.forward(a, 32, shot=s, threads=8, want_fields=True)
+        o64 = bridge.forward(a, 64, shot=s, threads=8, want_fields=True)
+        for which in range(3):
+            g = a.field(0, which, shot=s)
+            e32, e64 = rel_l2(g, o["psv"][which]), rel_l2(g, o64["psv"][which])
+            assert parity_ok(e32, e64, rel_l2(o["psv"][which], o64["psv"][which])), (s, which, e32, e64)
+
+
+@pytest.mark.parametrize("variant", [1, 3])
+def test_batched_sh_and_acoustic(variant):
+    """Packed and one-shot-per-lane batched kernels of the one-component media."""
+    p = small_elastic(sh=True, nstep=250, types=("displacement", "velocity"))
+    p.nshots = 2
+    p.sources = [ForceSource(x=1000.0 + 1000.0 * s, z=1500.0, f0=10.0, factor=1e10, shot=s) for s in range(2)]
+    sim = Simulation.structured(p)
+    sim.set_stiffness_variant(1, variant)
+    check(sim, "SH batched variant %d" % variant, shots=range(2))
+    p = StructuredProblem(nx=20, nz=16, x0=0, x1=1000, z0=0, z1=800,
+                          materials=[Material(1020.0, 1500.0, 0.0)],
+                          absorb=(True, True, False, True), dt=5e-4, nstep=300, nshots=2,
+                          sources=[ForceSource(x=380 + 200 * s, z=410, f0=6.0, factor=1e10, shot=s) for s in range(2)],
+                          stations=[Station(x=100 + 80 * k, z=700) for k in range(10)],
+                          seismogram_types=("pressure", "displacement"))
+    sim = Simulation.structured(p)
+    sim.set_stiffness_variant(3, variant)
+    check(sim, "acoustic batched variant %d" % variant, shots=range(2))
+
+
 def test_unfused_reference_granularity_path():
     from oracle import bridge
     p = small_elastic(nstep=150)
