@@ -144,6 +144,25 @@ SFB_API int sfb_get_info(const sfb_context *ctx, sfb_info *info);
  * reference's chunk size is a compile-time constant). */
 SFB_API int sfb_set_stiffness_variant(sfb_context *ctx, int medium, int variant);
 
+/* Kahan-compensated Newmark sums (enable != 0) in the fused forward driver
+ * (sfb_run_forward): the corrector and predictor additions to v and u carry
+ * their FP32 rounding error forward in two extra device arrays per medium
+ * (8 bytes per DOF and shot).  Compensation starts from zero when enabled;
+ * the reference-granularity entry points and the combined run are not
+ * compensated.  No reference counterpart (the reference sums in plain
+ * type_real, newmark.tpp:44-47, 98-105). */
+SFB_API int sfb_set_newmark_compensation(sfb_context *ctx, int enable);
+
+/* Forward snapshots for the combined run: every `interval` steps the forward
+ * run keeps (u at that step, v half a step later) of every shot in device
+ * memory, and the combined run restores the backward wavefield from them
+ * when it reaches that step, so the reconstructed backward wavefield carries
+ * at most `interval` steps of FP32 reversal error.  0 (default) = pure
+ * reconstruction from the last forward state and the Stacey store, the
+ * reference's scheme (time_marching.tpp:126-247).  Memory: 2 (nstep - 2) /
+ * interval copies of u.  Set before the forward run. */
+SFB_API int sfb_set_checkpoint_interval(sfb_context *ctx, int interval);
+
 /* ---- domain_kernels (include/kokkos_kernels/domain_kernels.hpp) -------- */
 
 /* domain_kernels::initialize(dt) (:136-163): mass matrix (FP64 accumulation,

@@ -67,6 +67,7 @@ struct WavefieldSet {
   bool allocated = false;
   dev::MediumFields f[4];
   DBuf<float> u[4], v[4], a[4];
+  DBuf<float> cu[4], cv[4];  // Kahan compensation of u and v (forward, when enabled)
   DBuf<float> seis;
   DBuf<dev::Control> ctrl;
   bool initialized = false;
@@ -134,6 +135,12 @@ struct sfb_context {
   // autotune_stiffness or set by the caller
   int shots_variant[4] = {0, 0, 0, 0};
   bool tuned = false;
+  bool compensated = false;  // Kahan-compensated Newmark sums in the fused forward
+  // forward snapshots restored into the backward wavefield of the combined
+  // run every ck_interval steps (0: pure reconstruction)
+  int ck_interval = 0, ck_count = 0;
+  DBuf<float> ck_u[4], ck_v[4];
+  size_t ck_stride[4] = {0, 0, 0, 0};
   cudaGraphExec_t graph = nullptr;
   int graph_steps = 0;
   uint64_t launches = 0;  // kernels launched so far (graph replays included)
@@ -640,7 +647,7 @@ void build_taps(sfb_context *c) {
 }
 
 dev::UpdateParams update_params(sfb_context *c, WavefieldSet &W, int last, bool advance, bool taps,
-                                bool private_done = false) {
+                                bool private_done = false, bool snapshots = false) {
   const Problem &P = c->P;
   dev::UpdateParams u{};
   u.nm = 0;
@@ -655,6 +662,13 @@ dev::UpdateParams update_params(sfb_context *c, WavefieldSet &W, int last, bool 
     M.minv = f.minv;
     M.ld2 = static_cast<size_t>(f.nglob + (f.nglob & 1)) * f.nc * P.nshots / 2;
     M.nc = f.nc;
+    M.cu = W.cu[m].p;
+    M.cv = W.cv[m].p;
+    if (snapshots && c->ck_count > 0) {
+      M.ck_u = c->ck_u[m].p;
+      M.ck_v = c->ck_v[m].p;
+      M.ck_stride = c->ck_stride[m];
+    }
     if (private_done && m == MEDIUM_ELASTIC_PSV && c->nprivate_points > 0) {
       M.list = c->shared_points.p;
       M.ld2 = static_cast<size_t>(c->nshared_points) * P.nshots;  // one float2 pair per (point, shot)
@@ -680,12 +694,18 @@ dev::UpdateParams update_params(sfb_context *c, WavefieldSet &W, int last, bool 
   u.slots = static_cast<int>(P.seismogram_types.size() * P.receivers.size() * 2);
   u.max_sig = P.max_sig_step();
   u.nsbs = P.nstep_between_samples;
+  if (snapshots && c->ck_count > 0) {
+    u.ck_interval = c->ck_interval;
+    u.ck_count = c->ck_count;
+  }
   return u;
 }
 
 // Element-private points are updated inside the batched P-SV stiffness launch
 // of the forward run unless an option needs every point in the update kernel.
-bool private_update_on(sfb_context *c) { return c->nprivate_points > 0; }
+bool private_update_on(sfb_context *c) {
+  return c->nprivate_points > 0 && !c->compensated && c->ck_count == 0;
+}
 
 // One fused forward step: sources, coupling and stiffness per medium in the
 // reference order, seismograms, then the update kernels.
@@ -738,7 +758,7 @@ void enqueue_fused_step(sfb_context *c, WavefieldSet &W, int last) {
   dev::launch_stiffness(dev::MED_SH, n, c->st, W.f[dev::MED_SH], S, ss, istep, c->stream, &tsh, nullptr,
                         c->shots_variant[dev::MED_SH]);
   build_taps(c);
-  dev::launch_update_all(update_params(c, W, last, true, true, fused), c->stream);
+  dev::launch_update_all(update_params(c, W, last, true, true, fused, true), c->stream);
 }
 
 // Number of kernels one fused step launches (mirrors the skip conditions of
@@ -755,7 +775,7 @@ void predictor_all(sfb_context *c, WavefieldSet &W, double sgn) {
   const Problem &P = c->P;
   for (int m : kMedia)
     dev::launch_predictor(W.f[m], P.nshots, static_cast<float>(sgn * P.dt), static_cast<float>(sgn * P.dt / 2.0),
-                          static_cast<float>(P.dt * P.dt / 2.0), c->stream);
+                          static_cast<float>(P.dt * P.dt / 2.0), c->stream, W.cu[m].p, W.cv[m].p);
 }
 
 void ensure_store(sfb_context *c) {
@@ -969,7 +989,27 @@ dev::UpdateParams update_params_signed(sfb_context *c, WavefieldSet &W, int last
   return u;
 }
 
+void enqueue_restore(sfb_context *c, WavefieldSet &A, WavefieldSet &B) {
+  if (c->ck_count == 0) return;
+  dev::RestoreParams r{};
+  for (int m : kMedia) {
+    if (!B.u[m].n) continue;
+    r.u[r.nm] = B.u[m].p;
+    r.v[r.nm] = B.v[m].p;
+    r.ck_u[r.nm] = c->ck_u[m].p;
+    r.ck_v[r.nm] = c->ck_v[m].p;
+    r.n[r.nm] = B.u[m].n;
+    r.ck_stride[r.nm] = c->ck_stride[m];
+    ++r.nm;
+  }
+  r.ctrl = A.ctrl.p;
+  r.interval = c->ck_interval;
+  r.count = c->ck_count;
+  dev::launch_restore(r, c->stream);
+}
+
 void enqueue_combined_step(sfb_context *c, WavefieldSet &A, WavefieldSet &B, int last) {
+  enqueue_restore(c, A, B);
   enqueue_adjoint_stiffness(c, A);
   enqueue_backward_stiffness(c, A, B);
   enqueue_frechet(c, A, B.f, 1, frechet_fused(c));
@@ -1054,7 +1094,7 @@ void run_combined_fused(sfb_context *c, int use_graph) {
       }
     }
   }
-  const int per_step = 7 - (frechet_fused(c) ? 1 : 0);
+  const int per_step = 7 + (c->ck_count > 0 ? 1 : 0) - (frechet_fused(c) ? 1 : 0);
   const int body = N - 2;  // steps N-2 .. 1 in the body, step 0 closes
   constexpr int K = 25;
   int done = 0;
@@ -1138,6 +1178,59 @@ SFB_API int sfb_get_info(const sfb_context *ctx, sfb_info *info) {
   for (int m = 0; m < 4; ++m) info->stiffness_variant[m] = ctx->shots_variant[m];
   info->private_points = ctx->nprivate_points;
   return SFB_OK;
+}
+
+SFB_API int sfb_set_newmark_compensation(sfb_context *ctx, int enable) {
+  if (!ctx) return SFB_E_INVALID;
+  return guarded(ctx, [&]() {
+    WavefieldSet &W = ensure_wavefield(ctx, SFB_WAVEFIELD_FORWARD);
+    for (int m : kMedia) {
+      if (enable) {
+        if (!W.cu[m].p && W.u[m].n) {
+          W.cu[m].alloc(W.u[m].n, &ctx->device_bytes);
+          W.cv[m].alloc(W.v[m].n, &ctx->device_bytes);
+        }
+      } else {
+        if (W.cu[m].p) ctx->device_bytes -= 2 * W.cu[m].n * sizeof(float);
+        W.cu[m].free();
+        W.cv[m].free();
+      }
+    }
+    ctx->compensated = enable != 0;
+    if (ctx->graph) cudaGraphExecDestroy(ctx->graph);  // captured launches hold the old pointers
+    ctx->graph = nullptr;
+    return SFB_OK;
+  });
+}
+
+SFB_API int sfb_set_checkpoint_interval(sfb_context *ctx, int interval) {
+  if (!ctx) return SFB_E_INVALID;
+  return guarded(ctx, [&]() {
+    if (interval < 0) throw std::invalid_argument("checkpoint interval must be >= 0");
+    WavefieldSet &F = ensure_wavefield(ctx, SFB_WAVEFIELD_FORWARD);
+    if (F.step != 0) throw StateError("set the checkpoint interval before the forward run");
+    const int N = ctx->P.nstep;
+    const int count = (interval > 0 && N >= 2) ? (N - 2) / interval : 0;
+    for (int m : kMedia) {
+      if (ctx->ck_u[m].p) ctx->device_bytes -= 2 * ctx->ck_u[m].n * sizeof(float);
+      ctx->ck_u[m].free();
+      ctx->ck_v[m].free();
+      ctx->ck_stride[m] = 0;
+      if (count > 0 && F.u[m].n) {
+        const size_t stride = (F.u[m].n + 3) & ~static_cast<size_t>(3);  // 16-byte aligned slots
+        ctx->ck_u[m].alloc(stride * count, &ctx->device_bytes);
+        ctx->ck_v[m].alloc(stride * count, &ctx->device_bytes);
+        ctx->ck_stride[m] = stride;
+      }
+    }
+    ctx->ck_interval = count > 0 ? interval : 0;
+    ctx->ck_count = count;
+    if (ctx->graph) cudaGraphExecDestroy(ctx->graph);
+    ctx->graph = nullptr;
+    if (ctx->graph_combined) cudaGraphExecDestroy(ctx->graph_combined);
+    ctx->graph_combined = nullptr;
+    return SFB_OK;
+  });
 }
 
 SFB_API int sfb_set_stiffness_variant(sfb_context *ctx, int medium, int variant) {
@@ -1609,6 +1702,10 @@ SFB_API int sfb_reset(sfb_context *ctx) {
       WavefieldSet &W = ctx->wf[w];
       if (!W.allocated) continue;
       zero_fields(ctx, W);
+      for (int m : kMedia) {
+        if (W.cu[m].p) ck(cudaMemsetAsync(W.cu[m].p, 0, W.cu[m].n * sizeof(float), ctx->stream), "zero cu");
+        if (W.cv[m].p) ck(cudaMemsetAsync(W.cv[m].p, 0, W.cv[m].n * sizeof(float), ctx->stream), "zero cv");
+      }
       W.step = 0;
     }
     if (ctx->stacey_data.p) ck(cudaMemsetAsync(ctx->stacey_data.p, 0, ctx->stacey_data.n * sizeof(float), ctx->stream), "zero store");

@@ -1132,14 +1132,33 @@ __global__ void k_receivers(Static st, ReceiverSet rec, MediumFields f_psv, Medi
 // [S][ld] floats with ld = (nglob + nglob%2) * nc, a multiple of 4 for P-SV
 // and of 2 otherwise; the float4 / float2 paths below rely on that.
 // ---------------------------------------------------------------------------
+// Kahan-compensated accumulation s += x with running compensation c
+// (Kahan 1965): the low-order bits lost by each FP32 add are carried to the
+// next one.  Explicit round-to-nearest adds keep the compiler from
+// contracting or reassociating the compensation away.
+__device__ __forceinline__ float kahan_add(float s, float &c, float x) {
+  const float y = __fsub_rn(x, c);
+  const float t = __fadd_rn(s, y);
+  c = __fsub_rn(__fsub_rn(t, s), y);
+  return t;
+}
+
 __global__ void k_predictor(float *u, float *v, float *a, size_t n, float dt, float dt2,
-                            float dtsq2) {
+                            float dtsq2, float *cu, float *cv) {
   for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<size_t>(gridDim.x) * blockDim.x) {
     const float ai = a[i];
     const float vi = v[i];
-    u[i] += dt * vi + dtsq2 * ai;
-    v[i] = vi + dt2 * ai;
+    if (cu) {
+      float c_u = cu[i], c_v = cv[i];
+      u[i] = kahan_add(u[i], c_u, dt * vi + dtsq2 * ai);
+      v[i] = kahan_add(vi, c_v, dt2 * ai);
+      cu[i] = c_u;
+      cv[i] = c_v;
+    } else {
+      u[i] += dt * vi + dtsq2 * ai;
+      v[i] = vi + dt2 * ai;
+    }
     a[i] = 0.f;
   }
 }
@@ -1157,6 +1176,30 @@ __global__ void k_divide(float *a, const float *minv, size_t n, int nshots, int 
 }
 
 __global__ void k_advance(Control *ctrl) { ctrl->istep += 1; }
+
+// Snapshot restore at the start of combined step istep: backward u := u at
+// step istep, v := v half a step later, both from the forward run.
+__global__ void k_restore(RestoreParams P) {
+  const int istep = P.ctrl->istep;
+  if (istep <= 0 || istep % P.interval != 0) return;
+  const int slot = istep / P.interval - 1;
+  if (slot >= P.count) return;
+  for (int m = 0; m < P.nm; ++m) {
+    const float *su = P.ck_u[m] + slot * P.ck_stride[m];
+    const float *sv = P.ck_v[m] + slot * P.ck_stride[m];
+    const size_t n4 = P.n[m] / 4;  // slots and fields start 16-byte aligned
+    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n4;
+         i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+      reinterpret_cast<float4 *>(P.u[m])[i] = reinterpret_cast<const float4 *>(su)[i];
+      reinterpret_cast<float4 *>(P.v[m])[i] = reinterpret_cast<const float4 *>(sv)[i];
+    }
+    for (size_t i = n4 * 4 + blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < P.n[m];
+         i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+      P.u[m][i] = su[i];
+      P.v[m][i] = sv[i];
+    }
+  }
+}
 
 // ---------------------------------------------------------------------------
 // Unified update: for every medium and shot, a = force * minv, v += dt/2 a
@@ -1185,6 +1228,14 @@ __global__ void k_update_all(UpdateParams P) {
   const int isig = record ? istep / P.nsbs : 0;
   const size_t total = P.begin[P.nm];
   const int S = P.nshots;
+  // snapshot slots this step writes (forward run with checkpoints)
+  int ck_uslot = -1, ck_vslot = -1;
+  if (P.ck_interval > 0 && istep >= 0 && !P.last) {
+    if ((istep + 1) % P.ck_interval == 0) ck_uslot = (istep + 1) / P.ck_interval - 1;
+    if (istep % P.ck_interval == 0) ck_vslot = istep / P.ck_interval - 1;
+    if (ck_uslot >= P.ck_count) ck_uslot = -1;
+    if (ck_vslot >= P.ck_count) ck_vslot = -1;
+  }
   for (size_t j = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; j < total;
        j += static_cast<size_t>(gridDim.x) * blockDim.x) {
     int mi = 0;
@@ -1218,8 +1269,16 @@ __global__ void k_update_all(UpdateParams P) {
     float2 acc, vel = Vv[at];
     acc.x = r.x * m.x;
     acc.y = r.y * m.y;
-    vel.x += P.dt2 * acc.x;  // corrector (newmark.tpp:44-47)
-    vel.y += P.dt2 * acc.y;
+    float2 cu = make_float2(0.f, 0.f), cv = cu;
+    if (M.cu) {
+      cu = reinterpret_cast<const float2 *>(M.cu)[at];
+      cv = reinterpret_cast<const float2 *>(M.cv)[at];
+      vel.x = kahan_add(vel.x, cv.x, P.dt2 * acc.x);
+      vel.y = kahan_add(vel.y, cv.y, P.dt2 * acc.y);
+    } else {
+      vel.x += P.dt2 * acc.x;  // corrector (newmark.tpp:44-47)
+      vel.y += P.dt2 * acc.y;
+    }
     float2 uu = U[at];
     if (record && M.taps.nsup > 0) {
       if (M.nc == 2) {
@@ -1235,6 +1294,15 @@ __global__ void k_update_all(UpdateParams P) {
     if (P.last) {
       A[at] = acc;
       Vv[at] = vel;
+    } else if (M.cu) {
+      uu.x = kahan_add(uu.x, cu.x, P.dt * vel.x + P.dtsq2 * acc.x);
+      uu.y = kahan_add(uu.y, cu.y, P.dt * vel.y + P.dtsq2 * acc.y);
+      vel.x = kahan_add(vel.x, cv.x, P.dt2 * acc.x);
+      vel.y = kahan_add(vel.y, cv.y, P.dt2 * acc.y);
+      U[at] = uu;
+      Vv[at] = vel;
+      A[at] = make_float2(0.f, 0.f);
+      reinterpret_cast<float2 *>(M.cu)[at] = cu;
     } else {
       uu.x += P.dt * vel.x + P.dtsq2 * acc.x;  // next predictor (newmark.tpp:98-105)
       uu.y += P.dt * vel.y + P.dtsq2 * acc.y;
@@ -1244,6 +1312,9 @@ __global__ void k_update_all(UpdateParams P) {
       Vv[at] = vel;
       A[at] = make_float2(0.f, 0.f);
     }
+    if (M.cu) reinterpret_cast<float2 *>(M.cv)[at] = cv;
+    if (M.ck_u && ck_uslot >= 0) reinterpret_cast<float2 *>(M.ck_u + ck_uslot * M.ck_stride)[at] = uu;
+    if (M.ck_u && ck_vslot >= 0) reinterpret_cast<float2 *>(M.ck_v + ck_vslot * M.ck_stride)[at] = vel;
   }
   if (P.ctrl) {
     __syncthreads();
@@ -1480,10 +1551,10 @@ void launch_receivers(int ngll, const Static &st, const ReceiverSet &rec, const 
 }
 
 void launch_predictor(const MediumFields &f, int nshots, float dt, float dt2, float dtsq2,
-                      cudaStream_t stream) {
+                      cudaStream_t stream, float *cu, float *cv) {
   const size_t n = field_ld(f) * nshots;
   if (n == 0) return;
-  k_predictor<<<grid_for(n, 256), 256, 0, stream>>>(f.u, f.v, f.a, n, dt, dt2, dtsq2);
+  k_predictor<<<grid_for(n, 256), 256, 0, stream>>>(f.u, f.v, f.a, n, dt, dt2, dtsq2, cu, cv);
 }
 void launch_corrector(const MediumFields &f, int nshots, float dt2, cudaStream_t stream) {
   const size_t n = field_ld(f) * nshots;
@@ -1496,6 +1567,17 @@ void launch_divide(const MediumFields &f, int nshots, cudaStream_t stream) {
   k_divide<<<grid_for(n, 256), 256, 0, stream>>>(f.a, f.minv, n, nshots, f.nc);
 }
 void launch_advance_step(Control *ctrl, cudaStream_t stream) { k_advance<<<1, 1, 0, stream>>>(ctrl); }
+
+void launch_restore(const RestoreParams &p, cudaStream_t stream) {
+  if (p.nm == 0 || p.interval <= 0 || p.count <= 0) return;
+  static int nsm = 0;
+  if (nsm == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  }
+  k_restore<<<nsm * 4, 256, 0, stream>>>(p);
+}
 
 void launch_update_all(const UpdateParams &p, cudaStream_t stream) {
   const size_t total = p.begin[p.nm];

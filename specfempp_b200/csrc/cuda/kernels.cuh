@@ -134,6 +134,12 @@ struct UpdateMedium {
   ReceiverTaps taps;
   const int *list;  // nc = 2 only: update just these points (the rest were
                     // updated inside the stiffness launch); null: every point
+  float *cu, *cv;   // Kahan compensation terms of u and v (same layout), or null
+  // forward snapshots for the combined run: slot c (c = 0 .. count-1) holds
+  // u at step (c+1)K (written by step (c+1)K - 1) and v half a step later
+  // (written by step (c+1)K); null when off
+  float *ck_u, *ck_v;
+  size_t ck_stride;  // floats per slot
 };
 
 // Newmark update of element-private points inside the batched stiffness
@@ -179,7 +185,21 @@ struct UpdateParams {
   unsigned *done;         // CTA completion counter (zero between launches)
   float *seis;            // [S][max_sig][slots]
   int slots, max_sig, nsbs;
+  int ck_interval, ck_count;  // snapshot cadence K and slots (0: none)
 };
+
+// Restore the backward wavefield of the combined run from the forward
+// snapshots when the step counter reaches a snapshot step (see UpdateMedium).
+struct RestoreParams {
+  float *u[3], *v[3];
+  const float *ck_u[3], *ck_v[3];
+  size_t n[3];        // floats per medium field ([g][S][nc] incl. padding)
+  size_t ck_stride[3];
+  int nm;
+  const Control *ctrl;
+  int interval, count;
+};
+void launch_restore(const RestoreParams &p, cudaStream_t stream);
 
 // ---- launchers (kernels.cu) ----
 void set_quadrature(int ngll, const float *hprime, const float *wgll);
@@ -218,8 +238,9 @@ void launch_receivers(int ngll, const Static &st, const ReceiverSet &rec,
                       const MediumFields *fields, int nshots, float dt2, int mode,
                       const int *istep_dev, cudaStream_t stream);
 // Newmark pieces (unfused API) and fused update.
+// cu, cv: Kahan compensation terms of u and v, or null for the plain update.
 void launch_predictor(const MediumFields &f, int nshots, float dt, float dt2, float dtsq2,
-                      cudaStream_t stream);
+                      cudaStream_t stream, float *cu = nullptr, float *cv = nullptr);
 void launch_corrector(const MediumFields &f, int nshots, float dt2, cudaStream_t stream);
 void launch_divide(const MediumFields &f, int nshots, cudaStream_t stream);
 void launch_advance_step(Control *ctrl, cudaStream_t stream);

@@ -259,6 +259,15 @@ class Simulation:
     def reset(self):
         self._check(self._lib.sfb_reset(self._h))
 
+    def set_newmark_compensation(self, enable: bool = True):
+        """Kahan-compensated u / v sums in the fused forward run."""
+        self._check(self._lib.sfb_set_newmark_compensation(self._h, 1 if enable else 0))
+
+    def set_checkpoint_interval(self, interval: int):
+        """Forward snapshots every `interval` steps restored into the
+        backward wavefield of the combined run (0: pure reconstruction)."""
+        self._check(self._lib.sfb_set_checkpoint_interval(self._h, interval))
+
     def set_stiffness_variant(self, medium: int, variant: int):
         """Batched stiffness kernel of `medium` (1 packed two-shot, 2 scalar
         two-shot, 3 one shot per lane; 0 autotuned)."""
