@@ -448,6 +448,8 @@ def main():
                     help="skip the batched-forward and batched-vs-single adjoint measurements")
     ap.add_argument("--scale", type=float, default=1.0,
                     help="shrink the workload's element counts (profiling captures); 1 = full size")
+    ap.add_argument("--fwi-only", action="store_true",
+                    help="only the batched-vs-single forward + adjoint comparison, over --steps time steps")
     args = ap.parse_args()
     global SCALE
     SCALE = args.scale
@@ -455,6 +457,11 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
+    if args.fwi_only:
+        import torch
+        torch.cuda.set_device(env_int("LOCAL_RANK", 0))
+        print(json.dumps(dict(fwi_comparison(nstep=args.steps), steps=args.steps)), flush=True)
+        return 0
     return run_ours(args)
 
 

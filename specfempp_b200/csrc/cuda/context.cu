@@ -941,7 +941,11 @@ bool frechet_fused(sfb_context *c) {
          dev::frechet_fusable(dev::MED_PSV, c->P.asmb.ngll, c->P.nshots);
 }
 
-void enqueue_backward_stiffness(sfb_context *c, WavefieldSet &A, WavefieldSet &B) {
+// In the fused backward launch the backward wavefield's element-private
+// points also finish their step (their Frechet contribution is taken first).
+bool backward_private_on(sfb_context *c) { return frechet_fused(c) && c->nprivate_points > 0; }
+
+void enqueue_backward_stiffness(sfb_context *c, WavefieldSet &A, WavefieldSet &B, int last) {
   const int S = c->P.nshots, n = c->P.asmb.ngll;
   const int *istep = &A.ctrl.p->istep;
   dev::StaceyStore ss = replay_store(c);
@@ -956,7 +960,17 @@ void enqueue_backward_stiffness(sfb_context *c, WavefieldSet &A, WavefieldSet &B
     fr.minv = c->minv[dev::MED_PSV].p;
     fr.kern = c->kern.p;
     fr.dt = static_cast<float>(c->P.dt);
-    dev::launch_stiffness_frechet(n, c->st, B.f[dev::MED_PSV], S, ss, istep, te, fr, c->stream);
+    dev::FusedUpdate fu{};
+    if (backward_private_on(c)) {
+      fu.enabled = 1;
+      fu.minv = c->minv[dev::MED_PSV].p;
+      fu.v = B.f[dev::MED_PSV].v;
+      fu.dt = static_cast<float>(-c->P.dt);
+      fu.dt2 = static_cast<float>(-c->P.dt / 2.0);
+      fu.dtsq2 = static_cast<float>(c->P.dt * c->P.dt / 2.0);
+      fu.last = last;
+    }
+    dev::launch_stiffness_frechet(n, c->st, B.f[dev::MED_PSV], S, ss, istep, te, fr, fu, c->stream);
   } else {
     dev::launch_stiffness(dev::MED_PSV, n, c->st, B.f[dev::MED_PSV], S, ss, istep, c->stream, &te, nullptr,
                           c->shots_variant[dev::MED_PSV]);
@@ -981,8 +995,8 @@ void enqueue_frechet(sfb_context *c, WavefieldSet &A, const dev::MediumFields *b
 }
 
 dev::UpdateParams update_params_signed(sfb_context *c, WavefieldSet &W, int last, bool advance, bool taps,
-                                       double sgn) {
-  dev::UpdateParams u = update_params(c, W, last, advance, taps);
+                                       double sgn, bool private_done = false) {
+  dev::UpdateParams u = update_params(c, W, last, advance, taps, private_done);
   u.dt = static_cast<float>(sgn * c->P.dt);
   u.dt2 = static_cast<float>(sgn * c->P.dt / 2.0);
   u.dir = -1;
@@ -1011,13 +1025,13 @@ void enqueue_restore(sfb_context *c, WavefieldSet &A, WavefieldSet &B) {
 void enqueue_combined_step(sfb_context *c, WavefieldSet &A, WavefieldSet &B, int last) {
   enqueue_restore(c, A, B);
   enqueue_adjoint_stiffness(c, A);
-  enqueue_backward_stiffness(c, A, B);
+  enqueue_backward_stiffness(c, A, B, last);
   enqueue_frechet(c, A, B.f, 1, frechet_fused(c));
   dev::UpdateParams ua = update_params_signed(c, A, last, false, false, 1.0);
   dev::launch_update_all(ua, c->stream);
   // the backward update records the backward seismograms and counts the
   // shared step counter (held by the adjoint set) down
-  dev::UpdateParams ub = update_params_signed(c, B, last, false, true, -1.0);
+  dev::UpdateParams ub = update_params_signed(c, B, last, false, true, -1.0, backward_private_on(c));
   ub.ctrl = A.ctrl.p;
   dev::launch_update_all(ub, c->stream);
 }

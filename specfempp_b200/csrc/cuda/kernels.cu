@@ -1481,11 +1481,11 @@ bool frechet_fusable(int medium, int ngll, int nshots) {
 
 void launch_stiffness_frechet(int ngll, const Static &st, const MediumFields &f, int S, const StaceyStore &ss,
                               const int *istep_dev, const TailWork &tw, const FrechetFuse &fr,
-                              cudaStream_t stream) {
+                              const FusedUpdate &fu, cudaStream_t stream) {
   if (f.nelem == 0 || !frechet_fusable(MED_PSV, ngll, S)) return;
   dim3 grid(f.nelem, (S / 2 + 31) / 32);
   k_stiffness_pk<MED_PSV, 5, 3, true><<<grid, 5 * 32, kFrechetDynSmem, stream>>>(st, f, S, ss, istep_dev, tw,
-                                                                                  FusedUpdate{}, fr);
+                                                                                  fu, fr);
 }
 
 void launch_stiffness(int medium, int ngll, const Static &st, const MediumFields &f, int nshots,

@@ -216,9 +216,11 @@ void launch_stiffness(int medium, int ngll, const Static &st, const MediumFields
 bool frechet_fusable(int medium, int ngll, int nshots);
 // Backward stiffness of the batched P-SV medium with the Frechet kernels
 // fused in (see FrechetFuse).
+// fu: element-private points of the backward wavefield finish their (-dt)
+// Newmark step in the launch, after their Frechet contribution is taken.
 void launch_stiffness_frechet(int ngll, const Static &st, const MediumFields &bwd, int nshots,
                               const StaceyStore &ss, const int *istep_dev, const TailWork &tw,
-                              const FrechetFuse &fr, cudaStream_t stream);
+                              const FrechetFuse &fr, const FusedUpdate &fu, cudaStream_t stream);
 // Once per process and device: kernel attributes (dynamic shared memory).
 void init_kernel_attributes();
 
