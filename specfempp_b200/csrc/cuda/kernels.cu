@@ -1208,7 +1208,15 @@ __global__ void k_restore(RestoreParams P) {
 // v += dt/2 a, force = 0 (newmark.tpp:98-105).  The step counter is read at
 // entry by every CTA and advanced by the last CTA to finish.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void apply_taps(const ReceiverTaps &tp, int g, const float fv[3], float *seis_row) {
+// The tapped nodal value: field (0 u, 1 v, 2 a) * 2 + component, picked
+// with selects (no indexed local array).
+__device__ __forceinline__ float pick6(int wh, float a0, float a1, float b0, float b1, float c0, float c1) {
+  const float lo = (wh & 1) ? a1 : a0, mid = (wh & 1) ? b1 : b0, hi = (wh & 1) ? c1 : c0;
+  return wh < 2 ? lo : (wh < 4 ? mid : hi);
+}
+
+__device__ __forceinline__ void apply_taps(const ReceiverTaps &tp, int g, float u0, float u1, float v0, float v1,
+                                           float a0, float a1, float *seis_row) {
   if (!((tp.mask[g >> 5] >> (g & 31)) & 1u)) return;
   int lo = 0, hi = tp.nsup - 1;
   while (lo < hi) {
@@ -1216,12 +1224,13 @@ __device__ __forceinline__ void apply_taps(const ReceiverTaps &tp, int g, const 
     if (tp.sup_g[mid] < g) lo = mid + 1; else hi = mid;
   }
   if (tp.sup_g[lo] != g) return;
-  for (int q = tp.sup_begin[lo]; q < tp.sup_begin[lo + 1]; ++q) {
-    const int wh = tp.which[q];
-    atomicAdd(seis_row + tp.slot[q], tp.w[q] * fv[wh]);
-  }
+  for (int q = tp.sup_begin[lo]; q < tp.sup_begin[lo + 1]; ++q)
+    atomicAdd(seis_row + tp.slot[q], tp.w[q] * pick6(tp.which[q], u0, u1, v0, v1, a0, a1));
 }
 
+// EXTRA: Kahan terms or snapshot writes present (a separate instantiation
+// keeps the plain update free of their registers and branches).
+template <bool EXTRA>
 __global__ void k_update_all(UpdateParams P) {
   const int istep = P.ctrl ? P.ctrl->istep : -1;
   const bool record = P.seis != nullptr && istep >= 0 && (istep % P.nsbs) == 0 && (istep / P.nsbs) < P.max_sig;
@@ -1230,7 +1239,7 @@ __global__ void k_update_all(UpdateParams P) {
   const int S = P.nshots;
   // snapshot slots this step writes (forward run with checkpoints)
   int ck_uslot = -1, ck_vslot = -1;
-  if (P.ck_interval > 0 && istep >= 0 && !P.last) {
+  if (EXTRA && P.ck_interval > 0 && istep >= 0 && !P.last) {
     if ((istep + 1) % P.ck_interval == 0) ck_uslot = (istep + 1) / P.ck_interval - 1;
     if (istep % P.ck_interval == 0) ck_vslot = istep / P.ck_interval - 1;
     if (ck_uslot >= P.ck_count) ck_uslot = -1;
@@ -1270,7 +1279,7 @@ __global__ void k_update_all(UpdateParams P) {
     acc.x = r.x * m.x;
     acc.y = r.y * m.y;
     float2 cu = make_float2(0.f, 0.f), cv = cu;
-    if (M.cu) {
+    if (EXTRA && M.cu) {
       cu = reinterpret_cast<const float2 *>(M.cu)[at];
       cv = reinterpret_cast<const float2 *>(M.cv)[at];
       vel.x = kahan_add(vel.x, cv.x, P.dt2 * acc.x);
@@ -1282,19 +1291,19 @@ __global__ void k_update_all(UpdateParams P) {
     float2 uu = U[at];
     if (record && M.taps.nsup > 0) {
       if (M.nc == 2) {
-        const float fv[6] = {uu.x, uu.y, vel.x, vel.y, acc.x, acc.y};
-        apply_taps(M.taps, g0, fv, P.seis + (static_cast<size_t>(s0) * P.max_sig + isig) * P.slots);
+        apply_taps(M.taps, g0, uu.x, uu.y, vel.x, vel.y, acc.x, acc.y,
+                   P.seis + (static_cast<size_t>(s0) * P.max_sig + isig) * P.slots);
       } else {
-        const float f0[6] = {uu.x, 0.f, vel.x, 0.f, acc.x, 0.f};
-        const float f1[6] = {uu.y, 0.f, vel.y, 0.f, acc.y, 0.f};
-        apply_taps(M.taps, g0, f0, P.seis + (static_cast<size_t>(s0) * P.max_sig + isig) * P.slots);
-        apply_taps(M.taps, g1, f1, P.seis + (static_cast<size_t>(s1) * P.max_sig + isig) * P.slots);
+        apply_taps(M.taps, g0, uu.x, 0.f, vel.x, 0.f, acc.x, 0.f,
+                   P.seis + (static_cast<size_t>(s0) * P.max_sig + isig) * P.slots);
+        apply_taps(M.taps, g1, uu.y, 0.f, vel.y, 0.f, acc.y, 0.f,
+                   P.seis + (static_cast<size_t>(s1) * P.max_sig + isig) * P.slots);
       }
     }
     if (P.last) {
       A[at] = acc;
       Vv[at] = vel;
-    } else if (M.cu) {
+    } else if (EXTRA && M.cu) {
       uu.x = kahan_add(uu.x, cu.x, P.dt * vel.x + P.dtsq2 * acc.x);
       uu.y = kahan_add(uu.y, cu.y, P.dt * vel.y + P.dtsq2 * acc.y);
       vel.x = kahan_add(vel.x, cv.x, P.dt2 * acc.x);
@@ -1312,9 +1321,11 @@ __global__ void k_update_all(UpdateParams P) {
       Vv[at] = vel;
       A[at] = make_float2(0.f, 0.f);
     }
-    if (M.cu) reinterpret_cast<float2 *>(M.cv)[at] = cv;
-    if (M.ck_u && ck_uslot >= 0) reinterpret_cast<float2 *>(M.ck_u + ck_uslot * M.ck_stride)[at] = uu;
-    if (M.ck_u && ck_vslot >= 0) reinterpret_cast<float2 *>(M.ck_v + ck_vslot * M.ck_stride)[at] = vel;
+    if constexpr (EXTRA) {
+      if (M.cu) reinterpret_cast<float2 *>(M.cv)[at] = cv;
+      if (M.ck_u && ck_uslot >= 0) reinterpret_cast<float2 *>(M.ck_u + ck_uslot * M.ck_stride)[at] = uu;
+      if (M.ck_u && ck_vslot >= 0) reinterpret_cast<float2 *>(M.ck_v + ck_vslot * M.ck_stride)[at] = vel;
+    }
   }
   if (P.ctrl) {
     __syncthreads();
@@ -1593,7 +1604,12 @@ void launch_update_all(const UpdateParams &p, cudaStream_t stream) {
   }
   const size_t want = (total + 255) / 256;
   const int grid = static_cast<int>(std::min<size_t>(want, static_cast<size_t>(nsm) * 8));
-  k_update_all<<<std::max(grid, 1), 256, 0, stream>>>(p);
+  bool extra = p.ck_interval > 0;
+  for (int m = 0; m < p.nm; ++m) extra = extra || p.m[m].cu != nullptr || p.m[m].ck_u != nullptr;
+  if (extra)
+    k_update_all<true><<<std::max(grid, 1), 256, 0, stream>>>(p);
+  else
+    k_update_all<false><<<std::max(grid, 1), 256, 0, stream>>>(p);
 }
 
 
