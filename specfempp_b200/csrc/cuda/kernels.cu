@@ -676,6 +676,19 @@ __device__ __forceinline__ void setpr(float2 &w, int, float2 v) { w = v; }
 __device__ __forceinline__ float4 swz(const float4 &w) { return make_float4(w.x, w.z, w.y, w.w); }
 __device__ __forceinline__ float2 swz(const float2 &w) { return w; }
 
+// Per-thread asynchronous global -> shared copies (cp.async, no multicast):
+// each thread later reads back only what it copied itself, after
+// cp.async.wait_all, so no barrier is needed for these.
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void *smem, const void *gmem) {
+  static_assert(BYTES == 8 || BYTES == 16, "cp.async size");
+  if constexpr (BYTES == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_u32(smem)), "l"(gmem) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(smem_u32(smem)), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 template <int MED, int N, int MINB, bool FR = false>
 __global__ void __launch_bounds__(N * 32, MINB)
 k_stiffness_pk(Static st, MediumFields f, int S, StaceyStore ss, const int *istep_dev, TailWork tw,
@@ -686,10 +699,13 @@ k_stiffness_pk(Static st, MediumFields f, int S, StaceyStore ss, const int *iste
   __shared__ W s_u[NN * 32];
   __shared__ W s_fg[NN * 32];
   __shared__ float2 s_g[8 * NN];  // xix, xiz, gammax, gammaz, jac, then P-SV (l+2m, l, m) / SH m / acoustic 1/rho
-  // FR: adjoint displacement staging and per-lane kernel values [3][NN][32]
+  __shared__ W s_vp[(N - 2) * (N - 2) * 32];  // velocity of the private points (prefetched)
+  // FR: adjoint displacement staging, adjoint force (prefetched) and
+  // per-lane kernel values [3][NN][32]
   extern __shared__ float4 s_dyn[];
   W *s_ua = reinterpret_cast<W *>(s_dyn);
-  float *s_red = reinterpret_cast<float *>(s_dyn + (FR ? NN * 32 : 0));
+  W *s_aa = reinterpret_cast<W *>(s_dyn + (FR ? NN * 32 : 0));
+  float *s_red = reinterpret_cast<float *>(s_dyn + (FR ? 2 * NN * 32 : 0));
   const int lane = threadIdx.x & 31, iz = threadIdx.x >> 5;
   const int e = f.elem_begin + blockIdx.x;
   const int s0 = (blockIdx.y * 32 + lane) * 2;
@@ -703,6 +719,22 @@ k_stiffness_pk(Static st, MediumFields f, int S, StaceyStore ss, const int *iste
   W *A = reinterpret_cast<W *>(f.a);
   const size_t Sv = static_cast<size_t>(S) / 2;
   const size_t lofs = static_cast<size_t>(s0) / 2;
+  const uint8_t eflag = st.eflag[e];
+  const bool fused = fu.enabled && (eflag & kElemPrivate) && iz >= 1 && iz <= N - 2;
+  if (fused && act) {
+    // velocity of this row's private points, needed after the divergence
+#pragma unroll
+    for (int ix = 1; ix <= N - 2; ++ix)
+      cp_async<sizeof(W)>(&s_vp[((iz - 1) * (N - 2) + ix - 1) * 32 + lane],
+                          reinterpret_cast<const W *>(fu.v) + g[ix] * Sv + lofs);
+  }
+  if constexpr (FR) {
+    if (act) {
+#pragma unroll
+      for (int ix = 0; ix < N; ++ix)
+        cp_async<sizeof(W)>(&s_aa[(iz * N + ix) * 32 + lane], reinterpret_cast<const W *>(fr.aa) + g[ix] * Sv + lofs);
+    }
+  }
   W ur[N];
 #pragma unroll
   for (int ix = 0; ix < N; ++ix) {
@@ -820,7 +852,8 @@ k_stiffness_pk(Static st, MediumFields f, int S, StaceyStore ss, const int *iste
       mu = fma2(mthird, kap, mu);
       float2 rho = make_float2(0.f, 0.f);
       if (act) {
-        const W fa = swz(reinterpret_cast<const W *>(fr.aa)[g[ix] * Sv + lofs]);
+        if (ix == 0) cp_async_wait_all();
+        const W fa = swz(s_aa[k * 32 + lane]);
 #pragma unroll
         for (int c = 0; c < 2; ++c) {
           const float mi = fr.minv[g[ix] * 2 + c];
@@ -854,9 +887,8 @@ k_stiffness_pk(Static st, MediumFields f, int S, StaceyStore ss, const int *iste
       fr.kern[p * 3 + which] += static_cast<double>(sum * scale);
     }
   }
-  const uint8_t eflag = st.eflag[e];
   const int slot = (ss.mode != 0) ? ss.slot[e] : -1;
-  const bool fused = fu.enabled && (eflag & kElemPrivate) && iz >= 1 && iz <= N - 2;
+  if (fused) cp_async_wait_all();
   const float2 wz = c_w2[iz];
   const float2 neg = make_float2(-1.0f, -1.0f);
 #pragma unroll
@@ -921,7 +953,7 @@ k_stiffness_pk(Static st, MediumFields f, int S, StaceyStore ss, const int *iste
       // (the update kernel's arithmetic, newmark.tpp:44-47 and 98-105)
       W *Vw = reinterpret_cast<W *>(fu.v);
       W *Uw = reinterpret_cast<W *>(f.u);
-      W vel = swz(Vw[at]), uu = s_u[(iz * N + ix) * 32 + lane], aa;
+      W vel = swz(s_vp[((iz - 1) * (N - 2) + ix - 1) * 32 + lane]), uu = s_u[(iz * N + ix) * 32 + lane], aa;
       const float2 dt = make_float2(fu.dt, fu.dt), dt2 = make_float2(fu.dt2, fu.dt2);
       const float2 dtsq2 = make_float2(fu.dtsq2, fu.dtsq2);
 #pragma unroll
@@ -974,7 +1006,7 @@ void launch_shots(const Static &st, const MediumFields &f, int S, const StaceySt
   k_stiffness_shots<MED, N, 1, MINB><<<grid, N * 32, 0, stream>>>(st, f, S, ss, istep_dev, tw, fu);
 }
 
-constexpr size_t kFrechetDynSmem = (25 * 32) * sizeof(float4) + 3 * 25 * 32 * sizeof(float);
+constexpr size_t kFrechetDynSmem = 2 * (25 * 32) * sizeof(float4) + 3 * 25 * 32 * sizeof(float);
 
 
 // ---------------------------------------------------------------------------
@@ -1511,8 +1543,8 @@ void launch_stiffness(int medium, int ngll, const Static &st, const MediumFields
   if (nshots > 1) {
     if (ngll == 5) {
       if (medium == MED_PSV) launch_shots<MED_PSV, 5, 4>(st, f, nshots, ss, istep_dev, w, u, variant, stream);
-      else if (medium == MED_SH) launch_shots<MED_SH, 5, 5>(st, f, nshots, ss, istep_dev, w, nofu, variant, stream);
-      else launch_shots<MED_AC, 5, 5>(st, f, nshots, ss, istep_dev, w, nofu, variant, stream);
+      else if (medium == MED_SH) launch_shots<MED_SH, 5, 4>(st, f, nshots, ss, istep_dev, w, nofu, variant, stream);
+      else launch_shots<MED_AC, 5, 4>(st, f, nshots, ss, istep_dev, w, nofu, variant, stream);
     } else if (ngll == 8) {
       if (medium == MED_PSV) launch_shots<MED_PSV, 8, 2>(st, f, nshots, ss, istep_dev, w, u, variant, stream);
       else if (medium == MED_SH) launch_shots<MED_SH, 8, 3>(st, f, nshots, ss, istep_dev, w, nofu, variant, stream);
