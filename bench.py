@@ -47,6 +47,13 @@ def env_int(name, default):
 
 
 SCALE = 1.0  # element-count scale of the workload (1 = the full configuration)
+VARIANT = 0  # batched stiffness kernel (0: autotuned; see sfb_set_stiffness_variant)
+
+
+def pin_variant(sim):
+    if VARIANT:
+        for medium in (0, 1, 3):
+            sim.set_stiffness_variant(medium, VARIANT)
 
 
 def make_problem(workload: str, nstep: int):
@@ -195,6 +202,7 @@ def batched_forward(steps):
     from specfempp_b200 import Simulation, _capi as A
     p = make_problem("batched", GRAPH_STEPS + 3 + steps + 1)
     with Simulation.structured(p) as sim:
+        pin_variant(sim)
         sim.initialize()
         stream = sim_stream(sim)
         sim.run_forward(GRAPH_STEPS)
@@ -230,6 +238,7 @@ def fwi_comparison(nshots=64, nstep=400, reps=2):
         p = W.adjoint_model(1.0, nshots=S, nstep=nstep)
         p.save_boundary_values = True
         with Simulation.structured(p) as sim:
+            pin_variant(sim)
             info = sim.info()
             rng = np.random.default_rng(3)
             for s in range(S):
@@ -317,6 +326,7 @@ def run_ours(args):
     nstep_total = GRAPH_STEPS + Wm + 2 * K + 2
     p = make_problem(args.workload, nstep_total)
     sim = Simulation.structured(p)
+    pin_variant(sim)
     sim.initialize()
     info = sim.info()
     lib = A.load()
@@ -448,11 +458,15 @@ def main():
                     help="skip the batched-forward and batched-vs-single adjoint measurements")
     ap.add_argument("--scale", type=float, default=1.0,
                     help="shrink the workload's element counts (profiling captures); 1 = full size")
+    ap.add_argument("--stiffness-variant", type=int, default=0, choices=[0, 1, 2, 3],
+                    help="pin the batched stiffness kernel (profiling: the autotuner's timings are "
+                         "distorted under a profiler); 0 = autotuned")
     ap.add_argument("--fwi-only", action="store_true",
                     help="only the batched-vs-single forward + adjoint comparison, over --steps time steps")
     args = ap.parse_args()
-    global SCALE
+    global SCALE, VARIANT
     SCALE = args.scale
+    VARIANT = args.stiffness_variant
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

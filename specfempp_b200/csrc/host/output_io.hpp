@@ -1,0 +1,60 @@
+// Output / checkpoint files in the reference's ASCII layout
+// (include/io/ASCII/impl/*): a "file" is a folder, a group a sub-folder, a
+// dataset <name>.meta ("rank R" / "dims d0 d1 ...") plus <name>.txt (one
+// value per line, 10-digit scientific for floating point).
+#pragma once
+#include <string>
+#include <vector>
+
+#include "problem.hpp"
+
+namespace sfb {
+
+// Create `dir` afresh (an existing folder of that name is removed first, as
+// the reference's writer does) and return it.
+std::string ascii_group(const std::string &dir);
+void ascii_write(const std::string &group, const std::string &name, const std::vector<long> &dims,
+                 const float *data, size_t n);
+void ascii_write(const std::string &group, const std::string &name, const std::vector<long> &dims,
+                 const double *data, size_t n);
+void ascii_write(const std::string &group, const std::string &name, const std::vector<long> &dims, const int *data,
+                 size_t n);
+// Read a dataset, checking its rank and dims against `dims`.
+std::vector<double> ascii_read(const std::string &group, const std::string &name, const std::vector<long> &dims);
+
+// One shot's forward state for the combined run: the fields after the last
+// step (per medium tag, [ncomp][nglob]: u, v, a) and this library's
+// boundary store (whole-element contributions of the Stacey elements per
+// step; slot per reference element in `slot`, -1 where none).
+struct ForwardSnapshot {
+  int step = 0;
+  std::vector<float> field[4][3];
+  std::vector<int> slot;        // [nspec]
+  int nstacey = 0;
+  std::vector<float> store;     // [nstep][nstacey][ngll*ngll][2] (device order)
+};
+
+// <dir>/ForwardWavefield/{Coordinates,StepNNNNNN} as the reference's
+// wavefield writer lays it out (include/io/wavefield/writer.tpp:14-150):
+// Coordinates/<medium>/{X,Z,mapping}; StepNNNNNN/<medium>/{Displacement,
+// Velocity,Acceleration} (acoustic: Potential, PotentialDot,
+// PotentialDotDot), [nglob][ncomp] column-major; StepNNNNNN/Boundary/Stacey/
+// {IndexMapping, ElementAcceleration [nstacey][nz][nx][nstep][2]
+// column-major}.  The reference stores the Stacey traction alone under
+// ElasticAcceleration / AcousticAcceleration; this library replays whole
+// element contributions, so its store has its own dataset name.
+void write_forward_wavefield(const Problem &P, const std::string &dir, const ForwardSnapshot &s);
+ForwardSnapshot read_forward_wavefield(const Problem &P, const std::string &dir, int nstacey);
+
+// <dir>/Kernels/<medium>_isotropic/{X, Z, rho, mu, kappa, rhop, alpha, beta}
+// (acoustic: rho, kappa, rhop, alpha), include/io/kernel/writer.tpp and
+// include/io/impl/medium_writer.tpp:14-70.  Each dataset has dims
+// (nelements, ngllz, ngllx) and the reference's storage order for an element
+// tile of `chunk` elements (domain_view.hpp:100-160; chunk 1 is the
+// reference's CPU build): tile (i / chunk), then i % chunk, iz, ix, element
+// fastest within a tile; the last tile is padded with zeros.  kern[q] holds
+// kernel q (rho, mu, kappa, rhop, alpha, beta) per local point, reference
+// element order.
+void write_kernels(const Problem &P, const std::string &dir, const std::vector<double> kern[6], int chunk);
+
+}  // namespace sfb
