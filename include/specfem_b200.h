@@ -134,6 +134,7 @@ typedef struct sfb_info {
                                3 one shot per lane                           */
   int private_points;    /* P-SV points updated inside the batched stiffness
                             launch of the forward run (0: none)             */
+  int nadjoint_sources;  /* adjoint sources given in the sources file        */
 } sfb_info;
 SFB_API int sfb_get_info(const sfb_context *ctx, sfb_info *info);
 
@@ -240,6 +241,36 @@ SFB_API int sfb_copy_forward_to_backward(const sfb_context *src,
  * (src/io/seismogram/writer.cpp:23-88) into `directory`. */
 SFB_API int sfb_write_seismograms(const sfb_context *ctx, int wavefield,
                                   int shot, const char *directory);
+
+/* ---- wavefield / kernel files and the whole-run driver ----------------- */
+
+/* Write shot `shot`'s forward state after the whole forward run to
+ * <directory>/ForwardWavefield in the reference's ASCII layout
+ * (include/io/wavefield/writer.tpp:14-150): Coordinates/<medium>/{X,Z,mapping}
+ * and Step<nstep>/<medium>/{Displacement,Velocity,Acceleration} (acoustic:
+ * Potential*), plus Step<nstep>/Boundary/Stacey/{IndexMapping,
+ * ElementAcceleration}: this library's boundary store (whole-element
+ * contributions of the Stacey elements for every step; the reference stores
+ * the Stacey traction alone, under other dataset names).  Needs
+ * save_boundary_values when the mesh has Stacey edges. */
+SFB_API int sfb_write_wavefield(const sfb_context *ctx, int shot, const char *directory);
+/* Read such a folder back as the forward run's final state and boundary
+ * store of shot `shot`, so sfb_run_combined can follow (the reference's
+ * wavefield reader, include/io/wavefield/reader.tpp). */
+SFB_API int sfb_read_wavefield(sfb_context *ctx, int shot, const char *directory);
+/* Write the accumulated kernels to <directory>/Kernels/<medium>_isotropic/
+ * {X,Z,rho,mu,kappa,rhop,alpha,beta} (acoustic: rho,kappa,rhop,alpha) as the
+ * reference's kernel writer does (include/io/kernel/writer.tpp,
+ * include/io/impl/medium_writer.tpp), values in the reference's storage
+ * order for an element tile of `element_chunk` elements (1 = its CPU
+ * build). */
+SFB_API int sfb_write_kernels(const sfb_context *ctx, const char *directory, int element_chunk);
+/* Run a parameter file end to end as the reference's specfem2d does
+ * (src/execute.cpp): forward mode runs, writes seismograms and, when asked,
+ * the forward wavefield; combined mode reads the wavefield, runs the
+ * adjoint + backward loop with the file's adjoint sources and writes the
+ * kernels.  Errors: sfb_last_error(NULL). */
+SFB_API int sfb_execute(const char *parameter_file, const char *default_file);
 
 /* Replace the source time function of source `isource` ([nstep][2] samples,
  * the second column only used by two-component media).  The reference's

@@ -90,7 +90,7 @@ def combined(sim, adjoint_stf, fwd, precision: int = 64, shot: int = 0, threads:
     result of ``forward(..., want_fields=True, want_stacey=True)`` (the
     forward run's last state and Stacey store); ``adjoint_stf`` is
     [nstep][nrec][2].  Returns FP64 kernels [nspec, ngll, ngll, 3]
-    (elastic: rho, mu, kappa; acoustic: rho, kappa, 0) and optionally the
+    (elastic: rho, mu, kappa; acoustic: rho, kappa, sum of per-step rho * kappa) and optionally the
     backward seismograms."""
     lib = load()
     view = sim.problem_view()

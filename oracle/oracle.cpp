@@ -465,7 +465,7 @@ template <typename T> struct Sim {
   // ---- Frechet kernels (compute_material_derivatives.tpp:84-153 and
   // medium/dim2/*/isotropic/frechet_derivative.hpp), per local point,
   // accumulated in FP64: k[p*3 + 0..2] = (rho, mu, kappa) for elastic,
-  // (rho, kappa, 0) for acoustic.
+  // (rho, kappa, sum of rho_kl * kappa_kl) for acoustic.
   static void frechet(const Sim &adj, const Sim &bwd, T dt, double *k) {
     const sfb_problem_view &pv = adj.pv;
     const int n = adj.n, nn = n * n;
@@ -515,6 +515,8 @@ template <typename T> struct Sim {
             const T kappa_kl = FA.a[g] * FB.u[g] * T(1) / kap * dt;
             k[p * 3 + 0] += static_cast<double>(rho_kl);
             k[p * 3 + 1] += static_cast<double>(kappa_kl);
+            // rhop = rho_kl * kappa_kl per step (point/kernels.hpp:189-192)
+            k[p * 3 + 2] += static_cast<double>(rho_kl * kappa_kl);
           }
         }
     }

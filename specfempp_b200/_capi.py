@@ -78,7 +78,7 @@ class sfb_info(C.Structure):
         ("nreceivers", C.c_int), ("nseismogram_types", C.c_int), ("nsources", C.c_int),
         ("simulation", C.c_int), ("dt", C.c_double), ("t0", C.c_double),
         ("device_bytes", C.c_size_t), ("kernel_launches", C.c_uint64),
-        ("stiffness_variant", C.c_int * 4), ("private_points", C.c_int),
+        ("stiffness_variant", C.c_int * 4), ("private_points", C.c_int), ("nadjoint_sources", C.c_int),
     ]
 
 
@@ -141,6 +141,10 @@ SIGNATURES = {
     "sfb_set_stiffness_variant": (C.c_int, [_ctx, C.c_int, C.c_int]),
     "sfb_set_newmark_compensation": (C.c_int, [_ctx, C.c_int]),
     "sfb_set_checkpoint_interval": (C.c_int, [_ctx, C.c_int]),
+    "sfb_write_wavefield": (C.c_int, [_ctx, C.c_int, C.c_char_p]),
+    "sfb_read_wavefield": (C.c_int, [_ctx, C.c_int, C.c_char_p]),
+    "sfb_write_kernels": (C.c_int, [_ctx, C.c_char_p, C.c_int]),
+    "sfb_execute": (C.c_int, [C.c_char_p, C.c_char_p]),
     "sfb_assemble_inverse_mass_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p,
                                                     C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                                     C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,

@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "../../../include/specfem_b200.h"
+#include "../host/output_io.hpp"
 #include "../host/problem.hpp"
 #include "kernels.cuh"
 
@@ -110,6 +111,7 @@ struct sfb_context {
   // Stacey replay store
   DBuf<float> stacey_data;  // [S][nstep][nstacey][N*N][2]
   DBuf<int> stacey_slot;
+  std::vector<int> h_stacey_slot;  // host copy, per device element
   int nstacey = 0;
   // adjoint sources: one per (shot, receiver), receiver Lagrange arrays
   DBuf<int> adj_elem, adj_shot, adj_medium;
@@ -396,6 +398,7 @@ void ensure_device(sfb_context *c) {
     for (int d = 0; d < a.nspec; ++d)
       if (eflag[d] & 1) slot[d] = c->nstacey++;
     c->stacey_slot.upload(slot, tot);
+    c->h_stacey_slot = slot;
   }
   c->on_device = true;
 }
@@ -873,7 +876,34 @@ dev::SourceSet adjoint_source_set(sfb_context *c) {
 }
 
 void ensure_adjoint_sources(sfb_context *c) {
-  if (c->nadj > 0 || c->P.receivers.empty()) return;
+  if (c->nadj > 0) return;
+  if (!c->P.located_adjoint.empty()) {
+    // adjoint sources from the sources file, with their own time functions
+    ensure_device(c);
+    const Problem &P = c->P;
+    const int nn = P.asmb.ngll * P.asmb.ngll;
+    c->nadj = static_cast<int>(P.located_adjoint.size());
+    std::vector<int> el(c->nadj), sh(c->nadj, 0), md(c->nadj);
+    std::vector<float> arr(static_cast<size_t>(c->nadj) * 2 * nn, 0.f), stf(static_cast<size_t>(c->nadj) * P.nstep * 2);
+    for (int i = 0; i < c->nadj; ++i) {
+      const LocatedSource &L = P.located_adjoint[i];
+      el[i] = c->inv[L.ispec];
+      md[i] = L.medium;
+      for (int cc = 0; cc < 2; ++cc)
+        for (int k = 0; k < nn; ++k) arr[(static_cast<size_t>(i) * 2 + cc) * nn + k] = L.array[static_cast<size_t>(cc) * nn + k];
+      for (int t = 0; t < P.nstep; ++t)
+        for (int cc = 0; cc < 2; ++cc)
+          stf[(static_cast<size_t>(i) * P.nstep + t) * 2 + cc] = L.stf[static_cast<size_t>(t) * 2 + cc];
+    }
+    size_t *tot = &c->device_bytes;
+    c->adj_elem.upload(el, tot);
+    c->adj_shot.upload(sh, tot);
+    c->adj_medium.upload(md, tot);
+    c->adj_array.upload(arr, tot);
+    c->adj_stf.upload(stf, tot);
+    return;
+  }
+  if (c->P.receivers.empty()) return;
   ensure_device(c);
   const Problem &P = c->P;
   const Assembly &a = P.asmb;
@@ -1191,6 +1221,7 @@ SFB_API int sfb_get_info(const sfb_context *ctx, sfb_info *info) {
   info->kernel_launches = ctx->launches;
   for (int m = 0; m < 4; ++m) info->stiffness_variant[m] = ctx->shots_variant[m];
   info->private_points = ctx->nprivate_points;
+  info->nadjoint_sources = static_cast<int>(P.adjoint_sources.size());
   return SFB_OK;
 }
 
@@ -1481,6 +1512,126 @@ SFB_API int sfb_write_seismograms(const sfb_context *cctx, int wavefield, int sh
   });
 }
 
+SFB_API int sfb_write_wavefield(const sfb_context *cctx, int shot, const char *directory) {
+  sfb_context *ctx = const_cast<sfb_context *>(cctx);
+  if (!ctx || !directory) return SFB_E_INVALID;
+  return guarded(ctx, [&]() {
+    const Problem &P = ctx->P;
+    if (shot < 0 || shot >= P.nshots) throw std::invalid_argument("shot out of range");
+    WavefieldSet &F = ensure_wavefield(ctx, SFB_WAVEFIELD_FORWARD);
+    if (F.step != P.nstep) throw StateError("write the forward wavefield after the whole forward run");
+    ForwardSnapshot snap;
+    snap.step = P.nstep;
+    for (int m : kMedia) {
+      const size_t n = static_cast<size_t>(P.asmb.nglob[m]) * P.asmb.ncomp(m);
+      for (int w = 0; w < 3; ++w) {
+        snap.field[m][w].assign(n, 0.f);
+        if (n) {
+          const int rc = sfb_get_field(ctx, SFB_WAVEFIELD_FORWARD, m, w, shot, snap.field[m][w].data(), n);
+          if (rc) throw std::runtime_error(ctx->err);
+        }
+      }
+    }
+    // boundary store of this shot, slots in reference element order
+    snap.slot.assign(P.asmb.nspec, -1);
+    for (int e = 0; e < P.asmb.nspec; ++e) snap.slot[e] = ctx->h_stacey_slot.empty() ? -1 : ctx->h_stacey_slot[ctx->inv[e]];
+    snap.nstacey = ctx->nstacey;
+    const size_t per = static_cast<size_t>(P.nstep) * ctx->nstacey * P.asmb.ngll * P.asmb.ngll * 2;
+    if (per && ctx->stacey_data.p) {
+      snap.store.resize(per);
+      ck(cudaStreamSynchronize(ctx->stream), "sync");
+      ck(cudaMemcpy(snap.store.data(), ctx->stacey_data.p + static_cast<size_t>(shot) * per, per * sizeof(float),
+                    cudaMemcpyDeviceToHost),
+         "store d2h");
+    } else if (per) {
+      throw StateError("the forward run kept no boundary store (save_boundary_values)");
+    }
+    write_forward_wavefield(P, directory, snap);
+    return SFB_OK;
+  });
+}
+
+SFB_API int sfb_read_wavefield(sfb_context *ctx, int shot, const char *directory) {
+  if (!ctx || !directory) return SFB_E_INVALID;
+  return guarded(ctx, [&]() {
+    const Problem &P = ctx->P;
+    if (shot < 0 || shot >= P.nshots) throw std::invalid_argument("shot out of range");
+    WavefieldSet &F = ensure_wavefield(ctx, SFB_WAVEFIELD_FORWARD);
+    if (!ctx->mass_ready) initialize_mass(ctx, P.dt);
+    ForwardSnapshot snap = read_forward_wavefield(P, directory, ctx->nstacey);
+    for (int e = 0; e < P.asmb.nspec; ++e) {
+      const int want = ctx->h_stacey_slot.empty() ? -1 : ctx->h_stacey_slot[ctx->inv[e]];
+      if (snap.slot[e] != want) throw std::runtime_error("the stored boundary layout does not match this mesh");
+    }
+    for (int m : kMedia) {
+      const size_t n = static_cast<size_t>(P.asmb.nglob[m]) * P.asmb.ncomp(m);
+      if (!n) continue;
+      for (int w = 0; w < 3; ++w) {
+        const int rc = sfb_set_field(ctx, SFB_WAVEFIELD_FORWARD, m, w, shot, snap.field[m][w].data(), n);
+        if (rc) throw std::runtime_error(ctx->err);
+      }
+    }
+    const size_t per = static_cast<size_t>(P.nstep) * ctx->nstacey * P.asmb.ngll * P.asmb.ngll * 2;
+    if (per) {
+      if (!ctx->stacey_data.p) {
+        const size_t total = per * P.nshots;
+        ctx->stacey_data.alloc(total, &ctx->device_bytes);
+      }
+      ck(cudaMemcpy(ctx->stacey_data.p + static_cast<size_t>(shot) * per, snap.store.data(), per * sizeof(float),
+                    cudaMemcpyHostToDevice),
+         "store h2d");
+    }
+    F.step = P.nstep;  // the combined run starts from this state
+    return SFB_OK;
+  });
+}
+
+SFB_API int sfb_write_kernels(const sfb_context *cctx, const char *directory, int element_chunk) {
+  sfb_context *ctx = const_cast<sfb_context *>(cctx);
+  if (!ctx || !directory) return SFB_E_INVALID;
+  return guarded(ctx, [&]() {
+    const size_t nloc = ctx->P.asmb.nloc();
+    std::vector<double> k[6];
+    for (int q = 0; q < 6; ++q) {
+      k[q].assign(nloc, 0.0);
+      const int rc = sfb_get_kernels(ctx, q, k[q].data(), nloc);
+      if (rc) throw std::runtime_error(ctx->err);
+    }
+    write_kernels(ctx->P, directory, k, element_chunk);
+    return SFB_OK;
+  });
+}
+
+// The reference's driver (src/execute.cpp): forward runs write seismograms
+// and, when asked, the forward wavefield; combined runs read that wavefield,
+// run the adjoint + backward loop and write the kernels.
+SFB_API int sfb_execute(const char *parameter_file, const char *default_file) {
+  sfb_context *ctx = nullptr;
+  int rc = sfb_create_from_yaml(parameter_file, default_file, &ctx);
+  if (rc) return rc;
+  std::unique_ptr<sfb_context, void (*)(sfb_context *)> own(ctx, sfb_destroy);
+  // the context goes away on return: its message moves to sfb_last_error(NULL)
+  auto failed = [&](int code) { return fail(nullptr, code, ctx->err); };
+  const Problem &P = ctx->P;
+  if (P.simulation == 0) {
+    if ((rc = sfb_run_forward(ctx, P.nstep, 1))) return failed(rc);
+    if (P.write_seismograms)
+      for (int s = 0; s < P.nshots; ++s)
+        if ((rc = sfb_write_seismograms(ctx, SFB_WAVEFIELD_FORWARD, s, P.seismogram_dir.c_str()))) return failed(rc);
+    if (!P.wavefield_dir.empty())
+      if ((rc = sfb_write_wavefield(ctx, 0, P.wavefield_dir.c_str()))) return failed(rc);
+  } else {
+    if (P.wavefield_dir.empty()) return fail(nullptr, SFB_E_INVALID, "combined run without a wavefield reader directory");
+    if ((rc = sfb_read_wavefield(ctx, 0, P.wavefield_dir.c_str()))) return failed(rc);
+    if ((rc = sfb_run_combined(ctx, P.nstep, 1))) return failed(rc);
+    if (!P.kernel_dir.empty())
+      if ((rc = sfb_write_kernels(ctx, P.kernel_dir.c_str(), 1))) return failed(rc);
+    if (P.write_seismograms)
+      if ((rc = sfb_write_seismograms(ctx, SFB_WAVEFIELD_BACKWARD, 0, P.seismogram_dir.c_str()))) return failed(rc);
+  }
+  return SFB_OK;
+}
+
 SFB_API int sfb_set_source_time_function(sfb_context *ctx, int isource, const float *host, size_t count) {
   if (!ctx || !host) return SFB_E_INVALID;
   return guarded(ctx, [&]() {
@@ -1574,6 +1725,7 @@ SFB_API int sfb_set_adjoint_sources(sfb_context *ctx, int shot, const float *hos
     const int nrec = static_cast<int>(P.receivers.size());
     const size_t n = static_cast<size_t>(P.nstep) * nrec * 2;
     if (count < n) throw std::invalid_argument("adjoint source buffer too small ([nstep][nreceivers][2])");
+    if (!P.located_adjoint.empty()) throw StateError("the adjoint sources come from the sources file");
     ensure_adjoint_sources(ctx);
     // device layout [source = shot * nrec + r][nstep][2]
     std::vector<float> tmp(n);
@@ -1608,7 +1760,9 @@ SFB_API int sfb_get_kernels(const sfb_context *cctx, int which, double *host, si
         const double k0 = k[pd * 3], k1 = k[pd * 3 + 1], k2 = k[pd * 3 + 2];
         double v = 0.0;
         if (a.medium[e] == MEDIUM_ACOUSTIC) {
-          v = which == 0 ? k0 : which == 2 ? k1 : 0.0;  // rho, kappa
+          // rho, kappa; rhop = sum over steps of rho_kl * kappa_kl, alpha =
+          // 2 kappa (point/kernels.hpp:189-192)
+          v = which == 0 ? k0 : which == 2 ? k1 : which == 3 ? k2 : which == 4 ? 2.0 * k1 : 0.0;
         } else {
           // derived kernels (frechet_derivative.hpp:117-135), linear in the
           // primaries at fixed model: kappa' = lambda + 2 mu - mu

@@ -1381,8 +1381,8 @@ __global__ void k_update_all(UpdateParams P) {
 // local point, EPB elements per CTA; gradients of the adjoint and backward
 // displacements through shared memory; the per-step FP32 contributions of
 // all shots are summed in FP64 registers and added once into the per-point
-// FP64 accumulators kern[p][3] = (rho, mu, kappa) elastic, (rho, kappa, 0)
-// acoustic.  The adjoint acceleration is its force times the inverse mass.
+// FP64 accumulators kern[p][3] = (rho, mu, kappa) elastic, (rho, kappa,
+// sum of rho_kl * kappa_kl) acoustic.  The adjoint acceleration is its force times the inverse mass.
 // ---------------------------------------------------------------------------
 template <int MED, int N, int EPB>
 __global__ void __launch_bounds__(EPB * N * N)
@@ -1450,6 +1450,7 @@ k_frechet(Static st, MediumFields A, MediumFields B, int S, float dt, double *ke
         const float kappa_kl = chi_dd * B.u[base] * 1.0f / m1 * dt;
         acc0 += static_cast<double>(rho_kl);
         acc1 += static_cast<double>(kappa_kl);
+        acc2 += static_cast<double>(rho_kl * kappa_kl);  // rhop per step (point/kernels.hpp:189-192)
       }
     }
     __syncthreads();

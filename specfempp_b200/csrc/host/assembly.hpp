@@ -22,7 +22,7 @@ struct CouplingPoint {
 };
 
 struct Source {
-  enum Kind { FORCE = 0, MOMENT_TENSOR = 1, EXTERNAL = 2 };
+  enum Kind { FORCE = 0, MOMENT_TENSOR = 1, EXTERNAL = 2, ADJOINT = 3 };
   enum Stf { RICKER = 0, DIRAC = 1, DGAUSSIAN = 2, TABLE = 3 };
   int kind = FORCE;
   double x = 0, z = 0;
@@ -32,7 +32,9 @@ struct Source {
   double f0 = 0, tshift = 0, factor = 1;
   bool use_trick_for_better_pressure = false;
   std::vector<double> stf_table;       // TABLE: [nstep][ncomp] user samples
+  double table_t0 = 0;                 // TABLE read from files: time of the first sample
   int wavefield = 0;                   // 0 forward/backward, 1 adjoint
+  std::string station, network;        // ADJOINT: the station it stands for
 
   double t0() const;                   // reference rule: -1.2 / f0 + tshift
   double value(double t) const;        // source time function at time t

@@ -1,0 +1,256 @@
+// ASCII output / checkpoint files in the reference's layout; see output_io.hpp.
+#include "output_io.hpp"
+
+#include <cstdio>
+#include <filesystem>
+#include <fstream>
+#include <functional>
+#include <type_traits>
+#include <sstream>
+#include <stdexcept>
+
+namespace fs = std::filesystem;
+
+namespace sfb {
+namespace {
+
+const char *medium_name(int m) {
+  return m == MEDIUM_ELASTIC_PSV ? "elastic_psv" : m == MEDIUM_ELASTIC_SH ? "elastic_sh" : "acoustic";
+}
+constexpr int kMediaTags[3] = {MEDIUM_ELASTIC_PSV, MEDIUM_ELASTIC_SH, MEDIUM_ACOUSTIC};
+
+void write_meta(const std::string &group, const std::string &name, const std::vector<long> &dims) {
+  std::ofstream m(fs::path(group) / (name + ".meta"));
+  if (!m) throw std::runtime_error("could not open " + (fs::path(group) / (name + ".meta")).string());
+  m << "rank " << dims.size() << "\n";
+  m << "dims ";
+  for (long d : dims) m << d << " ";
+  m << "\n";
+}
+
+size_t product(const std::vector<long> &dims) {
+  size_t n = 1;
+  for (long d : dims) n *= static_cast<size_t>(d);
+  return n;
+}
+
+template <typename T> void write_values(const std::string &group, const std::string &name, const T *data, size_t n) {
+  const std::string path = (fs::path(group) / (name + ".txt")).string();
+  FILE *f = std::fopen(path.c_str(), "w");
+  if (!f) throw std::runtime_error("could not open " + path);
+  for (size_t i = 0; i < n; ++i) {
+    if constexpr (std::is_integral_v<T>)
+      std::fprintf(f, "%d\n", static_cast<int>(data[i]));
+    else
+      std::fprintf(f, "%.10e\n", static_cast<double>(data[i]));  // setprecision(10), scientific
+  }
+  std::fclose(f);
+}
+
+template <typename T>
+void write_dataset(const std::string &group, const std::string &name, const std::vector<long> &dims, const T *data,
+                   size_t n) {
+  if (n != product(dims)) throw std::invalid_argument("dataset " + name + ": size does not match its dims");
+  write_meta(group, name, dims);
+  write_values(group, name, data, n);
+}
+
+}  // namespace
+
+std::string ascii_group(const std::string &dir) {
+  std::error_code ec;
+  if (fs::exists(dir)) fs::remove_all(dir, ec);
+  fs::create_directories(dir);
+  return dir;
+}
+
+void ascii_write(const std::string &g, const std::string &n, const std::vector<long> &d, const float *p, size_t k) {
+  write_dataset(g, n, d, p, k);
+}
+void ascii_write(const std::string &g, const std::string &n, const std::vector<long> &d, const double *p, size_t k) {
+  write_dataset(g, n, d, p, k);
+}
+void ascii_write(const std::string &g, const std::string &n, const std::vector<long> &d, const int *p, size_t k) {
+  write_dataset(g, n, d, p, k);
+}
+
+std::vector<double> ascii_read(const std::string &group, const std::string &name, const std::vector<long> &dims) {
+  const fs::path meta = fs::path(group) / (name + ".meta");
+  std::ifstream m(meta);
+  if (!m) throw std::runtime_error("missing dataset metadata " + meta.string());
+  std::string tok;
+  size_t rank = 0;
+  m >> tok >> rank;
+  if (tok != "rank") throw std::runtime_error("corrupted metadata " + meta.string());
+  m >> tok;
+  if (tok != "dims" || rank != dims.size()) throw std::runtime_error("dataset " + meta.string() + ": rank mismatch");
+  for (size_t i = 0; i < rank; ++i) {
+    long d = 0;
+    m >> d;
+    if (d != dims[i]) throw std::runtime_error("dataset " + meta.string() + ": dims mismatch");
+  }
+  const size_t n = product(dims);
+  std::vector<double> out(n);
+  const std::string path = (fs::path(group) / (name + ".txt")).string();
+  FILE *f = std::fopen(path.c_str(), "r");
+  if (!f) throw std::runtime_error("could not open " + path);
+  for (size_t i = 0; i < n; ++i)
+    if (std::fscanf(f, "%lf", &out[i]) != 1) {
+      std::fclose(f);
+      throw std::runtime_error("dataset " + path + " has fewer values than its dims");
+    }
+  std::fclose(f);
+  return out;
+}
+
+namespace {
+
+// Elements of medium m in reference (ispec) order, and each global point's
+// coordinates.
+std::vector<int> medium_elements(const Assembly &a, int m) {
+  std::vector<int> el;
+  for (int e = 0; e < a.nspec; ++e)
+    if (a.medium[e] == m) el.push_back(e);
+  return el;
+}
+
+std::string step_group(int step) {
+  char buf[32];
+  std::snprintf(buf, sizeof(buf), "Step%06d", step);  // utilities::to_zero_lead(istep, 6)
+  return buf;
+}
+
+const char *field_name(int m, int which) {
+  static const char *el[3] = {"Displacement", "Velocity", "Acceleration"};
+  static const char *ac[3] = {"Potential", "PotentialDot", "PotentialDotDot"};
+  return m == MEDIUM_ACOUSTIC ? ac[which] : el[which];
+}
+
+}  // namespace
+
+void write_forward_wavefield(const Problem &P, const std::string &dir, const ForwardSnapshot &s) {
+  const Assembly &a = P.asmb;
+  const int n = a.ngll, nn = n * n;
+  const std::string root = ascii_group((fs::path(dir) / "ForwardWavefield").string());
+  const std::string coords = ascii_group((fs::path(root) / "Coordinates").string());
+  for (int m : kMediaTags) {
+    const std::string g = ascii_group((fs::path(coords) / medium_name(m)).string());
+    const std::vector<int> el = medium_elements(a, m);
+    const long ne = static_cast<long>(el.size()), ng = a.nglob[m];
+    std::vector<float> x(ng, 0.f), z(ng, 0.f);
+    std::vector<int> mapping(static_cast<size_t>(ne) * nn);
+    for (long i = 0; i < ne; ++i)
+      for (int iz = 0; iz < n; ++iz)
+        for (int ix = 0; ix < n; ++ix) {
+          const size_t p = static_cast<size_t>(el[i]) * nn + iz * n + ix;
+          const int ig = a.iglob[p];
+          mapping[i + ne * (iz + static_cast<size_t>(n) * ix)] = ig;  // (nelem, nz, nx), column-major
+          x[ig] = static_cast<float>(a.coord[p * 2]);
+          z[ig] = static_cast<float>(a.coord[p * 2 + 1]);
+        }
+    ascii_write(g, "X", {ng}, x.data(), x.size());
+    ascii_write(g, "Z", {ng}, z.data(), z.size());
+    ascii_write(g, "mapping", {ne, n, n}, mapping.data(), mapping.size());
+  }
+  const std::string step = ascii_group((fs::path(root) / step_group(s.step)).string());
+  for (int m : kMediaTags) {
+    const std::string g = ascii_group((fs::path(step) / medium_name(m)).string());
+    const long ng = a.nglob[m], nc = a.ncomp(m);
+    for (int w = 0; w < 3; ++w) {
+      const std::vector<float> &f = s.field[m][w];
+      if (f.size() != static_cast<size_t>(ng * nc)) throw std::invalid_argument("snapshot field has the wrong size");
+      ascii_write(g, field_name(m, w), {ng, nc}, f.data(), f.size());  // [c][g] = (nglob, ncomp) column-major
+    }
+  }
+  const std::string stacey =
+      ascii_group((fs::path(ascii_group((fs::path(step) / "Boundary").string())) / "Stacey").string());
+  ascii_write(stacey, "IndexMapping", {static_cast<long>(a.nspec)}, s.slot.data(), s.slot.size());
+  const long T = P.nstep, K = s.nstacey;
+  std::vector<float> v(static_cast<size_t>(K) * nn * T * 2);
+  if (!s.store.empty()) {
+    if (s.store.size() != v.size()) throw std::invalid_argument("snapshot store has the wrong size");
+    for (long t = 0; t < T; ++t)
+      for (long k = 0; k < K; ++k)
+        for (int iz = 0; iz < n; ++iz)
+          for (int ix = 0; ix < n; ++ix)
+            for (int c = 0; c < 2; ++c)
+              v[k + K * (iz + n * (ix + static_cast<size_t>(n) * (t + T * c)))] =
+                  s.store[(((static_cast<size_t>(t) * K + k) * nn) + iz * n + ix) * 2 + c];
+  }
+  ascii_write(stacey, "ElementAcceleration", {K, n, n, T, 2}, v.data(), v.size());
+}
+
+ForwardSnapshot read_forward_wavefield(const Problem &P, const std::string &dir, int nstacey) {
+  const Assembly &a = P.asmb;
+  const int n = a.ngll, nn = n * n;
+  ForwardSnapshot s;
+  s.step = P.nstep;
+  s.nstacey = nstacey;
+  const fs::path step = fs::path(dir) / "ForwardWavefield" / step_group(P.nstep);
+  if (!fs::exists(step)) throw std::runtime_error("no forward wavefield at " + step.string());
+  for (int m : kMediaTags) {
+    const std::string g = (step / medium_name(m)).string();
+    const long ng = a.nglob[m], nc = a.ncomp(m);
+    for (int w = 0; w < 3; ++w) {
+      const std::vector<double> d = ascii_read(g, field_name(m, w), {ng, nc});
+      s.field[m][w].assign(d.begin(), d.end());
+    }
+  }
+  const std::string stacey = (step / "Boundary" / "Stacey").string();
+  const std::vector<double> map = ascii_read(stacey, "IndexMapping", {static_cast<long>(a.nspec)});
+  s.slot.assign(map.begin(), map.end());
+  const long T = P.nstep, K = nstacey;
+  const std::vector<double> v = ascii_read(stacey, "ElementAcceleration", {K, n, n, T, 2});
+  s.store.assign(static_cast<size_t>(T) * K * nn * 2, 0.f);
+  for (long t = 0; t < T; ++t)
+    for (long k = 0; k < K; ++k)
+      for (int iz = 0; iz < n; ++iz)
+        for (int ix = 0; ix < n; ++ix)
+          for (int c = 0; c < 2; ++c)
+            s.store[(((static_cast<size_t>(t) * K + k) * nn) + iz * n + ix) * 2 + c] =
+                static_cast<float>(v[k + K * (iz + n * (ix + static_cast<size_t>(n) * (t + T * c)))]);
+  return s;
+}
+
+void write_kernels(const Problem &P, const std::string &dir, const std::vector<double> kern[6], int chunk) {
+  const Assembly &a = P.asmb;
+  const int n = a.ngll, nn = n * n;
+  if (chunk < 1) throw std::invalid_argument("element chunk must be >= 1");
+  const std::string root = ascii_group((fs::path(dir) / "Kernels").string());
+  for (int m : kMediaTags) {
+    const std::string g = ascii_group((fs::path(root) / (std::string(medium_name(m)) + "_isotropic")).string());
+    const std::vector<int> el = medium_elements(a, m);
+    const long ne = static_cast<long>(el.size());
+    const long ntiles = (ne + chunk - 1) / chunk;
+    const size_t span = static_cast<size_t>(ntiles) * chunk * nn;
+    // domain_view.hpp:100-160: tile (i / chunk), then (i % chunk) + iz chunk + ix chunk nz
+    auto place = [&](const std::function<double(size_t)> &value, std::vector<double> &out) {
+      out.assign(span, 0.0);
+      for (long i = 0; i < ne; ++i)
+        for (int iz = 0; iz < n; ++iz)
+          for (int ix = 0; ix < n; ++ix) {
+            const size_t at = static_cast<size_t>(i / chunk) * chunk * nn + (i % chunk) +
+                              static_cast<size_t>(iz) * chunk + static_cast<size_t>(ix) * chunk * n;
+            out[at] = value(static_cast<size_t>(el[i]) * nn + iz * n + ix);
+          }
+    };
+    std::vector<double> buf;
+    std::vector<float> fbuf;
+    auto write_float = [&](const char *name, const std::function<double(size_t)> &value) {
+      place(value, buf);
+      fbuf.assign(buf.begin(), buf.end());
+      // the .meta carries the logical dims; the values are the padded tiles
+      write_meta(g, name, {ne, n, n});
+      write_values(g, name, fbuf.data(), fbuf.size());
+    };
+    write_float("X", [&](size_t p) { return a.coord[p * 2]; });
+    write_float("Z", [&](size_t p) { return a.coord[p * 2 + 1]; });
+    const std::vector<std::pair<const char *, int>> names =
+        m == MEDIUM_ACOUSTIC ? std::vector<std::pair<const char *, int>>{{"rho", 0}, {"kappa", 2}, {"rhop", 3}, {"alpha", 4}}
+                             : std::vector<std::pair<const char *, int>>{{"rho", 0}, {"mu", 1}, {"kappa", 2},
+                                                                         {"rhop", 3}, {"alpha", 4}, {"beta", 5}};
+    for (const auto &[name, q] : names) write_float(name, [&](size_t p) { return kern[q][p]; });
+  }
+}
+
+}  // namespace sfb

@@ -1,5 +1,7 @@
 #include "problem.hpp"
 
+#include <cctype>
+#include <cmath>
 #include <fstream>
 #include <stdexcept>
 #include <sys/stat.h>
@@ -49,7 +51,50 @@ int seismogram_type_of(const std::string &s) {
 
 // One entry of a sources file (reference: src/io/sources.cpp:54-90,
 // src/source/source.cpp, force_source.cpp, moment_tensor_source.cpp).
-Source parse_source(const YNode &entry, double dt) {
+// External source time function (src/source_time_function/external.cpp):
+// two-column "time value" ASCII files for the X and Z components; t0 is the
+// first file time, dt the spacing of the first two lines (checked against
+// the simulation's dt), then one sample per step.
+void read_external_stf(const YNode &ext, int nstep, double dt, const std::string &config, Source &s) {
+  if (const YNode *f = ext.get("format")) {
+    std::string fmt = f->str();
+    for (auto &ch : fmt) ch = static_cast<char>(std::tolower(ch));
+    if (fmt != "ascii") throw std::runtime_error("Only ASCII format is supported");
+  }
+  const YNode *stf = ext.get("stf");
+  if (!stf) throw std::runtime_error("Error: External source time function requires at least one component");
+  std::string files[2];
+  if (const YNode *x = stf->get("X-component")) files[0] = x->str();
+  if (const YNode *z = stf->get("Z-component")) files[1] = z->str();
+  if (files[0].empty() && files[1].empty()) {
+    if (stf->get("Y-component")) throw std::runtime_error("External source time function only supports 2 components");
+    throw std::runtime_error("Error: External source time function requires at least one component");
+  }
+  s.stf = Source::TABLE;
+  s.stf_table.assign(static_cast<size_t>(nstep) * 2, 0.0);
+  bool first = true;
+  for (int c = 0; c < 2; ++c) {
+    if (files[c].empty()) continue;
+    const std::string path = resolve(files[c], config);
+    std::ifstream in(path);
+    if (!in) throw std::runtime_error("Error: External source time function file " + path + " does not exist");
+    std::vector<std::pair<double, double>> rows;
+    double t, v;
+    while (in >> t >> v) rows.emplace_back(t, v);
+    if (rows.size() < 2) throw std::runtime_error("Seismogram file " + path + " is not formatted correctly");
+    if (first) {
+      s.table_t0 = rows[0].first;
+      if (std::abs((rows[1].first - rows[0].first) - dt) > 1e-6)
+        throw std::runtime_error("The time step of the external source time function does not match the simulation time step");
+      first = false;
+    }
+    if (rows.size() < static_cast<size_t>(nstep))
+      throw std::runtime_error("External source time function file " + path + " has fewer samples than nstep");
+    for (int i = 0; i < nstep; ++i) s.stf_table[static_cast<size_t>(i) * 2 + c] = rows[i].second;
+  }
+}
+
+Source parse_source(const YNode &entry, double dt, int nstep, const std::string &config) {
   Source s;
   const YNode *body = nullptr;
   if ((body = entry.get("force"))) {
@@ -60,11 +105,24 @@ Source parse_source(const YNode &entry, double dt) {
     s.mxx = body->get("Mxx")->num();
     s.mzz = body->get("Mzz")->num();
     s.mxz = body->get("Mxz")->num();
+  } else if ((body = entry.get("adjoint-source"))) {
+    // src/io/sources.cpp:92-99, src/source/adjoint_source.cpp
+    if (!body->get("station_name") || !body->get("network_name"))
+      throw std::runtime_error("Station name and network name are required for adjoint source");
+    s.kind = Source::ADJOINT;
+    s.station = body->get("station_name")->str();
+    s.network = body->get("network_name")->str();
+    s.wavefield = 1;
   } else {
-    throw std::runtime_error("Unknown source type (this path supports force and moment-tensor)");
+    throw std::runtime_error("Unknown source type (this path supports force, moment-tensor and adjoint-source)");
   }
   s.x = body->get("x")->num();
   s.z = body->get("z")->num();
+  if (const YNode *ext = body->get("External")) {
+    read_external_stf(*ext, nstep, dt, config, s);
+    return s;
+  }
+  if (s.kind == Source::ADJOINT) throw std::runtime_error("adjoint sources need an External source time function");
   const YNode *stf = nullptr;
   if ((stf = body->get("Ricker"))) {
     s.stf = Source::RICKER;
@@ -90,6 +148,12 @@ void Problem::finalize() {
   const int n = a.ngll;
   located_sources.clear();
   for (auto &s : sources) located_sources.push_back(locate_source(a, s, t0, dt, nstep));
+  located_adjoint.clear();
+  for (auto &s : adjoint_sources) {
+    located_adjoint.push_back(locate_source(a, s, t0, dt, nstep));
+    if (located_adjoint.back().medium != MEDIUM_ELASTIC_PSV)
+      throw std::runtime_error("adjoint sources from files are supported in elastic P-SV elements");
+  }
   located_receivers.clear();
   for (auto &r : receivers) located_receivers.push_back(locate_receiver(a, r));
   // flat copies
@@ -274,12 +338,29 @@ Problem problem_from_yaml(const std::string &parameter_file,
   }
   const YNode *list = sdict->get("sources");
   if (!list || !list->is_seq()) throw std::runtime_error("sources file has no 'sources' list");
-  for (auto &e : list->seq) P.sources.push_back(parse_source(*e, P.dt));
+  const std::string src_config = src->is_scalar() ? resolve(src->str(), parameter_file) : parameter_file;
+  for (auto &e : list->seq) P.sources.push_back(parse_source(*e, P.dt, P.nstep, src_config));
   if (const YNode *ns = sdict->get("number-of-sources"))
     if (ns->integer() != static_cast<int>(P.sources.size()))
       throw std::runtime_error("Found only " + std::to_string(P.sources.size()) +
                                " number of sources; the file announces " + ns->str());
+  int nadjoint = 0;
+  for (const Source &s : P.sources) nadjoint += s.kind == Source::ADJOINT;
+  if (nadjoint == static_cast<int>(P.sources.size())) throw std::runtime_error("No sources found in the sources file");
+  if (P.simulation == 1 && nadjoint == 0) throw std::runtime_error("No adjoint sources found in the sources file");
+  if (P.simulation == 0 && nadjoint > 0)
+    throw std::runtime_error("Adjoint sources found in the sources file for forward simulation");
   P.t0 = resolve_t0(P.sources, user_t0);
+  for (const Source &s : P.sources)
+    if (s.stf == Source::TABLE && std::abs(P.t0 - s.table_t0) > 1e-6)
+      throw std::runtime_error("The start time of the external source time function does not match the simulation start time");
+  // adjoint sources drive the adjoint wavefield; the others the forward
+  // (forward run) or backward (combined run) wavefield
+  {
+    std::vector<Source> keep;
+    for (Source &s : P.sources) (s.kind == Source::ADJOINT ? P.adjoint_sources : keep).push_back(s);
+    P.sources = keep;
+  }
   P.source_shot.assign(P.sources.size(), 0);
 
   // receivers

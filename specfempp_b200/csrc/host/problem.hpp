@@ -24,6 +24,12 @@ struct Problem {
   std::vector<LocatedSource> located_sources;
   std::vector<Receiver> receivers;
   std::vector<LocatedReceiver> located_receivers;
+  // adjoint sources given in the sources file (combined runs), located like
+  // point sources with Lagrange weights in both components and their own
+  // [nstep][2] time functions; empty: adjoint sources at the stations, set
+  // through sfb_set_adjoint_sources
+  std::vector<Source> adjoint_sources;
+  std::vector<LocatedSource> located_adjoint;
   bool save_boundary_values = false;
   bool elastic_sh = false;
   // Output settings from the YAML file.

@@ -3,6 +3,7 @@
 // both in std::scientific, files NET.STA.S2.BX{X,Z}.sem{d,v,a},
 // NET.STA.S2.PRE.semp and, for SH, NET.STA.S2.BXY.sem{d,v,a}.
 #include <cstdio>
+#include <filesystem>
 #include <fstream>
 #include <iomanip>
 #include <stdexcept>
@@ -16,6 +17,8 @@ namespace sfb {
 void write_seismograms_ascii(const Problem &P, const float *seis, int ntypes, int nrec, int max_sig,
                              const std::string &dir) {
   static const char *ext[] = {"semd", "semv", "sema", "semp", "semr"};
+  std::error_code ec;
+  std::filesystem::create_directories(dir, ec);  // the folder may not exist yet
   for (int r = 0; r < nrec; ++r) {
     const Receiver &rc = P.receivers[r];
     for (int it = 0; it < ntypes; ++it) {

@@ -245,7 +245,7 @@ class Simulation:
     def kernels(self, which: int) -> np.ndarray:
         """Frechet kernel summed over shots, [nspec][ngll][ngll] FP64:
         0 rho, 1 mu, 2 kappa, 3 rhop, 4 alpha, 5 beta (acoustic points:
-        0 rho, 2 kappa)."""
+        0 rho, 2 kappa, 3 rhop, 4 alpha)."""
         i = self.info()
         out = np.zeros((i.nspec, i.ngll, i.ngll), dtype=np.float64)
         self._check(self._lib.sfb_get_kernels(self._h, which, out.ctypes.data_as(C.POINTER(C.c_double)), out.size))
