@@ -136,3 +136,30 @@ def test_checkpoints_bound_backward_reconstruction(nshots):
     for c in range(3):
         assert parity_ok(rel_l2(K1[..., c], o32[..., c]), rel_l2(K1[..., c], o64[..., c]),
                          rel_l2(o32[..., c], o64[..., c]))
+
+
+def test_acoustic_kernels_match_oracle():
+    """Acoustic combined run: rho, kappa and the derived rhop (sum over steps
+    of rho_kl * kappa_kl) and alpha (2 kappa), point/kernels.hpp:189-192."""
+    from specfempp_b200 import StructuredProblem, Material, ForceSource, Station
+    p = StructuredProblem(nx=16, nz=12, x0=0, x1=800, z0=0, z1=600,
+                          materials=[Material(1020.0, 1500.0, 0.0)],
+                          absorb=(True, True, False, True), dt=5e-4, nstep=NSTEP,
+                          sources=[ForceSource(x=400, z=300, f0=8.0, factor=1e10)],
+                          stations=[Station(x=100 + 120 * k, z=500) for k in range(6)],
+                          seismogram_types=("pressure",), save_boundary_values=True)
+    sim = Simulation.structured(p)
+    sim.run_forward()
+    rng = np.random.default_rng(5)
+    stf = (1e-3 * rng.standard_normal((NSTEP, 6, 2))).astype(np.float32)
+    sim.set_adjoint_sources(stf)
+    sim.run_combined()
+    o32 = oracle_kernels(sim, [stf], 32)
+    o64 = oracle_kernels(sim, [stf], 64)
+    for which, ref in ((0, lambda o: o[..., 0]), (2, lambda o: o[..., 1]), (3, lambda o: o[..., 2]),
+                       (4, lambda o: 2.0 * o[..., 1])):
+        g = sim.kernels(which)
+        e32, e64, eref = rel_l2(g, ref(o32)), rel_l2(g, ref(o64)), rel_l2(ref(o32), ref(o64))
+        print("acoustic kernel %d: vs FP32 %.2e vs FP64 %.2e (FP32 oracle vs FP64 %.2e)" % (which, e32, e64, eref))
+        assert np.abs(g).max() > 0
+        assert parity_ok(e32, e64, eref), (which, e32, e64, eref)
