@@ -128,10 +128,11 @@ typedef struct sfb_info {
   double dt, t0;
   size_t device_bytes;   /* device memory held by the context                */
   uint64_t kernel_launches; /* kernels this context has launched so far      */
-  int stiffness_variant[4]; /* batched (nshots > 1) stiffness kernel per medium
-                               tag: 0 not chosen yet, 1 two shots per lane in
-                               packed FP32x2, 2 two shots per lane scalar,
-                               3 one shot per lane                           */
+  int stiffness_variant[4]; /* stiffness kernel per medium tag, 0 not chosen
+                               yet; nshots > 1: 1 two shots per lane in packed
+                               FP32x2, 2 two shots per lane scalar, 3 one shot
+                               per lane; nshots == 1 (NGLL 5): 1 row kernel
+                               with 32-element chunks, 2 with 16             */
   int private_points;    /* P-SV points updated inside the batched stiffness
                             launch of the forward run (0: none)             */
   int nadjoint_sources;  /* adjoint sources given in the sources file        */

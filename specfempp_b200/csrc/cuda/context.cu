@@ -411,7 +411,7 @@ void ensure_device(sfb_context *c) {
 void autotune_stiffness(sfb_context *c, WavefieldSet &W) {
   const Problem &P = c->P;
   const int S = P.nshots, n = P.asmb.ngll;
-  if (S < 2 || c->tuned) return;
+  if (c->tuned || (S == 1 && n != 5)) return;
   c->tuned = true;
   cudaEvent_t e0, e1;
   ck(cudaEventCreate(&e0), "event");
@@ -420,11 +420,16 @@ void autotune_stiffness(sfb_context *c, WavefieldSet &W) {
   for (int m : kMedia) {
     if (c->shots_variant[m] != dev::kShotsAuto || W.f[m].nelem == 0) continue;
     int cand[3], nc = 0;
-    if (S % 2 == 0 && n <= 5) {
-      cand[nc++] = dev::kShotsPacked;
-      cand[nc++] = dev::kShotsPair;
+    if (S == 1) {
+      cand[nc++] = dev::kRowFullChunk;
+      cand[nc++] = dev::kRowHalfChunk;
+    } else {
+      if (S % 2 == 0 && n <= 5) {
+        cand[nc++] = dev::kShotsPacked;
+        cand[nc++] = dev::kShotsPair;
+      }
+      cand[nc++] = dev::kShotsSingle;
     }
-    cand[nc++] = dev::kShotsSingle;
     float best = 0.f;
     int choice = cand[0];
     for (int i = 0; i < nc && nc > 1; ++i) {

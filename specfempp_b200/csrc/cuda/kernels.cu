@@ -1554,9 +1554,17 @@ void launch_stiffness(int medium, int ngll, const Static &st, const MediumFields
     return;
   }
   if (ngll == 5) {
-    if (medium == MED_PSV) launch_rp<MED_PSV, 5, 32, 3>(st, f, nshots, ss, istep_dev, w, stream);
-    else if (medium == MED_SH) launch_rp<MED_SH, 5, 32, 3>(st, f, nshots, ss, istep_dev, w, stream);
-    else launch_rp<MED_AC, 5, 32, 3>(st, f, nshots, ss, istep_dev, w, stream);
+    // single shot: the row kernel with 32 elements per chunk (variant 0 / 1),
+    // or 16 elements per chunk and twice the CTAs per SM (variant 2)
+    if (variant == kRowHalfChunk) {
+      if (medium == MED_PSV) launch_rp<MED_PSV, 5, 16, 6>(st, f, nshots, ss, istep_dev, w, stream);
+      else if (medium == MED_SH) launch_rp<MED_SH, 5, 16, 6>(st, f, nshots, ss, istep_dev, w, stream);
+      else launch_rp<MED_AC, 5, 16, 6>(st, f, nshots, ss, istep_dev, w, stream);
+    } else {
+      if (medium == MED_PSV) launch_rp<MED_PSV, 5, 32, 3>(st, f, nshots, ss, istep_dev, w, stream);
+      else if (medium == MED_SH) launch_rp<MED_SH, 5, 32, 3>(st, f, nshots, ss, istep_dev, w, stream);
+      else launch_rp<MED_AC, 5, 32, 3>(st, f, nshots, ss, istep_dev, w, stream);
+    }
   } else if (ngll == 8) {
     if (medium == MED_PSV) launch_rp<MED_PSV, 8, 16, 2>(st, f, nshots, ss, istep_dev, w, stream);
     else if (medium == MED_SH) launch_rp<MED_SH, 8, 16, 2>(st, f, nshots, ss, istep_dev, w, stream);

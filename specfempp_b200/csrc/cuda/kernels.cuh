@@ -208,6 +208,8 @@ void set_quadrature(int ngll, const float *hprime, const float *wgll);
 // TMA-fed row kernel; several shots: the shot-parallel kernel.
 // Kernel variants of the batched (nshots > 1) stiffness; see launch_shots.
 constexpr int kShotsAuto = 0, kShotsPacked = 1, kShotsPair = 2, kShotsSingle = 3;
+// Single-shot (nshots == 1, NGLL 5) variants: row kernel, 32 or 16 elements per chunk.
+constexpr int kRowFullChunk = 1, kRowHalfChunk = 2;
 void launch_stiffness(int medium, int ngll, const Static &st, const MediumFields &f,
                       int nshots, const StaceyStore &ss, const int *istep_dev,
                       cudaStream_t stream, const TailWork *tw = nullptr,
