@@ -28,7 +28,8 @@ def build():
 def load():
     global _lib
     if _lib is None:
-        if not os.path.exists(LIB):
+        src = os.path.join(HERE, "oracle.cpp")
+        if not os.path.exists(LIB) or os.path.getmtime(src) > os.path.getmtime(LIB):
             build()
         lib = C.CDLL(LIB)
         lib.oracle_forward.restype = C.c_int
