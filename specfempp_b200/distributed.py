@@ -42,7 +42,7 @@ def gpu_shard_compute(problem, model, observed):
     params = [torch.tensor(np.asarray(a, dtype=np.float64), requires_grad=True) for a in model]
     chi = WaveformMisfit.apply(*params, sim, torch.from_numpy(np.asarray(observed, dtype=np.float64)))
     chi.backward()
-    return float(chi), [p.grad.numpy() for p in params]
+    return float(chi.detach()), [p.grad.numpy() for p in params]
 
 
 class ShardedMisfit:
