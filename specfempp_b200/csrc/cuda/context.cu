@@ -129,9 +129,8 @@ struct sfb_context {
   } taps[4];
   bool taps_ready = false;
   DBuf<unsigned> done;  // CTA completion counter of the update kernel
-  // batched P-SV forward: points updated inside the stiffness launch are
-  // left out of the update kernel, which walks `shared_points` instead
-  DBuf<int> shared_points;
+  // P-SV points updated inside the stiffness launch of the forward run are
+  // numbered last; the update kernel then walks [0, nshared_points)
   int nshared_points = 0, nprivate_points = 0;
   // batched stiffness kernel per medium (dev::kShots*), chosen by
   // autotune_stiffness or set by the caller
@@ -260,37 +259,16 @@ void ensure_device(sfb_context *c) {
       eflag[d] |= a.bnd[p];
     }
   }
-  // Element-private points of the batched P-SV forward.  An element
-  // qualifies when it has no boundary points and hosts no source or
-  // receiver; its (N-2)^2 interior points then belong to it alone (checked
-  // by counting references) and are updated inside its stiffness launch.
-  if (c->P.nshots > 1 && c->med_count[MEDIUM_ELASTIC_PSV] > 0 && n > 2) {
+  // Element-private points (Problem::elem_private): the P-SV field is
+  // numbered shared points first, so the update kernel can stop at
+  // nshared_points when the stiffness launch has updated the rest.
+  {
     const int m = MEDIUM_ELASTIC_PSV;
-    std::vector<int> refs(a.nglob[m], 0);
+    const Problem &P0 = c->P;
     for (int d = c->med_begin[m]; d < c->med_begin[m] + c->med_count[m]; ++d)
-      for (int k = 0; k < nn; ++k) ++refs[iglob[static_cast<size_t>(d) * nn + k]];
-    std::vector<uint8_t> busy(a.nspec, 0);
-    for (int i : c->P.v_src_ispec) busy[c->inv[i]] = 1;
-    for (const auto &r : c->P.located_receivers) busy[c->inv[r.ispec]] = 1;
-    std::vector<uint8_t> priv(a.nglob[m], 0);
-    for (int d = c->med_begin[m]; d < c->med_begin[m] + c->med_count[m]; ++d) {
-      if (eflag[d] || busy[d]) continue;
-      bool ok = true;
-      for (int iz = 1; iz < n - 1 && ok; ++iz)
-        for (int ix = 1; ix < n - 1; ++ix)
-          if (refs[iglob[static_cast<size_t>(d) * nn + iz * n + ix]] != 1) { ok = false; break; }
-      if (!ok) continue;
-      eflag[d] |= dev::kElemPrivate;
-      for (int iz = 1; iz < n - 1; ++iz)
-        for (int ix = 1; ix < n - 1; ++ix) priv[iglob[static_cast<size_t>(d) * nn + iz * n + ix]] = 1;
-    }
-    std::vector<int> shared;
-    shared.reserve(a.nglob[m]);
-    for (int g = 0; g < a.nglob[m]; ++g)
-      if (!priv[g]) shared.push_back(g);
-    c->nshared_points = static_cast<int>(shared.size());
-    c->nprivate_points = a.nglob[m] - c->nshared_points;
-    if (c->nprivate_points > 0) c->shared_points.upload(shared, &c->device_bytes);
+      if (!P0.elem_private.empty() && P0.elem_private[c->perm[d]]) eflag[d] |= dev::kElemPrivate;
+    c->nshared_points = P0.nshared_psv;
+    c->nprivate_points = a.nglob[m] - P0.nshared_psv;
   }
   // packed per-element static block: iglob, xix, xiz, gammax, gammaz, jac, mat0, mat1
   std::vector<float> pack(nloc * dev::kPackFields);
@@ -677,10 +655,8 @@ dev::UpdateParams update_params(sfb_context *c, WavefieldSet &W, int last, bool 
       M.ck_v = c->ck_v[m].p;
       M.ck_stride = c->ck_stride[m];
     }
-    if (private_done && m == MEDIUM_ELASTIC_PSV && c->nprivate_points > 0) {
-      M.list = c->shared_points.p;
-      M.ld2 = static_cast<size_t>(c->nshared_points) * P.nshots;  // one float2 pair per (point, shot)
-    }
+    if (private_done && m == MEDIUM_ELASTIC_PSV && c->nprivate_points > 0)
+      M.ld2 = static_cast<size_t>(c->nshared_points) * P.nshots;  // shared points only, a float2 pair each
     if (taps && c->taps[m].nsup > 0) {
       const auto &T = c->taps[m];
       M.taps = {T.nsup, T.mask.p, T.sup_g.p, T.sup_begin.p, T.slot.p, T.which.p, T.w.p};

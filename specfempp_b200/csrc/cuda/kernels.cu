@@ -201,7 +201,8 @@ __device__ __forceinline__ void tail_work(const Static &st, const MediumFields &
 // force array.  Every mbarrier wait is bounded (SFB_DEVICE_WAIT_TIMEOUT).
 template <int MED, int N, int EPB, int MINB>
 __global__ void __launch_bounds__(N * EPB, MINB)
-k_stiffness_rp(Static st, MediumFields f, int nshots, StaceyStore ss, const int *istep_dev, TailWork tw) {
+k_stiffness_rp(Static st, MediumFields f, int nshots, StaceyStore ss, const int *istep_dev, TailWork tw,
+               FusedUpdate fu) {
   constexpr int NC = (MED == MED_PSV) ? 2 : 1;
   constexpr int NN = N * N;
   constexpr int ELEM_WORDS = kPackFields * NN;
@@ -268,6 +269,14 @@ k_stiffness_rp(Static st, MediumFields f, int nshots, StaceyStore ss, const int 
     const int e = f.elem_begin + (valid ? li : 0);
     const uint8_t eflag = valid ? st.eflag[e] : 0;
     const int slot = (ss.mode != 0 && valid) ? ss.slot[e] : -1;
+    // element-private points of this row (single shot): their velocity is
+    // needed after the divergence, so fetch it now
+    const bool fused = fu.enabled && nshots == 1 && (eflag & kElemPrivate) && iz >= 1 && iz <= N - 2;
+    V vp[N - 2];
+    if (fused) {
+#pragma unroll
+      for (int ix = 1; ix <= N - 2; ++ix) vp[ix - 1] = reinterpret_cast<const V *>(fu.v)[g[ix]];
+    }
     for (int s = 0; s < nshots; ++s) {
       if (s > 0) {
 #pragma unroll
@@ -391,6 +400,31 @@ k_stiffness_rp(Static st, MediumFields f, int nshots, StaceyStore ss, const int 
       if (valid) {
 #pragma unroll
         for (int ix = 0; ix < N; ++ix) {
+          if (fused && ix >= 1 && ix <= N - 2) {
+            // a = force / M, corrector, next predictor in registers
+            // (newmark.tpp:44-47, 98-105); the force never reaches memory
+            V vel = vp[ix - 1], uu = ur[ix], aa;
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+              const float a_c = accr[ix][c] * fu.minv[g[ix] * NC + c];
+              set_comp(aa, c, a_c);
+              set_comp(vel, c, comp(vel, c) + fu.dt2 * a_c);
+            }
+            V *Vw = reinterpret_cast<V *>(fu.v);
+            if (fu.last) {
+              abase[g[ix]] = aa;
+              Vw[g[ix]] = vel;
+            } else {
+#pragma unroll
+              for (int c = 0; c < NC; ++c) {
+                set_comp(uu, c, comp(uu, c) + fu.dt * comp(vel, c) + fu.dtsq2 * comp(aa, c));
+                set_comp(vel, c, comp(vel, c) + fu.dt2 * comp(aa, c));
+              }
+              reinterpret_cast<V *>(f.u)[g[ix]] = uu;
+              Vw[g[ix]] = vel;
+            }
+            continue;
+          }
           V out;
 #pragma unroll
           for (int c = 0; c < NC; ++c) set_comp(out, c, accr[ix][c]);
@@ -424,7 +458,7 @@ size_t rp_smem_bytes() {
 
 template <int MED, int N, int EPB, int MINB>
 void launch_rp(const Static &st, const MediumFields &f, int nshots, const StaceyStore &ss, const int *istep_dev,
-               const TailWork &tw, cudaStream_t stream) {
+               const TailWork &tw, const FusedUpdate &fu, cudaStream_t stream) {
   static int blocks_per_sm = -1, nsm = 0;
   const size_t smem = rp_smem_bytes<MED, N, EPB>();
   if (blocks_per_sm < 0) {
@@ -438,7 +472,7 @@ void launch_rp(const Static &st, const MediumFields &f, int nshots, const Stacey
   }
   const int nchunks = (f.nelem + EPB - 1) / EPB;
   const int grid = std::max(1, std::min(nchunks, nsm * blocks_per_sm));
-  k_stiffness_rp<MED, N, EPB, MINB><<<grid, N * EPB, smem, stream>>>(st, f, nshots, ss, istep_dev, tw);
+  k_stiffness_rp<MED, N, EPB, MINB><<<grid, N * EPB, smem, stream>>>(st, f, nshots, ss, istep_dev, tw, fu);
 }
 
 // Shot-parallel stiffness for S > 1 independent wavefields (batched shots).
@@ -1287,13 +1321,11 @@ __global__ void k_update_all(UpdateParams P) {
     // consecutive entries 2jj, 2jj + 1 of [g][s] (nc = 1)
     int g0, s0, g1, s1;
     float2 m;
-    size_t at = jj;  // pair index in the field arrays
+    const size_t at = jj;  // pair index in the field arrays
     if (M.nc == 2) {
       const uint32_t n = static_cast<uint32_t>(jj);
-      const int k = static_cast<int>(P.sdiv.div(n));
-      s0 = s1 = static_cast<int>(n - static_cast<uint32_t>(k) * S);
-      g0 = g1 = M.list ? M.list[k] : k;
-      if (M.list) at = static_cast<size_t>(g0) * S + s0;
+      g0 = g1 = static_cast<int>(P.sdiv.div(n));
+      s0 = s1 = static_cast<int>(n - static_cast<uint32_t>(g0) * S);
       m = reinterpret_cast<const float2 *>(M.minv)[g0];
     } else {
       const uint32_t n0 = static_cast<uint32_t>(2 * jj), n1 = n0 + 1;
@@ -1539,8 +1571,8 @@ void launch_stiffness(int medium, int ngll, const Static &st, const MediumFields
   const TailWork none{};
   const TailWork &w = tw ? *tw : none;
   const FusedUpdate nofu{};
-  // the in-launch update of private points exists for the batched P-SV kernels
-  const FusedUpdate &u = (fu && nshots > 1 && medium == MED_PSV) ? *fu : nofu;
+  // the in-launch update of private points exists for the P-SV kernels
+  const FusedUpdate &u = (fu && medium == MED_PSV) ? *fu : nofu;
   if (nshots > 1) {
     if (ngll == 5) {
       if (medium == MED_PSV) launch_shots<MED_PSV, 5, 4>(st, f, nshots, ss, istep_dev, w, u, variant, stream);
@@ -1557,18 +1589,18 @@ void launch_stiffness(int medium, int ngll, const Static &st, const MediumFields
     // single shot: the row kernel with 32 elements per chunk (variant 0 / 1),
     // or 16 elements per chunk and twice the CTAs per SM (variant 2)
     if (variant == kRowHalfChunk) {
-      if (medium == MED_PSV) launch_rp<MED_PSV, 5, 16, 6>(st, f, nshots, ss, istep_dev, w, stream);
-      else if (medium == MED_SH) launch_rp<MED_SH, 5, 16, 6>(st, f, nshots, ss, istep_dev, w, stream);
-      else launch_rp<MED_AC, 5, 16, 6>(st, f, nshots, ss, istep_dev, w, stream);
+      if (medium == MED_PSV) launch_rp<MED_PSV, 5, 16, 6>(st, f, nshots, ss, istep_dev, w, u, stream);
+      else if (medium == MED_SH) launch_rp<MED_SH, 5, 16, 6>(st, f, nshots, ss, istep_dev, w, nofu, stream);
+      else launch_rp<MED_AC, 5, 16, 6>(st, f, nshots, ss, istep_dev, w, nofu, stream);
     } else {
-      if (medium == MED_PSV) launch_rp<MED_PSV, 5, 32, 3>(st, f, nshots, ss, istep_dev, w, stream);
-      else if (medium == MED_SH) launch_rp<MED_SH, 5, 32, 3>(st, f, nshots, ss, istep_dev, w, stream);
-      else launch_rp<MED_AC, 5, 32, 3>(st, f, nshots, ss, istep_dev, w, stream);
+      if (medium == MED_PSV) launch_rp<MED_PSV, 5, 32, 3>(st, f, nshots, ss, istep_dev, w, u, stream);
+      else if (medium == MED_SH) launch_rp<MED_SH, 5, 32, 3>(st, f, nshots, ss, istep_dev, w, nofu, stream);
+      else launch_rp<MED_AC, 5, 32, 3>(st, f, nshots, ss, istep_dev, w, nofu, stream);
     }
   } else if (ngll == 8) {
-    if (medium == MED_PSV) launch_rp<MED_PSV, 8, 16, 2>(st, f, nshots, ss, istep_dev, w, stream);
-    else if (medium == MED_SH) launch_rp<MED_SH, 8, 16, 2>(st, f, nshots, ss, istep_dev, w, stream);
-    else launch_rp<MED_AC, 8, 16, 2>(st, f, nshots, ss, istep_dev, w, stream);
+    if (medium == MED_PSV) launch_rp<MED_PSV, 8, 16, 2>(st, f, nshots, ss, istep_dev, w, u, stream);
+    else if (medium == MED_SH) launch_rp<MED_SH, 8, 16, 2>(st, f, nshots, ss, istep_dev, w, nofu, stream);
+    else launch_rp<MED_AC, 8, 16, 2>(st, f, nshots, ss, istep_dev, w, nofu, stream);
   }
 }
 

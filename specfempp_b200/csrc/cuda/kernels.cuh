@@ -132,8 +132,6 @@ struct UpdateMedium {
   size_t ld2;    // float2 pairs of the whole [g][s][c] array
   int nc;        // components per point (1: a pair holds two entries)
   ReceiverTaps taps;
-  const int *list;  // nc = 2 only: update just these points (the rest were
-                    // updated inside the stiffness launch); null: every point
   float *cu, *cv;   // Kahan compensation terms of u and v (same layout), or null
   // forward snapshots for the combined run: slot c (c = 0 .. count-1) holds
   // u at step (c+1)K (written by step (c+1)K - 1) and v half a step later
@@ -142,13 +140,13 @@ struct UpdateMedium {
   size_t ck_stride;  // floats per slot
 };
 
-// Newmark update of element-private points inside the batched stiffness
-// launch.  A GLL point strictly inside an element belongs to that element
-// alone, so once the element's force is known the point's corrector and
-// next predictor can run in registers without the force ever reaching
-// memory.  Elements flagged kElemPrivate in `eflag` (no boundary points,
-// no source, no receiver) qualify; their (N-2)^2 interior points are left
-// out of the update kernel's point list.
+// Newmark update of element-private points inside the stiffness launch.  A
+// GLL point strictly inside an element belongs to that element alone, so
+// once the element's force is known the point's corrector and next
+// predictor can run in registers without the force ever reaching memory.
+// Elements flagged kElemPrivate in `eflag` (no boundary points, no source,
+// no receiver) qualify; their (N-2)^2 interior points are numbered after
+// every shared point of the P-SV field, which the update kernel covers.
 struct FusedUpdate {
   int enabled;
   const float *minv;   // [nglob][nc]

@@ -141,6 +141,57 @@ Source parse_source(const YNode &entry, double dt, int nstep, const std::string 
   return s;
 }
 
+// See Problem::elem_private.  The permutation keeps the relative order of
+// the shared points and of the private points, so applying it again is the
+// identity.
+void mark_private_points(Problem &P) {
+  Assembly &a = P.asmb;
+  const int n = a.ngll, nn = n * n, m = MEDIUM_ELASTIC_PSV;
+  P.elem_private.assign(a.nspec, 0);
+  P.nshared_psv = a.nglob[m];
+  if (n <= 2 || a.nglob[m] == 0) return;
+  std::vector<int> refs(a.nglob[m], 0);
+  std::vector<uint8_t> busy(a.nspec, 0);
+  for (int e = 0; e < a.nspec; ++e) {
+    if (a.medium[e] != m) continue;
+    for (int k = 0; k < nn; ++k) {
+      const size_t p = static_cast<size_t>(e) * nn + k;
+      ++refs[a.iglob[p]];
+      if (a.bnd[p]) busy[e] = 1;
+    }
+  }
+  for (const auto &s : P.located_sources) busy[s.ispec] = 1;
+  for (const auto &s : P.located_adjoint) busy[s.ispec] = 1;
+  for (const auto &r : P.located_receivers) busy[r.ispec] = 1;
+  std::vector<uint8_t> priv(a.nglob[m], 0);
+  for (int e = 0; e < a.nspec; ++e) {
+    if (a.medium[e] != m || busy[e]) continue;
+    bool ok = true;
+    for (int iz = 1; iz < n - 1 && ok; ++iz)
+      for (int ix = 1; ix < n - 1; ++ix)
+        if (refs[a.iglob[static_cast<size_t>(e) * nn + iz * n + ix]] != 1) { ok = false; break; }
+    if (!ok) continue;
+    P.elem_private[e] = 1;
+    for (int iz = 1; iz < n - 1; ++iz)
+      for (int ix = 1; ix < n - 1; ++ix) priv[a.iglob[static_cast<size_t>(e) * nn + iz * n + ix]] = 1;
+  }
+  std::vector<int> perm(a.nglob[m]);
+  int next = 0;
+  for (int g = 0; g < a.nglob[m]; ++g)
+    if (!priv[g]) perm[g] = next++;
+  P.nshared_psv = next;
+  for (int g = 0; g < a.nglob[m]; ++g)
+    if (priv[g]) perm[g] = next++;
+  for (int e = 0; e < a.nspec; ++e)
+    if (a.medium[e] == m)
+      for (int k = 0; k < nn; ++k) {
+        int &ig = a.iglob[static_cast<size_t>(e) * nn + k];
+        ig = perm[ig];
+      }
+  for (auto &c : a.couple_acoustic) c.coupled_iglob = perm[c.coupled_iglob];
+  for (auto &c : a.couple_elastic) c.self_iglob = perm[c.self_iglob];
+}
+
 }  // namespace
 
 void Problem::finalize() {
@@ -156,6 +207,7 @@ void Problem::finalize() {
   }
   located_receivers.clear();
   for (auto &r : receivers) located_receivers.push_back(locate_receiver(a, r));
+  mark_private_points(*this);
   // flat copies
   const size_t ns = sources.size();
   v_src_ispec.assign(ns, 0);

@@ -47,7 +47,13 @@ struct Problem {
   std::vector<float> v_rec_lagrange, v_rec_sin, v_rec_cos;
   std::vector<int> v_cp_ac_self, v_cp_ac_other, v_cp_el_self, v_cp_el_other;
   std::vector<float> v_cp_ac_f, v_cp_ac_nx, v_cp_ac_nz, v_cp_el_f, v_cp_el_nx, v_cp_el_nz;
-  void finalize();  // locate sources / receivers and fill the flat copies
+  // Element-private points (P-SV): elements with no boundary points and no
+  // source, receiver or adjoint source get elem_private = 1; their interior
+  // (N-2)^2 points belong to them alone.  finalize() renumbers the P-SV
+  // field so that the other (shared) points come first: [0, nshared_psv).
+  std::vector<uint8_t> elem_private;  // [nspec]
+  int nshared_psv = 0;
+  void finalize();  // locate sources / receivers, private points, flat copies
   void fill_view(sfb_problem_view *v) const;
 };
 

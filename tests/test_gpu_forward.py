@@ -166,6 +166,7 @@ def test_final_fields_match_oracle():
     p = small_elastic(nstep=300)
     sim = Simulation.structured(p)
     sim.run_forward()
+    assert sim.info().private_points > 0  # the single-shot kernel updated element-private points
     o = bridge.forward(sim, 32, threads=8, want_fields=True)
     o64 = bridge.forward(sim, 64, threads=8, want_fields=True)
     for which, name in ((0, "u"), (1, "v"), (2, "a"), (3, "minv")):
