@@ -417,7 +417,7 @@ k_stiffness_rp(Static st, MediumFields f, int nshots, StaceyStore ss, const int 
             } else {
 #pragma unroll
               for (int c = 0; c < NC; ++c) {
-                set_comp(uu, c, comp(uu, c) + fu.dt * comp(vel, c) + fu.dtsq2 * comp(aa, c));
+                set_comp(uu, c, comp(uu, c) + (fu.dt * comp(vel, c) + fu.dtsq2 * comp(aa, c)));
                 set_comp(vel, c, comp(vel, c) + fu.dt2 * comp(aa, c));
               }
               reinterpret_cast<V *>(f.u)[g[ix]] = uu;
@@ -668,7 +668,7 @@ k_stiffness_shots(Static st, MediumFields f, int S, StaceyStore ss, const int *i
       } else {
 #pragma unroll
         for (int q = 0; q < NV; ++q) {
-          vset(uu, q, vget(uu, q) + fu.dt * vget(vel, q) + fu.dtsq2 * vget(aa, q));
+          vset(uu, q, vget(uu, q) + (fu.dt * vget(vel, q) + fu.dtsq2 * vget(aa, q)));
           vset(vel, q, vget(vel, q) + fu.dt2 * vget(aa, q));
         }
         Uw[at] = uu;
@@ -1003,7 +1003,7 @@ k_stiffness_pk(Static st, MediumFields f, int S, StaceyStore ss, const int *iste
       } else {
 #pragma unroll
         for (int c = 0; c < NC; ++c) {
-          setpr(uu, c, fma2(dtsq2, pr(aa, c), fma2(dt, pr(vel, c), pr(uu, c))));
+          setpr(uu, c, add2(pr(uu, c), fma2(dt, pr(vel, c), mul2(dtsq2, pr(aa, c)))));
           setpr(vel, c, fma2(dt2, pr(aa, c), pr(vel, c)));
         }
         Uw[at] = swz(uu);
