@@ -3,10 +3,11 @@
 (include/io/wavefield/writer.tpp), traveltime adjoint sources made from the
 seismograms by the xadj_seismogram restatement, then a combined run that
 reads the wavefield and the External adjoint sources and writes the kernels
-(include/io/kernel/writer.tpp).  The kernel files must agree with the kernels
-of one in-memory context given the same adjoint sources, and the written
-wavefield with that context's final fields, to the run-to-run spread of
-FP32 red-add order (the file round trip itself is exact in FP32)."""
+(include/io/kernel/writer.tpp).  The kernels read back from the files must
+meet the kernel bar against the oracle run on the same problem and adjoint
+sources, and the written wavefield must agree with a second run's final
+fields to the run-to-run spread of FP32 red-add order (the file round trip
+itself is exact in FP32)."""
 import os
 
 import numpy as np
@@ -52,10 +53,29 @@ def test_two_phase_workflow_matches_in_memory(tmp_path):
     sim.set_adjoint_sources(stf)
     sim.run_combined()
     info = sim.info()
-    for q, name in enumerate(("rho", "mu", "kappa", "rhop", "alpha", "beta")):
-        k_file = read_kernel(os.path.join(root, "kernels"), "elastic_psv_isotropic", name, NX * NZ, info.ngll)
-        k_mem = sim.kernels(q)
-        err = rel_l2(k_file, k_mem)
-        print("kernel %s: file vs in-memory rel-L2 %.2e" % (name, err))
-        assert np.abs(k_mem).max() > 0
-        assert err <= 1e-3, (name, err)
+    from oracle import bridge
+    o = {}
+    for prec in (32, 64):
+        fwd = bridge.forward(sim, prec, threads=8, want_fields=True, want_stacey=True)
+        o[prec] = bridge.combined(sim, stf, fwd, precision=prec, threads=8)
+    files = {name: read_kernel(os.path.join(root, "kernels"), "elastic_psv_isotropic", name, NX * NZ, info.ngll)
+             for name in ("rho", "mu", "kappa", "rhop", "alpha", "beta")}
+    for q, name in enumerate(("rho", "mu", "kappa")):
+        k = files[name]
+        e32, e64, eref = rel_l2(k, o[32][..., q]), rel_l2(k, o[64][..., q]), rel_l2(o[32][..., q], o[64][..., q])
+        spread = rel_l2(k, sim.kernels(q))
+        print("kernel %s from files: vs FP32 oracle %.2e, vs FP64 %.2e (FP32 oracle vs FP64 %.2e); "
+              "vs a second GPU run %.2e" % (name, e32, e64, eref, spread))
+        assert np.abs(k).max() > 0
+        assert (e32 <= 1e-3 and e64 <= 1e-3) or e64 <= 1e-5 + 1.5 * eref, (name, e32, e64, eref)
+    # derived kernels in the files are the reference's combinations of the
+    # primaries (frechet_derivative.hpp:117-135)
+    kappa, mu, _ = sim.material()
+    kap = kappa + mu / 3.0
+    r = mu / kap
+    np.testing.assert_allclose(files["rhop"], files["rho"] + files["kappa"] + files["mu"], rtol=1e-5,
+                               atol=1e-6 * np.abs(files["rhop"]).max())
+    np.testing.assert_allclose(files["alpha"], 2.0 * (1.0 + 4.0 / 3.0 * r) * files["kappa"], rtol=1e-5,
+                               atol=1e-6 * np.abs(files["alpha"]).max())
+    np.testing.assert_allclose(files["beta"], 2.0 * (files["mu"] - 4.0 / 3.0 * r * files["kappa"]), rtol=1e-5,
+                               atol=1e-6 * np.abs(files["beta"]).max())
