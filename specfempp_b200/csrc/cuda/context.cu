@@ -83,10 +83,6 @@ struct sfb_context {
   bool on_device = false;
   int device = 0;
   cudaStream_t stream = nullptr;
-  // second stream and fork / join events: the acoustic stiffness of a
-  // coupled single-shot step runs beside the elastic one
-  cudaStream_t stream2 = nullptr;
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   size_t device_bytes = 0;
   // element permutation: device element d holds mesh element perm[d]
   std::vector<int> perm, inv;
@@ -154,9 +150,6 @@ struct sfb_context {
     if (graph) cudaGraphExecDestroy(graph);
     if (graph_combined) cudaGraphExecDestroy(graph_combined);
     if (stream) cudaStreamDestroy(stream);
-    if (stream2) cudaStreamDestroy(stream2);
-    if (ev_fork) cudaEventDestroy(ev_fork);
-    if (ev_join) cudaEventDestroy(ev_join);
   }
 };
 
@@ -226,9 +219,6 @@ void ensure_device(sfb_context *c) {
     throw CudaError(std::string("no CUDA device available: ") + cudaGetErrorString(e));
   ck(cudaGetDevice(&c->device), "cudaGetDevice");
   ck(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "cudaStreamCreate");
-  ck(cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking), "cudaStreamCreate");
-  ck(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming), "cudaEventCreate");
-  ck(cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming), "cudaEventCreate");
   const Assembly &a = c->P.asmb;
   const int n = a.ngll, nn = n * n;
   const size_t nloc = a.nloc();
@@ -725,33 +715,14 @@ void enqueue_fused_step(sfb_context *c, WavefieldSet &W, int last) {
   ta.cp = coupling_acoustic(c);
   ta.other = W.f[dev::MED_PSV];
   ta.cp_mode = ta.cp.n > 0 ? 1 : 0;
-  // Coupled single shot: the acoustic launch runs on the second stream beside
-  // the elastic one, each with its share of the persistent CTAs; the
-  // elastic <- acoustic coupling, which needs the finished acoustic force,
-  // follows both as its own small launch.
-  const bool side_by_side = S == 1 && n == 5 && W.f[dev::MED_AC].nelem > 0 && W.f[dev::MED_PSV].nelem > 0;
-  int ctas_ac = 0, ctas_el = 0;
-  if (side_by_side) {
-    int nsm = 0;
-    ck(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device), "SM count");
-    const int per_sm = dev::stiffness_ctas_per_sm(dev::MED_PSV, n, c->shots_variant[dev::MED_PSV]);
-    const double w_el = static_cast<double>(W.f[dev::MED_PSV].nelem) * 25 * 36 + 16.0 * W.f[dev::MED_PSV].nglob;
-    const double w_ac = static_cast<double>(W.f[dev::MED_AC].nelem) * 25 * 32 + 8.0 * W.f[dev::MED_AC].nglob;
-    const int total = nsm * per_sm;
-    ctas_ac = std::max(1, static_cast<int>(std::lround(total * w_ac / (w_el + w_ac))));
-    ctas_el = std::max(1, total - ctas_ac);
-    ck(cudaEventRecord(c->ev_fork, c->stream), "fork");
-    ck(cudaStreamWaitEvent(c->stream2, c->ev_fork, 0), "fork");
-  }
-  dev::launch_stiffness(dev::MED_AC, n, c->st, W.f[dev::MED_AC], S, ss, istep, side_by_side ? c->stream2 : c->stream,
-                        &ta, nullptr, c->shots_variant[dev::MED_AC], ctas_ac);
-  if (side_by_side) ck(cudaEventRecord(c->ev_join, c->stream2), "join");
+  dev::launch_stiffness(dev::MED_AC, n, c->st, W.f[dev::MED_AC], S, ss, istep, c->stream, &ta, nullptr,
+                        c->shots_variant[dev::MED_AC]);
   // elastic: coupling reads the final acoustic acceleration = force * minv
   dev::TailWork te{};
   te.src = src;
   te.cp = coupling_elastic(c);
   te.other = W.f[dev::MED_AC];
-  te.cp_mode = (te.cp.n > 0 && !side_by_side) ? 2 : 0;
+  te.cp_mode = te.cp.n > 0 ? 2 : 0;
   te.other_divided = 0;
   dev::FusedUpdate fu{};
   const bool fused = private_update_on(c);
@@ -765,11 +736,7 @@ void enqueue_fused_step(sfb_context *c, WavefieldSet &W, int last) {
     fu.last = last;
   }
   dev::launch_stiffness(dev::MED_PSV, n, c->st, W.f[dev::MED_PSV], S, ss, istep, c->stream, &te,
-                        fused ? &fu : nullptr, c->shots_variant[dev::MED_PSV], ctas_el);
-  if (side_by_side) {
-    ck(cudaStreamWaitEvent(c->stream, c->ev_join, 0), "join");
-    dev::launch_coupling_elastic(coupling_elastic(c), W.f[dev::MED_PSV], W.f[dev::MED_AC], S, 0, c->stream);
-  }
+                        fused ? &fu : nullptr, c->shots_variant[dev::MED_PSV]);
   dev::TailWork tsh{};
   tsh.src = src;
   dev::launch_stiffness(dev::MED_SH, n, c->st, W.f[dev::MED_SH], S, ss, istep, c->stream, &tsh, nullptr,
@@ -784,10 +751,7 @@ int fused_step_launches(sfb_context *c, WavefieldSet &W) {
   int n = 0;
   for (int m : {dev::MED_AC, dev::MED_PSV, dev::MED_SH})
     if (W.f[m].nelem > 0) ++n;  // stiffness (+ sources + coupling)
-  // the separate elastic <- acoustic coupling launch of a coupled single shot
-  if (c->P.nshots == 1 && c->P.asmb.ngll == 5 && W.f[dev::MED_AC].nelem > 0 && W.f[dev::MED_PSV].nelem > 0 &&
-      !c->P.v_cp_el_self.empty())
-    ++n;
+  (void)c;
   return n + 1;                 // one update launch for all media
 }
 

@@ -457,10 +457,11 @@ size_t rp_smem_bytes() {
 }
 
 template <int MED, int N, int EPB, int MINB>
-int rp_blocks_per_sm(int *nsm_out) {
+void launch_rp(const Static &st, const MediumFields &f, int nshots, const StaceyStore &ss, const int *istep_dev,
+               const TailWork &tw, const FusedUpdate &fu, cudaStream_t stream) {
   static int blocks_per_sm = -1, nsm = 0;
+  const size_t smem = rp_smem_bytes<MED, N, EPB>();
   if (blocks_per_sm < 0) {
-    const size_t smem = rp_smem_bytes<MED, N, EPB>();
     cudaFuncSetAttribute(k_stiffness_rp<MED, N, EPB, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          static_cast<int>(smem));
     int dev = 0;
@@ -469,20 +470,8 @@ int rp_blocks_per_sm(int *nsm_out) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_stiffness_rp<MED, N, EPB, MINB>, N * EPB, smem);
     if (blocks_per_sm < 1) blocks_per_sm = 1;
   }
-  if (nsm_out) *nsm_out = nsm;
-  return blocks_per_sm;
-}
-
-template <int MED, int N, int EPB, int MINB>
-void launch_rp(const Static &st, const MediumFields &f, int nshots, const StaceyStore &ss, const int *istep_dev,
-               const TailWork &tw, const FusedUpdate &fu, cudaStream_t stream, int max_ctas) {
-  int nsm = 0;
-  const int blocks_per_sm = rp_blocks_per_sm<MED, N, EPB, MINB>(&nsm);
-  const size_t smem = rp_smem_bytes<MED, N, EPB>();
   const int nchunks = (f.nelem + EPB - 1) / EPB;
-  int cap = nsm * blocks_per_sm;
-  if (max_ctas > 0) cap = std::min(cap, max_ctas);
-  const int grid = std::max(1, std::min(nchunks, cap));
+  const int grid = std::max(1, std::min(nchunks, nsm * blocks_per_sm));
   k_stiffness_rp<MED, N, EPB, MINB><<<grid, N * EPB, smem, stream>>>(st, f, nshots, ss, istep_dev, tw, fu);
 }
 
@@ -1575,17 +1564,9 @@ void launch_stiffness_frechet(int ngll, const Static &st, const MediumFields &f,
                                                                                   fu, fr);
 }
 
-int stiffness_ctas_per_sm(int medium, int ngll, int variant) {
-  if (ngll != 5) return 1;
-  const bool half = variant == kRowHalfChunk;
-  if (medium == MED_PSV) return half ? rp_blocks_per_sm<MED_PSV, 5, 16, 6>(nullptr) : rp_blocks_per_sm<MED_PSV, 5, 32, 3>(nullptr);
-  if (medium == MED_SH) return half ? rp_blocks_per_sm<MED_SH, 5, 16, 6>(nullptr) : rp_blocks_per_sm<MED_SH, 5, 32, 3>(nullptr);
-  return half ? rp_blocks_per_sm<MED_AC, 5, 16, 6>(nullptr) : rp_blocks_per_sm<MED_AC, 5, 32, 3>(nullptr);
-}
-
 void launch_stiffness(int medium, int ngll, const Static &st, const MediumFields &f, int nshots,
                       const StaceyStore &ss, const int *istep_dev, cudaStream_t stream, const TailWork *tw,
-                      const FusedUpdate *fu, int variant, int max_ctas) {
+                      const FusedUpdate *fu, int variant) {
   if (f.nelem == 0) return;
   const TailWork none{};
   const TailWork &w = tw ? *tw : none;
@@ -1608,18 +1589,18 @@ void launch_stiffness(int medium, int ngll, const Static &st, const MediumFields
     // single shot: the row kernel with 32 elements per chunk (variant 0 / 1),
     // or 16 elements per chunk and twice the CTAs per SM (variant 2)
     if (variant == kRowHalfChunk) {
-      if (medium == MED_PSV) launch_rp<MED_PSV, 5, 16, 6>(st, f, nshots, ss, istep_dev, w, u, stream, max_ctas);
-      else if (medium == MED_SH) launch_rp<MED_SH, 5, 16, 6>(st, f, nshots, ss, istep_dev, w, nofu, stream, max_ctas);
-      else launch_rp<MED_AC, 5, 16, 6>(st, f, nshots, ss, istep_dev, w, nofu, stream, max_ctas);
+      if (medium == MED_PSV) launch_rp<MED_PSV, 5, 16, 6>(st, f, nshots, ss, istep_dev, w, u, stream);
+      else if (medium == MED_SH) launch_rp<MED_SH, 5, 16, 6>(st, f, nshots, ss, istep_dev, w, nofu, stream);
+      else launch_rp<MED_AC, 5, 16, 6>(st, f, nshots, ss, istep_dev, w, nofu, stream);
     } else {
-      if (medium == MED_PSV) launch_rp<MED_PSV, 5, 32, 3>(st, f, nshots, ss, istep_dev, w, u, stream, max_ctas);
-      else if (medium == MED_SH) launch_rp<MED_SH, 5, 32, 3>(st, f, nshots, ss, istep_dev, w, nofu, stream, max_ctas);
-      else launch_rp<MED_AC, 5, 32, 3>(st, f, nshots, ss, istep_dev, w, nofu, stream, max_ctas);
+      if (medium == MED_PSV) launch_rp<MED_PSV, 5, 32, 3>(st, f, nshots, ss, istep_dev, w, u, stream);
+      else if (medium == MED_SH) launch_rp<MED_SH, 5, 32, 3>(st, f, nshots, ss, istep_dev, w, nofu, stream);
+      else launch_rp<MED_AC, 5, 32, 3>(st, f, nshots, ss, istep_dev, w, nofu, stream);
     }
   } else if (ngll == 8) {
-    if (medium == MED_PSV) launch_rp<MED_PSV, 8, 16, 2>(st, f, nshots, ss, istep_dev, w, u, stream, max_ctas);
-    else if (medium == MED_SH) launch_rp<MED_SH, 8, 16, 2>(st, f, nshots, ss, istep_dev, w, nofu, stream, max_ctas);
-    else launch_rp<MED_AC, 8, 16, 2>(st, f, nshots, ss, istep_dev, w, nofu, stream, max_ctas);
+    if (medium == MED_PSV) launch_rp<MED_PSV, 8, 16, 2>(st, f, nshots, ss, istep_dev, w, u, stream);
+    else if (medium == MED_SH) launch_rp<MED_SH, 8, 16, 2>(st, f, nshots, ss, istep_dev, w, nofu, stream);
+    else launch_rp<MED_AC, 8, 16, 2>(st, f, nshots, ss, istep_dev, w, nofu, stream);
   }
 }
 

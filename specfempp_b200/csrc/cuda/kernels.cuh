@@ -211,10 +211,7 @@ constexpr int kRowFullChunk = 1, kRowHalfChunk = 2;
 void launch_stiffness(int medium, int ngll, const Static &st, const MediumFields &f,
                       int nshots, const StaceyStore &ss, const int *istep_dev,
                       cudaStream_t stream, const TailWork *tw = nullptr,
-                      const FusedUpdate *fu = nullptr, int variant = kShotsAuto, int max_ctas = 0);
-// CTAs per SM of the single-shot stiffness kernel `variant` uses for `medium`
-// (its persistent grid is SMs x this; max_ctas above caps it).
-int stiffness_ctas_per_sm(int medium, int ngll, int variant);
+                      const FusedUpdate *fu = nullptr, int variant = kShotsAuto);
 // True when launch_stiffness_frechet applies (P-SV, even nshots > 1, NGLL 5).
 bool frechet_fusable(int medium, int ngll, int nshots);
 // Backward stiffness of the batched P-SV medium with the Frechet kernels
