@@ -205,3 +205,23 @@ def test_kahan_compensated_batched_forward():
     sim = Simulation.structured(p)
     sim.set_newmark_compensation(True)
     check(sim, "batched compensated", shots=range(2))
+
+
+@pytest.mark.parametrize("nshots", [1, 2])
+def test_gll7_elastic_sh_acoustic(nshots):
+    """NGLL = 8 (GLL7) kernels: the single-shot row kernel with 16-element
+    chunks and the one-shot-per-lane batched kernel, P-SV, SH and acoustic."""
+    for label, sh, vs, types in (("P-SV", False, 1732.0, ("displacement", "velocity")),
+                                 ("SH", True, 1732.0, ("displacement",)),
+                                 ("acoustic", False, 0.0, ("pressure",))):
+        p = small_elastic(sh=sh, nstep=250, types=types)
+        p.ngll = 8
+        p.nx, p.nz = 10, 8
+        p.x1, p.z1 = 10 * 80.0, 8 * 75.0
+        p.materials = [Material(2700.0 if vs else 1020.0, 3000.0 if vs else 1500.0, vs)]
+        p.dt = 2.5e-4
+        p.nshots = nshots
+        p.sources = [ForceSource(x=300.0 + 200.0 * s, z=300.0, f0=10.0 if vs else 6.0, factor=1e10, shot=s)
+                     for s in range(nshots)]
+        p.stations = [Station(x=100.0 + 150.0 * k, z=500.0) for k in range(4)]
+        check(Simulation.structured(p), "GLL7 %s S=%d" % (label, nshots), shots=range(nshots))
