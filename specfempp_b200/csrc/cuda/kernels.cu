@@ -272,10 +272,13 @@ k_stiffness_rp(Static st, MediumFields f, int nshots, StaceyStore ss, const int 
     // element-private points of this row (single shot): their velocity is
     // needed after the divergence, so fetch it now
     const bool fused = fu.enabled && nshots == 1 && (eflag & kElemPrivate) && iz >= 1 && iz <= N - 2;
-    V vp[N - 2];
+    V vp[N - 2], mp[N - 2];
     if (fused) {
 #pragma unroll
-      for (int ix = 1; ix <= N - 2; ++ix) vp[ix - 1] = reinterpret_cast<const V *>(fu.v)[g[ix]];
+      for (int ix = 1; ix <= N - 2; ++ix) {
+        vp[ix - 1] = reinterpret_cast<const V *>(fu.v)[g[ix]];
+        mp[ix - 1] = reinterpret_cast<const V *>(fu.minv)[g[ix]];
+      }
     }
     for (int s = 0; s < nshots; ++s) {
       if (s > 0) {
@@ -406,7 +409,7 @@ k_stiffness_rp(Static st, MediumFields f, int nshots, StaceyStore ss, const int 
             V vel = vp[ix - 1], uu = ur[ix], aa;
 #pragma unroll
             for (int c = 0; c < NC; ++c) {
-              const float a_c = accr[ix][c] * fu.minv[g[ix] * NC + c];
+              const float a_c = accr[ix][c] * comp(mp[ix - 1], c);
               set_comp(aa, c, a_c);
               set_comp(vel, c, comp(vel, c) + fu.dt2 * a_c);
             }
