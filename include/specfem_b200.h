@@ -212,6 +212,13 @@ SFB_API int sfb_run_combined(sfb_context *ctx, int nstep, int use_graph);
 
 /* ---- data movement ------------------------------------------------------ */
 
+/* The combined loop's overwrite of the backward wavefield with the forward
+ * "buffer" after its first backward step (time_marching.tpp:198-204), for a
+ * host loop driving the domain_* entry points: copies this context's forward
+ * wavefield (the forward run's final state, or one read back with
+ * sfb_read_wavefield) into its backward wavefield. */
+SFB_API int sfb_load_backward_from_forward(sfb_context *ctx);
+
 /* Seismograms [max_sig_step][ntypes][nreceivers][2] per shot, in the
  * reference's receiver frame after the angle rotation; `shot` selects the
  * wavefield copy.  count = number of floats the buffer holds. */

@@ -142,6 +142,7 @@ SIGNATURES = {
     "sfb_set_newmark_compensation": (C.c_int, [_ctx, C.c_int]),
     "sfb_set_checkpoint_interval": (C.c_int, [_ctx, C.c_int]),
     "sfb_write_wavefield": (C.c_int, [_ctx, C.c_int, C.c_char_p]),
+    "sfb_load_backward_from_forward": (C.c_int, [_ctx]),
     "sfb_read_wavefield": (C.c_int, [_ctx, C.c_int, C.c_char_p]),
     "sfb_write_kernels": (C.c_int, [_ctx, C.c_char_p, C.c_int]),
     "sfb_execute": (C.c_int, [C.c_char_p, C.c_char_p]),

@@ -810,6 +810,15 @@ void run_forward_fused(sfb_context *c, int nstep, int use_graph) {
   W.step += nstep;
 }
 
+dev::SourceSet adjoint_source_set(sfb_context *c);
+void ensure_adjoint_sources(sfb_context *c);
+dev::StaceyStore replay_store(sfb_context *c);
+void ensure_store(sfb_context *c);
+
+// domain_kernels<W>::update_wavefields<medium>(istep): coupling, sources
+// (forward and backward: the forward sources; adjoint: the adjoint sources),
+// stiffness (forward: storing the Stacey elements' contributions when
+// save_boundary_values; backward: replaying them), divide by mass.
 int update_wavefields(sfb_context *c, int w, int medium, int istep) {
   WavefieldSet &W = ensure_wavefield(c, w);
   const Problem &P = c->P;
@@ -817,13 +826,24 @@ int update_wavefields(sfb_context *c, int w, int medium, int istep) {
   set_step(c, W, istep);
   const int *is = &W.ctrl.p->istep;
   dev::StaceyStore ss{};
-  dev::SourceSet src = source_set(c);
+  if (w == SFB_WAVEFIELD_FORWARD && P.save_boundary_values && c->nstacey > 0) {
+    ensure_store(c);
+    ss.data = c->stacey_data.p;
+    ss.slot = c->stacey_slot.p;
+    ss.nstacey = c->nstacey;
+    ss.nstep = P.nstep;
+    ss.mode = 1;
+  } else if (w == SFB_WAVEFIELD_BACKWARD) {
+    ss = replay_store(c);
+  }
+  if (w == SFB_WAVEFIELD_ADJOINT) ensure_adjoint_sources(c);
+  dev::SourceSet src = w == SFB_WAVEFIELD_ADJOINT ? adjoint_source_set(c) : source_set(c);
   if (medium == dev::MED_AC) {
     dev::launch_coupling_acoustic(coupling_acoustic(c), W.f[dev::MED_AC], W.f[dev::MED_PSV], S, c->stream);
   } else if (medium == dev::MED_PSV) {
     dev::launch_coupling_elastic(coupling_elastic(c), W.f[dev::MED_PSV], W.f[dev::MED_AC], S, 1, c->stream);
   }
-  if (w != SFB_WAVEFIELD_ADJOINT) dev::launch_sources(n, c->st, src, W.f, S, medium, is, 0, c->stream);
+  dev::launch_sources(n, c->st, src, W.f, S, medium, is, 0, c->stream);
   dev::launch_stiffness(medium, n, c->st, W.f[medium], S, ss, is, c->stream, nullptr, nullptr,
                         c->shots_variant[medium]);
   dev::launch_divide(W.f[medium], S, c->stream);
@@ -1762,6 +1782,17 @@ SFB_API int sfb_get_kernels(const sfb_context *cctx, int which, double *host, si
         host[p] = v;
       }
     }
+    return SFB_OK;
+  });
+}
+
+SFB_API int sfb_load_backward_from_forward(sfb_context *ctx) {
+  if (!ctx) return SFB_E_INVALID;
+  return guarded(ctx, [&]() {
+    WavefieldSet &F = ensure_wavefield(ctx, SFB_WAVEFIELD_FORWARD);
+    WavefieldSet &B = ensure_wavefield(ctx, SFB_WAVEFIELD_BACKWARD);
+    copy_fields(ctx, B, F);
+    ck(cudaStreamSynchronize(ctx->stream), "copy");
     return SFB_OK;
   });
 }

@@ -177,3 +177,50 @@ def test_acoustic_kernels_match_oracle():
         print("acoustic kernel %d: vs FP32 %.2e vs FP64 %.2e (FP32 oracle vs FP64 %.2e)" % (which, e32, e64, eref))
         assert np.abs(g).max() > 0
         assert kernel_ok(e32, e64, eref), (which, e32, e64, eref)
+
+
+def test_reference_granularity_combined_loop():
+    """time_marching<combined>::run (time_marching.tpp:126-247) driven from
+    the host through the domain_kernels / newmark / frechet_kernels entry
+    points, as the reference's own loop would call them, after the fused
+    forward run: its kernels meet the kernel bar against the oracle."""
+    import ctypes as C
+    from specfempp_b200 import _capi as A
+    absorb = (True, True, False, True)
+    p, model, XZ = base_model(nstep=NSTEP)
+    obs = observed(anomaly(model, XZ, p), NSTEP, absorb)
+    sim = Simulation.structured(problem(model, NSTEP, absorb))
+    sim.run_forward()
+    stf = (sim.seismograms()[:, 0].astype(np.float64) - obs[0]).astype(np.float32)
+    sim.set_adjoint_sources(stf)
+    lib, h, dt = A.load(), sim.handle, sim.info().dt
+    ADJ, BWD, PSV, AC = 1, 2, 0, 3
+    n = C.c_int()
+
+    def call(rc):
+        A.check(rc, h)
+
+    for w in (ADJ, BWD):
+        call(lib.sfb_domain_initialize(h, w, dt))
+    for istep in range(NSTEP - 1, -1, -1):
+        for m in (AC, PSV):
+            call(lib.sfb_newmark_predictor(h, ADJ, m, C.byref(n)))
+        for m in (AC, PSV):
+            call(lib.sfb_domain_update_wavefields(h, ADJ, m, istep, C.byref(n)))
+            call(lib.sfb_newmark_corrector(h, ADJ, m, C.byref(n)))
+        for m in (PSV, AC):
+            call(lib.sfb_newmark_predictor(h, BWD, m, C.byref(n)))
+        for m in (PSV, AC):
+            call(lib.sfb_domain_update_wavefields(h, BWD, m, istep, C.byref(n)))
+            call(lib.sfb_newmark_corrector(h, BWD, m, C.byref(n)))
+        if istep == NSTEP - 1:
+            call(lib.sfb_load_backward_from_forward(h))
+        call(lib.sfb_frechet_compute_derivatives(h, dt))
+    K = np.stack([sim.kernels(0), sim.kernels(1), sim.kernels(2)], axis=-1)
+    o32 = oracle_kernels(sim, [stf], 32)
+    o64 = oracle_kernels(sim, [stf], 64)
+    for c, name in enumerate(("rho", "mu", "kappa")):
+        e32, e64, eref = rel_l2(K[..., c], o32[..., c]), rel_l2(K[..., c], o64[..., c]), rel_l2(o32[..., c], o64[..., c])
+        print("host-driven combined loop, kernel %s: vs FP32 %.2e vs FP64 %.2e (FP32 oracle vs FP64 %.2e)"
+              % (name, e32, e64, eref))
+        assert kernel_ok(e32, e64, eref), (name, e32, e64, eref)
