@@ -264,7 +264,7 @@ def fwi_comparison(nshots=64, nstep=400, reps=2):
     }
 
 
-def cpu_rate(workload, nstep_hint, threads, budget_s=12.0, sample_steps=None):
+def cpu_rate(workload, nstep_hint, threads, budget_s=15.0, sample_steps=None):
     """GLL point updates/s of the oracle (FP32 CPU restatement) on the host cores."""
     from oracle import bridge
     from specfempp_b200 import Simulation
@@ -274,7 +274,7 @@ def cpu_rate(workload, nstep_hint, threads, budget_s=12.0, sample_steps=None):
     t = time.perf_counter()
     bridge.forward(sim, 32, nstep=probe, threads=threads)
     per_step = (time.perf_counter() - t) / probe
-    n = sample_steps or max(4, min(400, int(budget_s / max(per_step, 1e-6))))
+    n = sample_steps or max(4, min(5000, int(budget_s / max(per_step, 1e-6))))
     p = make_problem(workload, n)
     sim = Simulation.structured(p)
     info = sim.info()
@@ -452,7 +452,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="coupled", choices=["coupled", "plain", "batched"])
-    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0,
+                    help="length of the timed CPU-baseline sample (about 10-30 s of CPU work)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-secondary", action="store_true",
                     help="skip the batched-forward and batched-vs-single adjoint measurements")
