@@ -9,7 +9,13 @@
  * for.  All entry points return 0 on success and a negative SFB_E* code on
  * failure; sfb_last_error() gives the message.  Buffers passed in are
  * caller-owned host memory; device memory is owned by the context.  One
- * context = one CUDA stream; a context is not thread-safe.
+ * context = one CUDA stream; a context is not thread-safe.  A context lives
+ * on the CUDA device current when it first touches the GPU; the library
+ * keeps per-process launch settings (SM count, occupancy) of the first
+ * device it sees, so use one process per GPU (the multi-GPU layout of this
+ * library).  Work on a context is asynchronous on its stream except where an
+ * entry point says it returns host data; the run drivers synchronise before
+ * they return.
  *
  * Integer tags equal the reference's enum ordinals:
  *   medium   (include/enumerations/medium.hpp:39):  0 elastic_psv,
