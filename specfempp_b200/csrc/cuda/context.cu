@@ -991,6 +991,14 @@ void enqueue_backward_stiffness(sfb_context *c, WavefieldSet &A, WavefieldSet &B
     fr.minv = c->minv[dev::MED_PSV].p;
     fr.kern = c->kern.p;
     fr.dt = static_cast<float>(c->P.dt);
+    if (backward_private_on(c)) {
+      fr.adjoint_update = 1;
+      fr.av = A.f[dev::MED_PSV].v;
+      fr.adt = static_cast<float>(c->P.dt);
+      fr.adt2 = static_cast<float>(c->P.dt / 2.0);
+      fr.adtsq2 = static_cast<float>(c->P.dt * c->P.dt / 2.0);
+      fr.last = last;
+    }
     dev::FusedUpdate fu{};
     if (backward_private_on(c)) {
       fu.enabled = 1;
@@ -1058,7 +1066,8 @@ void enqueue_combined_step(sfb_context *c, WavefieldSet &A, WavefieldSet &B, int
   enqueue_adjoint_stiffness(c, A);
   enqueue_backward_stiffness(c, A, B, last);
   enqueue_frechet(c, A, B.f, 1, frechet_fused(c));
-  dev::UpdateParams ua = update_params_signed(c, A, last, false, false, 1.0);
+  // with the fused Frechet launch, both wavefields' private points are done
+  dev::UpdateParams ua = update_params_signed(c, A, last, false, false, 1.0, backward_private_on(c));
   dev::launch_update_all(ua, c->stream);
   // the backward update records the backward seismograms and counts the
   // shared step counter (held by the adjoint set) down

@@ -712,6 +712,9 @@ __device__ __forceinline__ void setpr(float2 &w, int, float2 v) { w = v; }
 // memory order <-> pair order (an involution)
 __device__ __forceinline__ float4 swz(const float4 &w) { return make_float4(w.x, w.z, w.y, w.w); }
 __device__ __forceinline__ float2 swz(const float2 &w) { return w; }
+template <typename W> __device__ __forceinline__ W make_zero_w();
+template <> __device__ __forceinline__ float4 make_zero_w<float4>() { return make_float4(0.f, 0.f, 0.f, 0.f); }
+template <> __device__ __forceinline__ float2 make_zero_w<float2>() { return make_float2(0.f, 0.f); }
 
 // Per-thread asynchronous global -> shared copies (cp.async, no multicast):
 // each thread later reads back only what it copied itself, after
@@ -742,7 +745,8 @@ k_stiffness_pk(Static st, MediumFields f, int S, StaceyStore ss, const int *iste
   extern __shared__ float4 s_dyn[];
   W *s_ua = reinterpret_cast<W *>(s_dyn);
   W *s_aa = reinterpret_cast<W *>(s_dyn + (FR ? NN * 32 : 0));
-  float *s_red = reinterpret_cast<float *>(s_dyn + (FR ? 2 * NN * 32 : 0));
+  W *s_av = reinterpret_cast<W *>(s_dyn + (FR ? 2 * NN * 32 : 0));  // adjoint v of private points
+  float *s_red = reinterpret_cast<float *>(s_dyn + (FR ? 2 * NN * 32 + (N - 2) * (N - 2) * 32 : 0));
   const int lane = threadIdx.x & 31, iz = threadIdx.x >> 5;
   const int e = f.elem_begin + blockIdx.x;
   const int s0 = (blockIdx.y * 32 + lane) * 2;
@@ -765,11 +769,19 @@ k_stiffness_pk(Static st, MediumFields f, int S, StaceyStore ss, const int *iste
       cp_async<sizeof(W)>(&s_vp[((iz - 1) * (N - 2) + ix - 1) * 32 + lane],
                           reinterpret_cast<const W *>(fu.v) + g[ix] * Sv + lofs);
   }
+  bool fused_adj = false;
   if constexpr (FR) {
+    fused_adj = fr.adjoint_update && (eflag & kElemPrivate) && iz >= 1 && iz <= N - 2;
     if (act) {
 #pragma unroll
       for (int ix = 0; ix < N; ++ix)
         cp_async<sizeof(W)>(&s_aa[(iz * N + ix) * 32 + lane], reinterpret_cast<const W *>(fr.aa) + g[ix] * Sv + lofs);
+      if (fused_adj) {
+#pragma unroll
+        for (int ix = 1; ix <= N - 2; ++ix)
+          cp_async<sizeof(W)>(&s_av[((iz - 1) * (N - 2) + ix - 1) * 32 + lane],
+                              reinterpret_cast<const W *>(fr.av) + g[ix] * Sv + lofs);
+      }
     }
   }
   W ur[N];
@@ -985,6 +997,36 @@ k_stiffness_pk(Static st, MediumFields f, int S, StaceyStore ss, const int *iste
     }
     if (!act) continue;
     const size_t at = g[ix] * Sv + lofs;
+    if constexpr (FR && MED == MED_PSV) {
+      if (fused_adj && ix >= 1 && ix <= N - 2) {
+        // the adjoint wavefield's private point: its Frechet contribution
+        // was taken above; now a = force / M, corrector, next predictor
+        W va = swz(s_av[((iz - 1) * (N - 2) + ix - 1) * 32 + lane]), ua = s_ua[(iz * N + ix) * 32 + lane], aa;
+        const W fa = swz(s_aa[(iz * N + ix) * 32 + lane]);
+        const float2 adt = make_float2(fr.adt, fr.adt), adt2 = make_float2(fr.adt2, fr.adt2);
+        const float2 adtsq2 = make_float2(fr.adtsq2, fr.adtsq2);
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+          const float mi = fr.minv[g[ix] * NC + c];
+          const float2 a_c = mul2(pr(fa, c), make_float2(mi, mi));
+          setpr(aa, c, a_c);
+          setpr(va, c, fma2(adt2, a_c, pr(va, c)));
+        }
+        if (fr.last) {
+          reinterpret_cast<W *>(fr.aa)[at] = swz(aa);
+          reinterpret_cast<W *>(fr.av)[at] = swz(va);
+        } else {
+#pragma unroll
+          for (int c = 0; c < NC; ++c) {
+            setpr(ua, c, add2(pr(ua, c), fma2(adt, pr(va, c), mul2(adtsq2, pr(aa, c)))));
+            setpr(va, c, fma2(adt2, pr(aa, c), pr(va, c)));
+          }
+          reinterpret_cast<W *>(fr.au)[at] = swz(ua);
+          reinterpret_cast<W *>(fr.av)[at] = swz(va);
+          reinterpret_cast<W *>(fr.aa)[at] = swz(make_zero_w<W>());
+        }
+      }
+    }
     if (fused && ix >= 1 && ix <= N - 2) {
       // element-private point: a = force / M, corrector, next predictor
       // (the update kernel's arithmetic, newmark.tpp:44-47 and 98-105)
@@ -1043,7 +1085,7 @@ void launch_shots(const Static &st, const MediumFields &f, int S, const StaceySt
   k_stiffness_shots<MED, N, 1, MINB><<<grid, N * 32, 0, stream>>>(st, f, S, ss, istep_dev, tw, fu);
 }
 
-constexpr size_t kFrechetDynSmem = 2 * (25 * 32) * sizeof(float4) + 3 * 25 * 32 * sizeof(float);
+constexpr size_t kFrechetDynSmem = (2 * 25 + 9) * 32 * sizeof(float4) + 3 * 25 * 32 * sizeof(float);
 
 
 // ---------------------------------------------------------------------------

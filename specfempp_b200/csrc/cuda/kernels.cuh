@@ -163,11 +163,17 @@ constexpr uint8_t kElemPrivate = 4;
 // kernels, summed over the launch's shots, to kern[p][3] (FP64).
 struct FrechetFuse {
   int enabled;
-  const float *au;     // adjoint displacement [g][S][2]
-  const float *aa;     // adjoint force [g][S][2] (times minv = acceleration)
+  float *au;           // adjoint displacement [g][S][2]
+  float *aa;           // adjoint force [g][S][2] (times minv = acceleration)
   const float *minv;   // [nglob][2]
   double *kern;        // [nspec * N * N][3]: rho, mu, kappa
   float dt;
+  // the adjoint wavefield's element-private points also finish their (+dt)
+  // Newmark step here, after their Frechet contribution is taken
+  int adjoint_update;
+  float *av;           // adjoint velocity [g][S][2]
+  float adt, adt2, adtsq2;
+  int last;
 };
 
 struct UpdateParams {
