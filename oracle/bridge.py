@@ -40,6 +40,9 @@ def load():
         lib.oracle_combined.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int,
                                         C.POINTER(C.c_float), C.POINTER(C.POINTER(C.c_float)),
                                         C.POINTER(C.c_float), C.POINTER(C.c_double), C.POINTER(C.c_float)]
+        lib.oracle_seismograms.restype = C.c_int
+        lib.oracle_seismograms.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.POINTER(C.c_double)),
+                                           C.POINTER(C.c_float)]
         lib.oracle_last_error.restype = C.c_char_p
         _lib = lib
     return _lib
@@ -83,6 +86,31 @@ def forward(sim, precision: int = 32, shot: int = 0, nstep=None, threads: int = 
     if store is not None:
         out["stacey_store"] = store
     return out
+
+
+def seismograms(sim, fields, precision: int = 64):
+    """Seismograms of given fields (one record, [ntypes][nrec][2]), as the
+    reference's compute_seismograms(0) on a loaded wavefield.  ``fields``
+    maps ``psv`` / ``sh`` / ``acoustic`` to (u, v, a) arrays [nc][nglob] in
+    this library's numbering; missing media are zero."""
+    lib = load()
+    view = sim.problem_view()
+    info = sim.info()
+    ptrs = (C.POINTER(C.c_double) * 9)()
+    keep = []
+    k = 0
+    for name in ("psv", "sh", "acoustic"):
+        for which in range(3):
+            if name in fields:
+                a = np.ascontiguousarray(fields[name][which], dtype=np.float64)
+                keep.append(a)
+                ptrs[k] = a.ctypes.data_as(C.POINTER(C.c_double))
+            k += 1
+    seis = np.zeros((info.nseismogram_types, info.nreceivers, 2), dtype=np.float32)
+    rc = lib.oracle_seismograms(C.addressof(view), precision, ptrs, seis.ctypes.data_as(C.POINTER(C.c_float)))
+    if rc != 0:
+        raise RuntimeError("oracle failed: " + lib.oracle_last_error().decode())
+    return seis
 
 
 def combined(sim, adjoint_stf, fwd, precision: int = 64, shot: int = 0, threads: int = 1,

@@ -660,4 +660,33 @@ int oracle_combined(const sfb_problem_view *pv, int precision, int shot, int nst
   }
 }
 
+// Seismograms of given fields, one record: what compute_seismograms(0) gives
+// on a wavefield loaded from files (the reference's seismogram unit tests,
+// tests/unit-tests/seismogram/*/seismogram_tests.cpp).  fields_in: 9
+// pointers (u, v, a for P-SV, SH, acoustic; [ncomp][nglob] doubles, NULL =
+// zero); seis: [ntypes][nrec][2].
+int oracle_seismograms(const sfb_problem_view *pv, int precision, const double *const *fields_in, float *seis) {
+  auto run = [&](auto zero) -> int {
+    using T = decltype(zero);
+    Sim<T> s(*pv, 0);
+    int k = 0;
+    for (int m : {PSV, SH, ACOUSTIC}) {
+      for (auto *vec : {&s.f[m].u, &s.f[m].v, &s.f[m].a}) {
+        const double *src = fields_in[k++];
+        if (src)
+          for (size_t i = 0; i < vec->size(); ++i) (*vec)[i] = static_cast<T>(src[i]);
+      }
+    }
+    s.seismograms(seis, 0);
+    return 0;
+  };
+  try {
+    if (pv->ngll > 8) throw std::invalid_argument("ngll > 8");
+    return precision == 64 ? run(0.0) : run(0.0f);
+  } catch (const std::exception &e) {
+    g_err = e.what();
+    return -1;
+  }
+}
+
 }  // extern "C"

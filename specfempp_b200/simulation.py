@@ -207,6 +207,11 @@ class Simulation:
             nstep = self.info().nstep
         self._check(self._lib.sfb_run_forward_unfused(self._h, nstep))
 
+    def compute_seismograms(self, isig_step: int = 0, wavefield: int = 0):
+        """Record seismogram sample `isig_step` of the current fields
+        (``domain_kernels::compute_seismograms``)."""
+        self._check(self._lib.sfb_domain_compute_seismograms(self._h, wavefield, isig_step))
+
     def seismograms(self, wavefield: int = 0, shot: int = 0) -> np.ndarray:
         i = self.info()
         out = np.zeros((i.max_sig_step, i.nseismogram_types, i.nreceivers, 2), dtype=np.float32)
