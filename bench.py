@@ -51,7 +51,9 @@ VARIANT = 0  # batched stiffness kernel (0: autotuned; see sfb_set_stiffness_var
 
 
 def pin_variant(sim):
-    if VARIANT:
+    """Pin the stiffness kernel of every medium; variant 4 (compact block,
+    16-element chunks) exists for single-shot contexts only."""
+    if VARIANT and not (VARIANT == 4 and sim.info().nshots > 1):
         for medium in (0, 1, 3):
             sim.set_stiffness_variant(medium, VARIANT)
 
@@ -77,6 +79,9 @@ def workload_config(workload, info, p):
         "nshots": int(info.nshots),
         "dt": float(info.dt),
         "receivers": int(info.nreceivers),
+        "stiffness_variant": {name: int(info.stiffness_variant[m])
+                              for name, m in (("elastic_psv", 0), ("elastic_sh", 1), ("acoustic", 3))
+                              if info.nelements[m] > 0},
     }
 
 
@@ -136,40 +141,52 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def profiled_traffic(name):
-    """DRAM bytes per launch of the dominant kernel from the committed ncu summary."""
+def profiled_traffic(name, variant):
+    """DRAM bytes per launch of the dominant kernel, stiffness `variant`, from
+    the committed ncu summary (null when that variant was not captured)."""
     path = os.path.join(ROOT, "profiles", name)
+    key = "dram_bytes_per_launch_full_size[variant %d]:" % variant
     try:
         for line in open(path):
-            if line.startswith("dram_bytes_per_launch_full_size:"):
+            if line.startswith(key):
                 return float(line.split(":")[1])
     except OSError:
         pass
     return None
 
 
+def affine_block(info, medium):
+    """True when the single-shot stiffness of `medium` reads the compact block
+    of affine elements (variants 3 and 4): geometry per element, not per point."""
+    return info.nshots == 1 and info.stiffness_variant[medium] in (3, 4)
+
+
+def static_bytes(info, medium, P):
+    """Static words of one launch over `medium`: per local point 4 (global
+    index) + 4 * P (material; P = 3 elastic, 2 acoustic) and the geometry,
+    4 * 5 per local point, or 4 * 5 per element with the compact block."""
+    nel, nn = info.nelements[medium], info.ngll * info.ngll
+    geometry = nel * 20 if affine_block(info, medium) else nel * nn * 20
+    return nel * nn * (4 + 4 * P) + geometry
+
+
 def stiffness_bytes(info, problem_view, medium):
-    """Algorithmic bytes of one stiffness launch of `medium`: per local point
-    4 (global index) + 4 * 5 (geometry) + 4 * P (material; P = 3 elastic,
-    2 acoustic), plus one read of the displacement and one write of the force
-    per shot and DOF."""
-    nel = info.nelements[medium]
-    nn = info.ngll * info.ngll
+    """Algorithmic bytes of one stiffness launch of `medium`: the static words
+    plus one read of the displacement and one write of the force per shot and
+    DOF."""
     P = 3 if medium in (0, 1) else 2
     C = 2 if medium == 0 else 1
-    return nel * nn * (4 + 4 * 5 + 4 * P) + info.nshots * info.nglob[medium] * C * 4 * 2
+    return static_bytes(info, medium, P) + info.nshots * info.nglob[medium] * C * 4 * 2
 
 
 def step_bytes(info):
-    """Algorithmic HBM bytes of one whole time step: per local point the
-    static block (4 index + 4 * 5 geometry + 4 * P material), per global
-    point the inverse mass (4 C), and per shot and global point 28 C bytes
-    (displacement read by the stiffness; u, v, a read and written by the
-    update)."""
-    nn = info.ngll * info.ngll
+    """Algorithmic HBM bytes of one whole time step: the static words of every
+    medium, per global point the inverse mass (4 C), and per shot and global
+    point 28 C bytes (displacement read by the stiffness; u, v, a read and
+    written by the update)."""
     total = 0
     for m, (P, C) in ((0, (3, 2)), (1, (3, 1)), (3, (2, 1))):
-        total += info.nelements[m] * nn * (4 + 20 + 4 * P) + info.nglob[m] * 4 * C
+        total += static_bytes(info, m, P) + info.nglob[m] * 4 * C
         total += info.nshots * info.nglob[m] * 28 * C
     return total
 
@@ -401,7 +418,7 @@ def run_ours(args):
     bytes_launch = stiffness_bytes(info, view, dominant)
     achieved = bytes_launch / (mean_ms.value / 1000.0) / 1e9
     peak, peak_kind = measured_peak()
-    traffic = profiled_traffic("stiffness_%s.txt" % args.workload)
+    traffic = profiled_traffic("stiffness_%s.txt" % args.workload, info.stiffness_variant[dominant])
 
     if rank != 0:
         if world > 1:
@@ -459,9 +476,9 @@ def main():
                     help="skip the batched-forward and batched-vs-single adjoint measurements")
     ap.add_argument("--scale", type=float, default=1.0,
                     help="shrink the workload's element counts (profiling captures); 1 = full size")
-    ap.add_argument("--stiffness-variant", type=int, default=0, choices=[0, 1, 2, 3],
-                    help="pin the batched stiffness kernel (profiling: the autotuner's timings are "
-                         "distorted under a profiler); 0 = autotuned")
+    ap.add_argument("--stiffness-variant", type=int, default=0, choices=[0, 1, 2, 3, 4],
+                    help="pin the stiffness kernel (sfb_set_stiffness_variant; profiling: the autotuner's "
+                         "timings are distorted under a profiler); 0 = autotuned")
     ap.add_argument("--fwi-only", action="store_true",
                     help="only the batched-vs-single forward + adjoint comparison, over --steps time steps")
     args = ap.parse_args()

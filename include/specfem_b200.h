@@ -15,7 +15,10 @@
  * device it sees, so use one process per GPU (the multi-GPU layout of this
  * library).  Work on a context is asynchronous on its stream except where an
  * entry point says it returns host data; the run drivers synchronise before
- * they return.
+ * they return.  The time-step kernels are launched with programmatic
+ * dependent launch (each waits on its predecessor in the stream before
+ * touching a field); the environment variable SFB_PROGRAMMATIC_LAUNCH=0,
+ * read once per process, selects plain stream order instead.
  *
  * Integer tags equal the reference's enum ordinals:
  *   medium   (include/enumerations/medium.hpp:39):  0 elastic_psv,
@@ -137,19 +140,22 @@ typedef struct sfb_info {
   int stiffness_variant[4]; /* stiffness kernel per medium tag, 0 not chosen
                                yet; nshots > 1: 1 two shots per lane in packed
                                FP32x2, 2 two shots per lane scalar, 3 one shot
-                               per lane; nshots == 1 (NGLL 5): 1 row kernel
-                               with 32-element chunks, 2 with 16             */
+                               per lane; nshots == 1: 1 row kernel with
+                               32-element chunks, 2 with 16 (NGLL 5), 3 and
+                               4 the same reading the compact static block
+                               of a medium whose elements are all affine    */
   int private_points;    /* P-SV points updated inside the batched stiffness
                             launch of the forward run (0: none)             */
   int nadjoint_sources;  /* adjoint sources given in the sources file        */
 } sfb_info;
 SFB_API int sfb_get_info(const sfb_context *ctx, sfb_info *info);
 
-/* Batched stiffness kernel of `medium` (values of sfb_info.stiffness_variant;
+/* Stiffness kernel of `medium` (values of sfb_info.stiffness_variant;
  * 0 = let the autotuner choose).  The autotuner runs once, when the forward
  * fields are first allocated, and times every variant on this mesh; a
- * variant set before that is kept.  No reference counterpart (the
- * reference's chunk size is a compile-time constant). */
+ * variant set before that is kept (a compact-block variant on a medium that
+ * is not all affine becomes the full-block one).  No reference counterpart
+ * (the reference's chunk size is a compile-time constant). */
 SFB_API int sfb_set_stiffness_variant(sfb_context *ctx, int medium, int variant);
 
 /* Kahan-compensated Newmark sums (enable != 0) in the fused forward driver

@@ -93,6 +93,7 @@ struct sfb_context {
   DBuf<uint8_t> eflag, bnd;
   DBuf<float> bnd_nx, bnd_nz, bnd_w;
   DBuf<float> pack;  // [nspec][8][N*N] static block for the TMA-fed stiffness kernel
+  DBuf<float> pack_aff;  // compact block of affine elements (single-shot contexts)
   DBuf<int> dflag;   // device error flag
   DBuf<float> minv[4];
   DBuf<double> mass[4];
@@ -288,6 +289,53 @@ void ensure_device(sfb_context *c) {
     }
   size_t *tot = &c->device_bytes;
   c->pack.upload(pack, tot);
+  // Compact block for media whose elements are all affine (the Jacobian
+  // matrix and determinant constant over the element to 4e-7 relative, i.e.
+  // equal up to rounding): the single-shot row kernel then streams the
+  // per-point index and material and five constants per element instead of
+  // five geometry words per point.  Batched contexts read the static block
+  // once per element for all shots and keep the full block only.
+  if (c->P.nshots == 1) {
+    const int words = dev::affine_pack_words(n);
+    std::vector<float> aff;
+    for (int m : kMedia) {
+      if (c->med_count[m] == 0) continue;
+      bool all = true;
+      for (int d = c->med_begin[m]; all && d < c->med_begin[m] + c->med_count[m]; ++d) {
+        const size_t q0 = static_cast<size_t>(d) * nn;
+        const double scale = std::max(std::max(std::fabs(xix[q0]), std::fabs(xiz[q0])),
+                                      std::max(std::fabs(gax[q0]), std::fabs(gaz[q0])));
+        for (int k = 1; all && k < nn; ++k) {
+          const size_t q = q0 + k;
+          all = std::fabs(xix[q] - xix[q0]) <= 4e-7 * scale && std::fabs(xiz[q] - xiz[q0]) <= 4e-7 * scale &&
+                std::fabs(gax[q] - gax[q0]) <= 4e-7 * scale && std::fabs(gaz[q] - gaz[q0]) <= 4e-7 * scale &&
+                std::fabs(jac[q] - jac[q0]) <= 4e-7 * std::fabs(jac[q0]);
+        }
+      }
+      if (!all) continue;
+      if (aff.empty()) aff.assign(static_cast<size_t>(a.nspec) * words, 0.f);
+      c->st.affine[m] = 1;
+      for (int d = c->med_begin[m]; d < c->med_begin[m] + c->med_count[m]; ++d) {
+        float *blk = &aff[static_cast<size_t>(d) * words];
+        const size_t q0 = static_cast<size_t>(d) * nn;
+        double mean[5] = {0, 0, 0, 0, 0};
+        for (int k = 0; k < nn; ++k) {
+          const size_t q = q0 + k;
+          int gi = iglob[q];
+          std::memcpy(&blk[k], &gi, 4);
+          blk[nn + k] = m0[q];
+          blk[2 * nn + k] = m1[q];
+          mean[0] += xix[q];
+          mean[1] += xiz[q];
+          mean[2] += gax[q];
+          mean[3] += gaz[q];
+          mean[4] += jac[q];
+        }
+        for (int j = 0; j < 5; ++j) blk[3 * nn + j] = static_cast<float>(mean[j] / nn);
+      }
+    }
+    if (!aff.empty()) c->pack_aff.upload(aff, tot);
+  }
   c->dflag.alloc(1, tot);
   c->iglob.upload(iglob, tot);
   c->xix.upload(xix, tot);
@@ -320,6 +368,7 @@ void ensure_device(sfb_context *c) {
   c->st.bnd_nz = c->bnd_nz.p;
   c->st.bnd_w = c->bnd_w.p;
   c->st.pack = c->pack.p;
+  c->st.pack_aff = c->pack_aff.p;
   c->st.err = c->dflag.p;
   for (int m : kMedia) {
     const size_t ld = static_cast<size_t>(a.nglob[m] + (a.nglob[m] & 1)) * a.ncomp(m);
@@ -381,7 +430,7 @@ void ensure_device(sfb_context *c) {
   c->on_device = true;
 }
 
-// Batched stiffness autotuner: with the freshly allocated (all zero)
+// Stiffness autotuner: with the freshly allocated (all zero)
 // forward fields, time every applicable kernel variant of each medium (one
 // warm-up and three timed launches, no sources, coupling or store) and keep
 // the fastest.  The launches add zero forces; the force arrays are cleared
@@ -389,18 +438,26 @@ void ensure_device(sfb_context *c) {
 void autotune_stiffness(sfb_context *c, WavefieldSet &W) {
   const Problem &P = c->P;
   const int S = P.nshots, n = P.asmb.ngll;
-  if (c->tuned || (S == 1 && n != 5)) return;
+  if (c->tuned) return;
   c->tuned = true;
   cudaEvent_t e0, e1;
   ck(cudaEventCreate(&e0), "event");
   ck(cudaEventCreate(&e1), "event");
   const dev::StaceyStore none{};
   for (int m : kMedia) {
+    // a pinned compact-block variant on a medium that is not all affine
+    // runs (and reports) the full block of the same chunk size
+    if (S == 1 && !c->st.affine[m] && c->shots_variant[m] >= dev::kRowAffineFull)
+      c->shots_variant[m] -= dev::kRowAffineFull - dev::kRowFullChunk;
     if (c->shots_variant[m] != dev::kShotsAuto || W.f[m].nelem == 0) continue;
-    int cand[3], nc = 0;
+    int cand[4], nc = 0;
     if (S == 1) {
       cand[nc++] = dev::kRowFullChunk;
-      cand[nc++] = dev::kRowHalfChunk;
+      if (n == 5) cand[nc++] = dev::kRowHalfChunk;
+      if (c->st.affine[m] && c->st.pack_aff) {
+        cand[nc++] = dev::kRowAffineFull;
+        if (n == 5) cand[nc++] = dev::kRowAffineHalf;
+      }
     } else {
       if (S % 2 == 0 && n <= 5) {
         cand[nc++] = dev::kShotsPacked;
@@ -1292,7 +1349,8 @@ SFB_API int sfb_set_stiffness_variant(sfb_context *ctx, int medium, int variant)
   if (!ctx) return SFB_E_INVALID;
   return guarded(ctx, [&]() {
     if (!medium_index_ok(medium)) throw std::invalid_argument("unsupported medium tag");
-    if (variant < dev::kShotsAuto || variant > dev::kShotsSingle) throw std::invalid_argument("unknown stiffness variant");
+    const int top = ctx->P.nshots == 1 ? dev::kRowAffineHalf : dev::kShotsSingle;
+    if (variant < dev::kShotsAuto || variant > top) throw std::invalid_argument("unknown stiffness variant");
     ctx->shots_variant[medium] = variant;
     if (ctx->graph) cudaGraphExecDestroy(ctx->graph);  // captured launches use the old kernel
     ctx->graph = nullptr;
@@ -1868,6 +1926,18 @@ SFB_API int sfb_set_model(sfb_context *ctx, const float *rho, const float *vp, c
         }
       }
       ck(cudaMemcpy(ctx->pack.p, pack.data(), pack.size() * sizeof(float), cudaMemcpyHostToDevice), "pack h2d");
+      if (ctx->pack_aff.p) {
+        const int words = dev::affine_pack_words(ctx->P.asmb.ngll);
+        std::vector<float> aff(static_cast<size_t>(a.nspec) * words);
+        ck(cudaMemcpy(aff.data(), ctx->pack_aff.p, aff.size() * sizeof(float), cudaMemcpyDeviceToHost), "aff d2h");
+        for (int d = 0; d < a.nspec; ++d)
+          for (int k = 0; k < nn; ++k) {
+            const size_t q = static_cast<size_t>(d) * nn + k;
+            aff[static_cast<size_t>(d) * words + nn + k] = m0[q];
+            aff[static_cast<size_t>(d) * words + 2 * nn + k] = m1[q];
+          }
+        ck(cudaMemcpy(ctx->pack_aff.p, aff.data(), aff.size() * sizeof(float), cudaMemcpyHostToDevice), "aff h2d");
+      }
       ck(cudaMemcpy(ctx->mat0_all.p, m0.data(), nloc * sizeof(float), cudaMemcpyHostToDevice), "mat0");
       ck(cudaMemcpy(ctx->mat1_all.p, m1.data(), nloc * sizeof(float), cudaMemcpyHostToDevice), "mat1");
       ck(cudaMemcpy(ctx->mat2_all.p, m2.data(), nloc * sizeof(float), cudaMemcpyHostToDevice), "mat2");

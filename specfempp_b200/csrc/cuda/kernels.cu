@@ -12,6 +12,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 
 namespace sfb {
 namespace dev {
@@ -137,6 +138,45 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity
   return true;
 }
 
+// Programmatic dependent launch.  The time-step kernels (stiffness, update)
+// are launched with the programmatic-serialization attribute, so a launch
+// is set up while the previous one in the stream drains and flushes: it
+// stages what no launch writes (static block, GLL tables, barriers), then
+// griddepcontrol.wait holds it until the previous launch has completed and
+// its writes are visible.  Every block of such a kernel waits before its
+// first read or write of a field and before any return, so a completed
+// launch implies its predecessors completed.  No kernel triggers its
+// dependents early (griddepcontrol.launch_dependents): measured on B200, an
+// early trigger let the next launch's waiting CTAs occupy SM slots and made
+// the single-shot step about 10 % slower, while the implicit trigger at exit
+// makes it about 2 % faster than plain stream order.
+__device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+// Launch with the programmatic-serialization attribute (off when the
+// environment sets SFB_PROGRAMMATIC_LAUNCH=0: plain stream order).
+bool programmatic_launch() {
+  static const bool on = [] {
+    const char *e = std::getenv("SFB_PROGRAMMATIC_LAUNCH");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+template <typename... KArgs, typename... Args>
+void launch_step_kernel(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t stream,
+                        const Args &...args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = programmatic_launch() ? 1 : 0;
+  cudaLaunchKernelEx(&cfg, kern, args...);
+}
+
 // Point sources and fluid-solid coupling of one medium, spread over all CTAs
 // of a stiffness launch (`cta`, `ncta`); they only add into the force array.
 // Fields are point-major, shot-minor: value (g, s) at g * S + s.
@@ -199,13 +239,16 @@ __device__ __forceinline__ void tail_work(const Static &st, const MediumFields &
 // After the chunks every CTA takes a slice of the medium's point sources
 // and fluid-solid coupling points (TailWork); they only add into the same
 // force array.  Every mbarrier wait is bounded (SFB_DEVICE_WAIT_TIMEOUT).
-template <int MED, int N, int EPB, int MINB>
+template <int MED, int N, int EPB, int MINB, bool AFF>
 __global__ void __launch_bounds__(N * EPB, MINB)
 k_stiffness_rp(Static st, MediumFields f, int nshots, StaceyStore ss, const int *istep_dev, TailWork tw,
                FusedUpdate fu) {
   constexpr int NC = (MED == MED_PSV) ? 2 : 1;
   constexpr int NN = N * N;
-  constexpr int ELEM_WORDS = kPackFields * NN;
+  // AFF: the compact block of affine elements (iglob, mat0, mat1 per point,
+  // then the five geometry constants)
+  constexpr int ELEM_WORDS = AFF ? affine_pack_words(N) : kPackFields * NN;
+  constexpr int OFF_M0 = AFF ? NN : 6 * NN, OFF_M1 = AFF ? 2 * NN : 7 * NN;
   constexpr int STAGE_WORDS = EPB * ELEM_WORDS;
   using V = typename Vec<NC>::T;
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -227,10 +270,12 @@ k_stiffness_rp(Static st, MediumFields f, int nshots, StaceyStore ss, const int 
     const int first = chunk * EPB;
     const int count = min(EPB, f.nelem - first);
     const uint32_t bytes = static_cast<uint32_t>(count) * ELEM_WORDS * 4u;
-    const float *src = st.pack + static_cast<size_t>(f.elem_begin + first) * ELEM_WORDS;
+    const float *src = (AFF ? st.pack_aff : st.pack) + static_cast<size_t>(f.elem_begin + first) * ELEM_WORDS;
     mbar_arrive_expect_tx(&bar[stg], bytes);
     bulk_load(stage + stg * STAGE_WORDS, src, bytes, &bar[stg]);
   };
+  // the first chunk's static block does not depend on the previous launch
+  if (t == 0 && blockIdx.x < nchunks) issue(blockIdx.x, 0);
   float hpz[N], hpwz[N];
 #pragma unroll
   for (int l = 0; l < N; ++l) {
@@ -238,16 +283,16 @@ k_stiffness_rp(Static st, MediumFields f, int nshots, StaceyStore ss, const int 
     hpwz[l] = c_hpw[iz * N + l];
   }
   const float wz = c_w[iz];
+  grid_dep_wait();
   const int istep = (ss.mode != 0 || tw.src.n > 0) ? *istep_dev : 0;
   const V *vbase = reinterpret_cast<const V *>(f.u);
   V *abase = reinterpret_cast<V *>(f.a);
   bool ok = true;
 
-  // prologue: first chunk's static block and displacement gathers
+  // prologue: first chunk's displacement gathers
   int g[N];
   V ur[N];
   if (blockIdx.x < nchunks) {
-    if (t == 0) issue(blockIdx.x, 0);
     if (!mbar_wait_bounded(&bar[0], 0)) ok = false;
     const int li = blockIdx.x * EPB + el;
     const float *blk = stage + el * ELEM_WORDS;
@@ -269,6 +314,14 @@ k_stiffness_rp(Static st, MediumFields f, int nshots, StaceyStore ss, const int 
     const int e = f.elem_begin + (valid ? li : 0);
     const uint8_t eflag = valid ? st.eflag[e] : 0;
     const int slot = (ss.mode != 0 && valid) ? ss.slot[e] : -1;
+    float axix = 0.f, axiz = 0.f, agax = 0.f, agaz = 0.f, ajac = 0.f;
+    if constexpr (AFF) {
+      axix = blk[3 * NN + 0];
+      axiz = blk[3 * NN + 1];
+      agax = blk[3 * NN + 2];
+      agaz = blk[3 * NN + 3];
+      ajac = blk[3 * NN + 4];
+    }
     // element-private points of this row (single shot): their velocity is
     // needed after the divergence, so fetch it now
     const bool fused = fu.enabled && nshots == 1 && (eflag & kElemPrivate) && iz >= 1 && iz <= N - 2;
@@ -292,9 +345,10 @@ k_stiffness_rp(Static st, MediumFields f, int nshots, StaceyStore ss, const int 
 #pragma unroll
       for (int ix = 0; ix < N; ++ix) {
         const int k = iz * N + ix;
-        const float xix = blk[1 * NN + k], xiz = blk[2 * NN + k];
-        const float gax = blk[3 * NN + k], gaz = blk[4 * NN + k];
-        const float jac = blk[5 * NN + k], m0 = blk[6 * NN + k], m1 = blk[7 * NN + k];
+        const float xix = AFF ? axix : blk[1 * NN + k], xiz = AFF ? axiz : blk[2 * NN + k];
+        const float gax = AFF ? agax : blk[3 * NN + k], gaz = AFF ? agaz : blk[4 * NN + k];
+        const float jac = AFF ? ajac : blk[5 * NN + k];
+        const float m0 = blk[OFF_M0 + k], m1 = blk[OFF_M1 + k];
         float dxi[NC], dga[NC];
 #pragma unroll
         for (int c = 0; c < NC; ++c) { dxi[c] = 0.f; dga[c] = 0.f; }
@@ -363,7 +417,7 @@ k_stiffness_rp(Static st, MediumFields f, int nshots, StaceyStore ss, const int 
             float vel[2];
 #pragma unroll
             for (int c = 0; c < NC; ++c) vel[c] = comp(vv, c);
-            stacey<MED>(blk[6 * NN + iz * N + ix], blk[7 * NN + iz * N + ix], st.mat2 ? st.mat2[p] : 0.f,
+            stacey<MED>(blk[OFF_M0 + iz * N + ix], blk[OFF_M1 + iz * N + ix], st.mat2 ? st.mat2[p] : 0.f,
                         st.bnd_nx[p], st.bnd_nz[p], st.bnd_w[p], vel, accr[ix]);
           }
           if (b & 2) {
@@ -453,29 +507,43 @@ k_stiffness_rp(Static st, MediumFields f, int nshots, StaceyStore ss, const int 
   tail_work<MED, N>(st, f, nshots, istep, tw, blockIdx.x, gridDim.x);
 }
 
-template <int MED, int N, int EPB>
+template <int MED, int N, int EPB, bool AFF>
 size_t rp_smem_bytes() {
   constexpr int NC = (MED == MED_PSV) ? 2 : 1;
-  return 2 * EPB * kPackFields * N * N * 4 + 2 * EPB * N * N * NC * 4 + 16;
+  constexpr int words = AFF ? affine_pack_words(N) : kPackFields * N * N;
+  return 2 * EPB * words * 4 + 2 * EPB * N * N * NC * 4 + 16;
 }
 
-template <int MED, int N, int EPB, int MINB>
+template <int MED, int N, int EPB, int MINB, bool AFF>
 void launch_rp(const Static &st, const MediumFields &f, int nshots, const StaceyStore &ss, const int *istep_dev,
                const TailWork &tw, const FusedUpdate &fu, cudaStream_t stream) {
   static int blocks_per_sm = -1, nsm = 0;
-  const size_t smem = rp_smem_bytes<MED, N, EPB>();
+  const size_t smem = rp_smem_bytes<MED, N, EPB, AFF>();
   if (blocks_per_sm < 0) {
-    cudaFuncSetAttribute(k_stiffness_rp<MED, N, EPB, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(k_stiffness_rp<MED, N, EPB, MINB, AFF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          static_cast<int>(smem));
     int dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_stiffness_rp<MED, N, EPB, MINB>, N * EPB, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_stiffness_rp<MED, N, EPB, MINB, AFF>, N * EPB,
+                                                  smem);
     if (blocks_per_sm < 1) blocks_per_sm = 1;
   }
   const int nchunks = (f.nelem + EPB - 1) / EPB;
   const int grid = std::max(1, std::min(nchunks, nsm * blocks_per_sm));
-  k_stiffness_rp<MED, N, EPB, MINB><<<grid, N * EPB, smem, stream>>>(st, f, nshots, ss, istep_dev, tw, fu);
+  launch_step_kernel(k_stiffness_rp<MED, N, EPB, MINB, AFF>, grid, N * EPB, smem, stream, st, f, nshots, ss,
+                     istep_dev, tw, fu);
+}
+
+// One medium's single-shot launch: chunk size and occupancy, full or
+// compact static block.
+template <int MED, int N, int EPB, int MINB, int EPB_AFF, int MINB_AFF>
+void launch_row(const Static &st, const MediumFields &f, const StaceyStore &ss, const int *istep_dev,
+                const TailWork &tw, const FusedUpdate &fu, bool affine, cudaStream_t stream) {
+  if (affine)
+    launch_rp<MED, N, EPB_AFF, MINB_AFF, true>(st, f, 1, ss, istep_dev, tw, fu, stream);
+  else
+    launch_rp<MED, N, EPB, MINB, false>(st, f, 1, ss, istep_dev, tw, fu, stream);
 }
 
 // Shot-parallel stiffness for S > 1 independent wavefields (batched shots).
@@ -520,10 +588,11 @@ k_stiffness_shots(Static st, MediumFields f, int S, StaceyStore ss, const int *i
   const int e = f.elem_begin + blockIdx.x;
   const int s0 = (blockIdx.y * 32 + lane) * SPL;
   const bool act = s0 < S;
-  const int istep = (ss.mode != 0 || tw.src.n > 0) ? *istep_dev : 0;
   for (int i = threadIdx.x; i < kPackFields * NN; i += blockDim.x)
     s_st[i] = st.pack[static_cast<size_t>(e) * kPackFields * NN + i];
   __syncthreads();
+  grid_dep_wait();
+  const int istep = (ss.mode != 0 || tw.src.n > 0) ? *istep_dev : 0;
   int g[N];
 #pragma unroll
   for (int ix = 0; ix < N; ++ix) g[ix] = __float_as_int(s_st[iz * N + ix]);
@@ -751,11 +820,30 @@ k_stiffness_pk(Static st, MediumFields f, int S, StaceyStore ss, const int *iste
   const int e = f.elem_begin + blockIdx.x;
   const int s0 = (blockIdx.y * 32 + lane) * 2;
   const bool act = s0 < S;
-  const int istep = (ss.mode != 0 || tw.src.n > 0) ? *istep_dev : 0;
   const float *blk = st.pack + static_cast<size_t>(e) * kPackFields * NN;
   int g[N];
 #pragma unroll
   for (int ix = 0; ix < N; ++ix) g[ix] = __float_as_int(__ldg(blk + iz * N + ix));
+  // geometry and material pairs: static, staged before the dependency wait
+  for (int k = threadIdx.x; k < NN; k += blockDim.x) {
+#pragma unroll
+    for (int q = 1; q <= 5; ++q) {
+      const float v = __ldg(blk + q * NN + k);
+      s_g[(q - 1) * NN + k] = make_float2(v, v);
+    }
+    const float m0 = __ldg(blk + 6 * NN + k), m1 = __ldg(blk + 7 * NN + k);
+    if constexpr (MED == MED_PSV) {
+      const float l2m = m0 + static_cast<float>(4.0 / 3.0) * m1;
+      const float lam = l2m - 2.0f * m1;
+      s_g[5 * NN + k] = make_float2(l2m, l2m);
+      s_g[6 * NN + k] = make_float2(lam, lam);
+      s_g[7 * NN + k] = make_float2(m1, m1);
+    } else {
+      s_g[5 * NN + k] = make_float2(m0, m0);  // SH: mu; acoustic: 1/rho
+    }
+  }
+  grid_dep_wait();
+  const int istep = (ss.mode != 0 || tw.src.n > 0) ? *istep_dev : 0;
   const W *U = reinterpret_cast<const W *>(f.u);
   W *A = reinterpret_cast<W *>(f.a);
   const size_t Sv = static_cast<size_t>(S) / 2;
@@ -799,23 +887,6 @@ k_stiffness_pk(Static st, MediumFields f, int S, StaceyStore ss, const int *iste
       if (act) w = swz(UA[g[ix] * Sv + lofs]);
       else { for (int c = 0; c < NC; ++c) setpr(w, c, make_float2(0.f, 0.f)); }
       s_ua[(iz * N + ix) * 32 + lane] = w;
-    }
-  }
-  for (int k = threadIdx.x; k < NN; k += blockDim.x) {
-#pragma unroll
-    for (int q = 1; q <= 5; ++q) {
-      const float v = __ldg(blk + q * NN + k);
-      s_g[(q - 1) * NN + k] = make_float2(v, v);
-    }
-    const float m0 = __ldg(blk + 6 * NN + k), m1 = __ldg(blk + 7 * NN + k);
-    if constexpr (MED == MED_PSV) {
-      const float l2m = m0 + static_cast<float>(4.0 / 3.0) * m1;
-      const float lam = l2m - 2.0f * m1;
-      s_g[5 * NN + k] = make_float2(l2m, l2m);
-      s_g[6 * NN + k] = make_float2(lam, lam);
-      s_g[7 * NN + k] = make_float2(m1, m1);
-    } else {
-      s_g[5 * NN + k] = make_float2(m0, m0);  // SH: mu; acoustic: 1/rho
     }
   }
   __syncthreads();
@@ -1075,14 +1146,15 @@ void launch_shots(const Static &st, const MediumFields &f, int S, const StaceySt
     if (S % 2 == 0 && variant != kShotsSingle) {
       dim3 grid(f.nelem, (S / 2 + 31) / 32);
       if (variant == kShotsPair)
-        k_stiffness_shots<MED, N, 2, MINB><<<grid, N * 32, 0, stream>>>(st, f, S, ss, istep_dev, tw, fu);
+        launch_step_kernel(k_stiffness_shots<MED, N, 2, MINB>, grid, N * 32, 0, stream, st, f, S, ss, istep_dev, tw, fu);
       else
-        k_stiffness_pk<MED, N, MINB><<<grid, N * 32, 0, stream>>>(st, f, S, ss, istep_dev, tw, fu, FrechetFuse{});
+        launch_step_kernel(k_stiffness_pk<MED, N, MINB, false>, grid, N * 32, 0, stream, st, f, S, ss, istep_dev, tw, fu,
+                           FrechetFuse{});
       return;
     }
   }
   dim3 grid(f.nelem, (S + 31) / 32);
-  k_stiffness_shots<MED, N, 1, MINB><<<grid, N * 32, 0, stream>>>(st, f, S, ss, istep_dev, tw, fu);
+  launch_step_kernel(k_stiffness_shots<MED, N, 1, MINB>, grid, N * 32, 0, stream, st, f, S, ss, istep_dev, tw, fu);
 }
 
 constexpr size_t kFrechetDynSmem = (2 * 25 + 9) * 32 * sizeof(float4) + 3 * 25 * 32 * sizeof(float);
@@ -1343,6 +1415,7 @@ __device__ __forceinline__ void apply_taps(const ReceiverTaps &tp, int g, float 
 // keeps the plain update free of their registers and branches).
 template <bool EXTRA>
 __global__ void k_update_all(UpdateParams P) {
+  grid_dep_wait();
   const int istep = P.ctrl ? P.ctrl->istep : -1;
   const bool record = P.seis != nullptr && istep >= 0 && (istep % P.nsbs) == 0 && (istep / P.nsbs) < P.max_sig;
   const int isig = record ? istep / P.nsbs : 0;
@@ -1605,8 +1678,8 @@ void launch_stiffness_frechet(int ngll, const Static &st, const MediumFields &f,
                               const FusedUpdate &fu, cudaStream_t stream) {
   if (f.nelem == 0 || !frechet_fusable(MED_PSV, ngll, S)) return;
   dim3 grid(f.nelem, (S / 2 + 31) / 32);
-  k_stiffness_pk<MED_PSV, 5, 3, true><<<grid, 5 * 32, kFrechetDynSmem, stream>>>(st, f, S, ss, istep_dev, tw,
-                                                                                  fu, fr);
+  launch_step_kernel(k_stiffness_pk<MED_PSV, 5, 3, true>, grid, 5 * 32, kFrechetDynSmem, stream, st, f, S, ss,
+                     istep_dev, tw, fu, fr);
 }
 
 void launch_stiffness(int medium, int ngll, const Static &st, const MediumFields &f, int nshots,
@@ -1630,22 +1703,26 @@ void launch_stiffness(int medium, int ngll, const Static &st, const MediumFields
     }
     return;
   }
+  // single shot: the row kernel; the compact block only where every element
+  // of the medium is affine
+  const bool aff = (variant == kRowAffineFull || variant == kRowAffineHalf) && st.affine[medium] && st.pack_aff;
+  const bool half = variant == kRowHalfChunk || variant == kRowAffineHalf;
   if (ngll == 5) {
-    // single shot: the row kernel with 32 elements per chunk (variant 0 / 1),
-    // or 16 elements per chunk and twice the CTAs per SM (variant 2)
-    if (variant == kRowHalfChunk) {
-      if (medium == MED_PSV) launch_rp<MED_PSV, 5, 16, 6>(st, f, nshots, ss, istep_dev, w, u, stream);
-      else if (medium == MED_SH) launch_rp<MED_SH, 5, 16, 6>(st, f, nshots, ss, istep_dev, w, nofu, stream);
-      else launch_rp<MED_AC, 5, 16, 6>(st, f, nshots, ss, istep_dev, w, nofu, stream);
+    // 32 elements per chunk, or 16 and twice the CTAs per SM; the compact
+    // block needs a third of the shared memory, so more CTAs fit
+    if (half) {
+      if (medium == MED_PSV) launch_row<MED_PSV, 5, 16, 6, 16, 6>(st, f, ss, istep_dev, w, u, aff, stream);
+      else if (medium == MED_SH) launch_row<MED_SH, 5, 16, 6, 16, 7>(st, f, ss, istep_dev, w, nofu, aff, stream);
+      else launch_row<MED_AC, 5, 16, 6, 16, 7>(st, f, ss, istep_dev, w, nofu, aff, stream);
     } else {
-      if (medium == MED_PSV) launch_rp<MED_PSV, 5, 32, 3>(st, f, nshots, ss, istep_dev, w, u, stream);
-      else if (medium == MED_SH) launch_rp<MED_SH, 5, 32, 3>(st, f, nshots, ss, istep_dev, w, nofu, stream);
-      else launch_rp<MED_AC, 5, 32, 3>(st, f, nshots, ss, istep_dev, w, nofu, stream);
+      if (medium == MED_PSV) launch_row<MED_PSV, 5, 32, 3, 32, 4>(st, f, ss, istep_dev, w, u, aff, stream);
+      else if (medium == MED_SH) launch_row<MED_SH, 5, 32, 3, 32, 4>(st, f, ss, istep_dev, w, nofu, aff, stream);
+      else launch_row<MED_AC, 5, 32, 3, 32, 4>(st, f, ss, istep_dev, w, nofu, aff, stream);
     }
   } else if (ngll == 8) {
-    if (medium == MED_PSV) launch_rp<MED_PSV, 8, 16, 2>(st, f, nshots, ss, istep_dev, w, u, stream);
-    else if (medium == MED_SH) launch_rp<MED_SH, 8, 16, 2>(st, f, nshots, ss, istep_dev, w, nofu, stream);
-    else launch_rp<MED_AC, 8, 16, 2>(st, f, nshots, ss, istep_dev, w, nofu, stream);
+    if (medium == MED_PSV) launch_row<MED_PSV, 8, 16, 2, 16, 2>(st, f, ss, istep_dev, w, u, aff, stream);
+    else if (medium == MED_SH) launch_row<MED_SH, 8, 16, 2, 16, 2>(st, f, ss, istep_dev, w, nofu, aff, stream);
+    else launch_row<MED_AC, 8, 16, 2, 16, 2>(st, f, ss, istep_dev, w, nofu, aff, stream);
   }
 }
 
@@ -1725,9 +1802,9 @@ void launch_update_all(const UpdateParams &p, cudaStream_t stream) {
   bool extra = p.ck_interval > 0;
   for (int m = 0; m < p.nm; ++m) extra = extra || p.m[m].cu != nullptr || p.m[m].ck_u != nullptr;
   if (extra)
-    k_update_all<true><<<std::max(grid, 1), 256, 0, stream>>>(p);
+    launch_step_kernel(k_update_all<true>, std::max(grid, 1), 256, 0, stream, p);
   else
-    k_update_all<false><<<std::max(grid, 1), 256, 0, stream>>>(p);
+    launch_step_kernel(k_update_all<false>, std::max(grid, 1), 256, 0, stream, p);
 }
 
 

@@ -30,9 +30,11 @@ def _ints(*v):
 
 def write_database(path: str, nx: int, nz: int, x0: float, x1: float, z0: float, z1: float,
                    materials: Sequence, element_material=None, absorb=(True, True, False, True),
-                   free_top_acoustic: bool = True):
+                   free_top_acoustic: bool = True, deform=None):
     """materials: (rho, vp, vs) per material (vs = 0: acoustic);
-    element_material: 0-based material of each element [nz * nx]."""
+    element_material: 0-based material of each element [nz * nx];
+    deform: optional (x, z) -> (x, z) map of the control nodes (e.g. a
+    topography), which makes the elements general bilinear quads."""
     nspec = nx * nz
     npx, npz = nx + 1, nz + 1
     npgeo = npx * npz
@@ -68,7 +70,10 @@ def write_database(path: str, nx: int, nz: int, x0: float, x1: float, z0: float,
         for j in range(npz):
             for i in range(npx):
                 ip = j * npx + i + 1
-                _record(f, struct.pack("<idd", ip, x0 + (x1 - x0) * i / nx, z0 + (z1 - z0) * j / nz))
+                x, z = x0 + (x1 - x0) * i / nx, z0 + (z1 - z0) * j / nz
+                if deform is not None:
+                    x, z = deform(x, z)
+                _record(f, struct.pack("<idd", ip, float(x), float(z)))
         _record(f, _ints(len(materials), 4, nspec))
         _record(f, _ints(len(absorbing), 0, len(surface), len(fluid_solid), 0, 0, 0, 0))
         _record(f, struct.pack("<idi", 0, 0.0, 0))  # attenuation: n_sls, f0, read_velocities_at_f0

@@ -31,21 +31,26 @@ def parity_ok(e_gpu_fp32, e_gpu_fp64, e_fp32_fp64):
 
 
 def check(sim, label, shots=(0,), fp64_tol=1e-3, graph=True):
+    """Parity of every shot; the FP32 rounding level of the problem is the
+    largest FP32-oracle-vs-FP64 difference over its shots (shots of one
+    problem share its conditioning; a single shot's value is itself noisy)."""
     from oracle import bridge
     sim.run_forward(graph=graph)
-    worst = 0.0
+    rows = []
     for s in shots:
         gpu = sim.seismograms(shot=s)
         o32 = bridge.forward(sim, 32, shot=s, threads=8)["seismograms"]
         o64 = bridge.forward(sim, 64, shot=s, threads=8)["seismograms"]
         assert np.isfinite(gpu).all()
-        e32, e64 = rel_l2(gpu, o32), rel_l2(gpu, o64)
+        e32, e64, e_ref = rel_l2(gpu, o32), rel_l2(gpu, o64), rel_l2(o32, o64)
         print("%s shot %d: rel-L2 vs FP32 oracle %.2e, vs FP64 oracle %.2e (FP32 oracle vs FP64 %.2e)"
-              % (label, s, e32, e64, rel_l2(o32, o64)))
-        assert parity_ok(e32, e64, rel_l2(o32, o64)), (label, s, e32, e64)
+              % (label, s, e32, e64, e_ref))
+        rows.append((s, e32, e64, e_ref))
+    noise = max(r[3] for r in rows)
+    for s, e32, e64, _ in rows:
+        assert parity_ok(e32, e64, noise), (label, s, e32, e64, noise)
         assert e64 <= fp64_tol, (label, s, e64)
-        worst = max(worst, e32)
-    return worst
+    return max(r[1] for r in rows)
 
 
 def small_elastic(sh=False, nstep=400, types=("displacement", "velocity", "acceleration", "pressure")):
@@ -225,3 +230,83 @@ def test_gll7_elastic_sh_acoustic(nshots):
                      for s in range(nshots)]
         p.stations = [Station(x=100.0 + 150.0 * k, z=500.0) for k in range(4)]
         check(Simulation.structured(p), "GLL7 %s S=%d" % (label, nshots), shots=range(nshots))
+
+
+@pytest.mark.parametrize("kind", ["psv", "sh", "acoustic", "coupled"])
+def test_seismograms_of_given_fields(kind):
+    """sfb_domain_compute_seismograms on fields set through the ABI (two
+    shots, different random fields) against the oracle's FP64 seismograms of
+    the same fields.  Stations sit on an element corner, on an element edge
+    and inside elements, one with a receiver angle; all four seismogram
+    types.  The receiver path alone, as in the reference's seismogram tests."""
+    from oracle import bridge
+    solid, fluid = Material(2700.0, 3000.0, 1732.0), Material(1020.0, 1500.0, 0.0)
+    nx, nz = 10, 8
+    mats, emat = [solid], None
+    if kind == "acoustic":
+        mats = [fluid]
+    elif kind == "coupled":
+        mats = [solid, fluid]
+        emat = np.zeros((nz, nx), np.int32)
+        emat[5:, :] = 1  # top three element rows acoustic
+        emat = emat.ravel()
+    types = ("displacement", "velocity", "acceleration") if kind == "sh" else \
+        ("displacement", "velocity", "acceleration", "pressure")
+    stations = [Station(x=300, z=400), Station(x=350, z=400), Station(x=425, z=530, angle=30.0),
+                Station(x=610, z=180), Station(x=700, z=650), Station(x=120, z=710)]
+    p = StructuredProblem(nx=nx, nz=nz, x0=0, x1=1000, z0=0, z1=800, materials=mats, element_material=emat,
+                          elastic_sh=(kind == "sh"), dt=1e-4, nstep=10, nshots=2,
+                          sources=[ForceSource(x=500, z=250, f0=5.0, shot=s) for s in range(2)],
+                          stations=stations, seismogram_types=types)
+    sim = Simulation.structured(p)
+    info = sim.info()
+    media = [(m, nc) for m, nc in ((0, 2), (1, 1), (3, 1)) if info.nglob[m] > 0]
+    rng = np.random.default_rng(11)
+    for s in range(2):
+        fields = {}
+        for m, nc in media:
+            arrs = tuple(rng.standard_normal((nc, info.nglob[m])).astype(np.float32) for _ in range(3))
+            for which, a in enumerate(arrs):
+                sim.set_field(m, which, a, shot=s)
+            fields[{0: "psv", 1: "sh", 3: "acoustic"}[m]] = arrs
+        ref = bridge.seismograms(sim, fields, 64)
+        sim.compute_seismograms(0)
+        gpu = sim.seismograms(shot=s)[0]
+        assert np.isfinite(gpu).all()
+        for t, name in enumerate(types):  # per type: pressure is ~1e9 times the others here
+            err = rel_l2(gpu[t], ref[t])
+            print("%s shot %d %s: seismograms of given fields, rel-L2 vs FP64 oracle %.2e" % (kind, s, name, err))
+            assert np.abs(ref[t]).max() > 0 and err <= 2e-6, (kind, s, name, err)
+
+
+@pytest.mark.parametrize("workload,variant", [("plain", 1), ("plain", 2), ("plain", 3), ("plain", 4),
+                                              ("coupled", 3), ("coupled", 4)])
+def test_single_shot_row_variants(workload, variant):
+    """Every single-shot row-kernel variant: 32- or 16-element chunks, reading
+    the full static block or the compact block of affine elements (these
+    structured meshes are affine), P-SV and, coupled, acoustic."""
+    if workload == "plain":
+        sim = Simulation.structured(small_elastic(nstep=300))
+    else:
+        sim = Simulation.structured(W.coupled(scale=0.06, nstep=300, seismogram_types=("pressure", "displacement")))
+    for medium in (0, 3):
+        sim.set_stiffness_variant(medium, variant)
+    check(sim, "%s row variant %d" % (workload, variant))
+    info = sim.info()
+    for medium in (0, 3):
+        if info.nelements[medium]:
+            assert info.stiffness_variant[medium] == variant
+
+
+def test_non_affine_mesh_keeps_full_block(tmp_path):
+    """Control nodes moved by a topography-like map: the elements are general
+    bilinear quads, so a pinned compact-block variant runs the full block
+    (and says so); parity against the oracle on that geometry."""
+    import math
+    import workflow_util as WU
+    cfg = WU.write_forward(str(tmp_path), 300, 2.5e-4,
+                           deform=lambda x, z: (x, z + 25.0 * math.sin(2.0 * math.pi * x / WU.LX) * z / WU.LZ))
+    sim = Simulation.from_yaml(cfg)
+    sim.set_stiffness_variant(0, 3)
+    check(sim, "non-affine mesh")
+    assert sim.info().stiffness_variant[0] == 1

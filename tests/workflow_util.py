@@ -40,8 +40,9 @@ def force_entry():
 """ % SOURCE
 
 
-def write_mesh_and_stations(root):
-    write_database(os.path.join(root, "database.bin"), NX, NZ, 0.0, LX, 0.0, LZ, [MAT], absorb=ABSORB)
+def write_mesh_and_stations(root, deform=None):
+    write_database(os.path.join(root, "database.bin"), NX, NZ, 0.0, LX, 0.0, LZ, [MAT], absorb=ABSORB,
+                   deform=deform)
     with open(os.path.join(root, "STATIONS"), "w") as f:
         for k, (x, z) in enumerate(STATIONS):
             f.write("S%04d    AA    %.7f    %.7f    0.0    0.0\n" % (k + 1, x, z))
@@ -78,8 +79,8 @@ def config(root, nstep, dt, mode_block, sources_file):
 """ % (dt, nstep, mode_block, os.path.join(root, "STATIONS"), os.path.join(root, "database.bin"), sources_file)
 
 
-def write_forward(root, nstep, dt):
-    write_mesh_and_stations(root)
+def write_forward(root, nstep, dt, deform=None):
+    write_mesh_and_stations(root, deform)
     src = os.path.join(root, "forward_sources.yaml")
     with open(src, "w") as f:
         f.write("number-of-sources: 1\nsources:\n" + force_entry())
