@@ -51,9 +51,9 @@ VARIANT = 0  # batched stiffness kernel (0: autotuned; see sfb_set_stiffness_var
 
 
 def pin_variant(sim):
-    """Pin the stiffness kernel of every medium; variant 4 (compact block,
-    16-element chunks) exists for single-shot contexts only."""
-    if VARIANT and not (VARIANT == 4 and sim.info().nshots > 1):
+    """Pin the stiffness kernel of every medium (the numbers mean different
+    kernels for single-shot and batched contexts)."""
+    if VARIANT:
         for medium in (0, 1, 3):
             sim.set_stiffness_variant(medium, VARIANT)
 
@@ -157,8 +157,8 @@ def profiled_traffic(name, variant):
 
 def affine_block(info, medium):
     """True when the single-shot stiffness of `medium` reads the compact block
-    of affine elements (variants 3 and 4): geometry per element, not per point."""
-    return info.nshots == 1 and info.stiffness_variant[medium] in (3, 4)
+    of affine elements (variant 3): geometry per element, not per point."""
+    return info.nshots == 1 and info.stiffness_variant[medium] == 3
 
 
 def static_bytes(info, medium, P):
@@ -476,7 +476,7 @@ def main():
                     help="skip the batched-forward and batched-vs-single adjoint measurements")
     ap.add_argument("--scale", type=float, default=1.0,
                     help="shrink the workload's element counts (profiling captures); 1 = full size")
-    ap.add_argument("--stiffness-variant", type=int, default=0, choices=[0, 1, 2, 3, 4],
+    ap.add_argument("--stiffness-variant", type=int, default=0, choices=[0, 1, 2, 3],
                     help="pin the stiffness kernel (sfb_set_stiffness_variant; profiling: the autotuner's "
                          "timings are distorted under a profiler); 0 = autotuned")
     ap.add_argument("--fwi-only", action="store_true",

@@ -141,9 +141,9 @@ typedef struct sfb_info {
                                yet; nshots > 1: 1 two shots per lane in packed
                                FP32x2, 2 two shots per lane scalar, 3 one shot
                                per lane; nshots == 1: 1 row kernel with
-                               32-element chunks, 2 with 16 (NGLL 5), 3 and
-                               4 the same reading the compact static block
-                               of a medium whose elements are all affine    */
+                               32-element chunks, 2 with 16 (NGLL 5), 3 the
+                               compact-block kernel of a medium whose
+                               elements are all affine (NGLL 5)             */
   int private_points;    /* P-SV points updated inside the batched stiffness
                             launch of the forward run (0: none)             */
   int nadjoint_sources;  /* adjoint sources given in the sources file        */
@@ -153,8 +153,9 @@ SFB_API int sfb_get_info(const sfb_context *ctx, sfb_info *info);
 /* Stiffness kernel of `medium` (values of sfb_info.stiffness_variant;
  * 0 = let the autotuner choose).  The autotuner runs once, when the forward
  * fields are first allocated, and times every variant on this mesh; a
- * variant set before that is kept (a compact-block variant on a medium that
- * is not all affine becomes the full-block one).  No reference counterpart
+ * variant set before that is kept (the compact-block variant on a medium
+ * that is not all affine, or at NGLL 8, becomes variant 1).  No reference
+ * counterpart
  * (the reference's chunk size is a compile-time constant). */
 SFB_API int sfb_set_stiffness_variant(sfb_context *ctx, int medium, int variant);
 

@@ -291,13 +291,17 @@ void ensure_device(sfb_context *c) {
   c->pack.upload(pack, tot);
   // Compact block for media whose elements are all affine (the Jacobian
   // matrix and determinant constant over the element to 4e-7 relative, i.e.
-  // equal up to rounding): the single-shot row kernel then streams the
-  // per-point index and material and five constants per element instead of
-  // five geometry words per point.  Batched contexts read the static block
-  // once per element for all shots and keep the full block only.
-  if (c->P.nshots == 1) {
-    const int words = dev::affine_pack_words(n);
+  // equal up to rounding): the single-shot compact-block kernel then streams
+  // the per-point index and material and five constants per element instead
+  // of five geometry words per point; the batched kernels keep the five
+  // constants in registers instead of staging geometry per point.  Chunks of
+  // dev::kAffineChunk elements per medium, chunk-major (see
+  // dev::Static::pack_aff).
+  {
+    const int words = dev::affine_chunk_words(n);
+    const int E = dev::kAffineChunk;
     std::vector<float> aff;
+    int chunks = 0;
     for (int m : kMedia) {
       if (c->med_count[m] == 0) continue;
       bool all = true;
@@ -313,26 +317,31 @@ void ensure_device(sfb_context *c) {
         }
       }
       if (!all) continue;
-      if (aff.empty()) aff.assign(static_cast<size_t>(a.nspec) * words, 0.f);
+      const int mchunks = (c->med_count[m] + E - 1) / E;
       c->st.affine[m] = 1;
-      for (int d = c->med_begin[m]; d < c->med_begin[m] + c->med_count[m]; ++d) {
-        float *blk = &aff[static_cast<size_t>(d) * words];
+      c->st.aff_chunk0[m] = chunks;
+      aff.resize(static_cast<size_t>(chunks + mchunks) * words, 0.f);
+      for (int i = 0; i < c->med_count[m]; ++i) {
+        const int d = c->med_begin[m] + i;
+        float *chunk = &aff[static_cast<size_t>(chunks + i / E) * words];
+        const int el = i % E;
         const size_t q0 = static_cast<size_t>(d) * nn;
         double mean[5] = {0, 0, 0, 0, 0};
         for (int k = 0; k < nn; ++k) {
           const size_t q = q0 + k;
           int gi = iglob[q];
-          std::memcpy(&blk[k], &gi, 4);
-          blk[nn + k] = m0[q];
-          blk[2 * nn + k] = m1[q];
+          std::memcpy(&chunk[el * nn + k], &gi, 4);
+          chunk[E * nn + el * nn + k] = m0[q];
+          chunk[2 * E * nn + el * nn + k] = m1[q];
           mean[0] += xix[q];
           mean[1] += xiz[q];
           mean[2] += gax[q];
           mean[3] += gaz[q];
           mean[4] += jac[q];
         }
-        for (int j = 0; j < 5; ++j) blk[3 * nn + j] = static_cast<float>(mean[j] / nn);
+        for (int j = 0; j < 5; ++j) chunk[3 * E * nn + j * E + el] = static_cast<float>(mean[j] / nn);
       }
+      chunks += mchunks;
     }
     if (!aff.empty()) c->pack_aff.upload(aff, tot);
   }
@@ -447,17 +456,14 @@ void autotune_stiffness(sfb_context *c, WavefieldSet &W) {
   for (int m : kMedia) {
     // a pinned compact-block variant on a medium that is not all affine
     // runs (and reports) the full block of the same chunk size
-    if (S == 1 && !c->st.affine[m] && c->shots_variant[m] >= dev::kRowAffineFull)
-      c->shots_variant[m] -= dev::kRowAffineFull - dev::kRowFullChunk;
+    if (S == 1 && (!c->st.affine[m] || n != 5))
+      c->shots_variant[m] = dev::row_variant_without_affine(c->shots_variant[m]);
     if (c->shots_variant[m] != dev::kShotsAuto || W.f[m].nelem == 0) continue;
-    int cand[4], nc = 0;
+    int cand[3], nc = 0;
     if (S == 1) {
       cand[nc++] = dev::kRowFullChunk;
       if (n == 5) cand[nc++] = dev::kRowHalfChunk;
-      if (c->st.affine[m] && c->st.pack_aff) {
-        cand[nc++] = dev::kRowAffineFull;
-        if (n == 5) cand[nc++] = dev::kRowAffineHalf;
-      }
+      if (n == 5 && c->st.affine[m] && c->st.pack_aff) cand[nc++] = dev::kRowAffine;
     } else {
       if (S % 2 == 0 && n <= 5) {
         cand[nc++] = dev::kShotsPacked;
@@ -1349,7 +1355,7 @@ SFB_API int sfb_set_stiffness_variant(sfb_context *ctx, int medium, int variant)
   if (!ctx) return SFB_E_INVALID;
   return guarded(ctx, [&]() {
     if (!medium_index_ok(medium)) throw std::invalid_argument("unsupported medium tag");
-    const int top = ctx->P.nshots == 1 ? dev::kRowAffineHalf : dev::kShotsSingle;
+    const int top = ctx->P.nshots == 1 ? dev::kRowAffine : dev::kShotsSingle;
     if (variant < dev::kShotsAuto || variant > top) throw std::invalid_argument("unknown stiffness variant");
     ctx->shots_variant[medium] = variant;
     if (ctx->graph) cudaGraphExecDestroy(ctx->graph);  // captured launches use the old kernel
@@ -1927,15 +1933,24 @@ SFB_API int sfb_set_model(sfb_context *ctx, const float *rho, const float *vp, c
       }
       ck(cudaMemcpy(ctx->pack.p, pack.data(), pack.size() * sizeof(float), cudaMemcpyHostToDevice), "pack h2d");
       if (ctx->pack_aff.p) {
-        const int words = dev::affine_pack_words(ctx->P.asmb.ngll);
-        std::vector<float> aff(static_cast<size_t>(a.nspec) * words);
+        // the material words of the compact block
+        const int words = dev::affine_chunk_words(ctx->P.asmb.ngll);
+        const int E = dev::kAffineChunk;
+        std::vector<float> aff(ctx->pack_aff.n);
         ck(cudaMemcpy(aff.data(), ctx->pack_aff.p, aff.size() * sizeof(float), cudaMemcpyDeviceToHost), "aff d2h");
-        for (int d = 0; d < a.nspec; ++d)
-          for (int k = 0; k < nn; ++k) {
-            const size_t q = static_cast<size_t>(d) * nn + k;
-            aff[static_cast<size_t>(d) * words + nn + k] = m0[q];
-            aff[static_cast<size_t>(d) * words + 2 * nn + k] = m1[q];
+        for (int m : kMedia) {
+          if (!ctx->st.affine[m]) continue;
+          for (int i = 0; i < ctx->med_count[m]; ++i) {
+            const int d = ctx->med_begin[m] + i;
+            float *chunk = &aff[static_cast<size_t>(ctx->st.aff_chunk0[m] + i / E) * words];
+            const int el = i % E;
+            for (int k = 0; k < nn; ++k) {
+              const size_t q = static_cast<size_t>(d) * nn + k;
+              chunk[E * nn + el * nn + k] = m0[q];
+              chunk[2 * E * nn + el * nn + k] = m1[q];
+            }
           }
+        }
         ck(cudaMemcpy(ctx->pack_aff.p, aff.data(), aff.size() * sizeof(float), cudaMemcpyHostToDevice), "aff h2d");
       }
       ck(cudaMemcpy(ctx->mat0_all.p, m0.data(), nloc * sizeof(float), cudaMemcpyHostToDevice), "mat0");

@@ -138,6 +138,27 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity
   return true;
 }
 
+// Per-thread asynchronous global -> shared copies (cp.async, no multicast).
+// A thread may read back what it copied itself after cp.async.wait_*; other
+// threads' copies need a barrier after that wait as well.
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void *smem, const void *gmem) {
+  static_assert(BYTES == 4 || BYTES == 8 || BYTES == 16, "cp.async size");
+  if constexpr (BYTES == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_u32(smem)), "l"(gmem) : "memory");
+  else if constexpr (BYTES == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(smem_u32(smem)), "l"(gmem) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(smem_u32(smem)), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+// all but the newest `PENDING` committed groups of this thread have landed
+template <int PENDING>
+__device__ __forceinline__ void cp_async_wait_group() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(PENDING) : "memory");
+}
+
 // Programmatic dependent launch.  The time-step kernels (stiffness, update)
 // are launched with the programmatic-serialization attribute, so a launch
 // is set up while the previous one in the stream drains and flushes: it
@@ -239,16 +260,14 @@ __device__ __forceinline__ void tail_work(const Static &st, const MediumFields &
 // After the chunks every CTA takes a slice of the medium's point sources
 // and fluid-solid coupling points (TailWork); they only add into the same
 // force array.  Every mbarrier wait is bounded (SFB_DEVICE_WAIT_TIMEOUT).
-template <int MED, int N, int EPB, int MINB, bool AFF>
+template <int MED, int N, int EPB, int MINB>
 __global__ void __launch_bounds__(N * EPB, MINB)
 k_stiffness_rp(Static st, MediumFields f, int nshots, StaceyStore ss, const int *istep_dev, TailWork tw,
                FusedUpdate fu) {
   constexpr int NC = (MED == MED_PSV) ? 2 : 1;
   constexpr int NN = N * N;
-  // AFF: the compact block of affine elements (iglob, mat0, mat1 per point,
-  // then the five geometry constants)
-  constexpr int ELEM_WORDS = AFF ? affine_pack_words(N) : kPackFields * NN;
-  constexpr int OFF_M0 = AFF ? NN : 6 * NN, OFF_M1 = AFF ? 2 * NN : 7 * NN;
+  constexpr int ELEM_WORDS = kPackFields * NN;
+  constexpr int OFF_M0 = 6 * NN, OFF_M1 = 7 * NN;
   constexpr int STAGE_WORDS = EPB * ELEM_WORDS;
   using V = typename Vec<NC>::T;
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -270,7 +289,7 @@ k_stiffness_rp(Static st, MediumFields f, int nshots, StaceyStore ss, const int 
     const int first = chunk * EPB;
     const int count = min(EPB, f.nelem - first);
     const uint32_t bytes = static_cast<uint32_t>(count) * ELEM_WORDS * 4u;
-    const float *src = (AFF ? st.pack_aff : st.pack) + static_cast<size_t>(f.elem_begin + first) * ELEM_WORDS;
+    const float *src = st.pack + static_cast<size_t>(f.elem_begin + first) * ELEM_WORDS;
     mbar_arrive_expect_tx(&bar[stg], bytes);
     bulk_load(stage + stg * STAGE_WORDS, src, bytes, &bar[stg]);
   };
@@ -314,14 +333,6 @@ k_stiffness_rp(Static st, MediumFields f, int nshots, StaceyStore ss, const int 
     const int e = f.elem_begin + (valid ? li : 0);
     const uint8_t eflag = valid ? st.eflag[e] : 0;
     const int slot = (ss.mode != 0 && valid) ? ss.slot[e] : -1;
-    float axix = 0.f, axiz = 0.f, agax = 0.f, agaz = 0.f, ajac = 0.f;
-    if constexpr (AFF) {
-      axix = blk[3 * NN + 0];
-      axiz = blk[3 * NN + 1];
-      agax = blk[3 * NN + 2];
-      agaz = blk[3 * NN + 3];
-      ajac = blk[3 * NN + 4];
-    }
     // element-private points of this row (single shot): their velocity is
     // needed after the divergence, so fetch it now
     const bool fused = fu.enabled && nshots == 1 && (eflag & kElemPrivate) && iz >= 1 && iz <= N - 2;
@@ -345,9 +356,9 @@ k_stiffness_rp(Static st, MediumFields f, int nshots, StaceyStore ss, const int 
 #pragma unroll
       for (int ix = 0; ix < N; ++ix) {
         const int k = iz * N + ix;
-        const float xix = AFF ? axix : blk[1 * NN + k], xiz = AFF ? axiz : blk[2 * NN + k];
-        const float gax = AFF ? agax : blk[3 * NN + k], gaz = AFF ? agaz : blk[4 * NN + k];
-        const float jac = AFF ? ajac : blk[5 * NN + k];
+        const float xix = blk[1 * NN + k], xiz = blk[2 * NN + k];
+        const float gax = blk[3 * NN + k], gaz = blk[4 * NN + k];
+        const float jac = blk[5 * NN + k];
         const float m0 = blk[OFF_M0 + k], m1 = blk[OFF_M1 + k];
         float dxi[NC], dga[NC];
 #pragma unroll
@@ -507,43 +518,337 @@ k_stiffness_rp(Static st, MediumFields f, int nshots, StaceyStore ss, const int 
   tail_work<MED, N>(st, f, nshots, istep, tw, blockIdx.x, gridDim.x);
 }
 
-template <int MED, int N, int EPB, bool AFF>
+template <int MED, int N, int EPB>
 size_t rp_smem_bytes() {
   constexpr int NC = (MED == MED_PSV) ? 2 : 1;
-  constexpr int words = AFF ? affine_pack_words(N) : kPackFields * N * N;
-  return 2 * EPB * words * 4 + 2 * EPB * N * N * NC * 4 + 16;
+  return 2 * EPB * kPackFields * N * N * 4 + 2 * EPB * N * N * NC * 4 + 16;
 }
 
-template <int MED, int N, int EPB, int MINB, bool AFF>
+template <int MED, int N, int EPB, int MINB>
 void launch_rp(const Static &st, const MediumFields &f, int nshots, const StaceyStore &ss, const int *istep_dev,
                const TailWork &tw, const FusedUpdate &fu, cudaStream_t stream) {
   static int blocks_per_sm = -1, nsm = 0;
-  const size_t smem = rp_smem_bytes<MED, N, EPB, AFF>();
+  const size_t smem = rp_smem_bytes<MED, N, EPB>();
   if (blocks_per_sm < 0) {
-    cudaFuncSetAttribute(k_stiffness_rp<MED, N, EPB, MINB, AFF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(k_stiffness_rp<MED, N, EPB, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          static_cast<int>(smem));
     int dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_stiffness_rp<MED, N, EPB, MINB, AFF>, N * EPB,
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_stiffness_rp<MED, N, EPB, MINB>, N * EPB,
                                                   smem);
     if (blocks_per_sm < 1) blocks_per_sm = 1;
   }
   const int nchunks = (f.nelem + EPB - 1) / EPB;
   const int grid = std::max(1, std::min(nchunks, nsm * blocks_per_sm));
-  launch_step_kernel(k_stiffness_rp<MED, N, EPB, MINB, AFF>, grid, N * EPB, smem, stream, st, f, nshots, ss,
+  launch_step_kernel(k_stiffness_rp<MED, N, EPB, MINB>, grid, N * EPB, smem, stream, st, f, nshots, ss,
                      istep_dev, tw, fu);
 }
 
-// One medium's single-shot launch: chunk size and occupancy, full or
-// compact static block.
-template <int MED, int N, int EPB, int MINB, int EPB_AFF, int MINB_AFF>
-void launch_row(const Static &st, const MediumFields &f, const StaceyStore &ss, const int *istep_dev,
-                const TailWork &tw, const FusedUpdate &fu, bool affine, cudaStream_t stream) {
-  if (affine)
-    launch_rp<MED, N, EPB_AFF, MINB_AFF, true>(st, f, 1, ss, istep_dev, tw, fu, stream);
-  else
-    launch_rp<MED, N, EPB, MINB, false>(st, f, 1, ss, istep_dev, tw, fu, stream);
+// Single-shot row kernel for a medium of affine elements (same work,
+// arithmetic and outputs as k_stiffness_rp with one shot), reading the
+// compact block: per chunk of kAffineChunk elements, chunk-major,
+//   [0, E*NN) index, [E*NN, 2E*NN) mat0, [2E*NN, 3E*NN) mat1 (element el,
+//   point k at el*NN + k), then xix, xiz, gammax, gammaz, jac ([q][el]),
+// so a warp's reads of a stage are conflict-free.  Deeper pipeline: three
+// static stages (the block of chunk i+2 streams in while chunk i is
+// computed), so the indices of chunk i+1 are in shared memory when chunk i
+// starts; each thread then gathers its row of chunk i+1's displacement
+// straight into shared memory with cp.async, and those loads have the whole
+// of chunk i to land.  The displacement has two shared buffers.  Every
+// mbarrier wait is bounded and its outcome is made CTA-uniform with
+// __syncthreads_and; on expiry the CTA drains its own copies (bounded),
+// records kWaitTimeout in st.err and returns.
+template <int MED, int N, int MINB>
+__global__ void __launch_bounds__(N * kAffineChunk, MINB)
+k_stiffness_rpa(Static st, MediumFields f, StaceyStore ss, const int *istep_dev, TailWork tw, FusedUpdate fu) {
+  constexpr int NC = (MED == MED_PSV) ? 2 : 1;
+  constexpr int NN = N * N;
+  constexpr int EPB = kAffineChunk;
+  constexpr int OFF_M0 = EPB * NN, OFF_M1 = 2 * EPB * NN, OFF_GEO = 3 * EPB * NN;
+  constexpr int STAGES = 3;
+  constexpr int STAGE_WORDS = affine_chunk_words(N);
+  using V = typename Vec<NC>::T;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  float *stage = reinterpret_cast<float *>(smem_raw);            // [STAGES][STAGE_WORDS]
+  V *s_u = reinterpret_cast<V *>(stage + STAGES * STAGE_WORDS);  // [2][EPB][NN]
+  V *s_fg = s_u + 2 * EPB * NN;                                  // [EPB][NN] F(., gamma)
+  uint64_t *bar = reinterpret_cast<uint64_t *>(s_fg + EPB * NN);  // [STAGES]
+
+  const int t = threadIdx.x;
+  const int el = t / N, iz = t % N;
+  const int nchunks = (f.nelem + EPB - 1) / EPB;
+  const int G = gridDim.x;
+  if (t == 0) {
+    for (int q = 0; q < STAGES; ++q) mbar_init(&bar[q], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  // whole chunks: the compact block is padded to full chunks per medium
+  auto issue = [&](int chunk, int stg) {
+    const uint32_t bytes = static_cast<uint32_t>(STAGE_WORDS) * 4u;
+    const float *src = st.pack_aff + (static_cast<size_t>(st.aff_chunk0[MED]) + chunk) * STAGE_WORDS;
+    mbar_arrive_expect_tx(&bar[stg], bytes);
+    bulk_load(stage + stg * STAGE_WORDS, src, bytes, &bar[stg]);
+  };
+  // static blocks of the first two chunks (no launch writes them)
+  if (t == 0) {
+    if (blockIdx.x < nchunks) issue(blockIdx.x, 0);
+    if (blockIdx.x + G < nchunks) issue(blockIdx.x + G, 1);
+  }
+  int issued = blockIdx.x + G < nchunks ? 1 : (blockIdx.x < nchunks ? 0 : -1);  // last iteration issued
+  int waited = -1;  // last iteration whose static block every thread has waited for
+  float hpz[N], hpwz[N];
+#pragma unroll
+  for (int l = 0; l < N; ++l) {
+    hpz[l] = c_hp[iz * N + l];
+    hpwz[l] = c_hpw[iz * N + l];
+  }
+  const float wz = c_w[iz];
+  grid_dep_wait();
+  const int istep = (ss.mode != 0 || tw.src.n > 0) ? *istep_dev : 0;
+  const V *U = reinterpret_cast<const V *>(f.u);
+  V *A = reinterpret_cast<V *>(f.a);
+
+  // this thread's row of chunk `chunk` (iteration `it`) into s_u[it & 1]
+  auto gather = [&](int it, int chunk) {
+    const float *idx = stage + (it % STAGES) * STAGE_WORDS + el * NN + iz * N;
+    V *dst = s_u + (it & 1) * EPB * NN + el * NN + iz * N;
+    if (chunk * EPB + el < f.nelem) {
+#pragma unroll
+      for (int ix = 0; ix < N; ++ix) cp_async<sizeof(V)>(dst + ix, U + __float_as_int(idx[ix]));
+    } else {
+#pragma unroll
+      for (int ix = 0; ix < N; ++ix) dst[ix] = Vec<NC>::zero();
+    }
+  };
+  bool ok = true;
+  if (blockIdx.x < nchunks) {
+    const bool w0 = mbar_wait_bounded(&bar[0], 0);
+    if (w0) gather(0, blockIdx.x);
+    cp_async_commit();
+    ok = __syncthreads_and(w0);
+    if (ok) waited = 0;
+  }
+
+  for (int it = 0; ok; ++it) {
+    const int chunk = blockIdx.x + it * G;
+    if (chunk >= nchunks) break;
+    const int stg = it % STAGES;
+    // the static block of chunk it+2 into the stage chunk it-1 used
+    if (chunk + 2 * G < nchunks) {
+      if (t == 0) issue(chunk + 2 * G, (it + 2) % STAGES);
+      issued = it + 2;
+    }
+    // chunk it+1: wait for its static block (issued an iteration ago) and
+    // start its displacement gathers
+    const bool has_next = chunk + G < nchunks;
+    bool okw = true;
+    if (has_next) {
+      okw = mbar_wait_bounded(&bar[(it + 1) % STAGES], ((it + 1) / STAGES) & 1);
+      if (okw) gather(it + 1, chunk + G);
+    }
+    cp_async_commit();
+    cp_async_wait_group<1>();  // chunk it's gathers have landed
+    ok = __syncthreads_and(okw);
+    if (!ok) break;
+    if (has_next) waited = it + 1;
+
+    const float *blk = stage + stg * STAGE_WORDS + el * NN;  // this element's index and material words
+    const float *geo = stage + stg * STAGE_WORDS + OFF_GEO + el;
+    const V *su = s_u + (it & 1) * EPB * NN + el * NN;
+    const int li = chunk * EPB + el;
+    const bool valid = li < f.nelem;
+    const int e = f.elem_begin + (valid ? li : 0);
+    const uint8_t eflag = valid ? st.eflag[e] : 0;
+    const int slot = (ss.mode != 0 && valid) ? ss.slot[e] : -1;
+    int g[N];
+#pragma unroll
+    for (int ix = 0; ix < N; ++ix) g[ix] = __float_as_int(blk[iz * N + ix]);
+    const float xix = geo[0 * EPB], xiz = geo[1 * EPB], gax = geo[2 * EPB], gaz = geo[3 * EPB];
+    const float jac = geo[4 * EPB];
+    // element-private points of this row: velocity and inverse mass are
+    // needed after the divergence, so fetch them now
+    const bool fused = fu.enabled && (eflag & kElemPrivate) && iz >= 1 && iz <= N - 2;
+    V vp[N - 2], mp[N - 2];
+    if (fused) {
+#pragma unroll
+      for (int ix = 1; ix <= N - 2; ++ix) {
+        vp[ix - 1] = reinterpret_cast<const V *>(fu.v)[g[ix]];
+        mp[ix - 1] = reinterpret_cast<const V *>(fu.minv)[g[ix]];
+      }
+    }
+    V ur[N];
+#pragma unroll
+    for (int ix = 0; ix < N; ++ix) ur[ix] = su[iz * N + ix];
+    V fx[N];
+#pragma unroll
+    for (int ix = 0; ix < N; ++ix) {
+      const int k = iz * N + ix;
+      const float m0 = blk[OFF_M0 + k], m1 = blk[OFF_M1 + k];
+      float dxi[NC], dga[NC];
+#pragma unroll
+      for (int c = 0; c < NC; ++c) { dxi[c] = 0.f; dga[c] = 0.f; }
+#pragma unroll
+      for (int l = 0; l < N; ++l) {
+        const V col = su[l * N + ix];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+          dxi[c] += c_hp[ix * N + l] * comp(ur[l], c);
+          dga[c] += hpz[l] * comp(col, c);
+        }
+      }
+      float du[NC][2];
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        du[c][0] = xix * dxi[c] + gax * dga[c];
+        du[c][1] = xiz * dxi[c] + gaz * dga[c];
+      }
+      float T[NC][2];
+      if constexpr (MED == MED_PSV) {
+        const float l2m = m0 + static_cast<float>(4.0 / 3.0) * m1;
+        const float lam = l2m - 2.0f * m1;
+        T[0][0] = l2m * du[0][0] + lam * du[1][1];
+        T[1][1] = l2m * du[1][1] + lam * du[0][0];
+        T[0][1] = m1 * (du[0][1] + du[1][0]);
+        T[1][0] = T[0][1];
+      } else {
+        T[0][0] = m0 * du[0][0];
+        T[0][1] = m0 * du[0][1];
+      }
+      V f0, f1;
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        set_comp(f0, c, jac * (T[c][0] * xix + T[c][1] * xiz));
+        set_comp(f1, c, jac * (T[c][0] * gax + T[c][1] * gaz));
+      }
+      fx[ix] = f0;
+      s_fg[el * NN + k] = f1;
+    }
+    __syncthreads();
+    float accr[N][2];
+#pragma unroll
+    for (int ix = 0; ix < N; ++ix) {
+      float t1[NC], t2[NC];
+#pragma unroll
+      for (int c = 0; c < NC; ++c) { t1[c] = 0.f; t2[c] = 0.f; }
+#pragma unroll
+      for (int l = 0; l < N; ++l) {
+        const V col = s_fg[el * NN + l * N + ix];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+          t1[c] += comp(fx[l], c) * c_hpw[ix * N + l];
+          t2[c] += comp(col, c) * hpwz[l];
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < NC; ++c) accr[ix][c] = (wz * t1[c] + c_w[ix] * t2[c]) * -1.0f;
+    }
+    if (eflag & 3) {
+#pragma unroll
+      for (int ix = 0; ix < N; ++ix) {
+        const size_t p = (static_cast<size_t>(e) * N + iz) * N + ix;
+        const uint8_t b = st.bnd[p];
+        if (b & 1) {
+          const V vv = reinterpret_cast<const V *>(f.v)[g[ix]];
+          float vel[2];
+#pragma unroll
+          for (int c = 0; c < NC; ++c) vel[c] = comp(vv, c);
+          stacey<MED>(blk[OFF_M0 + iz * N + ix], blk[OFF_M1 + iz * N + ix], st.mat2 ? st.mat2[p] : 0.f,
+                      st.bnd_nx[p], st.bnd_nz[p], st.bnd_w[p], vel, accr[ix]);
+        }
+        if (b & 2) {
+#pragma unroll
+          for (int c = 0; c < NC; ++c) accr[ix][c] = 0.f;
+        }
+      }
+    }
+    if (slot >= 0) {
+#pragma unroll
+      for (int ix = 0; ix < N; ++ix) {
+        const size_t base = (((static_cast<size_t>(istep) * ss.nstacey + slot) * N + iz) * N + ix) * 2;
+        if (ss.mode == 1) {
+#pragma unroll
+          for (int c = 0; c < NC; ++c) ss.data[base + c] = accr[ix][c];
+        } else {
+#pragma unroll
+          for (int c = 0; c < NC; ++c) accr[ix][c] = ss.data[base + c];
+        }
+      }
+    }
+    if (valid) {
+#pragma unroll
+      for (int ix = 0; ix < N; ++ix) {
+        if (fused && ix >= 1 && ix <= N - 2) {
+          // a = force / M, corrector, next predictor in registers
+          // (newmark.tpp:44-47, 98-105); the force never reaches memory
+          V vel = vp[ix - 1], uu = ur[ix], aa;
+#pragma unroll
+          for (int c = 0; c < NC; ++c) {
+            const float a_c = accr[ix][c] * comp(mp[ix - 1], c);
+            set_comp(aa, c, a_c);
+            set_comp(vel, c, comp(vel, c) + fu.dt2 * a_c);
+          }
+          V *Vw = reinterpret_cast<V *>(fu.v);
+          if (fu.last) {
+            A[g[ix]] = aa;
+            Vw[g[ix]] = vel;
+          } else {
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+              set_comp(uu, c, comp(uu, c) + (fu.dt * comp(vel, c) + fu.dtsq2 * comp(aa, c)));
+              set_comp(vel, c, comp(vel, c) + fu.dt2 * comp(aa, c));
+            }
+            reinterpret_cast<V *>(f.u)[g[ix]] = uu;
+            Vw[g[ix]] = vel;
+          }
+          continue;
+        }
+        V out;
+#pragma unroll
+        for (int c = 0; c < NC; ++c) set_comp(out, c, accr[ix][c]);
+        red_add(A + g[ix], out);
+      }
+    }
+    __syncthreads();  // stage stg, s_u[it & 1] and s_fg are free again
+  }
+  if (!ok) {
+    cp_async_wait_all();
+    if (t == 0) {
+      for (int j = waited + 1; j <= issued; ++j) mbar_wait_bounded(&bar[j % STAGES], (j / STAGES) & 1);
+      atomicExch(st.err, kWaitTimeout);
+    }
+    return;
+  }
+  tail_work<MED, N>(st, f, 1, istep, tw, blockIdx.x, gridDim.x);
+}
+
+template <int MED, int N>
+size_t rpa_smem_bytes() {
+  constexpr int NC = (MED == MED_PSV) ? 2 : 1;
+  return 3 * affine_chunk_words(N) * 4 + 3 * kAffineChunk * N * N * NC * 4 + 3 * 8;
+}
+
+template <int MED, int N, int MINB>
+void launch_rpa(const Static &st, const MediumFields &f, const StaceyStore &ss, const int *istep_dev,
+                const TailWork &tw, const FusedUpdate &fu, cudaStream_t stream) {
+  static int blocks_per_sm = -1, nsm = 0;
+  const size_t smem = rpa_smem_bytes<MED, N>();
+  if (blocks_per_sm < 0) {
+    cudaFuncSetAttribute(k_stiffness_rpa<MED, N, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         static_cast<int>(smem));
+    cudaFuncSetAttribute(k_stiffness_rpa<MED, N, MINB>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_stiffness_rpa<MED, N, MINB>, N * kAffineChunk,
+                                                  smem);
+    if (blocks_per_sm < 1) blocks_per_sm = 1;
+  }
+  const int nchunks = (f.nelem + kAffineChunk - 1) / kAffineChunk;
+  const int grid = std::max(1, std::min(nchunks, nsm * blocks_per_sm));
+  launch_step_kernel(k_stiffness_rpa<MED, N, MINB>, grid, N * kAffineChunk, smem, stream, st, f, ss, istep_dev, tw,
+                     fu);
 }
 
 // Shot-parallel stiffness for S > 1 independent wavefields (batched shots).
@@ -785,20 +1090,8 @@ template <typename W> __device__ __forceinline__ W make_zero_w();
 template <> __device__ __forceinline__ float4 make_zero_w<float4>() { return make_float4(0.f, 0.f, 0.f, 0.f); }
 template <> __device__ __forceinline__ float2 make_zero_w<float2>() { return make_float2(0.f, 0.f); }
 
-// Per-thread asynchronous global -> shared copies (cp.async, no multicast):
-// each thread later reads back only what it copied itself, after
-// cp.async.wait_all, so no barrier is needed for these.
-template <int BYTES>
-__device__ __forceinline__ void cp_async(void *smem, const void *gmem) {
-  static_assert(BYTES == 8 || BYTES == 16, "cp.async size");
-  if constexpr (BYTES == 16)
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_u32(smem)), "l"(gmem) : "memory");
-  else
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(smem_u32(smem)), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
-template <int MED, int N, int MINB, bool FR = false>
+template <int MED, int N, int MINB, bool FR = false, bool AFF = false>
 __global__ void __launch_bounds__(N * 32, MINB)
 k_stiffness_pk(Static st, MediumFields f, int S, StaceyStore ss, const int *istep_dev, TailWork tw,
                FusedUpdate fu, FrechetFuse fr) {
@@ -820,18 +1113,41 @@ k_stiffness_pk(Static st, MediumFields f, int S, StaceyStore ss, const int *iste
   const int e = f.elem_begin + blockIdx.x;
   const int s0 = (blockIdx.y * 32 + lane) * 2;
   const bool act = s0 < S;
-  const float *blk = st.pack + static_cast<size_t>(e) * kPackFields * NN;
+  // static words of this element: index and material per point, geometry
+  // per point (full block) or five constants (AFF: the compact block of a
+  // medium of affine elements, chunk-major)
+  const float *bidx, *bm0, *bm1;
+  float2 cgeo[5];
+  if constexpr (AFF) {
+    const int c = blockIdx.x / kAffineChunk, el = blockIdx.x % kAffineChunk;
+    const float *base = st.pack_aff + (static_cast<size_t>(st.aff_chunk0[MED]) + c) * affine_chunk_words(N);
+    bidx = base + el * NN;
+    bm0 = base + kAffineChunk * NN + el * NN;
+    bm1 = base + 2 * kAffineChunk * NN + el * NN;
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+      const float v = __ldg(base + 3 * kAffineChunk * NN + q * kAffineChunk + el);
+      cgeo[q] = make_float2(v, v);
+    }
+  } else {
+    const float *blk = st.pack + static_cast<size_t>(e) * kPackFields * NN;
+    bidx = blk;
+    bm0 = blk + 6 * NN;
+    bm1 = blk + 7 * NN;
+  }
   int g[N];
 #pragma unroll
-  for (int ix = 0; ix < N; ++ix) g[ix] = __float_as_int(__ldg(blk + iz * N + ix));
+  for (int ix = 0; ix < N; ++ix) g[ix] = __float_as_int(__ldg(bidx + iz * N + ix));
   // geometry and material pairs: static, staged before the dependency wait
   for (int k = threadIdx.x; k < NN; k += blockDim.x) {
+    if constexpr (!AFF) {
 #pragma unroll
-    for (int q = 1; q <= 5; ++q) {
-      const float v = __ldg(blk + q * NN + k);
-      s_g[(q - 1) * NN + k] = make_float2(v, v);
+      for (int q = 1; q <= 5; ++q) {
+        const float v = __ldg(bidx + q * NN + k);
+        s_g[(q - 1) * NN + k] = make_float2(v, v);
+      }
     }
-    const float m0 = __ldg(blk + 6 * NN + k), m1 = __ldg(blk + 7 * NN + k);
+    const float m0 = __ldg(bm0 + k), m1 = __ldg(bm1 + k);
     if constexpr (MED == MED_PSV) {
       const float l2m = m0 + static_cast<float>(4.0 / 3.0) * m1;
       const float lam = l2m - 2.0f * m1;
@@ -912,8 +1228,9 @@ k_stiffness_pk(Static st, MediumFields f, int S, StaceyStore ss, const int *iste
         dga[c] = fma2(hpz[l], pr(col, c), dga[c]);
       }
     }
-    const float2 xix = s_g[0 * NN + k], xiz = s_g[1 * NN + k];
-    const float2 gax = s_g[2 * NN + k], gaz = s_g[3 * NN + k], jac = s_g[4 * NN + k];
+    const float2 xix = AFF ? cgeo[0] : s_g[0 * NN + k], xiz = AFF ? cgeo[1] : s_g[1 * NN + k];
+    const float2 gax = AFF ? cgeo[2] : s_g[2 * NN + k], gaz = AFF ? cgeo[3] : s_g[3 * NN + k];
+    const float2 jac = AFF ? cgeo[4] : s_g[4 * NN + k];
     float2 du[NC][2];
 #pragma unroll
     for (int c = 0; c < NC; ++c) {
@@ -999,7 +1316,7 @@ k_stiffness_pk(Static st, MediumFields f, int S, StaceyStore ss, const int *iste
       }
       const int which = q / NN, k = q % NN;
       const size_t p = static_cast<size_t>(e) * NN + k;
-      const float m0 = __ldg(blk + 6 * NN + k), m1 = __ldg(blk + 7 * NN + k);
+      const float m0 = __ldg(bm0 + k), m1 = __ldg(bm1 + k);
       float scale;
       if (which == 0) scale = -1.0f * st.mat2[p] * fr.dt;                            // rho
       else if (which == 1) scale = -2.0f * m1 * fr.dt;                               // mu
@@ -1042,7 +1359,7 @@ k_stiffness_pk(Static st, MediumFields f, int S, StaceyStore ss, const int *iste
           float vel[2];
 #pragma unroll
           for (int c = 0; c < NC; ++c) vel[c] = Vp[c];
-          stacey<MED>(__ldg(blk + 6 * NN + iz * N + ix), __ldg(blk + 7 * NN + iz * N + ix),
+          stacey<MED>(__ldg(bm0 + iz * N + ix), __ldg(bm1 + iz * N + ix),
                       st.mat2 ? st.mat2[p] : 0.f, st.bnd_nx[p], st.bnd_nz[p], st.bnd_w[p], vel, a2);
         }
         if (b & 2) {
@@ -1147,6 +1464,9 @@ void launch_shots(const Static &st, const MediumFields &f, int S, const StaceySt
       dim3 grid(f.nelem, (S / 2 + 31) / 32);
       if (variant == kShotsPair)
         launch_step_kernel(k_stiffness_shots<MED, N, 2, MINB>, grid, N * 32, 0, stream, st, f, S, ss, istep_dev, tw, fu);
+      else if (st.affine[MED] && st.pack_aff)  // compact block: geometry constants in registers
+        launch_step_kernel(k_stiffness_pk<MED, N, MINB, false, true>, grid, N * 32, 0, stream, st, f, S, ss, istep_dev,
+                           tw, fu, FrechetFuse{});
       else
         launch_step_kernel(k_stiffness_pk<MED, N, MINB, false>, grid, N * 32, 0, stream, st, f, S, ss, istep_dev, tw, fu,
                            FrechetFuse{});
@@ -1667,6 +1987,8 @@ size_t field_ld(const MediumFields &f) { return static_cast<size_t>(f.nglob + (f
 void init_kernel_attributes() {
   cudaFuncSetAttribute(k_stiffness_pk<MED_PSV, 5, 3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        static_cast<int>(kFrechetDynSmem));
+  cudaFuncSetAttribute(k_stiffness_pk<MED_PSV, 5, 3, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       static_cast<int>(kFrechetDynSmem));
 }
 
 bool frechet_fusable(int medium, int ngll, int nshots) {
@@ -1678,8 +2000,12 @@ void launch_stiffness_frechet(int ngll, const Static &st, const MediumFields &f,
                               const FusedUpdate &fu, cudaStream_t stream) {
   if (f.nelem == 0 || !frechet_fusable(MED_PSV, ngll, S)) return;
   dim3 grid(f.nelem, (S / 2 + 31) / 32);
-  launch_step_kernel(k_stiffness_pk<MED_PSV, 5, 3, true>, grid, 5 * 32, kFrechetDynSmem, stream, st, f, S, ss,
-                     istep_dev, tw, fu, fr);
+  if (st.affine[MED_PSV] && st.pack_aff)
+    launch_step_kernel(k_stiffness_pk<MED_PSV, 5, 3, true, true>, grid, 5 * 32, kFrechetDynSmem, stream, st, f, S, ss,
+                       istep_dev, tw, fu, fr);
+  else
+    launch_step_kernel(k_stiffness_pk<MED_PSV, 5, 3, true>, grid, 5 * 32, kFrechetDynSmem, stream, st, f, S, ss,
+                       istep_dev, tw, fu, fr);
 }
 
 void launch_stiffness(int medium, int ngll, const Static &st, const MediumFields &f, int nshots,
@@ -1703,26 +2029,27 @@ void launch_stiffness(int medium, int ngll, const Static &st, const MediumFields
     }
     return;
   }
-  // single shot: the row kernel; the compact block only where every element
-  // of the medium is affine
-  const bool aff = (variant == kRowAffineFull || variant == kRowAffineHalf) && st.affine[medium] && st.pack_aff;
-  const bool half = variant == kRowHalfChunk || variant == kRowAffineHalf;
-  if (ngll == 5) {
-    // 32 elements per chunk, or 16 and twice the CTAs per SM; the compact
-    // block needs a third of the shared memory, so more CTAs fit
-    if (half) {
-      if (medium == MED_PSV) launch_row<MED_PSV, 5, 16, 6, 16, 6>(st, f, ss, istep_dev, w, u, aff, stream);
-      else if (medium == MED_SH) launch_row<MED_SH, 5, 16, 6, 16, 7>(st, f, ss, istep_dev, w, nofu, aff, stream);
-      else launch_row<MED_AC, 5, 16, 6, 16, 7>(st, f, ss, istep_dev, w, nofu, aff, stream);
+  // single shot: the row kernel with 32- or 16-element chunks (NGLL 8: 16),
+  // or, where every element of the medium is affine (NGLL 5), the compact
+  // block kernel
+  if (variant == kRowAffine && ngll == 5 && st.affine[medium] && st.pack_aff) {
+    if (medium == MED_PSV) launch_rpa<MED_PSV, 5, 4>(st, f, ss, istep_dev, w, u, stream);
+    else if (medium == MED_SH) launch_rpa<MED_SH, 5, 4>(st, f, ss, istep_dev, w, nofu, stream);
+    else launch_rpa<MED_AC, 5, 4>(st, f, ss, istep_dev, w, nofu, stream);
+  } else if (ngll == 5) {
+    if (variant == kRowHalfChunk) {
+      if (medium == MED_PSV) launch_rp<MED_PSV, 5, 16, 6>(st, f, nshots, ss, istep_dev, w, u, stream);
+      else if (medium == MED_SH) launch_rp<MED_SH, 5, 16, 6>(st, f, nshots, ss, istep_dev, w, nofu, stream);
+      else launch_rp<MED_AC, 5, 16, 6>(st, f, nshots, ss, istep_dev, w, nofu, stream);
     } else {
-      if (medium == MED_PSV) launch_row<MED_PSV, 5, 32, 3, 32, 4>(st, f, ss, istep_dev, w, u, aff, stream);
-      else if (medium == MED_SH) launch_row<MED_SH, 5, 32, 3, 32, 4>(st, f, ss, istep_dev, w, nofu, aff, stream);
-      else launch_row<MED_AC, 5, 32, 3, 32, 4>(st, f, ss, istep_dev, w, nofu, aff, stream);
+      if (medium == MED_PSV) launch_rp<MED_PSV, 5, 32, 3>(st, f, nshots, ss, istep_dev, w, u, stream);
+      else if (medium == MED_SH) launch_rp<MED_SH, 5, 32, 3>(st, f, nshots, ss, istep_dev, w, nofu, stream);
+      else launch_rp<MED_AC, 5, 32, 3>(st, f, nshots, ss, istep_dev, w, nofu, stream);
     }
   } else if (ngll == 8) {
-    if (medium == MED_PSV) launch_row<MED_PSV, 8, 16, 2, 16, 2>(st, f, ss, istep_dev, w, u, aff, stream);
-    else if (medium == MED_SH) launch_row<MED_SH, 8, 16, 2, 16, 2>(st, f, ss, istep_dev, w, nofu, aff, stream);
-    else launch_row<MED_AC, 8, 16, 2, 16, 2>(st, f, ss, istep_dev, w, nofu, aff, stream);
+    if (medium == MED_PSV) launch_rp<MED_PSV, 8, 16, 2>(st, f, nshots, ss, istep_dev, w, u, stream);
+    else if (medium == MED_SH) launch_rp<MED_SH, 8, 16, 2>(st, f, nshots, ss, istep_dev, w, nofu, stream);
+    else launch_rp<MED_AC, 8, 16, 2>(st, f, nshots, ss, istep_dev, w, nofu, stream);
   }
 }
 
@@ -1791,16 +2118,21 @@ void launch_update_all(const UpdateParams &p, cudaStream_t stream) {
     if (p.ctrl) k_advance<<<1, 1, 0, stream>>>(p.ctrl);
     return;
   }
-  static int nsm = 0;
+  // one wave of resident CTAs (grid-stride): a grid beyond what fits leaves
+  // a partial second wave
+  static int nsm = 0, per_sm[2] = {0, 0};
   if (nsm == 0) {
     int dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[0], k_update_all<false>, 256, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[1], k_update_all<true>, 256, 0);
+    for (int &b : per_sm) b = std::max(b, 1);
   }
-  const size_t want = (total + 255) / 256;
-  const int grid = static_cast<int>(std::min<size_t>(want, static_cast<size_t>(nsm) * 8));
   bool extra = p.ck_interval > 0;
   for (int m = 0; m < p.nm; ++m) extra = extra || p.m[m].cu != nullptr || p.m[m].ck_u != nullptr;
+  const size_t want = (total + 255) / 256;
+  const int grid = static_cast<int>(std::min<size_t>(want, static_cast<size_t>(nsm) * per_sm[extra ? 1 : 0]));
   if (extra)
     launch_step_kernel(k_update_all<true>, std::max(grid, 1), 256, 0, stream, p);
   else

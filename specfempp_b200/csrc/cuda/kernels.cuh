@@ -31,12 +31,15 @@ struct Static {
   // pack[e][8][N*N] = iglob (int bits), xix, xiz, gammax, gammaz, jac, mat0, mat1.
   const float *pack;
   // Compact block of affine elements (constant Jacobian matrix, e.g. the
-  // parallelograms of a structured mesh), single-shot contexts only:
-  // pack_aff[e][affine_pack_words(N)] = iglob[N*N], mat0[N*N], mat1[N*N],
-  // xix, xiz, gammax, gammaz, jac.  affine[m] != 0 when every element of
-  // medium m is affine (and pack_aff holds them).
+  // parallelograms of a structured mesh), single-shot contexts only, in
+  // chunks of kAffineChunk elements of one medium (affine_chunk_words(N)
+  // words each, the last chunk zero-padded): index, mat0, mat1 per point
+  // ([3][chunk][N*N]), then xix, xiz, gammax, gammaz, jac ([5][chunk]).
+  // affine[m] != 0 when every element of medium m is affine; its chunks
+  // start at chunk aff_chunk0[m].
   const float *pack_aff;
   int affine[4];
+  int aff_chunk0[4];
   int *err;              // device error flag (bounded waits that expired)
 };
 
@@ -219,13 +222,16 @@ void set_quadrature(int ngll, const float *hprime, const float *wgll);
 // TMA-fed row kernel; several shots: the shot-parallel kernel.
 // Kernel variants of the batched (nshots > 1) stiffness; see launch_shots.
 constexpr int kShotsAuto = 0, kShotsPacked = 1, kShotsPair = 2, kShotsSingle = 3;
-// Single-shot (nshots == 1) variants of the row kernel: 32 or 16 elements
-// per chunk (NGLL 8: 16 in both), reading the full static block or, for a
-// medium of affine elements, the compact one.
-constexpr int kRowFullChunk = 1, kRowHalfChunk = 2, kRowAffineFull = 3, kRowAffineHalf = 4;
-// Words of one element's compact affine block (a multiple of 4: 16-byte
-// aligned bulk copies).
-constexpr int affine_pack_words(int n) { return (3 * n * n + 5 + 3) / 4 * 4; }
+// Single-shot (nshots == 1) variants: the row kernel with 32- or 16-element
+// chunks (NGLL 8: 16 in both) reading the full static block, or (NGLL 5, a
+// medium of affine elements) the compact-block kernel.
+constexpr int kRowFullChunk = 1, kRowHalfChunk = 2, kRowAffine = 3;
+// The variant a pinned one becomes on a medium that is not all affine.
+constexpr int row_variant_without_affine(int v) { return v == kRowAffine ? kRowFullChunk : v; }
+// Elements per chunk of the compact block, and words per chunk (a multiple
+// of 4: 16-byte aligned bulk copies).
+constexpr int kAffineChunk = 32;
+constexpr int affine_chunk_words(int n) { return kAffineChunk * (3 * n * n + 5); }
 void launch_stiffness(int medium, int ngll, const Static &st, const MediumFields &f,
                       int nshots, const StaceyStore &ss, const int *istep_dev,
                       cudaStream_t stream, const TailWork *tw = nullptr,

@@ -5,8 +5,14 @@ against finite differences.
 
 Kernels: relative L2 within 1e-3 of the FP32 oracle (the reference's
 arithmetic) and of the FP64 oracle, or, where even the FP32 oracle is
-further than that from FP64, no further from FP64 than the FP32 oracle is
-(x1.5).  Gradients: within 1e-3 of central finite differences.
+further than that from FP64, of the same order from FP64 as the FP32 oracle
+is: within 1e-3 + 2x its distance.  A kernel sums products of two
+wavefields over every step, one of them reconstructed backward in time
+through the Stacey replay, so its FP32 error is that reconstruction's
+drift; the GPU's and the oracle's FP32 runs are two independent
+realisations of it (their red-add order differs from run to run), which
+one realisation's size bounds only up to a factor of order one.
+Gradients: within 1e-3 of central finite differences.
 """
 import numpy as np
 import pytest
@@ -34,8 +40,9 @@ def parity_ok(e32, e64, e_ref):
 def kernel_ok(e32, e64, e_ref):
     """Kernels: within 1e-3 of the reference's FP32 arithmetic (the oracle)
     and of its FP64 run -- the gradient bar -- or, where the FP32 problem is
-    itself worse conditioned than that, the parity bar above."""
-    return (e32 <= 1e-3 and e64 <= 1e-3) or parity_ok(e32, e64, e_ref)
+    itself worse conditioned than that, of the same order from FP64 as the
+    FP32 oracle (module docstring)."""
+    return (e32 <= 1e-3 and e64 <= 1e-3) or e64 <= 1e-3 + 2.0 * e_ref
 
 
 def gpu_combined(model, obs, absorb, nshots=1, checkpoint_interval=0):

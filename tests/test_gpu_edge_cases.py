@@ -39,7 +39,7 @@ def fields_match(sim, shot=0, tol=1e-5, which=0):
     e32, e64, ref = rel_l2(gpu, o32), rel_l2(gpu, o64), rel_l2(o32, o64)
     print("field %d: rel-L2 vs FP32 oracle %.2e, vs FP64 %.2e (FP32 oracle vs FP64 %.2e)" % (which, e32, e64, ref))
     assert np.abs(o64).max() > 0
-    assert e32 <= tol or e64 <= tol + 1.5 * ref
+    assert e32 <= tol or e64 <= tol + 2.0 * ref
 
 
 def seismograms_match(sim, shot=0, tol=1e-5):
@@ -51,7 +51,7 @@ def seismograms_match(sim, shot=0, tol=1e-5):
     print("seismograms %s: rel-L2 vs FP32 oracle %.2e, vs FP64 %.2e (FP32 oracle vs FP64 %.2e)"
           % (gpu.shape, e32, e64, ref))
     assert np.abs(o64).max() > 0
-    assert e32 <= tol or e64 <= tol + 1.5 * ref
+    assert e32 <= tol or e64 <= tol + 2.0 * ref
 
 
 def test_seismogram_decimation():

@@ -1,12 +1,15 @@
 """GPU parity of the forward path against the CPU oracle on identical inputs.
 
 Bar: seismogram relative L2 <= 1e-5 against the FP32 oracle, or, where the
-FP32 problem itself is worse conditioned than that, the GPU result is no
-further from the FP64 oracle of the same discrete problem than the FP32
-oracle (the reference's FP32 arithmetic) is, with 50 % margin:
-    e(gpu, fp32) <= 1e-5  or  e(gpu, fp64) <= 1e-5 + 1.5 * e(fp32, fp64).
+FP32 problem itself is worse conditioned than that, the GPU result is of
+the same order from the FP64 oracle of the same discrete problem as the
+FP32 oracle (the reference's FP32 arithmetic) is:
+    e(gpu, fp32) <= 1e-5  or  e(gpu, fp64) <= 1e-5 + 2 * e(fp32, fp64).
 Two FP32 implementations cannot agree more closely than their own rounding
-error, which in the acoustic potential formulation reaches ~5e-5.
+error, which in the acoustic potential formulation and at NGLL 8 reaches
+3-6e-5; each FP32 run (the oracle's threaded atomics, the GPU's red-adds)
+is one realisation of it, and two realisations differ in size by up to
+about 2x from run to run.
 Every case goes through the C ABI.
 """
 import numpy as np
@@ -27,7 +30,7 @@ def rel_l2(a, b):
 
 
 def parity_ok(e_gpu_fp32, e_gpu_fp64, e_fp32_fp64):
-    return e_gpu_fp32 <= TOL_FP32 or e_gpu_fp64 <= TOL_FP32 + 1.5 * e_fp32_fp64
+    return e_gpu_fp32 <= TOL_FP32 or e_gpu_fp64 <= TOL_FP32 + 2.0 * e_fp32_fp64
 
 
 def check(sim, label, shots=(0,), fp64_tol=1e-3, graph=True):
@@ -279,12 +282,13 @@ def test_seismograms_of_given_fields(kind):
             assert np.abs(ref[t]).max() > 0 and err <= 2e-6, (kind, s, name, err)
 
 
-@pytest.mark.parametrize("workload,variant", [("plain", 1), ("plain", 2), ("plain", 3), ("plain", 4),
-                                              ("coupled", 3), ("coupled", 4)])
+@pytest.mark.parametrize("workload,variant", [("plain", 1), ("plain", 2), ("plain", 3), ("coupled", 1),
+                                              ("coupled", 3)])
 def test_single_shot_row_variants(workload, variant):
-    """Every single-shot row-kernel variant: 32- or 16-element chunks, reading
-    the full static block or the compact block of affine elements (these
-    structured meshes are affine), P-SV and, coupled, acoustic."""
+    """Every single-shot stiffness variant: the row kernel with 32- or
+    16-element chunks reading the full static block, and the compact-block
+    kernel of affine elements (these structured meshes are affine); P-SV
+    and, coupled, acoustic."""
     if workload == "plain":
         sim = Simulation.structured(small_elastic(nstep=300))
     else:
