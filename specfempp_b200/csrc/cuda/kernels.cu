@@ -1749,6 +1749,83 @@ __global__ void k_update_all(UpdateParams P) {
     if (ck_uslot >= P.ck_count) ck_uslot = -1;
     if (ck_vslot >= P.ck_count) ck_vslot = -1;
   }
+  if constexpr (!EXTRA) {
+    // plain update, two pairs per iteration: both pairs' loads are issued
+    // before either is stored, doubling the loads each thread has in flight
+    // (the kernel is bound by DRAM latency)
+    struct Pair {
+      int mi, g0, s0, g1, s1;
+      size_t at;
+      float2 m, r, vel, uu;
+    };
+    auto load = [&](size_t j, Pair &q) {
+      int mi = 0;
+      while (mi + 1 < P.nm && j >= P.begin[mi + 1]) ++mi;
+      const UpdateMedium &M = P.m[mi];
+      const size_t jj = j - P.begin[mi];
+      q.mi = mi;
+      q.at = jj;
+      if (M.nc == 2) {
+        const uint32_t n = static_cast<uint32_t>(jj);
+        q.g0 = q.g1 = static_cast<int>(P.sdiv.div(n));
+        q.s0 = q.s1 = static_cast<int>(n - static_cast<uint32_t>(q.g0) * S);
+        q.m = reinterpret_cast<const float2 *>(M.minv)[q.g0];
+      } else {
+        const uint32_t n0 = static_cast<uint32_t>(2 * jj), n1 = n0 + 1;
+        q.g0 = static_cast<int>(P.sdiv.div(n0));
+        q.s0 = static_cast<int>(n0 - static_cast<uint32_t>(q.g0) * S);
+        q.g1 = static_cast<int>(P.sdiv.div(n1));
+        q.s1 = static_cast<int>(n1 - static_cast<uint32_t>(q.g1) * S);
+        q.m = make_float2(M.minv[q.g0], M.minv[q.g1]);
+      }
+      q.r = reinterpret_cast<const float2 *>(M.a)[q.at];
+      q.vel = reinterpret_cast<const float2 *>(M.v)[q.at];
+      q.uu = reinterpret_cast<const float2 *>(M.u)[q.at];
+    };
+    auto finish = [&](Pair &q) {
+      const UpdateMedium &M = P.m[q.mi];
+      float2 acc, vel = q.vel, uu = q.uu;
+      acc.x = q.r.x * q.m.x;
+      acc.y = q.r.y * q.m.y;
+      vel.x += P.dt2 * acc.x;  // corrector (newmark.tpp:44-47)
+      vel.y += P.dt2 * acc.y;
+      if (record && M.taps.nsup > 0) {
+        if (M.nc == 2) {
+          apply_taps(M.taps, q.g0, uu.x, uu.y, vel.x, vel.y, acc.x, acc.y,
+                     P.seis + (static_cast<size_t>(q.s0) * P.max_sig + isig) * P.slots);
+        } else {
+          apply_taps(M.taps, q.g0, uu.x, 0.f, vel.x, 0.f, acc.x, 0.f,
+                     P.seis + (static_cast<size_t>(q.s0) * P.max_sig + isig) * P.slots);
+          apply_taps(M.taps, q.g1, uu.y, 0.f, vel.y, 0.f, acc.y, 0.f,
+                     P.seis + (static_cast<size_t>(q.s1) * P.max_sig + isig) * P.slots);
+        }
+      }
+      float2 *U = reinterpret_cast<float2 *>(M.u);
+      float2 *Vv = reinterpret_cast<float2 *>(M.v);
+      float2 *A = reinterpret_cast<float2 *>(M.a);
+      if (P.last) {
+        A[q.at] = acc;
+        Vv[q.at] = vel;
+      } else {
+        uu.x += P.dt * vel.x + P.dtsq2 * acc.x;  // next predictor (newmark.tpp:98-105)
+        uu.y += P.dt * vel.y + P.dtsq2 * acc.y;
+        vel.x += P.dt2 * acc.x;
+        vel.y += P.dt2 * acc.y;
+        U[q.at] = uu;
+        Vv[q.at] = vel;
+        A[q.at] = make_float2(0.f, 0.f);
+      }
+    };
+    const size_t stride = static_cast<size_t>(gridDim.x) * blockDim.x;
+    for (size_t j = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; j < total; j += 2 * stride) {
+      Pair qa, qb;
+      const bool two = j + stride < total;
+      load(j, qa);
+      if (two) load(j + stride, qb);
+      finish(qa);
+      if (two) finish(qb);
+    }
+  } else
   for (size_t j = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; j < total;
        j += static_cast<size_t>(gridDim.x) * blockDim.x) {
     int mi = 0;
