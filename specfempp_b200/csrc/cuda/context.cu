@@ -773,11 +773,15 @@ void enqueue_fused_step(sfb_context *c, WavefieldSet &W, int last) {
   dev::SourceSet src = source_set(c);
   // acoustic first (time_marching.tpp:48-52): stiffness + sources + coupling
   // from the predicted elastic displacement, in one launch
+  // single shot with both media: the elastic launch starts while the
+  // acoustic one finishes (its element loop does not depend on it)
+  const bool overlap = S == 1 && W.f[dev::MED_AC].nelem > 0 && W.f[dev::MED_PSV].nelem > 0;
   dev::TailWork ta{};
   ta.src = src;
   ta.cp = coupling_acoustic(c);
   ta.other = W.f[dev::MED_PSV];
   ta.cp_mode = ta.cp.n > 0 ? 1 : 0;
+  ta.overlap = overlap ? dev::kOverlapFirst : 0;
   dev::launch_stiffness(dev::MED_AC, n, c->st, W.f[dev::MED_AC], S, ss, istep, c->stream, &ta, nullptr,
                         c->shots_variant[dev::MED_AC]);
   // elastic: coupling reads the final acoustic acceleration = force * minv
@@ -787,6 +791,7 @@ void enqueue_fused_step(sfb_context *c, WavefieldSet &W, int last) {
   te.other = W.f[dev::MED_AC];
   te.cp_mode = te.cp.n > 0 ? 2 : 0;
   te.other_divided = 0;
+  te.overlap = overlap ? dev::kOverlapSecond : 0;
   dev::FusedUpdate fu{};
   const bool fused = private_update_on(c);
   if (fused) {

@@ -166,12 +166,33 @@ __device__ __forceinline__ void cp_async_wait_group() {
 // griddepcontrol.wait holds it until the previous launch has completed and
 // its writes are visible.  Every block of such a kernel waits before its
 // first read or write of a field and before any return, so a completed
-// launch implies its predecessors completed.  No kernel triggers its
-// dependents early (griddepcontrol.launch_dependents): measured on B200, an
-// early trigger let the next launch's waiting CTAs occupy SM slots and made
-// the single-shot step about 10 % slower, while the implicit trigger at exit
-// makes it about 2 % faster than plain stream order.
+// launch implies its predecessors completed.  Kernels trigger their
+// dependents at exit: measured on B200, an early trigger let the next
+// launch's waiting CTAs occupy SM slots and made the single-shot step about
+// 10 % slower, while the implicit trigger at exit makes it about 2 % faster
+// than plain stream order.  The exception is an overlapped stiffness pair
+// (TailWork::overlap), where the second launch works before it waits.
 __device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void grid_dep_launch_dependents() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+// Dependency wait of a single-shot stiffness launch at its start, and the
+// early trigger of the first launch of an overlapped pair (TailWork::overlap).
+// The second launch of a pair may start once every CTA of the first has
+// passed its own wait, i.e. after the previous step's update has completed
+// and its writes are visible; its element loop reads and writes only its own
+// medium's fields, which the first launch does not write, so only its tail
+// (sources, coupling from the acoustic force) waits for the first launch.
+__device__ __forceinline__ void stiffness_dep_start(const TailWork &tw) {
+  if (!(tw.overlap & kOverlapSecond)) grid_dep_wait();
+  if (tw.overlap & kOverlapFirst) grid_dep_launch_dependents();
+}
+// The deferred wait of the second launch of a pair, before its tail work
+// (and before any return, so a completed launch still implies completed
+// predecessors).
+__device__ __forceinline__ void stiffness_dep_tail(const TailWork &tw) {
+  if (tw.overlap & kOverlapSecond) grid_dep_wait();
+}
 
 // Launch with the programmatic-serialization attribute (off when the
 // environment sets SFB_PROGRAMMATIC_LAUNCH=0: plain stream order).
@@ -302,7 +323,7 @@ k_stiffness_rp(Static st, MediumFields f, int nshots, StaceyStore ss, const int 
     hpwz[l] = c_hpw[iz * N + l];
   }
   const float wz = c_w[iz];
-  grid_dep_wait();
+  stiffness_dep_start(tw);
   const int istep = (ss.mode != 0 || tw.src.n > 0) ? *istep_dev : 0;
   const V *vbase = reinterpret_cast<const V *>(f.u);
   V *abase = reinterpret_cast<V *>(f.a);
@@ -510,6 +531,7 @@ k_stiffness_rp(Static st, MediumFields f, int nshots, StaceyStore ss, const int 
       __syncthreads();
     }
   }
+  stiffness_dep_tail(tw);
   if (!ok) {
     if (t == 0) atomicExch(st.err, kWaitTimeout);
     return;
@@ -605,7 +627,7 @@ k_stiffness_rpa(Static st, MediumFields f, StaceyStore ss, const int *istep_dev,
     hpwz[l] = c_hpw[iz * N + l];
   }
   const float wz = c_w[iz];
-  grid_dep_wait();
+  stiffness_dep_start(tw);
   const int istep = (ss.mode != 0 || tw.src.n > 0) ? *istep_dev : 0;
   const V *U = reinterpret_cast<const V *>(f.u);
   V *A = reinterpret_cast<V *>(f.a);
@@ -812,6 +834,7 @@ k_stiffness_rpa(Static st, MediumFields f, StaceyStore ss, const int *istep_dev,
     }
     __syncthreads();  // stage stg, s_u[it & 1] and s_fg are free again
   }
+  stiffness_dep_tail(tw);
   if (!ok) {
     cp_async_wait_all();
     if (t == 0) {

@@ -102,7 +102,15 @@ struct TailWork {
   MediumFields other;  // the coupled medium
   int cp_mode;         // 0 none, 1 acoustic <- elastic displacement, 2 elastic <- acoustic acceleration
   int other_divided;   // mode 2: the acoustic array already holds chi_ddot
+  // Overlap of the two stiffness launches of a coupled single-shot step
+  // (programmatic dependent launch): kOverlapFirst lets the next launch start
+  // as soon as every CTA of this one has passed its dependency wait;
+  // kOverlapSecond (the elastic launch, whose element loop reads nothing the
+  // acoustic launch writes) waits for the acoustic launch only before its
+  // tail work, which reads the acoustic force.
+  int overlap;
 };
+constexpr int kOverlapFirst = 1, kOverlapSecond = 2;
 
 // Seismograms as a sparse linear map of nodal values, applied inside the
 // update kernel: seis[s][isig][slot] += w * field_which(g).  `mask` has one
