@@ -286,6 +286,15 @@ SFB_API int sfb_read_wavefield(sfb_context *ctx, int shot, const char *directory
  * order for an element tile of `element_chunk` elements (1 = its CPU
  * build). */
 SFB_API int sfb_write_kernels(const sfb_context *ctx, const char *directory, int element_chunk);
+/* The model per local point as the reference's property writer and reader
+ * store it (include/io/property/{writer,reader}.tpp): <directory>/
+ * Properties/<medium>_isotropic/{X,Z,kappa,mu,rho} (acoustic:
+ * {X,Z,rho_inverse,kappa}), same element order and tile layout as the
+ * kernels.  Reading replaces the context's model (the mass matrix is rebuilt
+ * on the next run); a parameter file selects either with
+ * databases.writer.properties / databases.reader.properties. */
+SFB_API int sfb_write_properties(const sfb_context *ctx, const char *directory, int element_chunk);
+SFB_API int sfb_read_properties(sfb_context *ctx, const char *directory, int element_chunk);
 /* Run a parameter file end to end as the reference's specfem2d does
  * (src/execute.cpp): forward mode runs, writes seismograms and, when asked,
  * the forward wavefield; combined mode reads the wavefield, runs the

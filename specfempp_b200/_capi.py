@@ -145,6 +145,8 @@ SIGNATURES = {
     "sfb_load_backward_from_forward": (C.c_int, [_ctx]),
     "sfb_read_wavefield": (C.c_int, [_ctx, C.c_int, C.c_char_p]),
     "sfb_write_kernels": (C.c_int, [_ctx, C.c_char_p, C.c_int]),
+    "sfb_write_properties": (C.c_int, [_ctx, C.c_char_p, C.c_int]),
+    "sfb_read_properties": (C.c_int, [_ctx, C.c_char_p, C.c_int]),
     "sfb_execute": (C.c_int, [C.c_char_p, C.c_char_p]),
     "sfb_assemble_inverse_mass_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p,
                                                     C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,

@@ -1681,6 +1681,26 @@ SFB_API int sfb_write_kernels(const sfb_context *cctx, const char *directory, in
   });
 }
 
+SFB_API int sfb_write_properties(const sfb_context *cctx, const char *directory, int element_chunk) {
+  sfb_context *ctx = const_cast<sfb_context *>(cctx);
+  if (!ctx || !directory) return SFB_E_INVALID;
+  return guarded(ctx, [&]() {
+    write_properties(ctx->P, directory, element_chunk);
+    return SFB_OK;
+  });
+}
+
+void refresh_model(sfb_context *ctx);
+
+SFB_API int sfb_read_properties(sfb_context *ctx, const char *directory, int element_chunk) {
+  if (!ctx || !directory) return SFB_E_INVALID;
+  return guarded(ctx, [&]() {
+    read_properties(ctx->P, directory, element_chunk);
+    refresh_model(ctx);
+    return SFB_OK;
+  });
+}
+
 // The reference's driver (src/execute.cpp): forward runs write seismograms
 // and, when asked, the forward wavefield; combined runs read that wavefield,
 // run the adjoint + backward loop and write the kernels.
@@ -1692,6 +1712,13 @@ SFB_API int sfb_execute(const char *parameter_file, const char *default_file) {
   // the context goes away on return: its message moves to sfb_last_error(NULL)
   auto failed = [&](int code) { return fail(nullptr, code, ctx->err); };
   const Problem &P = ctx->P;
+  // databases.writer.properties: write the model files and stop
+  // (execute.cpp:115-125); the reader side was applied when the context
+  // was built
+  if (P.property_mode == 1) {
+    if ((rc = sfb_write_properties(ctx, P.property_dir.c_str(), 1))) return failed(rc);
+    return SFB_OK;
+  }
   if (P.simulation == 0) {
     if ((rc = sfb_run_forward(ctx, P.nstep, 1))) return failed(rc);
     if (P.write_seismograms)
@@ -1897,6 +1924,66 @@ SFB_API int sfb_copy_forward_to_backward(const sfb_context *csrc, sfb_context *d
   });
 }
 
+// After the assembly's model changed on the host: refresh the material words
+// of the device's static blocks and per-point arrays; the mass matrix is
+// rebuilt on the next run.
+void refresh_model(sfb_context *ctx) {
+  Assembly &a = ctx->P.asmb;
+  const size_t nloc = a.nloc();
+  const int nn = a.ngll * a.ngll;
+  if (ctx->on_device) {
+    // refresh the material words of the packed and SoA device arrays
+    std::vector<float> m0(nloc), m1(nloc), m2(nloc);
+    std::vector<float> pack(nloc * dev::kPackFields);
+    ck(cudaMemcpy(pack.data(), ctx->pack.p, pack.size() * sizeof(float), cudaMemcpyDeviceToHost), "pack d2h");
+    for (int d = 0; d < a.nspec; ++d) {
+      const int e = ctx->perm[d];
+      const int m = a.medium[e];
+      for (int k = 0; k < nn; ++k) {
+        const size_t p = static_cast<size_t>(e) * nn + k, q = static_cast<size_t>(d) * nn + k;
+        if (m == MEDIUM_ELASTIC_PSV) { m0[q] = a.kappa[p]; m1[q] = a.mu[p]; m2[q] = a.rho[p]; }
+        else if (m == MEDIUM_ELASTIC_SH) { m0[q] = a.mu[p]; m1[q] = a.rho[p]; m2[q] = 0.f; }
+        else { m0[q] = a.rho_inverse[p]; m1[q] = a.kappa[p]; m2[q] = 0.f; }
+        float *blk = &pack[static_cast<size_t>(d) * dev::kPackFields * nn];
+        blk[6 * nn + k] = m0[q];
+        blk[7 * nn + k] = m1[q];
+      }
+    }
+    ck(cudaMemcpy(ctx->pack.p, pack.data(), pack.size() * sizeof(float), cudaMemcpyHostToDevice), "pack h2d");
+    if (ctx->pack_aff.p) {
+      // the material words of the compact block
+      const int words = dev::affine_chunk_words(ctx->P.asmb.ngll);
+      const int E = dev::kAffineChunk;
+      std::vector<float> aff(ctx->pack_aff.n);
+      ck(cudaMemcpy(aff.data(), ctx->pack_aff.p, aff.size() * sizeof(float), cudaMemcpyDeviceToHost), "aff d2h");
+      for (int m : kMedia) {
+        if (!ctx->st.affine[m]) continue;
+        for (int i = 0; i < ctx->med_count[m]; ++i) {
+          const int d = ctx->med_begin[m] + i;
+          float *chunk = &aff[static_cast<size_t>(ctx->st.aff_chunk0[m] + i / E) * words];
+          const int el = i % E;
+          for (int k = 0; k < nn; ++k) {
+            const size_t q = static_cast<size_t>(d) * nn + k;
+            chunk[E * nn + el * nn + k] = m0[q];
+            chunk[2 * E * nn + el * nn + k] = m1[q];
+          }
+        }
+      }
+      ck(cudaMemcpy(ctx->pack_aff.p, aff.data(), aff.size() * sizeof(float), cudaMemcpyHostToDevice), "aff h2d");
+    }
+    ck(cudaMemcpy(ctx->mat0_all.p, m0.data(), nloc * sizeof(float), cudaMemcpyHostToDevice), "mat0");
+    ck(cudaMemcpy(ctx->mat1_all.p, m1.data(), nloc * sizeof(float), cudaMemcpyHostToDevice), "mat1");
+    ck(cudaMemcpy(ctx->mat2_all.p, m2.data(), nloc * sizeof(float), cudaMemcpyHostToDevice), "mat2");
+    ctx->taps_ready = false;  // pressure taps carry the material
+    // captured graphs hold the old tap buffers
+    if (ctx->graph) cudaGraphExecDestroy(ctx->graph);
+    if (ctx->graph_combined) cudaGraphExecDestroy(ctx->graph_combined);
+    ctx->graph = nullptr;
+    ctx->graph_combined = nullptr;
+  }
+  ctx->mass_ready = false;
+}
+
 SFB_API int sfb_set_model(sfb_context *ctx, const float *rho, const float *vp, const float *vs, size_t count) {
   if (!ctx || !rho || !vp || !vs) return SFB_E_INVALID;
   return guarded(ctx, [&]() {
@@ -1918,57 +2005,7 @@ SFB_API int sfb_set_model(sfb_context *ctx, const float *rho, const float *vp, c
         a.rho_inverse[p] = 1.0f / static_cast<float>(r);
       }
     }
-    if (ctx->on_device) {
-      // refresh the material words of the packed and SoA device arrays
-      std::vector<float> m0(nloc), m1(nloc), m2(nloc);
-      std::vector<float> pack(nloc * dev::kPackFields);
-      ck(cudaMemcpy(pack.data(), ctx->pack.p, pack.size() * sizeof(float), cudaMemcpyDeviceToHost), "pack d2h");
-      for (int d = 0; d < a.nspec; ++d) {
-        const int e = ctx->perm[d];
-        const int m = a.medium[e];
-        for (int k = 0; k < nn; ++k) {
-          const size_t p = static_cast<size_t>(e) * nn + k, q = static_cast<size_t>(d) * nn + k;
-          if (m == MEDIUM_ELASTIC_PSV) { m0[q] = a.kappa[p]; m1[q] = a.mu[p]; m2[q] = a.rho[p]; }
-          else if (m == MEDIUM_ELASTIC_SH) { m0[q] = a.mu[p]; m1[q] = a.rho[p]; m2[q] = 0.f; }
-          else { m0[q] = a.rho_inverse[p]; m1[q] = a.kappa[p]; m2[q] = 0.f; }
-          float *blk = &pack[static_cast<size_t>(d) * dev::kPackFields * nn];
-          blk[6 * nn + k] = m0[q];
-          blk[7 * nn + k] = m1[q];
-        }
-      }
-      ck(cudaMemcpy(ctx->pack.p, pack.data(), pack.size() * sizeof(float), cudaMemcpyHostToDevice), "pack h2d");
-      if (ctx->pack_aff.p) {
-        // the material words of the compact block
-        const int words = dev::affine_chunk_words(ctx->P.asmb.ngll);
-        const int E = dev::kAffineChunk;
-        std::vector<float> aff(ctx->pack_aff.n);
-        ck(cudaMemcpy(aff.data(), ctx->pack_aff.p, aff.size() * sizeof(float), cudaMemcpyDeviceToHost), "aff d2h");
-        for (int m : kMedia) {
-          if (!ctx->st.affine[m]) continue;
-          for (int i = 0; i < ctx->med_count[m]; ++i) {
-            const int d = ctx->med_begin[m] + i;
-            float *chunk = &aff[static_cast<size_t>(ctx->st.aff_chunk0[m] + i / E) * words];
-            const int el = i % E;
-            for (int k = 0; k < nn; ++k) {
-              const size_t q = static_cast<size_t>(d) * nn + k;
-              chunk[E * nn + el * nn + k] = m0[q];
-              chunk[2 * E * nn + el * nn + k] = m1[q];
-            }
-          }
-        }
-        ck(cudaMemcpy(ctx->pack_aff.p, aff.data(), aff.size() * sizeof(float), cudaMemcpyHostToDevice), "aff h2d");
-      }
-      ck(cudaMemcpy(ctx->mat0_all.p, m0.data(), nloc * sizeof(float), cudaMemcpyHostToDevice), "mat0");
-      ck(cudaMemcpy(ctx->mat1_all.p, m1.data(), nloc * sizeof(float), cudaMemcpyHostToDevice), "mat1");
-      ck(cudaMemcpy(ctx->mat2_all.p, m2.data(), nloc * sizeof(float), cudaMemcpyHostToDevice), "mat2");
-      ctx->taps_ready = false;  // pressure taps carry the material
-      // captured graphs hold the old tap buffers
-      if (ctx->graph) cudaGraphExecDestroy(ctx->graph);
-      if (ctx->graph_combined) cudaGraphExecDestroy(ctx->graph_combined);
-      ctx->graph = nullptr;
-      ctx->graph_combined = nullptr;
-    }
-    ctx->mass_ready = false;
+    refresh_model(ctx);
     return SFB_OK;
   });
 }

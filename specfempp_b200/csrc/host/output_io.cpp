@@ -1,6 +1,7 @@
 // ASCII output / checkpoint files in the reference's layout; see output_io.hpp.
 #include "output_io.hpp"
 
+#include <cstdint>
 #include <cstdio>
 #include <filesystem>
 #include <fstream>
@@ -108,10 +109,50 @@ namespace {
 // Elements of medium m in reference (ispec) order, and each global point's
 // coordinates.
 std::vector<int> medium_elements(const Assembly &a, int m) {
+  // the reference's compute element order (compute_mesh.cpp:239-279): by
+  // element type in the order of material_definitions.hpp ELEMENT_TYPES --
+  // within a medium boundary tag none, then acoustic_free_surface, stacey,
+  // composite_stacey_dirichlet -- and mesh order within a type.  The tag of
+  // an element follows from its points' boundary bits (bit 0 Stacey, bit 1
+  // acoustic free surface).
+  const int nn = a.ngll * a.ngll;
+  auto tag = [&](int e) {
+    uint8_t bits = 0;
+    for (int k = 0; k < nn; ++k) bits |= a.bnd[static_cast<size_t>(e) * nn + k];
+    const bool stacey = bits & 1, surface = bits & 2;
+    return stacey && surface ? 3 : stacey ? 2 : surface ? 1 : 0;
+  };
   std::vector<int> el;
-  for (int e = 0; e < a.nspec; ++e)
-    if (a.medium[e] == m) el.push_back(e);
+  for (int t : {0, 1, 2, 3})
+    for (int e = 0; e < a.nspec; ++e)
+      if (a.medium[e] == m && tag(e) == t) el.push_back(e);
   return el;
+}
+
+// Raw values of a dataset whose .meta gives `dims` (the file may hold more
+// values than the dims' product: padded element tiles).
+std::vector<double> read_values(const std::string &group, const std::string &name, const std::vector<long> &dims,
+                                size_t count) {
+  ascii_read(group, name, dims);  // checks the metadata
+  std::vector<double> out(count);
+  const std::string path = (fs::path(group) / (name + ".txt")).string();
+  FILE *f = std::fopen(path.c_str(), "r");
+  if (!f) throw std::runtime_error("could not open " + path);
+  for (size_t i = 0; i < count; ++i)
+    if (std::fscanf(f, "%lf", &out[i]) != 1) {
+      std::fclose(f);
+      throw std::runtime_error("dataset " + path + " has fewer values than its element tiles");
+    }
+  std::fclose(f);
+  return out;
+}
+
+// Position of value (i, iz, ix) of an element-tiled dataset
+// (domain_view.hpp:100-160): tile i / chunk, then i % chunk + iz chunk +
+// ix chunk nz.
+size_t tile_index(long i, int iz, int ix, int chunk, int n) {
+  return static_cast<size_t>(i / chunk) * chunk * n * n + (i % chunk) + static_cast<size_t>(iz) * chunk +
+         static_cast<size_t>(ix) * chunk * n;
 }
 
 std::string step_group(int step) {
@@ -228,11 +269,8 @@ void write_kernels(const Problem &P, const std::string &dir, const std::vector<d
       out.assign(span, 0.0);
       for (long i = 0; i < ne; ++i)
         for (int iz = 0; iz < n; ++iz)
-          for (int ix = 0; ix < n; ++ix) {
-            const size_t at = static_cast<size_t>(i / chunk) * chunk * nn + (i % chunk) +
-                              static_cast<size_t>(iz) * chunk + static_cast<size_t>(ix) * chunk * n;
-            out[at] = value(static_cast<size_t>(el[i]) * nn + iz * n + ix);
-          }
+          for (int ix = 0; ix < n; ++ix)
+            out[tile_index(i, iz, ix, chunk, n)] = value(static_cast<size_t>(el[i]) * nn + iz * n + ix);
     };
     std::vector<double> buf;
     std::vector<float> fbuf;
@@ -250,6 +288,87 @@ void write_kernels(const Problem &P, const std::string &dir, const std::vector<d
                              : std::vector<std::pair<const char *, int>>{{"rho", 0}, {"mu", 1}, {"kappa", 2},
                                                                          {"rhop", 3}, {"alpha", 4}, {"beta", 5}};
     for (const auto &[name, q] : names) write_float(name, [&](size_t p) { return kern[q][p]; });
+  }
+}
+
+namespace {
+// Property datasets per medium (the reference's properties containers:
+// medium/dim2/elastic/isotropic/properties_container.hpp, kappa mu rho;
+// acoustic/isotropic/properties_container.hpp, rho_inverse kappa).
+std::vector<const char *> property_names(int m) {
+  if (m == MEDIUM_ACOUSTIC) return {"rho_inverse", "kappa"};
+  return {"kappa", "mu", "rho"};
+}
+template <typename A> auto property_array(A &a, const std::string &name) -> decltype(a.kappa.data()) {
+  if (name == "kappa") return a.kappa.data();
+  if (name == "mu") return a.mu.data();
+  if (name == "rho") return a.rho.data();
+  if (name == "rho_inverse") return a.rho_inverse.data();
+  throw std::invalid_argument("unknown property " + name);
+}
+}  // namespace
+
+void write_properties(const Problem &P, const std::string &dir, int chunk) {
+  const Assembly &a = P.asmb;
+  const int n = a.ngll, nn = n * n;
+  if (chunk < 1) throw std::invalid_argument("element chunk must be >= 1");
+  const std::string root = ascii_group((fs::path(dir) / "Properties").string());
+  for (int m : kMediaTags) {
+    const std::string g = ascii_group((fs::path(root) / (std::string(medium_name(m)) + "_isotropic")).string());
+    const std::vector<int> el = medium_elements(a, m);
+    const long ne = static_cast<long>(el.size());
+    const size_t span = static_cast<size_t>((ne + chunk - 1) / chunk) * chunk * nn;
+    std::vector<float> buf;
+    auto write_float = [&](const char *name, const std::function<float(size_t)> &value) {
+      buf.assign(span, 0.f);
+      for (long i = 0; i < ne; ++i)
+        for (int iz = 0; iz < n; ++iz)
+          for (int ix = 0; ix < n; ++ix)
+            buf[tile_index(i, iz, ix, chunk, n)] = value(static_cast<size_t>(el[i]) * nn + iz * n + ix);
+      write_meta(g, name, {ne, n, n});
+      write_values(g, name, buf.data(), buf.size());
+    };
+    write_float("X", [&](size_t p) { return static_cast<float>(a.coord[p * 2]); });
+    write_float("Z", [&](size_t p) { return static_cast<float>(a.coord[p * 2 + 1]); });
+    for (const char *name : property_names(m)) {
+      const float *v = property_array(a, name);
+      write_float(name, [&](size_t p) { return v[p]; });
+    }
+  }
+}
+
+void read_properties(Problem &P, const std::string &dir, int chunk) {
+  Assembly &a = P.asmb;
+  const int n = a.ngll, nn = n * n;
+  if (chunk < 1) throw std::invalid_argument("element chunk must be >= 1");
+  const fs::path root = fs::path(dir) / "Properties";
+  if (!fs::is_directory(root)) throw std::runtime_error("no Properties folder under " + dir);
+  for (int m : kMediaTags) {
+    const std::vector<int> el = medium_elements(a, m);
+    const long ne = static_cast<long>(el.size());
+    if (ne == 0) continue;
+    const std::string g = (root / (std::string(medium_name(m)) + "_isotropic")).string();
+    const size_t span = static_cast<size_t>((ne + chunk - 1) / chunk) * chunk * nn;
+    for (const char *name : property_names(m)) {
+      const std::vector<double> v = read_values(g, name, {ne, n, n}, span);
+      float *dst = property_array(a, name);
+      for (long i = 0; i < ne; ++i)
+        for (int iz = 0; iz < n; ++iz)
+          for (int ix = 0; ix < n; ++ix)
+            dst[static_cast<size_t>(el[i]) * nn + iz * n + ix] = static_cast<float>(v[tile_index(i, iz, ix, chunk, n)]);
+    }
+    // the quantities the kernels derive from the stored ones
+    for (long i = 0; i < ne; ++i)
+      for (int k = 0; k < nn; ++k) {
+        const size_t p = static_cast<size_t>(el[i]) * nn + k;
+        if (m == MEDIUM_ACOUSTIC) {
+          if (!(a.rho_inverse[p] > 0.f)) throw std::runtime_error("acoustic rho_inverse must be positive");
+          a.rho[p] = 1.0f / a.rho_inverse[p];
+        } else {
+          if (!(a.rho[p] > 0.f)) throw std::runtime_error("elastic rho must be positive");
+          a.rho_inverse[p] = 1.0f / a.rho[p];
+        }
+      }
   }
 }
 

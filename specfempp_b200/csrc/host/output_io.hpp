@@ -57,4 +57,14 @@ ForwardSnapshot read_forward_wavefield(const Problem &P, const std::string &dir,
 // element order.
 void write_kernels(const Problem &P, const std::string &dir, const std::vector<double> kern[6], int chunk);
 
+// <dir>/Properties/<medium>_isotropic/{X, Z, kappa, mu, rho} (acoustic: X, Z,
+// rho_inverse, kappa): the model per local point, the reference's property
+// writer / reader (include/io/property/{writer,reader}.tpp with
+// io/impl/medium_writer.tpp), same element order and tile layout as the
+// kernels.  read_properties replaces the assembly's model (and the rho /
+// rho_inverse it derives); groups of media the mesh does not hold are not
+// read.
+void write_properties(const Problem &P, const std::string &dir, int chunk);
+void read_properties(Problem &P, const std::string &dir, int chunk);
+
 }  // namespace sfb

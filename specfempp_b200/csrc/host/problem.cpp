@@ -2,10 +2,12 @@
 
 #include <cctype>
 #include <cmath>
+#include <filesystem>
 #include <fstream>
 #include <stdexcept>
 #include <sys/stat.h>
 
+#include "output_io.hpp"
 #include "yaml_lite.hpp"
 
 namespace sfb {
@@ -378,6 +380,24 @@ Problem problem_from_yaml(const std::string &parameter_file,
   if (!db) throw std::runtime_error("missing databases.mesh-database");
   Mesh2D mesh = read_database(resolve(db->str(), parameter_file), P.elastic_sh);
   P.asmb = build_assembly(mesh, ngll);
+
+  // model files (src/parameter_parser/setup.cpp:114-122,
+  // src/parameter_parser/writer/property.cpp:9-38)
+  for (const auto &[key, mode] : {std::pair<const char *, int>{"writer", 1}, {"reader", 2}}) {
+    const YNode *node = params->path({"databases", key, "properties"});
+    if (!node) continue;
+    std::string format = "ASCII";
+    if (const YNode *f = node->get("format")) format = f->str();
+    for (auto &ch : format) ch = static_cast<char>(std::tolower(static_cast<unsigned char>(ch)));
+    if (format != "ascii") throw std::runtime_error("model format " + format + " is not supported (ASCII only)");
+    std::string dir = ".";
+    if (const YNode *d = node->get("directory")) dir = resolve(d->str(), parameter_file);
+    if (!std::filesystem::is_directory(dir)) throw std::runtime_error("Model folder : " + dir + " does not exist.");
+    P.property_mode = mode;
+    P.property_dir = dir;
+    break;
+  }
+  if (P.property_mode == 2) read_properties(P, P.property_dir, 1);
 
   // sources
   const YNode *src = params->get("sources");

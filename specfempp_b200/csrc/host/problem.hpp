@@ -37,6 +37,11 @@ struct Problem {
   bool write_seismograms = false;
   std::string wavefield_dir;   // forward: writer.wavefield; combined: reader
   std::string kernel_dir;      // combined: writer.kernels
+  // databases.writer.properties / databases.reader.properties (ASCII):
+  // 1 write the model under property_dir and stop (the reference's driver
+  // does the same, src/execute.cpp:115-125), 2 read it from there
+  int property_mode = 0;
+  std::string property_dir;
 
   int max_sig_step() const { return nstep / nstep_between_samples; }
 

@@ -278,6 +278,15 @@ class Simulation:
         two-shot, 3 one shot per lane; 0 autotuned)."""
         self._check(self._lib.sfb_set_stiffness_variant(self._h, medium, variant))
 
+    def write_properties(self, directory: str, element_chunk: int = 1):
+        """Write the model as the reference's property writer does
+        (<directory>/Properties/<medium>_isotropic/...)."""
+        self._check(self._lib.sfb_write_properties(self._h, directory.encode(), element_chunk))
+
+    def read_properties(self, directory: str, element_chunk: int = 1):
+        """Replace the model from files in the reference's property layout."""
+        self._check(self._lib.sfb_read_properties(self._h, directory.encode(), element_chunk))
+
     def quadrature_volume(self) -> np.ndarray:
         """w_x w_z J per local point [nspec][ngll][ngll] (FP64)."""
         v = self.problem_view()

@@ -16,7 +16,8 @@ import pytest
 from specfempp_b200 import Simulation
 from specfempp_b200 import adjoint_sources as AS
 from specfempp_b200.__main__ import run
-from workflow_util import NX, NZ, STATIONS, read_kernel, structured, write_combined, write_forward
+from workflow_util import (NX, NZ, STATIONS, read_kernel, reference_element_order, structured,
+                           write_combined, write_forward)
 
 pytestmark = pytest.mark.gpu
 
@@ -58,7 +59,9 @@ def test_two_phase_workflow_matches_in_memory(tmp_path):
     for prec in (32, 64):
         fwd = bridge.forward(sim, prec, threads=8, want_fields=True, want_stacey=True)
         o[prec] = bridge.combined(sim, stf, fwd, precision=prec, threads=8)
-    files = {name: read_kernel(os.path.join(root, "kernels"), "elastic_psv_isotropic", name, NX * NZ, info.ngll)
+    order = reference_element_order(sim, 0)
+    files = {name: read_kernel(os.path.join(root, "kernels"), "elastic_psv_isotropic", name, NX * NZ, info.ngll,
+                               order)
              for name in ("rho", "mu", "kappa", "rhop", "alpha", "beta")}
     for q, name in enumerate(("rho", "mu", "kappa")):
         k = files[name]

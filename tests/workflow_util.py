@@ -134,13 +134,32 @@ def write_combined(root, nstep, dt, adj_folder, names):
     return path
 
 
-def read_kernel(folder, medium_group, name, nspec_medium, ngll):
+def reference_element_order(sim, medium):
+    """Elements of `medium` in the reference's compute order, which the
+    kernel and property writers follow: by boundary tag (none, acoustic free
+    surface, Stacey, both; from the points' boundary bits), mesh order within
+    a tag."""
+    info, view = sim.info(), sim.problem_view()
+    n, nspec = info.ngll, info.nspec
+    med = np.ctypeslib.as_array(view.medium, shape=(nspec,))
+    bits = np.bitwise_or.reduce(np.ctypeslib.as_array(view.bnd, shape=(nspec * n * n,)).reshape(nspec, n * n), axis=1)
+    stacey, surface = (bits & 1) != 0, (bits & 2) != 0
+    tag = np.where(stacey & surface, 3, np.where(stacey, 2, np.where(surface, 1, 0)))
+    return np.concatenate([np.nonzero((med == medium) & (tag == t))[0] for t in range(4)])
+
+
+def read_kernel(folder, medium_group, name, nspec_medium, ngll, order=None):
     """A kernel dataset written with element tile 1: value (i, iz, ix) at
-    i * n * n + iz + ix * n."""
+    i * n * n + iz + ix * n, element i of the writer's order; with `order`
+    (reference_element_order) the result is in mesh element order."""
     v = np.loadtxt(os.path.join(folder, "Kernels", medium_group, name + ".txt"))
     out = np.zeros((nspec_medium, ngll, ngll))
     for i in range(nspec_medium):
         for iz in range(ngll):
             for ix in range(ngll):
                 out[i, iz, ix] = v[i * ngll * ngll + iz + ix * ngll]
+    if order is not None:
+        mesh = np.zeros_like(out)
+        mesh[order] = out
+        out = mesh
     return out
