@@ -72,7 +72,8 @@ typedef struct sfb_material {
 } sfb_material;
 
 typedef struct sfb_source_desc {
-  int kind;        /* 0 force, 1 moment tensor                              */
+  int kind;        /* 0 force, 1 moment tensor, 2 user-defined (Lagrange
+                      weights in every component, src/source/external.cpp) */
   int shot;        /* shot index in [0, nshots)                              */
   int wavefield;   /* 0: forward (backward in combined runs), 1: adjoint     */
   int stf;         /* 0 Ricker, 1 Dirac, 2 dGaussian, 3 table                */

@@ -640,8 +640,9 @@ LocatedSource locate_source(const Assembly &a, const Source &s, double t0,
         out.array[iz * n + ix] = static_cast<float>(s.mxx * dsdx + s.mxz * dsdz);
         out.array[n * n + iz * n + ix] = static_cast<float>(s.mxz * dsdx + s.mzz * dsdz);
       }
-  } else if (s.kind == Source::ADJOINT) {
-    // reference: src/source/adjoint_source.cpp (Lagrange weights in every component)
+  } else if (s.kind == Source::ADJOINT || s.kind == Source::EXTERNAL) {
+    // reference: src/source/adjoint_source.cpp, src/source/external.cpp
+    // (Lagrange weights in every component)
     for (int c = 0; c < nc; ++c)
       for (int iz = 0; iz < n; ++iz)
         for (int ix = 0; ix < n; ++ix) out.array[static_cast<size_t>(c) * n * n + iz * n + ix] = static_cast<float>(hx[ix] * hz[iz]);

@@ -107,6 +107,10 @@ Source parse_source(const YNode &entry, double dt, int nstep, const std::string 
     s.mxx = body->get("Mxx")->num();
     s.mzz = body->get("Mzz")->num();
     s.mxz = body->get("Mxz")->num();
+  } else if ((body = entry.get("user-defined"))) {
+    // src/io/sources.cpp:88-91, src/source/external.cpp: Lagrange weights in
+    // every component, any source time function
+    s.kind = Source::EXTERNAL;
   } else if ((body = entry.get("adjoint-source"))) {
     // src/io/sources.cpp:92-99, src/source/adjoint_source.cpp
     if (!body->get("station_name") || !body->get("network_name"))
@@ -116,7 +120,7 @@ Source parse_source(const YNode &entry, double dt, int nstep, const std::string 
     s.network = body->get("network_name")->str();
     s.wavefield = 1;
   } else {
-    throw std::runtime_error("Unknown source type (this path supports force, moment-tensor and adjoint-source)");
+    throw std::runtime_error("Unknown source type (this path supports force, moment-tensor, user-defined and adjoint-source)");
   }
   s.x = body->get("x")->num();
   s.z = body->get("z")->num();
@@ -518,6 +522,7 @@ Problem problem_from_structured(const sfb_structured_desc &d) {
   for (int i = 0; i < d.nsources; ++i) {
     const sfb_source_desc &sd = d.sources[i];
     Source s;
+    if (sd.kind < Source::FORCE || sd.kind > Source::EXTERNAL) throw std::runtime_error("unknown source kind");
     s.kind = sd.kind;
     s.x = sd.x;
     s.z = sd.z;

@@ -32,7 +32,7 @@ class ForceSource:
     tshift: float = 0.0
     stf: str = "ricker"  # ricker | dirac | dgaussian
     shot: int = 0
-    kind: str = "force"  # force | moment_tensor
+    kind: str = "force"  # force | moment_tensor | user_defined
     mxx: float = 0.0
     mzz: float = 0.0
     mxz: float = 0.0
@@ -125,7 +125,7 @@ class Simulation:
         srcs = (A.sfb_source_desc * max(1, len(p.sources)))()
         stf_code = {"ricker": 0, "dirac": 1, "dgaussian": 2}
         for i, s in enumerate(p.sources):
-            srcs[i].kind = 0 if s.kind == "force" else 1
+            srcs[i].kind = {"force": 0, "moment_tensor": 1, "user_defined": 2}[s.kind]
             srcs[i].shot = s.shot
             srcs[i].wavefield = 0
             srcs[i].stf = stf_code[s.stf]

@@ -335,3 +335,16 @@ def test_model_read_from_property_files(tmp_path):
     check(from_files, "model from property files")
     # two GPU runs of one model differ by the order of their FP32 red-adds
     assert rel_l2(from_files.seismograms(), direct.seismograms()) <= TOL_FP32
+
+
+@pytest.mark.parametrize("medium", ["elastic", "acoustic"])
+def test_user_defined_source(medium):
+    """A user-defined source (src/source/external.cpp: Lagrange weights in
+    every component) with a Ricker time function, off the GLL points."""
+    mat = Material(2700.0, 3000.0, 1732.0) if medium == "elastic" else Material(1020.0, 1500.0, 0.0)
+    p = StructuredProblem(nx=16, nz=12, x0=0, x1=800, z0=0, z1=600, materials=[mat],
+                          absorb=(True, True, False, True), dt=2.5e-4, nstep=300,
+                          sources=[ForceSource(x=413.0, z=287.0, f0=10.0, factor=1e10, kind="user_defined")],
+                          stations=[Station(x=100 + 120 * k, z=500) for k in range(6)],
+                          seismogram_types=("displacement", "pressure") if medium == "acoustic" else ("displacement",))
+    check(Simulation.structured(p), "user-defined source, %s" % medium)

@@ -85,3 +85,23 @@ def test_adjoint_source_in_forward_mode_is_rejected(tmp_path, native_lib):
         f.write(text)
     with pytest.raises(SfbError, match="Adjoint sources found"):
         Simulation.from_yaml(cfg)
+
+
+def test_user_defined_source_in_a_sources_file(tmp_path, native_lib):
+    """A `user-defined` entry (src/io/sources.cpp:88-91): the source array is
+    the Lagrange weight of the location in every component."""
+    cfg = write_forward(str(tmp_path), NSTEP, DT)
+    src = os.path.join(str(tmp_path), "forward_sources.yaml")
+    with open(src, "w") as f:
+        f.write("number-of-sources: 1\nsources:\n  - user-defined:\n      x : 413.0\n      z : 287.0\n"
+                "      Ricker:\n        factor: 1e10\n        tshift: 0.0\n        f0: 10.0\n")
+    sim = Simulation.from_yaml(cfg)
+    view = sim.problem_view()
+    n = view.ngll
+    assert view.nsources == 1
+    a = np.ctypeslib.as_array(view.src_array, shape=(1, 2, n, n))
+    np.testing.assert_allclose(a.sum(axis=(2, 3)), [[1.0, 1.0]], rtol=1e-6)
+    np.testing.assert_array_equal(a[0, 0], a[0, 1])
+    stf = np.ctypeslib.as_array(view.src_stf, shape=(1, NSTEP, 2))
+    np.testing.assert_array_equal(stf[0, :, 0], stf[0, :, 1])
+    assert np.abs(stf).max() > 0
