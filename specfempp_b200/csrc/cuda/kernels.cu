@@ -869,7 +869,13 @@ void launch_rpa(const Static &st, const MediumFields &f, const StaceyStore &ss, 
     if (blocks_per_sm < 1) blocks_per_sm = 1;
   }
   const int nchunks = (f.nelem + kAffineChunk - 1) / kAffineChunk;
-  const int grid = std::max(1, std::min(nchunks, nsm * blocks_per_sm));
+  int grid = std::max(1, std::min(nchunks, nsm * blocks_per_sm));
+  if (tw.overlap & kOverlapFirst) {
+    // first launch of an overlapped pair: the fewest CTAs that keep the
+    // same number of chunks per CTA, so the slots it leaves go to the second
+    const int per = (nchunks + grid - 1) / grid;
+    grid = std::max(1, (nchunks + per - 1) / per);
+  }
   launch_step_kernel(k_stiffness_rpa<MED, N, MINB>, grid, N * kAffineChunk, smem, stream, st, f, ss, istep_dev, tw,
                      fu);
 }
