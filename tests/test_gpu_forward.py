@@ -348,3 +348,27 @@ def test_user_defined_source(medium):
                           stations=[Station(x=100 + 120 * k, z=500) for k in range(6)],
                           seismogram_types=("displacement", "pressure") if medium == "acoustic" else ("displacement",))
     check(Simulation.structured(p), "user-defined source, %s" % medium)
+
+
+def test_plain_stream_order_matches(tmp_path):
+    """SFB_PROGRAMMATIC_LAUNCH=0 (read once per process: a child process)
+    launches every step kernel in plain stream order; the coupled run then
+    meets the same bar against the oracle as with programmatic launch."""
+    import os
+    import subprocess
+    import sys
+    from oracle import bridge
+    out = tmp_path / "seis.npy"
+    code = ("import numpy as np; from specfempp_b200 import Simulation, workloads as W; "
+            "sim = Simulation.structured(W.coupled(scale=0.06, nstep=300, seismogram_types=('pressure', 'displacement'))); "
+            "sim.run_forward(); np.save(%r, sim.seismograms())" % str(out))
+    env = dict(os.environ, SFB_PROGRAMMATIC_LAUNCH="0")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    subprocess.run([sys.executable, "-c", code], check=True, env=env, cwd=root, timeout=600)
+    gpu = np.load(out)
+    sim = Simulation.structured(W.coupled(scale=0.06, nstep=300, seismogram_types=("pressure", "displacement")))
+    o32 = bridge.forward(sim, 32, threads=8)["seismograms"]
+    o64 = bridge.forward(sim, 64, threads=8)["seismograms"]
+    e32, e64, eref = rel_l2(gpu, o32), rel_l2(gpu, o64), rel_l2(o32, o64)
+    print("plain stream order: rel-L2 vs FP32 oracle %.2e, vs FP64 %.2e (FP32 oracle vs FP64 %.2e)" % (e32, e64, eref))
+    assert parity_ok(e32, e64, eref)
