@@ -1778,7 +1778,81 @@ __global__ void k_update_all(UpdateParams P) {
     if (ck_uslot >= P.ck_count) ck_uslot = -1;
     if (ck_vslot >= P.ck_count) ck_vslot = -1;
   }
-  if constexpr (!EXTRA) {
+  if (!EXTRA && P.quad) {
+    // plain update with an even shot count: quad q of a medium is pairs 2q
+    // and 2q + 1, read and written as one float4 per array (nc = 2: shots s
+    // and s + 1 of one point; nc = 1: four consecutive entries of [g][s])
+    const size_t totq = total / 2;
+    const size_t strideq = static_cast<size_t>(gridDim.x) * blockDim.x;
+    for (size_t q = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; q < totq; q += strideq) {
+      int mi = 0;
+      while (mi + 1 < P.nm && 2 * q >= P.begin[mi + 1]) ++mi;
+      const UpdateMedium &M = P.m[mi];
+      const size_t qq = q - P.begin[mi] / 2;
+      const float4 r = reinterpret_cast<const float4 *>(M.a)[qq];
+      float4 vel = reinterpret_cast<const float4 *>(M.v)[qq];
+      float4 uu = reinterpret_cast<const float4 *>(M.u)[qq];
+      float m[4];
+      int g[4], sh[4];
+      if (M.nc == 2) {
+        const uint32_t n = static_cast<uint32_t>(2 * qq);  // pair index of (g, s), s even
+        g[0] = static_cast<int>(P.sdiv.div(n));
+        sh[0] = static_cast<int>(n - static_cast<uint32_t>(g[0]) * S);
+        const float2 mm = reinterpret_cast<const float2 *>(M.minv)[g[0]];
+        m[0] = mm.x;
+        m[1] = mm.y;
+        m[2] = mm.x;
+        m[3] = mm.y;
+      } else {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const uint32_t n = static_cast<uint32_t>(4 * qq + i);
+          g[i] = static_cast<int>(P.sdiv.div(n));
+          sh[i] = static_cast<int>(n - static_cast<uint32_t>(g[i]) * S);
+          m[i] = M.minv[g[i]];
+        }
+      }
+      float4 acc = make_float4(r.x * m[0], r.y * m[1], r.z * m[2], r.w * m[3]);
+      vel.x += P.dt2 * acc.x;  // corrector (newmark.tpp:44-47)
+      vel.y += P.dt2 * acc.y;
+      vel.z += P.dt2 * acc.z;
+      vel.w += P.dt2 * acc.w;
+      if (record && M.taps.nsup > 0) {
+        if (M.nc == 2) {
+          apply_taps(M.taps, g[0], uu.x, uu.y, vel.x, vel.y, acc.x, acc.y,
+                     P.seis + (static_cast<size_t>(sh[0]) * P.max_sig + isig) * P.slots);
+          apply_taps(M.taps, g[0], uu.z, uu.w, vel.z, vel.w, acc.z, acc.w,
+                     P.seis + (static_cast<size_t>(sh[0] + 1) * P.max_sig + isig) * P.slots);
+        } else {
+          const float us[4] = {uu.x, uu.y, uu.z, uu.w}, vs[4] = {vel.x, vel.y, vel.z, vel.w};
+          const float as[4] = {acc.x, acc.y, acc.z, acc.w};
+#pragma unroll
+          for (int i = 0; i < 4; ++i)
+            apply_taps(M.taps, g[i], us[i], 0.f, vs[i], 0.f, as[i], 0.f,
+                       P.seis + (static_cast<size_t>(sh[i]) * P.max_sig + isig) * P.slots);
+        }
+      }
+      float4 *U = reinterpret_cast<float4 *>(M.u);
+      float4 *Vv = reinterpret_cast<float4 *>(M.v);
+      float4 *A = reinterpret_cast<float4 *>(M.a);
+      if (P.last) {
+        A[qq] = acc;
+        Vv[qq] = vel;
+      } else {
+        uu.x += P.dt * vel.x + P.dtsq2 * acc.x;  // next predictor (newmark.tpp:98-105)
+        uu.y += P.dt * vel.y + P.dtsq2 * acc.y;
+        uu.z += P.dt * vel.z + P.dtsq2 * acc.z;
+        uu.w += P.dt * vel.w + P.dtsq2 * acc.w;
+        vel.x += P.dt2 * acc.x;
+        vel.y += P.dt2 * acc.y;
+        vel.z += P.dt2 * acc.z;
+        vel.w += P.dt2 * acc.w;
+        U[qq] = uu;
+        Vv[qq] = vel;
+        A[qq] = make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+    }
+  } else if constexpr (!EXTRA) {
     // plain update, two pairs per iteration: both pairs' loads are issued
     // before either is stored, doubling the loads each thread has in flight
     // (the kernel is bound by DRAM latency)
