@@ -729,8 +729,6 @@ dev::UpdateParams update_params(sfb_context *c, WavefieldSet &W, int last, bool 
   }
   u.nshots = P.nshots;
   u.sdiv = dev::FastDiv::make(static_cast<uint32_t>(P.nshots));
-  u.quad = P.nshots % 2 == 0 ? 1 : 0;
-  for (int i = 0; i < u.nm; ++i) u.quad = u.quad && u.m[i].ld2 % 2 == 0;
   if (u.begin[u.nm] * 2 >= (1ull << 32)) throw std::invalid_argument("field too large for 32-bit update indexing");
   u.dt = static_cast<float>(P.dt);
   u.dt2 = static_cast<float>(P.dt / 2.0);

@@ -1778,41 +1778,63 @@ __global__ void k_update_all(UpdateParams P) {
     if (ck_uslot >= P.ck_count) ck_uslot = -1;
     if (ck_vslot >= P.ck_count) ck_vslot = -1;
   }
-  if (!EXTRA && P.quad) {
-    // plain update with an even shot count: quad q of a medium is pairs 2q
-    // and 2q + 1, read and written as one float4 per array (nc = 2: shots s
-    // and s + 1 of one point; nc = 1: four consecutive entries of [g][s])
-    const size_t totq = total / 2;
-    const size_t strideq = static_cast<size_t>(gridDim.x) * blockDim.x;
-    for (size_t q = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; q < totq; q += strideq) {
+  if constexpr (!EXTRA) {
+    // plain update: unit w of a medium is its pairs 2w and 2w + 1, read and
+    // written as one float4 per array (a medium with an odd number of pairs
+    // ends with a one-pair unit).  A pair is (g, s) with both components
+    // (nc = 2) or two consecutive entries of [g][s] (nc = 1); entry e of a
+    // unit is component e % 2 of its pair e / 2 (nc = 2) or entry e (nc = 1).
+    // first unit of media 1 and 2 (at most three media), in registers
+    const size_t ub1 = (P.begin[1] - P.begin[0] + 1) / 2;
+    const size_t ub2 = P.nm > 1 ? ub1 + (P.begin[2] - P.begin[1] + 1) / 2 : ub1;
+    const size_t units = P.nm > 2 ? ub2 + (P.begin[3] - P.begin[2] + 1) / 2 : ub2;
+    const size_t stride = static_cast<size_t>(gridDim.x) * blockDim.x;
+    for (size_t w = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; w < units; w += stride) {
       int mi = 0;
-      while (mi + 1 < P.nm && 2 * q >= P.begin[mi + 1]) ++mi;
+      size_t ub = 0;
+      if (P.nm > 1 && w >= ub1) { mi = 1; ub = ub1; }
+      if (P.nm > 2 && w >= ub2) { mi = 2; ub = ub2; }
       const UpdateMedium &M = P.m[mi];
-      const size_t qq = q - P.begin[mi] / 2;
-      const float4 r = reinterpret_cast<const float4 *>(M.a)[qq];
-      float4 vel = reinterpret_cast<const float4 *>(M.v)[qq];
-      float4 uu = reinterpret_cast<const float4 *>(M.u)[qq];
-      float m[4];
-      int g[4], sh[4];
-      if (M.nc == 2) {
-        const uint32_t n = static_cast<uint32_t>(2 * qq);  // pair index of (g, s), s even
-        g[0] = static_cast<int>(P.sdiv.div(n));
-        sh[0] = static_cast<int>(n - static_cast<uint32_t>(g[0]) * S);
-        const float2 mm = reinterpret_cast<const float2 *>(M.minv)[g[0]];
-        m[0] = mm.x;
-        m[1] = mm.y;
-        m[2] = mm.x;
-        m[3] = mm.y;
+      const size_t ld2 = P.begin[mi + 1] - P.begin[mi];
+      const size_t p0 = 2 * (w - ub);
+      const bool two = p0 + 1 < ld2;
+      float4 r, vel, uu;
+      if (two) {
+        r = reinterpret_cast<const float4 *>(M.a)[p0 / 2];
+        vel = reinterpret_cast<const float4 *>(M.v)[p0 / 2];
+        uu = reinterpret_cast<const float4 *>(M.u)[p0 / 2];
       } else {
+        const float2 r2 = reinterpret_cast<const float2 *>(M.a)[p0];
+        const float2 v2 = reinterpret_cast<const float2 *>(M.v)[p0];
+        const float2 u2 = reinterpret_cast<const float2 *>(M.u)[p0];
+        r = make_float4(r2.x, r2.y, 0.f, 0.f);
+        vel = make_float4(v2.x, v2.y, 0.f, 0.f);
+        uu = make_float4(u2.x, u2.y, 0.f, 0.f);
+      }
+      float m[4] = {0.f, 0.f, 0.f, 0.f};
+      int g[4] = {0, 0, 0, 0}, sh[4] = {0, 0, 0, 0};
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          const uint32_t n = static_cast<uint32_t>(4 * qq + i);
-          g[i] = static_cast<int>(P.sdiv.div(n));
-          sh[i] = static_cast<int>(n - static_cast<uint32_t>(g[i]) * S);
-          m[i] = M.minv[g[i]];
+      for (int i = 0; i < 2; ++i) {
+        if (i == 1 && !two) continue;
+        if (M.nc == 2) {
+          const uint32_t n = static_cast<uint32_t>(p0 + i);
+          const int gi = static_cast<int>(P.sdiv.div(n));
+          const float2 mm = reinterpret_cast<const float2 *>(M.minv)[gi];
+          g[2 * i] = g[2 * i + 1] = gi;
+          sh[2 * i] = sh[2 * i + 1] = static_cast<int>(n - static_cast<uint32_t>(gi) * S);
+          m[2 * i] = mm.x;
+          m[2 * i + 1] = mm.y;
+        } else {
+#pragma unroll
+          for (int j = 0; j < 2; ++j) {
+            const uint32_t n = static_cast<uint32_t>(2 * (p0 + i) + j);
+            g[2 * i + j] = static_cast<int>(P.sdiv.div(n));
+            sh[2 * i + j] = static_cast<int>(n - static_cast<uint32_t>(g[2 * i + j]) * S);
+            m[2 * i + j] = M.minv[g[2 * i + j]];
+          }
         }
       }
-      float4 acc = make_float4(r.x * m[0], r.y * m[1], r.z * m[2], r.w * m[3]);
+      const float4 acc = make_float4(r.x * m[0], r.y * m[1], r.z * m[2], r.w * m[3]);
       vel.x += P.dt2 * acc.x;  // corrector (newmark.tpp:44-47)
       vel.y += P.dt2 * acc.y;
       vel.z += P.dt2 * acc.z;
@@ -1821,24 +1843,20 @@ __global__ void k_update_all(UpdateParams P) {
         if (M.nc == 2) {
           apply_taps(M.taps, g[0], uu.x, uu.y, vel.x, vel.y, acc.x, acc.y,
                      P.seis + (static_cast<size_t>(sh[0]) * P.max_sig + isig) * P.slots);
-          apply_taps(M.taps, g[0], uu.z, uu.w, vel.z, vel.w, acc.z, acc.w,
-                     P.seis + (static_cast<size_t>(sh[0] + 1) * P.max_sig + isig) * P.slots);
+          if (two)
+            apply_taps(M.taps, g[2], uu.z, uu.w, vel.z, vel.w, acc.z, acc.w,
+                       P.seis + (static_cast<size_t>(sh[2]) * P.max_sig + isig) * P.slots);
         } else {
           const float us[4] = {uu.x, uu.y, uu.z, uu.w}, vs[4] = {vel.x, vel.y, vel.z, vel.w};
           const float as[4] = {acc.x, acc.y, acc.z, acc.w};
 #pragma unroll
-          for (int i = 0; i < 4; ++i)
-            apply_taps(M.taps, g[i], us[i], 0.f, vs[i], 0.f, as[i], 0.f,
-                       P.seis + (static_cast<size_t>(sh[i]) * P.max_sig + isig) * P.slots);
+          for (int e = 0; e < 4; ++e)
+            if (e < 2 || two)
+              apply_taps(M.taps, g[e], us[e], 0.f, vs[e], 0.f, as[e], 0.f,
+                         P.seis + (static_cast<size_t>(sh[e]) * P.max_sig + isig) * P.slots);
         }
       }
-      float4 *U = reinterpret_cast<float4 *>(M.u);
-      float4 *Vv = reinterpret_cast<float4 *>(M.v);
-      float4 *A = reinterpret_cast<float4 *>(M.a);
-      if (P.last) {
-        A[qq] = acc;
-        Vv[qq] = vel;
-      } else {
+      if (!P.last) {
         uu.x += P.dt * vel.x + P.dtsq2 * acc.x;  // next predictor (newmark.tpp:98-105)
         uu.y += P.dt * vel.y + P.dtsq2 * acc.y;
         uu.z += P.dt * vel.z + P.dtsq2 * acc.z;
@@ -1847,86 +1865,18 @@ __global__ void k_update_all(UpdateParams P) {
         vel.y += P.dt2 * acc.y;
         vel.z += P.dt2 * acc.z;
         vel.w += P.dt2 * acc.w;
-        U[qq] = uu;
-        Vv[qq] = vel;
-        A[qq] = make_float4(0.f, 0.f, 0.f, 0.f);
       }
-    }
-  } else if constexpr (!EXTRA) {
-    // plain update, two pairs per iteration: both pairs' loads are issued
-    // before either is stored, doubling the loads each thread has in flight
-    // (the kernel is bound by DRAM latency)
-    struct Pair {
-      int mi, g0, s0, g1, s1;
-      size_t at;
-      float2 m, r, vel, uu;
-    };
-    auto load = [&](size_t j, Pair &q) {
-      int mi = 0;
-      while (mi + 1 < P.nm && j >= P.begin[mi + 1]) ++mi;
-      const UpdateMedium &M = P.m[mi];
-      const size_t jj = j - P.begin[mi];
-      q.mi = mi;
-      q.at = jj;
-      if (M.nc == 2) {
-        const uint32_t n = static_cast<uint32_t>(jj);
-        q.g0 = q.g1 = static_cast<int>(P.sdiv.div(n));
-        q.s0 = q.s1 = static_cast<int>(n - static_cast<uint32_t>(q.g0) * S);
-        q.m = reinterpret_cast<const float2 *>(M.minv)[q.g0];
+      // last step: a and v stored, u kept; otherwise u, v stored and a = 0
+      const float4 a_out = P.last ? acc : make_float4(0.f, 0.f, 0.f, 0.f);
+      if (two) {
+        if (!P.last) reinterpret_cast<float4 *>(M.u)[p0 / 2] = uu;
+        reinterpret_cast<float4 *>(M.v)[p0 / 2] = vel;
+        reinterpret_cast<float4 *>(M.a)[p0 / 2] = a_out;
       } else {
-        const uint32_t n0 = static_cast<uint32_t>(2 * jj), n1 = n0 + 1;
-        q.g0 = static_cast<int>(P.sdiv.div(n0));
-        q.s0 = static_cast<int>(n0 - static_cast<uint32_t>(q.g0) * S);
-        q.g1 = static_cast<int>(P.sdiv.div(n1));
-        q.s1 = static_cast<int>(n1 - static_cast<uint32_t>(q.g1) * S);
-        q.m = make_float2(M.minv[q.g0], M.minv[q.g1]);
+        if (!P.last) reinterpret_cast<float2 *>(M.u)[p0] = make_float2(uu.x, uu.y);
+        reinterpret_cast<float2 *>(M.v)[p0] = make_float2(vel.x, vel.y);
+        reinterpret_cast<float2 *>(M.a)[p0] = make_float2(a_out.x, a_out.y);
       }
-      q.r = reinterpret_cast<const float2 *>(M.a)[q.at];
-      q.vel = reinterpret_cast<const float2 *>(M.v)[q.at];
-      q.uu = reinterpret_cast<const float2 *>(M.u)[q.at];
-    };
-    auto finish = [&](Pair &q) {
-      const UpdateMedium &M = P.m[q.mi];
-      float2 acc, vel = q.vel, uu = q.uu;
-      acc.x = q.r.x * q.m.x;
-      acc.y = q.r.y * q.m.y;
-      vel.x += P.dt2 * acc.x;  // corrector (newmark.tpp:44-47)
-      vel.y += P.dt2 * acc.y;
-      if (record && M.taps.nsup > 0) {
-        if (M.nc == 2) {
-          apply_taps(M.taps, q.g0, uu.x, uu.y, vel.x, vel.y, acc.x, acc.y,
-                     P.seis + (static_cast<size_t>(q.s0) * P.max_sig + isig) * P.slots);
-        } else {
-          apply_taps(M.taps, q.g0, uu.x, 0.f, vel.x, 0.f, acc.x, 0.f,
-                     P.seis + (static_cast<size_t>(q.s0) * P.max_sig + isig) * P.slots);
-          apply_taps(M.taps, q.g1, uu.y, 0.f, vel.y, 0.f, acc.y, 0.f,
-                     P.seis + (static_cast<size_t>(q.s1) * P.max_sig + isig) * P.slots);
-        }
-      }
-      float2 *U = reinterpret_cast<float2 *>(M.u);
-      float2 *Vv = reinterpret_cast<float2 *>(M.v);
-      float2 *A = reinterpret_cast<float2 *>(M.a);
-      if (P.last) {
-        A[q.at] = acc;
-        Vv[q.at] = vel;
-      } else {
-        uu.x += P.dt * vel.x + P.dtsq2 * acc.x;  // next predictor (newmark.tpp:98-105)
-        uu.y += P.dt * vel.y + P.dtsq2 * acc.y;
-        vel.x += P.dt2 * acc.x;
-        vel.y += P.dt2 * acc.y;
-        U[q.at] = uu;
-        Vv[q.at] = vel;
-        A[q.at] = make_float2(0.f, 0.f);
-      }
-    };
-    const size_t stride = static_cast<size_t>(gridDim.x) * blockDim.x;
-    for (size_t j = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; j < total; j += 2 * stride) {
-      Pair qa, qb;
-      const bool two = j + stride < total;
-      load(j, qa);
-      if (two) load(j + stride, qb);
-      finish(qa);
-      if (two) finish(qb);
     }
   } else
   for (size_t j = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; j < total;

@@ -208,9 +208,6 @@ struct UpdateParams {
   float *seis;            // [S][max_sig][slots]
   int slots, max_sig, nsbs;
   int ck_interval, ck_count;  // snapshot cadence K and slots (0: none)
-  // even shot count: every medium's range holds an even number of pairs and
-  // the plain update moves two pairs (one float4) per array access
-  int quad;
 };
 
 // Restore the backward wavefield of the combined run from the forward
