@@ -373,6 +373,28 @@ k_stiffness_rp(Static st, MediumFields f, int nshots, StaceyStore ss, const int 
 #pragma unroll
       for (int ix = 0; ix < N; ++ix) s_u[el * NN + iz * N + ix] = ur[ix];
       __syncthreads();
+      // gamma-derivative by columns (this thread takes column j = iz; same
+      // sums in the same order as the row form), left where the owner of
+      // each row reads it
+      V *sfg = s_fg + el * NN;
+      {
+        V colv[N];
+#pragma unroll
+        for (int l = 0; l < N; ++l) colv[l] = s_u[el * NN + l * N + iz];
+#pragma unroll
+        for (int p = 0; p < N; ++p) {
+          V d;
+#pragma unroll
+          for (int c = 0; c < NC; ++c) {
+            float sum = 0.f;
+#pragma unroll
+            for (int l = 0; l < N; ++l) sum += c_hp[p * N + l] * comp(colv[l], c);
+            set_comp(d, c, sum);
+          }
+          sfg[p * N + iz] = d;
+        }
+      }
+      __syncthreads();
       V fx[N];
 #pragma unroll
       for (int ix = 0; ix < N; ++ix) {
@@ -382,16 +404,13 @@ k_stiffness_rp(Static st, MediumFields f, int nshots, StaceyStore ss, const int 
         const float jac = blk[5 * NN + k];
         const float m0 = blk[OFF_M0 + k], m1 = blk[OFF_M1 + k];
         float dxi[NC], dga[NC];
+        const V dg = sfg[k];  // read before this thread overwrites point k with F(., gamma)
 #pragma unroll
-        for (int c = 0; c < NC; ++c) { dxi[c] = 0.f; dga[c] = 0.f; }
+        for (int c = 0; c < NC; ++c) { dxi[c] = 0.f; dga[c] = comp(dg, c); }
 #pragma unroll
         for (int l = 0; l < N; ++l) {
-          const V col = s_u[el * NN + l * N + ix];
 #pragma unroll
-          for (int c = 0; c < NC; ++c) {
-            dxi[c] += c_hp[ix * N + l] * comp(ur[l], c);
-            dga[c] += hpz[l] * comp(col, c);
-          }
+          for (int c = 0; c < NC; ++c) dxi[c] += c_hp[ix * N + l] * comp(ur[l], c);
         }
         float du[NC][2];
 #pragma unroll
@@ -418,23 +437,41 @@ k_stiffness_rp(Static st, MediumFields f, int nshots, StaceyStore ss, const int 
           set_comp(f1, c, jac * (T[c][0] * gax + T[c][1] * gaz));
         }
         fx[ix] = f0;
-        s_fg[el * NN + k] = f1;
+        sfg[k] = f1;
+      }
+      __syncthreads();
+      // gamma-sum of the divergence by columns, left in the displacement
+      // tile (free now: the rows are in registers)
+      V *st2 = s_u + el * NN;
+      {
+        V colf[N];
+#pragma unroll
+        for (int l = 0; l < N; ++l) colf[l] = sfg[l * N + iz];
+#pragma unroll
+        for (int p = 0; p < N; ++p) {
+          V d;
+#pragma unroll
+          for (int c = 0; c < NC; ++c) {
+            float sum = 0.f;
+#pragma unroll
+            for (int l = 0; l < N; ++l) sum += comp(colf[l], c) * c_hpw[p * N + l];
+            set_comp(d, c, sum);
+          }
+          st2[p * N + iz] = d;
+        }
       }
       __syncthreads();
       float accr[N][2];
 #pragma unroll
       for (int ix = 0; ix < N; ++ix) {
         float t1[NC], t2[NC];
+        const V g2 = st2[iz * N + ix];
 #pragma unroll
-        for (int c = 0; c < NC; ++c) { t1[c] = 0.f; t2[c] = 0.f; }
+        for (int c = 0; c < NC; ++c) { t1[c] = 0.f; t2[c] = comp(g2, c); }
 #pragma unroll
         for (int l = 0; l < N; ++l) {
-          const V col = s_fg[el * NN + l * N + ix];
 #pragma unroll
-          for (int c = 0; c < NC; ++c) {
-            t1[c] += comp(fx[l], c) * c_hpw[ix * N + l];
-            t2[c] += comp(col, c) * hpwz[l];
-          }
+          for (int c = 0; c < NC; ++c) t1[c] += comp(fx[l], c) * c_hpw[ix * N + l];
         }
 #pragma unroll
         for (int c = 0; c < NC; ++c) accr[ix][c] = (wz * t1[c] + c_w[ix] * t2[c]) * -1.0f;
@@ -703,22 +740,42 @@ k_stiffness_rpa(Static st, MediumFields f, StaceyStore ss, const int *istep_dev,
     V ur[N];
 #pragma unroll
     for (int ix = 0; ix < N; ++ix) ur[ix] = su[iz * N + ix];
+    // gamma-derivative by columns: this thread takes column j = iz of its
+    // element (5 shared loads instead of 25 for its row) and leaves the
+    // derivative of point (p, j) where the owner of row p reads it; same
+    // sums in the same order as the row form
+    V *sfg = s_fg + el * NN;
+    {
+      V colv[N];
+#pragma unroll
+      for (int l = 0; l < N; ++l) colv[l] = su[l * N + iz];
+#pragma unroll
+      for (int p = 0; p < N; ++p) {
+        V d;
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+          float sum = 0.f;
+#pragma unroll
+          for (int l = 0; l < N; ++l) sum += c_hp[p * N + l] * comp(colv[l], c);
+          set_comp(d, c, sum);
+        }
+        sfg[p * N + iz] = d;
+      }
+    }
+    __syncthreads();
     V fx[N];
 #pragma unroll
     for (int ix = 0; ix < N; ++ix) {
       const int k = iz * N + ix;
       const float m0 = blk[OFF_M0 + k], m1 = blk[OFF_M1 + k];
       float dxi[NC], dga[NC];
+      const V dg = sfg[k];  // read before this thread overwrites point k with F(., gamma)
 #pragma unroll
-      for (int c = 0; c < NC; ++c) { dxi[c] = 0.f; dga[c] = 0.f; }
+      for (int c = 0; c < NC; ++c) { dxi[c] = 0.f; dga[c] = comp(dg, c); }
 #pragma unroll
       for (int l = 0; l < N; ++l) {
-        const V col = su[l * N + ix];
 #pragma unroll
-        for (int c = 0; c < NC; ++c) {
-          dxi[c] += c_hp[ix * N + l] * comp(ur[l], c);
-          dga[c] += hpz[l] * comp(col, c);
-        }
+        for (int c = 0; c < NC; ++c) dxi[c] += c_hp[ix * N + l] * comp(ur[l], c);
       }
       float du[NC][2];
 #pragma unroll
@@ -745,23 +802,42 @@ k_stiffness_rpa(Static st, MediumFields f, StaceyStore ss, const int *istep_dev,
         set_comp(f1, c, jac * (T[c][0] * gax + T[c][1] * gaz));
       }
       fx[ix] = f0;
-      s_fg[el * NN + k] = f1;
+      sfg[k] = f1;
+    }
+    __syncthreads();
+    // gamma-sum of the divergence by columns, left in this chunk's
+    // displacement buffer (free now: the rows are in registers, the next
+    // chunk's gathers go to the other buffer)
+    V *st2 = s_u + (it & 1) * EPB * NN + el * NN;
+    {
+      V colf[N];
+#pragma unroll
+      for (int l = 0; l < N; ++l) colf[l] = sfg[l * N + iz];
+#pragma unroll
+      for (int p = 0; p < N; ++p) {
+        V d;
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+          float sum = 0.f;
+#pragma unroll
+          for (int l = 0; l < N; ++l) sum += comp(colf[l], c) * c_hpw[p * N + l];
+          set_comp(d, c, sum);
+        }
+        st2[p * N + iz] = d;
+      }
     }
     __syncthreads();
     float accr[N][2];
 #pragma unroll
     for (int ix = 0; ix < N; ++ix) {
       float t1[NC], t2[NC];
+      const V g2 = st2[iz * N + ix];
 #pragma unroll
-      for (int c = 0; c < NC; ++c) { t1[c] = 0.f; t2[c] = 0.f; }
+      for (int c = 0; c < NC; ++c) { t1[c] = 0.f; t2[c] = comp(g2, c); }
 #pragma unroll
       for (int l = 0; l < N; ++l) {
-        const V col = s_fg[el * NN + l * N + ix];
 #pragma unroll
-        for (int c = 0; c < NC; ++c) {
-          t1[c] += comp(fx[l], c) * c_hpw[ix * N + l];
-          t2[c] += comp(col, c) * hpwz[l];
-        }
+        for (int c = 0; c < NC; ++c) t1[c] += comp(fx[l], c) * c_hpw[ix * N + l];
       }
 #pragma unroll
       for (int c = 0; c < NC; ++c) accr[ix][c] = (wz * t1[c] + c_w[ix] * t2[c]) * -1.0f;
