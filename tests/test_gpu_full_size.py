@@ -1,10 +1,12 @@
-"""Parity at the benchmark's full size: the coupled acoustic-elastic forward
+"""Parity at the benchmark's full sizes.  The coupled acoustic-elastic forward
 on 400 x 300 NGLL=5 elements (1,924,402 points, the workload bench.py times),
 1400 steps (the source sits mid-water, 1.5 km above the sea floor: the wave
 reaches the elastic medium after about 1.25 s), final wavefields of both
 media and the receivers' pressure traces against the FP32 and FP64 oracle on
 identical inputs, for the compact-block kernel the autotuner picks there and
-for the full-block kernel.  Same bar as test_gpu_forward.py:
+for the full-block kernel; and the batched 64-shot workload (800 x 400), two
+of its shots against the oracle run of each alone.  Same bar as
+test_gpu_forward.py:
     e(gpu, fp32) <= 1e-5  or  e(gpu, fp64) <= 1e-5 + 2 * e(fp32, fp64).
 The oracle's CPU time is the limit on the step count (about 40 s per
 precision on 16 host threads)."""
@@ -65,3 +67,26 @@ def test_full_size_coupled_fields(oracle_fields, variant):
     print("variant %d pressure traces: vs FP32 oracle %.2e, vs FP64 %.2e (FP32 oracle vs FP64 %.2e)"
           % (variant, e32, e64, eref))
     assert e32 <= TOL_FP32 or e64 <= TOL_FP32 + 2.0 * eref, (variant, "traces", e32, e64, eref)
+
+
+def test_full_size_batched_shots():
+    """The batched workload at full size (800 x 400 NGLL=5 elements, 5.1 M
+    points, 64 shots in one context, the packed two-shots-per-lane kernel):
+    the first and the last shot's final P-SV fields after 300 steps against
+    the oracle run of that shot alone."""
+    from oracle import bridge
+    nstep = 300
+    sim = Simulation.structured(W.batched(1.0, nshots=64, nstep=nstep))
+    assert sim.info().nshots == 64
+    sim.run_forward()
+    threads = max(1, min(32, os.cpu_count() or 1))
+    for shot in (0, 63):
+        o32 = bridge.forward(sim, 32, shot=shot, threads=threads, want_fields=True)["psv"]
+        o64 = bridge.forward(sim, 64, shot=shot, threads=threads, want_fields=True)["psv"]
+        for which, name in ((0, "u"), (1, "v"), (2, "a")):
+            g = sim.field(0, which, shot=shot)
+            assert np.isfinite(g).all() and np.abs(o64[which]).max() > 0, (shot, name)
+            e32, e64, eref = rel_l2(g, o32[which]), rel_l2(g, o64[which]), rel_l2(o32[which], o64[which])
+            print("batched shot %d %s: vs FP32 oracle %.2e, vs FP64 %.2e (FP32 oracle vs FP64 %.2e)"
+                  % (shot, name, e32, e64, eref))
+            assert e32 <= TOL_FP32 or e64 <= TOL_FP32 + 2.0 * eref, (shot, name, e32, e64, eref)
