@@ -212,34 +212,85 @@ def sim_stream(sim):
     return torch.cuda.ExternalStream(ptr.value)
 
 
-def batched_forward(steps):
+def e2e_run(sim, stream, steps):
+    """End to end through the C ABI with host buffers: upload every source's
+    time function from pinned host memory (H2D), run `steps` fused steps,
+    read all seismograms back (D2H); device time of the whole sequence and
+    the bytes copied per step."""
+    import ctypes as C
+    import torch
+    from specfempp_b200 import _capi as A
+    lib = A.load()
+    info = sim.info()
+    view = sim.problem_view()
+    nsrc = view.nsources
+    n = info.nstep * 2
+    flat = np.ctypeslib.as_array(view.src_stf, shape=(nsrc * n,))
+    stf_pinned = [torch.from_numpy(flat[i * n:(i + 1) * n].copy()).pin_memory() for i in range(nsrc)]
+    seis = torch.empty((info.nshots, info.max_sig_step, info.nseismogram_types, info.nreceivers, 2),
+                       dtype=torch.float32).pin_memory()
+    torch.cuda.synchronize()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for i in range(nsrc):
+        A.check(lib.sfb_set_source_time_function(sim.handle, i, C.cast(stf_pinned[i].data_ptr(), C.POINTER(C.c_float)),
+                                                 stf_pinned[i].numel()), sim.handle)
+    sim.run_forward(steps)
+    per_shot = seis[0].numel()
+    for s in range(info.nshots):
+        A.check(lib.sfb_get_seismograms(sim.handle, 0, s, C.cast(seis[s].data_ptr(), C.POINTER(C.c_float)),
+                                        per_shot), sim.handle)
+    f1.record(stream)
+    f1.synchronize()
+    h2d = sum(t.numel() * 4 for t in stf_pinned)
+    d2h = seis.numel() * 4
+    return f0.elapsed_time(f1), h2d / steps, d2h / steps
+
+
+def batched_forward(steps, cpu_seconds=None):
     """The 64-shot batched forward (800 x 400 elements): device time per step
-    and whole-step algorithmic HBM bytes against the measured peak."""
+    and whole-step algorithmic HBM bytes against the measured peak, the same
+    run end to end through the C ABI with host buffers, and the oracle's
+    per-shot rate on the host cores."""
     import ctypes as C
     from specfempp_b200 import Simulation, _capi as A
-    p = make_problem("batched", GRAPH_STEPS + 3 + steps + 1)
+    p = make_problem("batched", GRAPH_STEPS + 3 + 3 * steps + 1)
     with Simulation.structured(p) as sim:
         pin_variant(sim)
         sim.initialize()
         stream = sim_stream(sim)
         sim.run_forward(GRAPH_STEPS)
+        sim.run_forward(steps)  # set-up: captures the graph of the remainder chunk
         sim.run_forward(3)
         ms = event_time(stream, lambda: sim.run_forward(steps))
+        ms_e2e, h2d, d2h = e2e_run(sim, stream, steps)
         info = sim.info()
         mean_ms = C.c_double()
         A.check(A.load().sfb_time_stiffness(sim.handle, 0, 10, C.byref(mean_ms)), sim.handle)
     peak, _ = measured_peak()
     per_step = ms / steps
     b = step_bytes(info)
-    return {
+    updates = info.nshots * sum(info.nglob) * steps
+    out = {
         "workload": workload_config("batched", info, p)["workload"],
-        "value": info.nshots * sum(info.nglob) * steps / (ms / 1000.0), "unit": "GLL-point-updates/s",
+        "value": updates / (ms / 1000.0), "unit": "GLL-point-updates/s",
         "ms_per_step": per_step, "steps": steps,
         "step_roofline": {"bound": "hbm", "algorithmic_bytes_per_step": b,
                           "achieved": b / (per_step / 1000.0) / 1e9, "peak": peak, "unit": "GB/s",
                           "frac": b / (per_step / 1000.0) / 1e9 / peak},
         "stiffness_ms": mean_ms.value,
+        "e2e": {"value": updates / (ms_e2e / 1000.0), "unit": "GLL-point-updates/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
     }
+    if cpu_seconds:
+        threads = os.cpu_count() or 1
+        rate, n, dt, _ = cpu_rate("batched", None, threads, budget_s=cpu_seconds)
+        out["cpu_baseline"] = {"value": rate, "unit": "GLL-point-updates/s", "cores": threads, "kind": "port",
+                               "sample": "shot 0 of the 64, %d full time steps (oracle FP32, OpenMP over "
+                                         "elements; shots are independent, so the per-shot rate is the "
+                                         "whole job's), %.1f s" % (n, dt)}
+    return out
 
 
 def fwi_comparison(nshots=64, nstep=400, reps=2):
@@ -298,7 +349,7 @@ def cpu_rate(workload, nstep_hint, threads, budget_s=15.0, sample_steps=None):
     t = time.perf_counter()
     bridge.forward(sim, 32, nstep=n, threads=threads)
     dt = time.perf_counter() - t
-    updates = info.nshots * sum(info.nglob) * n
+    updates = sum(info.nglob) * n  # the oracle runs one shot of the workload
     return updates / dt, n, dt, info
 
 
@@ -340,7 +391,7 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
     K, Wm = args.steps, args.warmup
-    nstep_total = GRAPH_STEPS + Wm + 2 * K + 2
+    nstep_total = GRAPH_STEPS + Wm + 3 * K + 2
     p = make_problem(args.workload, nstep_total)
     sim = Simulation.structured(p)
     pin_variant(sim)
@@ -351,8 +402,11 @@ def run_ours(args):
     A.check(lib.sfb_get_stream(sim.handle, C.byref(ptr)), sim.handle)
     stream = torch.cuda.ExternalStream(ptr.value)
 
-    # set-up: capture the CUDA graph of one 25-step chunk, then W warm-up steps
+    # set-up: capture the CUDA graphs of a 25-step chunk and of the remainder
+    # chunk of a K-step run (so the timed run is graph-launched for any K),
+    # then W warm-up steps
     sim.run_forward(GRAPH_STEPS)
+    sim.run_forward(K)
     sim.run_forward(Wm)
     launches0 = sim.info().kernel_launches
 
@@ -381,35 +435,15 @@ def run_ours(args):
 
     # end to end through the C ABI with host buffers: upload the source time
     # functions (H2D), run K steps, read the seismograms back (D2H)
-    view = sim.problem_view()
-    nsrc = view.nsources
-    stf = [np.ctypeslib.as_array(view.src_stf, shape=(nsrc * info.nstep * 2,))[i * info.nstep * 2:(i + 1) * info.nstep * 2].copy()
-           for i in range(nsrc)]
-    stf_pinned = [torch.from_numpy(s).pin_memory() for s in stf]
-    seis = torch.empty((info.max_sig_step, info.nseismogram_types, info.nreceivers, 2),
-                       dtype=torch.float32).pin_memory()
     if world > 1:
         dist.barrier()
-    torch.cuda.synchronize()
-    f0 = torch.cuda.Event(enable_timing=True)
-    f1 = torch.cuda.Event(enable_timing=True)
-    f0.record(stream)
-    for i in range(nsrc):
-        A.check(lib.sfb_set_source_time_function(sim.handle, i, C.cast(stf_pinned[i].data_ptr(), C.POINTER(C.c_float)),
-                                                 stf_pinned[i].numel()), sim.handle)
-    sim.run_forward(K)
-    A.check(lib.sfb_get_seismograms(sim.handle, 0, 0, C.cast(seis.data_ptr(), C.POINTER(C.c_float)), seis.numel()),
-            sim.handle)
-    f1.record(stream)
-    f1.synchronize()
-    ms_e2e = f0.elapsed_time(f1)
+    ms_e2e, h2d, d2h = e2e_run(sim, stream, K)
     if world > 1:
         t = torch.tensor([ms_e2e], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms_e2e = float(t.item())
     e2e_value = world * info.nshots * npts * K / (ms_e2e / 1000.0)
-    h2d = nsrc * 2 * 4  # one STF sample pair per source per step
-    d2h = info.nshots * info.nseismogram_types * info.nreceivers * 2 * 4 // max(1, info.nstep_between_samples)
+    view = sim.problem_view()
 
     # roofline of the dominant kernel (elastic stiffness)
     dominant = 0 if info.nelements[0] > 0 else (3 if info.nelements[3] > 0 else 1)
@@ -448,7 +482,7 @@ def run_ours(args):
                              "frac": step_b / (ms / K / 1000.0) / 1e9 / peak}
     if world == 1 and args.workload == "coupled" and not args.no_secondary:
         sim.close()
-        line["batched"] = batched_forward(min(K, 100))
+        line["batched"] = batched_forward(min(K, 100), None if args.no_cpu_baseline else args.cpu_seconds)
         line["fwi"] = fwi_comparison()
     if world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1

@@ -371,22 +371,25 @@ SFB_API int sfb_get_problem_view(const sfb_context *ctx,
 /* No counterpart in the reference.  Assembles the mass matrix of one medium
  * in FP64 and writes its FP32 inverse, for callers that cannot allocate
  * device memory where they need it: a host framework that hands out every
- * device buffer from its own pool, code running inside a CUDA stream capture
- * (cudaMalloc is not allowed there), or a real-time loop that must not touch
- * the allocator.  The caller passes device inputs (per local point of the
- * medium's `nelem` elements, point p = (e * ngll + iz) * ngll + ix: the
- * medium-local point index, the Jacobian, the material -- P-SV: kappa, mu,
- * rho; SH: mu, rho, unused; acoustic: rho_inverse, kappa, unused -- and
- * optionally the Stacey tags / normals / weights, NULL for none), the host
- * GLL weights, and the device output minv[npoints * ncomp] (components
- * interleaved).  Work is enqueued on `stream` (a cudaStream_t, NULL for the
- * default stream).
+ * device buffer from its own pool and forbids plugins from calling
+ * cudaMalloc, or a real-time loop that must not touch the allocator (a
+ * cudaMalloc can synchronise the device).  The caller passes device inputs
+ * (per local point of the medium's `nelem` elements, point
+ * p = (e * ngll + iz) * ngll + ix: the medium-local point index, the
+ * Jacobian, the material -- P-SV: kappa, mu, rho; SH: mu, rho, unused;
+ * acoustic: rho_inverse, kappa, unused -- and optionally the Stacey tags /
+ * normals / weights, NULL for none), the host GLL weights, and the device
+ * output minv[npoints * ncomp] (components interleaved).  Work is enqueued
+ * on `stream` (a cudaStream_t, NULL for the default stream).
  * The only scratch is a fixed FP64 device array of SFB_NOALLOC_MAX_DOFS
- * entries (16 MiB) that every GPU loading the library holds until exit;
- * npoints * ncomp above that limit is rejected with SFB_E_INVALID.  The
- * first call on a device looks up the array's address, so make it before any
- * stream capture.  All calls on a device share the array: each call clears
- * what it uses, and calls that overlap on the GPU race.  Errors are reported
+ * entries (16 MiB) plus one error word, which every GPU loading the library
+ * holds until exit; npoints * ncomp above that limit is rejected with
+ * SFB_E_INVALID.  The first call on a device looks up the array's address
+ * (cudaGetSymbolAddress), so make it before any stream capture; a device
+ * reset after it is not supported.  All calls on a device share the array:
+ * each call clears what it uses, and calls that overlap on the GPU race.  A
+ * point index outside [0, npoints) is skipped on the device and the whole
+ * output of that call is set to NaN.  Errors found on the host are reported
  * through sfb_noalloc_last_error(). */
 #define SFB_NOALLOC_MAX_DOFS (1 << 21)
 SFB_API int sfb_assemble_inverse_mass_noalloc(

@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -119,7 +120,7 @@ struct sfb_context {
   DBuf<float> adj_array, adj_stf;
   int nadj = 0;
   DBuf<double> kern;        // Frechet accumulators [nspec][N*N][3], device element order
-  cudaGraphExec_t graph_combined = nullptr;
+  std::map<int, cudaGraphExec_t> graphs_combined;  // combined-run graphs by step count
   std::vector<float> host_seis;
   // seismogram taps per medium (fused path)
   struct Taps {
@@ -143,13 +144,22 @@ struct sfb_context {
   int ck_interval = 0, ck_count = 0;
   DBuf<float> ck_u[4], ck_v[4];
   size_t ck_stride[4] = {0, 0, 0, 0};
-  cudaGraphExec_t graph = nullptr;
-  int graph_steps = 0;
+  // forward CUDA graphs by the number of fused steps they hold (the full
+  // chunk and the remainders met so far)
+  std::map<int, cudaGraphExec_t> graphs;
   uint64_t launches = 0;  // kernels launched so far (graph replays included)
 
+  void drop_forward_graphs() {
+    for (auto &kv : graphs) cudaGraphExecDestroy(kv.second);
+    graphs.clear();
+  }
+  void drop_combined_graphs() {
+    for (auto &kv : graphs_combined) cudaGraphExecDestroy(kv.second);
+    graphs_combined.clear();
+  }
   ~sfb_context() {
-    if (graph) cudaGraphExecDestroy(graph);
-    if (graph_combined) cudaGraphExecDestroy(graph_combined);
+    drop_forward_graphs();
+    drop_combined_graphs();
     if (stream) cudaStreamDestroy(stream);
   }
 };
@@ -850,26 +860,31 @@ void run_forward_fused(sfb_context *c, int nstep, int use_graph) {
   for (int m : kMedia)
     if (W.f[m].nglob > 0) ++c->launches;
   c->launches += static_cast<uint64_t>(fused_step_launches(c, W)) * nstep;
+  // the body runs as graph launches of K fused steps plus one graph of the
+  // remainder, each captured on first use and kept (a run of any length is
+  // graph-launched once its chunk sizes have been seen)
   const int body = nstep - 1;
-  constexpr int K = 25;  // fused steps per CUDA graph
-  if (use_graph && body >= K) {
-    if (!c->graph || c->graph_steps != K) {
-      if (c->graph) cudaGraphExecDestroy(c->graph);
-      c->graph = nullptr;
-      cudaGraph_t g;
-      ck(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
-      for (int k = 0; k < K; ++k) enqueue_fused_step(c, W, 0);
-      ck(cudaStreamEndCapture(c->stream, &g), "end capture");
-      ck(cudaGraphInstantiate(&c->graph, g, 0), "graph instantiate");
-      cudaGraphDestroy(g);
-      c->graph_steps = K;
-    }
+  constexpr int K = 25;  // fused steps per full CUDA graph
+  auto graph_of = [&](int steps) {
+    auto it = c->graphs.find(steps);
+    if (it != c->graphs.end()) return it->second;
+    cudaGraph_t g;
+    cudaGraphExec_t ex = nullptr;
+    ck(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+    for (int k = 0; k < steps; ++k) enqueue_fused_step(c, W, 0);
+    ck(cudaStreamEndCapture(c->stream, &g), "end capture");
+    ck(cudaGraphInstantiate(&ex, g, 0), "graph instantiate");
+    cudaGraphDestroy(g);
+    c->graphs[steps] = ex;
+    return ex;
+  };
+  if (use_graph && body > 0) {
     int done = 0;
     while (done + K <= body) {
-      ck(cudaGraphLaunch(c->graph, c->stream), "graph launch");
+      ck(cudaGraphLaunch(graph_of(K), c->stream), "graph launch");
       done += K;
     }
-    for (; done < body; ++done) enqueue_fused_step(c, W, 0);
+    if (done < body) ck(cudaGraphLaunch(graph_of(body - done), c->stream), "graph launch");
   } else {
     for (int k = 0; k < body; ++k) enqueue_fused_step(c, W, 0);
   }
@@ -1220,18 +1235,27 @@ void run_combined_fused(sfb_context *c, int use_graph) {
   const int body = N - 2;  // steps N-2 .. 1 in the body, step 0 closes
   constexpr int K = 25;
   int done = 0;
-  if (use_graph && body >= K) {
-    if (!c->graph_combined) {
-      cudaGraph_t g;
-      ck(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
-      for (int k = 0; k < K; ++k) enqueue_combined_step(c, A, B, 0);
-      ck(cudaStreamEndCapture(c->stream, &g), "end capture");
-      ck(cudaGraphInstantiate(&c->graph_combined, g, 0), "graph instantiate");
-      cudaGraphDestroy(g);
-    }
+  auto graph_of = [&](int steps) {
+    auto it = c->graphs_combined.find(steps);
+    if (it != c->graphs_combined.end()) return it->second;
+    cudaGraph_t g;
+    cudaGraphExec_t ex = nullptr;
+    ck(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+    for (int k = 0; k < steps; ++k) enqueue_combined_step(c, A, B, 0);
+    ck(cudaStreamEndCapture(c->stream, &g), "end capture");
+    ck(cudaGraphInstantiate(&ex, g, 0), "graph instantiate");
+    cudaGraphDestroy(g);
+    c->graphs_combined[steps] = ex;
+    return ex;
+  };
+  if (use_graph && body > 0) {
     while (done + K <= body) {
-      ck(cudaGraphLaunch(c->graph_combined, c->stream), "graph launch");
+      ck(cudaGraphLaunch(graph_of(K), c->stream), "graph launch");
       done += K;
+    }
+    if (done < body) {
+      ck(cudaGraphLaunch(graph_of(body - done), c->stream), "graph launch");
+      done = body;
     }
   }
   for (; done < body; ++done) enqueue_combined_step(c, A, B, 0);
@@ -1320,8 +1344,7 @@ SFB_API int sfb_set_newmark_compensation(sfb_context *ctx, int enable) {
       }
     }
     ctx->compensated = enable != 0;
-    if (ctx->graph) cudaGraphExecDestroy(ctx->graph);  // captured launches hold the old pointers
-    ctx->graph = nullptr;
+    ctx->drop_forward_graphs();  // captured launches hold the old pointers
     return SFB_OK;
   });
 }
@@ -1348,10 +1371,8 @@ SFB_API int sfb_set_checkpoint_interval(sfb_context *ctx, int interval) {
     }
     ctx->ck_interval = count > 0 ? interval : 0;
     ctx->ck_count = count;
-    if (ctx->graph) cudaGraphExecDestroy(ctx->graph);
-    ctx->graph = nullptr;
-    if (ctx->graph_combined) cudaGraphExecDestroy(ctx->graph_combined);
-    ctx->graph_combined = nullptr;
+    ctx->drop_forward_graphs();
+    ctx->drop_combined_graphs();
     return SFB_OK;
   });
 }
@@ -1363,10 +1384,8 @@ SFB_API int sfb_set_stiffness_variant(sfb_context *ctx, int medium, int variant)
     const int top = ctx->P.nshots == 1 ? dev::kRowAffine : dev::kShotsSingle;
     if (variant < dev::kShotsAuto || variant > top) throw std::invalid_argument("unknown stiffness variant");
     ctx->shots_variant[medium] = variant;
-    if (ctx->graph) cudaGraphExecDestroy(ctx->graph);  // captured launches use the old kernel
-    ctx->graph = nullptr;
-    if (ctx->graph_combined) cudaGraphExecDestroy(ctx->graph_combined);
-    ctx->graph_combined = nullptr;
+    ctx->drop_forward_graphs();  // captured launches use the old kernel
+    ctx->drop_combined_graphs();
     return SFB_OK;
   });
 }
@@ -1976,10 +1995,8 @@ void refresh_model(sfb_context *ctx) {
     ck(cudaMemcpy(ctx->mat2_all.p, m2.data(), nloc * sizeof(float), cudaMemcpyHostToDevice), "mat2");
     ctx->taps_ready = false;  // pressure taps carry the material
     // captured graphs hold the old tap buffers
-    if (ctx->graph) cudaGraphExecDestroy(ctx->graph);
-    if (ctx->graph_combined) cudaGraphExecDestroy(ctx->graph_combined);
-    ctx->graph = nullptr;
-    ctx->graph_combined = nullptr;
+    ctx->drop_forward_graphs();
+    ctx->drop_combined_graphs();
   }
   ctx->mass_ready = false;
 }

@@ -2,20 +2,25 @@
 //
 // Some callers cannot allocate device memory at the point where they need
 // the inverse mass matrix: a host framework that owns every device
-// allocation through its own pool, code running inside a CUDA stream capture
-// (where cudaMalloc is not allowed), or a real-time loop that must not touch
-// the allocator.  This entry point takes the caller's device inputs and
-// output and keeps its only scratch -- the FP64 accumulation buffer of the
-// assembled mass -- in a fixed, file-scope device array that every GPU
-// loading this library holds until the process exits.
+// allocation through its own pool and forbids plugins from calling
+// cudaMalloc, or a real-time loop that must not touch the allocator (a
+// cudaMalloc can synchronise the device and take milliseconds).  This entry
+// point takes the caller's device inputs and output and keeps its only
+// scratch -- the FP64 accumulation buffer of the assembled mass and one
+// error word -- in fixed, file-scope device arrays that every GPU loading
+// this library holds until the process exits.
 //
 // Set-up: the first call on a device looks up the array's device address
 // with cudaGetSymbolAddress (the array's name is only a host-side stand-in in
 // host code) and caches it for that device; make that first call before any
-// stream capture.  The scratch is shared by every call on a device and keeps
-// the last call's contents: each call clears the part it uses first, and
-// calls that overlap on the GPU (different streams, or threads calling
-// concurrently) race on it.
+// stream capture.  A device reset (cudaDeviceReset) after that first call is
+// not supported: the cached address would belong to the torn-down context.
+// The scratch is shared by every call on a device and keeps the last call's
+// contents: each call clears the part it uses first, and calls that overlap
+// on the GPU (different streams, or threads calling concurrently) race on it.
+// A point index outside [0, npoints) is never written through: the kernel
+// skips it, counts it in the error word, and the call then fills the whole
+// output with NaN so that the bad input cannot pass unnoticed.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -29,6 +34,8 @@
 namespace {
 
 __device__ __align__(256) double g_mass_scratch[SFB_NOALLOC_MAX_DOFS];
+// Out-of-range point indices seen by the current call (cleared by k_clear).
+__device__ unsigned int g_bad_index_count;
 
 constexpr int kMaxDevices = 64;
 double *g_scratch_ptr[kMaxDevices] = {nullptr};
@@ -40,6 +47,7 @@ struct Weights {
 };
 
 __global__ void k_clear(double *scratch, int n) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) g_bad_index_count = 0u;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) scratch[i] = 0.0;
 }
 
@@ -49,7 +57,7 @@ __global__ void k_clear(double *scratch, int n) {
 __global__ void k_mass_noalloc(int medium, int ngll, int nelem, const int *iglob, const float *jac,
                                const float *m0, const float *m1, const float *m2, const uint8_t *bnd,
                                const float *bnx, const float *bnz, const float *bw, float dt, Weights W,
-                               double *scratch) {
+                               int npoints, double *scratch) {
   const int nn = ngll * ngll;
   const int nc = (medium == SFB_MEDIUM_ELASTIC_PSV) ? 2 : 1;
   const size_t total = static_cast<size_t>(nelem) * nn;
@@ -84,13 +92,19 @@ __global__ void k_mass_noalloc(int medium, int ngll, int nelem, const int *iglob
       }
     }
     const int g = iglob[t];
+    if (g < 0 || g >= npoints) {  // never write outside the caller's points
+      atomicAdd(&g_bad_index_count, 1u);
+      continue;
+    }
     for (int c = 0; c < nc; ++c) atomicAdd(scratch + static_cast<size_t>(g) * nc + c, static_cast<double>(mm[c]));
   }
 }
 
+// A call that met an out-of-range index returns NaN everywhere.
 __global__ void k_invert_noalloc(const double *scratch, float *minv, int n) {
+  const bool bad = g_bad_index_count != 0u;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    minv[i] = static_cast<float>(1.0 / scratch[i]);
+    minv[i] = bad ? __int_as_float(0x7fc00000) : static_cast<float>(1.0 / scratch[i]);
 }
 
 int fail(int code, const std::string &msg) {
@@ -146,7 +160,7 @@ SFB_API int sfb_assemble_inverse_mass_noalloc(int medium, int ngll, int nelem, i
   const long long nloc = static_cast<long long>(nelem) * ngll * ngll;
   const int gmass = static_cast<int>(std::max<long long>(1, std::min<long long>((nloc + block - 1) / block, 4096)));
   k_mass_noalloc<<<gmass, block, 0, s>>>(medium, ngll, nelem, iglob, jacobian, mat0, mat1, mat2, bnd, bnd_nx,
-                                         bnd_nz, bnd_w, static_cast<float>(dt), W, scratch);
+                                         bnd_nz, bnd_w, static_cast<float>(dt), W, npoints, scratch);
   k_invert_noalloc<<<gclear, block, 0, s>>>(scratch, minv, static_cast<int>(ndof));
   e = cudaGetLastError();
   if (e != cudaSuccess) return fail(SFB_E_CUDA, std::string("launch: ") + cudaGetErrorString(e));

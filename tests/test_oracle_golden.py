@@ -9,7 +9,9 @@ import pytest
 
 from golden_util import CASES, station_errors
 
-DEFAULT_YAML = "/root/reference/parameter_files/defaults/default.yaml"
+from conftest import REFERENCE
+
+DEFAULT_YAML = os.path.join(REFERENCE, "parameter_files", "defaults", "default.yaml")
 
 
 @pytest.mark.parametrize("case", CASES)

@@ -1,9 +1,10 @@
 """The allocation-free inverse-mass entry point, called through the C ABI.
 
 sfb_assemble_inverse_mass_noalloc serves callers that cannot allocate device
-memory where they need the mass matrix (a host framework owning all device
-buffers, code inside a CUDA stream capture, a real-time loop): it keeps its
-FP64 accumulation scratch in a fixed device array instead of allocating.
+memory where they need the mass matrix (a host framework that hands out all
+device buffers from its own pool, a real-time loop that must not touch the
+allocator): it keeps its FP64 accumulation scratch in a fixed device array
+instead of allocating.
 Here the test itself provides the device inputs and output (through torch)
 and compares the result with the inverse mass the regular path computes, on
 two calls in a row (the second call must clear the scratch the first one
@@ -52,16 +53,31 @@ def _medium_inputs(sim, medium):
     return dev, w, len(sel), info.nglob[medium], info.dt
 
 
-@pytest.mark.parametrize("medium", [0, 3])
+def _problem(medium):
+    from specfempp_b200 import workloads as W
+    if medium == 0:
+        return W.plain_elastic(scale=0.3, nstep=10)
+    if medium == 1:
+        p = W.plain_elastic(scale=0.3, nstep=10)
+        p.elastic_sh = True
+        return p
+    return W.coupled(scale=0.08, nstep=10)
+
+
+def _call(lib, medium, ngll, nelem, npoints, dev, w, dt, out, stream):
+    ptr = lambda t: C.c_void_p(t.data_ptr())
+    return lib.sfb_assemble_inverse_mass_noalloc(
+        medium, ngll, nelem, npoints, ptr(dev["iglob"]), ptr(dev["jac"]), ptr(dev["m0"]),
+        ptr(dev["m1"]), ptr(dev["m2"]), ptr(dev["bnd"]), ptr(dev["bnx"]), ptr(dev["bnz"]),
+        ptr(dev["bw"]), w.ctypes.data_as(C.POINTER(C.c_double)), dt, ptr(out), C.c_void_p(stream))
+
+
+@pytest.mark.parametrize("medium", [0, 1, 3])
 def test_noalloc_inverse_mass_matches_regular_path(medium):
     import torch
     from specfempp_b200 import Simulation, _capi as A
-    from specfempp_b200 import workloads as W
 
-    if medium == 0:
-        p = W.plain_elastic(scale=0.3, nstep=10)
-    else:
-        p = W.coupled(scale=0.08, nstep=10)
+    p = _problem(medium)
     sim = Simulation.structured(p)
     sim.initialize()
     expected = sim.field(medium, 3)  # [ncomp][npoints] from the regular path
@@ -70,19 +86,46 @@ def test_noalloc_inverse_mass_matches_regular_path(medium):
     dev, w, nelem, npoints, dt = _medium_inputs(sim, medium)
     out = torch.empty(npoints * nc, dtype=torch.float32, device="cuda")
     stream = torch.cuda.current_stream().cuda_stream
-    ptr = lambda t: C.c_void_p(t.data_ptr())
     for call in range(2):
         out.fill_(float("nan"))
-        rc = lib.sfb_assemble_inverse_mass_noalloc(
-            medium, p.ngll, nelem, npoints, ptr(dev["iglob"]), ptr(dev["jac"]), ptr(dev["m0"]),
-            ptr(dev["m1"]), ptr(dev["m2"]), ptr(dev["bnd"]), ptr(dev["bnx"]), ptr(dev["bnz"]),
-            ptr(dev["bw"]), w.ctypes.data_as(C.POINTER(C.c_double)), dt, ptr(out), C.c_void_p(stream))
+        rc = _call(lib, medium, p.ngll, nelem, npoints, dev, w, dt, out, stream)
         assert rc == 0, lib.sfb_noalloc_last_error().decode()
         torch.cuda.synchronize()
         got = out.cpu().numpy().reshape(npoints, nc).T
         err = float(np.max(np.abs(got - expected) / np.abs(expected)))
         assert np.isfinite(got).all()
         assert err <= TOL, (call, err)
+
+
+def test_noalloc_out_of_range_index_poisons_output_only():
+    """An index past the caller's points is skipped on the device (nothing is
+    written outside the caller's range) and the call's output becomes NaN;
+    the next call with good indices is correct again."""
+    import torch
+    from specfempp_b200 import Simulation, _capi as A
+
+    p = _problem(0)
+    sim = Simulation.structured(p)
+    sim.initialize()
+    expected = sim.field(0, 3)
+    nc = expected.shape[0]
+    lib = A.load()
+    dev, w, nelem, npoints, dt = _medium_inputs(sim, 0)
+    out = torch.empty(npoints * nc + 64, dtype=torch.float32, device="cuda")
+    out.fill_(7.0)
+    bad = dict(dev)
+    bad["iglob"] = dev["iglob"].clone()
+    bad["iglob"][5] = npoints + 3
+    stream = torch.cuda.current_stream().cuda_stream
+    assert _call(lib, 0, p.ngll, nelem, npoints, bad, w, dt, out, stream) == 0
+    torch.cuda.synchronize()
+    got = out.cpu().numpy()
+    assert np.isnan(got[:npoints * nc]).all()
+    assert (got[npoints * nc:] == 7.0).all()  # the guard words past the output are untouched
+    assert _call(lib, 0, p.ngll, nelem, npoints, dev, w, dt, out, stream) == 0
+    torch.cuda.synchronize()
+    good = out.cpu().numpy()[:npoints * nc].reshape(npoints, nc).T
+    assert float(np.max(np.abs(good - expected) / np.abs(expected))) <= TOL
 
 
 def test_noalloc_rejects_oversized_problem():
