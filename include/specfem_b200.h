@@ -245,6 +245,18 @@ SFB_API int sfb_get_field(const sfb_context *ctx, int wavefield, int medium,
 SFB_API int sfb_set_field(sfb_context *ctx, int wavefield, int medium,
                           int which, int shot, const float *host,
                           size_t count);
+/* The same reads into FP64 host buffers (no reference counterpart): every
+ * bit of the device values in the FP64 verification build
+ * (libspecfem_b200_fp64.so, the same kernels compiled with FP64
+ * arithmetic); widened FP32 values in the product library. */
+SFB_API int sfb_get_seismograms_f64(const sfb_context *ctx, int wavefield,
+                                    int shot, double *host, size_t count);
+SFB_API int sfb_get_field_f64(const sfb_context *ctx, int wavefield,
+                              int medium, int which, int shot, double *host,
+                              size_t count);
+/* Bytes of the library's arithmetic type: 4 for the product library, 8 for
+ * the FP64 verification build. */
+SFB_API int sfb_real_bytes(void);
 /* Replace the adjoint source time functions (combined runs):
  * [nstep][nreceivers][2] for `shot`, receiver r acting at its station. */
 SFB_API int sfb_set_adjoint_sources(sfb_context *ctx, int shot,

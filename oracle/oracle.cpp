@@ -38,6 +38,7 @@
 #include <cstring>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #ifdef _OPENMP
@@ -72,8 +73,12 @@ template <typename T> struct Sim {
   std::vector<std::vector<int>> elems;  // per medium
   bool store_stacey = false;
   int istep_store = 0;
-  std::vector<float> *stacey_store = nullptr;  // [nstep][nloc][2] accelerations
+  // [nstep][nloc][2] accelerations, FP32 as the reference's store, or in the
+  // working precision for the FP64 oracle's exact outputs
+  std::vector<float> *stacey_store = nullptr;
+  std::vector<double> *stacey_store64 = nullptr;
   const std::vector<float> *stacey_replay = nullptr;
+  const std::vector<double> *stacey_replay64 = nullptr;
   bool backward = false;
   int threads = 1;
   // Optional adjoint sources: [nstep][nrec][2] acting through receiver arrays.
@@ -181,7 +186,7 @@ template <typename T> struct Sim {
       const int e = E[ie];
       T u[8 * 8 * 2], Fs[8 * 8 * 2 * 2];
       bool replay = false;
-      if (backward && stacey_replay) {
+      if (backward && (stacey_replay || stacey_replay64)) {
         for (int k = 0; k < nn && !replay; ++k) replay = pv.bnd[static_cast<size_t>(e) * nn + k] & 1;
         // Only elements carrying Stacey points are replayed; the reference
         // keys this on the element boundary tag (stacey or composite).
@@ -189,10 +194,11 @@ template <typename T> struct Sim {
       if (replay) {
         for (int k = 0; k < nn; ++k) {
           const size_t p = static_cast<size_t>(e) * nn + k;
-          const float *src = &(*stacey_replay)[(static_cast<size_t>(istep) * pv.nspec * nn + p) * 2];
+          const size_t at = (static_cast<size_t>(istep) * pv.nspec * nn + p) * 2;
           const int g = pv.iglob[p];
           for (int c = 0; c < nc; ++c) {
-            T val = static_cast<T>(src[c]);
+            T val = stacey_replay64 ? static_cast<T>((*stacey_replay64)[at + c])
+                                    : static_cast<T>((*stacey_replay)[at + c]);
 #pragma omp atomic
             F.a[static_cast<size_t>(c) * F.nglob + g] += val;
           }
@@ -268,14 +274,17 @@ template <typename T> struct Sim {
           }
           if (b & 2)
             for (int c = 0; c < nc; ++c) acc[c] = T(0);
-          if (store_stacey && stacey_store) {
+          if (store_stacey && (stacey_store || stacey_store64)) {
             // Forward runs keep the element-local acceleration of every
             // point of a Stacey element (compute_stiffness_interaction.tpp:251-255).
             bool stacey_elem = false;
             for (int k = 0; k < nn && !stacey_elem; ++k) stacey_elem = pv.bnd[static_cast<size_t>(e) * nn + k] & 1;
             if (stacey_elem) {
-              float *dst = &(*stacey_store)[(static_cast<size_t>(istep) * pv.nspec * nn + p) * 2];
-              for (int c = 0; c < nc; ++c) dst[c] = static_cast<float>(acc[c]);
+              const size_t at = (static_cast<size_t>(istep) * pv.nspec * nn + p) * 2;
+              for (int c = 0; c < nc; ++c) {
+                if (stacey_store64) (*stacey_store64)[at + c] = static_cast<double>(acc[c]);
+                else (*stacey_store)[at + c] = static_cast<float>(acc[c]);
+              }
             }
           }
           for (int c = 0; c < nc; ++c) {
@@ -372,7 +381,7 @@ template <typename T> struct Sim {
   }
 
   // ---- seismograms (compute_seismogram.tpp, wavefield.hpp) ---------------
-  void seismograms(float *out, int isig) {
+  template <typename O> void seismograms(O *out, int isig) {
     const int ntypes = pv.nseismogram_types, nrec = pv.nreceivers;
     for (int r = 0; r < nrec; ++r) {
       const int e = pv.rec_ispec[r];
@@ -437,9 +446,9 @@ template <typename T> struct Sim {
           acc[1] += h * wf[k * 2 + 1];
         }
         const T s = pv.rec_sin[r], c = pv.rec_cos[r];
-        float *o = out + ((static_cast<size_t>(isig) * ntypes + it) * nrec + r) * 2;
-        o[0] = static_cast<float>(c * acc[0] - s * acc[1]);
-        o[1] = static_cast<float>(s * acc[0] + c * acc[1]);
+        O *o = out + ((static_cast<size_t>(isig) * ntypes + it) * nrec + r) * 2;
+        o[0] = static_cast<O>(c * acc[0] - s * acc[1]);
+        o[1] = static_cast<O>(s * acc[0] + c * acc[1]);
       }
     }
   }
@@ -523,16 +532,20 @@ template <typename T> struct Sim {
   }
 };
 
-template <typename T>
+// T: arithmetic; O: type of the outputs (seismograms, fields, Stacey store):
+// FP32 as the reference writes them, or FP64 for the FP64 oracle's exact
+// values.
+template <typename T, typename O = float>
 int run_forward(const sfb_problem_view *pv, int shot, int nstep, int threads,
-                float *seis, float **fields_out, float *stacey_store_out) {
+                O *seis, O **fields_out, O *stacey_store_out) {
   Sim<T> s(*pv, shot);
   s.threads = threads;
-  std::vector<float> store;
+  std::vector<O> store;
   if (stacey_store_out) {
-    store.assign(static_cast<size_t>(nstep) * pv->nspec * pv->ngll * pv->ngll * 2, 0.f);
+    store.assign(static_cast<size_t>(nstep) * pv->nspec * pv->ngll * pv->ngll * 2, O(0));
     s.store_stacey = true;
-    s.stacey_store = &store;
+    if constexpr (std::is_same<O, double>::value) s.stacey_store64 = &store;
+    else s.stacey_store = &store;
   }
   s.init_mass();
   const int nsbs = pv->nstep_between_samples;
@@ -550,12 +563,12 @@ int run_forward(const sfb_problem_view *pv, int shot, int nstep, int threads,
     for (int m : {PSV, SH, ACOUSTIC}) {
       for (auto *vec : {&s.f[m].u, &s.f[m].v, &s.f[m].a, &s.f[m].minv}) {
         if (fields_out[k])
-          for (size_t i = 0; i < vec->size(); ++i) fields_out[k][i] = static_cast<float>((*vec)[i]);
+          for (size_t i = 0; i < vec->size(); ++i) fields_out[k][i] = static_cast<O>((*vec)[i]);
         ++k;
       }
     }
   }
-  if (stacey_store_out) std::memcpy(stacey_store_out, store.data(), store.size() * sizeof(float));
+  if (stacey_store_out) std::memcpy(stacey_store_out, store.data(), store.size() * sizeof(O));
   return 0;
 }
 
@@ -565,15 +578,16 @@ int run_forward(const sfb_problem_view *pv, int shot, int nstep, int threads,
 // reconstructed with -dt from the forward run's last state (`buffer`) with
 // Stacey elements replaying the stored element accelerations, Frechet
 // kernels accumulated every step.
-template <typename T>
+template <typename T, typename O = float>
 int run_combined(const sfb_problem_view *pv, int shot, int nstep, int threads, const float *adjoint_stf,
-                 const float *const *buffer, const std::vector<float> &store, double *kernels,
-                 float *bseis) {
+                 const O *const *buffer, const std::vector<O> &store, double *kernels,
+                 O *bseis) {
   Sim<T> adj(*pv, shot), bwd(*pv, shot);
   adj.threads = bwd.threads = threads;
   adj.adjoint_stf = adjoint_stf;
   bwd.backward = true;
-  bwd.stacey_replay = &store;
+  if constexpr (std::is_same<O, double>::value) bwd.stacey_replay64 = &store;
+  else bwd.stacey_replay = &store;
   adj.init_mass();
   bwd.init_mass();
   for (int e = 0; e < pv->nspec; ++e)
@@ -600,7 +614,7 @@ int run_combined(const sfb_problem_view *pv, int shot, int nstep, int threads, c
       int k = 0;
       for (int m : {PSV, SH, ACOUSTIC}) {
         for (auto *vec : {&bwd.f[m].u, &bwd.f[m].v, &bwd.f[m].a}) {
-          const float *src = buffer[k++];
+          const O *src = buffer[k++];
           if (src)
             for (size_t i = 0; i < vec->size(); ++i) (*vec)[i] = static_cast<T>(src[i]);
         }
@@ -618,6 +632,32 @@ int run_combined(const sfb_problem_view *pv, int shot, int nstep, int threads, c
 thread_local std::string g_err;
 
 }  // namespace
+
+// Seismograms of given fields (see oracle_seismograms).
+template <typename O>
+int seismograms_of_fields(const sfb_problem_view *pv, int precision, const double *const *fields_in, O *seis) {
+  auto run = [&](auto zero) -> int {
+    using T = decltype(zero);
+    Sim<T> s(*pv, 0);
+    int k = 0;
+    for (int m : {PSV, SH, ACOUSTIC}) {
+      for (auto *vec : {&s.f[m].u, &s.f[m].v, &s.f[m].a}) {
+        const double *src = fields_in[k++];
+        if (src)
+          for (size_t i = 0; i < vec->size(); ++i) (*vec)[i] = static_cast<T>(src[i]);
+      }
+    }
+    s.seismograms(seis, 0);
+    return 0;
+  };
+  try {
+    if (pv->ngll > 8) throw std::invalid_argument("ngll > 8");
+    return precision == 64 ? run(0.0) : run(0.0f);
+  } catch (const std::exception &e) {
+    g_err = e.what();
+    return -1;
+  }
+}
 
 extern "C" {
 
@@ -660,33 +700,46 @@ int oracle_combined(const sfb_problem_view *pv, int precision, int shot, int nst
   }
 }
 
+// The FP64 oracle with FP64 outputs: the same runs as oracle_forward /
+// oracle_combined with precision 64, but seismograms, fields, the Stacey
+// store, the backward initial state and the backward seismograms are
+// doubles (not rounded to FP32 on the way out).
+int oracle_forward_f64(const sfb_problem_view *pv, int shot, int nstep, int threads, double *seis,
+                       double **fields_out, double *stacey_store_out) {
+  try {
+    if (pv->ngll > 8) throw std::invalid_argument("ngll > 8");
+    return run_forward<double, double>(pv, shot, nstep, threads, seis, fields_out, stacey_store_out);
+  } catch (const std::exception &e) {
+    g_err = e.what();
+    return -1;
+  }
+}
+
+int oracle_combined_f64(const sfb_problem_view *pv, int shot, int nstep, int threads, const float *adjoint_stf,
+                        const double *const *buffer, const double *stacey_store, double *kernels_out,
+                        double *bseis) {
+  try {
+    const size_t nloc = static_cast<size_t>(pv->nspec) * pv->ngll * pv->ngll;
+    std::vector<double> store(stacey_store, stacey_store + static_cast<size_t>(nstep) * nloc * 2);
+    return run_combined<double, double>(pv, shot, nstep, threads, adjoint_stf, buffer, store, kernels_out, bseis);
+  } catch (const std::exception &e) {
+    g_err = e.what();
+    return -1;
+  }
+}
+
 // Seismograms of given fields, one record: what compute_seismograms(0) gives
 // on a wavefield loaded from files (the reference's seismogram unit tests,
 // tests/unit-tests/seismogram/*/seismogram_tests.cpp).  fields_in: 9
 // pointers (u, v, a for P-SV, SH, acoustic; [ncomp][nglob] doubles, NULL =
 // zero); seis: [ntypes][nrec][2].
 int oracle_seismograms(const sfb_problem_view *pv, int precision, const double *const *fields_in, float *seis) {
-  auto run = [&](auto zero) -> int {
-    using T = decltype(zero);
-    Sim<T> s(*pv, 0);
-    int k = 0;
-    for (int m : {PSV, SH, ACOUSTIC}) {
-      for (auto *vec : {&s.f[m].u, &s.f[m].v, &s.f[m].a}) {
-        const double *src = fields_in[k++];
-        if (src)
-          for (size_t i = 0; i < vec->size(); ++i) (*vec)[i] = static_cast<T>(src[i]);
-      }
-    }
-    s.seismograms(seis, 0);
-    return 0;
-  };
-  try {
-    if (pv->ngll > 8) throw std::invalid_argument("ngll > 8");
-    return precision == 64 ? run(0.0) : run(0.0f);
-  } catch (const std::exception &e) {
-    g_err = e.what();
-    return -1;
-  }
+  return seismograms_of_fields(pv, precision, fields_in, seis);
+}
+
+// The same in FP64 with FP64 outputs.
+int oracle_seismograms_f64(const sfb_problem_view *pv, const double *const *fields_in, double *seis) {
+  return seismograms_of_fields(pv, 64, fields_in, seis);
 }
 
 }  // extern "C"

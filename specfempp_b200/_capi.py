@@ -12,6 +12,9 @@ import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_lib", "libspecfem_b200.so")
+# Verification build: the same driver and generic kernels in FP64 (test
+# infrastructure for parity against the FP64 oracle; not a product path).
+LIB64_PATH = os.path.join(HERE, "_lib", "libspecfem_b200_fp64.so")
 
 SFB_OK = 0
 ERRORS = {
@@ -128,6 +131,9 @@ SIGNATURES = {
     "sfb_run_forward_unfused": (C.c_int, [_ctx, C.c_int]),
     "sfb_run_combined": (C.c_int, [_ctx, C.c_int, C.c_int]),
     "sfb_get_seismograms": (C.c_int, [_ctx, C.c_int, C.c_int, _P(C.c_float), C.c_size_t]),
+    "sfb_get_seismograms_f64": (C.c_int, [_ctx, C.c_int, C.c_int, _P(C.c_double), C.c_size_t]),
+    "sfb_get_field_f64": (C.c_int, [_ctx, C.c_int, C.c_int, C.c_int, C.c_int, _P(C.c_double), C.c_size_t]),
+    "sfb_real_bytes": (C.c_int, []),
     "sfb_get_field": (C.c_int, [_ctx, C.c_int, C.c_int, C.c_int, C.c_int, _P(C.c_float), C.c_size_t]),
     "sfb_set_field": (C.c_int, [_ctx, C.c_int, C.c_int, C.c_int, C.c_int, _P(C.c_float), C.c_size_t]),
     "sfb_set_adjoint_sources": (C.c_int, [_ctx, C.c_int, _P(C.c_float), C.c_size_t]),
@@ -157,24 +163,34 @@ SIGNATURES = {
     "sfb_reset": (C.c_int, [_ctx]),
 }
 
-_lib = None
+# entry points that only the product (FP32) library has
+FP32_ONLY = ("sfb_assemble_inverse_mass_noalloc", "sfb_noalloc_last_error")
+
+_libs = {}
 
 
-def load(path: str = LIB_PATH):
-    """Load the shared library (raises if it has not been built)."""
-    global _lib
-    if _lib is not None:
-        return _lib
+def load(precision: int = 32):
+    """Load the product library (precision 32) or the FP64 verification
+    build (precision 64); raises if it has not been built."""
+    if precision in _libs:
+        return _libs[precision]
+    if precision not in (32, 64):
+        raise ValueError("precision must be 32 or 64")
+    path = LIB_PATH if precision == 32 else LIB64_PATH
     if not os.path.exists(path):
         raise RuntimeError(
             "specfempp_b200 native library not built (%s); run "
             "`python -m specfempp_b200.build` or __graft_entry__.build()" % path)
     lib = C.CDLL(path)
     for name, (res, args) in SIGNATURES.items():
+        if precision == 64 and name in FP32_ONLY:
+            continue
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args
-    _lib = lib
+    if lib.sfb_real_bytes() * 8 != precision:
+        raise RuntimeError("%s computes in %d-bit reals, expected %d" % (path, lib.sfb_real_bytes() * 8, precision))
+    _libs[precision] = lib
     return lib
 
 
@@ -184,9 +200,9 @@ class SfbError(RuntimeError):
         self.code = code
 
 
-def check(code: int, ctx=None):
+def check(code: int, ctx=None, lib=None):
     if code != SFB_OK:
-        lib = load()
+        lib = lib or load()
         msg = lib.sfb_last_error(ctx)
         raise SfbError(code, msg.decode() if msg else "")
     return code

@@ -1,7 +1,16 @@
-"""Build the in-tree shared library ``specfempp_b200/_lib/libspecfem_b200.so``.
+"""Build the in-tree shared libraries under ``specfempp_b200/_lib``.
 
-Host C++ is compiled with g++, CUDA with nvcc for sm_100a; both are linked by
-nvcc into one shared object exporting the C ABI of ``include/specfem_b200.h``.
+``libspecfem_b200.so`` is the product: host C++ compiled with g++, CUDA with
+nvcc for sm_100a, linked by nvcc into one shared object exporting the C ABI
+of ``include/specfem_b200.h`` (FP32, the reference's type_real).
+
+``libspecfem_b200_fp64.so`` is the verification build: the same device
+driver and generic kernels compiled with ``-DSFB_FP64`` (every wavefield,
+geometry and per-step quantity in FP64), for parity tests against the FP64
+oracle at FP64 rounding level.  It is test infrastructure, not a product
+path; the FP32-only kernels and the allocation-free entry point are not in
+it.
+
 Object files are cached under ``specfempp_b200/_build`` keyed on source
 timestamps.
 """
@@ -19,6 +28,9 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIBDIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIBDIR, "libspecfem_b200.so")
+LIB64 = os.path.join(LIBDIR, "libspecfem_b200_fp64.so")
+# CUDA sources of the FP64 verification build (the device driver and kernels)
+FP64_CUDA = ("context.cu", "kernels.cu")
 
 NVCC = os.environ.get("NVCC", shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc")
 CXX = os.environ.get("CXX", "g++")
@@ -62,31 +74,44 @@ def _compile(src, obj, cuda, extra):
     return r.stderr
 
 
+def _link(out, objs):
+    cmd = [NVCC] + ARCH + ["-shared", "-o", out] + objs + ["-lcudart"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("link failed: %s\n%s" % (r.stdout, r.stderr))
+
+
 def build(verbose: bool = False, ptxas_info: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     os.makedirs(LIBDIR, exist_ok=True)
     host, cuda = _sources()
     headers = _headers()
     jobs = []
-    objs = []
+    objs, objs64 = [], []
     extra = ["-Xptxas", "-v"] if ptxas_info else []
     for src in host + cuda:
         is_cuda = src.endswith(".cu")
         obj = os.path.join(BUILD, os.path.basename(src) + ".o")
         objs.append(obj)
         if ptxas_info and is_cuda or _stale(obj, src, headers):
-            jobs.append((src, obj, is_cuda))
+            jobs.append((src, obj, is_cuda, extra))
+        if not is_cuda:
+            objs64.append(obj)
+        elif os.path.basename(src) in FP64_CUDA:
+            obj64 = os.path.join(BUILD, os.path.basename(src) + ".fp64.o")
+            objs64.append(obj64)
+            if _stale(obj64, src, headers):
+                jobs.append((src, obj64, True, ["-DSFB_FP64"]))
     logs = []
     if jobs:
         with cf.ThreadPoolExecutor(max_workers=min(8, len(jobs))) as ex:
-            futs = [ex.submit(_compile, s, o, c, extra) for s, o, c in jobs]
+            futs = [ex.submit(_compile, s, o, c, e) for s, o, c, e in jobs]
             for f in futs:
                 logs.append(f.result())
     if jobs or not os.path.exists(LIB):
-        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
-        r = subprocess.run(cmd, capture_output=True, text=True)
-        if r.returncode != 0:
-            raise RuntimeError("link failed: %s\n%s" % (r.stdout, r.stderr))
+        _link(LIB, objs)
+    if jobs or not os.path.exists(LIB64):
+        _link(LIB64, objs64)
     if verbose:
         for l in logs:
             if l:

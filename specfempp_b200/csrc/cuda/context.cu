@@ -11,6 +11,7 @@
 #include <memory>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../../include/specfem_b200.h"
@@ -24,6 +25,7 @@ void write_seismograms_ascii(const Problem &P, const float *seis, int ntypes, in
 }
 
 using namespace sfb;
+using dev::real;
 
 namespace {
 
@@ -40,6 +42,29 @@ void ck(cudaError_t e, const char *what) {
   if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
 }
 
+// Copies between host buffers of type H and device values of type `real`
+// (FP32 in the product library, FP64 in the verification library): a plain
+// copy when the types agree, through a converted host copy otherwise.
+template <typename H> void copy_d2h(H *host, const real *dev, size_t n, const char *what) {
+  if (!n) return;
+  if constexpr (std::is_same<H, real>::value) {
+    ck(cudaMemcpy(host, dev, n * sizeof(real), cudaMemcpyDeviceToHost), what);
+  } else {
+    std::vector<real> tmp(n);
+    ck(cudaMemcpy(tmp.data(), dev, n * sizeof(real), cudaMemcpyDeviceToHost), what);
+    for (size_t i = 0; i < n; ++i) host[i] = static_cast<H>(tmp[i]);
+  }
+}
+template <typename H> void copy_h2d(real *dev, const H *host, size_t n, const char *what) {
+  if (!n) return;
+  if constexpr (std::is_same<H, real>::value) {
+    ck(cudaMemcpy(dev, host, n * sizeof(real), cudaMemcpyHostToDevice), what);
+  } else {
+    std::vector<real> tmp(host, host + n);
+    ck(cudaMemcpy(dev, tmp.data(), n * sizeof(real), cudaMemcpyHostToDevice), what);
+  }
+}
+
 template <typename T> struct DBuf {
   T *p = nullptr;
   size_t n = 0;
@@ -51,9 +76,13 @@ template <typename T> struct DBuf {
     ck(cudaMemset(p, 0, count * sizeof(T)), "cudaMemset");
     if (total) *total += count * sizeof(T);
   }
-  void upload(const std::vector<T> &h, size_t *total) {
-    alloc(h.size(), total);
-    if (!h.empty()) ck(cudaMemcpy(p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice), "upload");
+  template <typename U> void upload(const std::vector<U> &h, size_t *total) {
+    if constexpr (std::is_same<U, T>::value) {
+      alloc(h.size(), total);
+      if (!h.empty()) ck(cudaMemcpy(p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice), "upload");
+    } else {
+      upload(std::vector<T>(h.begin(), h.end()), total);
+    }
   }
   void free() {
     if (p) cudaFree(p);
@@ -68,9 +97,9 @@ constexpr int kMedia[3] = {dev::MED_PSV, dev::MED_SH, dev::MED_AC};
 struct WavefieldSet {
   bool allocated = false;
   dev::MediumFields f[4];
-  DBuf<float> u[4], v[4], a[4];
-  DBuf<float> cu[4], cv[4];  // Kahan compensation of u and v (forward, when enabled)
-  DBuf<float> seis;
+  DBuf<real> u[4], v[4], a[4];
+  DBuf<real> cu[4], cv[4];  // Kahan compensation of u and v (forward, when enabled)
+  DBuf<real> seis;
   DBuf<dev::Control> ctrl;
   bool initialized = false;
   int step = 0;  // host copy of the next step index
@@ -89,35 +118,35 @@ struct sfb_context {
   std::vector<int> perm, inv;
   int med_begin[4] = {0, 0, 0, 0}, med_count[4] = {0, 0, 0, 0}, med_interior[4] = {0, 0, 0, 0};
   DBuf<int> iglob;
-  DBuf<float> xix, xiz, gax, gaz, jac, mat0[4], mat1[4], mat2[4];
-  DBuf<float> mat0_all, mat1_all, mat2_all;
+  DBuf<real> xix, xiz, gax, gaz, jac, mat0[4], mat1[4], mat2[4];
+  DBuf<real> mat0_all, mat1_all, mat2_all;
   DBuf<uint8_t> eflag, bnd;
-  DBuf<float> bnd_nx, bnd_nz, bnd_w;
-  DBuf<float> pack;  // [nspec][8][N*N] static block for the TMA-fed stiffness kernel
-  DBuf<float> pack_aff;  // compact block of affine elements (single-shot contexts)
+  DBuf<real> bnd_nx, bnd_nz, bnd_w;
+  DBuf<real> pack;  // [nspec][8][N*N] static block of the stiffness kernels
+  DBuf<float> pack_aff;  // compact block of affine elements (single-shot FP32 contexts)
   DBuf<int> dflag;   // device error flag
-  DBuf<float> minv[4];
+  DBuf<real> minv[4];
   DBuf<double> mass[4];
   // sources (forward / backward wavefield) and receivers
   DBuf<int> src_elem, src_shot, src_medium;
-  DBuf<float> src_array, src_stf;
+  DBuf<real> src_array, src_stf;
   int nsrc = 0;
   DBuf<int> rec_elem;
-  DBuf<float> rec_lag, rec_sin, rec_cos;
+  DBuf<real> rec_lag, rec_sin, rec_cos;
   DBuf<int> cp_ac_self, cp_ac_other, cp_el_self, cp_el_other;
-  DBuf<float> cp_ac_f, cp_ac_nx, cp_ac_nz, cp_el_f, cp_el_nx, cp_el_nz;
+  DBuf<real> cp_ac_f, cp_ac_nx, cp_ac_nz, cp_el_f, cp_el_nx, cp_el_nz;
   DBuf<int> step_scratch;  // host-driven step index for the unfused path
   WavefieldSet wf[3];
   dev::Static st{};
   bool mass_ready = false;
   // Stacey replay store
-  DBuf<float> stacey_data;  // [S][nstep][nstacey][N*N][2]
+  DBuf<real> stacey_data;  // [S][nstep][nstacey][N*N][2]
   DBuf<int> stacey_slot;
   std::vector<int> h_stacey_slot;  // host copy, per device element
   int nstacey = 0;
   // adjoint sources: one per (shot, receiver), receiver Lagrange arrays
   DBuf<int> adj_elem, adj_shot, adj_medium;
-  DBuf<float> adj_array, adj_stf;
+  DBuf<real> adj_array, adj_stf;
   int nadj = 0;
   DBuf<double> kern;        // Frechet accumulators [nspec][N*N][3], device element order
   std::map<int, cudaGraphExec_t> graphs_combined;  // combined-run graphs by step count
@@ -126,7 +155,7 @@ struct sfb_context {
   struct Taps {
     DBuf<uint32_t> mask;
     DBuf<int> sup_g, sup_begin, slot, which;
-    DBuf<float> w;
+    DBuf<real> w;
     int nsup = 0;
   } taps[4];
   bool taps_ready = false;
@@ -142,7 +171,7 @@ struct sfb_context {
   // forward snapshots restored into the backward wavefield of the combined
   // run every ck_interval steps (0: pure reconstruction)
   int ck_interval = 0, ck_count = 0;
-  DBuf<float> ck_u[4], ck_v[4];
+  DBuf<real> ck_u[4], ck_v[4];
   size_t ck_stride[4] = {0, 0, 0, 0};
   // forward CUDA graphs by the number of fused steps they hold (the full
   // chunk and the remainders met so far)
@@ -282,13 +311,17 @@ void ensure_device(sfb_context *c) {
     c->nprivate_points = a.nglob[m] - P0.nshared_psv;
   }
   // packed per-element static block: iglob, xix, xiz, gammax, gammaz, jac, mat0, mat1
-  std::vector<float> pack(nloc * dev::kPackFields);
+  std::vector<real> pack(nloc * dev::kPackFields);
   for (int d = 0; d < a.nspec; ++d)
     for (int k = 0; k < nn; ++k) {
       const size_t q = static_cast<size_t>(d) * nn + k;
-      float *blk = &pack[static_cast<size_t>(d) * dev::kPackFields * nn];
-      int gi = iglob[q];
-      std::memcpy(&blk[0 * nn + k], &gi, 4);
+      real *blk = &pack[static_cast<size_t>(d) * dev::kPackFields * nn];
+      const int gi = iglob[q];
+#ifdef SFB_FP64
+      blk[0 * nn + k] = static_cast<real>(gi);  // the index as a value (exact below 2^53)
+#else
+      std::memcpy(&blk[0 * nn + k], &gi, 4);  // the index's bits
+#endif
       blk[1 * nn + k] = xix[q];
       blk[2 * nn + k] = xiz[q];
       blk[3 * nn + k] = gax[q];
@@ -306,7 +339,9 @@ void ensure_device(sfb_context *c) {
   // of five geometry words per point; the batched kernels keep the five
   // constants in registers instead of staging geometry per point.  Chunks of
   // dev::kAffineChunk elements per medium, chunk-major (see
-  // dev::Static::pack_aff).
+  // dev::Static::pack_aff).  FP32 contexts only: the compact-block kernels
+  // are FP32 kernels.
+#ifndef SFB_FP64
   {
     const int words = dev::affine_chunk_words(n);
     const int E = dev::kAffineChunk;
@@ -355,6 +390,7 @@ void ensure_device(sfb_context *c) {
     }
     if (!aff.empty()) c->pack_aff.upload(aff, tot);
   }
+#endif
   c->dflag.alloc(1, tot);
   c->iglob.upload(iglob, tot);
   c->xix.upload(xix, tot);
@@ -395,9 +431,9 @@ void ensure_device(sfb_context *c) {
     c->mass[m].alloc(ld, tot);
   }
   // quadrature tables
-  std::vector<float> hp(nn), w(n);
-  for (int i = 0; i < nn; ++i) hp[i] = static_cast<float>(a.quad.hprime[i]);
-  for (int i = 0; i < n; ++i) w[i] = static_cast<float>(a.quad.w[i]);
+  std::vector<real> hp(nn), w(n);
+  for (int i = 0; i < nn; ++i) hp[i] = static_cast<real>(static_cast<float>(a.quad.hprime[i]));
+  for (int i = 0; i < n; ++i) w[i] = static_cast<real>(static_cast<float>(a.quad.w[i]));
   dev::set_quadrature(n, hp.data(), w.data());
   ck(cudaGetLastError(), "set_quadrature");
   dev::init_kernel_attributes();
@@ -501,7 +537,7 @@ void autotune_stiffness(sfb_context *c, WavefieldSet &W) {
     c->shots_variant[m] = choice;
     const dev::MediumFields &f = W.f[m];
     const size_t ld = static_cast<size_t>(f.nglob + (f.nglob & 1)) * f.nc * S;
-    ck(cudaMemsetAsync(f.a, 0, ld * sizeof(float), c->stream), "clear force");
+    ck(cudaMemsetAsync(f.a, 0, ld * sizeof(real), c->stream), "clear force");
   }
   ck(cudaGetLastError(), "autotune");
   ck(cudaStreamSynchronize(c->stream), "autotune");
@@ -592,7 +628,7 @@ void initialize_mass(sfb_context *c, double dt) {
     f.minv = c->minv[m].p;
     f.mass = c->mass[m].p;
     if (c->mass[m].n) ck(cudaMemsetAsync(c->mass[m].p, 0, c->mass[m].n * sizeof(double), c->stream), "memset mass");
-    dev::launch_mass(m, a.ngll, c->st, f, static_cast<float>(dt), c->stream);
+    dev::launch_mass(m, a.ngll, c->st, f, static_cast<real>(dt), c->stream);
     dev::launch_invert_mass(f, c->stream);
   }
   ck(cudaGetLastError(), "mass kernels");
@@ -642,7 +678,8 @@ void build_taps(sfb_context *c) {
           if (m == MEDIUM_ELASTIC_PSV) add(k, 1, 0.0, h);
         } else if (m == MEDIUM_ELASTIC_PSV && type == 3) {
           which = 0;
-          const double l2m = a.kappa[p] + (4.0 / 3.0) * a.mu[p];
+          // 4/3 as the reference's FP32 constant
+          const double l2m = a.kappa[p] + static_cast<double>(static_cast<float>(4.0 / 3.0)) * a.mu[p];
           const double cf = -((l2m - 2.0 * a.mu[p]) + (2.0 / 3.0) * a.mu[p]) * h;
           for (int l = 0; l < n; ++l) {
             const double hx = a.quad.hprime[kx * n + l], hz = a.quad.hprime[kz * n + l];
@@ -679,7 +716,7 @@ void build_taps(sfb_context *c) {
     auto &v = ent[m];
     std::sort(v.begin(), v.end(), [](const E &x, const E &y) { return x.g < y.g; });
     std::vector<int> sup_g, sup_begin, slot, which;
-    std::vector<float> w;
+    std::vector<real> w;
     for (size_t i = 0; i < v.size(); ++i) {
       if (sup_g.empty() || sup_g.back() != v[i].g) {
         sup_g.push_back(v[i].g);
@@ -687,7 +724,7 @@ void build_taps(sfb_context *c) {
       }
       slot.push_back(v[i].slot);
       which.push_back(v[i].which);
-      w.push_back(static_cast<float>(v[i].w));
+      w.push_back(static_cast<real>(v[i].w));
     }
     sup_begin.push_back(static_cast<int>(slot.size()));
     const int nglob = a.nglob[m];
@@ -740,9 +777,9 @@ dev::UpdateParams update_params(sfb_context *c, WavefieldSet &W, int last, bool 
   u.nshots = P.nshots;
   u.sdiv = dev::FastDiv::make(static_cast<uint32_t>(P.nshots));
   if (u.begin[u.nm] * 2 >= (1ull << 32)) throw std::invalid_argument("field too large for 32-bit update indexing");
-  u.dt = static_cast<float>(P.dt);
-  u.dt2 = static_cast<float>(P.dt / 2.0);
-  u.dtsq2 = static_cast<float>(P.dt * P.dt / 2.0);
+  u.dt = static_cast<real>(P.dt);
+  u.dt2 = static_cast<real>(P.dt / 2.0);
+  u.dtsq2 = static_cast<real>(P.dt * P.dt / 2.0);
   u.last = last;
   u.ctrl = advance ? W.ctrl.p : nullptr;
   u.dir = 1;
@@ -769,8 +806,8 @@ bool private_update_on(sfb_context *c) {
 void enqueue_fused_step(sfb_context *c, WavefieldSet &W, int last) {
   const Problem &P = c->P;
   const int S = P.nshots, n = P.asmb.ngll;
-  const float dt = static_cast<float>(P.dt);
-  const float dt2 = static_cast<float>(P.dt / 2.0), dtsq2 = static_cast<float>(P.dt * P.dt / 2.0);
+  const real dt = static_cast<real>(P.dt);
+  const real dt2 = static_cast<real>(P.dt / 2.0), dtsq2 = static_cast<real>(P.dt * P.dt / 2.0);
   const int *istep = &W.ctrl.p->istep;
   dev::StaceyStore ss{};
   if (P.save_boundary_values && c->stacey_data.p) {
@@ -836,8 +873,8 @@ int fused_step_launches(sfb_context *c, WavefieldSet &W) {
 void predictor_all(sfb_context *c, WavefieldSet &W, double sgn) {
   const Problem &P = c->P;
   for (int m : kMedia)
-    dev::launch_predictor(W.f[m], P.nshots, static_cast<float>(sgn * P.dt), static_cast<float>(sgn * P.dt / 2.0),
-                          static_cast<float>(P.dt * P.dt / 2.0), c->stream, W.cu[m].p, W.cv[m].p);
+    dev::launch_predictor(W.f[m], P.nshots, static_cast<real>(sgn * P.dt), static_cast<real>(sgn * P.dt / 2.0),
+                          static_cast<real>(P.dt * P.dt / 2.0), c->stream, W.cu[m].p, W.cv[m].p);
 }
 
 void ensure_store(sfb_context *c) {
@@ -968,7 +1005,7 @@ void ensure_adjoint_sources(sfb_context *c) {
     const int nn = P.asmb.ngll * P.asmb.ngll;
     c->nadj = static_cast<int>(P.located_adjoint.size());
     std::vector<int> el(c->nadj), sh(c->nadj, 0), md(c->nadj);
-    std::vector<float> arr(static_cast<size_t>(c->nadj) * 2 * nn, 0.f), stf(static_cast<size_t>(c->nadj) * P.nstep * 2);
+    std::vector<real> arr(static_cast<size_t>(c->nadj) * 2 * nn, 0), stf(static_cast<size_t>(c->nadj) * P.nstep * 2);
     for (int i = 0; i < c->nadj; ++i) {
       const LocatedSource &L = P.located_adjoint[i];
       el[i] = c->inv[L.ispec];
@@ -994,7 +1031,7 @@ void ensure_adjoint_sources(sfb_context *c) {
   const int nn = a.ngll * a.ngll, nrec = static_cast<int>(P.receivers.size()), S = P.nshots;
   c->nadj = S * nrec;
   std::vector<int> el(c->nadj), sh(c->nadj), md(c->nadj);
-  std::vector<float> arr(static_cast<size_t>(c->nadj) * 2 * nn, 0.f);
+  std::vector<real> arr(static_cast<size_t>(c->nadj) * 2 * nn, 0);
   for (int s = 0; s < S; ++s)
     for (int r = 0; r < nrec; ++r) {
       const int i = s * nrec + r;
@@ -1073,13 +1110,13 @@ void enqueue_backward_stiffness(sfb_context *c, WavefieldSet &A, WavefieldSet &B
     fr.aa = A.f[dev::MED_PSV].a;
     fr.minv = c->minv[dev::MED_PSV].p;
     fr.kern = c->kern.p;
-    fr.dt = static_cast<float>(c->P.dt);
+    fr.dt = static_cast<real>(c->P.dt);
     if (backward_private_on(c)) {
       fr.adjoint_update = 1;
       fr.av = A.f[dev::MED_PSV].v;
-      fr.adt = static_cast<float>(c->P.dt);
-      fr.adt2 = static_cast<float>(c->P.dt / 2.0);
-      fr.adtsq2 = static_cast<float>(c->P.dt * c->P.dt / 2.0);
+      fr.adt = static_cast<real>(c->P.dt);
+      fr.adt2 = static_cast<real>(c->P.dt / 2.0);
+      fr.adtsq2 = static_cast<real>(c->P.dt * c->P.dt / 2.0);
       fr.last = last;
     }
     dev::FusedUpdate fu{};
@@ -1087,9 +1124,9 @@ void enqueue_backward_stiffness(sfb_context *c, WavefieldSet &A, WavefieldSet &B
       fu.enabled = 1;
       fu.minv = c->minv[dev::MED_PSV].p;
       fu.v = B.f[dev::MED_PSV].v;
-      fu.dt = static_cast<float>(-c->P.dt);
-      fu.dt2 = static_cast<float>(-c->P.dt / 2.0);
-      fu.dtsq2 = static_cast<float>(c->P.dt * c->P.dt / 2.0);
+      fu.dt = static_cast<real>(-c->P.dt);
+      fu.dt2 = static_cast<real>(-c->P.dt / 2.0);
+      fu.dtsq2 = static_cast<real>(c->P.dt * c->P.dt / 2.0);
       fu.last = last;
     }
     dev::launch_stiffness_frechet(n, c->st, B.f[dev::MED_PSV], S, ss, istep, te, fr, fu, c->stream);
@@ -1108,7 +1145,7 @@ void enqueue_backward_stiffness(sfb_context *c, WavefieldSet &A, WavefieldSet &B
 
 void enqueue_frechet(sfb_context *c, WavefieldSet &A, const dev::MediumFields *bwd_fields, int a_is_force,
                      bool psv_done = false) {
-  const float dt = static_cast<float>(c->P.dt);
+  const real dt = static_cast<real>(c->P.dt);
   for (int m : {dev::MED_PSV, dev::MED_AC}) {
     if (m == dev::MED_PSV && psv_done) continue;
     dev::launch_frechet(m, c->P.asmb.ngll, c->st, A.f[m], bwd_fields[m], c->P.nshots, dt, c->kern.p, a_is_force,
@@ -1119,8 +1156,8 @@ void enqueue_frechet(sfb_context *c, WavefieldSet &A, const dev::MediumFields *b
 dev::UpdateParams update_params_signed(sfb_context *c, WavefieldSet &W, int last, bool advance, bool taps,
                                        double sgn, bool private_done = false) {
   dev::UpdateParams u = update_params(c, W, last, advance, taps, private_done);
-  u.dt = static_cast<float>(sgn * c->P.dt);
-  u.dt2 = static_cast<float>(sgn * c->P.dt / 2.0);
+  u.dt = static_cast<real>(sgn * c->P.dt);
+  u.dt2 = static_cast<real>(sgn * c->P.dt / 2.0);
   u.dir = -1;
   return u;
 }
@@ -1163,9 +1200,9 @@ void copy_fields(sfb_context *c, WavefieldSet &dst, const WavefieldSet &src) {
   for (int m : kMedia) {
     const size_t n = dst.u[m].n;
     if (!n) continue;
-    ck(cudaMemcpyAsync(dst.u[m].p, src.u[m].p, n * sizeof(float), cudaMemcpyDeviceToDevice, c->stream), "copy u");
-    ck(cudaMemcpyAsync(dst.v[m].p, src.v[m].p, n * sizeof(float), cudaMemcpyDeviceToDevice, c->stream), "copy v");
-    ck(cudaMemcpyAsync(dst.a[m].p, src.a[m].p, n * sizeof(float), cudaMemcpyDeviceToDevice, c->stream), "copy a");
+    ck(cudaMemcpyAsync(dst.u[m].p, src.u[m].p, n * sizeof(real), cudaMemcpyDeviceToDevice, c->stream), "copy u");
+    ck(cudaMemcpyAsync(dst.v[m].p, src.v[m].p, n * sizeof(real), cudaMemcpyDeviceToDevice, c->stream), "copy v");
+    ck(cudaMemcpyAsync(dst.a[m].p, src.a[m].p, n * sizeof(real), cudaMemcpyDeviceToDevice, c->stream), "copy a");
   }
 }
 
@@ -1173,11 +1210,11 @@ void zero_fields(sfb_context *c, WavefieldSet &W) {
   for (int m : kMedia) {
     const size_t n = W.u[m].n;
     if (!n) continue;
-    ck(cudaMemsetAsync(W.u[m].p, 0, n * sizeof(float), c->stream), "zero u");
-    ck(cudaMemsetAsync(W.v[m].p, 0, n * sizeof(float), c->stream), "zero v");
-    ck(cudaMemsetAsync(W.a[m].p, 0, n * sizeof(float), c->stream), "zero a");
+    ck(cudaMemsetAsync(W.u[m].p, 0, n * sizeof(real), c->stream), "zero u");
+    ck(cudaMemsetAsync(W.v[m].p, 0, n * sizeof(real), c->stream), "zero v");
+    ck(cudaMemsetAsync(W.a[m].p, 0, n * sizeof(real), c->stream), "zero a");
   }
-  if (W.seis.n) ck(cudaMemsetAsync(W.seis.p, 0, W.seis.n * sizeof(float), c->stream), "zero seis");
+  if (W.seis.n) ck(cudaMemsetAsync(W.seis.p, 0, W.seis.n * sizeof(real), c->stream), "zero seis");
 }
 
 void run_combined_fused(sfb_context *c, int use_graph) {
@@ -1215,8 +1252,8 @@ void run_combined_fused(sfb_context *c, int use_graph) {
   if (N > 1) {
     copy_fields(c, B, F);
     for (int m : kMedia)
-      dev::launch_predictor(B.f[m], P.nshots, static_cast<float>(-P.dt), static_cast<float>(-P.dt / 2.0),
-                            static_cast<float>(P.dt * P.dt / 2.0), c->stream);
+      dev::launch_predictor(B.f[m], P.nshots, static_cast<real>(-P.dt), static_cast<real>(-P.dt / 2.0),
+                            static_cast<real>(P.dt * P.dt / 2.0), c->stream);
     // backward seismogram of step N-1 is the forward run's last sample
     const int nsbs = P.nstep_between_samples;
     if ((N - 1) % nsbs == 0 && (N - 1) / nsbs < P.max_sig_step()) {
@@ -1225,7 +1262,7 @@ void run_combined_fused(sfb_context *c, int use_graph) {
       for (int s = 0; s < P.nshots; ++s) {
         const size_t off = (static_cast<size_t>(s) * P.max_sig_step() + isig) * slots;
         if (slots)
-          ck(cudaMemcpyAsync(B.seis.p + off, F.seis.p + off, slots * sizeof(float), cudaMemcpyDeviceToDevice,
+          ck(cudaMemcpyAsync(B.seis.p + off, F.seis.p + off, slots * sizeof(real), cudaMemcpyDeviceToDevice,
                              c->stream),
              "seismograms");
       }
@@ -1338,7 +1375,7 @@ SFB_API int sfb_set_newmark_compensation(sfb_context *ctx, int enable) {
           W.cv[m].alloc(W.v[m].n, &ctx->device_bytes);
         }
       } else {
-        if (W.cu[m].p) ctx->device_bytes -= 2 * W.cu[m].n * sizeof(float);
+        if (W.cu[m].p) ctx->device_bytes -= 2 * W.cu[m].n * sizeof(real);
         W.cu[m].free();
         W.cv[m].free();
       }
@@ -1358,7 +1395,7 @@ SFB_API int sfb_set_checkpoint_interval(sfb_context *ctx, int interval) {
     const int N = ctx->P.nstep;
     const int count = (interval > 0 && N >= 2) ? (N - 2) / interval : 0;
     for (int m : kMedia) {
-      if (ctx->ck_u[m].p) ctx->device_bytes -= 2 * ctx->ck_u[m].n * sizeof(float);
+      if (ctx->ck_u[m].p) ctx->device_bytes -= 2 * ctx->ck_u[m].n * sizeof(real);
       ctx->ck_u[m].free();
       ctx->ck_v[m].free();
       ctx->ck_stride[m] = 0;
@@ -1425,7 +1462,7 @@ SFB_API int sfb_domain_compute_seismograms(sfb_context *ctx, int wavefield, int 
     WavefieldSet &W = ensure_wavefield(ctx, wavefield);
     // the kernel derives isig from the step counter: isig * nsbs
     set_step(ctx, W, isig_step * ctx->P.nstep_between_samples);
-    dev::launch_receivers(ctx->P.asmb.ngll, ctx->st, receiver_set(ctx, W), W.f, ctx->P.nshots, 0.f, 0,
+    dev::launch_receivers(ctx->P.asmb.ngll, ctx->st, receiver_set(ctx, W), W.f, ctx->P.nshots, real(0), 0,
                           &W.ctrl.p->istep, ctx->stream);
     ck(cudaGetLastError(), "compute_seismograms");
     return SFB_OK;
@@ -1439,8 +1476,8 @@ SFB_API int sfb_newmark_predictor(sfb_context *ctx, int wavefield, int medium, i
     WavefieldSet &W = ensure_wavefield(ctx, wavefield);
     const double sgn = wavefield == SFB_WAVEFIELD_BACKWARD ? -1.0 : 1.0;
     const Problem &P = ctx->P;
-    dev::launch_predictor(W.f[medium], P.nshots, static_cast<float>(sgn * P.dt),
-                          static_cast<float>(sgn * P.dt / 2.0), static_cast<float>(P.dt * P.dt / 2.0),
+    dev::launch_predictor(W.f[medium], P.nshots, static_cast<real>(sgn * P.dt),
+                          static_cast<real>(sgn * P.dt / 2.0), static_cast<real>(P.dt * P.dt / 2.0),
                           ctx->stream);
     ck(cudaGetLastError(), "predictor");
     if (dofs) *dofs = W.f[medium].nglob * W.f[medium].nc;
@@ -1454,7 +1491,7 @@ SFB_API int sfb_newmark_corrector(sfb_context *ctx, int wavefield, int medium, i
     if (!medium_index_ok(medium)) throw std::invalid_argument("unsupported medium tag");
     WavefieldSet &W = ensure_wavefield(ctx, wavefield);
     const double sgn = wavefield == SFB_WAVEFIELD_BACKWARD ? -1.0 : 1.0;
-    dev::launch_corrector(W.f[medium], ctx->P.nshots, static_cast<float>(sgn * ctx->P.dt / 2.0), ctx->stream);
+    dev::launch_corrector(W.f[medium], ctx->P.nshots, static_cast<real>(sgn * ctx->P.dt / 2.0), ctx->stream);
     ck(cudaGetLastError(), "corrector");
     if (dofs) *dofs = W.f[medium].nglob * W.f[medium].nc;
     return SFB_OK;
@@ -1511,7 +1548,7 @@ SFB_API int sfb_run_forward_unfused(sfb_context *ctx, int nstep) {
       dofs += k;
       if (istep % P.nstep_between_samples == 0 && isig < P.max_sig_step()) {
         set_step(ctx, W, istep);
-        dev::launch_receivers(P.asmb.ngll, ctx->st, receiver_set(ctx, W), W.f, P.nshots, 0.f, 0,
+        dev::launch_receivers(P.asmb.ngll, ctx->st, receiver_set(ctx, W), W.f, P.nshots, real(0), 0,
                               &W.ctrl.p->istep, ctx->stream);
         ++isig;
       }
@@ -1538,14 +1575,31 @@ SFB_API int sfb_get_seismograms(const sfb_context *cctx, int wavefield, int shot
     if (shot < 0 || shot >= P.nshots) throw std::invalid_argument("shot out of range");
     if (count < per) throw std::invalid_argument("seismogram buffer too small");
     ck(cudaStreamSynchronize(ctx->stream), "sync");
-    if (per) ck(cudaMemcpy(host, W.seis.p + shot * per, per * sizeof(float), cudaMemcpyDeviceToHost), "seis d2h");
+    copy_d2h(host, W.seis.p + shot * per, per, "seis d2h");
     return SFB_OK;
   });
 }
 
-SFB_API int sfb_get_field(const sfb_context *cctx, int wavefield, int medium, int which, int shot, float *host,
-                          size_t count) {
+SFB_API int sfb_get_seismograms_f64(const sfb_context *cctx, int wavefield, int shot, double *host, size_t count) {
   sfb_context *ctx = const_cast<sfb_context *>(cctx);
+  if (!ctx || !host) return SFB_E_INVALID;
+  return guarded(ctx, [&]() {
+    WavefieldSet &W = ensure_wavefield(ctx, wavefield);
+    const Problem &P = ctx->P;
+    const size_t per = static_cast<size_t>(P.max_sig_step()) * P.seismogram_types.size() * P.receivers.size() * 2;
+    if (shot < 0 || shot >= P.nshots) throw std::invalid_argument("shot out of range");
+    if (count < per) throw std::invalid_argument("seismogram buffer too small");
+    ck(cudaStreamSynchronize(ctx->stream), "sync");
+    copy_d2h(host, W.seis.p + shot * per, per, "seis d2h");
+    return SFB_OK;
+  });
+}
+
+SFB_API int sfb_real_bytes(void) { return static_cast<int>(sizeof(real)); }
+
+namespace {
+template <typename H>
+int get_field_impl(sfb_context *ctx, int wavefield, int medium, int which, int shot, H *host, size_t count) {
   if (!ctx || !host) return SFB_E_INVALID;
   return guarded(ctx, [&]() {
     if (!medium_index_ok(medium)) throw std::invalid_argument("unsupported medium tag");
@@ -1554,21 +1608,33 @@ SFB_API int sfb_get_field(const sfb_context *cctx, int wavefield, int medium, in
     const size_t n = static_cast<size_t>(f.nglob) * f.nc;
     if (count < n) throw std::invalid_argument("field buffer too small");
     if (shot < 0 || shot >= ctx->P.nshots) throw std::invalid_argument("shot out of range");
-    const float *src = which == 0 ? f.u : which == 1 ? f.v : which == 2 ? f.a : f.minv;
+    const real *src = which == 0 ? f.u : which == 1 ? f.v : which == 2 ? f.a : f.minv;
     const int S = (which == 3) ? 1 : ctx->P.nshots;
     if (which == 3) shot = 0;
-    std::vector<float> tmp(n);
+    std::vector<real> tmp(n);
     ck(cudaStreamSynchronize(ctx->stream), "sync");
     // device layout [g][s][c]: gather shot `shot`, then transpose to [c][g]
     if (n)
-      ck(cudaMemcpy2D(tmp.data(), f.nc * sizeof(float), src + static_cast<size_t>(shot) * f.nc,
-                      static_cast<size_t>(S) * f.nc * sizeof(float), f.nc * sizeof(float), f.nglob,
+      ck(cudaMemcpy2D(tmp.data(), f.nc * sizeof(real), src + static_cast<size_t>(shot) * f.nc,
+                      static_cast<size_t>(S) * f.nc * sizeof(real), f.nc * sizeof(real), f.nglob,
                       cudaMemcpyDeviceToHost),
          "field d2h");
     for (int c = 0; c < f.nc; ++c)
-      for (int g = 0; g < f.nglob; ++g) host[static_cast<size_t>(c) * f.nglob + g] = tmp[static_cast<size_t>(g) * f.nc + c];
+      for (int g = 0; g < f.nglob; ++g)
+        host[static_cast<size_t>(c) * f.nglob + g] = static_cast<H>(tmp[static_cast<size_t>(g) * f.nc + c]);
     return SFB_OK;
   });
+}
+}  // namespace
+
+SFB_API int sfb_get_field(const sfb_context *cctx, int wavefield, int medium, int which, int shot, float *host,
+                          size_t count) {
+  return get_field_impl(const_cast<sfb_context *>(cctx), wavefield, medium, which, shot, host, count);
+}
+
+SFB_API int sfb_get_field_f64(const sfb_context *cctx, int wavefield, int medium, int which, int shot, double *host,
+                              size_t count) {
+  return get_field_impl(const_cast<sfb_context *>(cctx), wavefield, medium, which, shot, host, count);
 }
 
 SFB_API int sfb_set_field(sfb_context *ctx, int wavefield, int medium, int which, int shot, const float *host,
@@ -1581,15 +1647,15 @@ SFB_API int sfb_set_field(sfb_context *ctx, int wavefield, int medium, int which
     const size_t n = static_cast<size_t>(f.nglob) * f.nc;
     if (count < n) throw std::invalid_argument("field buffer too small");
     if (shot < 0 || shot >= ctx->P.nshots) throw std::invalid_argument("shot out of range");
-    std::vector<float> tmp(n);
+    std::vector<real> tmp(n);
     for (int c = 0; c < f.nc; ++c)
       for (int g = 0; g < f.nglob; ++g) tmp[static_cast<size_t>(g) * f.nc + c] = host[static_cast<size_t>(c) * f.nglob + g];
-    float *dst = which == 0 ? f.u : which == 1 ? f.v : f.a;
+    real *dst = which == 0 ? f.u : which == 1 ? f.v : f.a;
     const int S = ctx->P.nshots;
     ck(cudaStreamSynchronize(ctx->stream), "sync");
     if (n)
-      ck(cudaMemcpy2D(dst + static_cast<size_t>(shot) * f.nc, static_cast<size_t>(S) * f.nc * sizeof(float),
-                      tmp.data(), f.nc * sizeof(float), f.nc * sizeof(float), f.nglob, cudaMemcpyHostToDevice),
+      ck(cudaMemcpy2D(dst + static_cast<size_t>(shot) * f.nc, static_cast<size_t>(S) * f.nc * sizeof(real),
+                      tmp.data(), f.nc * sizeof(real), f.nc * sizeof(real), f.nglob, cudaMemcpyHostToDevice),
          "field h2d");
     return SFB_OK;
   });
@@ -1638,9 +1704,7 @@ SFB_API int sfb_write_wavefield(const sfb_context *cctx, int shot, const char *d
     if (per && ctx->stacey_data.p) {
       snap.store.resize(per);
       ck(cudaStreamSynchronize(ctx->stream), "sync");
-      ck(cudaMemcpy(snap.store.data(), ctx->stacey_data.p + static_cast<size_t>(shot) * per, per * sizeof(float),
-                    cudaMemcpyDeviceToHost),
-         "store d2h");
+      copy_d2h(snap.store.data(), ctx->stacey_data.p + static_cast<size_t>(shot) * per, per, "store d2h");
     } else if (per) {
       throw StateError("the forward run kept no boundary store (save_boundary_values)");
     }
@@ -1675,9 +1739,7 @@ SFB_API int sfb_read_wavefield(sfb_context *ctx, int shot, const char *directory
         const size_t total = per * P.nshots;
         ctx->stacey_data.alloc(total, &ctx->device_bytes);
       }
-      ck(cudaMemcpy(ctx->stacey_data.p + static_cast<size_t>(shot) * per, snap.store.data(), per * sizeof(float),
-                    cudaMemcpyHostToDevice),
-         "store h2d");
+      copy_h2d(ctx->stacey_data.p + static_cast<size_t>(shot) * per, snap.store.data(), per, "store h2d");
     }
     F.step = P.nstep;  // the combined run starts from this state
     return SFB_OK;
@@ -1765,9 +1827,15 @@ SFB_API int sfb_set_source_time_function(sfb_context *ctx, int isource, const fl
     const size_t n = static_cast<size_t>(P.nstep) * 2;
     if (count < n) throw std::invalid_argument("source time function buffer too small");
     std::copy(host, host + n, P.v_src_stf.begin() + static_cast<size_t>(isource) * n);
-    if (ctx->on_device)
-      ck(cudaMemcpyAsync(ctx->src_stf.p + static_cast<size_t>(isource) * n, host, n * sizeof(float),
-                         cudaMemcpyHostToDevice, ctx->stream), "stf h2d");
+    if (ctx->on_device) {
+      if constexpr (std::is_same<real, float>::value) {
+        ck(cudaMemcpyAsync(ctx->src_stf.p + static_cast<size_t>(isource) * n, host, n * sizeof(float),
+                           cudaMemcpyHostToDevice, ctx->stream), "stf h2d");
+      } else {
+        ck(cudaStreamSynchronize(ctx->stream), "sync");
+        copy_h2d(ctx->src_stf.p + static_cast<size_t>(isource) * n, host, n, "stf h2d");
+      }
+    }
     return SFB_OK;
   });
 }
@@ -1807,7 +1875,7 @@ SFB_API int sfb_time_stiffness(sfb_context *ctx, int medium, int reps, double *m
     // the repeated launches accumulated into the force array: clear it
     const dev::MediumFields &f = W.f[medium];
     const size_t ld = static_cast<size_t>(f.nglob + (f.nglob & 1)) * f.nc;
-    if (ld) ck(cudaMemsetAsync(f.a, 0, ld * ctx->P.nshots * sizeof(float), ctx->stream), "clear force");
+    if (ld) ck(cudaMemsetAsync(f.a, 0, ld * ctx->P.nshots * sizeof(real), ctx->stream), "clear force");
     ck(cudaStreamSynchronize(ctx->stream), "sync");
     return SFB_OK;
   });
@@ -1835,7 +1903,7 @@ SFB_API int sfb_frechet_compute_derivatives(sfb_context *ctx, double dt) {
       ctx->kern.alloc(nk, &ctx->device_bytes);
     }
     for (int m : {dev::MED_PSV, dev::MED_AC})
-      dev::launch_frechet(m, ctx->P.asmb.ngll, ctx->st, A.f[m], B.f[m], ctx->P.nshots, static_cast<float>(dt),
+      dev::launch_frechet(m, ctx->P.asmb.ngll, ctx->st, A.f[m], B.f[m], ctx->P.nshots, static_cast<real>(dt),
                           ctx->kern.p, 0, ctx->stream);
     ck(cudaGetLastError(), "frechet");
     return SFB_OK;
@@ -1858,9 +1926,8 @@ SFB_API int sfb_set_adjoint_sources(sfb_context *ctx, int shot, const float *hos
       for (int r = 0; r < nrec; ++r)
         for (int cc = 0; cc < 2; ++cc)
           tmp[(static_cast<size_t>(r) * P.nstep + t) * 2 + cc] = host[(static_cast<size_t>(t) * nrec + r) * 2 + cc];
-    ck(cudaMemcpy(ctx->adj_stf.p + static_cast<size_t>(shot) * n, tmp.data(), n * sizeof(float),
-                  cudaMemcpyHostToDevice),
-       "adjoint stf h2d");
+    ck(cudaStreamSynchronize(ctx->stream), "sync");
+    copy_h2d(ctx->adj_stf.p + static_cast<size_t>(shot) * n, tmp.data(), n, "adjoint stf h2d");
     return SFB_OK;
   });
 }
@@ -1933,7 +2000,7 @@ SFB_API int sfb_copy_forward_to_backward(const sfb_context *csrc, sfb_context *d
     copy_fields(dst, D, S);
     if (src->stacey_data.p) {
       ensure_store(dst);
-      ck(cudaMemcpyAsync(dst->stacey_data.p, src->stacey_data.p, src->stacey_data.n * sizeof(float),
+      ck(cudaMemcpyAsync(dst->stacey_data.p, src->stacey_data.p, src->stacey_data.n * sizeof(real),
                          cudaMemcpyDeviceToDevice, dst->stream),
          "copy store");
     }
@@ -1953,8 +2020,8 @@ void refresh_model(sfb_context *ctx) {
   if (ctx->on_device) {
     // refresh the material words of the packed and SoA device arrays
     std::vector<float> m0(nloc), m1(nloc), m2(nloc);
-    std::vector<float> pack(nloc * dev::kPackFields);
-    ck(cudaMemcpy(pack.data(), ctx->pack.p, pack.size() * sizeof(float), cudaMemcpyDeviceToHost), "pack d2h");
+    std::vector<real> pack(nloc * dev::kPackFields);
+    ck(cudaMemcpy(pack.data(), ctx->pack.p, pack.size() * sizeof(real), cudaMemcpyDeviceToHost), "pack d2h");
     for (int d = 0; d < a.nspec; ++d) {
       const int e = ctx->perm[d];
       const int m = a.medium[e];
@@ -1963,12 +2030,12 @@ void refresh_model(sfb_context *ctx) {
         if (m == MEDIUM_ELASTIC_PSV) { m0[q] = a.kappa[p]; m1[q] = a.mu[p]; m2[q] = a.rho[p]; }
         else if (m == MEDIUM_ELASTIC_SH) { m0[q] = a.mu[p]; m1[q] = a.rho[p]; m2[q] = 0.f; }
         else { m0[q] = a.rho_inverse[p]; m1[q] = a.kappa[p]; m2[q] = 0.f; }
-        float *blk = &pack[static_cast<size_t>(d) * dev::kPackFields * nn];
+        real *blk = &pack[static_cast<size_t>(d) * dev::kPackFields * nn];
         blk[6 * nn + k] = m0[q];
         blk[7 * nn + k] = m1[q];
       }
     }
-    ck(cudaMemcpy(ctx->pack.p, pack.data(), pack.size() * sizeof(float), cudaMemcpyHostToDevice), "pack h2d");
+    ck(cudaMemcpy(ctx->pack.p, pack.data(), pack.size() * sizeof(real), cudaMemcpyHostToDevice), "pack h2d");
     if (ctx->pack_aff.p) {
       // the material words of the compact block
       const int words = dev::affine_chunk_words(ctx->P.asmb.ngll);
@@ -1990,9 +2057,9 @@ void refresh_model(sfb_context *ctx) {
       }
       ck(cudaMemcpy(ctx->pack_aff.p, aff.data(), aff.size() * sizeof(float), cudaMemcpyHostToDevice), "aff h2d");
     }
-    ck(cudaMemcpy(ctx->mat0_all.p, m0.data(), nloc * sizeof(float), cudaMemcpyHostToDevice), "mat0");
-    ck(cudaMemcpy(ctx->mat1_all.p, m1.data(), nloc * sizeof(float), cudaMemcpyHostToDevice), "mat1");
-    ck(cudaMemcpy(ctx->mat2_all.p, m2.data(), nloc * sizeof(float), cudaMemcpyHostToDevice), "mat2");
+    copy_h2d(ctx->mat0_all.p, m0.data(), nloc, "mat0");
+    copy_h2d(ctx->mat1_all.p, m1.data(), nloc, "mat1");
+    copy_h2d(ctx->mat2_all.p, m2.data(), nloc, "mat2");
     ctx->taps_ready = false;  // pressure taps carry the material
     // captured graphs hold the old tap buffers
     ctx->drop_forward_graphs();
@@ -2036,12 +2103,12 @@ SFB_API int sfb_reset(sfb_context *ctx) {
       if (!W.allocated) continue;
       zero_fields(ctx, W);
       for (int m : kMedia) {
-        if (W.cu[m].p) ck(cudaMemsetAsync(W.cu[m].p, 0, W.cu[m].n * sizeof(float), ctx->stream), "zero cu");
-        if (W.cv[m].p) ck(cudaMemsetAsync(W.cv[m].p, 0, W.cv[m].n * sizeof(float), ctx->stream), "zero cv");
+        if (W.cu[m].p) ck(cudaMemsetAsync(W.cu[m].p, 0, W.cu[m].n * sizeof(real), ctx->stream), "zero cu");
+        if (W.cv[m].p) ck(cudaMemsetAsync(W.cv[m].p, 0, W.cv[m].n * sizeof(real), ctx->stream), "zero cv");
       }
       W.step = 0;
     }
-    if (ctx->stacey_data.p) ck(cudaMemsetAsync(ctx->stacey_data.p, 0, ctx->stacey_data.n * sizeof(float), ctx->stream), "zero store");
+    if (ctx->stacey_data.p) ck(cudaMemsetAsync(ctx->stacey_data.p, 0, ctx->stacey_data.n * sizeof(real), ctx->stream), "zero store");
     if (ctx->kern.p) ck(cudaMemsetAsync(ctx->kern.p, 0, ctx->kern.n * sizeof(double), ctx->stream), "zero kernels");
     ck(cudaStreamSynchronize(ctx->stream), "reset");
     return SFB_OK;

@@ -17,21 +17,24 @@
 namespace sfb {
 namespace dev {
 
-__constant__ float c_hp[64];   // hprime[i*N + j] = l_j'(xi_i)
-__constant__ float c_hpw[64];  // hprime_wgll[ix*N + l] = hprime[l*N + ix] * w[l]
-__constant__ float c_w[8];
+__constant__ real c_hp[64];   // hprime[i*N + j] = l_j'(xi_i)
+__constant__ real c_hpw[64];  // hprime_wgll[ix*N + l] = hprime[l*N + ix] * w[l]
+__constant__ real c_w[8];
+#ifndef SFB_FP64
 // the same tables as (v, v) pairs for the packed two-shot arithmetic
 __constant__ float2 c_hp2[64];
 __constant__ float2 c_hpw2[64];
 __constant__ float2 c_w2[8];
+#endif
 
-void set_quadrature(int n, const float *hp, const float *w) {
-  float hpw[64];
+void set_quadrature(int n, const real *hp, const real *w) {
+  real hpw[64];
   for (int ix = 0; ix < n; ++ix)
     for (int l = 0; l < n; ++l) hpw[ix * n + l] = hp[l * n + ix] * w[l];
-  cudaMemcpyToSymbol(c_hp, hp, sizeof(float) * n * n);
-  cudaMemcpyToSymbol(c_hpw, hpw, sizeof(float) * n * n);
-  cudaMemcpyToSymbol(c_w, w, sizeof(float) * n);
+  cudaMemcpyToSymbol(c_hp, hp, sizeof(real) * n * n);
+  cudaMemcpyToSymbol(c_hpw, hpw, sizeof(real) * n * n);
+  cudaMemcpyToSymbol(c_w, w, sizeof(real) * n);
+#ifndef SFB_FP64
   float2 hp2[64], hpw2[64], w2[8];
   for (int k = 0; k < n * n; ++k) {
     hp2[k] = make_float2(hp[k], hp[k]);
@@ -41,59 +44,81 @@ void set_quadrature(int n, const float *hp, const float *w) {
   cudaMemcpyToSymbol(c_hp2, hp2, sizeof(float2) * n * n);
   cudaMemcpyToSymbol(c_hpw2, hpw2, sizeof(float2) * n * n);
   cudaMemcpyToSymbol(c_w2, w2, sizeof(float2) * n);
+#endif
 }
 
 namespace {
 
 template <int NC> struct Vec;
 template <> struct Vec<1> {
-  using T = float;
-  __device__ static T zero() { return 0.f; }
+  using T = real;
+  __device__ static T zero() { return 0; }
 };
 template <> struct Vec<2> {
-  using T = float2;
-  __device__ static T zero() { return make_float2(0.f, 0.f); }
+  using T = real2;
+  __device__ static T zero() { return T{0, 0}; }
 };
 
-__device__ __forceinline__ float comp(float v, int) { return v; }
-__device__ __forceinline__ float comp(float2 v, int c) { return c == 0 ? v.x : v.y; }
-__device__ __forceinline__ void set_comp(float &v, int, float x) { v = x; }
-__device__ __forceinline__ void set_comp(float2 &v, int c, float x) {
+__device__ __forceinline__ real comp(real v, int) { return v; }
+__device__ __forceinline__ real comp(real2 v, int c) { return c == 0 ? v.x : v.y; }
+__device__ __forceinline__ void set_comp(real &v, int, real x) { v = x; }
+__device__ __forceinline__ void set_comp(real2 &v, int c, real x) {
   if (c == 0) v.x = x; else v.y = x;
 }
 
-// Vector reduction into global memory (RED.E.ADD.F32x2 on sm_90+).
-__device__ __forceinline__ void red_add(float *p, float v) { atomicAdd(p, v); }
+// Vector reduction into global memory (RED.E.ADD.F32x2 on sm_90+; FP64:
+// one atomic per component).
+__device__ __forceinline__ void red_add(real *p, real v) { atomicAdd(p, v); }
+#ifdef SFB_FP64
+__device__ __forceinline__ void red_add(real2 *p, real2 v) {
+  atomicAdd(&p->x, v.x);
+  atomicAdd(&p->y, v.y);
+}
+#else
 __device__ __forceinline__ void red_add(float2 *p, float2 v) { atomicAdd(p, v); }
+#endif
+
+// The reference's constants are type_real (FP32): 4/3 and 1/3 rounded to
+// FP32, kept so in the FP64 build, which computes the same discrete problem.
+constexpr real kFourThirds = static_cast<real>(static_cast<float>(4.0 / 3.0));
+constexpr real kOneThird = static_cast<real>(static_cast<float>(1.0 / 3.0));
+
+// Square root in the working precision.
+__device__ __forceinline__ float msqrt(float x) { return sqrtf(x); }
+__device__ __forceinline__ double msqrt(double x) { return sqrt(x); }
+// A point index held in a `real` word of a packed static block: its int bits
+// (FP32) or its value (FP64 build).
+__device__ __forceinline__ int pack_index(float v) { return __float_as_int(v); }
+__device__ __forceinline__ int pack_index(double v) { return static_cast<int>(v); }
 
 // Stacey traction added to `acc` for velocity `vel` (stacey.tpp:41-75 P-SV,
 // :125-145 SH, :178-212 acoustic).
 template <int MED>
-__device__ __forceinline__ void stacey(float m0, float m1, float m2, float nx, float nz,
-                                       float we, const float *vel, float *acc) {
-  const float jac1d = sqrtf(nx * nx + nz * nz);
+__device__ __forceinline__ void stacey(real m0, real m1, real m2, real nx, real nz,
+                                       real we, const real *vel, real *acc) {
+  const real jac1d = msqrt(nx * nx + nz * nz);
   if (MED == MED_PSV) {
-    const float kappa = m0, mu = m1, rho = m2;
-    const float l2m = kappa + static_cast<float>(4.0 / 3.0) * mu;
-    const float rho_vp = sqrtf(l2m / rho) * rho;
-    const float rho_vs = sqrtf(rho * mu);
-    const float vn = vel[0] * nx + vel[1] * nz;
-    const float dn[2] = {nx, nz};
+    const real kappa = m0, mu = m1, rho = m2;
+    const real l2m = kappa + kFourThirds * mu;
+    const real rho_vp = msqrt(l2m / rho) * rho;
+    const real rho_vs = msqrt(rho * mu);
+    const real vn = vel[0] * nx + vel[1] * nz;
+    const real dn[2] = {nx, nz};
 #pragma unroll
     for (int c = 0; c < 2; ++c) {
-      const float fac = ((vn * dn[c] / (jac1d * jac1d)) * (rho_vp - rho_vs)) + vel[c] * rho_vs;
-      acc[c] += -1.0f * fac * jac1d * we;
+      const real fac = ((vn * dn[c] / (jac1d * jac1d)) * (rho_vp - rho_vs)) + vel[c] * rho_vs;
+      acc[c] += static_cast<real>(-1) * fac * jac1d * we;
     }
   } else if (MED == MED_SH) {
-    const float mu = m0, rho = m1;
-    const float rho_vs = sqrtf(rho * mu);
-    const float fac = we * jac1d;
-    acc[0] += -1.0f * fac * rho_vs * vel[0];
+    const real mu = m0, rho = m1;
+    const real rho_vs = msqrt(rho * mu);
+    const real fac = we * jac1d;
+    acc[0] += static_cast<real>(-1) * fac * rho_vs * vel[0];
   } else {
-    const float rho_inv = m0, kappa = m1;
-    const float rvi = sqrtf(rho_inv * (1.0f / kappa));
-    const float fac = we * jac1d;
-    acc[0] += -1.0f * fac * rvi * vel[0];
+    const real rho_inv = m0, kappa = m1;
+    const real rvi = msqrt(rho_inv * (static_cast<real>(1) / kappa));
+    const real fac = we * jac1d;
+    acc[0] += static_cast<real>(-1) * fac * rvi * vel[0];
   }
 }
 
@@ -235,12 +260,12 @@ __device__ __forceinline__ void tail_work(const Static &st, const MediumFields &
       if (tw.src.medium[i] != MED) continue;
       const size_t p = static_cast<size_t>(tw.src.elem[i]) * NN + kk;
       const int gi = st.iglob[p];
-      float *A = f.a + (static_cast<size_t>(gi) * S + tw.src.shot[i]) * NC;
+      real *A = f.a + (static_cast<size_t>(gi) * S + tw.src.shot[i]) * NC;
 #pragma unroll
       for (int c = 0; c < NC; ++c) {
-        const float stf = tw.src.stf[(static_cast<size_t>(i) * tw.src.nstep + istep) * 2 + c];
-        const float arr = tw.src.array[(static_cast<size_t>(i) * 2 + c) * NN + kk];
-        float val = stf * arr;
+        const real stf = tw.src.stf[(static_cast<size_t>(i) * tw.src.nstep + istep) * 2 + c];
+        const real arr = tw.src.array[(static_cast<size_t>(i) * 2 + c) * NN + kk];
+        real val = stf * arr;
         if (MED == MED_AC) val = stf * arr / st.mat1[p];
         atomicAdd(A + c, val);
       }
@@ -252,14 +277,14 @@ __device__ __forceinline__ void tail_work(const Static &st, const MediumFields &
     for (int idx = gtid; idx < n * S; idx += gstride) {
       const int i = idx / S, s = idx % S;
       if (tw.cp_mode == 1) {  // acoustic self += w (n . u_elastic)
-        const float2 u = reinterpret_cast<const float2 *>(o.u)[static_cast<size_t>(tw.cp.other[i]) * S + s];
+        const real2 u = reinterpret_cast<const real2 *>(o.u)[static_cast<size_t>(tw.cp.other[i]) * S + s];
         atomicAdd(f.a + static_cast<size_t>(tw.cp.self[i]) * S + s,
                   tw.cp.factor[i] * (tw.cp.nx[i] * u.x + tw.cp.nz[i] * u.y));
       } else {  // elastic self += w n chi_ddot
         const int oi = tw.cp.other[i];
-        const float r = o.a[static_cast<size_t>(oi) * S + s];
-        const float chi_dd = tw.other_divided ? r : r * o.minv[oi];
-        float *A = f.a + (static_cast<size_t>(tw.cp.self[i]) * S + s) * 2;
+        const real r = o.a[static_cast<size_t>(oi) * S + s];
+        const real chi_dd = tw.other_divided ? r : r * o.minv[oi];
+        real *A = f.a + (static_cast<size_t>(tw.cp.self[i]) * S + s) * 2;
         atomicAdd(A, tw.cp.factor[i] * tw.cp.nx[i] * chi_dd);
         atomicAdd(A + 1, tw.cp.factor[i] * tw.cp.nz[i] * chi_dd);
       }
@@ -267,6 +292,7 @@ __device__ __forceinline__ void tail_work(const Static &st, const MediumFields &
   }
 }
 
+#ifndef SFB_FP64
 // Row-per-thread stiffness fed by bulk async copies, software-pipelined.
 // A CTA owns EPB elements; thread (el, iz) owns row iz of element el (N
 // points: the xi-contractions stay in registers, the gamma-contractions read
@@ -955,6 +981,7 @@ void launch_rpa(const Static &st, const MediumFields &f, const StaceyStore &ss, 
   launch_step_kernel(k_stiffness_rpa<MED, N, MINB>, grid, N * kAffineChunk, smem, stream, st, f, ss, istep_dev, tw,
                      fu);
 }
+#endif  // !SFB_FP64
 
 // Shot-parallel stiffness for S > 1 independent wavefields (batched shots).
 // One CTA per element and group of 32 * SPL shots; warp iz owns row iz of the
@@ -966,22 +993,43 @@ void launch_rpa(const Static &st, const MediumFields &f, const StaceyStore &ss, 
 // in shared memory and read by warp-uniform broadcasts.  Row contractions
 // stay in registers, column contractions read shared memory.
 template <int NV> struct VecN;
-template <> struct VecN<1> { using T = float; };
-template <> struct VecN<2> { using T = float2; };
-template <> struct VecN<4> { using T = float4; };
-__device__ __forceinline__ float vget(const float &v, int) { return v; }
-__device__ __forceinline__ float vget(const float2 &v, int i) { return i == 0 ? v.x : v.y; }
-__device__ __forceinline__ float vget(const float4 &v, int i) {
+template <> struct VecN<1> { using T = real; };
+template <> struct VecN<2> { using T = real2; };
+template <> struct VecN<4> { using T = real4; };
+__device__ __forceinline__ real vget(const real &v, int) { return v; }
+__device__ __forceinline__ real vget(const real2 &v, int i) { return i == 0 ? v.x : v.y; }
+__device__ __forceinline__ real vget(const real4 &v, int i) {
   return i == 0 ? v.x : i == 1 ? v.y : i == 2 ? v.z : v.w;
 }
-__device__ __forceinline__ void vset(float &v, int, float x) { v = x; }
-__device__ __forceinline__ void vset(float2 &v, int i, float x) { if (i == 0) v.x = x; else v.y = x; }
-__device__ __forceinline__ void vset(float4 &v, int i, float x) {
+__device__ __forceinline__ void vset(real &v, int, real x) { v = x; }
+__device__ __forceinline__ void vset(real2 &v, int i, real x) { if (i == 0) v.x = x; else v.y = x; }
+__device__ __forceinline__ void vset(real4 &v, int i, real x) {
   if (i == 0) v.x = x; else if (i == 1) v.y = x; else if (i == 2) v.z = x; else v.w = x;
 }
-__device__ __forceinline__ void vred(float *p, float v) { atomicAdd(p, v); }
+__device__ __forceinline__ void vred(real *p, real v) { atomicAdd(p, v); }
+#ifdef SFB_FP64
+__device__ __forceinline__ void vred(real2 *p, real2 v) {
+  atomicAdd(&p->x, v.x);
+  atomicAdd(&p->y, v.y);
+}
+__device__ __forceinline__ void vred(real4 *p, real4 v) {
+  atomicAdd(&p->x, v.x);
+  atomicAdd(&p->y, v.y);
+  atomicAdd(&p->z, v.z);
+  atomicAdd(&p->w, v.w);
+}
+#else
 __device__ __forceinline__ void vred(float2 *p, float2 v) { atomicAdd(p, v); }
 __device__ __forceinline__ void vred(float4 *p, float4 v) { atomicAdd(p, v); }
+#endif
+
+// Dynamic shared memory of k_stiffness_shots: the displacement and the
+// gamma fluxes of the element for the CTA's shots, and the static block.
+template <int MED, int N, int SPL>
+constexpr size_t shots_smem_bytes() {
+  return 2 * static_cast<size_t>(N * N * 32) * sizeof(typename VecN<((MED == MED_PSV) ? 2 : 1) * SPL>::T) +
+         static_cast<size_t>(kPackFields * N * N) * sizeof(real);
+}
 
 template <int MED, int N, int SPL, int MINB>
 __global__ void __launch_bounds__(N * 32, MINB)
@@ -991,9 +1039,10 @@ k_stiffness_shots(Static st, MediumFields f, int S, StaceyStore ss, const int *i
   constexpr int NN = N * N;
   constexpr int NV = NC * SPL;
   using W = typename VecN<NV>::T;
-  __shared__ W s_u[NN * 32];
-  __shared__ W s_fg[NN * 32];
-  __shared__ float s_st[kPackFields * NN];
+  extern __shared__ __align__(16) unsigned char shots_smem[];
+  W *s_u = reinterpret_cast<W *>(shots_smem);         // [NN * 32]
+  W *s_fg = s_u + NN * 32;                            // [NN * 32]
+  real *s_st = reinterpret_cast<real *>(s_fg + NN * 32);  // [kPackFields * NN]
   const int lane = threadIdx.x & 31, iz = threadIdx.x >> 5;
   const int e = f.elem_begin + blockIdx.x;
   const int s0 = (blockIdx.y * 32 + lane) * SPL;
@@ -1005,14 +1054,14 @@ k_stiffness_shots(Static st, MediumFields f, int S, StaceyStore ss, const int *i
   const int istep = (ss.mode != 0 || tw.src.n > 0) ? *istep_dev : 0;
   int g[N];
 #pragma unroll
-  for (int ix = 0; ix < N; ++ix) g[ix] = __float_as_int(s_st[iz * N + ix]);
-  float hpz[N], hpwz[N];
+  for (int ix = 0; ix < N; ++ix) g[ix] = pack_index(s_st[iz * N + ix]);
+  real hpz[N], hpwz[N];
 #pragma unroll
   for (int l = 0; l < N; ++l) {
     hpz[l] = c_hp[iz * N + l];
     hpwz[l] = c_hpw[iz * N + l];
   }
-  const float wz = c_w[iz];
+  const real wz = c_w[iz];
   // u(g, s) for s = s0 .. s0+SPL-1, components interleaved: (g*S + s0)*NC floats
   const W *U = reinterpret_cast<const W *>(f.u);
   W *A = reinterpret_cast<W *>(f.a);
@@ -1022,7 +1071,7 @@ k_stiffness_shots(Static st, MediumFields f, int S, StaceyStore ss, const int *i
 #pragma unroll
   for (int ix = 0; ix < N; ++ix) {
     if (act) ur[ix] = U[g[ix] * Sv + lofs];
-    else { for (int q = 0; q < NV; ++q) vset(ur[ix], q, 0.f); }
+    else { for (int q = 0; q < NV; ++q) vset(ur[ix], q, 0); }
     s_u[(iz * N + ix) * 32 + lane] = ur[ix];
   }
   __syncthreads();
@@ -1030,12 +1079,12 @@ k_stiffness_shots(Static st, MediumFields f, int S, StaceyStore ss, const int *i
 #pragma unroll
   for (int ix = 0; ix < N; ++ix) {
     const int k = iz * N + ix;
-    const float xix = s_st[1 * NN + k], xiz = s_st[2 * NN + k];
-    const float gax = s_st[3 * NN + k], gaz = s_st[4 * NN + k];
-    const float jac = s_st[5 * NN + k], m0 = s_st[6 * NN + k], m1 = s_st[7 * NN + k];
-    float dxi[NV], dga[NV];
+    const real xix = s_st[1 * NN + k], xiz = s_st[2 * NN + k];
+    const real gax = s_st[3 * NN + k], gaz = s_st[4 * NN + k];
+    const real jac = s_st[5 * NN + k], m0 = s_st[6 * NN + k], m1 = s_st[7 * NN + k];
+    real dxi[NV], dga[NV];
 #pragma unroll
-    for (int q = 0; q < NV; ++q) { dxi[q] = 0.f; dga[q] = 0.f; }
+    for (int q = 0; q < NV; ++q) { dxi[q] = 0; dga[q] = 0; }
 #pragma unroll
     for (int l = 0; l < N; ++l) {
       const W col = s_u[(l * N + ix) * 32 + lane];
@@ -1048,16 +1097,16 @@ k_stiffness_shots(Static st, MediumFields f, int S, StaceyStore ss, const int *i
     W f0, f1;
 #pragma unroll
     for (int j = 0; j < SPL; ++j) {
-      float du[NC][2];
+      real du[NC][2];
 #pragma unroll
       for (int c = 0; c < NC; ++c) {
         du[c][0] = xix * dxi[j * NC + c] + gax * dga[j * NC + c];
         du[c][1] = xiz * dxi[j * NC + c] + gaz * dga[j * NC + c];
       }
-      float T[NC][2];
+      real T[NC][2];
       if constexpr (MED == MED_PSV) {
-        const float l2m = m0 + static_cast<float>(4.0 / 3.0) * m1;
-        const float lam = l2m - 2.0f * m1;
+        const real l2m = m0 + kFourThirds * m1;
+        const real lam = l2m - static_cast<real>(2) * m1;
         T[0][0] = l2m * du[0][0] + lam * du[1][1];
         T[1][1] = l2m * du[1][1] + lam * du[0][0];
         T[0][1] = m1 * (du[0][1] + du[1][0]);
@@ -1081,9 +1130,9 @@ k_stiffness_shots(Static st, MediumFields f, int S, StaceyStore ss, const int *i
   const bool fused = fu.enabled && (eflag & kElemPrivate) && iz >= 1 && iz <= N - 2;
 #pragma unroll
   for (int ix = 0; ix < N; ++ix) {
-    float t1[NV], t2[NV];
+    real t1[NV], t2[NV];
 #pragma unroll
-    for (int q = 0; q < NV; ++q) { t1[q] = 0.f; t2[q] = 0.f; }
+    for (int q = 0; q < NV; ++q) { t1[q] = 0; t2[q] = 0; }
 #pragma unroll
     for (int l = 0; l < N; ++l) {
       const W col = s_fg[(l * N + ix) * 32 + lane];
@@ -1096,23 +1145,23 @@ k_stiffness_shots(Static st, MediumFields f, int S, StaceyStore ss, const int *i
     W out;
 #pragma unroll
     for (int j = 0; j < SPL; ++j) {
-      float acc[2];
+      real acc[2];
 #pragma unroll
-      for (int c = 0; c < NC; ++c) acc[c] = (wz * t1[j * NC + c] + c_w[ix] * t2[j * NC + c]) * -1.0f;
+      for (int c = 0; c < NC; ++c) acc[c] = (wz * t1[j * NC + c] + c_w[ix] * t2[j * NC + c]) * static_cast<real>(-1);
       if (eflag & 3) {
         const size_t p = (static_cast<size_t>(e) * N + iz) * N + ix;
         const uint8_t b = st.bnd[p];
         if ((b & 1) && act) {
-          const float *Vp = f.v + (static_cast<size_t>(g[ix]) * S + s0 + j) * NC;
-          float vel[2];
+          const real *Vp = f.v + (static_cast<size_t>(g[ix]) * S + s0 + j) * NC;
+          real vel[2];
 #pragma unroll
           for (int c = 0; c < NC; ++c) vel[c] = Vp[c];
-          stacey<MED>(s_st[6 * NN + iz * N + ix], s_st[7 * NN + iz * N + ix], st.mat2 ? st.mat2[p] : 0.f,
+          stacey<MED>(s_st[6 * NN + iz * N + ix], s_st[7 * NN + iz * N + ix], st.mat2 ? st.mat2[p] : real(0),
                       st.bnd_nx[p], st.bnd_nz[p], st.bnd_w[p], vel, acc);
         }
         if (b & 2) {
 #pragma unroll
-          for (int c = 0; c < NC; ++c) acc[c] = 0.f;
+          for (int c = 0; c < NC; ++c) acc[c] = 0;
         }
       }
       if (slot >= 0 && act) {
@@ -1140,7 +1189,7 @@ k_stiffness_shots(Static st, MediumFields f, int S, StaceyStore ss, const int *i
       W vel = Vw[at], uu = s_u[(iz * N + ix) * 32 + lane], aa;
 #pragma unroll
       for (int q = 0; q < NV; ++q) {
-        const float a_q = vget(out, q) * fu.minv[g[ix] * NC + (q % NC)];
+        const real a_q = vget(out, q) * fu.minv[g[ix] * NC + (q % NC)];
         vset(aa, q, a_q);
         vset(vel, q, vget(vel, q) + fu.dt2 * a_q);
       }
@@ -1164,6 +1213,7 @@ k_stiffness_shots(Static st, MediumFields f, int S, StaceyStore ss, const int *i
 }
 
 
+#ifndef SFB_FP64
 // ---------------------------------------------------------------------------
 // Batched stiffness, two shots per lane in packed FP32x2 arithmetic.  Same
 // work and launch shape as k_stiffness_shots<..., SPL = 2>, but every
@@ -1557,18 +1607,39 @@ k_stiffness_pk(Static st, MediumFields f, int S, StaceyStore ss, const int *iste
   tail_work<MED, N>(st, f, S, istep, tw, blockIdx.y * gridDim.x + blockIdx.x, gridDim.x * gridDim.y);
 }
 
+#endif  // !SFB_FP64
+
+// Dynamic shared memory above the default 48 KiB needs an opt-in once per
+// kernel instantiation.
+template <int MED, int N, int SPL, int MINB>
+size_t shots_smem_opt_in() {
+  constexpr size_t bytes = shots_smem_bytes<MED, N, SPL>();
+  if constexpr (bytes > 48 * 1024) {
+    static bool done = false;
+    if (!done) {
+      cudaFuncSetAttribute(k_stiffness_shots<MED, N, SPL, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           static_cast<int>(bytes));
+      done = true;
+    }
+  }
+  return bytes;
+}
+
 // variant: kShotsPacked (two shots per lane, f32x2), kShotsPair (two shots
 // per lane, scalar), kShotsSingle (one shot per lane); kShotsAuto picks the
 // packed kernel when it applies.  Two shots per lane need an even S and
-// (for the static shared staging) NGLL <= 5.
+// (for the static shared staging) NGLL <= 5.  The FP64 build has the
+// one-shot-per-lane kernel only.
 template <int MED, int N, int MINB>
 void launch_shots(const Static &st, const MediumFields &f, int S, const StaceyStore &ss, const int *istep_dev,
                   const TailWork &tw, const FusedUpdate &fu, int variant, cudaStream_t stream) {
+#ifndef SFB_FP64
   if constexpr (N <= 5) {
     if (S % 2 == 0 && variant != kShotsSingle) {
       dim3 grid(f.nelem, (S / 2 + 31) / 32);
       if (variant == kShotsPair)
-        launch_step_kernel(k_stiffness_shots<MED, N, 2, MINB>, grid, N * 32, 0, stream, st, f, S, ss, istep_dev, tw, fu);
+        launch_step_kernel(k_stiffness_shots<MED, N, 2, MINB>, grid, N * 32, shots_smem_opt_in<MED, N, 2, MINB>(),
+                           stream, st, f, S, ss, istep_dev, tw, fu);
       else if (st.affine[MED] && st.pack_aff)  // compact block: geometry constants in registers
         launch_step_kernel(k_stiffness_pk<MED, N, MINB, false, true>, grid, N * 32, 0, stream, st, f, S, ss, istep_dev,
                            tw, fu, FrechetFuse{});
@@ -1578,11 +1649,17 @@ void launch_shots(const Static &st, const MediumFields &f, int S, const StaceySt
       return;
     }
   }
+#else
+  (void)variant;
+#endif
   dim3 grid(f.nelem, (S + 31) / 32);
-  launch_step_kernel(k_stiffness_shots<MED, N, 1, MINB>, grid, N * 32, 0, stream, st, f, S, ss, istep_dev, tw, fu);
+  launch_step_kernel(k_stiffness_shots<MED, N, 1, MINB>, grid, N * 32, shots_smem_opt_in<MED, N, 1, MINB>(), stream,
+                     st, f, S, ss, istep_dev, tw, fu);
 }
 
+#ifndef SFB_FP64
 constexpr size_t kFrechetDynSmem = (2 * 25 + 9) * 32 * sizeof(float4) + 3 * 25 * 32 * sizeof(float);
+#endif
 
 
 // ---------------------------------------------------------------------------
@@ -1600,11 +1677,11 @@ __global__ void k_sources(Static st, SourceSet src, MediumFields f, int medium, 
   const size_t p = static_cast<size_t>(e) * N * N + k;
   const int gi = st.iglob[p];
   const int s = src.shot[i];
-  float *A = f.a + (static_cast<size_t>(gi) * nshots + s) * f.nc;
+  real *A = f.a + (static_cast<size_t>(gi) * nshots + s) * f.nc;
   for (int c = 0; c < f.nc; ++c) {
-    const float stf = src.stf[(static_cast<size_t>(i) * src.nstep + istep) * 2 + c];
-    const float arr = src.array[(static_cast<size_t>(i) * 2 + c) * N * N + k];
-    float val = stf * arr;
+    const real stf = src.stf[(static_cast<size_t>(i) * src.nstep + istep) * 2 + c];
+    const real arr = src.array[(static_cast<size_t>(i) * 2 + c) * N * N + k];
+    real val = stf * arr;
     if (medium == MED_AC) val = stf * arr / st.mat1[p];
     atomicAdd(A + c, val);
   }
@@ -1617,7 +1694,7 @@ __global__ void k_couple_acoustic(CouplingSet c, MediumFields ac, MediumFields e
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int s = blockIdx.y;
   if (i >= c.n || s >= nshots) return;
-  const float2 u = reinterpret_cast<const float2 *>(el.u)[static_cast<size_t>(c.other[i]) * nshots + s];
+  const real2 u = reinterpret_cast<const real2 *>(el.u)[static_cast<size_t>(c.other[i]) * nshots + s];
   atomicAdd(ac.a + static_cast<size_t>(c.self[i]) * nshots + s, c.factor[i] * (c.nx[i] * u.x + c.nz[i] * u.y));
 }
 
@@ -1627,9 +1704,9 @@ __global__ void k_couple_elastic(CouplingSet c, MediumFields el, MediumFields ac
   const int s = blockIdx.y;
   if (i >= c.n || s >= nshots) return;
   const int o = c.other[i];
-  const float r = ac.a[static_cast<size_t>(o) * nshots + s];
-  const float chi_dd = ac_divided ? r : r * ac.minv[o];
-  float *A = el.a + (static_cast<size_t>(c.self[i]) * nshots + s) * 2;
+  const real r = ac.a[static_cast<size_t>(o) * nshots + s];
+  const real chi_dd = ac_divided ? r : r * ac.minv[o];
+  real *A = el.a + (static_cast<size_t>(c.self[i]) * nshots + s) * 2;
   atomicAdd(A, c.factor[i] * c.nx[i] * chi_dd);
   atomicAdd(A + 1, c.factor[i] * c.nz[i] * chi_dd);
 }
@@ -1638,21 +1715,21 @@ __global__ void k_couple_elastic(CouplingSet c, MediumFields el, MediumFields ac
 // Receivers (compute_seismogram.tpp:98-135, wavefield.hpp): one block of 64
 // threads per (receiver, shot).
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ float ld_comp(const MediumFields &f, int which, int s, int g, int c,
-                                         float dt2, int mode, int S) {
+__device__ __forceinline__ real ld_comp(const MediumFields &f, int which, int s, int g, int c,
+                                        real dt2, int mode, int S) {
   const size_t idx = (static_cast<size_t>(g) * S + s) * f.nc + c;
   const size_t m = static_cast<size_t>(g) * f.nc + c;
   if (which == 0) return f.u[idx];
   if (mode == 0) return which == 1 ? f.v[idx] : f.a[idx];
-  const float a = f.a[idx] * f.minv[m];
+  const real a = f.a[idx] * f.minv[m];
   if (which == 2) return a;
   return f.v[idx] + dt2 * a;
 }
 
 __global__ void k_receivers(Static st, ReceiverSet rec, MediumFields f_psv, MediumFields f_sh,
-                            MediumFields f_ac, int N, float dt2, int mode, const int *istep_dev, int S) {
-  __shared__ float s_val[2][64];
-  __shared__ float s_red[2][64];
+                            MediumFields f_ac, int N, real dt2, int mode, const int *istep_dev, int S) {
+  __shared__ real s_val[2][64];
+  __shared__ real s_red[2][64];
   const int r = blockIdx.x, s = blockIdx.y, k = threadIdx.x;
   const int istep = *istep_dev;
   if (istep % rec.nsbs != 0) return;
@@ -1669,64 +1746,64 @@ __global__ void k_receivers(Static st, ReceiverSet rec, MediumFields f_psv, Medi
   else if (e >= f_sh.elem_begin && e < f_sh.elem_begin + f_sh.nelem) { med = MED_SH; F = &f_sh; }
   else { med = MED_AC; F = &f_ac; }
   const int g = (k < NN) ? st.iglob[p] : 0;
-  const float h = (k < NN) ? rec.lagrange[static_cast<size_t>(r) * NN + k] : 0.f;
+  const real h = (k < NN) ? rec.lagrange[static_cast<size_t>(r) * NN + k] : real(0);
   for (int it = 0; it < rec.ntypes; ++it) {
     const int type = rec.types[it];
-    float w0 = 0.f, w1 = 0.f;
+    real w0 = 0, w1 = 0;
     const bool need_grad = (med == MED_AC && type != 3) || (med == MED_PSV && type == 3);
     if (need_grad) {
       // field on all points of the element, then gradient at this point
       const int which = (med == MED_AC) ? (type == 3 ? 2 : type) : 0;
       if (k < NN) {
         s_val[0][k] = ld_comp(*F, which, s, g, 0, dt2, mode, S);
-        s_val[1][k] = (F->nc > 1) ? ld_comp(*F, which, s, g, 1, dt2, mode, S) : 0.f;
+        s_val[1][k] = (F->nc > 1) ? ld_comp(*F, which, s, g, 1, dt2, mode, S) : real(0);
       }
       __syncthreads();
       if (k < NN) {
-        float dxi[2] = {0.f, 0.f}, dga[2] = {0.f, 0.f};
+        real dxi[2] = {0, 0}, dga[2] = {0, 0};
         for (int l = 0; l < N; ++l)
           for (int c = 0; c < F->nc; ++c) {
             dxi[c] += c_hp[ix * N + l] * s_val[c][iz * N + l];
             dga[c] += c_hp[iz * N + l] * s_val[c][l * N + ix];
           }
-        const float xix = st.xix[p], xiz = st.xiz[p], gax = st.gax[p], gaz = st.gaz[p];
-        float du[2][2];
+        const real xix = st.xix[p], xiz = st.xiz[p], gax = st.gax[p], gaz = st.gaz[p];
+        real du[2][2];
         for (int c = 0; c < F->nc; ++c) {
           du[c][0] = xix * dxi[c] + gax * dga[c];
           du[c][1] = xiz * dxi[c] + gaz * dga[c];
         }
         if (med == MED_AC) {
-          const float ri = st.mat0[p];
+          const real ri = st.mat0[p];
           w0 = ri * du[0][0];
           w1 = ri * du[0][1];
         } else {
-          const float kappa = st.mat0[p], mu = st.mat1[p];
-          const float l2m = kappa + static_cast<float>(4.0 / 3.0) * mu;
-          const float lam = l2m - 2.0f * mu;
-          w0 = -1.0f * ((lam + static_cast<float>(2.0 / 3.0) * mu) * (du[0][0] + du[1][1]));
-          w1 = 0.f;
+          const real kappa = st.mat0[p], mu = st.mat1[p];
+          const real l2m = kappa + kFourThirds * mu;
+          const real lam = l2m - static_cast<real>(2) * mu;
+          w0 = static_cast<real>(-1) * ((lam + static_cast<real>(2.0 / 3.0) * mu) * (du[0][0] + du[1][1]));
+          w1 = 0;
         }
       }
       __syncthreads();
     } else if (k < NN) {
       if (med == MED_AC) {  // pressure = -chi_ddot
-        w0 = -1.0f * ld_comp(*F, 2, s, g, 0, dt2, mode, S);
+        w0 = static_cast<real>(-1) * ld_comp(*F, 2, s, g, 0, dt2, mode, S);
       } else {
         w0 = ld_comp(*F, type, s, g, 0, dt2, mode, S);
-        w1 = (F->nc > 1) ? ld_comp(*F, type, s, g, 1, dt2, mode, S) : 0.f;
+        w1 = (F->nc > 1) ? ld_comp(*F, type, s, g, 1, dt2, mode, S) : real(0);
       }
     }
     s_red[0][k] = h * w0;
     s_red[1][k] = h * w1;
     __syncthreads();
     if (k == 0) {
-      float a0 = 0.f, a1 = 0.f;
+      real a0 = 0, a1 = 0;
       for (int j = 0; j < NN; ++j) {
         a0 += s_red[0][j];
         a1 += s_red[1][j];
       }
-      const float sn = rec.sinv[r], cs = rec.cosv[r];
-      float *o = rec.seis + ((((static_cast<size_t>(s) * rec.max_sig + isig) * rec.ntypes + it) *
+      const real sn = rec.sinv[r], cs = rec.cosv[r];
+      real *o = rec.seis + ((((static_cast<size_t>(s) * rec.max_sig + isig) * rec.ntypes + it) *
                               rec.n + r) * 2);
       o[0] = cs * a0 - sn * a1;
       o[1] = sn * a0 + cs * a1;
@@ -1744,21 +1821,25 @@ __global__ void k_receivers(Static st, ReceiverSet rec, MediumFields f_psv, Medi
 // (Kahan 1965): the low-order bits lost by each FP32 add are carried to the
 // next one.  Explicit round-to-nearest adds keep the compiler from
 // contracting or reassociating the compensation away.
-__device__ __forceinline__ float kahan_add(float s, float &c, float x) {
-  const float y = __fsub_rn(x, c);
-  const float t = __fadd_rn(s, y);
-  c = __fsub_rn(__fsub_rn(t, s), y);
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ real kahan_add(real s, real &c, real x) {
+  const real y = sub_rn(x, c);
+  const real t = add_rn(s, y);
+  c = sub_rn(sub_rn(t, s), y);
   return t;
 }
 
-__global__ void k_predictor(float *u, float *v, float *a, size_t n, float dt, float dt2,
-                            float dtsq2, float *cu, float *cv) {
+__global__ void k_predictor(real *u, real *v, real *a, size_t n, real dt, real dt2,
+                            real dtsq2, real *cu, real *cv) {
   for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<size_t>(gridDim.x) * blockDim.x) {
-    const float ai = a[i];
-    const float vi = v[i];
+    const real ai = a[i];
+    const real vi = v[i];
     if (cu) {
-      float c_u = cu[i], c_v = cv[i];
+      real c_u = cu[i], c_v = cv[i];
       u[i] = kahan_add(u[i], c_u, dt * vi + dtsq2 * ai);
       v[i] = kahan_add(vi, c_v, dt2 * ai);
       cu[i] = c_u;
@@ -1767,15 +1848,15 @@ __global__ void k_predictor(float *u, float *v, float *a, size_t n, float dt, fl
       u[i] += dt * vi + dtsq2 * ai;
       v[i] = vi + dt2 * ai;
     }
-    a[i] = 0.f;
+    a[i] = 0;
   }
 }
-__global__ void k_corrector(float *v, const float *a, size_t n, float dt2) {
+__global__ void k_corrector(real *v, const real *a, size_t n, real dt2) {
   for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<size_t>(gridDim.x) * blockDim.x)
     v[i] += dt2 * a[i];
 }
-__global__ void k_divide(float *a, const float *minv, size_t n, int nshots, int nc) {
+__global__ void k_divide(real *a, const real *minv, size_t n, int nshots, int nc) {
   for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<size_t>(gridDim.x) * blockDim.x) {
     const size_t c = i % nc, g = (i / nc) / nshots;
@@ -1793,13 +1874,13 @@ __global__ void k_restore(RestoreParams P) {
   const int slot = istep / P.interval - 1;
   if (slot >= P.count) return;
   for (int m = 0; m < P.nm; ++m) {
-    const float *su = P.ck_u[m] + slot * P.ck_stride[m];
-    const float *sv = P.ck_v[m] + slot * P.ck_stride[m];
-    const size_t n4 = P.n[m] / 4;  // slots and fields start 16-byte aligned
+    const real *su = P.ck_u[m] + slot * P.ck_stride[m];
+    const real *sv = P.ck_v[m] + slot * P.ck_stride[m];
+    const size_t n4 = P.n[m] / 4;  // slots and fields start aligned to four values
     for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n4;
          i += static_cast<size_t>(gridDim.x) * blockDim.x) {
-      reinterpret_cast<float4 *>(P.u[m])[i] = reinterpret_cast<const float4 *>(su)[i];
-      reinterpret_cast<float4 *>(P.v[m])[i] = reinterpret_cast<const float4 *>(sv)[i];
+      reinterpret_cast<real4 *>(P.u[m])[i] = reinterpret_cast<const real4 *>(su)[i];
+      reinterpret_cast<real4 *>(P.v[m])[i] = reinterpret_cast<const real4 *>(sv)[i];
     }
     for (size_t i = n4 * 4 + blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < P.n[m];
          i += static_cast<size_t>(gridDim.x) * blockDim.x) {
@@ -1818,13 +1899,16 @@ __global__ void k_restore(RestoreParams P) {
 // ---------------------------------------------------------------------------
 // The tapped nodal value: field (0 u, 1 v, 2 a) * 2 + component, picked
 // with selects (no indexed local array).
-__device__ __forceinline__ float pick6(int wh, float a0, float a1, float b0, float b1, float c0, float c1) {
-  const float lo = (wh & 1) ? a1 : a0, mid = (wh & 1) ? b1 : b0, hi = (wh & 1) ? c1 : c0;
+__device__ __forceinline__ real pick6(int wh, real a0, real a1, real b0, real b1, real c0, real c1) {
+  const real lo = (wh & 1) ? a1 : a0, mid = (wh & 1) ? b1 : b0, hi = (wh & 1) ? c1 : c0;
   return wh < 2 ? lo : (wh < 4 ? mid : hi);
 }
 
-__device__ __forceinline__ void apply_taps(const ReceiverTaps &tp, int g, float u0, float u1, float v0, float v1,
-                                           float a0, float a1, float *seis_row) {
+__device__ __forceinline__ real2 mk2(real x, real y) { return real2{x, y}; }
+__device__ __forceinline__ real4 mk4(real x, real y, real z, real w) { return real4{x, y, z, w}; }
+
+__device__ __forceinline__ void apply_taps(const ReceiverTaps &tp, int g, real u0, real u1, real v0, real v1,
+                                           real a0, real a1, real *seis_row) {
   if (!((tp.mask[g >> 5] >> (g & 31)) & 1u)) return;
   int lo = 0, hi = tp.nsup - 1;
   while (lo < hi) {
@@ -1874,20 +1958,20 @@ __global__ void k_update_all(UpdateParams P) {
       const size_t ld2 = P.begin[mi + 1] - P.begin[mi];
       const size_t p0 = 2 * (w - ub);
       const bool two = p0 + 1 < ld2;
-      float4 r, vel, uu;
+      real4 r, vel, uu;
       if (two) {
-        r = reinterpret_cast<const float4 *>(M.a)[p0 / 2];
-        vel = reinterpret_cast<const float4 *>(M.v)[p0 / 2];
-        uu = reinterpret_cast<const float4 *>(M.u)[p0 / 2];
+        r = reinterpret_cast<const real4 *>(M.a)[p0 / 2];
+        vel = reinterpret_cast<const real4 *>(M.v)[p0 / 2];
+        uu = reinterpret_cast<const real4 *>(M.u)[p0 / 2];
       } else {
-        const float2 r2 = reinterpret_cast<const float2 *>(M.a)[p0];
-        const float2 v2 = reinterpret_cast<const float2 *>(M.v)[p0];
-        const float2 u2 = reinterpret_cast<const float2 *>(M.u)[p0];
-        r = make_float4(r2.x, r2.y, 0.f, 0.f);
-        vel = make_float4(v2.x, v2.y, 0.f, 0.f);
-        uu = make_float4(u2.x, u2.y, 0.f, 0.f);
+        const real2 r2 = reinterpret_cast<const real2 *>(M.a)[p0];
+        const real2 v2 = reinterpret_cast<const real2 *>(M.v)[p0];
+        const real2 u2 = reinterpret_cast<const real2 *>(M.u)[p0];
+        r = mk4(r2.x, r2.y, 0, 0);
+        vel = mk4(v2.x, v2.y, 0, 0);
+        uu = mk4(u2.x, u2.y, 0, 0);
       }
-      float m[4] = {0.f, 0.f, 0.f, 0.f};
+      real m[4] = {0, 0, 0, 0};
       int g[4] = {0, 0, 0, 0}, sh[4] = {0, 0, 0, 0};
 #pragma unroll
       for (int i = 0; i < 2; ++i) {
@@ -1895,7 +1979,7 @@ __global__ void k_update_all(UpdateParams P) {
         if (M.nc == 2) {
           const uint32_t n = static_cast<uint32_t>(p0 + i);
           const int gi = static_cast<int>(P.sdiv.div(n));
-          const float2 mm = reinterpret_cast<const float2 *>(M.minv)[gi];
+          const real2 mm = reinterpret_cast<const real2 *>(M.minv)[gi];
           g[2 * i] = g[2 * i + 1] = gi;
           sh[2 * i] = sh[2 * i + 1] = static_cast<int>(n - static_cast<uint32_t>(gi) * S);
           m[2 * i] = mm.x;
@@ -1910,7 +1994,7 @@ __global__ void k_update_all(UpdateParams P) {
           }
         }
       }
-      const float4 acc = make_float4(r.x * m[0], r.y * m[1], r.z * m[2], r.w * m[3]);
+      const real4 acc = mk4(r.x * m[0], r.y * m[1], r.z * m[2], r.w * m[3]);
       vel.x += P.dt2 * acc.x;  // corrector (newmark.tpp:44-47)
       vel.y += P.dt2 * acc.y;
       vel.z += P.dt2 * acc.z;
@@ -1923,12 +2007,12 @@ __global__ void k_update_all(UpdateParams P) {
             apply_taps(M.taps, g[2], uu.z, uu.w, vel.z, vel.w, acc.z, acc.w,
                        P.seis + (static_cast<size_t>(sh[2]) * P.max_sig + isig) * P.slots);
         } else {
-          const float us[4] = {uu.x, uu.y, uu.z, uu.w}, vs[4] = {vel.x, vel.y, vel.z, vel.w};
-          const float as[4] = {acc.x, acc.y, acc.z, acc.w};
+          const real us[4] = {uu.x, uu.y, uu.z, uu.w}, vs[4] = {vel.x, vel.y, vel.z, vel.w};
+          const real as[4] = {acc.x, acc.y, acc.z, acc.w};
 #pragma unroll
           for (int e = 0; e < 4; ++e)
             if (e < 2 || two)
-              apply_taps(M.taps, g[e], us[e], 0.f, vs[e], 0.f, as[e], 0.f,
+              apply_taps(M.taps, g[e], us[e], 0, vs[e], 0, as[e], 0,
                          P.seis + (static_cast<size_t>(sh[e]) * P.max_sig + isig) * P.slots);
         }
       }
@@ -1943,15 +2027,15 @@ __global__ void k_update_all(UpdateParams P) {
         vel.w += P.dt2 * acc.w;
       }
       // last step: a and v stored, u kept; otherwise u, v stored and a = 0
-      const float4 a_out = P.last ? acc : make_float4(0.f, 0.f, 0.f, 0.f);
+      const real4 a_out = P.last ? acc : mk4(0, 0, 0, 0);
       if (two) {
-        if (!P.last) reinterpret_cast<float4 *>(M.u)[p0 / 2] = uu;
-        reinterpret_cast<float4 *>(M.v)[p0 / 2] = vel;
-        reinterpret_cast<float4 *>(M.a)[p0 / 2] = a_out;
+        if (!P.last) reinterpret_cast<real4 *>(M.u)[p0 / 2] = uu;
+        reinterpret_cast<real4 *>(M.v)[p0 / 2] = vel;
+        reinterpret_cast<real4 *>(M.a)[p0 / 2] = a_out;
       } else {
-        if (!P.last) reinterpret_cast<float2 *>(M.u)[p0] = make_float2(uu.x, uu.y);
-        reinterpret_cast<float2 *>(M.v)[p0] = make_float2(vel.x, vel.y);
-        reinterpret_cast<float2 *>(M.a)[p0] = make_float2(a_out.x, a_out.y);
+        if (!P.last) reinterpret_cast<real2 *>(M.u)[p0] = mk2(uu.x, uu.y);
+        reinterpret_cast<real2 *>(M.v)[p0] = mk2(vel.x, vel.y);
+        reinterpret_cast<real2 *>(M.a)[p0] = mk2(a_out.x, a_out.y);
       }
     }
   } else
@@ -1964,47 +2048,47 @@ __global__ void k_update_all(UpdateParams P) {
     // pair jj holds (g, s) with both components (nc = 2), or the two
     // consecutive entries 2jj, 2jj + 1 of [g][s] (nc = 1)
     int g0, s0, g1, s1;
-    float2 m;
+    real2 m;
     const size_t at = jj;  // pair index in the field arrays
     if (M.nc == 2) {
       const uint32_t n = static_cast<uint32_t>(jj);
       g0 = g1 = static_cast<int>(P.sdiv.div(n));
       s0 = s1 = static_cast<int>(n - static_cast<uint32_t>(g0) * S);
-      m = reinterpret_cast<const float2 *>(M.minv)[g0];
+      m = reinterpret_cast<const real2 *>(M.minv)[g0];
     } else {
       const uint32_t n0 = static_cast<uint32_t>(2 * jj), n1 = n0 + 1;
       g0 = static_cast<int>(P.sdiv.div(n0));
       s0 = static_cast<int>(n0 - static_cast<uint32_t>(g0) * S);
       g1 = static_cast<int>(P.sdiv.div(n1));
       s1 = static_cast<int>(n1 - static_cast<uint32_t>(g1) * S);
-      m = make_float2(M.minv[g0], M.minv[g1]);
+      m = mk2(M.minv[g0], M.minv[g1]);
     }
-    float2 *U = reinterpret_cast<float2 *>(M.u);
-    float2 *Vv = reinterpret_cast<float2 *>(M.v);
-    float2 *A = reinterpret_cast<float2 *>(M.a);
-    const float2 r = A[at];
-    float2 acc, vel = Vv[at];
+    real2 *U = reinterpret_cast<real2 *>(M.u);
+    real2 *Vv = reinterpret_cast<real2 *>(M.v);
+    real2 *A = reinterpret_cast<real2 *>(M.a);
+    const real2 r = A[at];
+    real2 acc, vel = Vv[at];
     acc.x = r.x * m.x;
     acc.y = r.y * m.y;
-    float2 cu = make_float2(0.f, 0.f), cv = cu;
+    real2 cu = mk2(0, 0), cv = cu;
     if (EXTRA && M.cu) {
-      cu = reinterpret_cast<const float2 *>(M.cu)[at];
-      cv = reinterpret_cast<const float2 *>(M.cv)[at];
+      cu = reinterpret_cast<const real2 *>(M.cu)[at];
+      cv = reinterpret_cast<const real2 *>(M.cv)[at];
       vel.x = kahan_add(vel.x, cv.x, P.dt2 * acc.x);
       vel.y = kahan_add(vel.y, cv.y, P.dt2 * acc.y);
     } else {
       vel.x += P.dt2 * acc.x;  // corrector (newmark.tpp:44-47)
       vel.y += P.dt2 * acc.y;
     }
-    float2 uu = U[at];
+    real2 uu = U[at];
     if (record && M.taps.nsup > 0) {
       if (M.nc == 2) {
         apply_taps(M.taps, g0, uu.x, uu.y, vel.x, vel.y, acc.x, acc.y,
                    P.seis + (static_cast<size_t>(s0) * P.max_sig + isig) * P.slots);
       } else {
-        apply_taps(M.taps, g0, uu.x, 0.f, vel.x, 0.f, acc.x, 0.f,
+        apply_taps(M.taps, g0, uu.x, 0, vel.x, 0, acc.x, 0,
                    P.seis + (static_cast<size_t>(s0) * P.max_sig + isig) * P.slots);
-        apply_taps(M.taps, g1, uu.y, 0.f, vel.y, 0.f, acc.y, 0.f,
+        apply_taps(M.taps, g1, uu.y, 0, vel.y, 0, acc.y, 0,
                    P.seis + (static_cast<size_t>(s1) * P.max_sig + isig) * P.slots);
       }
     }
@@ -2018,8 +2102,8 @@ __global__ void k_update_all(UpdateParams P) {
       vel.y = kahan_add(vel.y, cv.y, P.dt2 * acc.y);
       U[at] = uu;
       Vv[at] = vel;
-      A[at] = make_float2(0.f, 0.f);
-      reinterpret_cast<float2 *>(M.cu)[at] = cu;
+      A[at] = mk2(0, 0);
+      reinterpret_cast<real2 *>(M.cu)[at] = cu;
     } else {
       uu.x += P.dt * vel.x + P.dtsq2 * acc.x;  // next predictor (newmark.tpp:98-105)
       uu.y += P.dt * vel.y + P.dtsq2 * acc.y;
@@ -2027,12 +2111,12 @@ __global__ void k_update_all(UpdateParams P) {
       vel.y += P.dt2 * acc.y;
       U[at] = uu;
       Vv[at] = vel;
-      A[at] = make_float2(0.f, 0.f);
+      A[at] = mk2(0, 0);
     }
     if constexpr (EXTRA) {
-      if (M.cu) reinterpret_cast<float2 *>(M.cv)[at] = cv;
-      if (M.ck_u && ck_uslot >= 0) reinterpret_cast<float2 *>(M.ck_u + ck_uslot * M.ck_stride)[at] = uu;
-      if (M.ck_u && ck_vslot >= 0) reinterpret_cast<float2 *>(M.ck_v + ck_vslot * M.ck_stride)[at] = vel;
+      if (M.cu) reinterpret_cast<real2 *>(M.cv)[at] = cv;
+      if (M.ck_u && ck_uslot >= 0) reinterpret_cast<real2 *>(M.ck_u + ck_uslot * M.ck_stride)[at] = uu;
+      if (M.ck_u && ck_vslot >= 0) reinterpret_cast<real2 *>(M.ck_v + ck_vslot * M.ck_stride)[at] = vel;
     }
   }
   if (P.ctrl) {
@@ -2062,11 +2146,11 @@ __global__ void k_update_all(UpdateParams P) {
 // ---------------------------------------------------------------------------
 template <int MED, int N, int EPB>
 __global__ void __launch_bounds__(EPB * N * N)
-k_frechet(Static st, MediumFields A, MediumFields B, int S, float dt, double *kern, int a_is_force) {
+k_frechet(Static st, MediumFields A, MediumFields B, int S, real dt, double *kern, int a_is_force) {
   constexpr int NC = (MED == MED_PSV) ? 2 : 1;
   constexpr int NN = N * N;
-  __shared__ float s_a[EPB][NC][NN];
-  __shared__ float s_b[EPB][NC][NN];
+  __shared__ real s_a[EPB][NC][NN];
+  __shared__ real s_b[EPB][NC][NN];
   const int t = threadIdx.x;
   const int el = t / NN, k = t % NN, iz = k / N, ix = k % N;
   const int li = blockIdx.x * EPB + el;
@@ -2074,22 +2158,22 @@ k_frechet(Static st, MediumFields A, MediumFields B, int S, float dt, double *ke
   const int e = A.elem_begin + (valid ? li : 0);
   const size_t p = static_cast<size_t>(e) * NN + k;
   const int g = valid ? st.iglob[p] : 0;
-  const float xix = st.xix[p], xiz = st.xiz[p], gax = st.gax[p], gaz = st.gaz[p];
-  const float m0 = st.mat0[p], m1 = st.mat1[p];
-  const float m2 = st.mat2 ? st.mat2[p] : 0.f;
+  const real xix = st.xix[p], xiz = st.xiz[p], gax = st.gax[p], gaz = st.gaz[p];
+  const real m0 = st.mat0[p], m1 = st.mat1[p];
+  const real m2 = st.mat2 ? st.mat2[p] : real(0);
   double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
   for (int s = 0; s < S; ++s) {
     const size_t base = (static_cast<size_t>(g) * S + s) * NC;
 #pragma unroll
     for (int c = 0; c < NC; ++c) {
-      s_a[el][c][k] = valid ? A.u[base + c] : 0.f;
-      s_b[el][c][k] = valid ? B.u[base + c] : 0.f;
+      s_a[el][c][k] = valid ? A.u[base + c] : real(0);
+      s_b[el][c][k] = valid ? B.u[base + c] : real(0);
     }
     __syncthreads();
-    float da[NC][2], db[NC][2];
+    real da[NC][2], db[NC][2];
 #pragma unroll
     for (int c = 0; c < NC; ++c) {
-      float axi = 0.f, aga = 0.f, bxi = 0.f, bga = 0.f;
+      real axi = 0, aga = 0, bxi = 0, bga = 0;
 #pragma unroll
       for (int l = 0; l < N; ++l) {
         axi += c_hp[ix * N + l] * s_a[el][c][iz * N + l];
@@ -2104,26 +2188,27 @@ k_frechet(Static st, MediumFields A, MediumFields B, int S, float dt, double *ke
     }
     if (valid) {
       if constexpr (MED == MED_PSV) {
-        const float l2m = m0 + static_cast<float>(4.0 / 3.0) * m1;
-        const float kappa = l2m - m1;
-        const float ad_dsxx = da[0][0], ad_dsxz = 0.5f * (da[1][0] + da[0][1]), ad_dszz = da[1][1];
-        const float b_dsxx = db[0][0], b_dsxz = 0.5f * (db[1][0] + db[0][1]), b_dszz = db[1][1];
-        float kappa_kl = (ad_dsxx + ad_dszz) * (b_dsxx + b_dszz);
-        float mu_kl = (ad_dsxx * b_dsxx + ad_dszz * b_dszz + 2.0f * ad_dsxz * b_dsxz -
-                       static_cast<float>(1.0 / 3.0) * kappa_kl);
-        const float ax = a_is_force ? A.a[base] * A.minv[static_cast<size_t>(g) * 2] : A.a[base];
-        const float az = a_is_force ? A.a[base + 1] * A.minv[static_cast<size_t>(g) * 2 + 1] : A.a[base + 1];
-        float rho_kl = ax * B.u[base] + az * B.u[base + 1];
-        kappa_kl = -1.0f * kappa * dt * kappa_kl;
-        mu_kl = -2.0f * m1 * dt * mu_kl;
-        rho_kl = -1.0f * m2 * dt * rho_kl;
+        const real l2m = m0 + kFourThirds * m1;
+        const real kappa = l2m - m1;
+        const real half = static_cast<real>(0.5);
+        const real ad_dsxx = da[0][0], ad_dsxz = half * (da[1][0] + da[0][1]), ad_dszz = da[1][1];
+        const real b_dsxx = db[0][0], b_dsxz = half * (db[1][0] + db[0][1]), b_dszz = db[1][1];
+        real kappa_kl = (ad_dsxx + ad_dszz) * (b_dsxx + b_dszz);
+        real mu_kl = (ad_dsxx * b_dsxx + ad_dszz * b_dszz + static_cast<real>(2) * ad_dsxz * b_dsxz -
+                      kOneThird * kappa_kl);
+        const real ax = a_is_force ? A.a[base] * A.minv[static_cast<size_t>(g) * 2] : A.a[base];
+        const real az = a_is_force ? A.a[base + 1] * A.minv[static_cast<size_t>(g) * 2 + 1] : A.a[base + 1];
+        real rho_kl = ax * B.u[base] + az * B.u[base + 1];
+        kappa_kl = static_cast<real>(-1) * kappa * dt * kappa_kl;
+        mu_kl = static_cast<real>(-2) * m1 * dt * mu_kl;
+        rho_kl = static_cast<real>(-1) * m2 * dt * rho_kl;
         acc0 += static_cast<double>(rho_kl);
         acc1 += static_cast<double>(mu_kl);
         acc2 += static_cast<double>(kappa_kl);
       } else {
-        const float rho_kl = (da[0][0] * db[0][0] + da[0][1] * db[0][1]) * m0 * dt;
-        const float chi_dd = a_is_force ? A.a[base] * A.minv[g] : A.a[base];
-        const float kappa_kl = chi_dd * B.u[base] * 1.0f / m1 * dt;
+        const real rho_kl = (da[0][0] * db[0][0] + da[0][1] * db[0][1]) * m0 * dt;
+        const real chi_dd = a_is_force ? A.a[base] * A.minv[g] : A.a[base];
+        const real kappa_kl = chi_dd * B.u[base] * static_cast<real>(1) / m1 * dt;
         acc0 += static_cast<double>(rho_kl);
         acc1 += static_cast<double>(kappa_kl);
         acc2 += static_cast<double>(rho_kl * kappa_kl);  // rhop per step (point/kernels.hpp:189-192)
@@ -2140,7 +2225,7 @@ k_frechet(Static st, MediumFields A, MediumFields B, int S, float dt, double *ke
 
 // Mass matrix (compute_mass_matrix.tpp:80-113) accumulated in FP64.
 template <int MED>
-__global__ void k_mass(Static st, MediumFields f, int N, float dt) {
+__global__ void k_mass(Static st, MediumFields f, int N, real dt) {
   constexpr int NC = (MED == MED_PSV) ? 2 : 1;
   const size_t nn = static_cast<size_t>(N) * N;
   const size_t total = static_cast<size_t>(f.nelem) * nn;
@@ -2150,15 +2235,16 @@ __global__ void k_mass(Static st, MediumFields f, int N, float dt) {
     const int k = static_cast<int>(t % nn);
     const int iz = k / N, ix = k % N;
     const size_t p = static_cast<size_t>(e) * nn + k;
-    float base;
-    if (MED == MED_PSV) base = st.mat2[p];        // rho
-    else if (MED == MED_SH) base = st.mat1[p];    // rho
-    else base = 1.0f / st.mat1[p];                // 1 / kappa
-    float mm[2];
+    real base;
+    if (MED == MED_PSV) base = st.mat2[p];                    // rho
+    else if (MED == MED_SH) base = st.mat1[p];                // rho
+    else base = static_cast<real>(1) / st.mat1[p];            // 1 / kappa
+    real mm[2];
     for (int c = 0; c < NC; ++c) mm[c] = base * (c_w[ix] * c_w[iz] * st.jac[p]);
     if (st.bnd[p] & 1) {
-      const float vf[2] = {-1.0f * dt * 0.5f, -1.0f * dt * 0.5f};
-      stacey<MED>(st.mat0[p], st.mat1[p], st.mat2 ? st.mat2[p] : 0.f, st.bnd_nx[p], st.bnd_nz[p],
+      const real hv = static_cast<real>(-1) * dt * static_cast<real>(0.5);
+      const real vf[2] = {hv, hv};
+      stacey<MED>(st.mat0[p], st.mat1[p], st.mat2 ? st.mat2[p] : real(0), st.bnd_nx[p], st.bnd_nz[p],
                   st.bnd_w[p], vf, mm);
     }
     const int g = st.iglob[p];
@@ -2166,16 +2252,16 @@ __global__ void k_mass(Static st, MediumFields f, int N, float dt) {
   }
 }
 
-__global__ void k_invert(const double *mass, float *minv, size_t n) {
+__global__ void k_invert(const double *mass, real *minv, size_t n) {
   for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<size_t>(gridDim.x) * blockDim.x)
-    minv[i] = static_cast<float>(1.0 / mass[i]);
+    minv[i] = static_cast<real>(1.0 / mass[i]);
 }
 
-__global__ void k_zero(float *p, size_t n) {
+__global__ void k_zero(real *p, size_t n) {
   for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<size_t>(gridDim.x) * blockDim.x)
-    p[i] = 0.f;
+    p[i] = 0;
 }
 
 int grid_for(size_t n, int block) {
@@ -2191,20 +2277,30 @@ size_t field_ld(const MediumFields &f) { return static_cast<size_t>(f.nglob + (f
 }  // namespace
 
 void init_kernel_attributes() {
+#ifndef SFB_FP64
   cudaFuncSetAttribute(k_stiffness_pk<MED_PSV, 5, 3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        static_cast<int>(kFrechetDynSmem));
   cudaFuncSetAttribute(k_stiffness_pk<MED_PSV, 5, 3, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        static_cast<int>(kFrechetDynSmem));
+#endif
 }
 
 bool frechet_fusable(int medium, int ngll, int nshots) {
+#ifdef SFB_FP64
+  (void)medium;
+  (void)ngll;
+  (void)nshots;
+  return false;  // the fused Frechet launch is the packed FP32 kernel
+#else
   return medium == MED_PSV && ngll == 5 && nshots > 1 && nshots % 2 == 0;
+#endif
 }
 
 void launch_stiffness_frechet(int ngll, const Static &st, const MediumFields &f, int S, const StaceyStore &ss,
                               const int *istep_dev, const TailWork &tw, const FrechetFuse &fr,
                               const FusedUpdate &fu, cudaStream_t stream) {
   if (f.nelem == 0 || !frechet_fusable(MED_PSV, ngll, S)) return;
+#ifndef SFB_FP64
   dim3 grid(f.nelem, (S / 2 + 31) / 32);
   if (st.affine[MED_PSV] && st.pack_aff)
     launch_step_kernel(k_stiffness_pk<MED_PSV, 5, 3, true, true>, grid, 5 * 32, kFrechetDynSmem, stream, st, f, S, ss,
@@ -2212,6 +2308,15 @@ void launch_stiffness_frechet(int ngll, const Static &st, const MediumFields &f,
   else
     launch_step_kernel(k_stiffness_pk<MED_PSV, 5, 3, true>, grid, 5 * 32, kFrechetDynSmem, stream, st, f, S, ss,
                        istep_dev, tw, fu, fr);
+#else
+  (void)st;
+  (void)ss;
+  (void)istep_dev;
+  (void)tw;
+  (void)fr;
+  (void)fu;
+  (void)stream;
+#endif
 }
 
 void launch_stiffness(int medium, int ngll, const Static &st, const MediumFields &f, int nshots,
@@ -2223,6 +2328,20 @@ void launch_stiffness(int medium, int ngll, const Static &st, const MediumFields
   const FusedUpdate nofu{};
   // the in-launch update of private points exists for the P-SV kernels
   const FusedUpdate &u = (fu && medium == MED_PSV) ? *fu : nofu;
+#ifdef SFB_FP64
+  // FP64 build: the scalar shot-parallel kernel for every shot count
+  (void)variant;
+  if (ngll == 5) {
+    if (medium == MED_PSV) launch_shots<MED_PSV, 5, 1>(st, f, nshots, ss, istep_dev, w, u, kShotsSingle, stream);
+    else if (medium == MED_SH) launch_shots<MED_SH, 5, 1>(st, f, nshots, ss, istep_dev, w, nofu, kShotsSingle, stream);
+    else launch_shots<MED_AC, 5, 1>(st, f, nshots, ss, istep_dev, w, nofu, kShotsSingle, stream);
+  } else if (ngll == 8) {
+    if (medium == MED_PSV) launch_shots<MED_PSV, 8, 1>(st, f, nshots, ss, istep_dev, w, u, kShotsSingle, stream);
+    else if (medium == MED_SH) launch_shots<MED_SH, 8, 1>(st, f, nshots, ss, istep_dev, w, nofu, kShotsSingle, stream);
+    else launch_shots<MED_AC, 8, 1>(st, f, nshots, ss, istep_dev, w, nofu, kShotsSingle, stream);
+  }
+  return;
+#else
   if (nshots > 1) {
     if (ngll == 5) {
       if (medium == MED_PSV) launch_shots<MED_PSV, 5, 4>(st, f, nshots, ss, istep_dev, w, u, variant, stream);
@@ -2257,6 +2376,7 @@ void launch_stiffness(int medium, int ngll, const Static &st, const MediumFields
     else if (medium == MED_SH) launch_rp<MED_SH, 8, 16, 2>(st, f, nshots, ss, istep_dev, w, nofu, stream);
     else launch_rp<MED_AC, 8, 16, 2>(st, f, nshots, ss, istep_dev, w, nofu, stream);
   }
+#endif
 }
 
 void launch_sources(int ngll, const Static &st, const SourceSet &src, MediumFields *fields,
@@ -2282,20 +2402,20 @@ void launch_coupling_elastic(const CouplingSet &c, const MediumFields &el, const
 }
 
 void launch_receivers(int ngll, const Static &st, const ReceiverSet &rec, const MediumFields *fields,
-                      int nshots, float dt2, int mode, const int *istep_dev, cudaStream_t stream) {
+                      int nshots, real dt2, int mode, const int *istep_dev, cudaStream_t stream) {
   if (rec.n == 0 || rec.ntypes == 0) return;
   dim3 grid(rec.n, nshots);
   k_receivers<<<grid, 64, 0, stream>>>(st, rec, fields[MED_PSV], fields[MED_SH], fields[MED_AC], ngll,
                                        dt2, mode, istep_dev, nshots);
 }
 
-void launch_predictor(const MediumFields &f, int nshots, float dt, float dt2, float dtsq2,
-                      cudaStream_t stream, float *cu, float *cv) {
+void launch_predictor(const MediumFields &f, int nshots, real dt, real dt2, real dtsq2,
+                      cudaStream_t stream, real *cu, real *cv) {
   const size_t n = field_ld(f) * nshots;
   if (n == 0) return;
   k_predictor<<<grid_for(n, 256), 256, 0, stream>>>(f.u, f.v, f.a, n, dt, dt2, dtsq2, cu, cv);
 }
-void launch_corrector(const MediumFields &f, int nshots, float dt2, cudaStream_t stream) {
+void launch_corrector(const MediumFields &f, int nshots, real dt2, cudaStream_t stream) {
   const size_t n = field_ld(f) * nshots;
   if (n == 0) return;
   k_corrector<<<grid_for(n, 256), 256, 0, stream>>>(f.v, f.a, n, dt2);
@@ -2346,7 +2466,7 @@ void launch_update_all(const UpdateParams &p, cudaStream_t stream) {
 }
 
 
-void launch_mass(int medium, int ngll, const Static &st, const MediumFields &f, float dt,
+void launch_mass(int medium, int ngll, const Static &st, const MediumFields &f, real dt,
                  cudaStream_t stream) {
   if (f.nelem == 0) return;
   const size_t n = static_cast<size_t>(f.nelem) * ngll * ngll;
@@ -2361,7 +2481,7 @@ void launch_invert_mass(const MediumFields &f, cudaStream_t stream) {
   k_invert<<<grid_for(n, 256), 256, 0, stream>>>(f.mass, f.minv, n);
 }
 void launch_frechet(int medium, int ngll, const Static &st, const MediumFields &adj, const MediumFields &bwd,
-                    int nshots, float dt, double *kern, int a_is_force, cudaStream_t stream) {
+                    int nshots, real dt, double *kern, int a_is_force, cudaStream_t stream) {
   if (adj.nelem == 0) return;
   if (ngll == 5) {
     constexpr int EPB = 8;
@@ -2376,7 +2496,7 @@ void launch_frechet(int medium, int ngll, const Static &st, const MediumFields &
   }
 }
 
-void launch_zero(float *p, size_t n, cudaStream_t stream) {
+void launch_zero(real *p, size_t n, cudaStream_t stream) {
   if (n == 0) return;
   k_zero<<<grid_for(n, 256), 256, 0, stream>>>(p, n);
 }

@@ -2,14 +2,14 @@
 //
 // Layout in HBM (device element order = elements sorted by medium, boundary
 // elements last within a medium, so each medium is one contiguous range):
-//   per local point p = (e * N + iz) * N + ix, SoA float arrays:
+//   per local point p = (e * N + iz) * N + ix, SoA arrays of `real` (FP32):
 //     iglob[p]                        index in the medium's field
 //     xix, xiz, gammax, gammaz, jac   geometry
 //     mat0, mat1, mat2                P-SV: kappa, mu, rho
 //                                     SH:   mu, rho, -
 //                                     acoustic: rho_inverse, kappa, -
-//   fields, point-major and shot-minor: value (g, s) at g * S + s, as float2
-//   (P-SV) or float (SH, acoustic); the inverse mass has no shot index.
+//   fields, point-major and shot-minor: value (g, s) at g * S + s, as a pair
+//   (P-SV) or a scalar (SH, acoustic); the inverse mass has no shot index.
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -17,19 +17,38 @@
 namespace sfb {
 namespace dev {
 
+// Arithmetic type of the wavefields, geometry, material and every per-step
+// quantity.  The product library is built with FP32 (the reference's
+// type_real).  The verification library (SFB_FP64) compiles the same
+// generic kernels -- the scalar batched stiffness, sources, coupling,
+// receivers, Newmark pieces, the fused update, Frechet kernels and the mass
+// matrix -- in FP64, so that the device path can be compared with the FP64
+// oracle at FP64 rounding level; the FP32-specific kernels (bulk-copy fed
+// row kernels, compact block, packed f32x2) are left out of that build.
+#ifdef SFB_FP64
+typedef double real;
+typedef double2 real2;
+typedef double4 real4;
+#else
+typedef float real;
+typedef float2 real2;
+typedef float4 real4;
+#endif
+
 enum { MED_PSV = 0, MED_SH = 1, MED_AC = 3 };
 
 struct Static {
   int ngll, nspec;
   const int *iglob;
-  const float *xix, *xiz, *gax, *gaz, *jac;
-  const float *mat0, *mat1, *mat2;
+  const real *xix, *xiz, *gax, *gaz, *jac;
+  const real *mat0, *mat1, *mat2;
   const uint8_t *eflag;  // per device element: bit0 Stacey points, bit1 free-surface points
   const uint8_t *bnd;    // per local point
-  const float *bnd_nx, *bnd_nz, *bnd_w;
+  const real *bnd_nx, *bnd_nz, *bnd_w;
   // Packed per-element block for the TMA-fed stiffness kernel:
-  // pack[e][8][N*N] = iglob (int bits), xix, xiz, gammax, gammaz, jac, mat0, mat1.
-  const float *pack;
+  // pack[e][8][N*N] = iglob (int bits; FP64 build: the index as a value),
+  // xix, xiz, gammax, gammaz, jac, mat0, mat1.
+  const real *pack;
   // Compact block of affine elements (constant Jacobian matrix, e.g. the
   // parallelograms of a structured mesh), single-shot contexts only, in
   // chunks of kAffineChunk elements of one medium (affine_chunk_words(N)
@@ -48,8 +67,8 @@ struct MediumFields {
   int nc;       // components
   int elem_begin, nelem;      // device element range
   int nelem_interior;         // elements [elem_begin, elem_begin+nelem_interior) have no boundary points
-  float *u, *v, *a;           // [nglob + nglob % 2][S][nc]
-  float *minv;                // [nglob*nc]
+  real *u, *v, *a;            // [nglob + nglob % 2][S][nc]
+  real *minv;                 // [nglob*nc]
   double *mass;               // scratch for initialize, [nglob*nc]
 };
 
@@ -62,32 +81,32 @@ struct SourceSet {
   const int *elem;       // device element
   const int *shot;
   const int *medium;
-  const float *array;    // [n][2][N*N]
-  const float *stf;      // [n][nstep][2]
+  const real *array;     // [n][2][N*N]
+  const real *stf;       // [n][nstep][2]
   int nstep;
 };
 
 struct ReceiverSet {
   int n;
   const int *elem;       // device element
-  const float *lagrange; // [n][N*N]
-  const float *sinv, *cosv;
+  const real *lagrange;  // [n][N*N]
+  const real *sinv, *cosv;
   int ntypes;
   int types[5];
   int max_sig, nsbs;
-  float *seis;           // [S][max_sig][ntypes][n][2]
+  real *seis;            // [S][max_sig][ntypes][n][2]
 };
 
 struct CouplingSet {
   int n;
   const int *self, *other;
-  const float *factor, *nx, *nz;
+  const real *factor, *nx, *nz;
 };
 
 // Stacey replay / store (adjoint reconstruction): element-local
 // accelerations of the Stacey elements, [S][nstep][nstacey][N*N][2].
 struct StaceyStore {
-  float *data;
+  real *data;
   const int *slot;   // per device element: slot index or -1
   int nstacey;
   int nstep;
@@ -122,7 +141,7 @@ struct ReceiverTaps {
   const int *sup_g, *sup_begin;
   const int *slot;    // (type * nrec + rec) * 2 + out component
   const int *which;   // field (0 u, 1 v, 2 a) * 2 + input component
-  const float *w;
+  const real *w;
 };
 
 // Unsigned 32-bit division by a runtime constant as multiply-high + shift
@@ -145,17 +164,17 @@ struct FastDiv {
 };
 
 struct UpdateMedium {
-  float *u, *v, *a;
-  const float *minv;
-  size_t ld2;    // float2 pairs of the whole [g][s][c] array
+  real *u, *v, *a;
+  const real *minv;
+  size_t ld2;    // pairs of values of the whole [g][s][c] array
   int nc;        // components per point (1: a pair holds two entries)
   ReceiverTaps taps;
-  float *cu, *cv;   // Kahan compensation terms of u and v (same layout), or null
+  real *cu, *cv;    // Kahan compensation terms of u and v (same layout), or null
   // forward snapshots for the combined run: slot c (c = 0 .. count-1) holds
   // u at step (c+1)K (written by step (c+1)K - 1) and v half a step later
   // (written by step (c+1)K); null when off
-  float *ck_u, *ck_v;
-  size_t ck_stride;  // floats per slot
+  real *ck_u, *ck_v;
+  size_t ck_stride;  // values per slot
 };
 
 // Newmark update of element-private points inside the stiffness launch.  A
@@ -167,9 +186,9 @@ struct UpdateMedium {
 // every shared point of the P-SV field, which the update kernel covers.
 struct FusedUpdate {
   int enabled;
-  const float *minv;   // [nglob][nc]
-  float *v;            // [g][S][nc]
-  float dt, dt2, dtsq2;
+  const real *minv;    // [nglob][nc]
+  real *v;             // [g][S][nc]
+  real dt, dt2, dtsq2;
   int last;            // 1: finish the step (store a and v, no predictor)
 };
 constexpr uint8_t kElemPrivate = 4;
@@ -181,16 +200,16 @@ constexpr uint8_t kElemPrivate = 4;
 // kernels, summed over the launch's shots, to kern[p][3] (FP64).
 struct FrechetFuse {
   int enabled;
-  float *au;           // adjoint displacement [g][S][2]
-  float *aa;           // adjoint force [g][S][2] (times minv = acceleration)
-  const float *minv;   // [nglob][2]
+  real *au;            // adjoint displacement [g][S][2]
+  real *aa;            // adjoint force [g][S][2] (times minv = acceleration)
+  const real *minv;   // [nglob][2]
   double *kern;        // [nspec * N * N][3]: rho, mu, kappa
-  float dt;
+  real dt;
   // the adjoint wavefield's element-private points also finish their (+dt)
   // Newmark step here, after their Frechet contribution is taken
   int adjoint_update;
-  float *av;           // adjoint velocity [g][S][2]
-  float adt, adt2, adtsq2;
+  real *av;            // adjoint velocity [g][S][2]
+  real adt, adt2, adtsq2;
   int last;
 };
 
@@ -200,12 +219,12 @@ struct UpdateParams {
   size_t begin[4];  // pair ranges of the media in the flat index space
   int nshots;
   FastDiv sdiv;           // division by nshots
-  float dt, dt2, dtsq2;
+  real dt, dt2, dtsq2;
   int last;               // 1: finish the step (no predictor for the next one)
   Control *ctrl;          // step counter, advanced by the last CTA to finish
   int dir;                // +1 forward in time, -1 for the combined (reversed) loop
   unsigned *done;         // CTA completion counter (zero between launches)
-  float *seis;            // [S][max_sig][slots]
+  real *seis;             // [S][max_sig][slots]
   int slots, max_sig, nsbs;
   int ck_interval, ck_count;  // snapshot cadence K and slots (0: none)
 };
@@ -213,9 +232,9 @@ struct UpdateParams {
 // Restore the backward wavefield of the combined run from the forward
 // snapshots when the step counter reaches a snapshot step (see UpdateMedium).
 struct RestoreParams {
-  float *u[3], *v[3];
-  const float *ck_u[3], *ck_v[3];
-  size_t n[3];        // floats per medium field ([g][S][nc] incl. padding)
+  real *u[3], *v[3];
+  const real *ck_u[3], *ck_v[3];
+  size_t n[3];        // values per medium field ([g][S][nc] incl. padding)
   size_t ck_stride[3];
   int nm;
   const Control *ctrl;
@@ -224,7 +243,7 @@ struct RestoreParams {
 void launch_restore(const RestoreParams &p, cudaStream_t stream);
 
 // ---- launchers (kernels.cu) ----
-void set_quadrature(int ngll, const float *hprime, const float *wgll);
+void set_quadrature(int ngll, const real *hprime, const real *wgll);
 
 // `tw` (may be null) is executed in the same launch.  One shot: the
 // TMA-fed row kernel; several shots: the shot-parallel kernel.
@@ -269,27 +288,27 @@ void launch_coupling_elastic(const CouplingSet &c, const MediumFields &el,
 // (u, v, a).  mode 1: fused loop, fields hold (u, v*, force) and the final
 // velocity/acceleration are formed on the fly.
 void launch_receivers(int ngll, const Static &st, const ReceiverSet &rec,
-                      const MediumFields *fields, int nshots, float dt2, int mode,
+                      const MediumFields *fields, int nshots, real dt2, int mode,
                       const int *istep_dev, cudaStream_t stream);
 // Newmark pieces (unfused API) and fused update.
 // cu, cv: Kahan compensation terms of u and v, or null for the plain update.
-void launch_predictor(const MediumFields &f, int nshots, float dt, float dt2, float dtsq2,
-                      cudaStream_t stream, float *cu = nullptr, float *cv = nullptr);
-void launch_corrector(const MediumFields &f, int nshots, float dt2, cudaStream_t stream);
+void launch_predictor(const MediumFields &f, int nshots, real dt, real dt2, real dtsq2,
+                      cudaStream_t stream, real *cu = nullptr, real *cv = nullptr);
+void launch_corrector(const MediumFields &f, int nshots, real dt2, cudaStream_t stream);
 void launch_divide(const MediumFields &f, int nshots, cudaStream_t stream);
 void launch_advance_step(Control *ctrl, cudaStream_t stream);
 // Fused divide + corrector (+ predictor of the next step) for every medium in
 // one launch, with the seismogram taps.
 void launch_update_all(const UpdateParams &p, cudaStream_t stream);
-void launch_mass(int medium, int ngll, const Static &st, const MediumFields &f, float dt,
+void launch_mass(int medium, int ngll, const Static &st, const MediumFields &f, real dt,
                  cudaStream_t stream);
 void launch_invert_mass(const MediumFields &f, cudaStream_t stream);
-void launch_zero(float *p, size_t n, cudaStream_t stream);
+void launch_zero(real *p, size_t n, cudaStream_t stream);
 // Frechet kernel accumulation for one medium (P-SV or acoustic) into
 // kern[p][3] (FP64, device element order).  a_is_force: the adjoint `a`
 // array holds the unassembled force of the fused loop (multiply by M^-1).
 void launch_frechet(int medium, int ngll, const Static &st, const MediumFields &adj, const MediumFields &bwd,
-                    int nshots, float dt, double *kern, int a_is_force, cudaStream_t stream);
+                    int nshots, real dt, double *kern, int a_is_force, cudaStream_t stream);
 
 }  // namespace dev
 }  // namespace sfb

@@ -79,26 +79,32 @@ def _fptr(a: np.ndarray):
 
 
 class Simulation:
-    """A simulation context (device buffers are created on first GPU use)."""
+    """A simulation context (device buffers are created on first GPU use).
 
-    def __init__(self, handle):
+    ``precision`` 32 (default) is the product library; 64 binds the FP64
+    verification build of the same kernels, for parity tests against the
+    FP64 oracle."""
+
+    def __init__(self, handle, precision: int = 32):
         self._h = handle
-        self._lib = A.load()
+        self.precision = precision
+        self._lib = A.load(precision)
         self._keep = []
 
     # ---- construction ---------------------------------------------------
     @classmethod
-    def from_yaml(cls, parameter_file: str, default_file: Optional[str] = None) -> "Simulation":
-        lib = A.load()
+    def from_yaml(cls, parameter_file: str, default_file: Optional[str] = None,
+                  precision: int = 32) -> "Simulation":
+        lib = A.load(precision)
         h = C.c_void_p()
         rc = lib.sfb_create_from_yaml(parameter_file.encode(),
                                       default_file.encode() if default_file else None, C.byref(h))
-        A.check(rc, None)
-        return cls(h)
+        A.check(rc, None, lib)
+        return cls(h, precision)
 
     @classmethod
-    def structured(cls, p: StructuredProblem) -> "Simulation":
-        lib = A.load()
+    def structured(cls, p: StructuredProblem, precision: int = 32) -> "Simulation":
+        lib = A.load(precision)
         keep = []
         d = A.sfb_structured_desc()
         d.nx, d.nz = p.nx, p.nz
@@ -153,8 +159,8 @@ class Simulation:
         d.simulation = p.simulation
         d.save_boundary_values = 1 if p.save_boundary_values else 0
         h = C.c_void_p()
-        A.check(lib.sfb_create_structured(C.byref(d), C.byref(h)), None)
-        return cls(h)
+        A.check(lib.sfb_create_structured(C.byref(d), C.byref(h)), None, lib)
+        return cls(h, precision)
 
     def close(self):
         if self._h:
@@ -178,7 +184,7 @@ class Simulation:
         return self._h
 
     def _check(self, rc):
-        return A.check(rc, self._h)
+        return A.check(rc, self._h, self._lib)
 
     # ---- info / view ----------------------------------------------------
     def info(self) -> A.sfb_info:
@@ -213,14 +219,29 @@ class Simulation:
         self._check(self._lib.sfb_domain_compute_seismograms(self._h, wavefield, isig_step))
 
     def seismograms(self, wavefield: int = 0, shot: int = 0) -> np.ndarray:
+        """[max_sig_step][ntypes][nreceivers][2]; float32, or float64 (every
+        bit the device computed) for an FP64 context."""
         i = self.info()
-        out = np.zeros((i.max_sig_step, i.nseismogram_types, i.nreceivers, 2), dtype=np.float32)
+        shape = (i.max_sig_step, i.nseismogram_types, i.nreceivers, 2)
+        if self.precision == 64:
+            out = np.zeros(shape, dtype=np.float64)
+            self._check(self._lib.sfb_get_seismograms_f64(self._h, wavefield, shot,
+                                                          out.ctypes.data_as(C.POINTER(C.c_double)), out.size))
+            return out
+        out = np.zeros(shape, dtype=np.float32)
         self._check(self._lib.sfb_get_seismograms(self._h, wavefield, shot, _fptr(out), out.size))
         return out
 
     def field(self, medium: int, which: int, wavefield: int = 0, shot: int = 0) -> np.ndarray:
+        """[ncomp][nglob] of u, v, a (which 0-2) or the inverse mass (3);
+        float32, or float64 for an FP64 context."""
         i = self.info()
         nc = 2 if medium == A.MEDIUM_ELASTIC_PSV else 1
+        if self.precision == 64:
+            out = np.zeros((nc, i.nglob[medium]), dtype=np.float64)
+            self._check(self._lib.sfb_get_field_f64(self._h, wavefield, medium, which, shot,
+                                                    out.ctypes.data_as(C.POINTER(C.c_double)), out.size))
+            return out
         out = np.zeros((nc, i.nglob[medium]), dtype=np.float32)
         self._check(self._lib.sfb_get_field(self._h, wavefield, medium, which, shot, _fptr(out), out.size))
         return out

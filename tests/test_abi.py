@@ -36,3 +36,14 @@ def test_errors_are_reported_not_thrown(native_lib):
         Simulation.from_yaml("/nonexistent/specfem_config.yaml")
     assert e.value.code == -3  # SFB_E_IO
     assert "open" in str(e.value)
+
+
+def test_fp64_verification_build_exports_the_same_abi(native_lib):
+    """The FP64 verification build exports every entry point except the
+    FP32-only allocation-free one, and reports its arithmetic width."""
+    from specfempp_b200 import _capi
+    lib = ctypes.CDLL(_capi.LIB64_PATH)
+    missing = [s for s in declared_symbols() if s not in _capi.FP32_ONLY and not hasattr(lib, s)]
+    assert not missing, missing
+    assert _capi.load(64).sfb_real_bytes() == 8
+    assert _capi.load(32).sfb_real_bytes() == 4
