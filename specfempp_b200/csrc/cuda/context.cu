@@ -657,6 +657,8 @@ void build_taps(sfb_context *c) {
   const int ntypes = static_cast<int>(P.seismogram_types.size());
   struct E { int g, slot, which; double w; };
   std::vector<E> ent[4];
+  // the derivative table as the kernels and the reference hold it (FP32)
+  auto hp32 = [&](int i) { return static_cast<double>(static_cast<float>(a.quad.hprime[i])); };
   for (int r = 0; r < nrec; ++r) {
     const LocatedReceiver &L = P.located_receivers[r];
     const int e = L.ispec, m = a.medium[e];
@@ -682,7 +684,7 @@ void build_taps(sfb_context *c) {
           const double l2m = a.kappa[p] + static_cast<double>(static_cast<float>(4.0 / 3.0)) * a.mu[p];
           const double cf = -((l2m - 2.0 * a.mu[p]) + (2.0 / 3.0) * a.mu[p]) * h;
           for (int l = 0; l < n; ++l) {
-            const double hx = a.quad.hprime[kx * n + l], hz = a.quad.hprime[kz * n + l];
+            const double hx = hp32(kx * n + l), hz = hp32(kz * n + l);
             add(kz * n + l, 0, cf * a.xix[p] * hx, 0.0);
             add(l * n + kx, 0, cf * a.gammax[p] * hz, 0.0);
             add(kz * n + l, 1, cf * a.xiz[p] * hx, 0.0);
@@ -694,7 +696,7 @@ void build_taps(sfb_context *c) {
         } else if (m == MEDIUM_ACOUSTIC) {
           const double ri = a.rho_inverse[p];
           for (int l = 0; l < n; ++l) {
-            const double hx = a.quad.hprime[kx * n + l], hz = a.quad.hprime[kz * n + l];
+            const double hx = hp32(kx * n + l), hz = hp32(kz * n + l);
             add(kz * n + l, 0, h * ri * a.xix[p] * hx, h * ri * a.xiz[p] * hx);
             add(l * n + kx, 0, h * ri * a.gammax[p] * hz, h * ri * a.gammaz[p] * hz);
           }
@@ -788,6 +790,7 @@ dev::UpdateParams update_params(sfb_context *c, WavefieldSet &W, int last, bool 
   u.slots = static_cast<int>(P.seismogram_types.size() * P.receivers.size() * 2);
   u.max_sig = P.max_sig_step();
   u.nsbs = P.nstep_between_samples;
+  u.nstep = P.nstep;
   if (snapshots && c->ck_count > 0) {
     u.ck_interval = c->ck_interval;
     u.ck_count = c->ck_count;
@@ -1254,15 +1257,18 @@ void run_combined_fused(sfb_context *c, int use_graph) {
     for (int m : kMedia)
       dev::launch_predictor(B.f[m], P.nshots, static_cast<real>(-P.dt), static_cast<real>(-P.dt / 2.0),
                             static_cast<real>(P.dt * P.dt / 2.0), c->stream);
-    // backward seismogram of step N-1 is the forward run's last sample
+    // the backward seismogram of step N-1 is the forward run's last sample;
+    // it is the backward run's first sample (backward samples are numbered
+    // in loop order, time_marching.tpp:208-212)
     const int nsbs = P.nstep_between_samples;
-    if ((N - 1) % nsbs == 0 && (N - 1) / nsbs < P.max_sig_step()) {
+    if ((N - 1) % nsbs == 0 && (N - 1) / nsbs < P.max_sig_step() && P.max_sig_step() > 0) {
       const size_t slots = P.seismogram_types.size() * P.receivers.size() * 2;
       const size_t isig = static_cast<size_t>((N - 1) / nsbs);
       for (int s = 0; s < P.nshots; ++s) {
-        const size_t off = (static_cast<size_t>(s) * P.max_sig_step() + isig) * slots;
+        const size_t src = (static_cast<size_t>(s) * P.max_sig_step() + isig) * slots;
+        const size_t dst = static_cast<size_t>(s) * P.max_sig_step() * slots;
         if (slots)
-          ck(cudaMemcpyAsync(B.seis.p + off, F.seis.p + off, slots * sizeof(real), cudaMemcpyDeviceToDevice,
+          ck(cudaMemcpyAsync(B.seis.p + dst, F.seis.p + src, slots * sizeof(real), cudaMemcpyDeviceToDevice,
                              c->stream),
              "seismograms");
       }

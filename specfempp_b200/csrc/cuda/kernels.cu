@@ -1926,8 +1926,13 @@ template <bool EXTRA>
 __global__ void k_update_all(UpdateParams P) {
   grid_dep_wait();
   const int istep = P.ctrl ? P.ctrl->istep : -1;
-  const bool record = P.seis != nullptr && istep >= 0 && (istep % P.nsbs) == 0 && (istep / P.nsbs) < P.max_sig;
-  const int isig = record ? istep / P.nsbs : 0;
+  // Sample index: istep / nsbs forward; in the backward run of the combined
+  // loop (dir -1) samples are numbered in the order the loop reaches them,
+  // from step nstep - 1 down (time_marching.tpp:208-212, the seismogram
+  // step counter of the time scheme).
+  const int isig_raw = P.dir < 0 ? (P.nstep - 1) / P.nsbs - istep / P.nsbs : istep / P.nsbs;
+  const bool record = P.seis != nullptr && istep >= 0 && (istep % P.nsbs) == 0 && isig_raw < P.max_sig;
+  const int isig = record ? isig_raw : 0;
   const size_t total = P.begin[P.nm];
   const int S = P.nshots;
   // snapshot slots this step writes (forward run with checkpoints)

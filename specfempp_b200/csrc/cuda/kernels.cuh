@@ -226,6 +226,7 @@ struct UpdateParams {
   unsigned *done;         // CTA completion counter (zero between launches)
   real *seis;             // [S][max_sig][slots]
   int slots, max_sig, nsbs;
+  int nstep;              // steps of the run (numbering of the backward samples)
   int ck_interval, ck_count;  // snapshot cadence K and slots (0: none)
 };
 

@@ -42,3 +42,25 @@ def station_errors(case, traces, stations, types, seis, times):
                 norm += np.abs(tr[:n, 1]).sum()
         errs.append(err / norm)
     return np.array(errs)
+
+
+FIXTURES = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "newmark")
+
+
+def fixture_case(case, workdir):
+    """Unpack the committed fixture of `case` (tests/golden/newmark/<case>,
+    made by tests/golden/make_newmark_fixtures.py) into `workdir`; returns
+    the parameter file, a trace loader (name -> (n, 2) array) and the
+    (network, station) pairs of its STATIONS file."""
+    import gzip
+    import shutil
+    src = os.path.join(FIXTURES, case)
+    for name in ("specfem_config.yaml", "sources.yaml", "STATIONS"):
+        shutil.copy(os.path.join(src, name), os.path.join(workdir, name))
+    with gzip.open(os.path.join(src, "database.bin.gz"), "rb") as f:
+        data = f.read()
+    with open(os.path.join(workdir, "database.bin"), "wb") as f:
+        f.write(data)
+    traces = np.load(os.path.join(src, "traces.npz"))
+    stations = [tuple(l.split()[:2][::-1]) for l in open(os.path.join(src, "STATIONS")) if l.strip()]
+    return os.path.join(workdir, "specfem_config.yaml"), (lambda n: traces[n].astype(np.float64)), stations
