@@ -160,6 +160,20 @@ SFB_API int sfb_get_info(const sfb_context *ctx, sfb_info *info);
  * (the reference's chunk size is a compile-time constant). */
 SFB_API int sfb_set_stiffness_variant(sfb_context *ctx, int medium, int variant);
 
+/* Deterministic assembly (no reference counterpart; the reference scatters
+ * with Kokkos::atomic_add, include/compute/fields/data_access.tpp:683-720,
+ * whose summation order changes from run to run).  enable = 1: the
+ * elements of each medium are coloured so that no two elements of a colour
+ * share a point and each colour is its own stiffness launch, point sources
+ * and coupling are summed per target point in a fixed order, seismograms
+ * come from the receiver kernel's fixed-order sums and the mass matrix is
+ * accumulated colour by colour: the same inputs give bit-identical fields,
+ * seismograms and kernels on every run (on the same GPU and build).  The
+ * compact block of affine elements is not used in this mode.  Call before
+ * the context's first device use; SFB_E_STATE afterwards.  New contexts
+ * start in this mode when the environment sets SFB_DETERMINISTIC=1. */
+SFB_API int sfb_set_deterministic(sfb_context *ctx, int enable);
+
 /* Kahan-compensated Newmark sums (enable != 0) in the fused forward driver
  * (sfb_run_forward): the corrector and predictor additions to v and u carry
  * their FP32 rounding error forward in two extra device arrays per medium

@@ -145,6 +145,7 @@ SIGNATURES = {
     "sfb_get_stream": (C.c_int, [_ctx, _P(C.c_void_p)]),
     "sfb_time_stiffness": (C.c_int, [_ctx, C.c_int, C.c_int, _P(C.c_double)]),
     "sfb_set_stiffness_variant": (C.c_int, [_ctx, C.c_int, C.c_int]),
+    "sfb_set_deterministic": (C.c_int, [_ctx, C.c_int]),
     "sfb_set_newmark_compensation": (C.c_int, [_ctx, C.c_int]),
     "sfb_set_checkpoint_interval": (C.c_int, [_ctx, C.c_int]),
     "sfb_write_wavefield": (C.c_int, [_ctx, C.c_int, C.c_char_p]),

@@ -177,6 +177,20 @@ struct sfb_context {
   // chunk and the remainders met so far)
   std::map<int, cudaGraphExec_t> graphs;
   uint64_t launches = 0;  // kernels launched so far (graph replays included)
+  // Deterministic assembly (sfb_set_deterministic): each medium's elements
+  // are coloured so that no two elements of a colour share a point, one
+  // stiffness launch per colour (device elements [col_begin, +col_count)),
+  // sources and coupling through owner-computes maps, seismograms from the
+  // receiver kernel: the same inputs give the same bits on every run.
+  bool deterministic = false;
+  int ncolor[4] = {0, 0, 0, 0};
+  std::vector<int> col_begin[4], col_count[4];
+  struct DetTailBuf {
+    DBuf<int> g, begin, ent;
+    int n = 0;
+    bool ready = false;
+  } det_tail[2][4];  // [forward sources / adjoint sources][medium]
+  std::vector<int> h_adj_elem, h_adj_medium;  // adjoint sources: device element, medium
 
   void drop_forward_graphs() {
     for (auto &kv : graphs) cudaGraphExecDestroy(kv.second);
@@ -222,6 +236,49 @@ template <typename F> int guarded(sfb_context *ctx, F &&fn) {
 
 int medium_index_ok(int m) { return m == 0 || m == 1 || m == 3; }
 
+// New contexts use the deterministic assembly when the environment sets
+// SFB_DETERMINISTIC=1 (file-driven runs, sfb_execute); sfb_set_deterministic
+// chooses per context.
+bool deterministic_default() {
+  const char *e = std::getenv("SFB_DETERMINISTIC");
+  return e && e[0] == '1';
+}
+
+// Greedy colouring of each medium's elements in mesh order: an element takes
+// the smallest colour none of the elements sharing one of its points has
+// (four colours on a structured quad mesh).
+std::vector<int> element_colours(const Assembly &a) {
+  const int nspec = a.nspec, nn = a.ngll * a.ngll;
+  std::vector<int> colour(nspec, -1);
+  for (int m : kMedia) {
+    const int np = a.nglob[m];
+    if (np == 0) continue;
+    std::vector<int> start(static_cast<size_t>(np) + 1, 0);
+    for (int e = 0; e < nspec; ++e)
+      if (a.medium[e] == m)
+        for (int k = 0; k < nn; ++k) ++start[a.iglob[static_cast<size_t>(e) * nn + k] + 1];
+    for (int g = 0; g < np; ++g) start[g + 1] += start[g];
+    std::vector<int> fill(start.begin(), start.end() - 1), elems(start[np]);
+    for (int e = 0; e < nspec; ++e)
+      if (a.medium[e] == m)
+        for (int k = 0; k < nn; ++k) elems[fill[a.iglob[static_cast<size_t>(e) * nn + k]]++] = e;
+    for (int e = 0; e < nspec; ++e) {
+      if (a.medium[e] != m) continue;
+      uint64_t used = 0;
+      for (int k = 0; k < nn; ++k) {
+        const int g = a.iglob[static_cast<size_t>(e) * nn + k];
+        for (int q = start[g]; q < start[g + 1]; ++q)
+          if (colour[elems[q]] >= 0) used |= uint64_t(1) << colour[elems[q]];
+      }
+      int col = 0;
+      while (col < 64 && ((used >> col) & 1)) ++col;
+      if (col == 64) throw std::runtime_error("element colouring needs more than 64 colours");
+      colour[e] = col;
+    }
+  }
+  return colour;
+}
+
 void build_permutation(sfb_context *c) {
   const Assembly &a = c->P.asmb;
   const int nspec = a.nspec, nn = a.ngll * a.ngll;
@@ -229,13 +286,31 @@ void build_permutation(sfb_context *c) {
   for (int e = 0; e < nspec; ++e)
     for (int k = 0; k < nn; ++k)
       if (a.bnd[static_cast<size_t>(e) * nn + k]) has_b[e] = 1;
+  // deterministic mode: colour ranges inside each medium
+  std::vector<int> colour(nspec, 0);
+  if (c->deterministic) colour = element_colours(a);
   c->perm.resize(nspec);
   for (int e = 0; e < nspec; ++e) c->perm[e] = e;
   auto rank = [](int m) { return m == 0 ? 0 : m == 1 ? 1 : 2; };
   std::stable_sort(c->perm.begin(), c->perm.end(), [&](int x, int y) {
     if (rank(a.medium[x]) != rank(a.medium[y])) return rank(a.medium[x]) < rank(a.medium[y]);
+    if (colour[x] != colour[y]) return colour[x] < colour[y];
     return has_b[x] < has_b[y];
   });
+  for (int m : kMedia) {
+    c->ncolor[m] = 0;
+    c->col_begin[m].clear();
+    c->col_count[m].clear();
+  }
+  for (int d = 0; d < nspec; ++d) {
+    const int e = c->perm[d], m = a.medium[e];
+    if (colour[e] >= c->ncolor[m]) {
+      c->ncolor[m] = colour[e] + 1;
+      c->col_begin[m].resize(c->ncolor[m], d);
+      c->col_count[m].resize(c->ncolor[m], 0);
+    }
+    ++c->col_count[m][colour[e]];
+  }
   c->inv.assign(nspec, 0);
   for (int d = 0; d < nspec; ++d) c->inv[c->perm[d]] = d;
   for (int m : kMedia) {
@@ -340,9 +415,10 @@ void ensure_device(sfb_context *c) {
   // constants in registers instead of staging geometry per point.  Chunks of
   // dev::kAffineChunk elements per medium, chunk-major (see
   // dev::Static::pack_aff).  FP32 contexts only: the compact-block kernels
-  // are FP32 kernels.
+  // are FP32 kernels.  The deterministic mode launches colour ranges, which
+  // the chunked compact block does not follow: it reads the full block.
 #ifndef SFB_FP64
-  {
+  if (!c->deterministic) {
     const int words = dev::affine_chunk_words(n);
     const int E = dev::kAffineChunk;
     std::vector<float> aff;
@@ -628,7 +704,17 @@ void initialize_mass(sfb_context *c, double dt) {
     f.minv = c->minv[m].p;
     f.mass = c->mass[m].p;
     if (c->mass[m].n) ck(cudaMemsetAsync(c->mass[m].p, 0, c->mass[m].n * sizeof(double), c->stream), "memset mass");
-    dev::launch_mass(m, a.ngll, c->st, f, static_cast<real>(dt), c->stream);
+    if (c->deterministic) {
+      // one launch per element colour: a fixed order of the FP64 sums
+      for (int k = 0; k < c->ncolor[m]; ++k) {
+        dev::MediumFields fk = f;
+        fk.elem_begin = c->col_begin[m][k];
+        fk.nelem = c->col_count[m][k];
+        dev::launch_mass(m, a.ngll, c->st, fk, static_cast<real>(dt), c->stream);
+      }
+    } else {
+      dev::launch_mass(m, a.ngll, c->st, f, static_cast<real>(dt), c->stream);
+    }
     dev::launch_invert_mass(f, c->stream);
   }
   ck(cudaGetLastError(), "mass kernels");
@@ -798,6 +884,73 @@ dev::UpdateParams update_params(sfb_context *c, WavefieldSet &W, int last, bool 
   return u;
 }
 
+// The owner-computes map of the sources (kind 0: the forward sources, kind 1:
+// the adjoint sources) and coupling points that medium m receives (see
+// dev::DetTail); built once per context.
+const dev::DetTail det_tail(sfb_context *c, int kind, int m) {
+  auto &T = c->det_tail[kind][m];
+  if (!T.ready) {
+    const Problem &P = c->P;
+    const Assembly &a = P.asmb;
+    const int nn = a.ngll * a.ngll;
+    std::vector<std::pair<int, int>> pairs;  // (target point, entry)
+    if (kind == 0) {
+      for (size_t i = 0; i < P.v_src_ispec.size(); ++i) {
+        const int e = P.v_src_ispec[i];
+        if (a.medium[e] != m) continue;
+        for (int k = 0; k < nn; ++k)
+          pairs.push_back({a.iglob[static_cast<size_t>(e) * nn + k], static_cast<int>(i) * nn + k});
+      }
+    } else {
+      for (size_t i = 0; i < c->h_adj_elem.size(); ++i) {
+        if (c->h_adj_medium[i] != m) continue;
+        const int e = c->perm[c->h_adj_elem[i]];
+        for (int k = 0; k < nn; ++k)
+          pairs.push_back({a.iglob[static_cast<size_t>(e) * nn + k], static_cast<int>(i) * nn + k});
+      }
+    }
+    const std::vector<int> *self = m == MEDIUM_ACOUSTIC ? &P.v_cp_ac_self : m == MEDIUM_ELASTIC_PSV ? &P.v_cp_el_self : nullptr;
+    if (self)
+      for (size_t i = 0; i < self->size(); ++i) pairs.push_back({(*self)[i], -static_cast<int>(i) - 1});
+    std::stable_sort(pairs.begin(), pairs.end(),
+                     [](const std::pair<int, int> &x, const std::pair<int, int> &y) { return x.first < y.first; });
+    std::vector<int> g, begin, ent;
+    for (size_t q = 0; q < pairs.size(); ++q) {
+      if (g.empty() || g.back() != pairs[q].first) {
+        g.push_back(pairs[q].first);
+        begin.push_back(static_cast<int>(q));
+      }
+      ent.push_back(pairs[q].second);
+    }
+    begin.push_back(static_cast<int>(pairs.size()));
+    T.n = static_cast<int>(g.size());
+    T.g.upload(g, &c->device_bytes);
+    T.begin.upload(begin, &c->device_bytes);
+    T.ent.upload(ent, &c->device_bytes);
+    T.ready = true;
+  }
+  return dev::DetTail{T.n, T.g.p, T.begin.p, T.ent.p};
+}
+
+// The stiffness of one medium with its sources and coupling (`tw`, may be
+// null): one launch in the atomic assembly, or, in the deterministic mode,
+// one launch per element colour and then the owner-computes tail launch.
+void stiffness_medium(sfb_context *c, int medium, const dev::MediumFields &f, const dev::StaceyStore &ss,
+                      const int *istep, const dev::TailWork *tw, const dev::FusedUpdate *fu, int src_kind) {
+  const int S = c->P.nshots, n = c->P.asmb.ngll;
+  if (!c->deterministic) {
+    dev::launch_stiffness(medium, n, c->st, f, S, ss, istep, c->stream, tw, fu, c->shots_variant[medium]);
+    return;
+  }
+  for (int k = 0; k < c->ncolor[medium]; ++k) {
+    dev::MediumFields fk = f;
+    fk.elem_begin = c->col_begin[medium][k];
+    fk.nelem = c->col_count[medium][k];
+    dev::launch_stiffness(medium, n, c->st, fk, S, ss, istep, c->stream, nullptr, fu, c->shots_variant[medium]);
+  }
+  if (tw && f.nelem > 0) dev::launch_tail_det(medium, n, c->st, f, S, istep, *tw, det_tail(c, src_kind, medium), c->stream);
+}
+
 // Element-private points are updated inside the batched P-SV stiffness launch
 // of the forward run unless an option needs every point in the update kernel.
 bool private_update_on(sfb_context *c) {
@@ -825,15 +978,14 @@ void enqueue_fused_step(sfb_context *c, WavefieldSet &W, int last) {
   // from the predicted elastic displacement, in one launch
   // single shot with both media: the elastic launch starts while the
   // acoustic one finishes (its element loop does not depend on it)
-  const bool overlap = S == 1 && W.f[dev::MED_AC].nelem > 0 && W.f[dev::MED_PSV].nelem > 0;
+  const bool overlap = S == 1 && W.f[dev::MED_AC].nelem > 0 && W.f[dev::MED_PSV].nelem > 0 && !c->deterministic;
   dev::TailWork ta{};
   ta.src = src;
   ta.cp = coupling_acoustic(c);
   ta.other = W.f[dev::MED_PSV];
   ta.cp_mode = ta.cp.n > 0 ? 1 : 0;
   ta.overlap = overlap ? dev::kOverlapFirst : 0;
-  dev::launch_stiffness(dev::MED_AC, n, c->st, W.f[dev::MED_AC], S, ss, istep, c->stream, &ta, nullptr,
-                        c->shots_variant[dev::MED_AC]);
+  stiffness_medium(c, dev::MED_AC, W.f[dev::MED_AC], ss, istep, &ta, nullptr, 0);
   // elastic: coupling reads the final acoustic acceleration = force * minv
   dev::TailWork te{};
   te.src = src;
@@ -853,24 +1005,36 @@ void enqueue_fused_step(sfb_context *c, WavefieldSet &W, int last) {
     fu.dtsq2 = dtsq2;
     fu.last = last;
   }
-  dev::launch_stiffness(dev::MED_PSV, n, c->st, W.f[dev::MED_PSV], S, ss, istep, c->stream, &te,
-                        fused ? &fu : nullptr, c->shots_variant[dev::MED_PSV]);
+  stiffness_medium(c, dev::MED_PSV, W.f[dev::MED_PSV], ss, istep, &te, fused ? &fu : nullptr, 0);
   dev::TailWork tsh{};
   tsh.src = src;
-  dev::launch_stiffness(dev::MED_SH, n, c->st, W.f[dev::MED_SH], S, ss, istep, c->stream, &tsh, nullptr,
-                        c->shots_variant[dev::MED_SH]);
+  stiffness_medium(c, dev::MED_SH, W.f[dev::MED_SH], ss, istep, &tsh, nullptr, 0);
   build_taps(c);
-  dev::launch_update_all(update_params(c, W, last, true, true, fused, true), c->stream);
+  if (c->deterministic) {
+    // seismograms in the receiver kernel's fixed summation order, from
+    // (u, v*, force) before the update
+    dev::launch_receivers(n, c->st, receiver_set(c, W), W.f, S, dt2, 1, istep, c->stream);
+    dev::launch_update_all(update_params(c, W, last, true, false, fused, true), c->stream);
+  } else {
+    dev::launch_update_all(update_params(c, W, last, true, true, fused, true), c->stream);
+  }
 }
 
 // Number of kernels one fused step launches (mirrors the skip conditions of
 // the launchers in kernels.cu).
 int fused_step_launches(sfb_context *c, WavefieldSet &W) {
   int n = 0;
-  for (int m : {dev::MED_AC, dev::MED_PSV, dev::MED_SH})
-    if (W.f[m].nelem > 0) ++n;  // stiffness (+ sources + coupling)
-  (void)c;
-  return n + 1;                 // one update launch for all media
+  for (int m : {dev::MED_AC, dev::MED_PSV, dev::MED_SH}) {
+    if (W.f[m].nelem == 0) continue;
+    if (!c->deterministic) {
+      ++n;  // stiffness (+ sources + coupling)
+    } else {
+      n += c->ncolor[m];                   // one stiffness launch per colour
+      if (det_tail(c, 0, m).ntarget) ++n;  // sources + coupling
+    }
+  }
+  if (c->deterministic && !c->P.receivers.empty() && !c->P.seismogram_types.empty()) ++n;  // receivers
+  return n + 1;  // one update launch for all media
 }
 
 void predictor_all(sfb_context *c, WavefieldSet &W, double sgn) {
@@ -961,6 +1125,26 @@ int update_wavefields(sfb_context *c, int w, int medium, int istep) {
   }
   if (w == SFB_WAVEFIELD_ADJOINT) ensure_adjoint_sources(c);
   dev::SourceSet src = w == SFB_WAVEFIELD_ADJOINT ? adjoint_source_set(c) : source_set(c);
+  if (c->deterministic) {
+    // colour launches, then sources and coupling (the acoustic medium is
+    // already divided by its mass here) through the owner-computes map
+    dev::TailWork tw{};
+    tw.src = src;
+    if (medium == dev::MED_AC) {
+      tw.cp = coupling_acoustic(c);
+      tw.other = W.f[dev::MED_PSV];
+      tw.cp_mode = tw.cp.n > 0 ? 1 : 0;
+    } else if (medium == dev::MED_PSV) {
+      tw.cp = coupling_elastic(c);
+      tw.other = W.f[dev::MED_AC];
+      tw.cp_mode = tw.cp.n > 0 ? 2 : 0;
+      tw.other_divided = 1;
+    }
+    stiffness_medium(c, medium, W.f[medium], ss, is, &tw, nullptr, w == SFB_WAVEFIELD_ADJOINT ? 1 : 0);
+    dev::launch_divide(W.f[medium], S, c->stream);
+    ck(cudaGetLastError(), "update_wavefields");
+    return W.f[medium].nelem;
+  }
   if (medium == dev::MED_AC) {
     dev::launch_coupling_acoustic(coupling_acoustic(c), W.f[dev::MED_AC], W.f[dev::MED_PSV], S, c->stream);
   } else if (medium == dev::MED_PSV) {
@@ -1025,6 +1209,8 @@ void ensure_adjoint_sources(sfb_context *c) {
     c->adj_medium.upload(md, tot);
     c->adj_array.upload(arr, tot);
     c->adj_stf.upload(stf, tot);
+    c->h_adj_elem = el;
+    c->h_adj_medium = md;
     return;
   }
   if (c->P.receivers.empty()) return;
@@ -1052,6 +1238,8 @@ void ensure_adjoint_sources(sfb_context *c) {
   c->adj_medium.upload(md, tot);
   c->adj_array.upload(arr, tot);
   c->adj_stf.alloc(static_cast<size_t>(c->nadj) * P.nstep * 2, tot);
+  c->h_adj_elem = el;
+  c->h_adj_medium = md;
 }
 
 dev::StaceyStore replay_store(sfb_context *c) {
@@ -1077,15 +1265,15 @@ void enqueue_adjoint_stiffness(sfb_context *c, WavefieldSet &A) {
   ta.cp = coupling_acoustic(c);
   ta.other = A.f[dev::MED_PSV];
   ta.cp_mode = ta.cp.n > 0 ? 1 : 0;
-  dev::launch_stiffness(dev::MED_AC, n, c->st, A.f[dev::MED_AC], S, none, istep, c->stream, &ta, nullptr,
-                        c->shots_variant[dev::MED_AC]);
+  stiffness_medium(c, dev::MED_AC, A.f[dev::MED_AC], none, istep, &ta, nullptr, 1);
   dev::TailWork te{};
   te.src = src;
   te.cp = coupling_elastic(c);
   te.other = A.f[dev::MED_AC];
   te.cp_mode = te.cp.n > 0 ? 2 : 0;
-  dev::launch_stiffness(dev::MED_PSV, n, c->st, A.f[dev::MED_PSV], S, none, istep, c->stream, &te, nullptr,
-                        c->shots_variant[dev::MED_PSV]);
+  stiffness_medium(c, dev::MED_PSV, A.f[dev::MED_PSV], none, istep, &te, nullptr, 1);
+  (void)S;
+  (void)n;
 }
 
 // The batched P-SV backward stiffness carries the Frechet kernels of its
@@ -1132,18 +1320,28 @@ void enqueue_backward_stiffness(sfb_context *c, WavefieldSet &A, WavefieldSet &B
       fu.dtsq2 = static_cast<real>(c->P.dt * c->P.dt / 2.0);
       fu.last = last;
     }
-    dev::launch_stiffness_frechet(n, c->st, B.f[dev::MED_PSV], S, ss, istep, te, fr, fu, c->stream);
+    if (!c->deterministic) {
+      dev::launch_stiffness_frechet(n, c->st, B.f[dev::MED_PSV], S, ss, istep, te, fr, fu, c->stream);
+    } else {
+      const dev::MediumFields &f = B.f[dev::MED_PSV];
+      for (int k = 0; k < c->ncolor[dev::MED_PSV]; ++k) {
+        dev::MediumFields fk = f;
+        fk.elem_begin = c->col_begin[dev::MED_PSV][k];
+        fk.nelem = c->col_count[dev::MED_PSV][k];
+        dev::launch_stiffness_frechet(n, c->st, fk, S, ss, istep, dev::TailWork{}, fr, fu, c->stream);
+      }
+      if (f.nelem > 0)
+        dev::launch_tail_det(dev::MED_PSV, n, c->st, f, S, istep, te, det_tail(c, 0, dev::MED_PSV), c->stream);
+    }
   } else {
-    dev::launch_stiffness(dev::MED_PSV, n, c->st, B.f[dev::MED_PSV], S, ss, istep, c->stream, &te, nullptr,
-                          c->shots_variant[dev::MED_PSV]);
+    stiffness_medium(c, dev::MED_PSV, B.f[dev::MED_PSV], ss, istep, &te, nullptr, 0);
   }
   dev::TailWork ta{};
   ta.src = src;
   ta.cp = coupling_acoustic(c);
   ta.other = B.f[dev::MED_PSV];
   ta.cp_mode = ta.cp.n > 0 ? 1 : 0;
-  dev::launch_stiffness(dev::MED_AC, n, c->st, B.f[dev::MED_AC], S, ss, istep, c->stream, &ta, nullptr,
-                        c->shots_variant[dev::MED_AC]);
+  stiffness_medium(c, dev::MED_AC, B.f[dev::MED_AC], ss, istep, &ta, nullptr, 0);
 }
 
 void enqueue_frechet(sfb_context *c, WavefieldSet &A, const dev::MediumFields *bwd_fields, int a_is_force,
@@ -1193,8 +1391,15 @@ void enqueue_combined_step(sfb_context *c, WavefieldSet &A, WavefieldSet &B, int
   dev::UpdateParams ua = update_params_signed(c, A, last, false, false, 1.0, backward_private_on(c));
   dev::launch_update_all(ua, c->stream);
   // the backward update records the backward seismograms and counts the
-  // shared step counter (held by the adjoint set) down
-  dev::UpdateParams ub = update_params_signed(c, B, last, false, true, -1.0, backward_private_on(c));
+  // shared step counter (held by the adjoint set) down; the deterministic
+  // mode records them with the receiver kernel first
+  if (c->deterministic) {
+    dev::ReceiverSet rs = receiver_set(c, B);
+    rs.backward_nstep = c->P.nstep;
+    dev::launch_receivers(c->P.asmb.ngll, c->st, rs, B.f, c->P.nshots, static_cast<real>(-c->P.dt / 2.0), 1,
+                          &A.ctrl.p->istep, c->stream);
+  }
+  dev::UpdateParams ub = update_params_signed(c, B, last, false, !c->deterministic, -1.0, backward_private_on(c));
   ub.ctrl = A.ctrl.p;
   dev::launch_update_all(ub, c->stream);
 }
@@ -1324,6 +1529,7 @@ SFB_API int sfb_create_from_yaml(const char *parameter_file, const char *default
   return guarded(nullptr, [&]() {
     std::unique_ptr<sfb_context> c(new sfb_context());
     c->P = problem_from_yaml(parameter_file, default_file ? default_file : "");
+    c->deterministic = deterministic_default();
     *out = c.release();
     return SFB_OK;
   });
@@ -1335,6 +1541,7 @@ SFB_API int sfb_create_structured(const sfb_structured_desc *desc, sfb_context *
   return guarded(nullptr, [&]() {
     std::unique_ptr<sfb_context> c(new sfb_context());
     c->P = problem_from_structured(*desc);
+    c->deterministic = deterministic_default();
     *out = c.release();
     return SFB_OK;
   });
@@ -1416,6 +1623,16 @@ SFB_API int sfb_set_checkpoint_interval(sfb_context *ctx, int interval) {
     ctx->ck_count = count;
     ctx->drop_forward_graphs();
     ctx->drop_combined_graphs();
+    return SFB_OK;
+  });
+}
+
+SFB_API int sfb_set_deterministic(sfb_context *ctx, int enable) {
+  if (!ctx) return SFB_E_INVALID;
+  return guarded(ctx, [&]() {
+    if (ctx->on_device && (enable != 0) != ctx->deterministic)
+      throw StateError("choose the assembly mode before the context's first device use");
+    ctx->deterministic = enable != 0;
     return SFB_OK;
   });
 }

@@ -154,11 +154,13 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// Bounded wait (about 2 s at 2 GHz).  Returns false on expiry.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
+// Bounded wait (by default 2^32 cycles, about 2 s at 2 GHz).  Returns false
+// on expiry.
+constexpr long long kWaitLimit = 1LL << 32;
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, long long limit = kWaitLimit) {
   const long long t0 = clock64();
   while (!mbar_try_wait(bar, parity)) {
-    if (clock64() - t0 > (1LL << 32)) return false;
+    if (clock64() - t0 > limit) return false;
   }
   return true;
 }
@@ -596,7 +598,7 @@ k_stiffness_rp(Static st, MediumFields f, int nshots, StaceyStore ss, const int 
   }
   stiffness_dep_tail(tw);
   if (!ok) {
-    if (t == 0) atomicExch(st.err, kWaitTimeout);
+    if (t == 0) atomicOr(st.err, kWaitTimeout);
     return;
   }
 
@@ -941,7 +943,7 @@ k_stiffness_rpa(Static st, MediumFields f, StaceyStore ss, const int *istep_dev,
     cp_async_wait_all();
     if (t == 0) {
       for (int j = waited + 1; j <= issued; ++j) mbar_wait_bounded(&bar[j % STAGES], (j / STAGES) & 1);
-      atomicExch(st.err, kWaitTimeout);
+      atomicOr(st.err, kWaitTimeout);
     }
     return;
   }
@@ -1712,6 +1714,52 @@ __global__ void k_couple_elastic(CouplingSet c, MediumFields el, MediumFields ac
 }
 
 // ---------------------------------------------------------------------------
+// Deterministic sources and coupling (see DetTail): the terms of tail_work,
+// summed per target point and shot in a fixed order.
+// ---------------------------------------------------------------------------
+template <int MED, int N>
+__global__ void k_tail_det(Static st, MediumFields f, int S, const int *istep_dev, TailWork tw, DetTail dt) {
+  constexpr int NC = (MED == MED_PSV) ? 2 : 1;
+  constexpr int NN = N * N;
+  const int istep = *istep_dev;
+  const bool src_on = tw.src.n > 0 && istep >= 0 && istep < tw.src.nstep;
+  const size_t total = static_cast<size_t>(dt.ntarget) * S;
+  for (size_t idx = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; idx < total;
+       idx += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const int t = static_cast<int>(idx / S), s = static_cast<int>(idx % S);
+    real acc[2] = {0, 0};
+    for (int q = dt.tgt_begin[t]; q < dt.tgt_begin[t + 1]; ++q) {
+      const int e = dt.ent[q];
+      if (e >= 0) {
+        const int i = e / NN, kk = e % NN;
+        if (!src_on || tw.src.shot[i] != s) continue;
+        const size_t p = static_cast<size_t>(tw.src.elem[i]) * NN + kk;
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+          const real stf = tw.src.stf[(static_cast<size_t>(i) * tw.src.nstep + istep) * 2 + c];
+          const real arr = tw.src.array[(static_cast<size_t>(i) * 2 + c) * NN + kk];
+          acc[c] += (MED == MED_AC) ? stf * arr / st.mat1[p] : stf * arr;
+        }
+      } else if (tw.cp_mode == 1) {  // acoustic self += w (n . u_elastic)
+        const int i = -e - 1;
+        const real2 u = reinterpret_cast<const real2 *>(tw.other.u)[static_cast<size_t>(tw.cp.other[i]) * S + s];
+        acc[0] += tw.cp.factor[i] * (tw.cp.nx[i] * u.x + tw.cp.nz[i] * u.y);
+      } else if (tw.cp_mode == 2) {  // elastic self += w n chi_ddot
+        const int i = -e - 1;
+        const int oi = tw.cp.other[i];
+        const real r = tw.other.a[static_cast<size_t>(oi) * S + s];
+        const real chi_dd = tw.other_divided ? r : r * tw.other.minv[oi];
+        acc[0] += tw.cp.factor[i] * tw.cp.nx[i] * chi_dd;
+        acc[1] += tw.cp.factor[i] * tw.cp.nz[i] * chi_dd;
+      }
+    }
+    real *A = f.a + (static_cast<size_t>(dt.tgt_g[t]) * S + s) * NC;
+#pragma unroll
+    for (int c = 0; c < NC; ++c) A[c] += acc[c];
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Receivers (compute_seismogram.tpp:98-135, wavefield.hpp): one block of 64
 // threads per (receiver, shot).
 // ---------------------------------------------------------------------------
@@ -1732,8 +1780,9 @@ __global__ void k_receivers(Static st, ReceiverSet rec, MediumFields f_psv, Medi
   __shared__ real s_red[2][64];
   const int r = blockIdx.x, s = blockIdx.y, k = threadIdx.x;
   const int istep = *istep_dev;
-  if (istep % rec.nsbs != 0) return;
-  const int isig = istep / rec.nsbs;
+  if (istep < 0 || istep % rec.nsbs != 0) return;
+  const int isig = rec.backward_nstep > 0 ? (rec.backward_nstep - 1) / rec.nsbs - istep / rec.nsbs
+                                          : istep / rec.nsbs;
   if (isig >= rec.max_sig) return;
   const int e = rec.elem[r];
   const int NN = N * N;
@@ -2263,6 +2312,33 @@ __global__ void k_invert(const double *mass, real *minv, size_t n) {
     minv[i] = static_cast<real>(1.0 / mass[i]);
 }
 
+// Error word bit set by k_nonfinite.
+constexpr int kNonFinite = 2;
+
+// NaN / Inf watchdog: sets kNonFinite in *err when any of p[0, n) is not
+// finite.
+__global__ void k_nonfinite(const real *p, size_t n, int *err) {
+  bool bad = false;
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x)
+    bad = bad || !isfinite(p[i]);
+  if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(err, kNonFinite);
+}
+
+// The bounded mbarrier wait of the stiffness kernels, run out on purpose: a
+// barrier in shared memory that expects one arrival which never comes, a
+// limit of `limit` cycles, then the timeout is recorded in *err exactly as
+// the stiffness kernels record it.  Nothing else is waited for or copied.
+__global__ void k_wait_probe(long long limit, int *err) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && !mbar_wait_bounded(&bar, 0, limit)) atomicOr(err, kWaitTimeout);
+}
+
 __global__ void k_zero(real *p, size_t n) {
   for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<size_t>(gridDim.x) * blockDim.x)
@@ -2406,6 +2482,21 @@ void launch_coupling_elastic(const CouplingSet &c, const MediumFields &el, const
   k_couple_elastic<<<grid, 128, 0, stream>>>(c, el, ac, nshots, ac_divided);
 }
 
+void launch_tail_det(int medium, int ngll, const Static &st, const MediumFields &f, int nshots,
+                     const int *istep_dev, const TailWork &tw, const DetTail &dt, cudaStream_t stream) {
+  if (dt.ntarget == 0) return;
+  const int grid = grid_for(static_cast<size_t>(dt.ntarget) * nshots, 128);
+  if (ngll == 5) {
+    if (medium == MED_PSV) k_tail_det<MED_PSV, 5><<<grid, 128, 0, stream>>>(st, f, nshots, istep_dev, tw, dt);
+    else if (medium == MED_SH) k_tail_det<MED_SH, 5><<<grid, 128, 0, stream>>>(st, f, nshots, istep_dev, tw, dt);
+    else k_tail_det<MED_AC, 5><<<grid, 128, 0, stream>>>(st, f, nshots, istep_dev, tw, dt);
+  } else if (ngll == 8) {
+    if (medium == MED_PSV) k_tail_det<MED_PSV, 8><<<grid, 128, 0, stream>>>(st, f, nshots, istep_dev, tw, dt);
+    else if (medium == MED_SH) k_tail_det<MED_SH, 8><<<grid, 128, 0, stream>>>(st, f, nshots, istep_dev, tw, dt);
+    else k_tail_det<MED_AC, 8><<<grid, 128, 0, stream>>>(st, f, nshots, istep_dev, tw, dt);
+  }
+}
+
 void launch_receivers(int ngll, const Static &st, const ReceiverSet &rec, const MediumFields *fields,
                       int nshots, real dt2, int mode, const int *istep_dev, cudaStream_t stream) {
   if (rec.n == 0 || rec.ntypes == 0) return;
@@ -2499,6 +2590,15 @@ void launch_frechet(int medium, int ngll, const Static &st, const MediumFields &
     if (medium == MED_PSV) k_frechet<MED_PSV, 8, EPB><<<grid, EPB * 64, 0, stream>>>(st, adj, bwd, nshots, dt, kern, a_is_force);
     else if (medium == MED_AC) k_frechet<MED_AC, 8, EPB><<<grid, EPB * 64, 0, stream>>>(st, adj, bwd, nshots, dt, kern, a_is_force);
   }
+}
+
+void launch_nonfinite_check(const real *p, size_t n, int *err, cudaStream_t stream) {
+  if (n == 0) return;
+  k_nonfinite<<<grid_for(n, 256), 256, 0, stream>>>(p, n, err);
+}
+
+void launch_wait_probe(long long limit_cycles, int *err, cudaStream_t stream) {
+  k_wait_probe<<<1, 32, 0, stream>>>(limit_cycles, err);
 }
 
 void launch_zero(real *p, size_t n, cudaStream_t stream) {

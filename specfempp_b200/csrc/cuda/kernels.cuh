@@ -95,6 +95,9 @@ struct ReceiverSet {
   int types[5];
   int max_sig, nsbs;
   real *seis;            // [S][max_sig][ntypes][n][2]
+  // > 0: the backward run of a combined loop of this many steps, whose
+  // samples are numbered in loop order (last step first)
+  int backward_nstep;
 };
 
 struct CouplingSet {
@@ -130,6 +133,19 @@ struct TailWork {
   int overlap;
 };
 constexpr int kOverlapFirst = 1, kOverlapSecond = 2;
+
+// Sources and coupling of one medium in the deterministic assembly mode, as
+// an owner-computes map: target point tgt_g[t] receives the entries
+// [tgt_begin[t], tgt_begin[t+1]) in that order, each a point source term
+// (source i, element point kk: i * N*N + kk >= 0) or a coupling entry
+// (-(index + 1)); one thread per (target, shot) sums them and adds the sum
+// once, so no two threads add into the same value.
+struct DetTail {
+  int ntarget;
+  const int *tgt_g;
+  const int *tgt_begin;
+  const int *ent;
+};
 
 // Seismograms as a sparse linear map of nodal values, applied inside the
 // update kernel: seis[s][isig][slot] += w * field_which(g).  `mask` has one
@@ -285,6 +301,10 @@ void launch_coupling_acoustic(const CouplingSet &c, const MediumFields &ac,
 void launch_coupling_elastic(const CouplingSet &c, const MediumFields &el,
                              const MediumFields &ac, int nshots, int ac_divided,
                              cudaStream_t stream);
+// Deterministic mode: the sources and coupling of `tw` through `dt` (see
+// DetTail), after the medium's stiffness launches.
+void launch_tail_det(int medium, int ngll, const Static &st, const MediumFields &f, int nshots,
+                     const int *istep_dev, const TailWork &tw, const DetTail &dt, cudaStream_t stream);
 // Seismograms at the end of a step.  mode 0: fields hold the final state
 // (u, v, a).  mode 1: fused loop, fields hold (u, v*, force) and the final
 // velocity/acceleration are formed on the fly.
@@ -305,6 +325,13 @@ void launch_mass(int medium, int ngll, const Static &st, const MediumFields &f, 
                  cudaStream_t stream);
 void launch_invert_mass(const MediumFields &f, cudaStream_t stream);
 void launch_zero(real *p, size_t n, cudaStream_t stream);
+// Error word bits: 1 a bounded device wait expired, 2 a non-finite value.
+constexpr int kErrWaitTimeout = 1, kErrNonFinite = 2;
+// Sets kErrNonFinite in *err when any of p[0, n) is NaN or infinite.
+void launch_nonfinite_check(const real *p, size_t n, int *err, cudaStream_t stream);
+// Test hook: a bounded mbarrier wait that nothing satisfies, run out after
+// `limit_cycles`, recorded in *err as the stiffness kernels record theirs.
+void launch_wait_probe(long long limit_cycles, int *err, cudaStream_t stream);
 // Frechet kernel accumulation for one medium (P-SV or acoustic) into
 // kern[p][3] (FP64, device element order).  a_is_force: the adjoint `a`
 // array holds the unassembled force of the fused loop (multiply by M^-1).

@@ -294,6 +294,11 @@ class Simulation:
         backward wavefield of the combined run (0: pure reconstruction)."""
         self._check(self._lib.sfb_set_checkpoint_interval(self._h, interval))
 
+    def set_deterministic(self, enable: bool = True):
+        """Bit-reproducible assembly (element colours, fixed-order sums);
+        before the first device use."""
+        self._check(self._lib.sfb_set_deterministic(self._h, 1 if enable else 0))
+
     def set_stiffness_variant(self, medium: int, variant: int):
         """Batched stiffness kernel of `medium` (1 packed two-shot, 2 scalar
         two-shot, 3 one shot per lane; 0 autotuned)."""
