@@ -233,6 +233,25 @@ SFB_API int sfb_run_forward(sfb_context *ctx, int nstep, int use_graph);
  * (predictor / update_wavefields / corrector per medium), with the
  * reference's DOF and element accounting checks (:90-108). */
 SFB_API int sfb_run_forward_unfused(sfb_context *ctx, int nstep);
+
+/* Failure reporting (no reference counterpart).  Device kernels record
+ * errors in a per-context error word: a bounded device-side wait that
+ * expired (every mbarrier wait of the stiffness kernels gives up after
+ * about 2 s), and non-finite values seen by the watchdog, which checks the
+ * wavefields (and kernels) at the end of every sfb_run_forward /
+ * sfb_run_combined and in sfb_synchronize.  The synchronising calls
+ * report them (SFB_E_CUDA for a wait, SFB_E_NONFINITE for NaN / Inf); the
+ * reference-granularity entry points (sfb_domain_*, sfb_newmark_*,
+ * sfb_frechet_compute_derivatives) report, without synchronising, what
+ * earlier launches recorded.  Reporting clears the word.
+ * sfb_synchronize waits for the context's stream, runs the watchdog over
+ * every allocated wavefield and reports. */
+SFB_API int sfb_synchronize(sfb_context *ctx);
+/* Test hook: enqueue one bounded mbarrier wait that nothing satisfies,
+ * giving up after `limit_cycles` GPU clock cycles ([0, 2^32]) and
+ * recording the timeout in the error word exactly as the stiffness
+ * kernels do; the next reporting call returns SFB_E_CUDA. */
+SFB_API int sfb_probe_device_wait(sfb_context *ctx, long long limit_cycles);
 /* Combined adjoint + backward loop with Frechet accumulation
  * (`time_marching<combined>::run`, :126-247).  Needs the forward run's last
  * state and Stacey replay store (sfb_copy_forward_to_backward). */
@@ -328,6 +347,14 @@ SFB_API int sfb_read_properties(sfb_context *ctx, const char *directory, int ele
  * adjoint + backward loop with the file's adjoint sources and writes the
  * kernels.  Errors: sfb_last_error(NULL). */
 SFB_API int sfb_execute(const char *parameter_file, const char *default_file);
+/* The same with the parameter and default dictionaries as YAML text, as the
+ * reference's Python entry point takes them (specfempp_core._execute,
+ * src/python/core.cpp:46-66); paths inside are relative to the working
+ * directory. */
+SFB_API int sfb_execute_text(const char *parameter_yaml, const char *default_yaml);
+SFB_API int sfb_create_from_yaml_text(const char *parameter_yaml,
+                                      const char *default_yaml,
+                                      sfb_context **out);
 
 /* Replace the source time function of source `isource` ([nstep][2] samples,
  * the second column only used by two-component media).  The reference's

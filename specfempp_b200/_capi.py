@@ -129,6 +129,8 @@ SIGNATURES = {
     "sfb_frechet_compute_derivatives": (C.c_int, [_ctx, C.c_double]),
     "sfb_run_forward": (C.c_int, [_ctx, C.c_int, C.c_int]),
     "sfb_run_forward_unfused": (C.c_int, [_ctx, C.c_int]),
+    "sfb_synchronize": (C.c_int, [_ctx]),
+    "sfb_probe_device_wait": (C.c_int, [_ctx, C.c_longlong]),
     "sfb_run_combined": (C.c_int, [_ctx, C.c_int, C.c_int]),
     "sfb_get_seismograms": (C.c_int, [_ctx, C.c_int, C.c_int, _P(C.c_float), C.c_size_t]),
     "sfb_get_seismograms_f64": (C.c_int, [_ctx, C.c_int, C.c_int, _P(C.c_double), C.c_size_t]),
@@ -155,6 +157,8 @@ SIGNATURES = {
     "sfb_write_properties": (C.c_int, [_ctx, C.c_char_p, C.c_int]),
     "sfb_read_properties": (C.c_int, [_ctx, C.c_char_p, C.c_int]),
     "sfb_execute": (C.c_int, [C.c_char_p, C.c_char_p]),
+    "sfb_execute_text": (C.c_int, [C.c_char_p, C.c_char_p]),
+    "sfb_create_from_yaml_text": (C.c_int, [C.c_char_p, C.c_char_p, _P(_ctx)]),
     "sfb_assemble_inverse_mass_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p,
                                                     C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                                     C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,

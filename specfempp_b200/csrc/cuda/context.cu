@@ -37,6 +37,9 @@ struct CudaError : std::runtime_error {
 struct StateError : std::runtime_error {
   using std::runtime_error::runtime_error;
 };
+struct NonFiniteError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
 
 void ck(cudaError_t e, const char *what) {
   if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
@@ -124,7 +127,8 @@ struct sfb_context {
   DBuf<real> bnd_nx, bnd_nz, bnd_w;
   DBuf<real> pack;  // [nspec][8][N*N] static block of the stiffness kernels
   DBuf<float> pack_aff;  // compact block of affine elements (single-shot FP32 contexts)
-  DBuf<int> dflag;   // device error flag
+  DBuf<int> dflag;   // device error word (dev::kErrWaitTimeout | dev::kErrNonFinite)
+  int *h_err = nullptr;  // pinned host copy of it, refreshed asynchronously after entry points
   DBuf<real> minv[4];
   DBuf<double> mass[4];
   // sources (forward / backward wavefield) and receivers
@@ -201,6 +205,7 @@ struct sfb_context {
     graphs_combined.clear();
   }
   ~sfb_context() {
+    if (h_err) cudaFreeHost(h_err);
     drop_forward_graphs();
     drop_combined_graphs();
     if (stream) cudaStreamDestroy(stream);
@@ -222,6 +227,8 @@ template <typename F> int guarded(sfb_context *ctx, F &&fn) {
     return fail(ctx, SFB_E_CUDA, e.what());
   } catch (const StateError &e) {
     return fail(ctx, SFB_E_STATE, e.what());
+  } catch (const NonFiniteError &e) {
+    return fail(ctx, SFB_E_NONFINITE, e.what());
   } catch (const std::invalid_argument &e) {
     return fail(ctx, SFB_E_INVALID, e.what());
   } catch (const std::bad_alloc &e) {
@@ -468,6 +475,8 @@ void ensure_device(sfb_context *c) {
   }
 #endif
   c->dflag.alloc(1, tot);
+  ck(cudaHostAlloc(reinterpret_cast<void **>(&c->h_err), sizeof(int), cudaHostAllocDefault), "cudaHostAlloc");
+  *c->h_err = 0;
   c->iglob.upload(iglob, tot);
   c->xix.upload(xix, tot);
   c->xiz.upload(xiz, tot);
@@ -1519,6 +1528,50 @@ void run_combined_fused(sfb_context *c, int use_graph) {
 // C ABI
 // ===========================================================================
 
+namespace {
+// The device error word: bit kErrWaitTimeout (a bounded device-side wait
+// expired) and bit kErrNonFinite (the watchdog saw NaN or Inf).  Entry
+// points report it without a device synchronisation: each one starts by
+// reading the pinned host copy that the previous one's asynchronous copy
+// left (poll_device_flag) and ends by enqueueing a new copy
+// (note_device_flag); the synchronising calls read it directly.
+void raise_device_error(sfb_context *c, int h) {
+  const int zero = 0;
+  cudaMemcpy(c->dflag.p, &zero, sizeof(int), cudaMemcpyHostToDevice);
+  if (c->h_err) *c->h_err = 0;
+  if (h & dev::kErrWaitTimeout)
+    throw CudaError("a device-side wait timed out (bounded mbarrier wait in a device kernel)");
+  throw NonFiniteError("non-finite values (NaN or Inf) in the wavefields or kernels");
+}
+void note_device_flag(sfb_context *c) {
+  if (c->dflag.p && c->h_err)
+    ck(cudaMemcpyAsync(c->h_err, c->dflag.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "error word");
+}
+void poll_device_flag(sfb_context *c) {
+  if (!c->h_err) return;
+  const int h = *static_cast<volatile int *>(c->h_err);
+  if (h != 0) {
+    ck(cudaStreamSynchronize(c->stream), "sync");
+    raise_device_error(c, h);
+  }
+}
+void check_device_flag(sfb_context *c) {
+  if (!c->dflag.p) return;
+  int h = 0;
+  ck(cudaStreamSynchronize(c->stream), "sync");
+  ck(cudaMemcpy(&h, c->dflag.p, sizeof(int), cudaMemcpyDeviceToHost), "error flag");
+  if (h != 0) raise_device_error(c, h);
+}
+// Watchdog over a wavefield set (u and v of every medium).
+void enqueue_nonfinite(sfb_context *c, WavefieldSet &W) {
+  for (int m : kMedia) {
+    dev::launch_nonfinite_check(W.u[m].p, W.u[m].n, c->dflag.p, c->stream);
+    dev::launch_nonfinite_check(W.v[m].p, W.v[m].n, c->dflag.p, c->stream);
+  }
+}
+
+}  // namespace
+
 SFB_API const char *sfb_last_error(const sfb_context *ctx) {
   return ctx ? ctx->err.c_str() : g_create_error.c_str();
 }
@@ -1529,6 +1582,18 @@ SFB_API int sfb_create_from_yaml(const char *parameter_file, const char *default
   return guarded(nullptr, [&]() {
     std::unique_ptr<sfb_context> c(new sfb_context());
     c->P = problem_from_yaml(parameter_file, default_file ? default_file : "");
+    c->deterministic = deterministic_default();
+    *out = c.release();
+    return SFB_OK;
+  });
+}
+
+SFB_API int sfb_create_from_yaml_text(const char *parameter_yaml, const char *default_yaml, sfb_context **out) {
+  if (!parameter_yaml || !out) return fail(nullptr, SFB_E_INVALID, "null argument");
+  *out = nullptr;
+  return guarded(nullptr, [&]() {
+    std::unique_ptr<sfb_context> c(new sfb_context());
+    c->P = problem_from_yaml_text(parameter_yaml, default_yaml ? default_yaml : "");
     c->deterministic = deterministic_default();
     *out = c.release();
     return SFB_OK;
@@ -1673,7 +1738,9 @@ SFB_API int sfb_domain_update_wavefields(sfb_context *ctx, int wavefield, int me
   return guarded(ctx, [&]() {
     if (!medium_index_ok(medium)) throw std::invalid_argument("unsupported medium tag");
     if (!ctx->mass_ready) throw StateError("domain_kernels::initialize has not been called");
+    poll_device_flag(ctx);
     const int n = update_wavefields(ctx, wavefield, medium, istep);
+    note_device_flag(ctx);
     if (elements_updated) *elements_updated = n;
     return SFB_OK;
   });
@@ -1683,11 +1750,13 @@ SFB_API int sfb_domain_compute_seismograms(sfb_context *ctx, int wavefield, int 
   if (!ctx) return SFB_E_INVALID;
   return guarded(ctx, [&]() {
     WavefieldSet &W = ensure_wavefield(ctx, wavefield);
+    poll_device_flag(ctx);
     // the kernel derives isig from the step counter: isig * nsbs
     set_step(ctx, W, isig_step * ctx->P.nstep_between_samples);
     dev::launch_receivers(ctx->P.asmb.ngll, ctx->st, receiver_set(ctx, W), W.f, ctx->P.nshots, real(0), 0,
                           &W.ctrl.p->istep, ctx->stream);
     ck(cudaGetLastError(), "compute_seismograms");
+    note_device_flag(ctx);
     return SFB_OK;
   });
 }
@@ -1699,6 +1768,7 @@ SFB_API int sfb_newmark_predictor(sfb_context *ctx, int wavefield, int medium, i
     WavefieldSet &W = ensure_wavefield(ctx, wavefield);
     const double sgn = wavefield == SFB_WAVEFIELD_BACKWARD ? -1.0 : 1.0;
     const Problem &P = ctx->P;
+    poll_device_flag(ctx);
     dev::launch_predictor(W.f[medium], P.nshots, static_cast<real>(sgn * P.dt),
                           static_cast<real>(sgn * P.dt / 2.0), static_cast<real>(P.dt * P.dt / 2.0),
                           ctx->stream);
@@ -1714,6 +1784,7 @@ SFB_API int sfb_newmark_corrector(sfb_context *ctx, int wavefield, int medium, i
     if (!medium_index_ok(medium)) throw std::invalid_argument("unsupported medium tag");
     WavefieldSet &W = ensure_wavefield(ctx, wavefield);
     const double sgn = wavefield == SFB_WAVEFIELD_BACKWARD ? -1.0 : 1.0;
+    poll_device_flag(ctx);
     dev::launch_corrector(W.f[medium], ctx->P.nshots, static_cast<real>(sgn * ctx->P.dt / 2.0), ctx->stream);
     ck(cudaGetLastError(), "corrector");
     if (dofs) *dofs = W.f[medium].nglob * W.f[medium].nc;
@@ -1721,22 +1792,34 @@ SFB_API int sfb_newmark_corrector(sfb_context *ctx, int wavefield, int medium, i
   });
 }
 
-// A bounded device-side wait that expired leaves a flag; report it.
-void check_device_flag(sfb_context *c) {
-  if (!c->dflag.p) return;
-  int h = 0;
-  ck(cudaMemcpy(&h, c->dflag.p, sizeof(int), cudaMemcpyDeviceToHost), "error flag");
-  if (h != 0) {
-    const int zero = 0;
-    cudaMemcpy(c->dflag.p, &zero, sizeof(int), cudaMemcpyHostToDevice);
-    throw CudaError("a device-side wait timed out (bounded mbarrier wait in the stiffness kernel)");
-  }
+SFB_API int sfb_synchronize(sfb_context *ctx) {
+  if (!ctx) return SFB_E_INVALID;
+  return guarded(ctx, [&]() {
+    if (!ctx->on_device) return SFB_OK;
+    for (int w = 0; w < 3; ++w)
+      if (ctx->wf[w].allocated) enqueue_nonfinite(ctx, ctx->wf[w]);
+    check_device_flag(ctx);
+    return SFB_OK;
+  });
+}
+
+SFB_API int sfb_probe_device_wait(sfb_context *ctx, long long limit_cycles) {
+  if (!ctx) return SFB_E_INVALID;
+  return guarded(ctx, [&]() {
+    if (limit_cycles < 0 || limit_cycles > (1LL << 32)) throw std::invalid_argument("limit_cycles must be in [0, 2^32]");
+    ensure_device(ctx);
+    dev::launch_wait_probe(limit_cycles, ctx->dflag.p, ctx->stream);
+    ck(cudaGetLastError(), "wait probe");
+    note_device_flag(ctx);
+    return SFB_OK;
+  });
 }
 
 SFB_API int sfb_run_forward(sfb_context *ctx, int nstep, int use_graph) {
   if (!ctx) return SFB_E_INVALID;
   return guarded(ctx, [&]() {
     run_forward_fused(ctx, nstep, use_graph);
+    enqueue_nonfinite(ctx, ctx->wf[SFB_WAVEFIELD_FORWARD]);
     ck(cudaStreamSynchronize(ctx->stream), "forward run");
     check_device_flag(ctx);
     return SFB_OK;
@@ -1746,6 +1829,7 @@ SFB_API int sfb_run_forward(sfb_context *ctx, int nstep, int use_graph) {
 SFB_API int sfb_run_forward_unfused(sfb_context *ctx, int nstep) {
   if (!ctx) return SFB_E_INVALID;
   return guarded(ctx, [&]() {
+    ctx->err.clear();  // the loop below detects failures of its own calls by the message
     WavefieldSet &W = ensure_wavefield(ctx, SFB_WAVEFIELD_FORWARD);
     if (!ctx->mass_ready) initialize_mass(ctx, ctx->P.dt);
     const Problem &P = ctx->P;
@@ -1782,7 +1866,9 @@ SFB_API int sfb_run_forward_unfused(sfb_context *ctx, int nstep) {
                         " of " + std::to_string(total_dofs) + ") or elements (" + std::to_string(elements) +
                         " of " + std::to_string(P.asmb.nspec) + ")");
     }
+    enqueue_nonfinite(ctx, W);
     ck(cudaStreamSynchronize(ctx->stream), "unfused forward run");
+    check_device_flag(ctx);
     W.step = start + nstep;
     return SFB_OK;
   });
@@ -2008,10 +2094,28 @@ SFB_API int sfb_read_properties(sfb_context *ctx, const char *directory, int ele
 // The reference's driver (src/execute.cpp): forward runs write seismograms
 // and, when asked, the forward wavefield; combined runs read that wavefield,
 // run the adjoint + backward loop and write the kernels.
+namespace {
+int execute_context(sfb_context *ctx);
+}
+
 SFB_API int sfb_execute(const char *parameter_file, const char *default_file) {
   sfb_context *ctx = nullptr;
-  int rc = sfb_create_from_yaml(parameter_file, default_file, &ctx);
+  const int rc = sfb_create_from_yaml(parameter_file, default_file, &ctx);
   if (rc) return rc;
+  return execute_context(ctx);
+}
+
+SFB_API int sfb_execute_text(const char *parameter_yaml, const char *default_yaml) {
+  sfb_context *ctx = nullptr;
+  const int rc = sfb_create_from_yaml_text(parameter_yaml, default_yaml, &ctx);
+  if (rc) return rc;
+  return execute_context(ctx);
+}
+
+namespace {
+// Runs the simulation a parameter file describes and destroys the context.
+int execute_context(sfb_context *ctx) {
+  int rc = 0;
   std::unique_ptr<sfb_context, void (*)(sfb_context *)> own(ctx, sfb_destroy);
   // the context goes away on return: its message moves to sfb_last_error(NULL)
   auto failed = [&](int code) { return fail(nullptr, code, ctx->err); };
@@ -2041,6 +2145,7 @@ SFB_API int sfb_execute(const char *parameter_file, const char *default_file) {
   }
   return SFB_OK;
 }
+}  // namespace
 
 SFB_API int sfb_set_source_time_function(sfb_context *ctx, int isource, const float *host, size_t count) {
   if (!ctx || !host) return SFB_E_INVALID;
@@ -2110,6 +2215,9 @@ SFB_API int sfb_run_combined(sfb_context *ctx, int nstep, int use_graph) {
   return guarded(ctx, [&]() {
     if (nstep != ctx->P.nstep) throw std::invalid_argument("the combined run covers the whole forward run (nstep)");
     run_combined_fused(ctx, use_graph);
+    enqueue_nonfinite(ctx, ctx->wf[SFB_WAVEFIELD_ADJOINT]);
+    enqueue_nonfinite(ctx, ctx->wf[SFB_WAVEFIELD_BACKWARD]);
+    dev::launch_nonfinite_check(ctx->kern.p, ctx->kern.n, ctx->dflag.p, ctx->stream);
     ck(cudaStreamSynchronize(ctx->stream), "combined run");
     check_device_flag(ctx);
     return SFB_OK;
@@ -2125,10 +2233,12 @@ SFB_API int sfb_frechet_compute_derivatives(sfb_context *ctx, double dt) {
     if (!ctx->kern.p) {
       ctx->kern.alloc(nk, &ctx->device_bytes);
     }
+    poll_device_flag(ctx);
     for (int m : {dev::MED_PSV, dev::MED_AC})
       dev::launch_frechet(m, ctx->P.asmb.ngll, ctx->st, A.f[m], B.f[m], ctx->P.nshots, static_cast<real>(dt),
                           ctx->kern.p, 0, ctx->stream);
     ck(cudaGetLastError(), "frechet");
+    note_device_flag(ctx);
     return SFB_OK;
   });
 }

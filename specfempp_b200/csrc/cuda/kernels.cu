@@ -2317,7 +2317,8 @@ constexpr int kNonFinite = 2;
 
 // NaN / Inf watchdog: sets kNonFinite in *err when any of p[0, n) is not
 // finite.
-__global__ void k_nonfinite(const real *p, size_t n, int *err) {
+template <typename T>
+__global__ void k_nonfinite(const T *p, size_t n, int *err) {
   bool bad = false;
   for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<size_t>(gridDim.x) * blockDim.x)
@@ -2594,8 +2595,14 @@ void launch_frechet(int medium, int ngll, const Static &st, const MediumFields &
 
 void launch_nonfinite_check(const real *p, size_t n, int *err, cudaStream_t stream) {
   if (n == 0) return;
-  k_nonfinite<<<grid_for(n, 256), 256, 0, stream>>>(p, n, err);
+  k_nonfinite<real><<<grid_for(n, 256), 256, 0, stream>>>(p, n, err);
 }
+#ifndef SFB_FP64
+void launch_nonfinite_check(const double *p, size_t n, int *err, cudaStream_t stream) {
+  if (n == 0) return;
+  k_nonfinite<double><<<grid_for(n, 256), 256, 0, stream>>>(p, n, err);
+}
+#endif
 
 void launch_wait_probe(long long limit_cycles, int *err, cudaStream_t stream) {
   k_wait_probe<<<1, 32, 0, stream>>>(limit_cycles, err);

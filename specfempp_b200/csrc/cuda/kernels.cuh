@@ -329,6 +329,9 @@ void launch_zero(real *p, size_t n, cudaStream_t stream);
 constexpr int kErrWaitTimeout = 1, kErrNonFinite = 2;
 // Sets kErrNonFinite in *err when any of p[0, n) is NaN or infinite.
 void launch_nonfinite_check(const real *p, size_t n, int *err, cudaStream_t stream);
+#ifndef SFB_FP64
+void launch_nonfinite_check(const double *p, size_t n, int *err, cudaStream_t stream);
+#endif
 // Test hook: a bounded mbarrier wait that nothing satisfies, run out after
 // `limit_cycles`, recorded in *err as the stiffness kernels record theirs.
 void launch_wait_probe(long long limit_cycles, int *err, cudaStream_t stream);

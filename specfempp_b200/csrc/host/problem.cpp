@@ -318,13 +318,34 @@ void Problem::fill_view(sfb_problem_view *v) const {
   v->seismogram_types = seismogram_types.data();
 }
 
+namespace {
+Problem problem_from_nodes(std::shared_ptr<YNode> root, std::shared_ptr<YNode> defaults,
+                           const std::string &parameter_file);
+}
+
 Problem problem_from_yaml(const std::string &parameter_file,
                           const std::string &default_file) {
   auto root = yaml_load_file(parameter_file);
-  const YNode *params = root->get("parameters");
-  if (!params) throw std::runtime_error("parameter file has no 'parameters' node");
   std::shared_ptr<YNode> defaults;
   if (!default_file.empty() && file_exists(default_file)) defaults = yaml_load_file(default_file);
+  return problem_from_nodes(root, defaults, parameter_file);
+}
+
+// The reference's Python entry point takes the parameter and default
+// dictionaries as YAML text (src/python/core.cpp:46-66); file paths in them
+// are relative to the working directory.
+Problem problem_from_yaml_text(const std::string &parameter_text, const std::string &default_text) {
+  auto root = yaml_parse(parameter_text);
+  std::shared_ptr<YNode> defaults;
+  if (!default_text.empty()) defaults = yaml_parse(default_text);
+  return problem_from_nodes(root, defaults, "");
+}
+
+namespace {
+Problem problem_from_nodes(std::shared_ptr<YNode> root, std::shared_ptr<YNode> defaults,
+                           const std::string &parameter_file) {
+  const YNode *params = root->get("parameters");
+  if (!params) throw std::runtime_error("parameter file has no 'parameters' node");
 
   const YNode *setup = params->get("simulation-setup");
   if (!setup) throw std::runtime_error("parameter file has no 'simulation-setup'");
@@ -472,6 +493,7 @@ Problem problem_from_yaml(const std::string &parameter_file,
   P.finalize();
   return P;
 }
+}  // namespace
 
 Problem problem_from_structured(const sfb_structured_desc &d) {
   if (d.ngll != 5 && d.ngll != 8) throw std::invalid_argument("ngll must be 5 or 8");

@@ -62,6 +62,7 @@ struct Problem {
   void fill_view(sfb_problem_view *v) const;
 };
 
+Problem problem_from_yaml_text(const std::string &parameter_text, const std::string &default_text);
 Problem problem_from_yaml(const std::string &parameter_file,
                           const std::string &default_file);
 Problem problem_from_structured(const sfb_structured_desc &d);

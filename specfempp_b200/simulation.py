@@ -294,6 +294,11 @@ class Simulation:
         backward wavefield of the combined run (0: pure reconstruction)."""
         self._check(self._lib.sfb_set_checkpoint_interval(self._h, interval))
 
+    def synchronize(self):
+        """Wait for the context's work, run the NaN / Inf watchdog and report
+        recorded device errors (SfbError)."""
+        self._check(self._lib.sfb_synchronize(self._h))
+
     def set_deterministic(self, enable: bool = True):
         """Bit-reproducible assembly (element colours, fixed-order sums);
         before the first device use."""
