@@ -293,6 +293,28 @@ def batched_forward(steps, cpu_seconds=None):
     return out
 
 
+def deterministic_forward(workload, steps):
+    """The same forward with the deterministic assembly (element colours,
+    fixed-order sums): device time per step, beside the atomic mode's."""
+    from specfempp_b200 import Simulation
+    p = make_problem(workload, GRAPH_STEPS + 3 + 2 * steps + 1)
+    with Simulation.structured(p) as sim:
+        sim.set_deterministic(True)
+        pin_variant(sim)
+        sim.initialize()
+        stream = sim_stream(sim)
+        sim.run_forward(GRAPH_STEPS)
+        sim.run_forward(steps)  # set-up: captures the graph of the remainder chunk
+        sim.run_forward(3)
+        ms = event_time(stream, lambda: sim.run_forward(steps))
+        info = sim.info()
+    return {"ms_per_step": ms / steps, "value": info.nshots * sum(info.nglob) * steps / (ms / 1000.0),
+            "unit": "GLL-point-updates/s", "steps": steps,
+            "stiffness_variant": {name: int(info.stiffness_variant[m])
+                                  for name, m in (("elastic_psv", 0), ("elastic_sh", 1), ("acoustic", 3))
+                                  if info.nelements[m] > 0}}
+
+
 def fwi_comparison(nshots=64, nstep=400, reps=2):
     """Forward + combined (adjoint + backward + Frechet kernels) run of the
     200 x 200 adjoint mesh: `nshots` shots batched in one context against one
@@ -482,7 +504,10 @@ def run_ours(args):
                              "frac": step_b / (ms / K / 1000.0) / 1e9 / peak}
     if world == 1 and args.workload == "coupled" and not args.no_secondary:
         sim.close()
+        line["deterministic"] = dict(deterministic_forward("coupled", K),
+                                     note="bit-reproducible assembly (sfb_set_deterministic) on the same workload")
         line["batched"] = batched_forward(min(K, 100), None if args.no_cpu_baseline else args.cpu_seconds)
+        line["batched"]["deterministic"] = deterministic_forward("batched", min(K, 100))
         line["fwi"] = fwi_comparison()
     if world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1

@@ -296,9 +296,20 @@ SFB_API int sfb_set_adjoint_sources(sfb_context *ctx, int shot,
                                     const float *host, size_t count);
 /* Frechet kernels summed over shots, per local point [nspec][ngll][ngll]:
  * which = 0 rho, 1 mu, 2 kappa, 3 rhop, 4 alpha, 5 beta (elastic) or
- * 0 rho, 1 kappa (acoustic points).  FP64. */
+ * 0 rho, 1 kappa (acoustic points).  FP64.  which = 6, 7 (after a combined
+ * run with sfb_set_stacey_kernels): the Stacey-traction derivatives
+ * dchi/d(rho vp), dchi/d(rho vs) per P-SV boundary point (zero elsewhere). */
 SFB_API int sfb_get_kernels(const sfb_context *ctx, int which, double *host,
                             size_t count);
+/* No reference counterpart: also accumulate, in combined runs, the model
+ * derivative of the Stacey traction of the P-SV medium, which the
+ * reference's kernels leave out (frechet_derivative.hpp:14-138): per
+ * boundary point -dt w |n| sum (s_adj.n^)(v.n^) and
+ * -dt w |n| sum (s_adj.v - (s_adj.n^)(v.n^)), the derivatives of the misfit
+ * with respect to rho vp and rho vs there (read with sfb_get_kernels 6, 7).
+ * With them the gradient is the derivative of the discrete misfit on
+ * absorbing meshes; without them it is the reference's. */
+SFB_API int sfb_set_stacey_kernels(sfb_context *ctx, int enable);
 /* Move the forward run's end state and Stacey replay store into the
  * backward wavefield of `dst` (reference: wavefield writer / reader tasks,
  * include/io/wavefield/{writer,reader}.tpp). */
@@ -321,6 +332,13 @@ SFB_API int sfb_write_seismograms(const sfb_context *ctx, int wavefield,
  * the Stacey traction alone, under other dataset names).  Needs
  * save_boundary_values when the mesh has Stacey edges. */
 SFB_API int sfb_write_wavefield(const sfb_context *ctx, int shot, const char *directory);
+/* One more step group, StepNNNNNN for the forward steps run so far, in an
+ * existing (or new) ForwardWavefield folder, without removing the steps
+ * already there: the reference's periodic wavefield writer
+ * (include/periodic_tasks/wavefield_writer.hpp; `time_interval` of the
+ * parameter file's writer.wavefield, src/parameter_parser/writer/
+ * wavefield.cpp:36-66). */
+SFB_API int sfb_write_wavefield_step(const sfb_context *ctx, int shot, const char *directory);
 /* Read such a folder back as the forward run's final state and boundary
  * store of shot `shot`, so sfb_run_combined can follow (the reference's
  * wavefield reader, include/io/wavefield/reader.tpp). */

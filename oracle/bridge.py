@@ -47,7 +47,8 @@ def load():
         lib.oracle_combined_f64.restype = C.c_int
         lib.oracle_combined_f64.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int,
                                             C.POINTER(C.c_float), C.POINTER(C.POINTER(C.c_double)),
-                                            C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]
+                                            C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                            C.POINTER(C.c_double)]
         lib.oracle_seismograms_f64.restype = C.c_int
         lib.oracle_seismograms_f64.argtypes = [C.c_void_p, C.POINTER(C.POINTER(C.c_double)),
                                                C.POINTER(C.c_double)]
@@ -141,13 +142,16 @@ def seismograms(sim, fields, precision: int = 64, exact: bool = False):
 
 
 def combined(sim, adjoint_stf, fwd, precision: int = 64, shot: int = 0, threads: int = 1,
-             want_backward_seismograms: bool = False, exact: bool = False):
+             want_backward_seismograms: bool = False, exact: bool = False, stacey_kernels: bool = False):
     """Run the oracle's combined (adjoint + backward) loop.  ``fwd`` is the
     result of ``forward(..., want_fields=True, want_stacey=True)`` (the
     forward run's last state and Stacey store; with ``exact``, of an exact
     forward); ``adjoint_stf`` is [nstep][nrec][2].  Returns FP64 kernels
     [nspec, ngll, ngll, 3] (elastic: rho, mu, kappa; acoustic: rho, kappa,
-    sum of per-step rho * kappa) and optionally the backward seismograms."""
+    sum of per-step rho * kappa) and optionally the backward seismograms.
+    ``stacey_kernels`` (exact only): also the P-SV Stacey-traction
+    derivatives [nspec, ngll, ngll, 2] (dchi/d(rho vp), dchi/d(rho vs)),
+    returned after the kernels."""
     lib = load()
     view = sim.problem_view()
     info = sim.info()
@@ -171,12 +175,18 @@ def combined(sim, adjoint_stf, fwd, precision: int = 64, shot: int = 0, threads:
     bseis = None
     if want_backward_seismograms:
         bseis = np.zeros((info.max_sig_step, info.nseismogram_types, info.nreceivers, 2), dtype=dt)
+    kb = None
+    if stacey_kernels:
+        if not exact:
+            raise ValueError("the Stacey-traction derivatives come with exact outputs")
+        kb = np.zeros((info.nspec, info.ngll, info.ngll, 2), dtype=np.float64)
     if exact:
         rc = lib.oracle_combined_f64(C.addressof(view), shot, nstep, threads,
                                      stf.ctypes.data_as(C.POINTER(C.c_float)), bufs,
                                      store.ctypes.data_as(C.POINTER(ct)),
                                      kernels.ctypes.data_as(C.POINTER(C.c_double)),
-                                     bseis.ctypes.data_as(C.POINTER(ct)) if bseis is not None else None)
+                                     bseis.ctypes.data_as(C.POINTER(ct)) if bseis is not None else None,
+                                     kb.ctypes.data_as(C.POINTER(C.c_double)) if kb is not None else None)
     else:
         rc = lib.oracle_combined(C.addressof(view), precision, shot, nstep, threads,
                                  stf.ctypes.data_as(C.POINTER(C.c_float)), bufs,
@@ -185,4 +195,9 @@ def combined(sim, adjoint_stf, fwd, precision: int = 64, shot: int = 0, threads:
                                  bseis.ctypes.data_as(C.POINTER(C.c_float)) if bseis is not None else None)
     if rc != 0:
         raise RuntimeError("oracle failed: " + lib.oracle_last_error().decode())
-    return (kernels, bseis) if want_backward_seismograms else kernels
+    out = [kernels]
+    if want_backward_seismograms:
+        out.append(bseis)
+    if kb is not None:
+        out.append(kb)
+    return tuple(out) if len(out) > 1 else kernels

@@ -106,6 +106,22 @@ template <typename T> struct Sim {
 
   size_t P(int e, int iz, int ix) const { return (static_cast<size_t>(e) * n + iz) * n + ix; }
 
+  // The element's boundary tag is stacey: Stacey points and no acoustic
+  // free-surface point (enumerations/boundary.hpp:50-105 makes an element
+  // with both composite_stacey_dirichlet).  Only these are stored by the
+  // forward run and replayed by the backward run
+  // (compute_stiffness_interaction.tpp:123-137, 251-255); composite
+  // elements are computed in the backward run like any other.
+  bool stacey_tagged(int e) const {
+    const int nn = n * n;
+    bool st = false, fs = false;
+    for (int k = 0; k < nn; ++k) {
+      st = st || (pv.bnd[static_cast<size_t>(e) * nn + k] & 1);
+      fs = fs || (pv.bnd[static_cast<size_t>(e) * nn + k] & 2);
+    }
+    return st && !fs;
+  }
+
   // ---- Newmark (newmark.tpp:60-117 predictor, :11-56 corrector) ---------
   void predictor(int m, T sgn) {
     Field<T> &F = f[m];
@@ -186,11 +202,7 @@ template <typename T> struct Sim {
       const int e = E[ie];
       T u[8 * 8 * 2], Fs[8 * 8 * 2 * 2];
       bool replay = false;
-      if (backward && (stacey_replay || stacey_replay64)) {
-        for (int k = 0; k < nn && !replay; ++k) replay = pv.bnd[static_cast<size_t>(e) * nn + k] & 1;
-        // Only elements carrying Stacey points are replayed; the reference
-        // keys this on the element boundary tag (stacey or composite).
-      }
+      if (backward && (stacey_replay || stacey_replay64)) replay = stacey_tagged(e);
       if (replay) {
         for (int k = 0; k < nn; ++k) {
           const size_t p = static_cast<size_t>(e) * nn + k;
@@ -277,9 +289,7 @@ template <typename T> struct Sim {
           if (store_stacey && (stacey_store || stacey_store64)) {
             // Forward runs keep the element-local acceleration of every
             // point of a Stacey element (compute_stiffness_interaction.tpp:251-255).
-            bool stacey_elem = false;
-            for (int k = 0; k < nn && !stacey_elem; ++k) stacey_elem = pv.bnd[static_cast<size_t>(e) * nn + k] & 1;
-            if (stacey_elem) {
+            if (stacey_tagged(e)) {
               const size_t at = (static_cast<size_t>(istep) * pv.nspec * nn + p) * 2;
               for (int c = 0; c < nc; ++c) {
                 if (stacey_store64) (*stacey_store64)[at + c] = static_cast<double>(acc[c]);
@@ -475,6 +485,33 @@ template <typename T> struct Sim {
   // medium/dim2/*/isotropic/frechet_derivative.hpp), per local point,
   // accumulated in FP64: k[p*3 + 0..2] = (rho, mu, kappa) for elastic,
   // (rho, kappa, sum of rho_kl * kappa_kl) for acoustic.
+  // Model derivative of the P-SV Stacey traction (left out of the
+  // reference's kernels): kb[p] += -dt w |n| ((s.n^)(v.n^), s.v - (s.n^)(v.n^))
+  // at Stacey points, s the adjoint displacement and v the backward
+  // wavefield's velocity after its corrector.
+  static void stacey_frechet(const Sim &adj, const Sim &bwd, T dt, double *kb) {
+    const sfb_problem_view &pv = adj.pv;
+    const int n = adj.n;
+    for (int e = 0; e < pv.nspec; ++e) {
+      if (pv.medium[e] != PSV) continue;
+      const Field<T> &FA = adj.f[PSV], &FB = bwd.f[PSV];
+      for (int iz = 0; iz < n; ++iz)
+        for (int ix = 0; ix < n; ++ix) {
+          const size_t p = adj.P(e, iz, ix);
+          if (!(pv.bnd[p] & 1)) continue;
+          const int g = pv.iglob[p];
+          const double nx = pv.bnd_nx[p], nz = pv.bnd_nz[p], we = pv.bnd_w[p];
+          const double j = std::sqrt(nx * nx + nz * nz), ux = nx / j, uz = nz / j;
+          const double sx = FA.u[g], sz = FA.u[static_cast<size_t>(FA.nglob) + g];
+          const double vx = FB.v[g], vz = FB.v[static_cast<size_t>(FB.nglob) + g];
+          const double sn = sx * ux + sz * uz, vn = vx * ux + vz * uz;
+          const double f = -static_cast<double>(dt) * we * j;
+          kb[p * 2 + 0] += f * sn * vn;
+          kb[p * 2 + 1] += f * (sx * vx + sz * vz - sn * vn);
+        }
+    }
+  }
+
   static void frechet(const Sim &adj, const Sim &bwd, T dt, double *k) {
     const sfb_problem_view &pv = adj.pv;
     const int n = adj.n, nn = n * n;
@@ -581,7 +618,7 @@ int run_forward(const sfb_problem_view *pv, int shot, int nstep, int threads,
 template <typename T, typename O = float>
 int run_combined(const sfb_problem_view *pv, int shot, int nstep, int threads, const float *adjoint_stf,
                  const O *const *buffer, const std::vector<O> &store, double *kernels,
-                 O *bseis) {
+                 O *bseis, double *kb = nullptr) {
   Sim<T> adj(*pv, shot), bwd(*pv, shot);
   adj.threads = bwd.threads = threads;
   adj.adjoint_stf = adjoint_stf;
@@ -621,6 +658,7 @@ int run_combined(const sfb_problem_view *pv, int shot, int nstep, int threads, c
       }
     }
     Sim<T>::frechet(adj, bwd, static_cast<T>(pv->dt), kernels);
+    if (kb) Sim<T>::stacey_frechet(adj, bwd, static_cast<T>(pv->dt), kb);
     if (istep % nsbs == 0 && isig < max_sig) {
       if (bseis) bwd.seismograms(bseis, isig);
       ++isig;
@@ -717,11 +755,12 @@ int oracle_forward_f64(const sfb_problem_view *pv, int shot, int nstep, int thre
 
 int oracle_combined_f64(const sfb_problem_view *pv, int shot, int nstep, int threads, const float *adjoint_stf,
                         const double *const *buffer, const double *stacey_store, double *kernels_out,
-                        double *bseis) {
+                        double *bseis, double *stacey_kernels_out) {
   try {
     const size_t nloc = static_cast<size_t>(pv->nspec) * pv->ngll * pv->ngll;
     std::vector<double> store(stacey_store, stacey_store + static_cast<size_t>(nstep) * nloc * 2);
-    return run_combined<double, double>(pv, shot, nstep, threads, adjoint_stf, buffer, store, kernels_out, bseis);
+    return run_combined<double, double>(pv, shot, nstep, threads, adjoint_stf, buffer, store, kernels_out, bseis,
+                                        stacey_kernels_out);
   } catch (const std::exception &e) {
     g_err = e.what();
     return -1;

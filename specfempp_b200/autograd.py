@@ -17,8 +17,16 @@ kappa' = lambda + mu):
     d chi / d rho   = wJ * K_rho / rho       (wJ = w_x w_z J per point)
 
 and kappa = rho (vp^2 - 4/3 vs^2), mu = rho vs^2 give the gradient with
-respect to (rho, vp, vs).  The Stacey terms' own dependence on the model is
-not part of the reference's kernels (it is absent here too).  Elastic P-SV
+respect to (rho, vp, vs).  The Stacey traction's own dependence on the model
+is not part of the reference's kernels; by default it is absent here too (the
+gradient is the reference's).  With ``boundary_term=True`` (sixth argument)
+the combined run also accumulates dchi/d(rho vp) and dchi/d(rho vs) at the
+absorbing boundary points (sfb_set_stacey_kernels) and the gradient adds
+
+    d chi / d rho += vp dchi/d(rho vp) + vs dchi/d(rho vs),
+    d chi / d vp  += rho dchi/d(rho vp),   d chi / d vs += rho dchi/d(rho vs),
+
+the derivative of the discrete misfit on absorbing meshes.  Elastic P-SV
 models only.
 """
 from __future__ import annotations
@@ -53,7 +61,7 @@ def gradients_from_kernels(sim: Simulation, rho, vp, vs):
 
 class WaveformMisfit(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, rho, vp, vs, sim: Simulation, observed):
+    def forward(ctx, rho, vp, vs, sim: Simulation, observed, boundary_term: bool = False):
         info = sim.info()
         if info.nelements[3] or info.nelements[1]:
             raise NotImplementedError("WaveformMisfit supports elastic P-SV models")
@@ -73,6 +81,7 @@ class WaveformMisfit(torch.autograd.Function):
             res.append(rr)
             chi += 0.5 * float(np.sum(rr * rr)) * info.dt
         ctx.sim = sim
+        ctx.boundary_term = bool(boundary_term)
         ctx.res = res
         ctx.model = (r, p, s)
         ctx.device = rho.device
@@ -87,8 +96,15 @@ class WaveformMisfit(torch.autograd.Function):
             raise NotImplementedError("adjoint sources need one seismogram sample per step")
         for shot, rr in enumerate(ctx.res):
             sim.set_adjoint_sources(rr.astype(np.float32), shot=shot)
+        sim.set_stacey_kernels(ctx.boundary_term)
         sim.run_combined()
         g_rho, g_vp, g_vs = gradients_from_kernels(sim, *ctx.model)
+        if ctx.boundary_term:
+            rho, vp, vs = ctx.model
+            b_vp, b_vs = sim.kernels(6), sim.kernels(7)
+            g_rho = g_rho + vp * b_vp + vs * b_vs
+            g_vp = g_vp + rho * b_vp
+            g_vs = g_vs + rho * b_vs
         go = float(grad_out)
         to = lambda g: torch.as_tensor(g * go, dtype=ctx.dtype, device=ctx.device)
-        return to(g_rho), to(g_vp), to(g_vs), None, None
+        return to(g_rho), to(g_vp), to(g_vs), None, None, None

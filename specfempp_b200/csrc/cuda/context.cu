@@ -153,6 +153,9 @@ struct sfb_context {
   DBuf<real> adj_array, adj_stf;
   int nadj = 0;
   DBuf<double> kern;        // Frechet accumulators [nspec][N*N][3], device element order
+  // Stacey-traction model derivatives [nspec][N*N][2] (sfb_set_stacey_kernels)
+  bool stacey_kernels = false;
+  DBuf<double> kern_b;
   std::map<int, cudaGraphExec_t> graphs_combined;  // combined-run graphs by step count
   std::vector<float> host_seis;
   // seismogram taps per medium (fused path)
@@ -558,12 +561,16 @@ void ensure_device(sfb_context *c) {
   c->cp_el_nx.upload(P.v_cp_el_nx, tot);
   c->cp_el_nz.upload(P.v_cp_el_nz, tot);
   c->step_scratch.alloc(4, tot);
-  // Stacey replay slots: one per device element carrying Stacey points
+  // Stacey replay slots: one per device element whose boundary tag is
+  // stacey -- Stacey points and no acoustic free-surface point; composite
+  // Stacey / Dirichlet elements are computed in the backward run, not
+  // replayed (compute_stiffness_interaction.tpp:123-137 replays the stacey
+  // tag only; enumerations/boundary.hpp:50-105 combines the tags)
   {
     std::vector<int> slot(a.nspec, -1);
     c->nstacey = 0;
     for (int d = 0; d < a.nspec; ++d)
-      if (eflag[d] & 1) slot[d] = c->nstacey++;
+      if ((eflag[d] & 3) == 1) slot[d] = c->nstacey++;
     c->stacey_slot.upload(slot, tot);
     c->h_stacey_slot = slot;
   }
@@ -1060,6 +1067,30 @@ void ensure_store(sfb_context *c) {
   c->stacey_data.alloc(n, &c->device_bytes);
 }
 
+// Everything the deterministic mode's launches allocate, built before any
+// stream capture (no allocation may happen inside one).
+void prepare_deterministic(sfb_context *c) {
+  if (!c->deterministic) return;
+  for (int m : kMedia) {
+    det_tail(c, 0, m);
+    if (!c->h_adj_elem.empty()) det_tail(c, 1, m);
+  }
+}
+
+// Enqueue a capture's work; if it throws, end the capture (discarding the
+// partial graph) so that the stream is usable again, and rethrow.
+template <typename F> void capture_steps(sfb_context *c, F &&enqueue) {
+  try {
+    enqueue();
+  } catch (...) {
+    cudaGraph_t g = nullptr;
+    cudaStreamEndCapture(c->stream, &g);
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    throw;
+  }
+}
+
 void run_forward_fused(sfb_context *c, int nstep, int use_graph) {
   WavefieldSet &W = ensure_wavefield(c, SFB_WAVEFIELD_FORWARD);
   if (c->P.save_boundary_values) ensure_store(c);
@@ -1078,13 +1109,16 @@ void run_forward_fused(sfb_context *c, int nstep, int use_graph) {
   // graph-launched once its chunk sizes have been seen)
   const int body = nstep - 1;
   constexpr int K = 25;  // fused steps per full CUDA graph
+  prepare_deterministic(c);
   auto graph_of = [&](int steps) {
     auto it = c->graphs.find(steps);
     if (it != c->graphs.end()) return it->second;
     cudaGraph_t g;
     cudaGraphExec_t ex = nullptr;
     ck(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
-    for (int k = 0; k < steps; ++k) enqueue_fused_step(c, W, 0);
+    capture_steps(c, [&]() {
+      for (int k = 0; k < steps; ++k) enqueue_fused_step(c, W, 0);
+    });
     ck(cudaStreamEndCapture(c->stream, &g), "end capture");
     ck(cudaGraphInstantiate(&ex, g, 0), "graph instantiate");
     cudaGraphDestroy(g);
@@ -1354,8 +1388,11 @@ void enqueue_backward_stiffness(sfb_context *c, WavefieldSet &A, WavefieldSet &B
 }
 
 void enqueue_frechet(sfb_context *c, WavefieldSet &A, const dev::MediumFields *bwd_fields, int a_is_force,
-                     bool psv_done = false) {
+                     bool psv_done = false, real vcorr = 0) {
   const real dt = static_cast<real>(c->P.dt);
+  if (c->stacey_kernels)
+    dev::launch_stacey_frechet(c->P.asmb.ngll, c->st, A.f[dev::MED_PSV], bwd_fields[dev::MED_PSV], c->P.nshots, dt,
+                               vcorr, c->kern_b.p, c->stream);
   for (int m : {dev::MED_PSV, dev::MED_AC}) {
     if (m == dev::MED_PSV && psv_done) continue;
     dev::launch_frechet(m, c->P.asmb.ngll, c->st, A.f[m], bwd_fields[m], c->P.nshots, dt, c->kern.p, a_is_force,
@@ -1395,7 +1432,9 @@ void enqueue_combined_step(sfb_context *c, WavefieldSet &A, WavefieldSet &B, int
   enqueue_restore(c, A, B);
   enqueue_adjoint_stiffness(c, A);
   enqueue_backward_stiffness(c, A, B, last);
-  enqueue_frechet(c, A, B.f, 1, frechet_fused(c));
+  // the backward fields hold (u, v*, force) here: the step's final velocity
+  // is v* - dt/2 force M^-1
+  enqueue_frechet(c, A, B.f, 1, frechet_fused(c), static_cast<real>(-c->P.dt / 2.0));
   // with the fused Frechet launch, both wavefields' private points are done
   dev::UpdateParams ua = update_params_signed(c, A, last, false, false, 1.0, backward_private_on(c));
   dev::launch_update_all(ua, c->stream);
@@ -1450,9 +1489,14 @@ void run_combined_fused(sfb_context *c, int use_graph) {
   ensure_adjoint_sources(c);
   if (!c->mass_ready) initialize_mass(c, P.dt);
   build_taps(c);
+  prepare_deterministic(c);
   const size_t nk = P.asmb.nloc() * 3;
   if (!c->kern.p) c->kern.alloc(nk, &c->device_bytes);
   ck(cudaMemsetAsync(c->kern.p, 0, nk * sizeof(double), c->stream), "zero kernels");
+  if (c->stacey_kernels) {
+    if (!c->kern_b.p) c->kern_b.alloc(P.asmb.nloc() * 2, &c->device_bytes);
+    ck(cudaMemsetAsync(c->kern_b.p, 0, c->kern_b.n * sizeof(double), c->stream), "zero boundary kernels");
+  }
   zero_fields(c, A);
   zero_fields(c, B);
   const int N = P.nstep;
@@ -1498,7 +1542,9 @@ void run_combined_fused(sfb_context *c, int use_graph) {
     cudaGraph_t g;
     cudaGraphExec_t ex = nullptr;
     ck(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
-    for (int k = 0; k < steps; ++k) enqueue_combined_step(c, A, B, 0);
+    capture_steps(c, [&]() {
+      for (int k = 0; k < steps; ++k) enqueue_combined_step(c, A, B, 0);
+    });
     ck(cudaStreamEndCapture(c->stream, &g), "end capture");
     ck(cudaGraphInstantiate(&ex, g, 0), "graph instantiate");
     cudaGraphDestroy(g);
@@ -1688,6 +1734,15 @@ SFB_API int sfb_set_checkpoint_interval(sfb_context *ctx, int interval) {
     ctx->ck_count = count;
     ctx->drop_forward_graphs();
     ctx->drop_combined_graphs();
+    return SFB_OK;
+  });
+}
+
+SFB_API int sfb_set_stacey_kernels(sfb_context *ctx, int enable) {
+  if (!ctx) return SFB_E_INVALID;
+  return guarded(ctx, [&]() {
+    if (ctx->stacey_kernels != (enable != 0)) ctx->drop_combined_graphs();  // captured steps hold the old launches
+    ctx->stacey_kernels = enable != 0;
     return SFB_OK;
   });
 }
@@ -1985,39 +2040,59 @@ SFB_API int sfb_write_seismograms(const sfb_context *cctx, int wavefield, int sh
   });
 }
 
+namespace {
+// The forward state of `shot` after the steps run so far, with the boundary
+// store, in the reference's layout (fresh: a new file with coordinates;
+// otherwise one more step group).
+void write_snapshot(sfb_context *ctx, int shot, const char *directory, bool fresh) {
+  const Problem &P = ctx->P;
+  if (shot < 0 || shot >= P.nshots) throw std::invalid_argument("shot out of range");
+  WavefieldSet &F = ensure_wavefield(ctx, SFB_WAVEFIELD_FORWARD);
+  if (F.step < 1) throw StateError("no forward step has run");
+  ForwardSnapshot snap;
+  snap.step = F.step;
+  for (int m : kMedia) {
+    const size_t n = static_cast<size_t>(P.asmb.nglob[m]) * P.asmb.ncomp(m);
+    for (int w = 0; w < 3; ++w) {
+      snap.field[m][w].assign(n, 0.f);
+      if (n) {
+        const int rc = sfb_get_field(ctx, SFB_WAVEFIELD_FORWARD, m, w, shot, snap.field[m][w].data(), n);
+        if (rc) throw std::runtime_error(ctx->err);
+      }
+    }
+  }
+  // boundary store of this shot, slots by mesh element
+  snap.slot.assign(P.asmb.nspec, -1);
+  for (int e = 0; e < P.asmb.nspec; ++e) snap.slot[e] = ctx->h_stacey_slot.empty() ? -1 : ctx->h_stacey_slot[ctx->inv[e]];
+  snap.nstacey = ctx->nstacey;
+  const size_t per = static_cast<size_t>(P.nstep) * ctx->nstacey * P.asmb.ngll * P.asmb.ngll * 2;
+  if (per && ctx->stacey_data.p) {
+    snap.store.resize(per);
+    ck(cudaStreamSynchronize(ctx->stream), "sync");
+    copy_d2h(snap.store.data(), ctx->stacey_data.p + static_cast<size_t>(shot) * per, per, "store d2h");
+  } else if (per) {
+    throw StateError("the forward run kept no boundary store (save_boundary_values)");
+  }
+  write_forward_wavefield(P, directory, snap, fresh);
+}
+}  // namespace
+
 SFB_API int sfb_write_wavefield(const sfb_context *cctx, int shot, const char *directory) {
   sfb_context *ctx = const_cast<sfb_context *>(cctx);
   if (!ctx || !directory) return SFB_E_INVALID;
   return guarded(ctx, [&]() {
-    const Problem &P = ctx->P;
-    if (shot < 0 || shot >= P.nshots) throw std::invalid_argument("shot out of range");
-    WavefieldSet &F = ensure_wavefield(ctx, SFB_WAVEFIELD_FORWARD);
-    if (F.step != P.nstep) throw StateError("write the forward wavefield after the whole forward run");
-    ForwardSnapshot snap;
-    snap.step = P.nstep;
-    for (int m : kMedia) {
-      const size_t n = static_cast<size_t>(P.asmb.nglob[m]) * P.asmb.ncomp(m);
-      for (int w = 0; w < 3; ++w) {
-        snap.field[m][w].assign(n, 0.f);
-        if (n) {
-          const int rc = sfb_get_field(ctx, SFB_WAVEFIELD_FORWARD, m, w, shot, snap.field[m][w].data(), n);
-          if (rc) throw std::runtime_error(ctx->err);
-        }
-      }
-    }
-    // boundary store of this shot, slots in reference element order
-    snap.slot.assign(P.asmb.nspec, -1);
-    for (int e = 0; e < P.asmb.nspec; ++e) snap.slot[e] = ctx->h_stacey_slot.empty() ? -1 : ctx->h_stacey_slot[ctx->inv[e]];
-    snap.nstacey = ctx->nstacey;
-    const size_t per = static_cast<size_t>(P.nstep) * ctx->nstacey * P.asmb.ngll * P.asmb.ngll * 2;
-    if (per && ctx->stacey_data.p) {
-      snap.store.resize(per);
-      ck(cudaStreamSynchronize(ctx->stream), "sync");
-      copy_d2h(snap.store.data(), ctx->stacey_data.p + static_cast<size_t>(shot) * per, per, "store d2h");
-    } else if (per) {
-      throw StateError("the forward run kept no boundary store (save_boundary_values)");
-    }
-    write_forward_wavefield(P, directory, snap);
+    if (ensure_wavefield(ctx, SFB_WAVEFIELD_FORWARD).step != ctx->P.nstep)
+      throw StateError("write the forward wavefield after the whole forward run");
+    write_snapshot(ctx, shot, directory, true);
+    return SFB_OK;
+  });
+}
+
+SFB_API int sfb_write_wavefield_step(const sfb_context *cctx, int shot, const char *directory) {
+  sfb_context *ctx = const_cast<sfb_context *>(cctx);
+  if (!ctx || !directory) return SFB_E_INVALID;
+  return guarded(ctx, [&]() {
+    write_snapshot(ctx, shot, directory, false);
     return SFB_OK;
   });
 }
@@ -2029,11 +2104,10 @@ SFB_API int sfb_read_wavefield(sfb_context *ctx, int shot, const char *directory
     if (shot < 0 || shot >= P.nshots) throw std::invalid_argument("shot out of range");
     WavefieldSet &F = ensure_wavefield(ctx, SFB_WAVEFIELD_FORWARD);
     if (!ctx->mass_ready) initialize_mass(ctx, P.dt);
-    ForwardSnapshot snap = read_forward_wavefield(P, directory, ctx->nstacey);
-    for (int e = 0; e < P.asmb.nspec; ++e) {
-      const int want = ctx->h_stacey_slot.empty() ? -1 : ctx->h_stacey_slot[ctx->inv[e]];
-      if (snap.slot[e] != want) throw std::runtime_error("the stored boundary layout does not match this mesh");
-    }
+    std::vector<int> slot(P.asmb.nspec, -1);
+    for (int e = 0; e < P.asmb.nspec; ++e)
+      if (!ctx->h_stacey_slot.empty()) slot[e] = ctx->h_stacey_slot[ctx->inv[e]];
+    ForwardSnapshot snap = read_forward_wavefield(P, directory, slot, ctx->nstacey);
     for (int m : kMedia) {
       const size_t n = static_cast<size_t>(P.asmb.nglob[m]) * P.asmb.ncomp(m);
       if (!n) continue;
@@ -2128,12 +2202,32 @@ int execute_context(sfb_context *ctx) {
     return SFB_OK;
   }
   if (P.simulation == 0) {
-    if ((rc = sfb_run_forward(ctx, P.nstep, 1))) return failed(rc);
+    // the forward run, in pieces between the wavefield writer's snapshots
+    // (periodic_tasks/wavefield_writer.hpp: after step k when k is a
+    // multiple of time_interval, and after the last step when
+    // include_last_step), the coordinates with the first
+    const int K = P.wavefield_dir.empty() ? 0 : P.wavefield_time_interval;
+    int done = 0;
+    bool fresh = true;
+    while (done < P.nstep) {
+      const int next = K > 0 ? std::min(P.nstep, (done / K + 1) * K) : P.nstep;
+      if ((rc = sfb_run_forward(ctx, next - done, 1))) return failed(rc);
+      done = next;
+      const bool periodic = K > 0 && done % K == 0;
+      const bool last = done == P.nstep && P.wavefield_include_last_step;
+      if (!P.wavefield_dir.empty() && (periodic || last)) {
+        // the first snapshot starts the file (with the coordinates)
+        rc = guarded(ctx, [&]() {
+          write_snapshot(ctx, 0, P.wavefield_dir.c_str(), fresh);
+          return SFB_OK;
+        });
+        if (rc) return failed(rc);
+        fresh = false;
+      }
+    }
     if (P.write_seismograms)
       for (int s = 0; s < P.nshots; ++s)
         if ((rc = sfb_write_seismograms(ctx, SFB_WAVEFIELD_FORWARD, s, P.seismogram_dir.c_str()))) return failed(rc);
-    if (!P.wavefield_dir.empty())
-      if ((rc = sfb_write_wavefield(ctx, 0, P.wavefield_dir.c_str()))) return failed(rc);
   } else {
     if (P.wavefield_dir.empty()) return fail(nullptr, SFB_E_INVALID, "combined run without a wavefield reader directory");
     if ((rc = sfb_read_wavefield(ctx, 0, P.wavefield_dir.c_str()))) return failed(rc);
@@ -2237,6 +2331,11 @@ SFB_API int sfb_frechet_compute_derivatives(sfb_context *ctx, double dt) {
     for (int m : {dev::MED_PSV, dev::MED_AC})
       dev::launch_frechet(m, ctx->P.asmb.ngll, ctx->st, A.f[m], B.f[m], ctx->P.nshots, static_cast<real>(dt),
                           ctx->kern.p, 0, ctx->stream);
+    if (ctx->stacey_kernels) {
+      if (!ctx->kern_b.p) ctx->kern_b.alloc(ctx->P.asmb.nloc() * 2, &ctx->device_bytes);
+      dev::launch_stacey_frechet(ctx->P.asmb.ngll, ctx->st, A.f[dev::MED_PSV], B.f[dev::MED_PSV], ctx->P.nshots,
+                                 static_cast<real>(dt), real(0), ctx->kern_b.p, ctx->stream);
+    }
     ck(cudaGetLastError(), "frechet");
     note_device_flag(ctx);
     return SFB_OK;
@@ -2269,7 +2368,22 @@ SFB_API int sfb_get_kernels(const sfb_context *cctx, int which, double *host, si
   sfb_context *ctx = const_cast<sfb_context *>(cctx);
   if (!ctx || !host) return SFB_E_INVALID;
   return guarded(ctx, [&]() {
-    if (which < 0 || which > 5) throw std::invalid_argument("kernel selector must be in [0, 5]");
+    if (which < 0 || which > 7) throw std::invalid_argument("kernel selector must be in [0, 7]");
+    if (which >= 6) {
+      // Stacey-traction derivatives, dchi/d(rho vp) and dchi/d(rho vs)
+      if (!ctx->kern_b.p) throw StateError("no Stacey-traction kernels have been accumulated (sfb_set_stacey_kernels)");
+      const Assembly &a = ctx->P.asmb;
+      const size_t nloc = a.nloc();
+      const int nn = a.ngll * a.ngll;
+      if (count < nloc) throw std::invalid_argument("kernel buffer too small ([nspec][ngll][ngll])");
+      std::vector<double> k(nloc * 2);
+      ck(cudaStreamSynchronize(ctx->stream), "sync");
+      ck(cudaMemcpy(k.data(), ctx->kern_b.p, k.size() * sizeof(double), cudaMemcpyDeviceToHost), "kernels d2h");
+      for (int e = 0; e < a.nspec; ++e)
+        for (int q = 0; q < nn; ++q)
+          host[static_cast<size_t>(e) * nn + q] = k[(static_cast<size_t>(ctx->inv[e]) * nn + q) * 2 + (which - 6)];
+      return SFB_OK;
+    }
     const Assembly &a = ctx->P.asmb;
     const size_t nloc = a.nloc();
     const int nn = a.ngll * a.ngll;

@@ -2277,6 +2277,53 @@ k_frechet(Static st, MediumFields A, MediumFields B, int S, real dt, double *ker
   }
 }
 
+// Model derivative of the Stacey traction, which the reference's kernels
+// leave out (frechet_derivative.hpp:14-138 has no boundary term).  With the
+// kernels' convention dchi/dm = dt sum_steps s_adj . d(force)/dm and the P-SV
+// Stacey force -w |n| [(rho vp - rho vs)(v.n^)n^ + rho vs v]
+// (stacey.tpp:41-75), per Stacey point of a P-SV element
+//   kb[p][0] += -dt w |n| (s_adj.n^)(v.n^)              dchi / d(rho vp)
+//   kb[p][1] += -dt w |n| (s_adj.v - (s_adj.n^)(v.n^))  dchi / d(rho vs)
+// summed over the shots, with v the backward wavefield's velocity at the end
+// of the step: the field value plus vcorr * force * M^-1 when the update
+// has not run yet (the implicit dt/2 mass term makes the damping act on the
+// corrected velocity).
+template <int N>
+__global__ void k_stacey_frechet(Static st, MediumFields A, MediumFields B, int S, real dt, real vcorr,
+                                 double *kb) {
+  constexpr int NN = N * N;
+  const size_t total = static_cast<size_t>(A.nelem) * NN;
+  for (size_t t = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; t < total;
+       t += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const int e = A.elem_begin + static_cast<int>(t / NN);
+    if (!(st.eflag[e] & 1)) continue;
+    const size_t p = static_cast<size_t>(e) * NN + t % NN;
+    if (!(st.bnd[p] & 1)) continue;
+    const int g = st.iglob[p];
+    const real nx = st.bnd_nx[p], nz = st.bnd_nz[p], we = st.bnd_w[p];
+    const real jac1d = msqrt(nx * nx + nz * nz);
+    const real ux = nx / jac1d, uz = nz / jac1d;
+    double k0 = 0.0, k1 = 0.0;
+    for (int s = 0; s < S; ++s) {
+      const size_t base = (static_cast<size_t>(g) * S + s) * 2;
+      real vx = B.v[base], vz = B.v[base + 1];
+      if (vcorr != real(0)) {
+        vx += vcorr * B.a[base] * B.minv[static_cast<size_t>(g) * 2];
+        vz += vcorr * B.a[base + 1] * B.minv[static_cast<size_t>(g) * 2 + 1];
+      }
+      const real ax = A.u[base], az = A.u[base + 1];
+      const double an = static_cast<double>(ax) * ux + static_cast<double>(az) * uz;
+      const double vn = static_cast<double>(vx) * ux + static_cast<double>(vz) * uz;
+      const double av = static_cast<double>(ax) * vx + static_cast<double>(az) * vz;
+      k0 += an * vn;
+      k1 += av - an * vn;
+    }
+    const double f = -static_cast<double>(dt) * we * jac1d;
+    kb[p * 2 + 0] += f * k0;
+    kb[p * 2 + 1] += f * k1;
+  }
+}
+
 // Mass matrix (compute_mass_matrix.tpp:80-113) accumulated in FP64.
 template <int MED>
 __global__ void k_mass(Static st, MediumFields f, int N, real dt) {
@@ -2591,6 +2638,14 @@ void launch_frechet(int medium, int ngll, const Static &st, const MediumFields &
     if (medium == MED_PSV) k_frechet<MED_PSV, 8, EPB><<<grid, EPB * 64, 0, stream>>>(st, adj, bwd, nshots, dt, kern, a_is_force);
     else if (medium == MED_AC) k_frechet<MED_AC, 8, EPB><<<grid, EPB * 64, 0, stream>>>(st, adj, bwd, nshots, dt, kern, a_is_force);
   }
+}
+
+void launch_stacey_frechet(int ngll, const Static &st, const MediumFields &adj, const MediumFields &bwd, int nshots,
+                           real dt, real vcorr, double *kb, cudaStream_t stream) {
+  if (adj.nelem == 0) return;
+  const size_t n = static_cast<size_t>(adj.nelem) * ngll * ngll;
+  if (ngll == 5) k_stacey_frechet<5><<<grid_for(n, 256), 256, 0, stream>>>(st, adj, bwd, nshots, dt, vcorr, kb);
+  else if (ngll == 8) k_stacey_frechet<8><<<grid_for(n, 256), 256, 0, stream>>>(st, adj, bwd, nshots, dt, vcorr, kb);
 }
 
 void launch_nonfinite_check(const real *p, size_t n, int *err, cudaStream_t stream) {

@@ -325,6 +325,12 @@ void launch_mass(int medium, int ngll, const Static &st, const MediumFields &f, 
                  cudaStream_t stream);
 void launch_invert_mass(const MediumFields &f, cudaStream_t stream);
 void launch_zero(real *p, size_t n, cudaStream_t stream);
+// Stacey-traction model derivatives of the P-SV medium (see k_stacey_frechet)
+// into kb[p][2] (FP64, device element order): dchi/d(rho vp), dchi/d(rho vs).
+// vcorr: 0 when bwd.v is the step's final velocity, else the factor of
+// force * M^-1 that completes it (-dt/2 for the backward run's update).
+void launch_stacey_frechet(int ngll, const Static &st, const MediumFields &adj, const MediumFields &bwd, int nshots,
+                           real dt, real vcorr, double *kb, cudaStream_t stream);
 // Error word bits: 1 a bounded device wait expired, 2 a non-finite value.
 constexpr int kErrWaitTimeout = 1, kErrNonFinite = 2;
 // Sets kErrNonFinite in *err when any of p[0, n) is NaN or infinite.

@@ -169,12 +169,49 @@ const char *field_name(int m, int which) {
 
 }  // namespace
 
-void write_forward_wavefield(const Problem &P, const std::string &dir, const ForwardSnapshot &s) {
+namespace {
+// Media the reference's wavefield writer and reader visit besides the three
+// this library computes (include/io/wavefield/{writer,reader}.tpp): their
+// groups are written empty, with the reference's component counts
+// (enumerations/medium.hpp: poroelastic 4, elastic_psv_t 3).
+struct ExtraMedium {
+  const char *name;
+  int ncomp;
+};
+constexpr ExtraMedium kExtraMedia[2] = {{"poroelastic", 4}, {"elastic_psv_t", 3}};
+
+// The reference's Stacey store (compute/boundary_values/*): per medium with a
+// container (elastic_psv, acoustic) the elements whose boundary tag is
+// stacey, numbered in mesh order (IndexMapping, -1 elsewhere); values
+// (nelements, nz, nx, nstep, ncomp) column-major.  `slot` gives this
+// library's store slot per mesh element (exactly those elements; SH
+// elements have no reference container and are left out).
+struct RefStacey {
+  std::vector<int> mapping;  // [nspec]
+  long count[4] = {0, 0, 0, 0};
+};
+RefStacey ref_stacey(const Assembly &a, const std::vector<int> &slot) {
+  RefStacey r;
+  r.mapping.assign(a.nspec, -1);
+  for (int e = 0; e < a.nspec; ++e) {
+    const int m = a.medium[e];
+    if (slot[e] < 0 || m == MEDIUM_ELASTIC_SH) continue;
+    r.mapping[e] = static_cast<int>(r.count[m]++);
+  }
+  return r;
+}
+}  // namespace
+
+void write_forward_wavefield(const Problem &P, const std::string &dir, const ForwardSnapshot &s, bool fresh) {
   const Assembly &a = P.asmb;
   const int n = a.ngll, nn = n * n;
-  const std::string root = ascii_group((fs::path(dir) / "ForwardWavefield").string());
-  const std::string coords = ascii_group((fs::path(root) / "Coordinates").string());
+  const fs::path rootp = fs::path(dir) / "ForwardWavefield";
+  // a fresh file starts empty; a periodic snapshot adds its step group
+  const std::string root = fresh ? ascii_group(rootp.string()) : (fs::create_directories(rootp), rootp.string());
+  const bool coordinates = fresh || !fs::exists(rootp / "Coordinates");
+  const std::string coords = coordinates ? ascii_group((rootp / "Coordinates").string()) : std::string();
   for (int m : kMediaTags) {
+    if (!coordinates) break;
     const std::string g = ascii_group((fs::path(coords) / medium_name(m)).string());
     const std::vector<int> el = medium_elements(a, m);
     const long ne = static_cast<long>(el.size()), ng = a.nglob[m];
@@ -193,6 +230,13 @@ void write_forward_wavefield(const Problem &P, const std::string &dir, const For
     ascii_write(g, "Z", {ng}, z.data(), z.size());
     ascii_write(g, "mapping", {ne, n, n}, mapping.data(), mapping.size());
   }
+  for (const ExtraMedium &x : kExtraMedia) {
+    if (!coordinates) break;
+    const std::string g = ascii_group((fs::path(coords) / x.name).string());
+    ascii_write(g, "X", {0}, static_cast<const float *>(nullptr), 0);
+    ascii_write(g, "Z", {0}, static_cast<const float *>(nullptr), 0);
+    ascii_write(g, "mapping", {0, n, n}, static_cast<const int *>(nullptr), 0);
+  }
   const std::string step = ascii_group((fs::path(root) / step_group(s.step)).string());
   for (int m : kMediaTags) {
     const std::string g = ascii_group((fs::path(step) / medium_name(m)).string());
@@ -203,30 +247,45 @@ void write_forward_wavefield(const Problem &P, const std::string &dir, const For
       ascii_write(g, field_name(m, w), {ng, nc}, f.data(), f.size());  // [c][g] = (nglob, ncomp) column-major
     }
   }
+  for (const ExtraMedium &x : kExtraMedia) {
+    const std::string g = ascii_group((fs::path(step) / x.name).string());
+    for (int w = 0; w < 3; ++w) ascii_write(g, field_name(0, w), {0, x.ncomp}, static_cast<const float *>(nullptr), 0);
+  }
   const std::string stacey =
       ascii_group((fs::path(ascii_group((fs::path(step) / "Boundary").string())) / "Stacey").string());
-  ascii_write(stacey, "IndexMapping", {static_cast<long>(a.nspec)}, s.slot.data(), s.slot.size());
+  const RefStacey r = ref_stacey(a, s.slot);
+  ascii_write(stacey, "IndexMapping", {static_cast<long>(a.nspec)}, r.mapping.data(), r.mapping.size());
   const long T = P.nstep, K = s.nstacey;
-  std::vector<float> v(static_cast<size_t>(K) * nn * T * 2);
-  if (!s.store.empty()) {
-    if (s.store.size() != v.size()) throw std::invalid_argument("snapshot store has the wrong size");
-    for (long t = 0; t < T; ++t)
-      for (long k = 0; k < K; ++k)
-        for (int iz = 0; iz < n; ++iz)
-          for (int ix = 0; ix < n; ++ix)
-            for (int c = 0; c < 2; ++c)
-              v[k + K * (iz + n * (ix + static_cast<size_t>(n) * (t + T * c)))] =
-                  s.store[(((static_cast<size_t>(t) * K + k) * nn) + iz * n + ix) * 2 + c];
+  if (!s.store.empty() && s.store.size() != static_cast<size_t>(T) * K * nn * 2)
+    throw std::invalid_argument("snapshot store has the wrong size");
+  for (const auto &[m, name] : {std::pair<int, const char *>{MEDIUM_ELASTIC_PSV, "ElasticAcceleration"},
+                                std::pair<int, const char *>{MEDIUM_ACOUSTIC, "AcousticAcceleration"}}) {
+    const long ne = r.count[m], nc = a.ncomp(m);
+    std::vector<float> v(static_cast<size_t>(ne) * nn * T * nc, 0.f);
+    if (!s.store.empty())
+      for (int e = 0; e < a.nspec; ++e) {
+        if (a.medium[e] != m || r.mapping[e] < 0) continue;
+        const long i = r.mapping[e], k = s.slot[e];
+        for (long t = 0; t < T; ++t)
+          for (int iz = 0; iz < n; ++iz)
+            for (int ix = 0; ix < n; ++ix)
+              for (int c = 0; c < nc; ++c)
+                v[i + ne * (iz + n * (ix + static_cast<size_t>(n) * (t + T * c)))] =
+                    s.store[(((static_cast<size_t>(t) * K + k) * nn) + iz * n + ix) * 2 + c];
+      }
+    ascii_write(stacey, name, {ne, n, n, T, nc}, v.data(), v.size());
   }
-  ascii_write(stacey, "ElementAcceleration", {K, n, n, T, 2}, v.data(), v.size());
+  ascii_write(stacey, "PoroelasticAcceleration", {0, n, n, T, 4}, static_cast<const float *>(nullptr), 0);
 }
 
-ForwardSnapshot read_forward_wavefield(const Problem &P, const std::string &dir, int nstacey) {
+ForwardSnapshot read_forward_wavefield(const Problem &P, const std::string &dir, const std::vector<int> &slot,
+                                       int nstacey) {
   const Assembly &a = P.asmb;
   const int n = a.ngll, nn = n * n;
   ForwardSnapshot s;
   s.step = P.nstep;
   s.nstacey = nstacey;
+  s.slot = slot;
   const fs::path step = fs::path(dir) / "ForwardWavefield" / step_group(P.nstep);
   if (!fs::exists(step)) throw std::runtime_error("no forward wavefield at " + step.string());
   for (int m : kMediaTags) {
@@ -239,17 +298,27 @@ ForwardSnapshot read_forward_wavefield(const Problem &P, const std::string &dir,
   }
   const std::string stacey = (step / "Boundary" / "Stacey").string();
   const std::vector<double> map = ascii_read(stacey, "IndexMapping", {static_cast<long>(a.nspec)});
-  s.slot.assign(map.begin(), map.end());
+  const RefStacey r = ref_stacey(a, slot);
+  for (int e = 0; e < a.nspec; ++e)
+    if (static_cast<int>(map[e]) != r.mapping[e])
+      throw std::runtime_error("the stored boundary layout does not match this mesh");
   const long T = P.nstep, K = nstacey;
-  const std::vector<double> v = ascii_read(stacey, "ElementAcceleration", {K, n, n, T, 2});
   s.store.assign(static_cast<size_t>(T) * K * nn * 2, 0.f);
-  for (long t = 0; t < T; ++t)
-    for (long k = 0; k < K; ++k)
-      for (int iz = 0; iz < n; ++iz)
-        for (int ix = 0; ix < n; ++ix)
-          for (int c = 0; c < 2; ++c)
-            s.store[(((static_cast<size_t>(t) * K + k) * nn) + iz * n + ix) * 2 + c] =
-                static_cast<float>(v[k + K * (iz + n * (ix + static_cast<size_t>(n) * (t + T * c)))]);
+  for (const auto &[m, name] : {std::pair<int, const char *>{MEDIUM_ELASTIC_PSV, "ElasticAcceleration"},
+                                std::pair<int, const char *>{MEDIUM_ACOUSTIC, "AcousticAcceleration"}}) {
+    const long ne = r.count[m], nc = a.ncomp(m);
+    const std::vector<double> v = ascii_read(stacey, name, {ne, n, n, T, nc});
+    for (int e = 0; e < a.nspec; ++e) {
+      if (a.medium[e] != m || r.mapping[e] < 0) continue;
+      const long i = r.mapping[e], k = slot[e];
+      for (long t = 0; t < T; ++t)
+        for (int iz = 0; iz < n; ++iz)
+          for (int ix = 0; ix < n; ++ix)
+            for (int c = 0; c < nc; ++c)
+              s.store[(((static_cast<size_t>(t) * K + k) * nn) + iz * n + ix) * 2 + c] =
+                  static_cast<float>(v[i + ne * (iz + n * (ix + static_cast<size_t>(n) * (t + T * c)))]);
+    }
+  }
   return s;
 }
 

@@ -23,28 +23,36 @@ void ascii_write(const std::string &group, const std::string &name, const std::v
 std::vector<double> ascii_read(const std::string &group, const std::string &name, const std::vector<long> &dims);
 
 // One shot's forward state for the combined run: the fields after the last
-// step (per medium tag, [ncomp][nglob]: u, v, a) and this library's
-// boundary store (whole-element contributions of the Stacey elements per
-// step; slot per reference element in `slot`, -1 where none).
+// step (per medium tag, [ncomp][nglob]: u, v, a) and the boundary store:
+// the element-local accelerations of the elements whose boundary tag is
+// stacey (not composite Stacey / Dirichlet), per step; `slot` gives each
+// mesh element's slot, -1 where none.
 struct ForwardSnapshot {
   int step = 0;
   std::vector<float> field[4][3];
   std::vector<int> slot;        // [nspec]
   int nstacey = 0;
-  std::vector<float> store;     // [nstep][nstacey][ngll*ngll][2] (device order)
+  std::vector<float> store;     // [nstep][nstacey][ngll*ngll][2] (slot order)
 };
 
 // <dir>/ForwardWavefield/{Coordinates,StepNNNNNN} as the reference's
 // wavefield writer lays it out (include/io/wavefield/writer.tpp:14-150):
 // Coordinates/<medium>/{X,Z,mapping}; StepNNNNNN/<medium>/{Displacement,
 // Velocity,Acceleration} (acoustic: Potential, PotentialDot,
-// PotentialDotDot), [nglob][ncomp] column-major; StepNNNNNN/Boundary/Stacey/
-// {IndexMapping, ElementAcceleration [nstacey][nz][nx][nstep][2]
-// column-major}.  The reference stores the Stacey traction alone under
-// ElasticAcceleration / AcousticAcceleration; this library replays whole
-// element contributions, so its store has its own dataset name.
-void write_forward_wavefield(const Problem &P, const std::string &dir, const ForwardSnapshot &s);
-ForwardSnapshot read_forward_wavefield(const Problem &P, const std::string &dir, int nstacey);
+// PotentialDotDot), [nglob][ncomp] column-major, with empty groups for the
+// poroelastic and elastic_psv_t media the reference also visits;
+// StepNNNNNN/Boundary/Stacey/{IndexMapping, ElasticAcceleration,
+// AcousticAcceleration, PoroelasticAcceleration}: the reference's Stacey
+// containers (compute/boundary_values/*): per medium the stacey-tagged
+// elements in mesh order, values (nelements, nz, nx, nstep, ncomp)
+// column-major.  Files written by either program are read by the other.
+// fresh: start the file anew (coordinates and this step); otherwise add or
+// replace this step's group (periodic snapshots, time_interval).
+void write_forward_wavefield(const Problem &P, const std::string &dir, const ForwardSnapshot &s, bool fresh = true);
+// `slot`: this context's store slot per mesh element (the layout the file
+// must match).
+ForwardSnapshot read_forward_wavefield(const Problem &P, const std::string &dir, const std::vector<int> &slot,
+                                       int nstacey);
 
 // <dir>/Kernels/<medium>_isotropic/{X, Z, rho, mu, kappa, rhop, alpha, beta}
 // (acoustic: rho, kappa, rhop, alpha), include/io/kernel/writer.tpp and

@@ -395,8 +395,20 @@ Problem problem_from_nodes(std::shared_ptr<YNode> root, std::shared_ptr<YNode> d
       P.seismogram_dir = d ? d->str() : ".";
     }
     if (const YNode *w = mode->path({"forward", "writer", "wavefield"})) {
+      // src/parameter_parser/writer/wavefield.cpp:10-76: the folder must
+      // exist (default: the working directory); time_interval and the
+      // (parsed, otherwise unused) time_interval_by_memory exclude each
+      // other; include_last_step defaults to true
       P.save_boundary_values = true;
-      if (const YNode *d = w->get("directory")) P.wavefield_dir = d->str();
+      const YNode *d = w->get("directory");
+      P.wavefield_dir = d ? d->str() : ".";
+      if (!std::filesystem::is_directory(P.wavefield_dir))
+        throw std::runtime_error("Output folder : " + P.wavefield_dir + " does not exist.");
+      if (const YNode *t = w->get("time_interval")) P.wavefield_time_interval = t->integer();
+      if (w->get("time_interval_by_memory") && P.wavefield_time_interval != 0)
+        throw std::runtime_error("time_interval and time_interval_by_memory cannot be used simultaneously");
+      if (const YNode *l = w->get("include_last_step")) P.wavefield_include_last_step = l->boolean();
+      if (P.wavefield_time_interval < 0) throw std::runtime_error("time_interval must be >= 0");
     }
   }
 

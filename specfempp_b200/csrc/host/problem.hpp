@@ -36,6 +36,11 @@ struct Problem {
   std::string seismogram_dir;
   bool write_seismograms = false;
   std::string wavefield_dir;   // forward: writer.wavefield; combined: reader
+  // forward writer.wavefield: a snapshot every time_interval steps (0: none)
+  // and one of the last step when include_last_step
+  // (src/parameter_parser/writer/wavefield.cpp:36-66)
+  int wavefield_time_interval = 0;
+  bool wavefield_include_last_step = true;
   std::string kernel_dir;      // combined: writer.kernels
   // databases.writer.properties / databases.reader.properties (ASCII):
   // 1 write the model under property_dir and stop (the reference's driver

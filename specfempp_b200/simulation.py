@@ -299,6 +299,11 @@ class Simulation:
         recorded device errors (SfbError)."""
         self._check(self._lib.sfb_synchronize(self._h))
 
+    def set_stacey_kernels(self, enable: bool = True):
+        """Also accumulate the Stacey traction's model derivatives in combined
+        runs (kernels 6, 7: dchi/d(rho vp), dchi/d(rho vs))."""
+        self._check(self._lib.sfb_set_stacey_kernels(self._h, 1 if enable else 0))
+
     def set_deterministic(self, enable: bool = True):
         """Bit-reproducible assembly (element colours, fixed-order sums);
         before the first device use."""

@@ -28,3 +28,45 @@ def test_oracle_adjoint_gradient_matches_finite_differences(absorb, tol, native_
         fd = misfit_fd_oracle(model, obs, NSTEP, absorb, d)
         ad = sum(float(np.sum(g * dd)) for g, dd in zip(grads, d))
         assert abs(ad - fd) <= tol * abs(fd), (trial, ad, fd)
+
+
+def test_stacey_traction_derivative_completes_the_gradient(native_lib, oracle_lib):
+    """All sides absorbing, waves crossing the boundaries many times (1500
+    steps on the 1 km model): the reference's kernels leave out the Stacey
+    traction's model derivative and miss the finite difference by 0.3-1.1 %;
+    with the derivative (dchi/d(rho vp), dchi/d(rho vs) at the boundary
+    points) the gradient is the discrete misfit's own (FP64, directional
+    derivatives from the perturbation the FP32 model arrays hold)."""
+    from oracle import bridge
+    from specfempp_b200 import Simulation
+    nstep = 1500
+    absorb = (True,) * 4
+    p, model, XZ = base_model(nstep=nstep)
+    obs = observed(anomaly(model, XZ, p), nstep, absorb)
+    m32 = [a.astype(np.float32) for a in model]
+    sim = Simulation.structured(problem(m32, nstep, absorb))
+    fwd = bridge.forward(sim, 64, threads=8, want_fields=True, want_stacey=True, exact=True)
+    res = fwd["seismograms"][:, 0] - obs[0]
+    K, KB = bridge.combined(sim, res.astype(np.float32), fwd, precision=64, threads=8, exact=True,
+                            stacey_kernels=True)
+    m64 = [a.astype(np.float64) for a in m32]
+    g = kernel_gradient(sim, K, m64)
+    rho, vp, vs = m64
+    gb = (g[0] + vp * KB[..., 0] + vs * KB[..., 1], g[1] + rho * KB[..., 0], g[2] + rho * KB[..., 1])
+
+    def misfit(m):
+        s = Simulation.structured(problem(m, nstep, absorb))
+        syn = bridge.forward(s, 64, threads=8, exact=True)["seismograms"][:, 0]
+        return 0.5 * np.sum((syn - obs[0]) ** 2) * s.info().dt
+
+    for trial in range(2):
+        d = directions(m64, XZ, trial)
+        mp = [(m + 1e-4 * dd).astype(np.float32) for m, dd in zip(m64, d)]
+        mm = [(m - 1e-4 * dd).astype(np.float32) for m, dd in zip(m64, d)]
+        fd = misfit(mp) - misfit(mm)
+        dm = [a.astype(np.float64) - b.astype(np.float64) for a, b in zip(mp, mm)]
+        ref = sum(float(np.sum(x * y)) for x, y in zip(g, dm))
+        full = sum(float(np.sum(x * y)) for x, y in zip(gb, dm))
+        print("trial %d: reference kernels / FD %.6f, with the Stacey term %.6f" % (trial, ref / fd, full / fd))
+        assert abs(full / fd - 1.0) <= 1e-5
+        assert abs(ref / fd - 1.0) > 1e-3  # the term matters on this problem

@@ -16,9 +16,12 @@ Checks, through the C ABI:
     restated in FP64 and pinned to the FP64 oracle at 1e-10).
 The reference's kernels leave out the Stacey traction's own dependence on
 the model (include/medium/dim2/elastic/isotropic/frechet_derivative.hpp:
-14-138); the FD check reports how far that leaves the gradient from the
-misfit's derivative on this all-absorbing configuration, and the same
-check with free boundaries shows the gradient where no such term exists.
+14-138): on this all-absorbing configuration, with sources and receivers
+250 m inside the boundaries, that gradient misses the finite differences
+by up to a few per cent (reported).  With the Stacey-traction derivative
+(WaveformMisfit boundary_term) the gradient must meet the 1e-3 bar on every
+direction; with free boundaries, where no such term exists, the reference's
+gradient must.
 """
 import numpy as np
 import pytest
@@ -85,7 +88,7 @@ def observed64(p):
     return obs
 
 
-def run_case(absorb, ndir, checkpoint=500):
+def run_case(absorb, ndir, checkpoint=500, boundary_term=False):
     p = W.adjoint_model(1.0)
     p.absorb = absorb
     p.save_boundary_values = True
@@ -100,22 +103,33 @@ def run_case(absorb, ndir, checkpoint=500):
     chi.backward()
     grads = [t.grad.numpy() for t in params]
     K32 = np.stack([sim.kernels(q) for q in range(3)], axis=-1)
+    grads_b = None
+    if boundary_term:
+        params = [torch.tensor(a, dtype=torch.float64, requires_grad=True) for a in model]
+        chi = WaveformMisfit.apply(*params, sim, torch.from_numpy(obs), True)
+        chi.backward()
+        grads_b = [t.grad.numpy() for t in params]
     rows = []
     for k, d in enumerate(smooth_directions(p, ndir)):
         mp = [(m * (1 + H * dd)).astype(np.float32) for m, dd in zip(model, d)]
         mm = [(m * (1 - H * dd)).astype(np.float32) for m, dd in zip(model, d)]
         fd = misfit64(p, mp, obs) - misfit64(p, mm, obs)
-        ad = sum(float(np.sum(g * (a.astype(np.float64) - b.astype(np.float64)))) for g, a, b in zip(grads, mp, mm))
-        rows.append((k, ad, fd, ad / fd))
-        print("absorb=%s direction %2d: adjoint %.8e FD %.8e ratio %.6f" % (absorb, k, ad, fd, ad / fd))
+        dm = [a.astype(np.float64) - b.astype(np.float64) for a, b in zip(mp, mm)]
+        ad = sum(float(np.sum(g * x)) for g, x in zip(grads, dm))
+        adb = sum(float(np.sum(g * x)) for g, x in zip(grads_b, dm)) if grads_b else float("nan")
+        rows.append((k, ad, fd, ad / fd, adb / fd))
+        print("absorb=%s direction %2d: adjoint %.8e FD %.8e ratio %.6f; with the Stacey term %.6f"
+              % (absorb, k, ad, fd, ad / fd, adb / fd))
     return sim, p, obs, K32, rows
 
 
 def test_config4_gradient_all_stacey():
-    sim, p, obs, K32, rows = run_case((True,) * 4, NDIR)
+    sim, p, obs, K32, rows = run_case((True,) * 4, NDIR, boundary_term=True)
     dev = max(abs(r[3] - 1.0) for r in rows)
-    print("all-Stacey: largest |adjoint / FD - 1| over %d directions: %.3e (north-star bar 1e-3: %s)"
-          % (NDIR, dev, "met" if dev <= 1e-3 else "not met"))
+    devb = max(abs(r[4] - 1.0) for r in rows)
+    print("all-Stacey: largest |adjoint / FD - 1| over %d directions: reference kernels %.3e, with the Stacey "
+          "term %.3e (north-star bar 1e-3)" % (NDIR, dev, devb))
+    assert devb <= 1e-3
     # kernels against the FP64 build's (the reference's kernels in FP64)
     model = [a.astype(np.float32) for a in p.gll_model]
     s64 = Simulation.structured(p, precision=64)

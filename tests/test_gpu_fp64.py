@@ -301,3 +301,31 @@ def test_fp64_checkpointed_combined_keeps_kernels():
         e = rel_l2(K[..., c], ref[..., c])
         print("checkpointed kernel %d: FP64 rel-L2 vs FP64 oracle %.2e" % (c, e))
         assert e <= BAR
+
+
+def test_fp64_stacey_traction_kernels():
+    """The Stacey-traction model derivatives (sfb_set_stacey_kernels) of the
+    FP64 build against the oracle's, all sides absorbing."""
+    from oracle import bridge
+    nstep = 600
+    absorb = (True,) * 4
+    p, model, XZ = base_model(nshots=2, nstep=nstep)
+    obs = observed(anomaly(model, XZ, p), nstep, absorb, nshots=2)
+    sim = Simulation.structured(problem(model, nstep, absorb, 2), precision=64)
+    sim.set_stacey_kernels(True)
+    sim.run_forward()
+    stfs = []
+    for s in range(2):
+        stf = (sim.seismograms(shot=s)[:, 0] - obs[s]).astype(np.float32)
+        stfs.append(stf)
+        sim.set_adjoint_sources(stf, shot=s)
+    sim.run_combined()
+    ref = None
+    for s in range(2):
+        fwd = exact(sim, s, fields=True, stacey=True)
+        _, kb = bridge.combined(sim, stfs[s], fwd, precision=64, shot=s, threads=8, exact=True, stacey_kernels=True)
+        ref = kb if ref is None else ref + kb
+    for q in (0, 1):
+        e = rel_l2(sim.kernels(6 + q), ref[..., q])
+        print("Stacey-traction kernel %d: FP64 build vs FP64 oracle %.2e" % (q, e))
+        assert np.abs(ref[..., q]).max() > 0 and e <= BAR
