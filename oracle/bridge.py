@@ -28,8 +28,8 @@ def build():
 def load():
     global _lib
     if _lib is None:
-        src = os.path.join(HERE, "oracle.cpp")
-        if not os.path.exists(LIB) or os.path.getmtime(src) > os.path.getmtime(LIB):
+        srcs = [os.path.join(HERE, f) for f in ("oracle.cpp", "oracle3d.cpp")]
+        if not os.path.exists(LIB) or max(os.path.getmtime(f) for f in srcs) > os.path.getmtime(LIB):
             build()
         lib = C.CDLL(LIB)
         lib.oracle_forward.restype = C.c_int

@@ -49,7 +49,7 @@ def _sources():
 
 
 def _headers():
-    out = [os.path.join(ROOT, "include", "specfem_b200.h")]
+    out = [os.path.join(ROOT, "include", h) for h in ("specfem_b200.h", "specfem_b200_3d.h")]
     for sub in ("host", "cuda"):
         d = os.path.join(CSRC, sub)
         out += [os.path.join(d, f) for f in os.listdir(d) if f.endswith((".hpp", ".cuh", ".h"))]

