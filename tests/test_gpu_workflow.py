@@ -75,7 +75,11 @@ def test_two_phase_workflow_matches_in_memory(tmp_path, monkeypatch):
         print("kernel %s from files: vs FP32 oracle %.2e, vs FP64 %.2e (FP32 oracle vs FP64 %.2e); "
               "vs a second GPU run %.2e" % (name, e32, e64, eref, spread))
         assert np.abs(k).max() > 0
-        assert spread <= 1e-9, (name, spread)  # the files' ten digits
+        # both runs are deterministic; the file-driven run applies the
+        # adjoint sources as sources-file entries (located as sources), the
+        # in-memory run through the array API (located as receivers), whose
+        # Lagrange weights may differ in the last bit
+        assert spread <= 1e-6, (name, spread)
         # cross-correlation traveltime kernels cancel heavily over time: the
         # FP32 oracle alone is 0.3-0.5 % from FP64 here, and the adjoint
         # sources come from this run's own seismograms.  Numerical parity is
