@@ -8,12 +8,17 @@ The metric is GLL point updates per second: nshots * nglob * steps / time,
 nglob summed over media.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload coupled|plain|batched] [--no-secondary]
+                  [--workload coupled|plain|batched|hex3d] [--no-secondary]
 
 On one GPU the default line also carries `batched` (the 64-shot 800 x 400
 batched forward: rate and whole-step HBM fraction) and `fwi` (forward +
 adjoint gradient of 64 shots batched against one shot alone on the
 200 x 200 adjoint mesh: per-shot device time and speed-up).
+
+`--workload hex3d` times the 3D batched elastic forward on config 5's
+hexahedral mesh (16 shots; `--scale` shrinks the element counts) and
+reports its stiffness launch against max(bytes / HBM peak, flops / FP32
+peak).
 
 Under torchrun each rank runs an independent replica (the forward path does
 not shard; "replicas only"); the reported value sums all ranks' point updates
@@ -521,13 +526,148 @@ def run_ours(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# 3D batched elastic forward (config 5's mesh, model, shots and receivers)
+FP32_FLOPS_PER_POINT_SHOT = 250  # stiffness arithmetic per local point and shot (see hex3d_flops)
+
+
+def hex3d_stiffness_bytes(info):
+    """Algorithmic bytes of one 3D stiffness launch: per local point the
+    global index, kappa and mu (12 B), per element the geometry (16 B), and
+    per global point and shot one read of the displacement and one write
+    of the force (2 x 12 B)."""
+    return info.nspec * 125 * 12 + info.nspec * 16 + info.nshots * info.nglob * 24
+
+
+def hex3d_flops(info):
+    """FP32 operations of one 3D stiffness launch: per local point and shot
+    the three directional derivatives (45 FMA), the strain-stress map and
+    F = J T dxi/dx (about 50), the weak divergence (45 FMA) and the weights
+    (about 20): 250."""
+    return FP32_FLOPS_PER_POINT_SHOT * info.nspec * 125 * info.nshots
+
+
+def hex3d_step_bytes(info):
+    """Algorithmic bytes of one 3D forward step: the stiffness launch, the
+    Newmark update (per global point and shot u, v, force read, u, v
+    written, force zeroed: 6 x 12 B; the inverse mass 12 B per point) and
+    the Stacey points (velocity read, force read and written: 3 x 12 B per
+    point and shot, 16 B per point of static data)."""
+    return (hex3d_stiffness_bytes(info) + info.nshots * info.nglob * 72 + info.nglob * 12
+            + info.nboundary_points * (info.nshots * 36 + 16))
+
+
+def fp32_peak_tflops():
+    """Nominal FP32 FMA throughput of the 148 SMs (128 lanes each) at the
+    maximum SM clock (MEASURED_PEAKS.json sm_max_mhz, else 1965 MHz)."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            mhz = float(json.load(f).get("sm_max_mhz", 1965.0))
+    except Exception:
+        mhz = 1965.0
+    return 148 * 128 * 2 * mhz * 1e6 / 1e12
+
+
+def hex3d_cpu_rate(budget_s, threads):
+    """The 3D oracle (FP32, OpenMP over elements) on an eighth of config 5's
+    elements per axis (one shot), timed over as many steps as fit in about
+    `budget_s` seconds: GLL point updates per second."""
+    from oracle import bridge3d
+    from specfempp_b200.hex3d import config5_problem
+    probe = config5_problem(scale=0.125, nstep=4, nshots=1, nrec=16, save_boundary_values=False)
+    t0 = time.perf_counter()
+    bridge3d.forward(probe, 0, 32, threads=threads, want_store=False)
+    per_step = (time.perf_counter() - t0) / 4
+    n = max(4, int(budget_s / max(per_step, 1e-6)))
+    p = config5_problem(scale=0.125, nstep=n, nshots=1, nrec=16, save_boundary_values=False)
+    t0 = time.perf_counter()
+    bridge3d.forward(p, 0, 32, threads=threads, want_store=False)
+    dt = time.perf_counter() - t0
+    nglob = (4 * p.nx + 1) * (4 * p.ny + 1) * (4 * p.nz + 1)
+    return nglob * n / dt, n, dt, (p.nx, p.ny, p.nz)
+
+
+def run_hex3d(args):
+    """3D batched forward: config 5's mesh (96 x 96 x 48 hexahedra at full
+    scale), model, 16 shots and 1000 receivers; K forward steps timed with
+    CUDA events on the context's stream (sfb3_time_kernel)."""
+    import torch
+    from specfempp_b200.hex3d import Simulation3D, config5_problem
+    torch.cuda.set_device(env_int("LOCAL_RANK", 0))
+    K, Wm = args.steps, args.warmup
+    p = config5_problem(scale=SCALE, nstep=Wm + 2 * K + 1, save_boundary_values=False)
+    sim = Simulation3D(p)
+    info = sim.info()
+    sim.run_forward(Wm)
+    launches0 = sim.info().kernel_launches
+    sampler = ClockSampler(env_int("LOCAL_RANK", 0))
+    torch.cuda.synchronize()
+    sampler.start()
+    ms = sim.time_kernel(3, K)           # mean per step over K steps
+    clocks = sampler.stop()
+    launches = sim.info().kernel_launches - launches0
+    pts = info.nglob * info.nshots
+    value = pts / (ms / 1000.0)
+    # end to end through the public API: K steps and every shot's
+    # seismograms read back to the host (synchronous calls, wall clock)
+    t0 = time.perf_counter()
+    sim.run_forward(K)
+    seis = [sim.seismograms(shot=s) for s in range(info.nshots)]
+    t_e2e = time.perf_counter() - t0
+    d2h = sum(a.nbytes for a in seis)
+    ms_stiff = sim.time_kernel(0, 5)
+    ms_newmark = sim.time_kernel(1, 5)
+    peak, peak_kind = measured_peak()
+    b = hex3d_stiffness_bytes(info)
+    f = hex3d_flops(info)
+    fp32 = fp32_peak_tflops()
+    t_mem, t_fp = b / (peak * 1e9), f / (fp32 * 1e12)
+    target = max(t_mem, t_fp)
+    sb = hex3d_step_bytes(info)
+    line = {
+        "metric": "GLL pt-updates/s", "value": value, "unit": "GLL-point-updates/s", "n_gpus": 1,
+        "steps": K, "warmup": Wm, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded depth-gradient model with a random-field perturbation, random double couples)",
+        "config": {"workload": "3D batched elastic forward (config 5 mesh, model, shots, receivers)",
+                   "elements": [p.nx, p.ny, p.nz], "ngll": 5, "nglob": info.nglob, "nshots": info.nshots,
+                   "nreceivers": info.nreceivers, "scale": SCALE, "dt": p.dt,
+                   "l2_policy": "working set %.1f GB > 126 MB L2; no flush" % (info.device_bytes / 1e9)},
+        "roofline": {"bound": "hbm" if t_mem >= t_fp else "fp32", "kernel": "k3_stiffness",
+                     "achieved": b / (ms_stiff / 1000.0) / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": target / (ms_stiff / 1000.0),
+                     "frac_definition": "max(bytes / HBM peak, flops / FP32 peak) / measured launch time",
+                     "algorithmic_bytes_per_launch": b, "flops_per_launch": f,
+                     "fp32_peak_tflops": fp32, "achieved_tflops": f / (ms_stiff / 1000.0) / 1e12,
+                     "mean_launch_ms": ms_stiff, "peak_kind": peak_kind, "traffic": None},
+        "step_roofline": {"bound": "hbm", "algorithmic_bytes_per_step": sb,
+                          "achieved": sb / (ms / 1000.0) / 1e9, "peak": peak, "unit": "GB/s",
+                          "frac": sb / (ms / 1000.0) / 1e9 / peak,
+                          "newmark_ms": ms_newmark, "stiffness_ms": ms_stiff},
+        "e2e": {"value": pts * K / t_e2e, "unit": "GLL-point-updates/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": d2h / K,
+                "note": "K steps + all seismograms to host through sfb3_run_forward / sfb3_get_seismograms"},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+    }
+    if not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        rate, n, dt, els = hex3d_cpu_rate(args.cpu_seconds, threads)
+        line["cpu_baseline"] = {"value": rate, "unit": "GLL-point-updates/s", "cores": threads, "kind": "port",
+                                "sample": "%d steps of the 3D oracle (FP32, OpenMP) on %dx%dx%d elements of the "
+                                          "same model, one shot, %.1f s" % (n, els[0], els[1], els[2], dt)}
+    print(json.dumps(line), flush=True)
+    sim.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="coupled", choices=["coupled", "plain", "batched"])
+    ap.add_argument("--workload", default="coupled", choices=["coupled", "plain", "batched", "hex3d"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0,
                     help="length of the timed CPU-baseline sample (about 10-30 s of CPU work)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -548,6 +688,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "hex3d":
+        return run_hex3d(args)
     if args.fwi_only:
         import torch
         torch.cuda.set_device(env_int("LOCAL_RANK", 0))

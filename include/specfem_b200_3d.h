@@ -105,6 +105,13 @@ SFB_API int sfb3_get_kernels(sfb3_context *ctx, int which, double *host, size_t 
 SFB_API int sfb3_get_field(sfb3_context *ctx, int wavefield, int which, int shot, float *host, size_t count);
 /* Zero every wavefield, the seismograms and the kernels; step count 0. */
 SFB_API int sfb3_reset(sfb3_context *ctx);
+/* Stiffness / Frechet kernel variant: 0 automatic, 1 one shot per thread,
+ * 2 two shots per thread in packed FP32x2 arithmetic (the automatic choice
+ * for an even shot count), 3 the same compiled for three resident CTAs per
+ * SM.  Odd shot counts always use variant 1.  sfb3_get_variant returns the
+ * variant in use. */
+SFB_API int sfb3_set_variant(sfb3_context *ctx, int variant);
+SFB_API int sfb3_get_variant(const sfb3_context *ctx);
 /* Mean device time (ms) of `reps` launches of one kernel on the forward
  * fields: what 0 stiffness, 1 Newmark update, 2 Frechet kernels, 3 one
  * whole forward step.  The fields are left unchanged except for kind 3,

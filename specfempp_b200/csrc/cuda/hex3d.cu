@@ -163,6 +163,218 @@ __global__ void __launch_bounds__(SG * NN, 2) k3_stiffness(Dev3 d, const float *
   }
 }
 
+// ---------------------------------------------------------------------------
+// Packed variants for an even number of shots: each thread holds two
+// adjacent shots of its row and applies every per-point operation to the
+// pair with one f32x2 instruction (each lane rounds as one IEEE fma / mul /
+// add), loads and stores the pair as one float2 and adds it to the force
+// with one vector atomic.  CTA: 8 lanes x 25 rows (16 shots).
+// ---------------------------------------------------------------------------
+constexpr int PL = SG / 2;  // lanes of a row in the packed kernels
+
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 dup(float v) { return make_float2(v, v); }
+__device__ __forceinline__ float2 lds2(const float *t, int q, int c, int lane) {
+  return *reinterpret_cast<const float2 *>(t + (q * 3 + c) * SG + 2 * lane);
+}
+__device__ __forceinline__ void sts2(float *t, int q, int c, int lane, float2 v) {
+  *reinterpret_cast<float2 *>(t + (q * 3 + c) * SG + 2 * lane) = v;
+}
+
+template <int MINB>
+__global__ void __launch_bounds__(PL * NN, MINB) k3_stiffness_pk(Dev3 d, const float *__restrict__ u, float *a) {
+  extern __shared__ float smem[];
+  float *s_u = smem, *s_fy = smem + TILE, *s_fz = smem + 2 * TILE;
+  const int lane = threadIdx.x, row = threadIdx.y;
+  const int k = row / N, j = row % N;
+  const int e = blockIdx.x;
+  const int S = d.S;
+  const int s = blockIdx.y * SG + 2 * lane;  // the lane's shots s, s + 1
+  const bool act = s < S;
+  const float4 gg = d.geo[e];
+  const float2 xix = dup(gg.x), etay = dup(gg.y), gaz = dup(gg.z), jac = dup(gg.w);
+  const size_t p0 = static_cast<size_t>(e) * NNN + row * N;
+  const float2 zero = make_float2(0.f, 0.f);
+  int g[N];
+  float2 ur[N][3];
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+    g[i] = d.iglob[p0 + i];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      ur[i][c] = act ? *reinterpret_cast<const float2 *>(u + fidx(g[i], c, s, S)) : zero;
+      sts2(s_u, row * N + i, c, lane, ur[i][c]);
+    }
+  }
+  __syncthreads();
+  float2 fx[N][3];
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+    float2 dxi[3] = {zero, zero, zero}, deta[3] = {zero, zero, zero}, dzeta[3] = {zero, zero, zero};
+#pragma unroll
+    for (int l = 0; l < N; ++l) {
+      const float2 hx = dup(c3_hp[i * N + l]), hy = dup(c3_hp[j * N + l]), hz = dup(c3_hp[k * N + l]);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        dxi[c] = fma2(hx, ur[l][c], dxi[c]);
+        deta[c] = fma2(hy, lds2(s_u, (k * N + l) * N + i, c, lane), deta[c]);
+        dzeta[c] = fma2(hz, lds2(s_u, (l * N + j) * N + i, c, lane), dzeta[c]);
+      }
+    }
+    const float kap = d.kappa[p0 + i], muv = d.mu[p0 + i];
+    const float l2ms = kap + kFourThirds * muv;
+    const float2 l2m = dup(l2ms), lam = dup(l2ms - 2.0f * muv), mu = dup(muv);
+    float2 du[3][3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      du[c][0] = mul2(xix, dxi[c]);
+      du[c][1] = mul2(etay, deta[c]);
+      du[c][2] = mul2(gaz, dzeta[c]);
+    }
+    const float2 sxx = fma2(l2m, du[0][0], mul2(lam, add2(du[1][1], du[2][2])));
+    const float2 syy = fma2(l2m, du[1][1], mul2(lam, add2(du[0][0], du[2][2])));
+    const float2 szz = fma2(l2m, du[2][2], mul2(lam, add2(du[0][0], du[1][1])));
+    const float2 sxy = mul2(mu, add2(du[0][1], du[1][0]));
+    const float2 sxz = mul2(mu, add2(du[0][2], du[2][0]));
+    const float2 syz = mul2(mu, add2(du[1][2], du[2][1]));
+    const float2 T[3][3] = {{sxx, sxy, sxz}, {sxy, syy, syz}, {sxz, syz, szz}};
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      fx[i][c] = mul2(jac, mul2(T[c][0], xix));
+      sts2(s_fy, row * N + i, c, lane, mul2(jac, mul2(T[c][1], etay)));
+      sts2(s_fz, row * N + i, c, lane, mul2(jac, mul2(T[c][2], gaz)));
+    }
+  }
+  __syncthreads();
+  if (!act) return;
+  const float2 neg = dup(-1.0f);
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+    float2 t1[3] = {zero, zero, zero}, t2[3] = {zero, zero, zero}, t3[3] = {zero, zero, zero};
+#pragma unroll
+    for (int l = 0; l < N; ++l) {
+      const float2 hx = dup(c3_hpw[i * N + l]), hy = dup(c3_hpw[j * N + l]), hz = dup(c3_hpw[k * N + l]);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        t1[c] = fma2(fx[l][c], hx, t1[c]);
+        t2[c] = fma2(lds2(s_fy, (k * N + l) * N + i, c, lane), hy, t2[c]);
+        t3[c] = fma2(lds2(s_fz, (l * N + j) * N + i, c, lane), hz, t3[c]);
+      }
+    }
+    const float2 wjk = dup(c3_w[j] * c3_w[k]), wik = dup(c3_w[i] * c3_w[k]), wij = dup(c3_w[i] * c3_w[j]);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const float2 r = mul2(fma2(wjk, t1[c], fma2(wik, t2[c], mul2(wij, t3[c]))), neg);
+      atomicAdd(reinterpret_cast<float2 *>(a + fidx(g[i], c, s, S)), r);
+    }
+  }
+}
+
+// Frechet kernels, packed: the lane's two shots are summed in FP64, then
+// the 8 lanes of the row by shuffles.
+template <int MINB>
+__global__ void __launch_bounds__(PL * NN, MINB) k3_frechet_pk(Dev3 d, const float *__restrict__ au,
+                                                           const float *__restrict__ aa,
+                                                           const float *__restrict__ bu, float dt, double *kern,
+                                                           int atomic) {
+  extern __shared__ float smem[];
+  float *s_a = smem, *s_b = smem + TILE;
+  const int lane = threadIdx.x, row = threadIdx.y;
+  const int k = row / N, j = row % N;
+  const int e = blockIdx.x;
+  const int S = d.S;
+  const int s = blockIdx.y * SG + 2 * lane;
+  const bool act = s < S;
+  const float4 gg = d.geo[e];
+  const float2 xix = dup(gg.x), etay = dup(gg.y), gaz = dup(gg.z);
+  const size_t p0 = static_cast<size_t>(e) * NNN + row * N;
+  const float2 zero = make_float2(0.f, 0.f);
+  int g[N];
+  float2 ra[N][3], rb[N][3];
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+    g[i] = d.iglob[p0 + i];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      ra[i][c] = act ? *reinterpret_cast<const float2 *>(au + fidx(g[i], c, s, S)) : zero;
+      rb[i][c] = act ? *reinterpret_cast<const float2 *>(bu + fidx(g[i], c, s, S)) : zero;
+      sts2(s_a, row * N + i, c, lane, ra[i][c]);
+      sts2(s_b, row * N + i, c, lane, rb[i][c]);
+    }
+  }
+  __syncthreads();
+  // a warp holds four rows of 8 lanes
+  const unsigned seg = 0xffu << (8 * (threadIdx.y & 3));
+  double mine[2] = {0.0, 0.0};
+  const float2 half = dup(0.5f);
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+    float2 da[3][3], db[3][3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      float2 axi = zero, aeta = zero, azeta = zero, bxi = zero, beta = zero, bzeta = zero;
+#pragma unroll
+      for (int l = 0; l < N; ++l) {
+        const float2 hx = dup(c3_hp[i * N + l]), hy = dup(c3_hp[j * N + l]), hz = dup(c3_hp[k * N + l]);
+        axi = fma2(hx, ra[l][c], axi);
+        bxi = fma2(hx, rb[l][c], bxi);
+        aeta = fma2(hy, lds2(s_a, (k * N + l) * N + i, c, lane), aeta);
+        beta = fma2(hy, lds2(s_b, (k * N + l) * N + i, c, lane), beta);
+        azeta = fma2(hz, lds2(s_a, (l * N + j) * N + i, c, lane), azeta);
+        bzeta = fma2(hz, lds2(s_b, (l * N + j) * N + i, c, lane), bzeta);
+      }
+      da[c][0] = mul2(xix, axi);
+      da[c][1] = mul2(etay, aeta);
+      da[c][2] = mul2(gaz, azeta);
+      db[c][0] = mul2(xix, bxi);
+      db[c][1] = mul2(etay, beta);
+      db[c][2] = mul2(gaz, bzeta);
+    }
+    const size_t p = p0 + i;
+    const float2 diva = add2(add2(da[0][0], da[1][1]), da[2][2]);
+    const float2 divb = add2(add2(db[0][0], db[1][1]), db[2][2]);
+    float2 ee = zero;
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int x = 0; x < 3; ++x)
+        ee = fma2(mul2(half, add2(da[c][x], da[x][c])), mul2(half, add2(db[c][x], db[x][c])), ee);
+    float2 kappa_kl = mul2(diva, divb);
+    float2 mu_kl = fma2(dup(-kOneThird), kappa_kl, ee);
+    float2 rho_kl = zero;
+    if (act) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+        rho_kl = fma2(*reinterpret_cast<const float2 *>(aa + fidx(g[i], c, s, S)), rb[i][c], rho_kl);
+    }
+    kappa_kl = mul2(mul2(dup(-1.0f * d.kappa[p]), dup(dt)), kappa_kl);
+    mu_kl = mul2(mul2(dup(-2.0f * d.mu[p]), dup(dt)), mu_kl);
+    rho_kl = mul2(mul2(dup(-1.0f * d.rho[p]), dup(dt)), rho_kl);
+    double r[3] = {act ? static_cast<double>(rho_kl.x) + static_cast<double>(rho_kl.y) : 0.0,
+                   act ? static_cast<double>(mu_kl.x) + static_cast<double>(mu_kl.y) : 0.0,
+                   act ? static_cast<double>(kappa_kl.x) + static_cast<double>(kappa_kl.y) : 0.0};
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+#pragma unroll
+      for (int off = PL / 2; off > 0; off >>= 1) r[q] += __shfl_xor_sync(seg, r[q], off, PL);
+      const int v = i * 3 + q;  // value v of the row goes to lane v % 8, slot v / 8
+      if (lane == (v & (PL - 1))) mine[v / PL] = r[q];
+    }
+  }
+  // the row's 15 values: lanes 0-7 (values 0-7), lanes 0-6 (values 8-14)
+#pragma unroll
+  for (int slot = 0; slot < 2; ++slot) {
+    const int v = slot * PL + lane;
+    if (v < 3 * N) {
+      double *dst = kern + p0 * 3 + v;
+      if (atomic) atomicAdd(dst, mine[slot]);
+      else *dst += mine[slot];
+    }
+  }
+}
+
 // Stacey traction at the boundary points: a += -A v (mode 0), the same and
 // kept in `slot` (mode 1), or the kept traction (mode 2).
 __global__ void k3_stacey(const int *__restrict__ bpoint, const float *__restrict__ bdiag, const float *__restrict__ v,
@@ -490,6 +702,7 @@ struct sfb3_context {
   int seg_len = 0, nseg = 1;
   bool ckpt_host = false;
   bool fwd_final = true;       // the forward fields hold the state after `step` steps
+  int variant = 0;             // kernel variant (variant_of)
   sfb::Quadrature quad{N};
   cudaStream_t stream = nullptr;
   size_t bytes = 0, host_bytes = 0;
@@ -558,9 +771,23 @@ void locate(const sfb3_context *c, double x, double y, double z, int &e, double 
   e = (ie[2] * c->ny + ie[1]) * c->nx + ie[0];
 }
 
+// Kernel variant: packed kernels for an even shot count (pairs stay 8-byte
+// aligned), the scalar ones otherwise.  Variant 1 forces the scalar
+// kernels; 2 (default) and 3 are the packed kernels compiled for two and
+// three resident CTAs per SM.
+int variant_of(const sfb3_context *c) {
+  if (c->S % 2 != 0 || c->variant == 1) return 1;
+  return c->variant == 3 ? 3 : 2;
+}
+
 void launch_stiffness(sfb3_context *c, const float *u, float *a) {
-  dim3 grid(c->nspec, (c->S + SG - 1) / SG), block(SG, NN);
-  k3_stiffness<<<grid, block, 3 * TILE * sizeof(float), c->stream>>>(c->dev(), u, a);
+  dim3 grid(c->nspec, (c->S + SG - 1) / SG);
+  const size_t sm = 3 * TILE * sizeof(float);
+  switch (variant_of(c)) {
+    case 1: k3_stiffness<<<grid, dim3(SG, NN), sm, c->stream>>>(c->dev(), u, a); break;
+    case 3: k3_stiffness_pk<3><<<grid, dim3(PL, NN), sm, c->stream>>>(c->dev(), u, a); break;
+    default: k3_stiffness_pk<2><<<grid, dim3(PL, NN), sm, c->stream>>>(c->dev(), u, a); break;
+  }
   ++c->launches;
 }
 
@@ -613,9 +840,19 @@ void receivers(sfb3_context *c, const float *u, float *seis, int isig) {
 }
 
 void frechet(sfb3_context *c, const float *au, const float *aa, const float *bu) {
-  dim3 grid(c->nspec, (c->S + SG - 1) / SG), block(SG, NN);
-  k3_frechet<<<grid, block, 2 * TILE * sizeof(float), c->stream>>>(c->dev(), au, aa, bu, static_cast<float>(c->dt),
-                                                                     c->kern.p, grid.y > 1 ? 1 : 0);
+  dim3 grid(c->nspec, (c->S + SG - 1) / SG);
+  const size_t sm = 2 * TILE * sizeof(float);
+  const float dt = static_cast<float>(c->dt);
+  const int atomic = grid.y > 1 ? 1 : 0;
+  switch (variant_of(c)) {
+    case 1: k3_frechet<<<grid, dim3(SG, NN), sm, c->stream>>>(c->dev(), au, aa, bu, dt, c->kern.p, atomic); break;
+    case 3:
+      k3_frechet_pk<3><<<grid, dim3(PL, NN), sm, c->stream>>>(c->dev(), au, aa, bu, dt, c->kern.p, atomic);
+      break;
+    default:
+      k3_frechet_pk<2><<<grid, dim3(PL, NN), sm, c->stream>>>(c->dev(), au, aa, bu, dt, c->kern.p, atomic);
+      break;
+  }
   ++c->launches;
 }
 
@@ -725,6 +962,14 @@ SFB_API int sfb3_create(const sfb3_desc *d, sfb3_context **out) {
         "attribute");
     ck3(cudaFuncSetAttribute(k3_frechet, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * TILE * sizeof(float)),
         "attribute");
+    for (const void *f : {reinterpret_cast<const void *>(k3_stiffness_pk<2>),
+                          reinterpret_cast<const void *>(k3_stiffness_pk<3>)})
+      ck3(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 3 * TILE * sizeof(float)),
+          "attribute");
+    for (const void *f : {reinterpret_cast<const void *>(k3_frechet_pk<2>),
+                          reinterpret_cast<const void *>(k3_frechet_pk<3>)})
+      ck3(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * TILE * sizeof(float)),
+          "attribute");
     size_t *tot = &c->bytes;
     const int nspec = c->nspec;
     const size_t nloc = static_cast<size_t>(nspec) * NNN;
@@ -1127,6 +1372,14 @@ SFB_API int sfb3_reset(sfb3_context *c) {
     return SFB_OK;
   });
 }
+
+SFB_API int sfb3_set_variant(sfb3_context *c, int variant) {
+  if (!c || variant < 0 || variant > 3) return SFB_E_INVALID;
+  c->variant = variant;
+  return SFB_OK;
+}
+
+SFB_API int sfb3_get_variant(const sfb3_context *c) { return c ? variant_of(c) : SFB_E_INVALID; }
 
 SFB_API int sfb3_time_kernel(sfb3_context *c, int what, int reps, double *mean_ms) {
   if (!c || !mean_ms || reps < 1 || what < 0 || what > 3) return SFB_E_INVALID;

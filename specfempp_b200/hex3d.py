@@ -71,6 +71,8 @@ SIGNATURES3 = {
     "sfb3_get_field": (C.c_int, [_ctx, C.c_int, C.c_int, C.c_int, _f, C.c_size_t]),
     "sfb3_reset": (C.c_int, [_ctx]),
     "sfb3_time_kernel": (C.c_int, [_ctx, C.c_int, C.c_int, _d]),
+    "sfb3_set_variant": (C.c_int, [_ctx, C.c_int]),
+    "sfb3_get_variant": (C.c_int, [_ctx]),
 }
 
 _lib3 = None
@@ -348,6 +350,14 @@ class Simulation3D:
 
     def reset(self):
         _check(self._lib.sfb3_reset(self.handle), self.handle)
+
+    def set_variant(self, variant):
+        """Stiffness / Frechet kernels: 0 automatic, 1 scalar, 2 / 3 packed
+        FP32x2 (two / three resident CTAs per SM)."""
+        _check(self._lib.sfb3_set_variant(self.handle, variant), self.handle)
+
+    def variant(self):
+        return self._lib.sfb3_get_variant(self.handle)
 
     def time_kernel(self, what, reps):
         ms = C.c_double()
