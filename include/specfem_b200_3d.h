@@ -112,10 +112,11 @@ SFB_API int sfb3_reset(sfb3_context *ctx);
  * variant in use. */
 SFB_API int sfb3_set_variant(sfb3_context *ctx, int variant);
 SFB_API int sfb3_get_variant(const sfb3_context *ctx);
-/* Mean device time (ms) of `reps` launches of one kernel on the forward
- * fields: what 0 stiffness, 1 Newmark update, 2 Frechet kernels, 3 one
- * whole forward step.  The fields are left unchanged except for kind 3,
- * which advances the state. */
+/* Mean device time (ms) of `reps` launches of one kernel on a copy of the
+ * forward fields (kept in the adjoint wavefield's buffers, which it
+ * overwrites): what 0 stiffness, 1 Newmark update, 2 Frechet kernels,
+ * 4 the backward stiffness with the fused Frechet kernels (packed
+ * variants); 3 times `reps` whole forward steps, which advance the state. */
 SFB_API int sfb3_time_kernel(sfb3_context *ctx, int what, int reps, double *mean_ms);
 
 #ifdef __cplusplus

@@ -183,10 +183,68 @@ __device__ __forceinline__ void sts2(float *t, int q, int c, int lane, float2 v)
   *reinterpret_cast<float2 *>(t + (q * 3 + c) * SG + 2 * lane) = v;
 }
 
-template <int MINB>
-__global__ void __launch_bounds__(PL * NN, MINB) k3_stiffness_pk(Dev3 d, const float *__restrict__ u, float *a) {
+// Frechet accumulation fused into the backward stiffness launch of the
+// combined run: the adjoint displacement, the adjoint force of the same
+// step (complete: its stiffness, Stacey and sources launches came first)
+// and the inverse mass give the adjoint acceleration a = f M^-1 the
+// corrector would produce; the backward displacement is the launch's own.
+struct FrArgs {
+  const float *au, *af, *minv;
+  double *kern;
+  float dt;
+  int atomic;
+};
+
+// Kernels of one point for the lane's two shots, summed in FP64 over the
+// pair and the 8 lanes of the row; value v = i * 3 + q lands in lane v % 8,
+// slot v / 8 of `mine`.
+__device__ __forceinline__ void frechet_point(const float2 (&da)[3][3], const float2 (&db)[3][3], float2 rho_dot,
+                                              float kap, float muv, float rhov, float dt, bool act, int i, int lane,
+                                              unsigned seg, double (&mine)[2]) {
+  const float2 zero = make_float2(0.f, 0.f), half = dup(0.5f);
+  const float2 diva = add2(add2(da[0][0], da[1][1]), da[2][2]);
+  const float2 divb = add2(add2(db[0][0], db[1][1]), db[2][2]);
+  float2 ee = zero;
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+#pragma unroll
+    for (int x = 0; x < 3; ++x)
+      ee = fma2(mul2(half, add2(da[c][x], da[x][c])), mul2(half, add2(db[c][x], db[x][c])), ee);
+  float2 kappa_kl = mul2(diva, divb);
+  float2 mu_kl = fma2(dup(-kOneThird), kappa_kl, ee);
+  kappa_kl = mul2(mul2(dup(-1.0f * kap), dup(dt)), kappa_kl);
+  mu_kl = mul2(mul2(dup(-2.0f * muv), dup(dt)), mu_kl);
+  const float2 rho_kl = mul2(mul2(dup(-1.0f * rhov), dup(dt)), rho_dot);
+  double r[3] = {act ? static_cast<double>(rho_kl.x) + static_cast<double>(rho_kl.y) : 0.0,
+                 act ? static_cast<double>(mu_kl.x) + static_cast<double>(mu_kl.y) : 0.0,
+                 act ? static_cast<double>(kappa_kl.x) + static_cast<double>(kappa_kl.y) : 0.0};
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+#pragma unroll
+    for (int off = PL / 2; off > 0; off >>= 1) r[q] += __shfl_xor_sync(seg, r[q], off, PL);
+    const int v = i * 3 + q;
+    if (lane == (v & (PL - 1))) mine[v / PL] = r[q];
+  }
+}
+
+// The row's 15 kernel values: lanes 0-7 hold values 0-7, lanes 0-6 values 8-14.
+__device__ __forceinline__ void frechet_store(double *kern, size_t p0, int lane, const double (&mine)[2], int atomic) {
+#pragma unroll
+  for (int slot = 0; slot < 2; ++slot) {
+    const int v = slot * PL + lane;
+    if (v < 3 * N) {
+      double *dst = kern + p0 * 3 + v;
+      if (atomic) atomicAdd(dst, mine[slot]);
+      else *dst += mine[slot];
+    }
+  }
+}
+
+template <int MINB, bool FR>
+__global__ void __launch_bounds__(PL * NN, MINB) k3_stiffness_pk(Dev3 d, const float *__restrict__ u, float *a,
+                                                                 FrArgs fr) {
   extern __shared__ float smem[];
-  float *s_u = smem, *s_fy = smem + TILE, *s_fz = smem + 2 * TILE;
+  float *s_u = smem, *s_fy = smem + TILE, *s_fz = smem + 2 * TILE, *s_a = smem + 3 * TILE;
   const int lane = threadIdx.x, row = threadIdx.y;
   const int k = row / N, j = row % N;
   const int e = blockIdx.x;
@@ -206,9 +264,12 @@ __global__ void __launch_bounds__(PL * NN, MINB) k3_stiffness_pk(Dev3 d, const f
     for (int c = 0; c < 3; ++c) {
       ur[i][c] = act ? *reinterpret_cast<const float2 *>(u + fidx(g[i], c, s, S)) : zero;
       sts2(s_u, row * N + i, c, lane, ur[i][c]);
+      if (FR) sts2(s_a, row * N + i, c, lane, act ? *reinterpret_cast<const float2 *>(fr.au + fidx(g[i], c, s, S)) : zero);
     }
   }
   __syncthreads();
+  const unsigned seg = 0xffu << (8 * (threadIdx.y & 3));  // a warp holds four rows of 8 lanes
+  double mine[2] = {0.0, 0.0};
   float2 fx[N][3];
 #pragma unroll
   for (int i = 0; i < N; ++i) {
@@ -233,6 +294,34 @@ __global__ void __launch_bounds__(PL * NN, MINB) k3_stiffness_pk(Dev3 d, const f
       du[c][1] = mul2(etay, deta[c]);
       du[c][2] = mul2(gaz, dzeta[c]);
     }
+    if (FR) {
+      // the adjoint gradient at this point (all three directions from the
+      // shared tile) and the adjoint acceleration
+      float2 da[3][3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        float2 axi = zero, aeta = zero, azeta = zero;
+#pragma unroll
+        for (int l = 0; l < N; ++l) {
+          axi = fma2(dup(c3_hp[i * N + l]), lds2(s_a, (k * N + j) * N + l, c, lane), axi);
+          aeta = fma2(dup(c3_hp[j * N + l]), lds2(s_a, (k * N + l) * N + i, c, lane), aeta);
+          azeta = fma2(dup(c3_hp[k * N + l]), lds2(s_a, (l * N + j) * N + i, c, lane), azeta);
+        }
+        da[c][0] = mul2(xix, axi);
+        da[c][1] = mul2(etay, aeta);
+        da[c][2] = mul2(gaz, azeta);
+      }
+      float2 rho_dot = zero;
+      if (act) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const float m = fr.minv[static_cast<size_t>(g[i]) * 3 + c];
+          const float2 acc = mul2(*reinterpret_cast<const float2 *>(fr.af + fidx(g[i], c, s, S)), dup(m));
+          rho_dot = fma2(acc, ur[i][c], rho_dot);
+        }
+      }
+      frechet_point(da, du, rho_dot, kap, muv, d.rho[p0 + i], fr.dt, act, i, lane, seg, mine);
+    }
     const float2 sxx = fma2(l2m, du[0][0], mul2(lam, add2(du[1][1], du[2][2])));
     const float2 syy = fma2(l2m, du[1][1], mul2(lam, add2(du[0][0], du[2][2])));
     const float2 szz = fma2(l2m, du[2][2], mul2(lam, add2(du[0][0], du[1][1])));
@@ -247,6 +336,7 @@ __global__ void __launch_bounds__(PL * NN, MINB) k3_stiffness_pk(Dev3 d, const f
       sts2(s_fz, row * N + i, c, lane, mul2(jac, mul2(T[c][2], gaz)));
     }
   }
+  if (FR) frechet_store(fr.kern, p0, lane, mine, fr.atomic);
   __syncthreads();
   if (!act) return;
   const float2 neg = dup(-1.0f);
@@ -783,11 +873,23 @@ int variant_of(const sfb3_context *c) {
 void launch_stiffness(sfb3_context *c, const float *u, float *a) {
   dim3 grid(c->nspec, (c->S + SG - 1) / SG);
   const size_t sm = 3 * TILE * sizeof(float);
+  const FrArgs none{};
   switch (variant_of(c)) {
     case 1: k3_stiffness<<<grid, dim3(SG, NN), sm, c->stream>>>(c->dev(), u, a); break;
-    case 3: k3_stiffness_pk<3><<<grid, dim3(PL, NN), sm, c->stream>>>(c->dev(), u, a); break;
-    default: k3_stiffness_pk<2><<<grid, dim3(PL, NN), sm, c->stream>>>(c->dev(), u, a); break;
+    case 3: k3_stiffness_pk<3, false><<<grid, dim3(PL, NN), sm, c->stream>>>(c->dev(), u, a, none); break;
+    default: k3_stiffness_pk<2, false><<<grid, dim3(PL, NN), sm, c->stream>>>(c->dev(), u, a, none); break;
   }
+  ++c->launches;
+}
+
+// The backward stiffness with the step's Frechet kernels (packed variants):
+// au / af the adjoint displacement and complete adjoint force of the step.
+void launch_stiffness_frechet(sfb3_context *c, const float *u, float *a, const float *au, const float *af) {
+  dim3 grid(c->nspec, (c->S + SG - 1) / SG);
+  const FrArgs fr{au, af, c->minv.p, c->kern.p, static_cast<float>(c->dt), grid.y > 1 ? 1 : 0};
+  const size_t sm = 4 * TILE * sizeof(float);
+  if (variant_of(c) == 3) k3_stiffness_pk<3, true><<<grid, dim3(PL, NN), sm, c->stream>>>(c->dev(), u, a, fr);
+  else k3_stiffness_pk<2, true><<<grid, dim3(PL, NN), sm, c->stream>>>(c->dev(), u, a, fr);
   ++c->launches;
 }
 
@@ -962,9 +1064,13 @@ SFB_API int sfb3_create(const sfb3_desc *d, sfb3_context **out) {
         "attribute");
     ck3(cudaFuncSetAttribute(k3_frechet, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * TILE * sizeof(float)),
         "attribute");
-    for (const void *f : {reinterpret_cast<const void *>(k3_stiffness_pk<2>),
-                          reinterpret_cast<const void *>(k3_stiffness_pk<3>)})
+    for (const void *f : {reinterpret_cast<const void *>(k3_stiffness_pk<2, false>),
+                          reinterpret_cast<const void *>(k3_stiffness_pk<3, false>)})
       ck3(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 3 * TILE * sizeof(float)),
+          "attribute");
+    for (const void *f : {reinterpret_cast<const void *>(k3_stiffness_pk<2, true>),
+                          reinterpret_cast<const void *>(k3_stiffness_pk<3, true>)})
+      ck3(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 4 * TILE * sizeof(float)),
           "attribute");
     for (const void *f : {reinterpret_cast<const void *>(k3_frechet_pk<2>),
                           reinterpret_cast<const void *>(k3_frechet_pk<3>)})
@@ -1306,6 +1412,17 @@ SFB_API int sfb3_run_combined(sfb3_context *c) {
     // reference overwrites its first reversed step with it)
     if (c->nseg == 1) copy_wave(c, c->bwd, c->fwd);
     else checkpoint(c, c->nseg - 1, c->bwd, false);
+    // Per reversed step: adjoint predictor (+dt), adjoint sources,
+    // stiffness and Stacey; backward predictor (-dt), forward sources,
+    // stiffness, replayed tractions; correctors; the step's kernels; the
+    // backward seismogram.  With the packed kernels the kernels are added
+    // by the backward stiffness launch (from the adjoint force before its
+    // corrector) and each wavefield's corrector is fused with its next
+    // step's predictor; the first reversed step keeps the forward run's
+    // last state as the backward state (no backward step) and adds its
+    // kernels with the separate Frechet launch.
+    const bool fused = variant_of(c) != 1;
+    newmark(c, c->adj, c->dt, 0);
     int isig = 0;
     for (int seg = c->nseg - 1; seg >= 0; --seg) {
       const int s0 = seg * c->seg_len, s1 = std::min(c->nstep, s0 + c->seg_len);
@@ -1317,22 +1434,38 @@ SFB_API int sfb3_run_combined(sfb3_context *c) {
         march_forward(c, s0, s1, c->nb ? 1 : 0, s0, false);
       }
       for (int istep = s1 - 1; istep >= s0; --istep) {
-        // adjoint: +dt, adjoint sources, absorbing boundaries
-        newmark(c, c->adj, c->dt, 0);
+        const bool last = istep == 0;
         adjoint_sources(c, c->adj.a.p, istep);
         launch_stiffness(c, c->adj.u.p, c->adj.a.p);
         launch_stacey(c, c->adj.v.p, c->adj.a.p, 0, 0);
-        newmark(c, c->adj, c->dt, 1);
-        // backward: -dt, forward sources, kept tractions
-        if (istep != c->nstep - 1) {
-          newmark(c, c->bwd, -c->dt, 0);
-          forward_sources(c, c->bwd.a.p, istep);
-          launch_stiffness(c, c->bwd.u.p, c->bwd.a.p);
-          launch_stacey(c, c->bwd.v.p, c->bwd.a.p, 2, istep - s0);
-          newmark(c, c->bwd, -c->dt, 1);
+        if (istep == c->nstep - 1) {
+          newmark(c, c->adj, c->dt, 1);
+          frechet(c, c->adj.u.p, c->adj.a.p, c->bwd.u.p);
+          receivers(c, c->bwd.u.p, c->seis_b.p, isig++);
+          if (!last) {
+            newmark(c, c->adj, c->dt, 0);
+            newmark(c, c->bwd, -c->dt, 0);
+          }
+          continue;
         }
-        frechet(c, c->adj.u.p, c->adj.a.p, c->bwd.u.p);
-        receivers(c, c->bwd.u.p, c->seis_b.p, isig++);
+        forward_sources(c, c->bwd.a.p, istep);
+        if (fused) launch_stiffness_frechet(c, c->bwd.u.p, c->bwd.a.p, c->adj.u.p, c->adj.a.p);
+        else launch_stiffness(c, c->bwd.u.p, c->bwd.a.p);
+        launch_stacey(c, c->bwd.v.p, c->bwd.a.p, 2, istep - s0);
+        if (fused) {
+          receivers(c, c->bwd.u.p, c->seis_b.p, isig++);
+          newmark(c, c->adj, c->dt, last ? 1 : 2);
+          newmark(c, c->bwd, -c->dt, last ? 1 : 2);
+        } else {
+          newmark(c, c->adj, c->dt, 1);
+          newmark(c, c->bwd, -c->dt, 1);
+          frechet(c, c->adj.u.p, c->adj.a.p, c->bwd.u.p);
+          receivers(c, c->bwd.u.p, c->seis_b.p, isig++);
+          if (!last) {
+            newmark(c, c->adj, c->dt, 0);
+            newmark(c, c->bwd, -c->dt, 0);
+          }
+        }
       }
     }
     if (c->nseg > 1) {
@@ -1382,12 +1515,14 @@ SFB_API int sfb3_set_variant(sfb3_context *c, int variant) {
 SFB_API int sfb3_get_variant(const sfb3_context *c) { return c ? variant_of(c) : SFB_E_INVALID; }
 
 SFB_API int sfb3_time_kernel(sfb3_context *c, int what, int reps, double *mean_ms) {
-  if (!c || !mean_ms || reps < 1 || what < 0 || what > 3) return SFB_E_INVALID;
+  if (!c || !mean_ms || reps < 1 || what < 0 || what > 4) return SFB_E_INVALID;
   return guarded3(c, [&]() {
     if (what == 3 && (c->step + reps > c->nstep || !c->fwd_final))
       throw std::invalid_argument("the timed steps would pass the configured steps");
-    if (what == 2 && !c->kern.p) throw std::invalid_argument("the context keeps no kernels (save_boundary_values)");
-    if (what < 3) {
+    if ((what == 2 || what == 4) && !c->kern.p)
+      throw std::invalid_argument("the context keeps no kernels (save_boundary_values)");
+    if (what == 4 && variant_of(c) == 1) throw std::invalid_argument("the fused launch needs the packed kernels");
+    if (what != 3) {
       ensure_scratch(c);
       copy_wave(c, c->adj, c->fwd);
     }
@@ -1401,7 +1536,8 @@ SFB_API int sfb3_time_kernel(sfb3_context *c, int what, int reps, double *mean_m
       for (int r = 0; r < reps; ++r) {
         if (what == 0) launch_stiffness(c, c->adj.u.p, c->adj.a.p);
         else if (what == 1) newmark(c, c->adj, c->dt, 2);
-        else frechet(c, c->adj.u.p, c->adj.a.p, c->fwd.u.p);
+        else if (what == 2) frechet(c, c->adj.u.p, c->adj.a.p, c->fwd.u.p);
+        else launch_stiffness_frechet(c, c->adj.u.p, c->adj.a.p, c->fwd.u.p, c->fwd.a.p);
       }
     }
     ck3(cudaEventRecord(e1, c->stream), "event");
@@ -1411,8 +1547,8 @@ SFB_API int sfb3_time_kernel(sfb3_context *c, int what, int reps, double *mean_m
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     *mean_ms = ms / reps;
-    if (what == 2) ck3(cudaMemsetAsync(c->kern.p, 0, c->kern.n * sizeof(double), c->stream), "zero");
-    if (what < 3) zero_wave(c, c->adj);
+    if (what == 2 || what == 4) ck3(cudaMemsetAsync(c->kern.p, 0, c->kern.n * sizeof(double), c->stream), "zero");
+    if (what != 3) zero_wave(c, c->adj);
     ck3(cudaGetLastError(), "timing");
     ck3(cudaStreamSynchronize(c->stream), "timing");
     return SFB_OK;
