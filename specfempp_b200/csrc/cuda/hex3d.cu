@@ -73,6 +73,17 @@ struct Dev3 {
   const int *iglob;       // [nspec * 125]
   const float4 *geo;      // [nspec]: xix, etay, gammaz, jacobian
   const float *kappa, *mu, *rho;
+  const unsigned char *priv;  // [nspec]: 1 = the element's 27 interior points are private
+};
+
+// Forward steps: the stiffness launch finishes the private points of marked
+// elements (a = f M^-1, corrector, and unless `last` the next predictor).
+struct PrivArgs {
+  float *v;
+  const float *minv;
+  float dt, dt2, dtsq2;
+  int last;
+  int enabled;
 };
 
 __device__ __forceinline__ size_t fidx(int g, int c, int s, int S) {
@@ -176,6 +187,19 @@ __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __
 __device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
 __device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
 __device__ __forceinline__ float2 dup(float v) { return make_float2(v, v); }
+__device__ __forceinline__ void cp_async8(void *dst, const void *src) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void *dst, const void *src) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.commit_group;\ncp.async.wait_all;\n" ::: "memory"); }
+
+// Shared words of the private-point prefetch: velocity [27][3][16], inverse mass [27][3].
+constexpr int PRIV_WORDS = 27 * 3 * SG + 27 * 3;
+
 __device__ __forceinline__ float2 lds2(const float *t, int q, int c, int lane) {
   return *reinterpret_cast<const float2 *>(t + (q * 3 + c) * SG + 2 * lane);
 }
@@ -241,10 +265,11 @@ __device__ __forceinline__ void frechet_store(double *kern, size_t p0, int lane,
 }
 
 template <int MINB, bool FR>
-__global__ void __launch_bounds__(PL * NN, MINB) k3_stiffness_pk(Dev3 d, const float *__restrict__ u, float *a,
-                                                                 FrArgs fr) {
+__global__ void __launch_bounds__(PL * NN, MINB) k3_stiffness_pk(Dev3 d, const float *u, float *a, FrArgs fr,
+                                                                 PrivArgs pv) {
   extern __shared__ float smem[];
   float *s_u = smem, *s_fy = smem + TILE, *s_fz = smem + 2 * TILE, *s_a = smem + 3 * TILE;
+  float *s_pv = smem + 3 * TILE, *s_pm = s_pv + 27 * 3 * SG;  // private prefetch (not with FR)
   const int lane = threadIdx.x, row = threadIdx.y;
   const int k = row / N, j = row % N;
   const int e = blockIdx.x;
@@ -255,6 +280,7 @@ __global__ void __launch_bounds__(PL * NN, MINB) k3_stiffness_pk(Dev3 d, const f
   const float2 xix = dup(gg.x), etay = dup(gg.y), gaz = dup(gg.z), jac = dup(gg.w);
   const size_t p0 = static_cast<size_t>(e) * NNN + row * N;
   const float2 zero = make_float2(0.f, 0.f);
+  const bool private_row = !FR && pv.enabled && d.priv[e] && j >= 1 && j <= N - 2 && k >= 1 && k <= N - 2;
   int g[N];
   float2 ur[N][3];
 #pragma unroll
@@ -265,6 +291,19 @@ __global__ void __launch_bounds__(PL * NN, MINB) k3_stiffness_pk(Dev3 d, const f
       ur[i][c] = act ? *reinterpret_cast<const float2 *>(u + fidx(g[i], c, s, S)) : zero;
       sts2(s_u, row * N + i, c, lane, ur[i][c]);
       if (FR) sts2(s_a, row * N + i, c, lane, act ? *reinterpret_cast<const float2 *>(fr.au + fidx(g[i], c, s, S)) : zero);
+    }
+  }
+  if (private_row) {
+    // the private points' velocity and inverse mass, needed after the
+    // divergence: copied to shared memory while the element is computed
+#pragma unroll
+    for (int i = 1; i <= N - 2; ++i) {
+      const int pi = ((k - 1) * 3 + (j - 1)) * 3 + (i - 1);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        if (act) cp_async8(s_pv + (pi * 3 + c) * SG + 2 * lane, pv.v + fidx(g[i], c, s, S));
+        if (lane == 0) cp_async4(s_pm + pi * 3 + c, pv.minv + static_cast<size_t>(g[i]) * 3 + c);
+      }
     }
   }
   __syncthreads();
@@ -337,6 +376,7 @@ __global__ void __launch_bounds__(PL * NN, MINB) k3_stiffness_pk(Dev3 d, const f
     }
   }
   if (FR) frechet_store(fr.kern, p0, lane, mine, fr.atomic);
+  if (private_row) cp_async_wait_all();
   __syncthreads();
   if (!act) return;
   const float2 neg = dup(-1.0f);
@@ -354,11 +394,33 @@ __global__ void __launch_bounds__(PL * NN, MINB) k3_stiffness_pk(Dev3 d, const f
       }
     }
     const float2 wjk = dup(c3_w[j] * c3_w[k]), wik = dup(c3_w[i] * c3_w[k]), wij = dup(c3_w[i] * c3_w[j]);
+    float2 r[3];
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      const float2 r = mul2(fma2(wjk, t1[c], fma2(wik, t2[c], mul2(wij, t3[c]))), neg);
-      atomicAdd(reinterpret_cast<float2 *>(a + fidx(g[i], c, s, S)), r);
+    for (int c = 0; c < 3; ++c) r[c] = mul2(fma2(wjk, t1[c], fma2(wik, t2[c], mul2(wij, t3[c]))), neg);
+    if (private_row) {
+      if (i >= 1 && i <= N - 2) {
+        // a = f M^-1, corrector and next predictor in registers
+        // (newmark.tpp:44-47, 98-105); the force never reaches memory
+        const int pi = ((k - 1) * 3 + (j - 1)) * 3 + (i - 1);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const size_t at = fidx(g[i], c, s, S);
+          const float2 acc = mul2(r[c], dup(s_pm[pi * 3 + c]));
+          float2 vel = fma2(dup(pv.dt2), acc, lds2(s_pv, pi, c, lane));
+          if (pv.last) {
+            *reinterpret_cast<float2 *>(a + at) = acc;
+          } else {
+            *reinterpret_cast<float2 *>(const_cast<float *>(u) + at) =
+                add2(ur[i][c], fma2(dup(pv.dt), vel, mul2(dup(pv.dtsq2), acc)));
+            vel = fma2(dup(pv.dt2), acc, vel);
+          }
+          *reinterpret_cast<float2 *>(pv.v + at) = vel;
+        }
+        continue;
+      }
     }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) atomicAdd(reinterpret_cast<float2 *>(a + fidx(g[i], c, s, S)), r[c]);
   }
 }
 
@@ -786,6 +848,8 @@ thread_local std::string g_err3;
 struct sfb3_context {
   std::string err;
   int nx = 0, ny = 0, nz = 0, nspec = 0, nglob = 0, S = 0, nstep = 0, nrec = 0, nsrc = 0, nb = 0;
+  int nshared = 0, nprivate = 0;  // point numbering: shared points first, private points last
+  std::vector<int> perm;          // lattice index -> device point index
   double x0 = 0, y0 = 0, z0 = 0, dx = 0, dy = 0, dz = 0, dt = 0, t0 = 0;
   bool save = false;
   int step = 0;
@@ -799,6 +863,7 @@ struct sfb3_context {
   unsigned long long launches = 0;
   // mesh, model, boundary
   Buf<int> iglob, bpoint, bindex;
+  Buf<unsigned char> priv;
   Buf<float4> geo;
   Buf<float> kappa, mu, rho, bdiag, minv;
   // sources and receivers
@@ -824,6 +889,7 @@ struct sfb3_context {
     d.kappa = kappa.p;
     d.mu = mu.p;
     d.rho = rho.p;
+    d.priv = priv.p;
     return d;
   }
   ~sfb3_context() {
@@ -870,14 +936,22 @@ int variant_of(const sfb3_context *c) {
   return c->variant == 3 ? 3 : 2;
 }
 
-void launch_stiffness(sfb3_context *c, const float *u, float *a) {
+// Does the forward stiffness launch finish the private points?  (Packed
+// kernels only; otherwise the update kernel walks every point.)
+bool private_on(const sfb3_context *c) { return c->nprivate > 0 && variant_of(c) != 1; }
+
+// `pv` null: every point's force is scattered (adjoint and backward runs,
+// timing); otherwise the private points of marked elements are finished.
+void launch_stiffness(sfb3_context *c, const float *u, float *a, const PrivArgs *pv = nullptr) {
   dim3 grid(c->nspec, (c->S + SG - 1) / SG);
-  const size_t sm = 3 * TILE * sizeof(float);
+  const size_t sm = (3 * TILE + PRIV_WORDS) * sizeof(float);
   const FrArgs none{};
+  const PrivArgs off{};
+  const PrivArgs &p = (pv && private_on(c)) ? *pv : off;
   switch (variant_of(c)) {
-    case 1: k3_stiffness<<<grid, dim3(SG, NN), sm, c->stream>>>(c->dev(), u, a); break;
-    case 3: k3_stiffness_pk<3, false><<<grid, dim3(PL, NN), sm, c->stream>>>(c->dev(), u, a, none); break;
-    default: k3_stiffness_pk<2, false><<<grid, dim3(PL, NN), sm, c->stream>>>(c->dev(), u, a, none); break;
+    case 1: k3_stiffness<<<grid, dim3(SG, NN), 3 * TILE * sizeof(float), c->stream>>>(c->dev(), u, a); break;
+    case 3: k3_stiffness_pk<3, false><<<grid, dim3(PL, NN), sm, c->stream>>>(c->dev(), u, a, none, p); break;
+    default: k3_stiffness_pk<2, false><<<grid, dim3(PL, NN), sm, c->stream>>>(c->dev(), u, a, none, p); break;
   }
   ++c->launches;
 }
@@ -888,8 +962,9 @@ void launch_stiffness_frechet(sfb3_context *c, const float *u, float *a, const f
   dim3 grid(c->nspec, (c->S + SG - 1) / SG);
   const FrArgs fr{au, af, c->minv.p, c->kern.p, static_cast<float>(c->dt), grid.y > 1 ? 1 : 0};
   const size_t sm = 4 * TILE * sizeof(float);
-  if (variant_of(c) == 3) k3_stiffness_pk<3, true><<<grid, dim3(PL, NN), sm, c->stream>>>(c->dev(), u, a, fr);
-  else k3_stiffness_pk<2, true><<<grid, dim3(PL, NN), sm, c->stream>>>(c->dev(), u, a, fr);
+  const PrivArgs off{};
+  if (variant_of(c) == 3) k3_stiffness_pk<3, true><<<grid, dim3(PL, NN), sm, c->stream>>>(c->dev(), u, a, fr, off);
+  else k3_stiffness_pk<2, true><<<grid, dim3(PL, NN), sm, c->stream>>>(c->dev(), u, a, fr, off);
   ++c->launches;
 }
 
@@ -902,8 +977,10 @@ void launch_stacey(sfb3_context *c, const float *v, float *a, int mode, int slot
   ++c->launches;
 }
 
-void newmark(sfb3_context *c, Wave &w, double sdt, int mode) {
-  const size_t n = c->field_n();
+// `shared_only`: the update walks the shared points (the prefix of the
+// numbering); the forward stiffness launch finished the private ones.
+void newmark(sfb3_context *c, Wave &w, double sdt, int mode, bool shared_only = false) {
+  const size_t n = static_cast<size_t>(shared_only && private_on(c) ? c->nshared : c->nglob) * 3 * c->S;
   const float dt = static_cast<float>(sdt), dt2 = static_cast<float>(sdt / 2.0),
               dtsq2 = static_cast<float>(c->dt * c->dt / 2.0);
   if (c->S % 4 == 0) {
@@ -992,12 +1069,15 @@ void checkpoint(sfb3_context *c, int slot, Wave &w, bool save) {
 void march_forward(sfb3_context *c, int s0, int s1, int store_mode, int slot_base, bool record) {
   if (s1 <= s0) return;
   newmark(c, c->fwd, c->dt, 0);
+  PrivArgs pv{c->fwd.v.p, c->minv.p, static_cast<float>(c->dt), static_cast<float>(c->dt / 2.0),
+              static_cast<float>(c->dt * c->dt / 2.0), 0, 1};
   for (int istep = s0; istep < s1; ++istep) {
+    pv.last = istep + 1 == s1 ? 1 : 0;
     forward_sources(c, c->fwd.a.p, istep);
-    launch_stiffness(c, c->fwd.u.p, c->fwd.a.p);
+    launch_stiffness(c, c->fwd.u.p, c->fwd.a.p, &pv);
     launch_stacey(c, c->fwd.v.p, c->fwd.a.p, store_mode, istep - slot_base);
     if (record) receivers(c, c->fwd.u.p, c->seis_f.p, istep);
-    newmark(c, c->fwd, c->dt, istep + 1 == s1 ? 1 : 2);
+    newmark(c, c->fwd, c->dt, pv.last ? 1 : 2, true);
   }
 }
 
@@ -1066,7 +1146,8 @@ SFB_API int sfb3_create(const sfb3_desc *d, sfb3_context **out) {
         "attribute");
     for (const void *f : {reinterpret_cast<const void *>(k3_stiffness_pk<2, false>),
                           reinterpret_cast<const void *>(k3_stiffness_pk<3, false>)})
-      ck3(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 3 * TILE * sizeof(float)),
+      ck3(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (3 * TILE + PRIV_WORDS) * sizeof(float)),
           "attribute");
     for (const void *f : {reinterpret_cast<const void *>(k3_stiffness_pk<2, true>),
                           reinterpret_cast<const void *>(k3_stiffness_pk<3, true>)})
@@ -1152,13 +1233,10 @@ SFB_API int sfb3_create(const sfb3_desc *d, sfb3_context **out) {
     const float4 g4 = make_float4(static_cast<float>(2.0 / c->dx), static_cast<float>(2.0 / c->dy),
                                   static_cast<float>(2.0 / c->dz),
                                   static_cast<float>(c->dx * c->dy * c->dz / 8.0));
-    c->iglob.upload(iglob, tot);
     c->geo.upload(std::vector<float4>(nspec, g4), tot);
     c->kappa.upload(kap, tot);
     c->mu.upload(mu, tot);
     c->rho.upload(rho, tot);
-    c->bpoint.upload(bpoint, tot);
-    c->bindex.upload(bindex, tot);
     c->bdiag.upload(bdiag, tot);
     // sources: t0 and time shifts as io/sources.cpp:128-158 sets them
     std::vector<sfb::Source> srcs(d->nsources);
@@ -1220,6 +1298,39 @@ SFB_API int sfb3_create(const sfb3_desc *d, sfb3_context **out) {
     }
     c->rec_elem.upload(relem, tot);
     c->rec_lag.upload(rlag, tot);
+    // Element-private points: the 27 interior points of an element without
+    // sources or receivers belong to it alone; they are numbered after all
+    // shared points so that the forward update walks a prefix, and the
+    // forward stiffness launch finishes them (lattice order kept in each
+    // group).
+    {
+      std::vector<unsigned char> priv(nspec, 1);
+      for (int e : selem) priv[e] = 0;
+      for (int e : relem) priv[e] = 0;
+      std::vector<char> is_private(c->nglob, 0);
+      for (int e = 0; e < nspec; ++e) {
+        if (!priv[e]) continue;
+        for (int k = 1; k < N - 1; ++k)
+          for (int j = 1; j < N - 1; ++j)
+            for (int i = 1; i < N - 1; ++i) is_private[iglob[static_cast<size_t>(e) * NNN + (k * N + j) * N + i]] = 1;
+      }
+      c->perm.assign(c->nglob, 0);
+      int next = 0;
+      for (int g = 0; g < c->nglob; ++g)
+        if (!is_private[g]) c->perm[g] = next++;
+      c->nshared = next;
+      for (int g = 0; g < c->nglob; ++g)
+        if (is_private[g]) c->perm[g] = next++;
+      c->nprivate = c->nglob - c->nshared;
+      for (auto &g : iglob) g = c->perm[g];
+      for (auto &g : bpoint) g = c->perm[g];
+      std::vector<int> bidx(c->nglob, -1);
+      for (int g = 0; g < c->nglob; ++g) bidx[c->perm[g]] = bindex[g];
+      c->iglob.upload(iglob, tot);
+      c->bpoint.upload(bpoint, tot);
+      c->bindex.upload(bidx, tot);
+      c->priv.upload(priv, tot);
+    }
     // state
     const size_t nf = c->field_n();
     const size_t nseis = std::max<size_t>(1, static_cast<size_t>(c->nstep) * c->nrec * 3 * c->S);
@@ -1380,8 +1491,8 @@ SFB_API int sfb3_get_field(sfb3_context *c, int wavefield, int which, int shot, 
       ck3(cudaMemcpyAsync(tmp.data(), c->scratch.p, 3 * n * sizeof(float), cudaMemcpyDeviceToHost, c->stream), "d2h");
     }
     ck3(cudaStreamSynchronize(c->stream), "d2h");
-    for (size_t g = 0; g < n; ++g)
-      for (int cc = 0; cc < 3; ++cc) host[cc * n + g] = tmp[g * 3 + cc];
+    for (size_t g = 0; g < n; ++g)  // lattice order
+      for (int cc = 0; cc < 3; ++cc) host[cc * n + g] = tmp[static_cast<size_t>(c->perm[g]) * 3 + cc];
     return SFB_OK;
   });
 }
