@@ -617,6 +617,17 @@ def run_hex3d(args):
     d2h = sum(a.nbytes for a in seis)
     ms_stiff = sim.time_kernel(0, 5)
     ms_newmark = sim.time_kernel(1, 5)
+    sim.close()
+    # the gradient path: forward + combined (adjoint, backward, kernels) of
+    # all shots over a slice of the run, adjoint sources = the synthetics
+    pa = config5_problem(scale=SCALE, nstep=min(K, 100), save_boundary_values=True)
+    sa = Simulation3D(pa)
+    ms_fwd = sa.time_kernel(3, pa.nstep)
+    for s in range(info.nshots):
+        sa.set_adjoint_sources(sa.seismograms(shot=s), shot=s)
+    ms_comb = sa.time_kernel(5, 1)
+    ia = sa.info()
+    sa.close()
     peak, peak_kind = measured_peak()
     b = hex3d_stiffness_bytes(info)
     f = hex3d_flops(info)
@@ -649,6 +660,11 @@ def run_hex3d(args):
                 "note": "K steps + all seismograms to host through sfb3_run_forward / sfb3_get_seismograms"},
         "gpu_launches": int(launches),
         "clocks": clocks,
+        "adjoint": {"steps": pa.nstep, "forward_ms_per_step": ms_fwd, "combined_ms_per_step": ms_comb,
+                    "gradient_ms_per_shot_per_step": (ms_fwd + ms_comb) / info.nshots,
+                    "segments": ia.nsegments,
+                    "note": "forward then the combined run (adjoint + backward + Frechet kernels) of all "
+                            "%d shots, CUDA events" % info.nshots},
     }
     if not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -657,7 +673,6 @@ def run_hex3d(args):
                                 "sample": "%d steps of the 3D oracle (FP32, OpenMP) on %dx%dx%d elements of the "
                                           "same model, one shot, %.1f s" % (n, els[0], els[1], els[2], dt)}
     print(json.dumps(line), flush=True)
-    sim.close()
     return 0
 
 

@@ -116,7 +116,9 @@ SFB_API int sfb3_get_variant(const sfb3_context *ctx);
  * forward fields (kept in the adjoint wavefield's buffers, which it
  * overwrites): what 0 stiffness, 1 Newmark update, 2 Frechet kernels,
  * 4 the backward stiffness with the fused Frechet kernels (packed
- * variants); 3 times `reps` whole forward steps, which advance the state. */
+ * variants); 3 times `reps` whole forward steps, which advance the state;
+ * 5 runs the whole combined run (as sfb3_run_combined, `reps` ignored) and
+ * gives its mean time per step. */
 SFB_API int sfb3_time_kernel(sfb3_context *ctx, int what, int reps, double *mean_ms);
 
 #ifdef __cplusplus

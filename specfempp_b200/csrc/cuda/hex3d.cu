@@ -1096,6 +1096,78 @@ void run_forward_impl(sfb3_context *c, int nstep) {
   c->fwd_final = true;
 }
 
+// The combined run (time_marching.tpp:126-247), enqueued on the context's stream.
+void run_combined_impl(sfb3_context *c) {
+  if (!c->save) throw std::invalid_argument("the context keeps no adjoint state (save_boundary_values)");
+  if (c->step != c->nstep) throw std::invalid_argument("run the whole forward simulation first");
+  zero_wave(c, c->adj);
+  ck3(cudaMemsetAsync(c->kern.p, 0, c->kern.n * sizeof(double), c->stream), "zero");
+  // the backward wavefield starts from the forward run's last state (the
+  // reference overwrites its first reversed step with it)
+  if (c->nseg == 1) copy_wave(c, c->bwd, c->fwd);
+  else checkpoint(c, c->nseg - 1, c->bwd, false);
+  // Per reversed step: adjoint predictor (+dt), adjoint sources,
+  // stiffness and Stacey; backward predictor (-dt), forward sources,
+  // stiffness, replayed tractions; correctors; the step's kernels; the
+  // backward seismogram.  With the packed kernels the kernels are added
+  // by the backward stiffness launch (from the adjoint force before its
+  // corrector) and each wavefield's corrector is fused with its next
+  // step's predictor; the first reversed step keeps the forward run's
+  // last state as the backward state (no backward step) and adds its
+  // kernels with the separate Frechet launch.
+  const bool fused = variant_of(c) != 1;
+  newmark(c, c->adj, c->dt, 0);
+  int isig = 0;
+  for (int seg = c->nseg - 1; seg >= 0; --seg) {
+    const int s0 = seg * c->seg_len, s1 = std::min(c->nstep, s0 + c->seg_len);
+    if (c->nseg > 1) {
+      // recompute this segment's forward steps, keeping the tractions
+      if (seg == 0) zero_wave(c, c->fwd);
+      else checkpoint(c, seg - 1, c->fwd, false);
+      c->fwd_final = false;
+      march_forward(c, s0, s1, c->nb ? 1 : 0, s0, false);
+    }
+    for (int istep = s1 - 1; istep >= s0; --istep) {
+      const bool last = istep == 0;
+      adjoint_sources(c, c->adj.a.p, istep);
+      launch_stiffness(c, c->adj.u.p, c->adj.a.p);
+      launch_stacey(c, c->adj.v.p, c->adj.a.p, 0, 0);
+      if (istep == c->nstep - 1) {
+        newmark(c, c->adj, c->dt, 1);
+        frechet(c, c->adj.u.p, c->adj.a.p, c->bwd.u.p);
+        receivers(c, c->bwd.u.p, c->seis_b.p, isig++);
+        if (!last) {
+          newmark(c, c->adj, c->dt, 0);
+          newmark(c, c->bwd, -c->dt, 0);
+        }
+        continue;
+      }
+      forward_sources(c, c->bwd.a.p, istep);
+      if (fused) launch_stiffness_frechet(c, c->bwd.u.p, c->bwd.a.p, c->adj.u.p, c->adj.a.p);
+      else launch_stiffness(c, c->bwd.u.p, c->bwd.a.p);
+      launch_stacey(c, c->bwd.v.p, c->bwd.a.p, 2, istep - s0);
+      if (fused) {
+        receivers(c, c->bwd.u.p, c->seis_b.p, isig++);
+        newmark(c, c->adj, c->dt, last ? 1 : 2);
+        newmark(c, c->bwd, -c->dt, last ? 1 : 2);
+      } else {
+        newmark(c, c->adj, c->dt, 1);
+        newmark(c, c->bwd, -c->dt, 1);
+        frechet(c, c->adj.u.p, c->adj.a.p, c->bwd.u.p);
+        receivers(c, c->bwd.u.p, c->seis_b.p, isig++);
+        if (!last) {
+          newmark(c, c->adj, c->dt, 0);
+          newmark(c, c->bwd, -c->dt, 0);
+        }
+      }
+    }
+  }
+  if (c->nseg > 1) {
+    checkpoint(c, c->nseg - 1, c->fwd, false);
+    c->fwd_final = true;
+  }
+}
+
 void ensure_scratch(sfb3_context *c) {
   if (!c->adj.ready()) c->adj.alloc(c->field_n(), &c->bytes);
 }
@@ -1515,74 +1587,7 @@ SFB_API int sfb3_set_adjoint_sources(sfb3_context *c, int shot, const float *hos
 SFB_API int sfb3_run_combined(sfb3_context *c) {
   if (!c) return SFB_E_INVALID;
   return guarded3(c, [&]() {
-    if (!c->save) throw std::invalid_argument("the context keeps no adjoint state (save_boundary_values)");
-    if (c->step != c->nstep) throw std::invalid_argument("run the whole forward simulation first");
-    zero_wave(c, c->adj);
-    ck3(cudaMemsetAsync(c->kern.p, 0, c->kern.n * sizeof(double), c->stream), "zero");
-    // the backward wavefield starts from the forward run's last state (the
-    // reference overwrites its first reversed step with it)
-    if (c->nseg == 1) copy_wave(c, c->bwd, c->fwd);
-    else checkpoint(c, c->nseg - 1, c->bwd, false);
-    // Per reversed step: adjoint predictor (+dt), adjoint sources,
-    // stiffness and Stacey; backward predictor (-dt), forward sources,
-    // stiffness, replayed tractions; correctors; the step's kernels; the
-    // backward seismogram.  With the packed kernels the kernels are added
-    // by the backward stiffness launch (from the adjoint force before its
-    // corrector) and each wavefield's corrector is fused with its next
-    // step's predictor; the first reversed step keeps the forward run's
-    // last state as the backward state (no backward step) and adds its
-    // kernels with the separate Frechet launch.
-    const bool fused = variant_of(c) != 1;
-    newmark(c, c->adj, c->dt, 0);
-    int isig = 0;
-    for (int seg = c->nseg - 1; seg >= 0; --seg) {
-      const int s0 = seg * c->seg_len, s1 = std::min(c->nstep, s0 + c->seg_len);
-      if (c->nseg > 1) {
-        // recompute this segment's forward steps, keeping the tractions
-        if (seg == 0) zero_wave(c, c->fwd);
-        else checkpoint(c, seg - 1, c->fwd, false);
-        c->fwd_final = false;
-        march_forward(c, s0, s1, c->nb ? 1 : 0, s0, false);
-      }
-      for (int istep = s1 - 1; istep >= s0; --istep) {
-        const bool last = istep == 0;
-        adjoint_sources(c, c->adj.a.p, istep);
-        launch_stiffness(c, c->adj.u.p, c->adj.a.p);
-        launch_stacey(c, c->adj.v.p, c->adj.a.p, 0, 0);
-        if (istep == c->nstep - 1) {
-          newmark(c, c->adj, c->dt, 1);
-          frechet(c, c->adj.u.p, c->adj.a.p, c->bwd.u.p);
-          receivers(c, c->bwd.u.p, c->seis_b.p, isig++);
-          if (!last) {
-            newmark(c, c->adj, c->dt, 0);
-            newmark(c, c->bwd, -c->dt, 0);
-          }
-          continue;
-        }
-        forward_sources(c, c->bwd.a.p, istep);
-        if (fused) launch_stiffness_frechet(c, c->bwd.u.p, c->bwd.a.p, c->adj.u.p, c->adj.a.p);
-        else launch_stiffness(c, c->bwd.u.p, c->bwd.a.p);
-        launch_stacey(c, c->bwd.v.p, c->bwd.a.p, 2, istep - s0);
-        if (fused) {
-          receivers(c, c->bwd.u.p, c->seis_b.p, isig++);
-          newmark(c, c->adj, c->dt, last ? 1 : 2);
-          newmark(c, c->bwd, -c->dt, last ? 1 : 2);
-        } else {
-          newmark(c, c->adj, c->dt, 1);
-          newmark(c, c->bwd, -c->dt, 1);
-          frechet(c, c->adj.u.p, c->adj.a.p, c->bwd.u.p);
-          receivers(c, c->bwd.u.p, c->seis_b.p, isig++);
-          if (!last) {
-            newmark(c, c->adj, c->dt, 0);
-            newmark(c, c->bwd, -c->dt, 0);
-          }
-        }
-      }
-    }
-    if (c->nseg > 1) {
-      checkpoint(c, c->nseg - 1, c->fwd, false);
-      c->fwd_final = true;
-    }
+    run_combined_impl(c);
     ck3(cudaGetLastError(), "combined");
     ck3(cudaStreamSynchronize(c->stream), "combined");
     return SFB_OK;
@@ -1626,8 +1631,26 @@ SFB_API int sfb3_set_variant(sfb3_context *c, int variant) {
 SFB_API int sfb3_get_variant(const sfb3_context *c) { return c ? variant_of(c) : SFB_E_INVALID; }
 
 SFB_API int sfb3_time_kernel(sfb3_context *c, int what, int reps, double *mean_ms) {
-  if (!c || !mean_ms || reps < 1 || what < 0 || what > 4) return SFB_E_INVALID;
+  if (!c || !mean_ms || reps < 1 || what < 0 || what > 5) return SFB_E_INVALID;
   return guarded3(c, [&]() {
+    if (what == 5) {
+      // the whole combined run, timed on the context's stream: mean per step
+      if (!c->save || c->step != c->nstep) throw std::invalid_argument("run the whole forward simulation first");
+      cudaEvent_t e0, e1;
+      ck3(cudaEventCreate(&e0), "event");
+      ck3(cudaEventCreate(&e1), "event");
+      ck3(cudaEventRecord(e0, c->stream), "event");
+      run_combined_impl(c);
+      ck3(cudaEventRecord(e1, c->stream), "event");
+      ck3(cudaEventSynchronize(e1), "event");
+      float ms = 0.f;
+      ck3(cudaEventElapsedTime(&ms, e0, e1), "event");
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      ck3(cudaGetLastError(), "timing");
+      *mean_ms = ms / c->nstep;
+      return SFB_OK;
+    }
     if (what == 3 && (c->step + reps > c->nstep || !c->fwd_final))
       throw std::invalid_argument("the timed steps would pass the configured steps");
     if ((what == 2 || what == 4) && !c->kern.p)
