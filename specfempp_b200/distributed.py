@@ -8,9 +8,11 @@ one all-reduce of the FP64 misfit and one of the FP64 gradient at the end
 communication; the reference has no distributed solver (its MPI layer only
 wraps scalar reductions, include/specfem_mpi/specfem_mpi.hpp:44-230).
 
-`ShardedMisfit` takes a problem builder (shot list -> StructuredProblem with
-those shots renumbered 0..k-1) and a per-shard compute function; the default
-compute runs the GPU forward + combined loop of this package.
+`ShardedMisfit` takes a problem (a 2D StructuredProblem or a 3D
+HexProblem; each rank keeps its shots, renumbered 0..k-1) and a per-shard
+compute function; the default compute runs the GPU forward + combined loop
+of this package (`gpu_shard_compute`, or `gpu_shard_compute3d` for the 3D
+path).
 """
 from __future__ import annotations
 
@@ -45,11 +47,26 @@ def gpu_shard_compute(problem, model, observed):
     return float(chi.detach()), [p.grad.numpy() for p in params]
 
 
+def gpu_shard_compute3d(problem, model, observed):
+    """Misfit and gradient of one shard of a 3D problem (HexProblem, the
+    model per local point) on this rank's GPU: a batched context of the
+    shard's shots, forward and combined run (WaveformMisfit3D)."""
+    from .hex3d import Simulation3D, WaveformMisfit3D
+    rho, vp, vs = (np.asarray(a, dtype=np.float32) for a in model)
+    sim = Simulation3D(replace(problem, rho=rho, vp=vp, vs=vs, save_boundary_values=True))
+    params = [torch.tensor(np.asarray(a, dtype=np.float64), requires_grad=True) for a in model]
+    chi = WaveformMisfit3D.apply(*params, sim, np.asarray(observed, dtype=np.float64))
+    chi.backward()
+    sim.close()
+    return float(chi.detach()), [p.grad.numpy() for p in params]
+
+
 class ShardedMisfit:
     def __init__(self, problem, observed: np.ndarray,
                  compute: Callable = gpu_shard_compute, group=None, device: str = "cpu"):
-        """problem: StructuredProblem with all shots; observed: displacement
-        seismograms [nshots][nsig][nrec][2]."""
+        """problem: StructuredProblem (or HexProblem) with all shots;
+        observed: displacement seismograms [nshots][nsig][nrec][2] (3D:
+        [nshots][nstep][nrec][3])."""
         self.problem = problem
         self.observed = np.asarray(observed)
         self.compute = compute

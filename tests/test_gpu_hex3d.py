@@ -255,3 +255,21 @@ def test_kernel_variants_agree():
     odd = Simulation3D(make_problem(nshots=3))
     odd.set_variant(2)
     assert odd.variant() == 1      # odd shot counts keep the scalar kernels
+
+
+def test_sharded_misfit_3d_matches_the_oracle():
+    """The 3D per-shard GPU compute that ShardedMisfit runs on each rank
+    (gpu_shard_compute3d: batched context, forward, combined run, gradient)
+    against the FP64 oracle's misfit and gradient of the same shots."""
+    from test_distributed import oracle_shard_compute3d, setup_case3d
+    from specfempp_b200.distributed import ShardedMisfit, gpu_shard_compute3d
+    prob, model, obs = setup_case3d()
+    chi, grads = ShardedMisfit(prob, obs, compute=gpu_shard_compute3d)(model)
+    chi64, grads64 = oracle_shard_compute3d(prob, model, obs)
+    e = abs(chi - chi64) / chi64
+    print("3D sharded misfit: GPU vs FP64 oracle %.2e" % e)
+    assert e < 1e-5
+    for k, (g, g64) in enumerate(zip(grads, grads64)):
+        e = rel_l2(g, g64)
+        print("3D sharded gradient %d: GPU vs FP64 oracle %.2e" % (k, e))
+        assert e < 1e-3
