@@ -76,7 +76,11 @@ template <typename T> struct DBuf {
     n = count;
     if (count == 0) return;
     ck(cudaMalloc(&p, count * sizeof(T)), "cudaMalloc");
+    // zeroed on the legacy default stream, which the contexts' non-blocking
+    // streams do not wait for: finish it before any kernel can read the
+    // buffer (reused memory still holds a freed buffer's data)
     ck(cudaMemset(p, 0, count * sizeof(T)), "cudaMemset");
+    ck(cudaStreamSynchronize(0), "cudaMemset");
     if (total) *total += count * sizeof(T);
   }
   template <typename U> void upload(const std::vector<U> &h, size_t *total) {

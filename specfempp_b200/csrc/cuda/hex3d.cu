@@ -813,7 +813,11 @@ template <typename T> struct Buf {
       n = 0;
       throw std::runtime_error("cudaMalloc of " + std::to_string(count * sizeof(T)) + " bytes failed");
     }
+    // zeroed on the legacy default stream, which the contexts' non-blocking
+    // streams do not wait for: finish it before any kernel can read the
+    // buffer (reused memory still holds a freed buffer's data)
     ck3(cudaMemset(p, 0, count * sizeof(T)), "cudaMemset");
+    ck3(cudaStreamSynchronize(0), "cudaMemset");
     *tot += count * sizeof(T);
   }
   void upload(const std::vector<T> &h, size_t *tot) {
