@@ -51,6 +51,13 @@ def test_config5_full_size_forward_and_gradient():
     del obs_sim
     p = config5_problem()
     sim = Simulation3D(p)
+    try:
+        _full_size_run(sim, p, obs, t_setup)
+    finally:
+        sim.close()      # 181 GB of device memory, whatever the outcome
+
+
+def _full_size_run(sim, p, obs, t_setup):
     i = sim.info()
     print("config 5: nspec %d nglob %d shots %d steps %d receivers %d boundary points %d" % (
         i.nspec, i.nglob, i.nshots, i.nstep, i.nreceivers, i.nboundary_points))
