@@ -147,10 +147,12 @@ def measured_peak():
 
 
 def profiled_traffic(name, variant):
-    """DRAM bytes per launch of the dominant kernel, stiffness `variant`, from
-    the committed ncu summary (null when that variant was not captured)."""
+    """DRAM bytes per launch of the dominant kernel, stiffness `variant` (a
+    number, or a name), from the committed ncu summary (null when that
+    variant was not captured)."""
     path = os.path.join(ROOT, "profiles", name)
-    key = "dram_bytes_per_launch_full_size[variant %d]:" % variant
+    key = ("dram_bytes_per_launch_full_size[variant %d]:" % variant if isinstance(variant, int)
+           else "dram_bytes_per_launch_full_size[%s]:" % variant)
     try:
         for line in open(path):
             if line.startswith(key):
@@ -635,6 +637,9 @@ def run_hex3d(args):
     t_mem, t_fp = b / (peak * 1e9), f / (fp32 * 1e12)
     target = max(t_mem, t_fp)
     sb = hex3d_step_bytes(info)
+    traffic = profiled_traffic("stiffness_hex3d.txt", "hex3d")
+    if traffic is not None:
+        traffic *= info.nglob / 28607425.0  # the summary's figure is for the full-size mesh
     line = {
         "metric": "GLL pt-updates/s", "value": value, "unit": "GLL-point-updates/s", "n_gpus": 1,
         "steps": K, "warmup": Wm, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
@@ -650,7 +655,7 @@ def run_hex3d(args):
                      "frac_definition": "max(bytes / HBM peak, flops / FP32 peak) / measured launch time",
                      "algorithmic_bytes_per_launch": b, "flops_per_launch": f,
                      "fp32_peak_tflops": fp32, "achieved_tflops": f / (ms_stiff / 1000.0) / 1e12,
-                     "mean_launch_ms": ms_stiff, "peak_kind": peak_kind, "traffic": None},
+                     "mean_launch_ms": ms_stiff, "peak_kind": peak_kind, "traffic": traffic},
         "step_roofline": {"bound": "hbm", "algorithmic_bytes_per_step": sb,
                           "achieved": sb / (ms / 1000.0) / 1e9, "peak": peak, "unit": "GB/s",
                           "frac": sb / (ms / 1000.0) / 1e9 / peak,
