@@ -17,23 +17,36 @@
 namespace sfb {
 namespace dev {
 
-__constant__ real c_hp[64];   // hprime[i*N + j] = l_j'(xi_i)
-__constant__ real c_hpw[64];  // hprime_wgll[ix*N + l] = hprime[l*N + ix] * w[l]
-__constant__ real c_w[8];
+// GLL tables, one bank per NGLL (N = 2..8): a context writes only its own
+// NGLL's bank, so contexts of different NGLL in one process never see each
+// other's tables (contexts of the same NGLL write identical values).
+//   hprime[i*N + j] = l_j'(xi_i); hprime_wgll[ix*N + l] = hprime[l*N + ix] * w[l]
+constexpr int kQBanks = 7;
+__constant__ real c_hp_bank[kQBanks][64];
+__constant__ real c_hpw_bank[kQBanks][64];
+__constant__ real c_w_bank[kQBanks][8];
 #ifndef SFB_FP64
 // the same tables as (v, v) pairs for the packed two-shot arithmetic
-__constant__ float2 c_hp2[64];
-__constant__ float2 c_hpw2[64];
-__constant__ float2 c_w2[8];
+__constant__ float2 c_hp2_bank[kQBanks][64];
+__constant__ float2 c_hpw2_bank[kQBanks][64];
+__constant__ float2 c_w2_bank[kQBanks][8];
 #endif
+// accessors: the bank of the NGLL `N` in scope at the use
+#define C_HP(i) c_hp_bank[(N) - 2][i]
+#define C_HPW(i) c_hpw_bank[(N) - 2][i]
+#define C_W(i) c_w_bank[(N) - 2][i]
+#define C_HP2(i) c_hp2_bank[(N) - 2][i]
+#define C_HPW2(i) c_hpw2_bank[(N) - 2][i]
+#define C_W2(i) c_w2_bank[(N) - 2][i]
 
 void set_quadrature(int n, const real *hp, const real *w) {
   real hpw[64];
   for (int ix = 0; ix < n; ++ix)
     for (int l = 0; l < n; ++l) hpw[ix * n + l] = hp[l * n + ix] * w[l];
-  cudaMemcpyToSymbol(c_hp, hp, sizeof(real) * n * n);
-  cudaMemcpyToSymbol(c_hpw, hpw, sizeof(real) * n * n);
-  cudaMemcpyToSymbol(c_w, w, sizeof(real) * n);
+  const size_t b = static_cast<size_t>(n - 2);
+  cudaMemcpyToSymbol(c_hp_bank, hp, sizeof(real) * n * n, b * 64 * sizeof(real));
+  cudaMemcpyToSymbol(c_hpw_bank, hpw, sizeof(real) * n * n, b * 64 * sizeof(real));
+  cudaMemcpyToSymbol(c_w_bank, w, sizeof(real) * n, b * 8 * sizeof(real));
 #ifndef SFB_FP64
   float2 hp2[64], hpw2[64], w2[8];
   for (int k = 0; k < n * n; ++k) {
@@ -41,9 +54,9 @@ void set_quadrature(int n, const real *hp, const real *w) {
     hpw2[k] = make_float2(hpw[k], hpw[k]);
   }
   for (int k = 0; k < n; ++k) w2[k] = make_float2(w[k], w[k]);
-  cudaMemcpyToSymbol(c_hp2, hp2, sizeof(float2) * n * n);
-  cudaMemcpyToSymbol(c_hpw2, hpw2, sizeof(float2) * n * n);
-  cudaMemcpyToSymbol(c_w2, w2, sizeof(float2) * n);
+  cudaMemcpyToSymbol(c_hp2_bank, hp2, sizeof(float2) * n * n, b * 64 * sizeof(float2));
+  cudaMemcpyToSymbol(c_hpw2_bank, hpw2, sizeof(float2) * n * n, b * 64 * sizeof(float2));
+  cudaMemcpyToSymbol(c_w2_bank, w2, sizeof(float2) * n, b * 8 * sizeof(float2));
 #endif
 }
 
@@ -347,10 +360,10 @@ k_stiffness_rp(Static st, MediumFields f, int nshots, StaceyStore ss, const int 
   float hpz[N], hpwz[N];
 #pragma unroll
   for (int l = 0; l < N; ++l) {
-    hpz[l] = c_hp[iz * N + l];
-    hpwz[l] = c_hpw[iz * N + l];
+    hpz[l] = C_HP(iz * N + l);
+    hpwz[l] = C_HPW(iz * N + l);
   }
-  const float wz = c_w[iz];
+  const float wz = C_W(iz);
   stiffness_dep_start(tw);
   const int istep = (ss.mode != 0 || tw.src.n > 0) ? *istep_dev : 0;
   const V *vbase = reinterpret_cast<const V *>(f.u);
@@ -416,7 +429,7 @@ k_stiffness_rp(Static st, MediumFields f, int nshots, StaceyStore ss, const int 
           for (int c = 0; c < NC; ++c) {
             float sum = 0.f;
 #pragma unroll
-            for (int l = 0; l < N; ++l) sum += c_hp[p * N + l] * comp(colv[l], c);
+            for (int l = 0; l < N; ++l) sum += C_HP(p * N + l) * comp(colv[l], c);
             set_comp(d, c, sum);
           }
           sfg[p * N + iz] = d;
@@ -438,7 +451,7 @@ k_stiffness_rp(Static st, MediumFields f, int nshots, StaceyStore ss, const int 
 #pragma unroll
         for (int l = 0; l < N; ++l) {
 #pragma unroll
-          for (int c = 0; c < NC; ++c) dxi[c] += c_hp[ix * N + l] * comp(ur[l], c);
+          for (int c = 0; c < NC; ++c) dxi[c] += C_HP(ix * N + l) * comp(ur[l], c);
         }
         float du[NC][2];
 #pragma unroll
@@ -482,7 +495,7 @@ k_stiffness_rp(Static st, MediumFields f, int nshots, StaceyStore ss, const int 
           for (int c = 0; c < NC; ++c) {
             float sum = 0.f;
 #pragma unroll
-            for (int l = 0; l < N; ++l) sum += comp(colf[l], c) * c_hpw[p * N + l];
+            for (int l = 0; l < N; ++l) sum += comp(colf[l], c) * C_HPW(p * N + l);
             set_comp(d, c, sum);
           }
           st2[p * N + iz] = d;
@@ -499,10 +512,10 @@ k_stiffness_rp(Static st, MediumFields f, int nshots, StaceyStore ss, const int 
 #pragma unroll
         for (int l = 0; l < N; ++l) {
 #pragma unroll
-          for (int c = 0; c < NC; ++c) t1[c] += comp(fx[l], c) * c_hpw[ix * N + l];
+          for (int c = 0; c < NC; ++c) t1[c] += comp(fx[l], c) * C_HPW(ix * N + l);
         }
 #pragma unroll
-        for (int c = 0; c < NC; ++c) accr[ix][c] = (wz * t1[c] + c_w[ix] * t2[c]) * -1.0f;
+        for (int c = 0; c < NC; ++c) accr[ix][c] = (wz * t1[c] + C_W(ix) * t2[c]) * -1.0f;
       }
       if (eflag & 3) {
 #pragma unroll
@@ -688,10 +701,10 @@ k_stiffness_rpa(Static st, MediumFields f, StaceyStore ss, const int *istep_dev,
   float hpz[N], hpwz[N];
 #pragma unroll
   for (int l = 0; l < N; ++l) {
-    hpz[l] = c_hp[iz * N + l];
-    hpwz[l] = c_hpw[iz * N + l];
+    hpz[l] = C_HP(iz * N + l);
+    hpwz[l] = C_HPW(iz * N + l);
   }
-  const float wz = c_w[iz];
+  const float wz = C_W(iz);
   stiffness_dep_start(tw);
   const int istep = (ss.mode != 0 || tw.src.n > 0) ? *istep_dev : 0;
   const V *U = reinterpret_cast<const V *>(f.u);
@@ -784,7 +797,7 @@ k_stiffness_rpa(Static st, MediumFields f, StaceyStore ss, const int *istep_dev,
         for (int c = 0; c < NC; ++c) {
           float sum = 0.f;
 #pragma unroll
-          for (int l = 0; l < N; ++l) sum += c_hp[p * N + l] * comp(colv[l], c);
+          for (int l = 0; l < N; ++l) sum += C_HP(p * N + l) * comp(colv[l], c);
           set_comp(d, c, sum);
         }
         sfg[p * N + iz] = d;
@@ -803,7 +816,7 @@ k_stiffness_rpa(Static st, MediumFields f, StaceyStore ss, const int *istep_dev,
 #pragma unroll
       for (int l = 0; l < N; ++l) {
 #pragma unroll
-        for (int c = 0; c < NC; ++c) dxi[c] += c_hp[ix * N + l] * comp(ur[l], c);
+        for (int c = 0; c < NC; ++c) dxi[c] += C_HP(ix * N + l) * comp(ur[l], c);
       }
       float du[NC][2];
 #pragma unroll
@@ -848,7 +861,7 @@ k_stiffness_rpa(Static st, MediumFields f, StaceyStore ss, const int *istep_dev,
         for (int c = 0; c < NC; ++c) {
           float sum = 0.f;
 #pragma unroll
-          for (int l = 0; l < N; ++l) sum += comp(colf[l], c) * c_hpw[p * N + l];
+          for (int l = 0; l < N; ++l) sum += comp(colf[l], c) * C_HPW(p * N + l);
           set_comp(d, c, sum);
         }
         st2[p * N + iz] = d;
@@ -865,10 +878,10 @@ k_stiffness_rpa(Static st, MediumFields f, StaceyStore ss, const int *istep_dev,
 #pragma unroll
       for (int l = 0; l < N; ++l) {
 #pragma unroll
-        for (int c = 0; c < NC; ++c) t1[c] += comp(fx[l], c) * c_hpw[ix * N + l];
+        for (int c = 0; c < NC; ++c) t1[c] += comp(fx[l], c) * C_HPW(ix * N + l);
       }
 #pragma unroll
-      for (int c = 0; c < NC; ++c) accr[ix][c] = (wz * t1[c] + c_w[ix] * t2[c]) * -1.0f;
+      for (int c = 0; c < NC; ++c) accr[ix][c] = (wz * t1[c] + C_W(ix) * t2[c]) * -1.0f;
     }
     if (eflag & 3) {
 #pragma unroll
@@ -1060,10 +1073,10 @@ k_stiffness_shots(Static st, MediumFields f, int S, StaceyStore ss, const int *i
   real hpz[N], hpwz[N];
 #pragma unroll
   for (int l = 0; l < N; ++l) {
-    hpz[l] = c_hp[iz * N + l];
-    hpwz[l] = c_hpw[iz * N + l];
+    hpz[l] = C_HP(iz * N + l);
+    hpwz[l] = C_HPW(iz * N + l);
   }
-  const real wz = c_w[iz];
+  const real wz = C_W(iz);
   // u(g, s) for s = s0 .. s0+SPL-1, components interleaved: (g*S + s0)*NC floats
   const W *U = reinterpret_cast<const W *>(f.u);
   W *A = reinterpret_cast<W *>(f.a);
@@ -1092,7 +1105,7 @@ k_stiffness_shots(Static st, MediumFields f, int S, StaceyStore ss, const int *i
       const W col = s_u[(l * N + ix) * 32 + lane];
 #pragma unroll
       for (int q = 0; q < NV; ++q) {
-        dxi[q] += c_hp[ix * N + l] * vget(ur[l], q);
+        dxi[q] += C_HP(ix * N + l) * vget(ur[l], q);
         dga[q] += hpz[l] * vget(col, q);
       }
     }
@@ -1140,7 +1153,7 @@ k_stiffness_shots(Static st, MediumFields f, int S, StaceyStore ss, const int *i
       const W col = s_fg[(l * N + ix) * 32 + lane];
 #pragma unroll
       for (int q = 0; q < NV; ++q) {
-        t1[q] += vget(fx[l], q) * c_hpw[ix * N + l];
+        t1[q] += vget(fx[l], q) * C_HPW(ix * N + l);
         t2[q] += vget(col, q) * hpwz[l];
       }
     }
@@ -1149,7 +1162,7 @@ k_stiffness_shots(Static st, MediumFields f, int S, StaceyStore ss, const int *i
     for (int j = 0; j < SPL; ++j) {
       real acc[2];
 #pragma unroll
-      for (int c = 0; c < NC; ++c) acc[c] = (wz * t1[j * NC + c] + c_w[ix] * t2[j * NC + c]) * static_cast<real>(-1);
+      for (int c = 0; c < NC; ++c) acc[c] = (wz * t1[j * NC + c] + C_W(ix) * t2[j * NC + c]) * static_cast<real>(-1);
       if (eflag & 3) {
         const size_t p = (static_cast<size_t>(e) * N + iz) * N + ix;
         const uint8_t b = st.bnd[p];
@@ -1366,8 +1379,8 @@ k_stiffness_pk(Static st, MediumFields f, int S, StaceyStore ss, const int *iste
   float2 hpz[N], hpwz[N];
 #pragma unroll
   for (int l = 0; l < N; ++l) {
-    hpz[l] = c_hp2[iz * N + l];
-    hpwz[l] = c_hpw2[iz * N + l];
+    hpz[l] = C_HP2(iz * N + l);
+    hpwz[l] = C_HPW2(iz * N + l);
   }
   W fx[N];
 #pragma unroll
@@ -1381,7 +1394,7 @@ k_stiffness_pk(Static st, MediumFields f, int S, StaceyStore ss, const int *iste
       const W col = s_u[(l * N + ix) * 32 + lane];
 #pragma unroll
       for (int c = 0; c < NC; ++c) {
-        dxi[c] = fma2(c_hp2[ix * N + l], pr(ur[l], c), dxi[c]);
+        dxi[c] = fma2(C_HP2(ix * N + l), pr(ur[l], c), dxi[c]);
         dga[c] = fma2(hpz[l], pr(col, c), dga[c]);
       }
     }
@@ -1422,7 +1435,7 @@ k_stiffness_pk(Static st, MediumFields f, int S, StaceyStore ss, const int *iste
         const W col = s_ua[(l * N + ix) * 32 + lane];
 #pragma unroll
         for (int c = 0; c < 2; ++c) {
-          axi[c] = fma2(c_hp2[ix * N + l], pr(row, c), axi[c]);
+          axi[c] = fma2(C_HP2(ix * N + l), pr(row, c), axi[c]);
           aga[c] = fma2(hpz[l], pr(col, c), aga[c]);
         }
       }
@@ -1483,7 +1496,7 @@ k_stiffness_pk(Static st, MediumFields f, int S, StaceyStore ss, const int *iste
   }
   const int slot = (ss.mode != 0) ? ss.slot[e] : -1;
   if (fused) cp_async_wait_all();
-  const float2 wz = c_w2[iz];
+  const float2 wz = C_W2(iz);
   const float2 neg = make_float2(-1.0f, -1.0f);
 #pragma unroll
   for (int ix = 0; ix < N; ++ix) {
@@ -1495,13 +1508,13 @@ k_stiffness_pk(Static st, MediumFields f, int S, StaceyStore ss, const int *iste
       const W col = s_fg[(l * N + ix) * 32 + lane];
 #pragma unroll
       for (int c = 0; c < NC; ++c) {
-        t1[c] = fma2(pr(fx[l], c), c_hpw2[ix * N + l], t1[c]);
+        t1[c] = fma2(pr(fx[l], c), C_HPW2(ix * N + l), t1[c]);
         t2[c] = fma2(pr(col, c), hpwz[l], t2[c]);
       }
     }
     float2 acc[NC];
 #pragma unroll
-    for (int c = 0; c < NC; ++c) acc[c] = mul2(fma2(wz, t1[c], mul2(c_w2[ix], t2[c])), neg);
+    for (int c = 0; c < NC; ++c) acc[c] = mul2(fma2(wz, t1[c], mul2(C_W2(ix), t2[c])), neg);
     if ((eflag & 3) || slot >= 0) {
       // boundary elements: Stacey, free surface and the Stacey store, per shot
       const size_t p = (static_cast<size_t>(e) * N + iz) * N + ix;
@@ -1812,8 +1825,8 @@ __global__ void k_receivers(Static st, ReceiverSet rec, MediumFields f_psv, Medi
         real dxi[2] = {0, 0}, dga[2] = {0, 0};
         for (int l = 0; l < N; ++l)
           for (int c = 0; c < F->nc; ++c) {
-            dxi[c] += c_hp[ix * N + l] * s_val[c][iz * N + l];
-            dga[c] += c_hp[iz * N + l] * s_val[c][l * N + ix];
+            dxi[c] += C_HP(ix * N + l) * s_val[c][iz * N + l];
+            dga[c] += C_HP(iz * N + l) * s_val[c][l * N + ix];
           }
         const real xix = st.xix[p], xiz = st.xiz[p], gax = st.gax[p], gaz = st.gaz[p];
         real du[2][2];
@@ -2230,10 +2243,10 @@ k_frechet(Static st, MediumFields A, MediumFields B, int S, real dt, double *ker
       real axi = 0, aga = 0, bxi = 0, bga = 0;
 #pragma unroll
       for (int l = 0; l < N; ++l) {
-        axi += c_hp[ix * N + l] * s_a[el][c][iz * N + l];
-        aga += c_hp[iz * N + l] * s_a[el][c][l * N + ix];
-        bxi += c_hp[ix * N + l] * s_b[el][c][iz * N + l];
-        bga += c_hp[iz * N + l] * s_b[el][c][l * N + ix];
+        axi += C_HP(ix * N + l) * s_a[el][c][iz * N + l];
+        aga += C_HP(iz * N + l) * s_a[el][c][l * N + ix];
+        bxi += C_HP(ix * N + l) * s_b[el][c][iz * N + l];
+        bga += C_HP(iz * N + l) * s_b[el][c][l * N + ix];
       }
       da[c][0] = xix * axi + gax * aga;
       da[c][1] = xiz * axi + gaz * aga;
@@ -2341,7 +2354,7 @@ __global__ void k_mass(Static st, MediumFields f, int N, real dt) {
     else if (MED == MED_SH) base = st.mat1[p];                // rho
     else base = static_cast<real>(1) / st.mat1[p];            // 1 / kappa
     real mm[2];
-    for (int c = 0; c < NC; ++c) mm[c] = base * (c_w[ix] * c_w[iz] * st.jac[p]);
+    for (int c = 0; c < NC; ++c) mm[c] = base * (C_W(ix) * C_W(iz) * st.jac[p]);
     if (st.bnd[p] & 1) {
       const real hv = static_cast<real>(-1) * dt * static_cast<real>(0.5);
       const real vf[2] = {hv, hv};

@@ -103,3 +103,18 @@ def test_odd_shot_count():
     assert sim.info().stiffness_variant[0] == 3
     for s in range(3):
         seismograms_match(sim, shot=s)
+
+
+def test_contexts_of_different_ngll_interleaved():
+    """Two live contexts of different NGLL (5 and 8) in one process, their
+    steps interleaved: each keeps its own GLL tables (one constant-memory
+    bank per NGLL), so both still match the oracle."""
+    from dataclasses import replace
+    a = Simulation.structured(problem(nstep=200))
+    b = Simulation.structured(replace(problem(nstep=200), ngll=8))
+    a.run_forward(60)        # set up with NGLL 5 ...
+    b.run_forward(60)        # ... then NGLL 8 ...
+    a.run_forward(140)       # ... then NGLL 5 again
+    b.run_forward(140)
+    seismograms_match(a)
+    seismograms_match(b)
