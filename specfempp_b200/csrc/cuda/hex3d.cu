@@ -794,6 +794,11 @@ int grid_of(size_t n, int block) {
   return static_cast<int>(std::max<size_t>(1, std::min<size_t>(g, static_cast<size_t>(148) * 16)));
 }
 
+// Device or host memory that could not be had: reported as SFB_E_NOMEM.
+struct NoMemError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
 void ck3(cudaError_t e, const char *what) {
   if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
 }
@@ -811,7 +816,7 @@ template <typename T> struct Buf {
       cudaGetLastError();
       p = nullptr;
       n = 0;
-      throw std::runtime_error("cudaMalloc of " + std::to_string(count * sizeof(T)) + " bytes failed");
+      throw NoMemError("cudaMalloc of " + std::to_string(count * sizeof(T)) + " bytes failed");
     }
     // zeroed on the legacy default stream, which the contexts' non-blocking
     // streams do not wait for: finish it before any kernel can read the
@@ -912,6 +917,9 @@ template <typename F> int guarded3(sfb3_context *c, F &&fn) {
   } catch (const std::invalid_argument &e) {
     (c ? c->err : g_err3) = e.what();
     return SFB_E_INVALID;
+  } catch (const NoMemError &e) {
+    (c ? c->err : g_err3) = e.what();
+    return SFB_E_NOMEM;
   } catch (const std::exception &e) {
     (c ? c->err : g_err3) = e.what();
     return SFB_E_CUDA;
@@ -919,11 +927,17 @@ template <typename F> int guarded3(sfb3_context *c, F &&fn) {
 }
 
 // Element containing (x, y, z) and the reference coordinates there.
+// Points outside the mesh are rejected rather than extrapolated from the
+// nearest element's interpolants.
 void locate(const sfb3_context *c, double x, double y, double z, int &e, double r[3]) {
   const double v[3] = {x, y, z}, o[3] = {c->x0, c->y0, c->z0}, h[3] = {c->dx, c->dy, c->dz};
   const int n[3] = {c->nx, c->ny, c->nz};
   int ie[3];
   for (int a = 0; a < 3; ++a) {
+    const double tol = 1e-9 * h[a] * n[a];
+    if (!(v[a] >= o[a] - tol && v[a] <= o[a] + h[a] * n[a] + tol))
+      throw std::invalid_argument("point (" + std::to_string(x) + ", " + std::to_string(y) + ", " +
+                                  std::to_string(z) + ") lies outside the mesh");
     ie[a] = static_cast<int>(std::floor((v[a] - o[a]) / h[a]));
     ie[a] = std::min(std::max(ie[a], 0), n[a] - 1);
     r[a] = 2.0 * (v[a] - (o[a] + ie[a] * h[a])) / h[a] - 1.0;
@@ -1460,7 +1474,7 @@ SFB_API int sfb3_create(const sfb3_desc *d, sfb3_context **out) {
         if (len == 0) {
           host = true;
           len = static_cast<int>(std::min<size_t>(c->nstep, budget / sps));
-          if (len < 1) throw std::runtime_error("not enough device memory for one step of Stacey tractions");
+          if (len < 1) throw NoMemError("not enough device memory for one step of Stacey tractions");
         }
       }
       c->seg_len = std::max(1, len);
@@ -1477,14 +1491,14 @@ SFB_API int sfb3_create(const sfb3_desc *d, sfb3_context **out) {
           // never more than half of the host memory still available
           const double avail = static_cast<double>(sysconf(_SC_AVPHYS_PAGES)) * sysconf(_SC_PAGESIZE);
           if (static_cast<double>(nck) * sizeof(float) > 0.5 * avail)
-            throw std::runtime_error("the checkpoints (" + std::to_string(nck * sizeof(float) >> 20) +
+            throw NoMemError("the checkpoints (" + std::to_string(nck * sizeof(float) >> 20) +
                                      " MiB) need more host memory than is available");
           if (cudaHostAlloc(reinterpret_cast<void **>(&c->ckpt_host_p), nck * sizeof(float), cudaHostAllocDefault) !=
               cudaSuccess) {
             cudaGetLastError();
             c->ckpt_host_p = nullptr;
             c->ckpt_pageable = static_cast<float *>(std::malloc(nck * sizeof(float)));
-            if (!c->ckpt_pageable) throw std::runtime_error("host allocation of the checkpoints failed");
+            if (!c->ckpt_pageable) throw NoMemError("host allocation of the checkpoints failed");
           }
           c->host_bytes = nck * sizeof(float);
         } else {

@@ -273,3 +273,16 @@ def test_sharded_misfit_3d_matches_the_oracle():
         e = rel_l2(g, g64)
         print("3D sharded gradient %d: GPU vs FP64 oracle %.2e" % (k, e))
         assert e < 1e-3
+
+
+def test_points_outside_the_mesh_are_rejected():
+    from specfempp_b200 import SfbError
+    p = make_problem(nshots=2)
+    p.receivers = np.array([[300.0, 400.0, 1500.0], [2500.0, 400.0, 700.0]])
+    with pytest.raises(SfbError) as e:
+        Simulation3D(p)
+    assert e.value.code == -1 and "outside the mesh" in str(e.value)
+    q = make_problem(nshots=2)
+    q.sources[0].z = -10.0
+    with pytest.raises(SfbError):
+        Simulation3D(q)
