@@ -2462,6 +2462,9 @@ void refresh_model(sfb_context *ctx) {
   const size_t nloc = a.nloc();
   const int nn = a.ngll * a.ngll;
   if (ctx->on_device) {
+    // the copies below run on the legacy stream, which does not wait for
+    // the context's stream: let launches that read the model finish first
+    ck(cudaStreamSynchronize(ctx->stream), "sync");
     // refresh the material words of the packed and SoA device arrays
     std::vector<float> m0(nloc), m1(nloc), m2(nloc);
     std::vector<real> pack(nloc * dev::kPackFields);
