@@ -128,7 +128,7 @@ def test_config4_gradient_all_stacey():
     dev = max(abs(r[3] - 1.0) for r in rows)
     devb = max(abs(r[4] - 1.0) for r in rows)
     print("all-Stacey: largest |adjoint / FD - 1| over %d directions: reference kernels %.3e, with the Stacey "
-          "term %.3e (north-star bar 1e-3)" % (NDIR, dev, devb))
+          "term %.3e (gradient bar 1e-3)" % (NDIR, dev, devb))
     assert devb <= 1e-3
     # kernels against the FP64 build's (the reference's kernels in FP64)
     model = [a.astype(np.float32) for a in p.gll_model]

@@ -44,7 +44,7 @@ def rel_l2(a, b):
 
 def fp32_ok(label, g, o32, o64):
     e32, e64, eref = rel_l2(g, o32), rel_l2(g, o64), rel_l2(o32, o64)
-    print("%s: FP32 vs FP32 oracle %.2e (north-star bar 1e-5: %s), vs FP64 %.2e (FP32 oracle vs FP64 %.2e)"
+    print("%s: FP32 vs FP32 oracle %.2e (seismogram bar 1e-5: %s), vs FP64 %.2e (FP32 oracle vs FP64 %.2e)"
           % (label, e32, "met" if e32 <= TOL_FP32 else "not met", e64, eref))
     assert np.isfinite(g).all() and np.abs(o64).max() > 0, label
     assert e32 <= TOL_FP32 or e64 <= TOL_FP32 + 2.0 * eref, (label, e32, e64, eref)
