@@ -106,7 +106,7 @@ def test_two_rank_gloo_matches_single_process(tmp_path, native_lib, oracle_lib):
 NSTEP3 = 150
 
 
-def oracle_shard_compute3d(problem, model, observed):
+def oracle_shard_compute3d(problem, model, observed, precision=64):
     from dataclasses import replace
     from oracle import bridge3d
     from specfempp_b200.hex3d import gradients_from_kernels
@@ -115,10 +115,10 @@ def oracle_shard_compute3d(problem, model, observed):
     chi = 0.0
     k = np.zeros((p.nspec * 125, 3))
     for s in range(p.nshots):
-        fwd = bridge3d.forward(p, s, 64, threads=1)
+        fwd = bridge3d.forward(p, s, precision, threads=1)
         res = fwd["seismograms"] - observed[s]
         chi += 0.5 * float(np.sum(res * res)) * p.dt
-        bridge3d.combined(p, fwd, res, s, 64, threads=1, kernels=k)
+        bridge3d.combined(p, fwd, res, s, precision, threads=1, kernels=k)
     k = k.reshape(p.nspec, 5, 5, 5, 3)
     return chi, list(gradients_from_kernels(p, k[..., 0], k[..., 1], k[..., 2]))
 

@@ -266,9 +266,13 @@ def test_sharded_misfit_3d_matches_the_oracle():
     prob, model, obs = setup_case3d()
     chi, grads = ShardedMisfit(prob, obs, compute=gpu_shard_compute3d)(model)
     chi64, grads64 = oracle_shard_compute3d(prob, model, obs)
-    e = abs(chi - chi64) / chi64
-    print("3D sharded misfit: GPU vs FP64 oracle %.2e" % e)
-    assert e < 1e-5
+    chi32, _ = oracle_shard_compute3d(prob, model, obs, precision=32)
+    # the misfit of a small perturbation is a difference of nearly equal
+    # traces, so FP32 rounding is amplified: the suite's rule applies (1e-5,
+    # or within twice the FP32 oracle's own distance from FP64)
+    e, eref = abs(chi - chi64) / chi64, abs(chi32 - chi64) / chi64
+    print("3D sharded misfit: GPU vs FP64 oracle %.2e (FP32 oracle vs FP64 %.2e)" % (e, eref))
+    assert e <= 1e-5 or e <= 2.0 * eref + 1e-6
     for k, (g, g64) in enumerate(zip(grads, grads64)):
         e = rel_l2(g, g64)
         print("3D sharded gradient %d: GPU vs FP64 oracle %.2e" % (k, e))
