@@ -69,6 +69,11 @@ typedef struct sfb3_desc {
   int save_boundary_values;   /* allocate the adjoint / backward state */
   int segment_steps;          /* steps per segment; 0 = as many as fit */
   int host_checkpoints;       /* 1: keep checkpoints in pinned host memory */
+  int deterministic;          /* 1: bit-reproducible runs (element colours:
+                                 one stiffness launch per colour of
+                                 hexahedra sharing no point, plain adds;
+                                 sources, adjoint sources and mass in a
+                                 fixed order) */
 } sfb3_desc;
 
 typedef struct sfb3_info {

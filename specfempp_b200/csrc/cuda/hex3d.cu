@@ -74,7 +74,15 @@ struct Dev3 {
   const float4 *geo;      // [nspec]: xix, etay, gammaz, jacobian
   const float *kappa, *mu, *rho;
   const unsigned char *priv;  // [nspec]: 1 = the element's 27 interior points are private
+  // Deterministic mode: a launch covers one colour of elements (elist[elist_off
+  // + blockIdx.x]; no two elements of a colour share a point) and one group
+  // of 16 shots (sgroup + blockIdx.y), and scatters with plain adds.
+  const int *elist;
+  int elist_off, sgroup, det;
 };
+
+__device__ __forceinline__ int elem_of(const Dev3 &d) { return d.elist ? d.elist[d.elist_off + blockIdx.x] : blockIdx.x; }
+__device__ __forceinline__ int group_of(const Dev3 &d) { return d.sgroup + blockIdx.y; }
 
 // Forward steps: the stiffness launch finishes the private points of marked
 // elements (a = f M^-1, corrector, and unless `last` the next predictor).
@@ -96,9 +104,9 @@ __global__ void __launch_bounds__(SG * NN, 2) k3_stiffness(Dev3 d, const float *
   float *s_u = smem, *s_fy = smem + TILE, *s_fz = smem + 2 * TILE;
   const int lane = threadIdx.x, row = threadIdx.y;  // row = k * 5 + j
   const int k = row / N, j = row % N;
-  const int e = blockIdx.x;
+  const int e = elem_of(d);
   const int S = d.S;
-  const int s = blockIdx.y * SG + lane;
+  const int s = group_of(d) * SG + lane;
   const bool act = s < S;
   const float4 gg = d.geo[e];
   const float xix = gg.x, etay = gg.y, gaz = gg.z, jac = gg.w;
@@ -170,7 +178,11 @@ __global__ void __launch_bounds__(SG * NN, 2) k3_stiffness(Dev3 d, const float *
     }
     const float wjk = c3_w[j] * c3_w[k], wik = c3_w[i] * c3_w[k], wij = c3_w[i] * c3_w[j];
 #pragma unroll
-    for (int c = 0; c < 3; ++c) atomicAdd(a + fidx(g[i], c, s, S), (wjk * t1[c] + wik * t2[c] + wij * t3[c]) * -1.0f);
+    for (int c = 0; c < 3; ++c) {
+      const float r = (wjk * t1[c] + wik * t2[c] + wij * t3[c]) * -1.0f;
+      if (d.det) a[fidx(g[i], c, s, S)] += r;
+      else atomicAdd(a + fidx(g[i], c, s, S), r);
+    }
   }
 }
 
@@ -272,9 +284,9 @@ __global__ void __launch_bounds__(PL * NN, MINB) k3_stiffness_pk(Dev3 d, const f
   float *s_pv = smem + 3 * TILE, *s_pm = s_pv + 27 * 3 * SG;  // private prefetch (not with FR)
   const int lane = threadIdx.x, row = threadIdx.y;
   const int k = row / N, j = row % N;
-  const int e = blockIdx.x;
+  const int e = elem_of(d);
   const int S = d.S;
-  const int s = blockIdx.y * SG + 2 * lane;  // the lane's shots s, s + 1
+  const int s = group_of(d) * SG + 2 * lane;  // the lane's shots s, s + 1
   const bool act = s < S;
   const float4 gg = d.geo[e];
   const float2 xix = dup(gg.x), etay = dup(gg.y), gaz = dup(gg.z), jac = dup(gg.w);
@@ -420,7 +432,11 @@ __global__ void __launch_bounds__(PL * NN, MINB) k3_stiffness_pk(Dev3 d, const f
       }
     }
 #pragma unroll
-    for (int c = 0; c < 3; ++c) atomicAdd(reinterpret_cast<float2 *>(a + fidx(g[i], c, s, S)), r[c]);
+    for (int c = 0; c < 3; ++c) {
+      float2 *dst = reinterpret_cast<float2 *>(a + fidx(g[i], c, s, S));
+      if (d.det) *dst = add2(*dst, r[c]);
+      else atomicAdd(dst, r[c]);
+    }
   }
 }
 
@@ -435,9 +451,9 @@ __global__ void __launch_bounds__(PL * NN, MINB) k3_frechet_pk(Dev3 d, const flo
   float *s_a = smem, *s_b = smem + TILE;
   const int lane = threadIdx.x, row = threadIdx.y;
   const int k = row / N, j = row % N;
-  const int e = blockIdx.x;
+  const int e = elem_of(d);
   const int S = d.S;
-  const int s = blockIdx.y * SG + 2 * lane;
+  const int s = group_of(d) * SG + 2 * lane;
   const bool act = s < S;
   const float4 gg = d.geo[e];
   const float2 xix = dup(gg.x), etay = dup(gg.y), gaz = dup(gg.z);
@@ -661,14 +677,60 @@ __global__ void k3_newmark_scalar(float *u, float *v, float *a, const float *__r
 }
 
 // Mass matrix: rho w_i w_j w_k J per local point, FP64 accumulation.
-__global__ void k3_mass(Dev3 d, double *mass) {
-  const size_t total = static_cast<size_t>(d.nspec) * NNN;
+// `count` elements: all of them, or (deterministic mode) one colour of
+// d.elist, whose points no other element of the launch shares (plain adds).
+__global__ void k3_mass(Dev3 d, double *mass, int count) {
+  const size_t total = static_cast<size_t>(count) * NNN;
   for (size_t t = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; t < total;
        t += static_cast<size_t>(gridDim.x) * blockDim.x) {
-    const int e = static_cast<int>(t / NNN), q = static_cast<int>(t % NNN);
+    const int le = static_cast<int>(t / NNN), q = static_cast<int>(t % NNN);
+    const int e = d.elist ? d.elist[d.elist_off + le] : le;
     const int k = q / NN, j = (q / N) % N, i = q % N;
-    const float m = d.rho[t] * (c3_w[i] * c3_w[j] * c3_w[k] * d.geo[e].w);
-    atomicAdd(mass + d.iglob[t], static_cast<double>(m));
+    const size_t p = static_cast<size_t>(e) * NNN + q;
+    const float m = d.rho[p] * (c3_w[i] * c3_w[j] * c3_w[k] * d.geo[e].w);
+    if (d.det) mass[d.iglob[p]] += static_cast<double>(m);
+    else atomicAdd(mass + d.iglob[p], static_cast<double>(m));
+  }
+}
+
+// Point sources one after another (deterministic mode): one CTA, thread q
+// = local point.
+__global__ void k3_sources_det(Dev3 d, int nsrc, const int *elem, const int *shot, const float *array,
+                               const float *stf, int nstep, float *a, int istep) {
+  const int q = threadIdx.x;
+  for (int i = 0; i < nsrc; ++i) {
+    if (q < NNN) {
+      const int g = d.iglob[static_cast<size_t>(elem[i]) * NNN + q];
+      const float f = stf[static_cast<size_t>(i) * nstep + istep];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) a[fidx(g, c, shot[i], d.S)] += f * array[(static_cast<size_t>(i) * 3 + c) * NNN + q];
+    }
+    __syncthreads();
+  }
+}
+
+// Adjoint sources one receiver after another (deterministic mode): one CTA
+// per group of 16 shots, thread (lane, row) over five points.
+__global__ void __launch_bounds__(SG * NN) k3_adjoint_sources_det(Dev3 d, int nrec, const int *relem,
+                                                                  const float *rlag, const float *stf, float *a,
+                                                                  int istep) {
+  const int lane = threadIdx.x, row = threadIdx.y;
+  const int S = d.S;
+  const int s = blockIdx.x * SG + lane;
+  for (int r = 0; r < nrec; ++r) {
+    if (s < S) {
+      const size_t at = (static_cast<size_t>(istep) * nrec + r) * 3 * S;
+      const float f[3] = {stf[at + s], stf[at + S + s], stf[at + 2 * S + s]};
+      const size_t p0 = static_cast<size_t>(relem[r]) * NNN + row * N;
+#pragma unroll
+      for (int i = 0; i < N; ++i) {
+        const int g = d.iglob[p0 + i];
+        const float h = rlag[static_cast<size_t>(r) * NNN + row * N + i];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) a[fidx(g, c, s, S)] += f[c] * h;
+      }
+    }
+    __syncthreads();
   }
 }
 
@@ -695,9 +757,9 @@ __global__ void __launch_bounds__(SG * NN, 2) k3_frechet(Dev3 d, const float *__
   float *s_a = smem, *s_b = smem + TILE;
   const int lane = threadIdx.x, row = threadIdx.y;
   const int k = row / N, j = row % N;
-  const int e = blockIdx.x;
+  const int e = elem_of(d);
   const int S = d.S;
-  const int s = blockIdx.y * SG + lane;
+  const int s = group_of(d) * SG + lane;
   const bool act = s < S;
   const float4 gg = d.geo[e];
   const float xix = gg.x, etay = gg.y, gaz = gg.z;
@@ -866,6 +928,8 @@ struct sfb3_context {
   bool ckpt_host = false;
   bool fwd_final = true;       // the forward fields hold the state after `step` steps
   int variant = 0;             // kernel variant (variant_of)
+  bool det = false;            // deterministic assembly (colour launches, fixed-order sums)
+  int col_off[9] = {0};        // elements of colour c: elist[col_off[c], col_off[c + 1])
   sfb::Quadrature quad{N};
   cudaStream_t stream = nullptr;
   size_t bytes = 0, host_bytes = 0;
@@ -873,6 +937,7 @@ struct sfb3_context {
   // mesh, model, boundary
   Buf<int> iglob, bpoint, bindex;
   Buf<unsigned char> priv;
+  Buf<int> elist;
   Buf<float4> geo;
   Buf<float> kappa, mu, rho, bdiag, minv;
   // sources and receivers
@@ -899,6 +964,7 @@ struct sfb3_context {
     d.mu = mu.p;
     d.rho = rho.p;
     d.priv = priv.p;
+    d.det = det ? 1 : 0;
     return d;
   }
   ~sfb3_context() {
@@ -960,30 +1026,56 @@ bool private_on(const sfb3_context *c) { return c->nprivate > 0 && variant_of(c)
 
 // `pv` null: every point's force is scattered (adjoint and backward runs,
 // timing); otherwise the private points of marked elements are finished.
+// The element kernels' launches: one over all elements and shot groups, or
+// in the deterministic mode one per shot group and element colour (group
+// outer, colours 0-7 inner), so that every point's sum is taken in the same
+// order on every run.  `launch(d, grid)` issues one launch.
+template <typename F> void element_launches(sfb3_context *c, F &&launch) {
+  const int groups = (c->S + SG - 1) / SG;
+  Dev3 d = c->dev();
+  if (!c->det) {
+    launch(d, dim3(c->nspec, groups));
+    return;
+  }
+  d.elist = c->elist.p;
+  for (int g = 0; g < groups; ++g)
+    for (int col = 0; col < 8; ++col) {
+      const int n = c->col_off[col + 1] - c->col_off[col];
+      if (n == 0) continue;
+      d.elist_off = c->col_off[col];
+      d.sgroup = g;
+      launch(d, dim3(n, 1));
+    }
+}
+
 void launch_stiffness(sfb3_context *c, const float *u, float *a, const PrivArgs *pv = nullptr) {
-  dim3 grid(c->nspec, (c->S + SG - 1) / SG);
   const size_t sm = (3 * TILE + PRIV_WORDS) * sizeof(float);
   const FrArgs none{};
   const PrivArgs off{};
   const PrivArgs &p = (pv && private_on(c)) ? *pv : off;
-  switch (variant_of(c)) {
-    case 1: k3_stiffness<<<grid, dim3(SG, NN), 3 * TILE * sizeof(float), c->stream>>>(c->dev(), u, a); break;
-    case 3: k3_stiffness_pk<3, false><<<grid, dim3(PL, NN), sm, c->stream>>>(c->dev(), u, a, none, p); break;
-    default: k3_stiffness_pk<2, false><<<grid, dim3(PL, NN), sm, c->stream>>>(c->dev(), u, a, none, p); break;
-  }
-  ++c->launches;
+  const int v = variant_of(c);
+  element_launches(c, [&](const Dev3 &d, dim3 grid) {
+    switch (v) {
+      case 1: k3_stiffness<<<grid, dim3(SG, NN), 3 * TILE * sizeof(float), c->stream>>>(d, u, a); break;
+      case 3: k3_stiffness_pk<3, false><<<grid, dim3(PL, NN), sm, c->stream>>>(d, u, a, none, p); break;
+      default: k3_stiffness_pk<2, false><<<grid, dim3(PL, NN), sm, c->stream>>>(d, u, a, none, p); break;
+    }
+    ++c->launches;
+  });
 }
 
 // The backward stiffness with the step's Frechet kernels (packed variants):
 // au / af the adjoint displacement and complete adjoint force of the step.
 void launch_stiffness_frechet(sfb3_context *c, const float *u, float *a, const float *au, const float *af) {
-  dim3 grid(c->nspec, (c->S + SG - 1) / SG);
-  const FrArgs fr{au, af, c->minv.p, c->kern.p, static_cast<float>(c->dt), grid.y > 1 ? 1 : 0};
   const size_t sm = 4 * TILE * sizeof(float);
   const PrivArgs off{};
-  if (variant_of(c) == 3) k3_stiffness_pk<3, true><<<grid, dim3(PL, NN), sm, c->stream>>>(c->dev(), u, a, fr, off);
-  else k3_stiffness_pk<2, true><<<grid, dim3(PL, NN), sm, c->stream>>>(c->dev(), u, a, fr, off);
-  ++c->launches;
+  const int v = variant_of(c);
+  element_launches(c, [&](const Dev3 &d, dim3 grid) {
+    const FrArgs fr{au, af, c->minv.p, c->kern.p, static_cast<float>(c->dt), grid.y > 1 ? 1 : 0};
+    if (v == 3) k3_stiffness_pk<3, true><<<grid, dim3(PL, NN), sm, c->stream>>>(d, u, a, fr, off);
+    else k3_stiffness_pk<2, true><<<grid, dim3(PL, NN), sm, c->stream>>>(d, u, a, fr, off);
+    ++c->launches;
+  });
 }
 
 void launch_stacey(sfb3_context *c, const float *v, float *a, int mode, int slot) {
@@ -1017,15 +1109,23 @@ void newmark(sfb3_context *c, Wave &w, double sdt, int mode, bool shared_only = 
 
 void forward_sources(sfb3_context *c, float *a, int istep) {
   if (c->nsrc == 0) return;
-  k3_sources<<<c->nsrc, 128, 0, c->stream>>>(c->dev(), c->nsrc, c->src_elem.p, c->src_shot.p, c->src_array.p,
+  if (c->det)
+    k3_sources_det<<<1, 128, 0, c->stream>>>(c->dev(), c->nsrc, c->src_elem.p, c->src_shot.p, c->src_array.p,
                                               c->src_stf.p, c->nstep, a, istep);
+  else
+    k3_sources<<<c->nsrc, 128, 0, c->stream>>>(c->dev(), c->nsrc, c->src_elem.p, c->src_shot.p, c->src_array.p,
+                                                c->src_stf.p, c->nstep, a, istep);
   ++c->launches;
 }
 
 void adjoint_sources(sfb3_context *c, float *a, int istep) {
   if (c->nrec == 0) return;
-  k3_adjoint_sources<<<dim3(c->nrec, (c->S + SG - 1) / SG), dim3(SG, NN), 0, c->stream>>>(
-      c->dev(), c->nrec, c->rec_elem.p, c->rec_lag.p, c->adj_stf.p, a, istep);
+  if (c->det)
+    k3_adjoint_sources_det<<<(c->S + SG - 1) / SG, dim3(SG, NN), 0, c->stream>>>(
+        c->dev(), c->nrec, c->rec_elem.p, c->rec_lag.p, c->adj_stf.p, a, istep);
+  else
+    k3_adjoint_sources<<<dim3(c->nrec, (c->S + SG - 1) / SG), dim3(SG, NN), 0, c->stream>>>(
+        c->dev(), c->nrec, c->rec_elem.p, c->rec_lag.p, c->adj_stf.p, a, istep);
   ++c->launches;
 }
 
@@ -1037,20 +1137,18 @@ void receivers(sfb3_context *c, const float *u, float *seis, int isig) {
 }
 
 void frechet(sfb3_context *c, const float *au, const float *aa, const float *bu) {
-  dim3 grid(c->nspec, (c->S + SG - 1) / SG);
   const size_t sm = 2 * TILE * sizeof(float);
   const float dt = static_cast<float>(c->dt);
-  const int atomic = grid.y > 1 ? 1 : 0;
-  switch (variant_of(c)) {
-    case 1: k3_frechet<<<grid, dim3(SG, NN), sm, c->stream>>>(c->dev(), au, aa, bu, dt, c->kern.p, atomic); break;
-    case 3:
-      k3_frechet_pk<3><<<grid, dim3(PL, NN), sm, c->stream>>>(c->dev(), au, aa, bu, dt, c->kern.p, atomic);
-      break;
-    default:
-      k3_frechet_pk<2><<<grid, dim3(PL, NN), sm, c->stream>>>(c->dev(), au, aa, bu, dt, c->kern.p, atomic);
-      break;
-  }
-  ++c->launches;
+  const int v = variant_of(c);
+  element_launches(c, [&](const Dev3 &d, dim3 grid) {
+    const int atomic = grid.y > 1 ? 1 : 0;
+    switch (v) {
+      case 1: k3_frechet<<<grid, dim3(SG, NN), sm, c->stream>>>(d, au, aa, bu, dt, c->kern.p, atomic); break;
+      case 3: k3_frechet_pk<3><<<grid, dim3(PL, NN), sm, c->stream>>>(d, au, aa, bu, dt, c->kern.p, atomic); break;
+      default: k3_frechet_pk<2><<<grid, dim3(PL, NN), sm, c->stream>>>(d, au, aa, bu, dt, c->kern.p, atomic); break;
+    }
+    ++c->launches;
+  });
 }
 
 void copy_wave(sfb3_context *c, Wave &dst, const Wave &src) {
@@ -1229,6 +1327,7 @@ SFB_API int sfb3_create(const sfb3_desc *d, sfb3_context **out) {
     c->save = d->save_boundary_values != 0;
     c->nrec = d->nreceivers;
     c->nsrc = d->nsources;
+    c->det = d->deterministic != 0;
     ck3(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "stream");
     ck3(cudaFuncSetAttribute(k3_stiffness, cudaFuncAttributeMaxDynamicSharedMemorySize, 3 * TILE * sizeof(float)),
         "attribute");
@@ -1417,6 +1516,18 @@ SFB_API int sfb3_create(const sfb3_desc *d, sfb3_context **out) {
       std::vector<int> bidx(c->nglob, -1);
       for (int g = 0; g < c->nglob; ++g) bidx[c->perm[g]] = bindex[g];
       c->iglob.upload(iglob, tot);
+      // element colours by coordinate parity: hexahedra of one colour share
+      // no point (deterministic mode)
+      std::vector<int> el;
+      el.reserve(nspec);
+      c->col_off[0] = 0;
+      for (int col = 0; col < 8; ++col) {
+        for (int ez = col >> 2 & 1; ez < d->nz; ez += 2)
+          for (int ey = col >> 1 & 1; ey < d->ny; ey += 2)
+            for (int ex = col & 1; ex < d->nx; ex += 2) el.push_back((ez * d->ny + ey) * d->nx + ex);
+        c->col_off[col + 1] = static_cast<int>(el.size());
+      }
+      c->elist.upload(el, tot);
       c->bpoint.upload(bpoint, tot);
       c->bindex.upload(bidx, tot);
       c->priv.upload(priv, tot);
@@ -1434,10 +1545,24 @@ SFB_API int sfb3_create(const sfb3_desc *d, sfb3_context **out) {
       Buf<double> mass;
       size_t tmp = 0;
       mass.alloc(c->nglob, &tmp);
-      k3_mass<<<grid_of(nloc, 256), 256, 0, c->stream>>>(c->dev(), mass.p);
+      if (c->det) {
+        // colour by colour: each point's terms added in the same order
+        Dev3 dd = c->dev();
+        dd.elist = c->elist.p;
+        for (int col = 0; col < 8; ++col) {
+          const int n = c->col_off[col + 1] - c->col_off[col];
+          if (n == 0) continue;
+          dd.elist_off = c->col_off[col];
+          k3_mass<<<grid_of(static_cast<size_t>(n) * NNN, 256), 256, 0, c->stream>>>(dd, mass.p, n);
+          ++c->launches;
+        }
+      } else {
+        k3_mass<<<grid_of(nloc, 256), 256, 0, c->stream>>>(c->dev(), mass.p, nspec);
+        ++c->launches;
+      }
       k3_invert<<<grid_of(static_cast<size_t>(c->nglob) * 3, 256), 256, 0, c->stream>>>(
           mass.p, c->bindex.p, c->bdiag.p, static_cast<float>(c->dt), c->minv.p, c->nglob);
-      c->launches += 2;
+      ++c->launches;
       ck3(cudaGetLastError(), "mass");
       ck3(cudaStreamSynchronize(c->stream), "mass");
     }

@@ -44,7 +44,8 @@ class sfb3_desc(C.Structure):
                 ("dt", C.c_double), ("nstep", C.c_int), ("nshots", C.c_int),
                 ("nsources", C.c_int), ("sources", C.POINTER(sfb3_source)),
                 ("nreceivers", C.c_int), ("receivers", C.POINTER(C.c_double)),
-                ("save_boundary_values", C.c_int), ("segment_steps", C.c_int), ("host_checkpoints", C.c_int)]
+                ("save_boundary_values", C.c_int), ("segment_steps", C.c_int), ("host_checkpoints", C.c_int),
+                ("deterministic", C.c_int)]
 
 
 class sfb3_info(C.Structure):
@@ -140,6 +141,7 @@ class HexProblem:
     save_boundary_values: bool = False
     segment_steps: int = 0
     host_checkpoints: bool = False
+    deterministic: bool = False
 
     @property
     def nspec(self):
@@ -164,7 +166,7 @@ class HexProblem:
                       keep["rho"].ctypes.data_as(_f), keep["vp"].ctypes.data_as(_f), keep["vs"].ctypes.data_as(_f),
                       self.dt, self.nstep, self.nshots, len(self.sources), srcs, rec.shape[0],
                       rec.ctypes.data_as(_d), int(self.save_boundary_values), int(self.segment_steps),
-                      int(self.host_checkpoints))
+                      int(self.host_checkpoints), int(self.deterministic))
         return d, keep
 
 
