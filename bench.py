@@ -620,6 +620,13 @@ def run_hex3d(args):
     ms_stiff = sim.time_kernel(0, 5)
     ms_newmark = sim.time_kernel(1, 5)
     sim.close()
+    # the deterministic assembly (element colours, fixed-order sums) on the
+    # same workload
+    pd = config5_problem(scale=SCALE, nstep=Wm + min(K, 20) + 1, save_boundary_values=False, deterministic=True)
+    sd = Simulation3D(pd)
+    sd.run_forward(Wm)
+    ms_det = sd.time_kernel(3, min(K, 20))
+    sd.close()
     # the gradient path: forward + combined (adjoint, backward, kernels) of
     # all shots over a slice of the run, adjoint sources = the synthetics
     pa = config5_problem(scale=SCALE, nstep=min(K, 100), save_boundary_values=True)
@@ -665,6 +672,8 @@ def run_hex3d(args):
                 "note": "K steps + all seismograms to host through sfb3_run_forward / sfb3_get_seismograms"},
         "gpu_launches": int(launches),
         "clocks": clocks,
+        "deterministic": {"ms_per_step": ms_det, "value": pts / (ms_det / 1000.0), "unit": "GLL-point-updates/s",
+                          "steps": min(K, 20), "note": "bit-reproducible assembly (element colours) on the same workload"},
         "adjoint": {"steps": pa.nstep, "forward_ms_per_step": ms_fwd, "combined_ms_per_step": ms_comb,
                     "gradient_ms_per_shot_per_step": (ms_fwd + ms_comb) / info.nshots,
                     "segments": ia.nsegments,
